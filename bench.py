@@ -1,0 +1,493 @@
+#!/usr/bin/env python
+"""Headline benchmark: FEM system assembly on one B200 (matrix nnz/s).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload p2|p1|p1big|vp2] [--variant atomic|deterministic]
+
+Default workload (the configuration the headline metric is quoted on): P2
+Poisson on the unit cube, 96^3 hexes x 6 = 5,308,416 tets, 7,189,057 dofs,
+nnz 204,763,393, k a P1 field with log k ~ N(0,1) per vertex, f DG0 ~ U[-1,1],
+Dirichlet g = x+y+z on the whole boundary with lifting; FP64.
+
+One step = zero A, assemble A with BC rows/cols skipped and unit diagonal,
+assemble b, apply lifting, set_bc (the five calls of the reference's
+examples/poisson.py timing loop).  ``value`` = nnz per second of whole steps
+with all inputs resident in HBM (CUDA events on the launching stream, max over
+ranks); ``e2e`` = the same through the public Python API with host buffers:
+the coefficient upload (H2D, pinned) that the reference performs on every
+assemble call and the read-back of b (D2H) are inside the timed region.
+The CSR value array (1.64 GB) exceeds the 126 MB L2, so no flush is needed
+between steps.
+
+Multi-GPU: replicas only (the north-star path is one GPU with no ghost
+exchange); each rank assembles its own copy, value = N * nnz / max step time.
+``--impl reference`` times the C restatement of the reference's CPU path
+(oracle/cfem.c: per-cell tabulation, binary-search CSR insertion, row-owning
+threads) with all host threads on the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "cuda-dolfinx_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+WORKLOADS = {
+    "p2": dict(kind="p2", n=96, precision="fp64",
+               desc="P2 Poisson n=96: 5,308,416 tets, k P1 lognormal, f DG0 U[-1,1], g=x+y+z"),
+    "p1": dict(kind="p1", n=32, precision="fp64",
+               desc="P1 Poisson n=32: 196,608 tets, k=1, f=P1(sin sin sin), homogeneous Dirichlet"),
+    "p1big": dict(kind="p1", n=128, precision="fp64",
+                  desc="P1 Poisson n=128: 12,582,912 tets, k=1, f=P1(sin sin sin), homogeneous Dirichlet"),
+    "vp2": dict(kind="vp2", n=64, precision="fp32",
+                desc="vector-P2 elasticity n=64: 1,572,864 jittered tets, lam/mu DG0, FP32 element tensors"),
+}
+KERNELS_PER_STEP = 7  # zero A, matrix, set_diagonal, zero b, vector, lifting, set_bc
+_PINNED: list = []
+
+
+# ---------------------------------------------------------------------------
+# problem construction (host, seeded)
+# ---------------------------------------------------------------------------
+def make_inputs(kind: str, n: int, seed: int = 0, pinned: bool = False):
+    """Seeded synthetic inputs with the shapes of the benchmark configuration."""
+    from cudolfinx import fem
+
+    rng = np.random.default_rng(seed)
+    mesh = fem.create_unit_cube(n, jitter=0.2 if kind == "vp2" else 0.0, seed=seed)
+    C = mesh.num_cells
+
+    def host(a):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        if not pinned:
+            return a
+        import torch
+        t = torch.empty(a.shape, dtype=torch.float64, pin_memory=True)
+        _PINNED.append(t)  # keep the pinned buffer alive with its numpy view
+        out = t.numpy()
+        out[...] = a
+        return out
+
+    I = {"kind": kind, "n": n, "mesh": mesh}
+    if kind == "p1":
+        V = fem.functionspace(mesh, ("P", 1))
+        X = V.tabulate_dof_coordinates()
+        f = fem.Function(V)
+        f.x.array = host(np.sin(np.pi * X[:, 0]) * np.sin(np.pi * X[:, 1]) * np.sin(np.pi * X[:, 2]))
+        a = fem.stiffness(V, 1.0)
+        L = fem.load(V, f)
+        g = fem.Function(V)
+        I.update(k=None, f=f.x.array, g=g.x.array)
+    elif kind == "p2":
+        V = fem.functionspace(mesh, ("P", 2))
+        V1 = fem.functionspace(mesh, ("P", 1))
+        W = fem.functionspace(mesh, ("DG", 0))
+        k = fem.Function(V1)
+        k.x.array = host(np.exp(rng.standard_normal(V1.num_dofs)))
+        f = fem.Function(W)
+        f.x.array = host(rng.uniform(-1.0, 1.0, size=C))
+        g = fem.Function(V)
+        g.x.array[:] = V.tabulate_dof_coordinates().sum(axis=1)
+        a = fem.stiffness(V, k)
+        L = fem.load(V, f)
+        I.update(k=k.x.array, f=f.x.array, g=g.x.array)
+    elif kind == "vp2":
+        V = fem.functionspace(mesh, ("P", 2, (3,)))
+        W = fem.functionspace(mesh, ("DG", 0))
+        W3 = fem.functionspace(mesh, ("DG", 0, (3,)))
+        lam = fem.Function(W)
+        lam.x.array = host(rng.uniform(0.5, 2.0, size=C))
+        mu = fem.Function(W)
+        mu.x.array = host(rng.uniform(0.2, 1.0, size=C))
+        f = fem.Function(W3)
+        f.x.array = host(np.tile([0.0, 0.0, -1.0], C))
+        a = fem.elasticity(V, lam, mu, precision="fp32")
+        L = fem.load(V, f)
+        g = fem.Function(V)
+        I.update(lam=lam.x.array, mu=mu.x.array, f=f.x.array, g=g.x.array)
+    else:
+        raise ValueError(kind)
+    bc_dofs = fem.locate_boundary_dofs(V)
+    bc = fem.dirichletbc(g, bc_dofs)
+    I.update(V=V, a=a, L=L, bc=bc, bc_dofs=bc_dofs, ndof=V.num_nodes, bs=V.bs, dofs=V.dofs,
+             coords=mesh.geometry_x, cells=mesh.cells)
+    return I
+
+
+def host_pattern(I):
+    """CSR pattern on the host (same builder as the device path; bit-exact with
+    the oracle in tests/test_host.py)."""
+    from cudolfinx import _lib
+
+    d = np.ascontiguousarray(I["dofs"], dtype=np.int32)
+    nnz = ctypes.c_int64()
+    rp, cl = ctypes.c_void_p(), ctypes.c_void_p()
+    _lib.check(_lib.lib.fe_pattern_build_host(d.ctypes.data, d.ctypes.data, d.shape[0], d.shape[1], d.shape[1],
+                                              I["bs"], I["bs"], I["ndof"], I["ndof"], ctypes.byref(nnz),
+                                              ctypes.byref(rp), ctypes.byref(cl)), "fe_pattern_build_host")
+    nrows = I["ndof"] * I["bs"]
+    row_ptr = np.ctypeslib.as_array((ctypes.c_int32 * (nrows + 1)).from_address(rp.value)).copy()
+    col = np.ctypeslib.as_array((ctypes.c_int32 * nnz.value).from_address(cl.value)).copy()
+    _lib.lib.fe_free_host(rp)
+    _lib.lib.fe_free_host(cl)
+    return row_ptr, col
+
+
+def oracle_problem(I):
+    P = {"kind": I["kind"], "n": I["n"], "coords": I["coords"], "cells": I["cells"], "dofs": I["dofs"],
+         "bs": I["bs"], "ndof": I["ndof"], "bc_dofs": I["bc_dofs"], "g": I["g"], "f": I["f"]}
+    if I["kind"] == "vp2":
+        P.update(lam=I["lam"], mu=I["mu"], f=np.asarray(I["f"]).reshape(-1, 3))
+    else:
+        P["k"] = I.get("k")
+    return P
+
+
+# ---------------------------------------------------------------------------
+# CPU legs (C restatement of the reference algorithm)
+# ---------------------------------------------------------------------------
+def cpu_assembler(I, row_ptr, col):
+    from oracle import cfem
+
+    threads = os.cpu_count() or 1
+    return cfem.CpuAssembler(oracle_problem(I), row_ptr, col, nthreads=threads), threads
+
+
+def cpu_step(C):
+    t0 = time.perf_counter()
+    C.assemble_matrix()
+    C.assemble_rhs()
+    return time.perf_counter() - t0
+
+
+def cpu_baseline(I, row_ptr, col, nnz, reps=2):
+    C, threads = cpu_assembler(I, row_ptr, col)
+    cpu_step(C)  # warm (page-in, thread start)
+    times = [cpu_step(C) for _ in range(reps)]
+    C.close()
+    t = statistics.median(times)
+    return {"value": nnz / t, "unit": "nnz/s", "cores": threads, "kind": "port",
+            "sample": f"full workload ({len(I['cells'])} cells, nnz {nnz}): matrix + vector + lifting + set_bc, "
+                      f"median of {reps} after 1 warm-up, {threads} threads, C port of the reference CPU "
+                      "path (oracle/cfem.c)", "seconds_per_step": t}
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# GPU leg
+# ---------------------------------------------------------------------------
+def algorithmic_matrix_bytes(I, nnz):
+    """Bytes one matrix-assembly launch must move (the roofline basis):
+    CSR values written once (8/nnz), the cell-to-slot byte map (k^2 per cell),
+    the form's cell dofmap (4k per cell), the geometry dofmap (16 per cell),
+    coordinates (24 per node), coefficient data, row_ptr (4 per row) and BC
+    markers (1 per row)."""
+    C = len(I["cells"])
+    k = I["dofs"].shape[1]
+    nnodes = len(I["coords"])
+    nrows = I["ndof"] * I["bs"]
+    b = 8 * nnz + k * k * C + 4 * k * C + 16 * C + 24 * nnodes + 4 * (nrows + 1) + nrows
+    if I["kind"] == "p2":
+        b += 16 * C + 8 * nnodes  # P1 coefficient: its dofmap + vertex values
+    elif I["kind"] == "vp2":
+        b += 16 * C  # lam, mu DG0
+    return b
+
+
+def load_traffic(kernel_key: str):
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(path) as fh:
+            return json.load(fh).get(kernel_key)
+    except (OSError, ValueError):
+        return None
+
+
+def run_gpu(args, rank, world, local_rank):
+    import torch
+
+    import cudolfinx as cx
+    from cudolfinx import _lib
+
+    torch.cuda.set_device(local_rank)
+    W = WORKLOADS[args.workload]
+    t_setup = time.perf_counter()
+    I = make_inputs(W["kind"], W["n"], seed=args.seed)
+    asm = cx.CUDAAssembler()
+    a = cx.form(I["a"])
+    L = cx.form(I["L"])
+    A = asm.create_matrix(a)
+    b = asm.create_vector(L)
+    dbc = asm.pack_bcs([I["bc"]])
+    hbc = dbc._get_cpp_bcs(I["V"]).handle
+    nnz = A.sparsity.nnz
+    nrows = A.sparsity.num_rows
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+    flags = _lib.ASM_DETERMINISTIC if args.variant == "deterministic" else 0
+    forms = (ctypes.c_void_p * 1)(a.cuda_form)
+    bcs1 = (ctypes.c_void_p * 1)(hbc)
+    Lib = _lib.lib
+    Ap, bp = A.values.data_ptr(), b.vector.data_ptr()
+
+    def step(ev0=None, ev1=None):
+        _lib.check(Lib.fe_zero_entries(Ap, nnz, sp), "zero")
+        if ev0 is not None:
+            ev0.record(stream)
+        _lib.check(Lib.fe_assemble_matrix(a.cuda_form, Ap, hbc, hbc, 1.0, flags, sp), "matrix")
+        if ev1 is not None:
+            ev1.record(stream)
+        _lib.check(Lib.fe_assemble_vector(L.cuda_form, bp, _lib.ASM_ZERO, sp), "vector")
+        _lib.check(Lib.fe_apply_lifting(bp, 1, forms, bcs1, None, 1.0, sp), "lifting")
+        _lib.check(Lib.fe_set_bc(bp, nrows, hbc, None, 1.0, sp), "set_bc")
+
+    step()  # plan build (deterministic), lift-cell list
+    torch.cuda.synchronize()
+    setup_s = time.perf_counter() - t_setup
+    for _ in range(args.warmup):
+        step()
+    dist = torch.distributed if world > 1 else None
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    time.sleep(0.3)
+    e_start = torch.cuda.Event(enable_timing=True)
+    e_end = torch.cuda.Event(enable_timing=True)
+    mats = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    e_start.record(stream)
+    for k in range(args.steps):
+        step(*mats[k])
+    e_end.record(stream)
+    torch.cuda.synchronize()
+    total_ms = e_start.elapsed_time(e_end)
+    mat_ms = statistics.mean(m0.elapsed_time(m1) for m0, m1 in mats)
+    clk = clocks.stop()
+    if dist:
+        t = torch.tensor([total_ms, mat_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms, mat_ms = float(t[0]), float(t[1])
+    ms_per_step = total_ms / args.steps
+    cx.get_cuda_context().synchronize()
+
+    # ---- e2e through the public API with pinned host buffers -------------
+    e2e = None
+    if not args.no_e2e:
+        I2 = make_inputs(W["kind"], W["n"], seed=args.seed, pinned=True)
+        a2 = cx.form(I2["a"])
+        L2 = cx.form(I2["L"])
+        A2 = cx.CUDAMatrix(asm._ctx, A.sparsity)
+        b2 = asm.create_vector(L2)
+        dbc2 = asm.pack_bcs([I2["bc"]])
+        bhost = torch.empty(nrows, dtype=torch.float64, pin_memory=True)
+        coef_bytes = sum(np.asarray(c.x.array).nbytes for c in I2["a"].coefficients + I2["L"].coefficients
+                         if hasattr(c, "x"))
+
+        def e2e_step():
+            asm.assemble_matrix(a2, A2, bcs=dbc2)
+            asm.assemble_vector(L2, b2)
+            asm.apply_lifting(b2, [a2], [dbc2])
+            asm.set_bc(b2, dbc2, I2["V"])
+            bhost.copy_(b2.vector, non_blocking=True)
+
+        for _ in range(max(1, args.warmup)):
+            e2e_step()
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        s0 = torch.cuda.Event(enable_timing=True)
+        s1 = torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        for _ in range(args.steps):
+            e2e_step()
+        s1.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms = s0.elapsed_time(s1)
+        if dist:
+            t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_ms = float(t[0])
+        # parity of the two legs (same seeded inputs)
+        same = bool(torch.allclose(bhost.to(b.vector.device), b.vector, rtol=1e-12, atol=1e-13))
+        e2e = {"value": world * nnz * args.steps / (e2e_ms / 1e3), "unit": "nnz/s",
+               "h2d_bytes_per_step": int(coef_bytes), "d2h_bytes_per_step": int(nrows * 8),
+               "ms_per_step": e2e_ms / args.steps, "path": "cudolfinx.CUDAAssembler (Python API -> C-ABI)",
+               "matches_device_leg": same}
+
+    alg = algorithmic_matrix_bytes(I, nnz)
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            peaks = json.load(fh)
+    except (OSError, ValueError):
+        pass
+    peak = peaks.get("hbm_gbs", 6650.0)
+    achieved = alg / (mat_ms / 1e3) / 1e9
+    kernel_key = f"{args.workload}:{args.variant}"
+    traffic = load_traffic(kernel_key)
+    out = {
+        "metric": "matrix nnz/s",
+        "value": world * nnz * args.steps / (total_ms / 1e3),
+        "unit": "nnz/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_per_step,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64" if W["precision"] == "fp64" else "f32-element/f64-accumulate",
+        "data": "synthetic (seeded numpy inputs with the configuration's shapes and distributions)",
+        "config": {"workload": W["desc"], "cells": len(I["cells"]), "dofs": nrows, "nnz": nnz,
+                   "step": "zero A + assemble A (BC skip, unit diagonal) + assemble b + lifting + set_bc",
+                   "variant": args.variant, "l2": "inputs larger than L2 (CSR values %.2f GB)" % (8 * nnz / 1e9),
+                   "parallelism": f"replicas x{world}"},
+        "roofline": {"bound": "hbm", "kernel": "matrix assembly (%s)" % args.variant,
+                     "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic, "algorithmic_bytes": alg,
+                     "kernel_ms": mat_ms, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"
+                     if "hbm_gbs" in peaks else "fallback 6650 GB/s"},
+        "matrix_nnz_per_s": nnz / (mat_ms / 1e3),
+        "gpu_launches": KERNELS_PER_STEP * args.steps + (1 if args.variant == "deterministic" else 0) * args.steps,
+        "clocks": clk,
+        "setup_s": setup_s,
+    }
+    if e2e:
+        out["e2e"] = e2e
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        row_ptr, col = A.sparsity.to_host()
+        out["cpu_baseline"] = cpu_baseline(I, row_ptr, col, nnz)
+    return out
+
+
+def run_reference(args):
+    W = WORKLOADS[args.workload]
+    I = make_inputs(W["kind"], W["n"], seed=args.seed)
+    row_ptr, col = host_pattern(I)
+    nnz = len(col)
+    C, threads = cpu_assembler(I, row_ptr, col)
+    for _ in range(args.warmup):
+        cpu_step(C)
+    times = [cpu_step(C) for _ in range(args.steps)]
+    C.close()
+    total = sum(times)
+    v = nnz * args.steps / total
+    return {"impl": "reference", "metric": "matrix nnz/s", "value": v, "unit": "nnz/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded)",
+            "config": {"workload": W["desc"], "cells": len(I["cells"]), "nnz": nnz,
+                       "step": "zero A + assemble A + assemble b + lifting + set_bc"},
+            "cpu_baseline": {"value": v, "unit": "nnz/s", "cores": threads, "kind": "port",
+                             "sample": "full workload each step; C port of the reference CPU path "
+                                       "(oracle/cfem.c); the reference itself needs DOLFINx + PETSc"},
+            "e2e": {"value": v, "unit": "nnz/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="p2")
+    ap.add_argument("--variant", choices=["atomic", "deterministic"], default="atomic")
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args)), flush=True)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local_rank))
+    try:
+        out = run_gpu(args, rank, world, local_rank)
+        if rank == 0:
+            print(json.dumps(out), flush=True)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,226 @@
+// Internal declarations shared by the host ABI (fe_abi.cu), the host sparsity
+// builder (fe_sparsity.cpp) and the kernels (fe_kernels.cu, fe_pcg.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/cudolfinx_b200.h"
+
+namespace fe {
+
+// Error carrying an fe_status code; caught at the ABI boundary and turned into
+// a status + thread-local message.
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+[[noreturn]] void fail(int code, const std::string& msg, const char* file, int line);
+void set_last_error(const std::string& msg);
+void check_cuda(cudaError_t e, const char* what, const char* file, int line);
+
+#define FE_FAIL(code, msg) ::fe::fail((code), (msg), __FILE__, __LINE__)
+#define FE_CUDA(call) ::fe::check_cuda((call), #call, __FILE__, __LINE__)
+#define FE_REQUIRE(cond, msg)                  \
+  do {                                         \
+    if (!(cond)) FE_FAIL(FE_ERR_ARG, (msg));   \
+  } while (0)
+
+// Device error word bits (set with atomicOr by kernels; never a trap).
+enum DeviceError : unsigned {
+  DEV_ERR_PATTERN = 1u,    // a cell coupling was not found in the CSR row
+  DEV_ERR_ROW_WIDE = 2u,   // a block row has more than 255 block columns
+  DEV_ERR_BLOCK = 4u,      // the CSR rows of one block row differ
+  DEV_ERR_INDEX = 8u       // an index outside its array
+};
+
+// RAII device buffer.
+template <typename T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  explicit DevBuf(size_t count) { alloc(count); }
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  void alloc(size_t count) {
+    release();
+    n = count;
+    if (count) {
+      cudaError_t e = cudaMalloc((void**)&p, count * sizeof(T));
+      if (e != cudaSuccess) {
+        p = nullptr;
+        n = 0;
+        (void)cudaGetLastError();
+        throw Error(FE_ERR_NOMEM, std::string("cudaMalloc of ") + std::to_string(count * sizeof(T)) +
+                                      " bytes failed: " + cudaGetErrorString(e));
+      }
+    }
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  size_t bytes() const { return n * sizeof(T); }
+};
+
+}  // namespace fe
+
+struct fe_context_s {
+  int device = 0;
+  int num_sms = 0;
+  fe::DevBuf<unsigned> err;  // device error word
+};
+
+struct fe_mesh_s {
+  fe_context ctx = nullptr;
+  int64_t num_nodes = 0, num_cells = 0;
+  int nodes_per_cell = 4;
+  fe::DevBuf<double> x;      // [num_nodes*3]
+  fe::DevBuf<int32_t> geom;  // [num_cells*4]
+};
+
+struct fe_dofmap_s {
+  fe_context ctx = nullptr;
+  int64_t num_cells = 0, num_blocks = 0;
+  int k = 0, bs = 1;
+  fe::DevBuf<int32_t> dofs;      // [num_cells*k] block dofs
+  std::vector<int32_t> host;     // host copy (sparsity build)
+  uint64_t id = 0;               // unique id for caches
+};
+
+struct fe_sparsity_s {
+  fe_context ctx = nullptr;
+  int64_t num_rows = 0, num_cols = 0, nnz = 0;
+  fe::DevBuf<int32_t> row_ptr;   // [num_rows+1]
+  fe::DevBuf<int32_t> col;       // [nnz]
+  fe::DevBuf<int32_t> diag;      // [num_rows] slot of (r, r) or -1
+  uint64_t id = 0;
+};
+
+struct fe_bc_s {
+  fe_context ctx = nullptr;
+  int64_t num_dofs = 0, n_bc = 0, n_owned = 0;
+  fe::DevBuf<uint8_t> markers;   // [num_dofs]
+  fe::DevBuf<int32_t> dofs;      // [n_bc], owned first
+  fe::DevBuf<double> g;          // [num_dofs]
+  // cells with a marked dof, per dofmap id (lifting); built on first use
+  struct CellList {
+    fe::DevBuf<int32_t> cells;
+    int64_t count = 0;
+  };
+  std::map<uint64_t, std::unique_ptr<CellList>> lift_cells;
+};
+
+namespace fe {
+struct Coefficient {
+  int kind = -1;                 // fe_coeff_kind, -1 = unset
+  fe_dofmap map = nullptr;       // P1 dofmap
+  const double* values = nullptr;  // device pointer (own or caller's)
+  DevBuf<double> own;            // storage when uploaded from host
+  int64_t n = 0;
+  double constant[3] = {1.0, 1.0, 1.0};
+};
+}  // namespace fe
+
+struct fe_form_s {
+  fe_context ctx = nullptr;
+  int kind = 0, rank = 0;
+  int precision = FE_PREC_FP64;
+  fe_mesh mesh = nullptr;
+  fe_dofmap V0 = nullptr, V1 = nullptr;
+  fe::Coefficient coeff[2];
+  fe_sparsity sp = nullptr;
+  fe::DevBuf<uint8_t> pos;       // [num_cells * k0 * k1] block column positions (padded to 16 B)
+  // deterministic sorted-slot plan (fe_gather.cu); built on first use
+  struct Gather;
+  std::unique_ptr<Gather> gather;
+  fe_form_s();
+  ~fe_form_s();
+};
+
+namespace fe {
+
+// ---- host sparsity (fe_sparsity.cpp) ----
+void build_block_pattern(const int32_t* dofs0, const int32_t* dofs1, int64_t num_cells, int k0, int k1,
+                         int64_t nblock_rows, int64_t nblock_cols, std::vector<int64_t>& bptr,
+                         std::vector<int32_t>& bcol);
+void unroll_pattern(const std::vector<int64_t>& bptr, const std::vector<int32_t>& bcol, int bs0, int bs1,
+                    std::vector<int32_t>& row_ptr, std::vector<int32_t>& col, std::vector<int32_t>& diag);
+
+// ---- kernels (fe_kernels.cu) ----
+struct MatLaunch {
+  int kind, precision;
+  int64_t num_cells;
+  const double* x;
+  const int32_t* geom;
+  const int32_t* dofs0;
+  const int32_t* dofs1;
+  int k0, k1, bs;
+  const uint8_t* pos;
+  const int32_t* row_ptr;
+  const uint8_t* bc0;
+  const uint8_t* bc1;
+  const Coefficient* c0;
+  const Coefficient* c1;
+  double* values;
+};
+void launch_zero(double* v, int64_t n, cudaStream_t s);
+void launch_build_slotmap(const fe_form_s& f, cudaStream_t s);
+void launch_matrix_atomic(const MatLaunch& a, cudaStream_t s);
+void launch_set_diagonal(const fe_sparsity_s& sp, const fe_bc_s& bc, double diagonal, double* values,
+                         cudaStream_t s);
+
+struct VecLaunch {
+  int kind;
+  int64_t num_cells;
+  const double* x;
+  const int32_t* geom;
+  const int32_t* dofs;
+  int k, bs;
+  const Coefficient* f;
+  double* b;
+  int64_t num_values;
+};
+void launch_vector(const VecLaunch& a, cudaStream_t s);
+
+struct LiftLaunch {
+  int kind, precision;
+  const int32_t* cells;   // cells with a marked trial dof
+  int64_t num_list;
+  const double* x;
+  const int32_t* geom;
+  const int32_t* dofs0;
+  const int32_t* dofs1;
+  int k0, k1, bs;
+  const Coefficient* c0;
+  const Coefficient* c1;
+  const uint8_t* bc1;
+  const double* g;
+  const double* x0;
+  double scale;
+  double* b;
+  int64_t num_values;
+};
+void launch_lifting(const LiftLaunch& a, cudaStream_t s);
+void launch_mark_cells(const int32_t* dofs, int64_t num_cells, int k, int bs, const uint8_t* markers,
+                       int32_t* out_cells, unsigned long long* out_count, cudaStream_t s);
+void launch_set_bc(double* b, int64_t num_values, const int32_t* dofs, int64_t n_bc, const double* g,
+                   const double* x0, double scale, cudaStream_t s);
+
+// error word of the current context's kernels
+unsigned* device_error_word(fe_context ctx);
+
+// drops the deterministic plan of a form (fe_gather.cu)
+void reset_gather_plan(fe_form_s& f);
+
+}  // namespace fe

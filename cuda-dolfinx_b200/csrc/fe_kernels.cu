@@ -1,0 +1,756 @@
+// sm_100a assembly kernels: element tensors + scatter through the cell-to-slot
+// map, vector assembly, lifting, set_bc, set_diagonal, slot-map construction.
+//
+// Reference counterparts (NVRTC string templates, one thread per cell, binary
+// search per element entry, FP64 atomicAdd):
+//   matrix   cpp/cudolfinx/fem/CUDAFormIntegral.cpp:1103-1226
+//   vector   cpp/cudolfinx/fem/CUDAFormIntegral.cpp:270-357
+//   lifting  cpp/cudolfinx/fem/CUDAFormIntegral.cpp:603-717
+//   utils    cpp/cudolfinx/fem/CUDAAssembler.cpp:38-164
+//
+// Here the column search is replaced by a per-cell byte map `pos` built once
+// (block position of column dof j inside block row dof i), the slot is
+// row_ptr[bs*dof_i + a] + bs*pos + b, element tensors use the symmetric half
+// only, and coefficients are gathered in-kernel (no separate packing pass).
+#include <cuda_runtime.h>
+
+#include "fe_element_code.cuh"
+#include "fe_internal.h"
+
+namespace fe {
+namespace {
+
+constexpr int kBlock = 128;  // threads (= cells) per CTA for thread-per-cell kernels
+
+__device__ __forceinline__ void raise_err(unsigned* err, unsigned bit) { atomicOr(err, bit); }
+
+struct CoefDev {
+  int kind;            // fe_coeff_kind
+  const double* v;     // DG0: [cells*ncomp]; P1: [nodes]
+  const int32_t* map;  // P1: [cells*4]
+  double c[3];         // constant
+};
+
+CoefDev to_dev(const Coefficient* c) {
+  CoefDev d{};
+  if (!c || c->kind < 0) {
+    d.kind = FE_COEFF_CONSTANT;
+    d.c[0] = d.c[1] = d.c[2] = 1.0;
+    return d;
+  }
+  d.kind = c->kind;
+  d.v = c->values;
+  d.map = c->map ? c->map->dofs.p : nullptr;
+  for (int i = 0; i < 3; ++i) d.c[i] = c->constant[i];
+  return d;
+}
+
+// cellwise scalar value of a DG0 / constant coefficient
+__device__ __forceinline__ double coef_cell(const CoefDev& k, int64_t c) {
+  return k.kind == FE_COEFF_DG0 ? __ldg(k.v + c) : k.c[0];
+}
+
+// ---------------------------------------------------------------------------
+// Geometry of an affine tetrahedron: K = J^{-1}, |det J|
+// ---------------------------------------------------------------------------
+struct CellGeo {
+  double K[3][3];
+  double adet;
+};
+
+__device__ __forceinline__ void cell_geometry(const double* __restrict__ x, int4 v, CellGeo& g) {
+  double x0[3], J[3][3];
+  const int vv[3] = {v.y, v.z, v.w};
+#pragma unroll
+  for (int r = 0; r < 3; ++r) x0[r] = __ldg(x + 3 * (int64_t)v.x + r);
+#pragma unroll
+  for (int cc = 0; cc < 3; ++cc)
+#pragma unroll
+    for (int r = 0; r < 3; ++r) J[r][cc] = __ldg(x + 3 * (int64_t)vv[cc] + r) - x0[r];
+  const double c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1];
+  const double c01 = J[1][2] * J[2][0] - J[1][0] * J[2][2];
+  const double c02 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
+  const double det = J[0][0] * c00 + J[0][1] * c01 + J[0][2] * c02;
+  const double id = 1.0 / det;
+  g.K[0][0] = c00 * id;
+  g.K[1][0] = c01 * id;
+  g.K[2][0] = c02 * id;
+  g.K[0][1] = (J[0][2] * J[2][1] - J[0][1] * J[2][2]) * id;
+  g.K[1][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) * id;
+  g.K[2][1] = (J[0][1] * J[2][0] - J[0][0] * J[2][1]) * id;
+  g.K[0][2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) * id;
+  g.K[1][2] = (J[0][2] * J[1][0] - J[0][0] * J[1][2]) * id;
+  g.K[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) * id;
+  g.adet = fabs(det);
+}
+
+__device__ __forceinline__ int4 load_geom(const int32_t* __restrict__ geom, int64_t c) {
+  return __ldg(reinterpret_cast<const int4*>(geom) + c);
+}
+
+// Ghat_s = adet * (K K^T)_s, s over (00,11,22,01,02,12)
+__device__ __forceinline__ void ghat(const CellGeo& g, double G[6]) {
+  const int pa[6] = {0, 1, 2, 0, 0, 1}, pb[6] = {0, 1, 2, 1, 2, 2};
+#pragma unroll
+  for (int s = 0; s < 6; ++s)
+    G[s] = g.adet * (g.K[pa[s]][0] * g.K[pb[s]][0] + g.K[pa[s]][1] * g.K[pb[s]][1] +
+                     g.K[pa[s]][2] * g.K[pb[s]][2]);
+}
+
+// P1 reference gradients dotted with K: grad phi_i = K^T ghat_i
+__device__ __forceinline__ void p1_grads(const CellGeo& g, double G[4][3]) {
+#pragma unroll
+  for (int b = 0; b < 3; ++b) {
+    G[1][b] = g.K[0][b];
+    G[2][b] = g.K[1][b];
+    G[3][b] = g.K[2][b];
+    G[0][b] = -(g.K[0][b] + g.K[1][b] + g.K[2][b]);
+  }
+}
+
+// Stage a tile of the byte map into shared memory.  The map buffer is padded
+// to a multiple of 16 bytes and tiles start at multiples of 16 bytes.
+template <int BYTES_PER_CELL>
+__device__ __forceinline__ void stage_pos(uint8_t* spos, const uint8_t* __restrict__ pos, int64_t c0,
+                                          int ncell) {
+  const uint4* src = reinterpret_cast<const uint4*>(pos + c0 * BYTES_PER_CELL);
+  uint4* dst = reinterpret_cast<uint4*>(spos);
+  const int nvec = (ncell * BYTES_PER_CELL + 15) / 16;
+  for (int t = threadIdx.x; t < nvec; t += blockDim.x) dst[t] = __ldg(src + t);
+}
+
+struct MatArgs {
+  int64_t num_cells;
+  const double* __restrict__ x;
+  const int32_t* __restrict__ geom;
+  const int32_t* __restrict__ dofs0;
+  const int32_t* __restrict__ dofs1;
+  const uint8_t* __restrict__ pos;
+  const int32_t* __restrict__ row_ptr;
+  const uint8_t* __restrict__ bc0;
+  const uint8_t* __restrict__ bc1;
+  CoefDev c0, c1;
+  double* __restrict__ values;
+};
+
+// ---------------------------------------------------------------------------
+// P1 stiffness, one thread per cell, FP64 atomics
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kBlock) k_mat_p1_atomic(const MatArgs a) {
+  const int64_t c = blockIdx.x * (int64_t)kBlock + threadIdx.x;
+  if (c >= a.num_cells) return;
+  CellGeo g;
+  cell_geometry(a.x, load_geom(a.geom, c), g);
+  double G[4][3];
+  p1_grads(g, G);
+  const double s = g.adet * (1.0 / 6.0) * coef_cell(a.c0, c);
+  const int4 d0 = __ldg(reinterpret_cast<const int4*>(a.dofs0) + c);
+  const int4 d1 = (a.dofs1 == a.dofs0) ? d0 : __ldg(reinterpret_cast<const int4*>(a.dofs1) + c);
+  const int r[4] = {d0.x, d0.y, d0.z, d0.w};
+  const int cl[4] = {d1.x, d1.y, d1.z, d1.w};
+  const uint4 pw = __ldg(reinterpret_cast<const uint4*>(a.pos) + c);
+  const uint32_t pws[4] = {pw.x, pw.y, pw.z, pw.w};
+  unsigned mr = 0, mc = 0;
+  if (a.bc0)
+#pragma unroll
+    for (int i = 0; i < 4; ++i) mr |= (__ldg(a.bc0 + r[i]) ? 1u : 0u) << i;
+  if (a.bc1)
+#pragma unroll
+    for (int i = 0; i < 4; ++i) mc |= (__ldg(a.bc1 + cl[i]) ? 1u : 0u) << i;
+  int rp[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) rp[i] = __ldg(a.row_ptr + r[i]);
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = i; j < 4; ++j) {
+      const double v = s * (G[i][0] * G[j][0] + G[i][1] * G[j][1] + G[i][2] * G[j][2]);
+      if (!(((mr >> i) | (mc >> j)) & 1u)) atomicAdd(a.values + rp[i] + ((pws[i] >> (8 * j)) & 0xffu), v);
+      if (i != j && !(((mr >> j) | (mc >> i)) & 1u))
+        atomicAdd(a.values + rp[j] + ((pws[j] >> (8 * i)) & 0xffu), v);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// P2 stiffness, one thread per cell, FP64 atomics
+// ---------------------------------------------------------------------------
+template <int COEF, typename T>
+__global__ void __launch_bounds__(kBlock) k_mat_p2_atomic(const MatArgs a) {
+  __shared__ __align__(16) uint8_t spos[kBlock * 100];
+  const int64_t c0 = blockIdx.x * (int64_t)kBlock;
+  const int64_t left = a.num_cells - c0;
+  const int ncell = left < kBlock ? (int)left : kBlock;
+  stage_pos<100>(spos, a.pos, c0, ncell);
+  __syncthreads();
+  if ((int)threadIdx.x >= ncell) return;
+  const int64_t c = c0 + threadIdx.x;
+  const uint8_t* p = spos + threadIdx.x * 100;
+
+  const int4 gv = load_geom(a.geom, c);
+  CellGeo g;
+  cell_geometry(a.x, gv, g);
+  double Gh[6];
+  ghat(g, Gh);
+
+  int rp[10];
+  unsigned mr = 0, mc = 0;
+  const int32_t* d0 = a.dofs0 + c * 10;
+  const int32_t* d1 = a.dofs1 + c * 10;
+#pragma unroll
+  for (int i = 0; i < 10; ++i) {
+    const int r = __ldg(d0 + i);
+    rp[i] = __ldg(a.row_ptr + r);
+    if (a.bc0) mr |= (__ldg(a.bc0 + r) ? 1u : 0u) << i;
+    if (a.bc1) mc |= (__ldg(a.bc1 + __ldg(d1 + i)) ? 1u : 0u) << i;
+  }
+  double* __restrict__ vals = a.values;
+  auto emit = [&](int i, int j, T vt) {
+    const double v = (double)vt;
+    if (!(((mr >> i) | (mc >> j)) & 1u)) atomicAdd(vals + rp[i] + p[i * 10 + j], v);
+    if (i != j && !(((mr >> j) | (mc >> i)) & 1u)) atomicAdd(vals + rp[j] + p[j * 10 + i], v);
+  };
+  if constexpr (COEF == FE_COEFF_P1) {
+    const int4 km = __ldg(reinterpret_cast<const int4*>(a.c0.map) + c);
+    const double k[4] = {__ldg(a.c0.v + km.x), __ldg(a.c0.v + km.y), __ldg(a.c0.v + km.z),
+                         __ldg(a.c0.v + km.w)};
+    T q[24];
+#pragma unroll
+    for (int m = 0; m < 4; ++m)
+#pragma unroll
+      for (int s = 0; s < 6; ++s) q[m * 6 + s] = (T)(k[m] * Gh[s]);
+    p2_stiffness_p1coef<T>(q, emit);
+  } else {
+    const double k = coef_cell(a.c0, c);
+    T gq[6];
+#pragma unroll
+    for (int s = 0; s < 6; ++s) gq[s] = (T)(k * Gh[s]);
+    p2_stiffness_const<T>(gq, emit);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Vector-P2 elasticity (bs = 3), one thread per cell, FP64 atomics
+// A[(i,a),(j,b)] = sum_pq W_ab[p][q] R0[p][q][i][j],
+// W_ab[p][q] = |det| (mu (delta_ab (KK^T)_pq + K_pb K_qa) + lam K_pa K_qb)
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ void elasticity_weights(const CellGeo& g, double lam, double mu, int a, int b,
+                                                   T W[9]) {
+#pragma unroll
+  for (int p = 0; p < 3; ++p)
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      double kk = 0.0;
+      if (a == b) kk = g.K[p][0] * g.K[q][0] + g.K[p][1] * g.K[q][1] + g.K[p][2] * g.K[q][2];
+      W[p * 3 + q] = (T)(g.adet * (mu * (kk + g.K[p][b] * g.K[q][a]) + lam * g.K[p][a] * g.K[q][b]));
+    }
+}
+
+template <typename T, typename EmitAB>
+__device__ __forceinline__ void elasticity_blocks(const CellGeo& g, double lam, double mu, EmitAB&& emit_ab) {
+#pragma unroll 1
+  for (int blk = 0; blk < 6; ++blk) {
+    const int a = blk < 3 ? blk : (blk == 3 ? 0 : (blk == 4 ? 0 : 1));
+    const int b = blk < 3 ? blk : (blk == 3 ? 1 : 2);
+    T W[9];
+    elasticity_weights<T>(g, lam, mu, a, b, W);
+    auto emit = [&](int i, int j, T v) { emit_ab(a, b, i, j, v); };
+    if (a == b)
+      p2_block_upper<T>(W, emit);
+    else
+      p2_block_full<T>(W, emit);
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kBlock) k_mat_vp2_atomic(const MatArgs a) {
+  __shared__ __align__(16) uint8_t spos[kBlock * 100];
+  const int64_t c0 = blockIdx.x * (int64_t)kBlock;
+  const int64_t left = a.num_cells - c0;
+  const int ncell = left < kBlock ? (int)left : kBlock;
+  stage_pos<100>(spos, a.pos, c0, ncell);
+  __syncthreads();
+  if ((int)threadIdx.x >= ncell) return;
+  const int64_t c = c0 + threadIdx.x;
+  const uint8_t* p = spos + threadIdx.x * 100;
+
+  CellGeo g;
+  cell_geometry(a.x, load_geom(a.geom, c), g);
+  const double lam = coef_cell(a.c0, c), mu = coef_cell(a.c1, c);
+
+  int rp[10], L[10];
+  unsigned mr = 0, mc = 0;
+  const int32_t* d0 = a.dofs0 + c * 10;
+  const int32_t* d1 = a.dofs1 + c * 10;
+#pragma unroll
+  for (int i = 0; i < 10; ++i) {
+    const int R = __ldg(d0 + i);
+    rp[i] = __ldg(a.row_ptr + 3 * R);
+    L[i] = __ldg(a.row_ptr + 3 * R + 1) - rp[i];
+    const int C = __ldg(d1 + i);
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      if (a.bc0) mr |= (__ldg(a.bc0 + 3 * R + q) ? 1u : 0u) << (3 * i + q);
+      if (a.bc1) mc |= (__ldg(a.bc1 + 3 * C + q) ? 1u : 0u) << (3 * i + q);
+    }
+  }
+  double* __restrict__ vals = a.values;
+  elasticity_blocks<T>(g, lam, mu, [&](int ca, int cb, int i, int j, T vt) {
+    const double v = (double)vt;
+    if (!(((mr >> (3 * i + ca)) | (mc >> (3 * j + cb))) & 1u))
+      atomicAdd(vals + rp[i] + ca * L[i] + 3 * p[i * 10 + j] + cb, v);
+    if (!(ca == cb && i == j) && !(((mr >> (3 * j + cb)) | (mc >> (3 * i + ca))) & 1u))
+      atomicAdd(vals + rp[j] + cb * L[j] + 3 * p[j * 10 + i] + ca, v);
+  });
+}
+
+// ---------------------------------------------------------------------------
+// Utilities
+// ---------------------------------------------------------------------------
+__global__ void k_zero(double* __restrict__ v, int64_t n) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if ((reinterpret_cast<uintptr_t>(v) & 15) == 0) {
+    double2* v2 = reinterpret_cast<double2*>(v);
+    const int64_t n2 = n / 2;
+    for (int64_t t = i; t < n2; t += stride) v2[t] = make_double2(0.0, 0.0);
+    if (i == 0 && (n & 1)) v[n - 1] = 0.0;
+  } else {
+    for (int64_t t = i; t < n; t += stride) v[t] = 0.0;
+  }
+}
+
+// set_diagonal (CUDAAssembler.cpp:131-164) with the diagonal slot precomputed
+__global__ void k_set_diagonal(const int32_t* __restrict__ dofs, int64_t n_owned,
+                               const int32_t* __restrict__ diag, int64_t num_rows, double value,
+                               double* __restrict__ values) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= n_owned) return;
+  const int32_t r = dofs[t];
+  if (r < 0 || r >= num_rows) return;
+  const int32_t s = diag[r];
+  if (s >= 0) values[s] = value;
+}
+
+// Cell-to-slot map: block position of dofs1[c,j] inside block row dofs0[c,i].
+__global__ void k_build_slotmap(const int32_t* __restrict__ dofs0, const int32_t* __restrict__ dofs1,
+                                int64_t num_cells, int k0, int k1, int bs0, int bs1,
+                                const int32_t* __restrict__ row_ptr, const int32_t* __restrict__ col,
+                                int64_t num_rows, uint8_t* __restrict__ pos, unsigned* err) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= num_cells * k0) return;
+  const int64_t c = t / k0;
+  const int i = (int)(t % k0);
+  const int64_t R = dofs0[c * k0 + i];
+  const int64_t r = R * bs0;
+  if (R < 0 || r + bs0 > num_rows) {
+    raise_err(err, DEV_ERR_INDEX);
+    return;
+  }
+  const int32_t lo = row_ptr[r], hi = row_ptr[r + 1];
+  for (int j = 0; j < k1; ++j) {
+    const int32_t key = dofs1[c * k1 + j] * bs1;
+    int32_t a = lo, b = hi;
+    while (a < b) {
+      const int32_t m = (a + b) >> 1;
+      if (col[m] < key) a = m + 1;
+      else b = m;
+    }
+    uint8_t out = 0;
+    if (a >= hi || col[a] != key) {
+      raise_err(err, DEV_ERR_PATTERN);
+    } else {
+      const int32_t off = a - lo;
+      if (off % bs1) raise_err(err, DEV_ERR_BLOCK);
+      const int32_t pb = off / bs1;
+      if (pb > 255) raise_err(err, DEV_ERR_ROW_WIDE);
+      else out = (uint8_t)pb;
+      for (int q = 1; q < bs1; ++q)
+        if (a + q >= hi || col[a + q] != key + q) raise_err(err, DEV_ERR_BLOCK);
+      for (int q = 1; q < bs0; ++q) {
+        const int32_t lq = row_ptr[r + q];
+        if (row_ptr[r + q + 1] - lq != hi - lo || col[lq + off] != key) raise_err(err, DEV_ERR_BLOCK);
+      }
+    }
+    pos[t * k1 + j] = out;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Vector assembly (element vector -> atomicAdd), CUDAFormIntegral.cpp:270-357
+// ---------------------------------------------------------------------------
+struct VecArgs {
+  int64_t num_cells;
+  const double* __restrict__ x;
+  const int32_t* __restrict__ geom;
+  const int32_t* __restrict__ dofs;
+  CoefDev f;
+  double* __restrict__ b;
+  int64_t num_values;
+};
+
+__device__ __forceinline__ void add_guarded(double* b, int64_t row, int64_t n, double v) {
+  if (row >= 0 && row < n) atomicAdd(b + row, v);
+}
+
+__global__ void __launch_bounds__(kBlock) k_vec_p1(const VecArgs a) {
+  const int64_t c = blockIdx.x * (int64_t)kBlock + threadIdx.x;
+  if (c >= a.num_cells) return;
+  CellGeo g;
+  cell_geometry(a.x, load_geom(a.geom, c), g);
+  const int4 d = __ldg(reinterpret_cast<const int4*>(a.dofs) + c);
+  const int r[4] = {d.x, d.y, d.z, d.w};
+  double f[4];
+  if (a.f.kind == FE_COEFF_P1) {
+    const int4 m = __ldg(reinterpret_cast<const int4*>(a.f.map) + c);
+    f[0] = __ldg(a.f.v + m.x);
+    f[1] = __ldg(a.f.v + m.y);
+    f[2] = __ldg(a.f.v + m.z);
+    f[3] = __ldg(a.f.v + m.w);
+  } else {
+    const double fc = coef_cell(a.f, c);
+    f[0] = f[1] = f[2] = f[3] = fc;
+  }
+  const double s = f[0] + f[1] + f[2] + f[3];
+  const double w = g.adet * (1.0 / 120.0);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) add_guarded(a.b, r[i], a.num_values, w * (f[i] + s));
+}
+
+__global__ void __launch_bounds__(kBlock) k_vec_p2(const VecArgs a) {
+  const int64_t c = blockIdx.x * (int64_t)kBlock + threadIdx.x;
+  if (c >= a.num_cells) return;
+  CellGeo g;
+  cell_geometry(a.x, load_geom(a.geom, c), g);
+  const double s = coef_cell(a.f, c) * g.adet;
+  const int32_t* d = a.dofs + c * 10;
+#pragma unroll
+  for (int i = 0; i < 10; ++i) add_guarded(a.b, __ldg(d + i), a.num_values, s * p2_basis_integral(i));
+}
+
+__global__ void __launch_bounds__(kBlock) k_vec_vp2(const VecArgs a) {
+  const int64_t c = blockIdx.x * (int64_t)kBlock + threadIdx.x;
+  if (c >= a.num_cells) return;
+  CellGeo g;
+  cell_geometry(a.x, load_geom(a.geom, c), g);
+  double f[3];
+#pragma unroll
+  for (int q = 0; q < 3; ++q) f[q] = (a.f.kind == FE_COEFF_DG0 ? __ldg(a.f.v + 3 * c + q) : a.f.c[q]) * g.adet;
+  const int32_t* d = a.dofs + c * 10;
+#pragma unroll
+  for (int i = 0; i < 10; ++i) {
+    const int64_t R = __ldg(d + i);
+    const double w = p2_basis_integral(i);
+#pragma unroll
+    for (int q = 0; q < 3; ++q) add_guarded(a.b, 3 * R + q, a.num_values, f[q] * w);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Lifting: for cells with a marked trial dof, be = -scale * Ae[:, bc] (g - x0)
+// (CUDAFormIntegral.cpp:603-717; rows are not masked, as in the reference)
+// ---------------------------------------------------------------------------
+struct LiftArgs {
+  const int32_t* __restrict__ cells;
+  int64_t num_list;
+  const double* __restrict__ x;
+  const int32_t* __restrict__ geom;
+  const int32_t* __restrict__ dofs0;
+  const int32_t* __restrict__ dofs1;
+  CoefDev c0, c1;
+  const uint8_t* __restrict__ bc1;
+  const double* __restrict__ g;
+  const double* __restrict__ x0;
+  double scale;
+  double* __restrict__ b;
+  int64_t num_values;
+};
+
+__global__ void __launch_bounds__(kBlock) k_lift_p1(const LiftArgs a) {
+  const int64_t t = blockIdx.x * (int64_t)kBlock + threadIdx.x;
+  if (t >= a.num_list) return;
+  const int64_t c = a.cells[t];
+  CellGeo g;
+  cell_geometry(a.x, load_geom(a.geom, c), g);
+  double G[4][3];
+  p1_grads(g, G);
+  const double s = g.adet * (1.0 / 6.0) * coef_cell(a.c0, c);
+  const int4 d0 = __ldg(reinterpret_cast<const int4*>(a.dofs0) + c);
+  const int4 d1 = __ldg(reinterpret_cast<const int4*>(a.dofs1) + c);
+  const int r[4] = {d0.x, d0.y, d0.z, d0.w};
+  const int cl[4] = {d1.x, d1.y, d1.z, d1.w};
+  double dv[4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j)
+    dv[j] = __ldg(a.bc1 + cl[j]) ? (__ldg(a.g + cl[j]) - (a.x0 ? __ldg(a.x0 + cl[j]) : 0.0)) : 0.0;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    double acc = 0.0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc += s * (G[i][0] * G[j][0] + G[i][1] * G[j][1] + G[i][2] * G[j][2]) * dv[j];
+    add_guarded(a.b, r[i], a.num_values, -a.scale * acc);
+  }
+}
+
+template <int COEF, typename T>
+__global__ void __launch_bounds__(kBlock) k_lift_p2(const LiftArgs a) {
+  const int64_t t = blockIdx.x * (int64_t)kBlock + threadIdx.x;
+  if (t >= a.num_list) return;
+  const int64_t c = a.cells[t];
+  CellGeo g;
+  cell_geometry(a.x, load_geom(a.geom, c), g);
+  double Gh[6];
+  ghat(g, Gh);
+  double dv[10], be[10];
+  const int32_t* d0 = a.dofs0 + c * 10;
+  const int32_t* d1 = a.dofs1 + c * 10;
+#pragma unroll
+  for (int j = 0; j < 10; ++j) {
+    const int C = __ldg(d1 + j);
+    dv[j] = __ldg(a.bc1 + C) ? (__ldg(a.g + C) - (a.x0 ? __ldg(a.x0 + C) : 0.0)) : 0.0;
+    be[j] = 0.0;
+  }
+  auto emit = [&](int i, int j, T vt) {
+    const double v = (double)vt;
+    be[i] += v * dv[j];
+    if (i != j) be[j] += v * dv[i];
+  };
+  if constexpr (COEF == FE_COEFF_P1) {
+    const int4 km = __ldg(reinterpret_cast<const int4*>(a.c0.map) + c);
+    const double k[4] = {__ldg(a.c0.v + km.x), __ldg(a.c0.v + km.y), __ldg(a.c0.v + km.z),
+                         __ldg(a.c0.v + km.w)};
+    T q[24];
+#pragma unroll
+    for (int m = 0; m < 4; ++m)
+#pragma unroll
+      for (int s = 0; s < 6; ++s) q[m * 6 + s] = (T)(k[m] * Gh[s]);
+    p2_stiffness_p1coef<T>(q, emit);
+  } else {
+    const double k = coef_cell(a.c0, c);
+    T gq[6];
+#pragma unroll
+    for (int s = 0; s < 6; ++s) gq[s] = (T)(k * Gh[s]);
+    p2_stiffness_const<T>(gq, emit);
+  }
+#pragma unroll
+  for (int i = 0; i < 10; ++i) add_guarded(a.b, __ldg(d0 + i), a.num_values, -a.scale * be[i]);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kBlock) k_lift_vp2(const LiftArgs a) {
+  const int64_t t = blockIdx.x * (int64_t)kBlock + threadIdx.x;
+  if (t >= a.num_list) return;
+  const int64_t c = a.cells[t];
+  CellGeo g;
+  cell_geometry(a.x, load_geom(a.geom, c), g);
+  const double lam = coef_cell(a.c0, c), mu = coef_cell(a.c1, c);
+  double dv[30], be[30];
+  const int32_t* d0 = a.dofs0 + c * 10;
+  const int32_t* d1 = a.dofs1 + c * 10;
+#pragma unroll
+  for (int j = 0; j < 10; ++j) {
+    const int64_t C = __ldg(d1 + j);
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      const int64_t s = 3 * C + q;
+      dv[3 * j + q] = __ldg(a.bc1 + s) ? (__ldg(a.g + s) - (a.x0 ? __ldg(a.x0 + s) : 0.0)) : 0.0;
+      be[3 * j + q] = 0.0;
+    }
+  }
+  elasticity_blocks<T>(g, lam, mu, [&](int ca, int cb, int i, int j, T vt) {
+    const double v = (double)vt;
+    be[3 * i + ca] += v * dv[3 * j + cb];
+    if (!(ca == cb && i == j)) be[3 * j + cb] += v * dv[3 * i + ca];
+  });
+#pragma unroll
+  for (int i = 0; i < 10; ++i) {
+    const int64_t R = __ldg(d0 + i);
+#pragma unroll
+    for (int q = 0; q < 3; ++q) add_guarded(a.b, 3 * R + q, a.num_values, -a.scale * be[3 * i + q]);
+  }
+}
+
+__global__ void k_mark_cells(const int32_t* __restrict__ dofs, int64_t num_cells, int k, int bs,
+                             const uint8_t* __restrict__ markers, int32_t* __restrict__ out,
+                             unsigned long long* count) {
+  const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (c >= num_cells) return;
+  bool any = false;
+  for (int i = 0; i < k && !any; ++i) {
+    const int64_t D = dofs[c * k + i];
+    for (int q = 0; q < bs; ++q) any |= markers[D * bs + q] != 0;
+  }
+  if (any) out[atomicAdd(count, 1ull)] = (int32_t)c;
+}
+
+__global__ void k_set_bc(double* __restrict__ b, int64_t num_values, const int32_t* __restrict__ dofs,
+                         int64_t n_bc, const double* __restrict__ g, const double* __restrict__ x0,
+                         double scale) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= n_bc) return;
+  const int32_t d = dofs[t];
+  if (d < 0 || d >= num_values) return;
+  b[d] = scale * (g[d] - (x0 ? x0[d] : 0.0));
+}
+
+unsigned grid_for(int64_t n, int block) { return (unsigned)((n + block - 1) / block); }
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Host launchers
+// ---------------------------------------------------------------------------
+void launch_zero(double* v, int64_t n, cudaStream_t s) {
+  if (n <= 0) return;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int64_t want = (n / 2 + 255) / 256;
+  const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)sms * 8));
+  k_zero<<<grid, 256, 0, s>>>(v, n);
+  FE_CUDA(cudaGetLastError());
+}
+
+void launch_build_slotmap(const fe_form_s& f, cudaStream_t s) {
+  const fe_dofmap_s& V0 = *f.V0;
+  const fe_dofmap_s& V1 = *f.V1;
+  const int64_t n = V0.num_cells * V0.k;
+  if (n == 0) return;
+  k_build_slotmap<<<grid_for(n, 256), 256, 0, s>>>(V0.dofs.p, V1.dofs.p, V0.num_cells, V0.k, V1.k, V0.bs,
+                                                   V1.bs, f.sp->row_ptr.p, f.sp->col.p, f.sp->num_rows,
+                                                   f.pos.p, device_error_word(f.ctx));
+  FE_CUDA(cudaGetLastError());
+}
+
+void launch_matrix_atomic(const MatLaunch& L, cudaStream_t s) {
+  if (L.num_cells == 0) return;
+  MatArgs a{};
+  a.num_cells = L.num_cells;
+  a.x = L.x;
+  a.geom = L.geom;
+  a.dofs0 = L.dofs0;
+  a.dofs1 = L.dofs1;
+  a.pos = L.pos;
+  a.row_ptr = L.row_ptr;
+  a.bc0 = L.bc0;
+  a.bc1 = L.bc1;
+  a.c0 = to_dev(L.c0);
+  a.c1 = to_dev(L.c1);
+  a.values = L.values;
+  const unsigned grid = grid_for(L.num_cells, kBlock);
+  const bool f32 = L.precision == FE_PREC_FP32;
+  switch (L.kind) {
+    case FE_FORM_P1_STIFFNESS:
+      k_mat_p1_atomic<<<grid, kBlock, 0, s>>>(a);
+      break;
+    case FE_FORM_P2_STIFFNESS:
+      if (a.c0.kind == FE_COEFF_P1) {
+        if (f32) k_mat_p2_atomic<FE_COEFF_P1, float><<<grid, kBlock, 0, s>>>(a);
+        else k_mat_p2_atomic<FE_COEFF_P1, double><<<grid, kBlock, 0, s>>>(a);
+      } else {
+        if (f32) k_mat_p2_atomic<FE_COEFF_DG0, float><<<grid, kBlock, 0, s>>>(a);
+        else k_mat_p2_atomic<FE_COEFF_DG0, double><<<grid, kBlock, 0, s>>>(a);
+      }
+      break;
+    case FE_FORM_VP2_ELASTICITY:
+      if (f32) k_mat_vp2_atomic<float><<<grid, kBlock, 0, s>>>(a);
+      else k_mat_vp2_atomic<double><<<grid, kBlock, 0, s>>>(a);
+      break;
+    default:
+      FE_FAIL(FE_ERR_ARG, "not a bilinear form kind: " + std::to_string(L.kind));
+  }
+  FE_CUDA(cudaGetLastError());
+}
+
+void launch_set_diagonal(const fe_sparsity_s& sp, const fe_bc_s& bc, double diagonal, double* values,
+                         cudaStream_t s) {
+  if (bc.n_owned == 0) return;
+  k_set_diagonal<<<grid_for(bc.n_owned, 256), 256, 0, s>>>(bc.dofs.p, bc.n_owned, sp.diag.p, sp.num_rows,
+                                                           diagonal, values);
+  FE_CUDA(cudaGetLastError());
+}
+
+void launch_vector(const VecLaunch& L, cudaStream_t s) {
+  if (L.num_cells == 0) return;
+  VecArgs a{};
+  a.num_cells = L.num_cells;
+  a.x = L.x;
+  a.geom = L.geom;
+  a.dofs = L.dofs;
+  a.f = to_dev(L.f);
+  a.b = L.b;
+  a.num_values = L.num_values;
+  const unsigned grid = grid_for(L.num_cells, kBlock);
+  switch (L.kind) {
+    case FE_FORM_P1_LOAD:
+      k_vec_p1<<<grid, kBlock, 0, s>>>(a);
+      break;
+    case FE_FORM_P2_LOAD:
+      k_vec_p2<<<grid, kBlock, 0, s>>>(a);
+      break;
+    case FE_FORM_VP2_LOAD:
+      k_vec_vp2<<<grid, kBlock, 0, s>>>(a);
+      break;
+    default:
+      FE_FAIL(FE_ERR_ARG, "not a linear form kind: " + std::to_string(L.kind));
+  }
+  FE_CUDA(cudaGetLastError());
+}
+
+void launch_lifting(const LiftLaunch& L, cudaStream_t s) {
+  if (L.num_list == 0) return;
+  LiftArgs a{};
+  a.cells = L.cells;
+  a.num_list = L.num_list;
+  a.x = L.x;
+  a.geom = L.geom;
+  a.dofs0 = L.dofs0;
+  a.dofs1 = L.dofs1;
+  a.c0 = to_dev(L.c0);
+  a.c1 = to_dev(L.c1);
+  a.bc1 = L.bc1;
+  a.g = L.g;
+  a.x0 = L.x0;
+  a.scale = L.scale;
+  a.b = L.b;
+  a.num_values = L.num_values;
+  const unsigned grid = grid_for(L.num_list, kBlock);
+  const bool f32 = L.precision == FE_PREC_FP32;
+  switch (L.kind) {
+    case FE_FORM_P1_STIFFNESS:
+      k_lift_p1<<<grid, kBlock, 0, s>>>(a);
+      break;
+    case FE_FORM_P2_STIFFNESS:
+      if (a.c0.kind == FE_COEFF_P1) {
+        if (f32) k_lift_p2<FE_COEFF_P1, float><<<grid, kBlock, 0, s>>>(a);
+        else k_lift_p2<FE_COEFF_P1, double><<<grid, kBlock, 0, s>>>(a);
+      } else {
+        if (f32) k_lift_p2<FE_COEFF_DG0, float><<<grid, kBlock, 0, s>>>(a);
+        else k_lift_p2<FE_COEFF_DG0, double><<<grid, kBlock, 0, s>>>(a);
+      }
+      break;
+    case FE_FORM_VP2_ELASTICITY:
+      if (f32) k_lift_vp2<float><<<grid, kBlock, 0, s>>>(a);
+      else k_lift_vp2<double><<<grid, kBlock, 0, s>>>(a);
+      break;
+    default:
+      FE_FAIL(FE_ERR_ARG, "lifting needs a bilinear form, got kind " + std::to_string(L.kind));
+  }
+  FE_CUDA(cudaGetLastError());
+}
+
+void launch_mark_cells(const int32_t* dofs, int64_t num_cells, int k, int bs, const uint8_t* markers,
+                       int32_t* out_cells, unsigned long long* out_count, cudaStream_t s) {
+  if (num_cells == 0) return;
+  k_mark_cells<<<grid_for(num_cells, 256), 256, 0, s>>>(dofs, num_cells, k, bs, markers, out_cells, out_count);
+  FE_CUDA(cudaGetLastError());
+}
+
+void launch_set_bc(double* b, int64_t num_values, const int32_t* dofs, int64_t n_bc, const double* g,
+                   const double* x0, double scale, cudaStream_t s) {
+  if (n_bc == 0) return;
+  k_set_bc<<<grid_for(n_bc, 256), 256, 0, s>>>(b, num_values, dofs, n_bc, g, x0, scale);
+  FE_CUDA(cudaGetLastError());
+}
+
+}  // namespace fe

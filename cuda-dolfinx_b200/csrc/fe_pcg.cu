@@ -1,0 +1,268 @@
+// On-device Jacobi-preconditioned conjugate gradients.
+//
+// The reference hands the assembled CUDA matrix/vector to PETSc
+// (KSP "cg" + PC "jacobi", python/examples/poisson.py:116-125).  Here the
+// solver runs on the engine's own CSR arrays:
+//   * SpMV with a sub-warp per row (width from the mean row length) fused
+//     with the p.Ap dot product;
+//   * x/r/z update fused with the r.z and r.r dot products;
+//   * dot products reduce per block into fixed slots, then one block sums the
+//     slots in a fixed order, so the iteration is bitwise reproducible;
+//   * alpha/beta and the stopping test live on the device: every kernel
+//     returns immediately once `done` is set, so the host enqueues iterations
+//     in batches and synchronises once per batch.
+#include <cuda_runtime.h>
+
+#include "fe_internal.h"
+
+namespace fe {
+namespace {
+
+constexpr int kThreads = 256;
+
+struct Scalars {
+  double rz, rz_new, pAp, rr, bb, alpha, beta, tol2;
+  int iter, max_iter, done, pad;
+};
+
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) sh[wid] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (threadIdx.x < 32) {
+    t = (threadIdx.x < blockDim.x / 32) ? sh[threadIdx.x] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+  }
+  return t;  // valid in thread 0
+}
+
+// y_r = sum_s A_rs x_s for the row handled by this SUB-lane group.  Called by
+// all 32 lanes of a warp together (the shuffles name the full warp); a group
+// whose row is past the end passes active = false and contributes nothing.
+template <int SUB>
+__device__ __forceinline__ double row_dot(const int32_t* __restrict__ rp, const int32_t* __restrict__ col,
+                                          const double* __restrict__ val, const double* __restrict__ x, int64_t r,
+                                          bool active, int lane) {
+  double acc = 0.0;
+  const int32_t lo = active ? __ldg(rp + r) : 0, hi = active ? __ldg(rp + r + 1) : 0;
+  for (int32_t s = lo + lane; s < hi; s += SUB) acc += __ldg(val + s) * __ldg(x + __ldg(col + s));
+#pragma unroll
+  for (int o = SUB / 2; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o, SUB);
+  return acc;
+}
+
+// Row loop with a trip count that is uniform across each warp: warp w handles
+// rows [w*32/SUB, w*32/SUB + 32/SUB) + k*stride.
+template <int SUB, typename F>
+__device__ __forceinline__ void for_rows(int64_t n, F&& body) {
+  constexpr int kGroups = 32 / SUB;
+  const int64_t warp = (blockIdx.x * (int64_t)kThreads + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * kThreads) >> 5;
+  const int sub = (threadIdx.x & 31) / SUB;
+  for (int64_t base = warp * kGroups; base < n; base += nwarps * kGroups) {
+    const int64_t row = base + sub;
+    body(row, row < n);
+  }
+}
+
+template <int SUB>
+__global__ void __launch_bounds__(kThreads) k_init(int64_t n, const int32_t* __restrict__ rp,
+                                                   const int32_t* __restrict__ col, const double* __restrict__ val,
+                                                   const int32_t* __restrict__ diag, const double* __restrict__ b,
+                                                   const double* __restrict__ x, double* __restrict__ r,
+                                                   double* __restrict__ z, double* __restrict__ p,
+                                                   double* __restrict__ dinv, double* __restrict__ part) {
+  __shared__ double sh[32];
+  const int lane = threadIdx.x % SUB;
+  double rz = 0.0, rr = 0.0, bb = 0.0;
+  for_rows<SUB>(n, [&](int64_t row, bool active) {
+    const double ax = row_dot<SUB>(rp, col, val, x, row, active, lane);
+    if (active && lane == 0) {
+      const int32_t ds = diag[row];
+      const double d = ds >= 0 ? val[ds] : 1.0;
+      const double di = d != 0.0 ? 1.0 / d : 1.0;
+      const double rv = b[row] - ax;
+      const double zv = di * rv;
+      dinv[row] = di;
+      r[row] = rv;
+      z[row] = zv;
+      p[row] = zv;
+      rz += rv * zv;
+      rr += rv * rv;
+      bb += b[row] * b[row];
+    }
+  });
+  rz = block_sum(rz, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = rz;
+  rr = block_sum(rr, sh);
+  if (threadIdx.x == 0) part[gridDim.x + blockIdx.x] = rr;
+  bb = block_sum(bb, sh);
+  if (threadIdx.x == 0) part[2 * gridDim.x + blockIdx.x] = bb;
+}
+
+// sums `nparts` partial arrays of length m in a fixed order; stage selects the scalar update
+__global__ void k_reduce(const double* __restrict__ part, int m, int stage, Scalars* sc) {
+  __shared__ double sh[32];
+  __shared__ double res[3];
+  if (stage != 0 && sc->done) return;
+  const int nparts = stage == 1 ? 1 : (stage == 0 ? 3 : 2);
+  for (int q = 0; q < nparts; ++q) {
+    double v = 0.0;
+    for (int i = threadIdx.x; i < m; i += blockDim.x) v += part[q * m + i];
+    v = block_sum(v, sh);
+    if (threadIdx.x == 0) res[q] = v;
+    __syncthreads();
+  }
+  if (threadIdx.x != 0) return;
+  if (stage == 0) {  // init: rz, rr, bb
+    sc->rz = res[0];
+    sc->rr = res[1];
+    sc->bb = res[2];
+    sc->iter = 0;
+    sc->done = (res[1] <= sc->tol2 * res[2]) || res[2] == 0.0 || sc->max_iter <= 0;
+  } else if (stage == 1) {  // alpha
+    sc->pAp = res[0];
+    if (res[0] == 0.0) sc->done = 1;
+    else sc->alpha = sc->rz / res[0];
+  } else {  // beta: rz_new, rr
+    sc->rz_new = res[0];
+    sc->rr = res[1];
+    sc->beta = res[0] / sc->rz;
+    sc->rz = res[0];
+    sc->iter += 1;
+    if (res[1] <= sc->tol2 * sc->bb || sc->iter >= sc->max_iter) sc->done = 1;
+  }
+}
+
+template <int SUB>
+__global__ void __launch_bounds__(kThreads) k_spmv(int64_t n, const int32_t* __restrict__ rp,
+                                                   const int32_t* __restrict__ col, const double* __restrict__ val,
+                                                   const double* __restrict__ p, double* __restrict__ Ap,
+                                                   double* __restrict__ part, const Scalars* sc) {
+  __shared__ double sh[32];
+  if (sc->done) return;
+  const int lane = threadIdx.x % SUB;
+  double pap = 0.0;
+  for_rows<SUB>(n, [&](int64_t row, bool active) {
+    const double y = row_dot<SUB>(rp, col, val, p, row, active, lane);
+    if (active && lane == 0) {
+      Ap[row] = y;
+      pap += p[row] * y;
+    }
+  });
+  pap = block_sum(pap, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = pap;
+}
+
+__global__ void __launch_bounds__(kThreads) k_update(int64_t n, double* __restrict__ x, double* __restrict__ r,
+                                                     double* __restrict__ z, const double* __restrict__ p,
+                                                     const double* __restrict__ Ap, const double* __restrict__ dinv,
+                                                     double* __restrict__ part, const Scalars* sc) {
+  __shared__ double sh[32];
+  if (sc->done) return;
+  const double alpha = sc->alpha;
+  double rz = 0.0, rr = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)kThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kThreads) {
+    x[i] += alpha * p[i];
+    const double rv = r[i] - alpha * Ap[i];
+    r[i] = rv;
+    const double zv = dinv[i] * rv;
+    z[i] = zv;
+    rz += rv * zv;
+    rr += rv * rv;
+  }
+  rz = block_sum(rz, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = rz;
+  rr = block_sum(rr, sh);
+  if (threadIdx.x == 0) part[gridDim.x + blockIdx.x] = rr;
+}
+
+__global__ void __launch_bounds__(kThreads) k_update_p(int64_t n, const double* __restrict__ z,
+                                                       double* __restrict__ p, const Scalars* sc) {
+  if (sc->done) return;
+  const double beta = sc->beta;
+  for (int64_t i = blockIdx.x * (int64_t)kThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kThreads)
+    p[i] = z[i] + beta * p[i];
+}
+
+template <int SUB>
+void run(const fe_sparsity_s& A, const double* val, const double* b, double* x, double rtol, int max_iter,
+         int* iterations, double* rel_res, cudaStream_t s) {
+  const int64_t n = A.num_rows;
+  const unsigned grid = (unsigned)(A.ctx->num_sms * 4);
+  double *r, *z, *p, *Ap, *dinv, *part;
+  Scalars* sc;
+  FE_CUDA(cudaMallocAsync((void**)&r, n * sizeof(double), s));
+  FE_CUDA(cudaMallocAsync((void**)&z, n * sizeof(double), s));
+  FE_CUDA(cudaMallocAsync((void**)&p, n * sizeof(double), s));
+  FE_CUDA(cudaMallocAsync((void**)&Ap, n * sizeof(double), s));
+  FE_CUDA(cudaMallocAsync((void**)&dinv, n * sizeof(double), s));
+  FE_CUDA(cudaMallocAsync((void**)&part, 3 * grid * sizeof(double), s));
+  FE_CUDA(cudaMallocAsync((void**)&sc, sizeof(Scalars), s));
+  Scalars h{};
+  h.tol2 = rtol * rtol;
+  h.max_iter = max_iter;
+  FE_CUDA(cudaMemcpyAsync(sc, &h, sizeof(h), cudaMemcpyHostToDevice, s));
+  k_init<SUB><<<grid, kThreads, 0, s>>>(n, A.row_ptr.p, A.col.p, val, A.diag.p, b, x, r, z, p, dinv, part);
+  k_reduce<<<1, 1024, 0, s>>>(part, grid, 0, sc);
+  FE_CUDA(cudaGetLastError());
+  const int batch = 16;
+  for (int it = 0;; it += batch) {
+    for (int q = 0; q < batch; ++q) {
+      k_spmv<SUB><<<grid, kThreads, 0, s>>>(n, A.row_ptr.p, A.col.p, val, p, Ap, part, sc);
+      k_reduce<<<1, 1024, 0, s>>>(part, grid, 1, sc);
+      k_update<<<grid, kThreads, 0, s>>>(n, x, r, z, p, Ap, dinv, part, sc);
+      k_reduce<<<1, 1024, 0, s>>>(part, grid, 2, sc);
+      k_update_p<<<grid, kThreads, 0, s>>>(n, z, p, sc);
+    }
+    FE_CUDA(cudaGetLastError());
+    FE_CUDA(cudaMemcpyAsync(&h, sc, sizeof(h), cudaMemcpyDeviceToHost, s));
+    FE_CUDA(cudaStreamSynchronize(s));
+    if (h.done || it >= max_iter) break;
+  }
+  for (void* q : {(void*)r, (void*)z, (void*)p, (void*)Ap, (void*)dinv, (void*)part, (void*)sc})
+    FE_CUDA(cudaFreeAsync(q, s));
+  *iterations = h.iter;
+  *rel_res = h.bb > 0 ? sqrt(h.rr / h.bb) : 0.0;
+}
+
+}  // namespace
+
+int pcg_solve(const fe_sparsity_s& A, const double* val, const double* b, double* x, double rtol, int max_iter,
+              int* iterations, double* rel_res, cudaStream_t s) {
+  FE_REQUIRE(A.num_rows == A.num_cols, "PCG needs a square matrix");
+  const double mean = A.num_rows ? (double)A.nnz / (double)A.num_rows : 0.0;
+  if (mean <= 6) run<4>(A, val, b, x, rtol, max_iter, iterations, rel_res, s);
+  else if (mean <= 14) run<8>(A, val, b, x, rtol, max_iter, iterations, rel_res, s);
+  else if (mean <= 40) run<16>(A, val, b, x, rtol, max_iter, iterations, rel_res, s);
+  else run<32>(A, val, b, x, rtol, max_iter, iterations, rel_res, s);
+  return *iterations;
+}
+
+}  // namespace fe
+
+extern "C" int fe_pcg_solve(fe_sparsity s, const double* values, const double* b, double* x, double rtol,
+                            int max_iter, int* iterations, double* rel_residual, void* stream) {
+  int it = 0;
+  double res = 0.0;
+  int status = FE_OK;
+  try {
+    if (!s || !values || !b || !x) FE_FAIL(FE_ERR_ARG, "null argument");
+    FE_CUDA(cudaSetDevice(s->ctx->device));
+    fe::pcg_solve(*s, values, b, x, rtol, max_iter, &it, &res, reinterpret_cast<cudaStream_t>(stream));
+    if (iterations) *iterations = it;
+    if (rel_residual) *rel_residual = res;
+    if (!(res <= rtol)) status = FE_ERR_NOT_CONVERGED;
+  } catch (const fe::Error& e) {
+    fe::set_last_error(e.what());
+    return e.code;
+  }
+  if (status != FE_OK) fe::set_last_error("PCG stopped after " + std::to_string(it) + " iterations at relative residual " +
+                                          std::to_string(res));
+  return status;
+}

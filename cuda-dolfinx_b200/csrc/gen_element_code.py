@@ -1,0 +1,181 @@
+"""Build-time generator of the element-tensor bodies used by the CUDA kernels.
+
+The reference wraps FFCx ``tabulate_tensor`` C bodies into NVRTC kernels at
+run time (python/cudolfinx/jit.py:61-114, cpp/cudolfinx/fem/CUDAFormIntegral.cpp:
+2366-2469).  For the built-in forms this engine writes the element tensors
+from the mathematics instead: the reference-element tensors below are
+integrated exactly in rational arithmetic and emitted as straight-line
+``fma`` code with every structurally-zero term removed (744 of 1320 terms
+survive for P2 stiffness with a P1 coefficient).
+
+Output: fe_element_code.cuh (regenerated by the package build when this file
+is newer).
+
+Conventions
+* P2 local dofs: 4 vertices, then edges in basix order (2,3),(1,3),(1,2),(0,3),(0,2),(0,1).
+* Symmetric geometry pairs s: (0,0),(1,1),(2,2),(0,1),(0,2),(1,2).
+* Unique symmetric entries e enumerate (i, j) with i <= j row by row.
+"""
+from __future__ import annotations
+
+import os
+import sys
+from fractions import Fraction
+from math import factorial
+
+EDGES = ((2, 3), (1, 3), (1, 2), (0, 3), (0, 2), (0, 1))
+PAIRS = ((0, 0), (1, 1), (2, 2), (0, 1), (0, 2), (1, 2))
+
+
+def mono_int(a, b, c):
+    return Fraction(factorial(a) * factorial(b) * factorial(c), factorial(a + b + c + 3))
+
+
+def pmul(p, q):
+    r = {}
+    for k1, v1 in p.items():
+        for k2, v2 in q.items():
+            k = (k1[0] + k2[0], k1[1] + k2[1], k1[2] + k2[2])
+            r[k] = r.get(k, 0) + v1 * v2
+    return {k: v for k, v in r.items() if v != 0}
+
+
+def padd(p, q, s=1):
+    r = dict(p)
+    for k, v in q.items():
+        r[k] = r.get(k, 0) + s * v
+    return {k: v for k, v in r.items() if v != 0}
+
+
+def pdiff(p, ax):
+    r = {}
+    for k, v in p.items():
+        if k[ax]:
+            kk = list(k)
+            kk[ax] -= 1
+            r[tuple(kk)] = r.get(tuple(kk), 0) + v * k[ax]
+    return r
+
+
+def pint(p):
+    return sum((v * mono_int(*k) for k, v in p.items()), Fraction(0))
+
+
+LAM = [
+    {(0, 0, 0): Fraction(1), (1, 0, 0): Fraction(-1), (0, 1, 0): Fraction(-1), (0, 0, 1): Fraction(-1)},
+    {(1, 0, 0): Fraction(1)},
+    {(0, 1, 0): Fraction(1)},
+    {(0, 0, 1): Fraction(1)},
+]
+PHI = ([pmul(l, padd({k: 2 * v for k, v in l.items()}, {(0, 0, 0): Fraction(1)}, -1)) for l in LAM]
+       + [{k: 4 * v for k, v in pmul(LAM[a], LAM[b]).items()} for a, b in EDGES])
+DPHI = [[pdiff(p, ax) for ax in range(3)] for p in PHI]
+UNIQ = [(i, j) for i in range(10) for j in range(i, 10)]
+
+
+def lit(x: Fraction) -> str:
+    """Exact-as-possible C double literal (hex float of the rounded value)."""
+    return float(x).hex()
+
+
+def r_weighted(m, a, b, i, j):
+    return pint(pmul(LAM[m], pmul(DPHI[i][a], DPHI[j][b])))
+
+
+def r_plain(a, b, i, j):
+    return pint(pmul(DPHI[i][a], DPHI[j][b]))
+
+
+def sym_pair(fn, s, i, j):
+    a, b = PAIRS[s]
+    v = fn(a, b, i, j)
+    if a != b:
+        v += fn(b, a, i, j)
+    return v
+
+
+def gen() -> str:
+    out = []
+    w = out.append
+    w("// GENERATED by gen_element_code.py -- do not edit.\n")
+    w("#pragma once\n\n")
+    w("namespace fe {\n\n")
+    # integrals of the P2 basis
+    ints = [pint(p) for p in PHI]
+    w("// int_ref phi_i (reference volume 1/6)\n")
+    w("__device__ __forceinline__ double p2_basis_integral(int i) {\n")
+    w("  return i < 4 ? " + lit(ints[0]) + " : " + lit(ints[4]) + ";\n}\n\n")
+
+    # P2 stiffness, P1 coefficient: q[m*6+s] = k_m * Ghat_s
+    w("// P2 stiffness with a P1 coefficient: q[m*6+s] = k_m * Ghat_s,\n")
+    w("// Ghat = |detJ| K K^T (s over (00,11,22,01,02,12)).  Calls emit(i, j, value)\n")
+    w("// for the 55 unique entries i <= j.\n")
+    w("template <typename T, typename Emit>\n")
+    w("__device__ __forceinline__ void p2_stiffness_p1coef(const T* q, Emit&& emit) {\n")
+    nterms = 0
+    for (i, j) in UNIQ:
+        terms = []
+        for m in range(4):
+            for s in range(6):
+                c = sym_pair(lambda a, b, ii, jj: r_weighted(m, a, b, ii, jj), s, i, j)
+                if c != 0:
+                    terms.append((m * 6 + s, c))
+        nterms += len(terms)
+        expr = "T(0)"
+        for idx, c in terms:
+            expr = f"fma(q[{idx}], T({lit(c)}), {expr})"
+        w(f"  emit({i}, {j}, {expr});\n")
+    w("}\n")
+    w(f"// terms: {nterms}\n\n")
+
+    # P2 stiffness, cellwise-constant coefficient: g[s] = k * Ghat_s
+    w("// P2 stiffness with a cellwise-constant coefficient: g[s] = k * Ghat_s.\n")
+    w("template <typename T, typename Emit>\n")
+    w("__device__ __forceinline__ void p2_stiffness_const(const T* g, Emit&& emit) {\n")
+    for (i, j) in UNIQ:
+        terms = []
+        for s in range(6):
+            c = sym_pair(r_plain, s, i, j)
+            if c != 0:
+                terms.append((s, c))
+        expr = "T(0)"
+        for idx, c in terms:
+            expr = f"fma(g[{idx}], T({lit(c)}), {expr})"
+        w(f"  emit({i}, {j}, {expr});\n")
+    w("}\n\n")
+
+    # vector P2 elasticity: block (a,b), entry (i,j): sum_pq W[p*3+q] R0[p][q][i][j]
+    w("// One 10x10 block of vector-P2 elasticity: value(i,j) = sum_pq W[p*3+q] *\n")
+    w("// int_ref d_p phi_i d_q phi_j.  full=false emits only i <= j (diagonal blocks).\n")
+    for full in (True, False):
+        name = "p2_block_full" if full else "p2_block_upper"
+        w("template <typename T, typename Emit>\n")
+        w(f"__device__ __forceinline__ void {name}(const T* W, Emit&& emit) {{\n")
+        for i in range(10):
+            for j in range(10) if full else range(i, 10):
+                terms = []
+                for p in range(3):
+                    for q in range(3):
+                        c = r_plain(p, q, i, j)
+                        if c != 0:
+                            terms.append((p * 3 + q, c))
+                expr = "T(0)"
+                for idx, c in terms:
+                    expr = f"fma(W[{idx}], T({lit(c)}), {expr})"
+                w(f"  emit({i}, {j}, {expr});\n")
+        w("}\n\n")
+    w("}  // namespace fe\n")
+    return "".join(out)
+
+
+def main(argv):
+    here = os.path.dirname(os.path.abspath(__file__))
+    dst = argv[1] if len(argv) > 1 else os.path.join(here, "fe_element_code.cuh")
+    text = gen()
+    if not os.path.exists(dst) or open(dst).read() != text:
+        with open(dst, "w") as fh:
+            fh.write(text)
+
+
+if __name__ == "__main__":
+    main(sys.argv)

@@ -1,0 +1,107 @@
+"""ctypes binding of libcudolfinx_b200.so (the C ABI in include/cudolfinx_b200.h).
+
+Plays the role of the reference's nanobind module ``cudolfinx.cpp``
+(python/cudolfinx/wrappers/fem.cpp:74-407): every failing call raises
+RuntimeError with the library's message, as nanobind does for the
+reference's std::runtime_error.  There is no fallback: if the shared library
+is missing or does not load, importing this module fails.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.environ.get("CUDOLFINX_B200_LIB",
+                          os.path.join(os.path.dirname(_HERE), "lib", "libcudolfinx_b200.so"))
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(f"libcudolfinx_b200.so not found at {LIB_PATH}; build it with "
+                      "`python cuda-dolfinx_b200/build.py`")
+
+lib = ctypes.CDLL(LIB_PATH)
+
+vp = ctypes.c_void_p
+i64 = ctypes.c_int64
+i32 = ctypes.c_int
+u32 = ctypes.c_uint
+dbl = ctypes.c_double
+PP = ctypes.POINTER(ctypes.c_void_p)
+
+FE_OK = 0
+FE_ERR_NOT_CONVERGED = 6
+
+# enum values (include/cudolfinx_b200.h)
+FORM = {"P1_STIFFNESS": 1, "P2_STIFFNESS": 2, "VP2_ELASTICITY": 3, "P1_LOAD": 11, "P2_LOAD": 12, "VP2_LOAD": 13}
+COEFF_CONSTANT, COEFF_DG0, COEFF_P1 = 0, 1, 2
+PREC_FP64, PREC_FP32 = 0, 1
+ASM_ZERO, ASM_DETERMINISTIC = 1, 2
+
+_SIGS = {
+    "fe_last_error": (ctypes.c_char_p, []),
+    "fe_version": (ctypes.c_char_p, []),
+    "fe_context_create": (i32, [i32, PP]),
+    "fe_context_destroy": (i32, [vp]),
+    "fe_context_synchronize": (i32, [vp]),
+    "fe_mesh_create": (i32, [vp, vp, i64, vp, i64, i32, PP]),
+    "fe_mesh_destroy": (i32, [vp]),
+    "fe_dofmap_create": (i32, [vp, vp, i64, i32, i32, i64, PP]),
+    "fe_dofmap_destroy": (i32, [vp]),
+    "fe_sparsity_build": (i32, [vp, vp, PP]),
+    "fe_sparsity_create": (i32, [vp, vp, vp, i64, i64, PP]),
+    "fe_sparsity_info": (i32, [vp, ctypes.POINTER(i64), ctypes.POINTER(i64), ctypes.POINTER(i64)]),
+    "fe_sparsity_copy_to_host": (i32, [vp, vp, vp]),
+    "fe_sparsity_device_arrays": (i32, [vp, PP, PP]),
+    "fe_sparsity_destroy": (i32, [vp]),
+    "fe_pattern_build_host": (i32, [vp, vp, i64, i32, i32, i32, i32, i64, i64, ctypes.POINTER(i64), PP, PP]),
+    "fe_free_host": (None, [vp]),
+    "fe_form_create": (i32, [vp, i32, vp, vp, vp, PP]),
+    "fe_form_set_coefficient": (i32, [vp, i32, i32, vp, vp, i64, i32, vp]),
+    "fe_form_set_precision": (i32, [vp, i32]),
+    "fe_form_bind_sparsity": (i32, [vp, vp, vp]),
+    "fe_form_destroy": (i32, [vp]),
+    "fe_bc_create": (i32, [vp, i64, vp, vp, i64, i64, vp, PP]),
+    "fe_bc_update": (i32, [vp, vp, vp]),
+    "fe_bc_destroy": (i32, [vp]),
+    "fe_assemble_matrix": (i32, [vp, vp, vp, vp, dbl, u32, vp]),
+    "fe_zero_entries": (i32, [vp, i64, vp]),
+    "fe_assemble_vector": (i32, [vp, vp, u32, vp]),
+    "fe_apply_lifting": (i32, [vp, i32, vp, vp, vp, dbl, vp]),
+    "fe_set_bc": (i32, [vp, i64, vp, vp, dbl, vp]),
+    "fe_pcg_solve": (i32, [vp, vp, vp, vp, dbl, i32, ctypes.POINTER(i32), ctypes.POINTER(dbl), vp]),
+}
+
+for _name, (_res, _args) in _SIGS.items():
+    _f = getattr(lib, _name)
+    _f.restype = _res
+    _f.argtypes = _args
+
+EXPORTED = tuple(_SIGS)
+
+
+def last_error() -> str:
+    msg = lib.fe_last_error()
+    return msg.decode() if msg else ""
+
+
+def check(status: int, what: str = "") -> int:
+    if status != FE_OK:
+        raise RuntimeError(f"{what} failed (status {status}): {last_error()}")
+    return status
+
+
+def out_handle():
+    return ctypes.c_void_p()
+
+
+def ptr(x) -> int | None:
+    """Device/host address of a torch tensor, numpy array or int (None passes NULL)."""
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return x
+    if hasattr(x, "data_ptr"):
+        return x.data_ptr()
+    if hasattr(x, "ctypes"):
+        return x.ctypes.data
+    raise TypeError(f"cannot take the address of {type(x)}")

@@ -1,0 +1,269 @@
+"""Host-side stand-ins for the DOLFINx objects the cudolfinx API consumes.
+
+The reference takes DOLFINx meshes, function spaces, Functions, DirichletBCs
+and UFL forms (python/cudolfinx/assemble.py, form.py, bcs.py).  DOLFINx is not
+part of this engine, so this module provides the minimal equivalents the
+assembly path needs, with DOLFINx's data layout:
+
+* ``create_unit_cube(n)``  -- the topology of ``dolfinx.mesh.create_box`` with
+  ``CellType.tetrahedron``: n^3 hexes, 6 tets each, sharing the v0-v7 diagonal
+  (python/examples/poisson.py:34-40); vertex (ix,iy,iz) -> iz(n+1)^2 + iy(n+1) + ix.
+* ``functionspace(mesh, ("P", 1|2[, (3,)]))`` -- Lagrange dofmaps, local dof
+  order = basix (4 vertices, then edges (2,3),(1,3),(1,2),(0,3),(0,2),(0,1));
+  blocked spaces keep one block dof per node (bs = 3), as DOLFINx does.
+* ``Function``, ``dirichletbc``, ``locate_boundary_dofs``.
+* form constructors ``stiffness``, ``elasticity``, ``load`` returning
+  ``FormSpec`` objects that ``cudolfinx.form`` compiles (they stand where the
+  UFL forms stand in the reference).
+
+P2 numbering: every point of the doubled (2n+1)^3 grid is a P2 node on this
+mesh (vertices: all coordinates even; axis edges: one odd; the face diagonals
+v0-v3, v0-v5, v0-v6 and their translates: two odd; body diagonals: three
+odd), so dof = (Z*(2n+1) + Y)*(2n+1) + X, which keeps neighbouring nodes close
+in memory.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+from typing import Callable, Optional, Sequence, Union
+
+import numpy as np
+
+TET_EDGES = ((2, 3), (1, 3), (1, 2), (0, 3), (0, 2), (0, 1))
+
+
+class Mesh:
+    """Affine tetrahedral mesh: coordinates (N,3) float64 and cells (C,4) int32."""
+
+    def __init__(self, coords: np.ndarray, cells: np.ndarray, grid_n: Optional[int] = None):
+        self.geometry_x = np.ascontiguousarray(coords, dtype=np.float64)
+        self.cells = np.ascontiguousarray(cells, dtype=np.int32)
+        self.grid_n = grid_n  # structured unit-cube resolution, if any
+        self._uid = id(self)
+
+    @property
+    def num_cells(self) -> int:
+        return len(self.cells)
+
+    @property
+    def num_vertices(self) -> int:
+        return len(self.geometry_x)
+
+
+def create_unit_cube(n: int, jitter: float = 0.0, seed: int = 0) -> Mesh:
+    """Unit cube, n^3 hexes x 6 tets.  ``jitter`` moves every vertex by
+    U[-jitter*h, jitter*h] per coordinate except normal to the boundary planes
+    it lies on (the domain stays the unit cube)."""
+    n1 = n + 1
+    ix = np.arange(n1 ** 3) % n1
+    iy = (np.arange(n1 ** 3) // n1) % n1
+    iz = np.arange(n1 ** 3) // (n1 * n1)
+    idx = np.stack([ix, iy, iz], axis=1)
+    coords = idx / float(n)
+    if jitter > 0:
+        rng = np.random.default_rng(seed)
+        d = rng.uniform(-jitter / n, jitter / n, size=coords.shape)
+        d[(idx == 0) | (idx == n)] = 0.0
+        coords = coords + d
+    hz, hy, hx = np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij")
+    v0 = (hz * n1 * n1 + hy * n1 + hx).ravel()
+    s_x, s_y, s_z = 1, n1, n1 * n1
+    v1, v2, v3 = v0 + s_x, v0 + s_y, v0 + s_x + s_y
+    v4, v5, v6, v7 = v0 + s_z, v1 + s_z, v2 + s_z, v3 + s_z
+    cells = np.stack([
+        np.stack([v0, v1, v3, v7], 1), np.stack([v0, v1, v7, v5], 1), np.stack([v0, v5, v7, v4], 1),
+        np.stack([v0, v3, v2, v7], 1), np.stack([v0, v6, v4, v7], 1), np.stack([v0, v2, v6, v7], 1),
+    ], axis=1).reshape(-1, 4)
+    return Mesh(coords, cells.astype(np.int32), grid_n=n)
+
+
+class FunctionSpace:
+    """Lagrange space of degree 1 or 2 (scalar or 3-vector) on a Mesh."""
+
+    def __init__(self, mesh: Mesh, element):
+        family, degree = element[0], int(element[1])
+        shape = tuple(element[2]) if len(element) > 2 else ()
+        if family not in ("P", "Lagrange", "CG", "DG"):
+            raise ValueError(f"unsupported family {family}")
+        self.mesh = mesh
+        self.family = "DG" if family == "DG" else "P"
+        self.degree = degree
+        self.bs = 1 if shape == () else int(np.prod(shape))
+        if self.bs not in (1, 3):
+            raise ValueError("value shape must be () or (3,)")
+        if self.family == "DG":
+            if degree != 0:
+                raise ValueError("only DG0 is supported")
+            self.dofs = np.arange(mesh.num_cells, dtype=np.int32).reshape(-1, 1)
+            self.num_nodes = mesh.num_cells
+            self._node_x = None
+            self._grid = None
+        elif degree == 1:
+            self.dofs = mesh.cells.copy()
+            self.num_nodes = mesh.num_vertices
+            self._grid = None
+        elif degree == 2:
+            self._build_p2()
+        else:
+            raise ValueError("degree must be 1 or 2")
+        self._uid = id(self)
+
+    def _build_p2(self):
+        m = self.mesh
+        if m.grid_n is None:
+            raise ValueError("P2 spaces are built for structured unit-cube meshes")
+        n = m.grid_n
+        n1, M = n + 1, 2 * n + 1
+        v = m.cells.astype(np.int64)
+        g = np.stack([v % n1, (v // n1) % n1, v // (n1 * n1)], axis=-1)  # [C,4,3]
+        pts = [2 * g[:, a] for a in range(4)] + [g[:, a] + g[:, b] for a, b in TET_EDGES]
+        P = np.stack(pts, axis=1)
+        self.dofs = ((P[..., 2] * M + P[..., 1]) * M + P[..., 0]).astype(np.int32)
+        self.num_nodes = M ** 3
+        self._grid = (n, M)
+
+    # --- layout ------------------------------------------------------------
+    @property
+    def num_dofs(self) -> int:
+        """Scalar (unrolled) dofs."""
+        return self.num_nodes * self.bs
+
+    @property
+    def dofs_per_cell(self) -> int:
+        return self.dofs.shape[1]
+
+    def tabulate_dof_coordinates(self) -> np.ndarray:
+        """(num_nodes, 3) physical node coordinates (affine cells)."""
+        m = self.mesh
+        X = np.zeros((self.num_nodes, 3))
+        cx = m.geometry_x[m.cells]
+        if self.family == "DG":
+            return cx.mean(axis=1)
+        if self.degree == 1:
+            X[self.dofs.ravel()] = m.geometry_x[m.cells.ravel()]
+            return X
+        pts = [cx[:, a] for a in range(4)] + [0.5 * (cx[:, a] + cx[:, b]) for a, b in TET_EDGES]
+        X[self.dofs.ravel()] = np.stack(pts, axis=1).reshape(-1, 3)
+        return X
+
+    def boundary_nodes(self) -> np.ndarray:
+        """Nodes on the boundary of the unit cube (exact, from grid indices)."""
+        m = self.mesh
+        if m.grid_n is None:
+            raise ValueError("boundary location needs a structured unit-cube mesh")
+        n = m.grid_n
+        if self.degree == 1:
+            ext, N = n, n + 1
+        else:
+            ext, N = 2 * n, 2 * n + 1
+        k = np.arange(N ** 3)
+        ijk = np.stack([k % N, (k // N) % N, k // (N * N)], axis=1)
+        return np.nonzero(np.any((ijk == 0) | (ijk == ext), axis=1))[0].astype(np.int32)
+
+    def contains(self, other: "FunctionSpace") -> bool:
+        return other is self
+
+
+def functionspace(mesh: Mesh, element) -> FunctionSpace:
+    return FunctionSpace(mesh, element)
+
+
+class Function:
+    """Finite-element function: host values ``x.array`` (scalar dofs)."""
+
+    class _Vec:
+        def __init__(self, n):
+            self.array = np.zeros(n)
+
+    def __init__(self, V: FunctionSpace, values: Optional[np.ndarray] = None):
+        self.function_space = V
+        self.x = Function._Vec(V.num_dofs)
+        if values is not None:
+            self.x.array[:] = values
+
+    def interpolate(self, f: Callable[[np.ndarray], np.ndarray]):
+        """Nodal interpolation: f receives x of shape (3, num_nodes)."""
+        X = self.function_space.tabulate_dof_coordinates().T
+        vals = np.asarray(f(X), dtype=np.float64)
+        if self.function_space.bs == 1:
+            self.x.array[:] = vals.reshape(-1)
+        else:
+            self.x.array[:] = vals.reshape(self.function_space.bs, -1).T.reshape(-1)
+
+
+def locate_boundary_dofs(V: FunctionSpace) -> np.ndarray:
+    """Scalar dofs on the boundary facets (blocked: every component)."""
+    nodes = V.boundary_nodes()
+    if V.bs == 1:
+        return nodes
+    return (nodes[:, None] * V.bs + np.arange(V.bs)).ravel().astype(np.int32)
+
+
+class DirichletBC:
+    """u = g on ``dofs`` (scalar dofs of V); g is a Function on V or a float."""
+
+    def __init__(self, value: Union[Function, float], dofs: np.ndarray, V: Optional[FunctionSpace] = None):
+        if isinstance(value, Function):
+            V = value.function_space if V is None else V
+        if V is None:
+            raise ValueError("a constant BC value needs the function space V")
+        self.function_space = V
+        self.value = value
+        self.dofs = np.ascontiguousarray(np.unique(np.asarray(dofs, dtype=np.int32)))
+
+    def values(self) -> np.ndarray:
+        g = np.zeros(self.function_space.num_dofs)
+        if isinstance(self.value, Function):
+            g[self.dofs] = self.value.x.array[self.dofs]
+        else:
+            g[self.dofs] = float(self.value)
+        return g
+
+
+def dirichletbc(value, dofs, V: Optional[FunctionSpace] = None) -> DirichletBC:
+    return DirichletBC(value, dofs, V)
+
+
+Coefficient = Union[Function, float, Sequence[float], np.ndarray]
+
+
+@dataclass
+class FormSpec:
+    """A built-in variational form (stands where a UFL form stands)."""
+    kind: str                      # 'P1_STIFFNESS', 'P2_STIFFNESS', 'VP2_ELASTICITY', '*_LOAD'
+    V: FunctionSpace
+    coefficients: list = field(default_factory=list)
+    rank: int = 2
+    precision: str = "fp64"
+
+    @property
+    def function_spaces(self):
+        return [self.V, self.V] if self.rank == 2 else [self.V]
+
+    @property
+    def mesh(self):
+        return self.V.mesh
+
+
+def stiffness(V: FunctionSpace, k: Coefficient = 1.0, precision: str = "fp64") -> FormSpec:
+    """k * inner(grad(u), grad(v)) * dx on a scalar P1/P2 space."""
+    if V.bs != 1 or V.family != "P":
+        raise ValueError("stiffness needs a scalar Lagrange space")
+    kind = "P1_STIFFNESS" if V.degree == 1 else "P2_STIFFNESS"
+    return FormSpec(kind, V, [k], 2, precision)
+
+
+def elasticity(V: FunctionSpace, lam: Coefficient, mu: Coefficient, precision: str = "fp64") -> FormSpec:
+    """2 mu eps(u):eps(v) + lam div(u) div(v) on a vector P2 space."""
+    if V.bs != 3 or V.degree != 2:
+        raise ValueError("elasticity needs a vector P2 space")
+    return FormSpec("VP2_ELASTICITY", V, [lam, mu], 2, precision)
+
+
+def load(V: FunctionSpace, f: Coefficient) -> FormSpec:
+    """inner(f, v) * dx on P1 / P2 / vector P2."""
+    if V.bs == 3:
+        kind = "VP2_LOAD"
+    else:
+        kind = "P1_LOAD" if V.degree == 1 else "P2_LOAD"
+    return FormSpec(kind, V, [f], 1)

@@ -1,0 +1,134 @@
+"""Device matrix/vector handles (mirror python/cudolfinx/la.py:9-75).
+
+In the reference these wrap PETSc AIJCUSPARSE / VECCUDA objects whose device
+arrays the kernels write (cpp/cudolfinx/la/CUDASeqMatrix.cpp:435-457,
+CUDAVector.cpp:348-365).  Here the device arrays are torch tensors (device
+memory only; torch is not on the compute path) and the CSR pattern belongs to
+an engine sparsity object.  ``.mat`` / ``.vector`` hand out what a PETSc-free
+consumer needs: ``mat`` is a host scipy CSR copy, ``device_csr()`` gives the
+device arrays (row_ptr, col, values) for a GPU solver, and ``vector`` is the
+device tensor.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib
+
+
+class Sparsity:
+    """Engine CSR pattern (create_cuda_matrix, cpp/cudolfinx/la/petsc.cpp:14-151)."""
+
+    def __init__(self, ctx, handle):
+        self.ctx = ctx
+        self.handle = handle
+        r, c, n = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        _lib.check(_lib.lib.fe_sparsity_info(handle, ctypes.byref(r), ctypes.byref(c), ctypes.byref(n)),
+                   "fe_sparsity_info")
+        self.num_rows, self.num_cols, self.nnz = r.value, c.value, n.value
+
+    @classmethod
+    def build(cls, ctx, dofmap0, dofmap1):
+        h = _lib.out_handle()
+        _lib.check(_lib.lib.fe_sparsity_build(dofmap0.handle, dofmap1.handle, h), "fe_sparsity_build")
+        return cls(ctx, h.value)
+
+    @classmethod
+    def from_csr(cls, ctx, row_ptr, col, num_cols):
+        rp = np.ascontiguousarray(row_ptr, dtype=np.int32)
+        cl = np.ascontiguousarray(col, dtype=np.int32)
+        h = _lib.out_handle()
+        _lib.check(_lib.lib.fe_sparsity_create(ctx.handle, rp.ctypes.data, cl.ctypes.data if cl.size else None,
+                                               len(rp) - 1, num_cols, h), "fe_sparsity_create")
+        return cls(ctx, h.value)
+
+    def to_host(self):
+        rp = np.empty(self.num_rows + 1, dtype=np.int32)
+        cl = np.empty(self.nnz, dtype=np.int32)
+        _lib.check(_lib.lib.fe_sparsity_copy_to_host(self.handle, rp.ctypes.data, cl.ctypes.data if self.nnz else None),
+                   "fe_sparsity_copy_to_host")
+        return rp, cl
+
+    def device_arrays(self):
+        """(row_ptr, col) as int32 device tensors viewing the engine's arrays."""
+        rp, cl = ctypes.c_void_p(), ctypes.c_void_p()
+        _lib.check(_lib.lib.fe_sparsity_device_arrays(self.handle, ctypes.byref(rp), ctypes.byref(cl)),
+                   "fe_sparsity_device_arrays")
+        return (_DeviceView(rp.value, self.num_rows + 1, "<i4", self).tensor(),
+                _DeviceView(cl.value, self.nnz, "<i4", self).tensor())
+
+    def __del__(self):
+        if getattr(self, "handle", None):
+            _lib.lib.fe_sparsity_destroy(self.handle)
+            self.handle = None
+
+
+class _DeviceView:
+    """__cuda_array_interface__ view of engine-owned device memory."""
+
+    def __init__(self, ptr, n, typestr, owner):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": typestr, "data": (ptr or 0, False),
+                                         "version": 3, "strides": None}
+        self._owner = owner
+
+    def tensor(self):
+        return torch.as_tensor(self, device="cuda")
+
+
+class CUDAVector:
+    """Vector on the device."""
+
+    def __init__(self, ctx, n: int, values: torch.Tensor | None = None):
+        self._ctx = ctx
+        self.size = n
+        self._values = values if values is not None else torch.zeros(n, dtype=torch.float64,
+                                                                      device=ctx.torch_device)
+
+    @property
+    def vector(self) -> torch.Tensor:
+        """The device values (stand-in for the PETSc Vec of the reference)."""
+        return self._values
+
+    @property
+    def array(self) -> np.ndarray:
+        return self.to_host()
+
+    def to_host(self) -> np.ndarray:
+        """Copy device values to a host array (CUDAVector::copy_vector_values_to_host)."""
+        torch.cuda.current_stream(self._ctx.device).synchronize()
+        return self._values.cpu().numpy()
+
+
+class CUDAMatrix:
+    """CSR matrix on the device: engine pattern + torch value array."""
+
+    def __init__(self, ctx, sparsity: Sparsity, values: torch.Tensor | None = None):
+        self._ctx = ctx
+        self.sparsity = sparsity
+        self._values = values if values is not None else torch.zeros(sparsity.nnz, dtype=torch.float64,
+                                                                     device=ctx.torch_device)
+
+    @property
+    def values(self) -> torch.Tensor:
+        return self._values
+
+    def assemble(self):
+        """Finalise: wait for the assembly and surface device error words
+        (the reference calls MatAssemblyBegin/End here, wrappers/fem.cpp:176-181)."""
+        self._ctx.synchronize()
+
+    def device_csr(self):
+        rp, cl = self.sparsity.device_arrays()
+        return rp, cl, self._values
+
+    @property
+    def mat(self):
+        """Host scipy.sparse CSR copy (PETSc-free stand-in for the reference's petsc4py Mat)."""
+        import scipy.sparse as sp
+        self.assemble()
+        rp, cl = self.sparsity.to_host()
+        return sp.csr_matrix((self._values.cpu().numpy(), cl, rp),
+                             shape=(self.sparsity.num_rows, self.sparsity.num_cols))

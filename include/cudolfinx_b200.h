@@ -1,0 +1,196 @@
+/* cudolfinx_b200.h -- C ABI of the B200 finite-element assembly engine.
+ *
+ * Drop-in boundary for the cudolfinx assembly path.  Every entry point returns
+ * an int status (FE_OK = 0); on failure fe_last_error() gives a thread-local
+ * message naming the failing call and source location, the same information
+ * the reference puts in its std::runtime_error (e.g.
+ * cpp/cudolfinx/fem/CUDAFormIntegral.h:961-975) which nanobind turns into a
+ * Python RuntimeError.
+ *
+ * Conventions
+ *  - Sizes are int64_t, indices int32_t (the reference's dofmaps and CSR are
+ *    int32: cpp/cudolfinx/fem/CUDADofMap.cpp:199-236, la/CUDASeqMatrix.cpp:101-198).
+ *  - Pointers documented "host" are read during the call; "device" pointers
+ *    must be device memory of the context's GPU.  CSR value arrays and vectors
+ *    are caller-owned device memory (PETSc lends its AIJCUSPARSE / VECCUDA
+ *    arrays in the reference: la/CUDASeqMatrix.cpp:435-457,
+ *    la/CUDAVector.cpp:348-365).
+ *  - `stream` is a cudaStream_t passed as void* (NULL = the legacy default
+ *    stream).  Work is enqueued asynchronously; nothing synchronises unless
+ *    documented.  The reference launches on the NULL stream and calls
+ *    cuCtxSynchronize after each kernel (CUDAFormIntegral.cpp:2354-2361).
+ */
+#ifndef CUDOLFINX_B200_H
+#define CUDOLFINX_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum fe_status {
+  FE_OK = 0,
+  FE_ERR_ARG = 1,       /* invalid argument / size mismatch            */
+  FE_ERR_CUDA = 2,      /* a CUDA runtime call or kernel failed         */
+  FE_ERR_PATTERN = 3,   /* an element coupling is missing from the CSR  */
+  FE_ERR_NOMEM = 4,     /* device allocation refused                    */
+  FE_ERR_DEVICE = 5,    /* a kernel reported an error word (no trap)    */
+  FE_ERR_NOT_CONVERGED = 6
+};
+
+typedef struct fe_context_s* fe_context;
+typedef struct fe_mesh_s* fe_mesh;
+typedef struct fe_dofmap_s* fe_dofmap;
+typedef struct fe_sparsity_s* fe_sparsity;
+typedef struct fe_bc_s* fe_bc;
+typedef struct fe_form_s* fe_form;
+
+/* Built-in forms (element tensors written from the mathematics; replaces the
+ * FFCx tabulate_tensor bodies wrapped by python/cudolfinx/jit.py:61-114). */
+enum fe_form_kind {
+  FE_FORM_P1_STIFFNESS = 1,    /* k*inner(grad u, grad v)*dx, P1;   coeff 0 = k    */
+  FE_FORM_P2_STIFFNESS = 2,    /* k*inner(grad u, grad v)*dx, P2;   coeff 0 = k    */
+  FE_FORM_VP2_ELASTICITY = 3,  /* 2mu eps(u):eps(v) + lam div u div v, vector P2;
+                                  coeff 0 = lam, coeff 1 = mu                       */
+  FE_FORM_P1_LOAD = 11,        /* f*v*dx, P1;        coeff 0 = f                    */
+  FE_FORM_P2_LOAD = 12,        /* f*v*dx, P2;        coeff 0 = f                    */
+  FE_FORM_VP2_LOAD = 13        /* inner(f, v)*dx, vector P2; coeff 0 = f (3 comps)  */
+};
+
+/* Coefficient representations (CUDAFormCoefficients.h:352-365 packs these
+ * per cell; here the element kernels gather them directly). */
+enum fe_coeff_kind {
+  FE_COEFF_CONSTANT = 0, /* one value (or 3 for a vector load) for all cells */
+  FE_COEFF_DG0 = 1,      /* one value per cell (3 per cell for a vector load) */
+  FE_COEFF_P1 = 2        /* vertex values through a P1 dofmap                 */
+};
+
+/* Element-tensor precision of a matrix form. */
+enum fe_precision {
+  FE_PREC_FP64 = 0, /* FP64 throughout (parity path)                                   */
+  FE_PREC_FP32 = 1  /* FP64 geometry, FP32 element-tensor contraction, FP64 accumulation */
+};
+
+/* Scatter variants of fe_assemble_matrix (flags). */
+#define FE_ASM_ZERO 1u            /* zero the values first (assemble.py:52 zero=True) */
+#define FE_ASM_DETERMINISTIC 2u   /* bitwise-reproducible owner-computes gather        */
+
+/* ---- errors / context --------------------------------------------------- */
+const char* fe_last_error(void);
+const char* fe_version(void);
+
+/* Replaces CUDA::Context (cpp/cudolfinx/common/CUDA.cpp:28-52) and
+ * cudolfinx.context.get_cuda_context (python/cudolfinx/context.py:29-35). */
+int fe_context_create(int device, fe_context* out);
+int fe_context_destroy(fe_context ctx);
+/* Blocks until all work of the context's GPU is done; returns the first
+ * pending device error word (see FE_ERR_DEVICE). */
+int fe_context_synchronize(fe_context ctx);
+
+/* ---- mesh / dofmaps ------------------------------------------------------ */
+/* Replaces CUDAMesh (cpp/cudolfinx/mesh/CUDAMesh.h:41-163): 3 FP64 coordinates
+ * per node (host) and the affine-tet geometry dofmap int32[num_cells*4] (host). */
+int fe_mesh_create(fe_context ctx, const double* coords, int64_t num_nodes,
+                   const int32_t* geom_dofmap, int64_t num_cells, int nodes_per_cell,
+                   fe_mesh* out);
+int fe_mesh_destroy(fe_mesh m);
+
+/* Replaces CUDADofMap (cpp/cudolfinx/fem/CUDADofMap.cpp:199-236).  Cell dofs
+ * are BLOCK dofs int32[num_cells*dofs_per_cell] (host); scalar dof = block*bs + comp
+ * is derived in the kernels instead of storing the unrolled map. */
+int fe_dofmap_create(fe_context ctx, const int32_t* cell_dofs, int64_t num_cells,
+                     int dofs_per_cell, int bs, int64_t num_blocks, fe_dofmap* out);
+int fe_dofmap_destroy(fe_dofmap d);
+
+/* ---- sparsity ------------------------------------------------------------ */
+/* Replaces create_cuda_matrix (cpp/cudolfinx/fem/petsc.h:31-37 ->
+ * la/petsc.cpp:14-151): the DOLFINx SparsityPattern of a cell integral (sorted
+ * unique block columns per block row) unrolled to scalar AIJ exactly as
+ * la/petsc.cpp:45-65 does.  Built on the host from the dofmaps. */
+int fe_sparsity_build(fe_dofmap rows, fe_dofmap cols, fe_sparsity* out);
+/* Adopt an existing pattern (e.g. the arrays of a PETSc AIJ matrix); host arrays. */
+int fe_sparsity_create(fe_context ctx, const int32_t* row_ptr, const int32_t* col,
+                       int64_t num_rows, int64_t num_cols, fe_sparsity* out);
+int fe_sparsity_info(fe_sparsity s, int64_t* num_rows, int64_t* num_cols, int64_t* nnz);
+/* Copy the pattern to host arrays of num_rows+1 and nnz entries. */
+int fe_sparsity_copy_to_host(fe_sparsity s, int32_t* row_ptr, int32_t* col);
+/* Host-only construction of the same pattern, without a GPU (e.g. to create
+ * the PETSc AIJ matrix that the device values are later written into).  The
+ * arrays are allocated by the library and released with fe_free_host. */
+int fe_pattern_build_host(const int32_t* dofs0, const int32_t* dofs1, int64_t num_cells, int k0, int k1,
+                          int bs0, int bs1, int64_t num_blocks0, int64_t num_blocks1, int64_t* nnz,
+                          int32_t** row_ptr, int32_t** col);
+void fe_free_host(void* p);
+/* Device pointers of the pattern (owned by the sparsity object). */
+int fe_sparsity_device_arrays(fe_sparsity s, const int32_t** row_ptr, const int32_t** col);
+int fe_sparsity_destroy(fe_sparsity s);
+
+/* ---- forms ------------------------------------------------------------- */
+/* Replaces CUDAForm (cpp/cudolfinx/fem/CUDAForm.h:40-147) for the built-in
+ * forms.  `trial` is NULL for linear forms. */
+int fe_form_create(fe_context ctx, int form_kind, fe_mesh mesh, fe_dofmap test,
+                   fe_dofmap trial, fe_form* out);
+/* Upload coefficient `index` (replaces CUDAForm::to_device + pack_coefficients,
+ * CUDAForm.h:195-199, CUDAAssembler.h:177-283).  `values` is host memory when
+ * values_on_device == 0 (copied on `stream`), else device memory that the form
+ * reads in place during later assembly calls.  P1 coefficients need the P1
+ * dofmap `cmap`; n is the number of values. */
+int fe_form_set_coefficient(fe_form f, int index, int coeff_kind, fe_dofmap cmap,
+                            const double* values, int64_t n, int values_on_device,
+                            void* stream);
+int fe_form_set_precision(fe_form f, int precision);
+/* Bind the matrix pattern and build the cell-to-slot map once (the reference's
+ * unused lookup-table prototype, CUDAFormIntegral.cpp:1230-1407, made the
+ * default).  Fails with FE_ERR_PATTERN if a cell coupling is missing. */
+int fe_form_bind_sparsity(fe_form f, fe_sparsity s, void* stream);
+int fe_form_destroy(fe_form f);
+
+/* ---- Dirichlet BCs ------------------------------------------------------- */
+/* Replaces CUDADirichletBC (cpp/cudolfinx/fem/CUDADirichletBC.h:56-194):
+ * markers u8[num_dofs] (scalar dofs), dof list int32[n_bc] with the n_owned
+ * owned dofs first, and full-length values g f64[num_dofs]; host arrays. */
+int fe_bc_create(fe_context ctx, int64_t num_dofs, const uint8_t* markers,
+                 const int32_t* dofs, int64_t n_bc, int64_t n_owned, const double* g,
+                 fe_bc* out);
+/* Replaces CUDADirichletBC::update (CUDADirichletBC.h:255-261). */
+int fe_bc_update(fe_bc bc, const double* g, void* stream);
+int fe_bc_destroy(fe_bc bc);
+
+/* ---- assembly ----------------------------------------------------------- */
+/* Replaces zero_matrix_entries + assemble_matrix_on_device + set_diagonal
+ * (python/cudolfinx/wrappers/fem.cpp:212-252, CUDAAssembler.h:681-740,
+ * CUDAAssembler.cpp:131-164).  values: device f64[nnz] of the bound pattern.
+ * BC rows/cols of bc0/bc1 (may be NULL) receive no element contributions and
+ * owned bc0 rows get `diagonal` on the diagonal when the form is square. */
+int fe_assemble_matrix(fe_form a, double* values, fe_bc bc0, fe_bc bc1, double diagonal,
+                       unsigned flags, void* stream);
+/* Replaces zero_matrix_entries / zero_vector_entries (wrappers/fem.cpp:212-222,
+ * 256-266; kernel CUDAAssembler.cpp:38-56): values[0..n) = 0 on `stream`. */
+int fe_zero_entries(double* values, int64_t n, void* stream);
+/* Replaces zero_vector_entries + assemble_vector_on_device
+ * (wrappers/fem.cpp:254-289, CUDAAssembler.h:367-424). b: device f64. */
+int fe_assemble_vector(fe_form L, double* b, unsigned flags, void* stream);
+/* Replaces apply_lifting_on_device (wrappers/fem.cpp:327-355,
+ * CUDAAssembler.h:562-603): b -= scale * A_i (g_i - x0_i) for each form a[i]
+ * on the columns of bc1[i]; x0 may be NULL or hold NULL entries. */
+int fe_apply_lifting(double* b, int num_forms, const fe_form* a, const fe_bc* bc1,
+                     const double* const* x0, double scale, void* stream);
+/* Replaces set_bc_on_device (wrappers/fem.cpp:357-383, CUDAAssembler.h:443-529):
+ * b[d] = scale * (g[d] - x0[d]) for the BC dofs; x0 may be NULL. */
+int fe_set_bc(double* b, int64_t num_values, fe_bc bc, const double* x0, double scale,
+              void* stream);
+
+/* ---- solver (the reference hands A, b to PETSc KSP cg + jacobi:
+ * python/examples/poisson.py:116-125) ------------------------------------ */
+/* Jacobi-preconditioned CG on device.  x is the initial guess and the result
+ * (device f64[n]).  Stops when ||r||_2 <= rtol*||b||_2 or after max_iter; then
+ * *iterations and *rel_residual are written (host) and the call synchronises
+ * the stream.  Returns FE_ERR_NOT_CONVERGED if max_iter was reached. */
+int fe_pcg_solve(fe_sparsity s, const double* values, const double* b, double* x, double rtol,
+                 int max_iter, int* iterations, double* rel_residual, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CUDOLFINX_B200_H */

@@ -1,0 +1,400 @@
+/* C restatement of the cudolfinx assembly path (TEST INFRASTRUCTURE ONLY).
+ *
+ * This is the checker and the timed CPU baseline ("port" kind), never the
+ * product: only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline /
+ * --impl reference legs load it.  Parity status: unpinned against DOLFINx
+ * (the reference and DOLFINx cannot run here); pinned to the closed-form
+ * checks in tests/test_oracle.py and to the numpy oracle.
+ *
+ * Algorithm (reference file:line, paths relative to the cuda-dolfinx tree):
+ *   matrix  : per cell tabulate Ae, skip BC rows/cols, locate each column in
+ *             its CSR row by binary search and add
+ *             (cpp/cudolfinx/fem/CUDAFormIntegral.cpp:1154-1224,
+ *              binary_search :2572-2602), then set the diagonal of owned BC
+ *             rows (cpp/cudolfinx/fem/CUDAAssembler.cpp:131-164).  This is also
+ *             the structure of DOLFINx's CPU assemble_matrix + MatSetValues.
+ *   vector  : per cell element vector added into b
+ *             (cpp/cudolfinx/fem/CUDAFormIntegral.cpp:309-355).
+ *   lifting : b -= scale*Ae[:,bc](g - x0)[bc] for cells with a BC column
+ *             (cpp/cudolfinx/fem/CUDAFormIntegral.cpp:647-715).
+ *   set_bc  : b[d] = scale*(g[d]-x0[d]) (cpp/cudolfinx/fem/CUDAAssembler.cpp:115-124).
+ *
+ * Threading follows DOLFINx's ghosted MPI assembly: each thread owns a range
+ * of block rows and assembles every cell touching them, inserting only its
+ * own rows (no atomics; shared cells are recomputed).
+ *
+ * Element kinds: 1 = P1 Poisson (k DG0 or 1), 2 = P2 Poisson (k P1 field),
+ * 3 = vector P2 elasticity (lam, mu DG0).  Reference tensors are passed in
+ * by cfem_set_tables() from the exact rational tables of fem_oracle.py.
+ */
+#include <math.h>
+#include <pthread.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+static double R2w[4][3][3][10][10]; /* int lambda_m d_a phi_i d_b phi_j */
+static double R2[3][3][10][10];     /* int d_a phi_i d_b phi_j          */
+static double W2[10];               /* int phi_i                         */
+
+void cfem_set_tables(const double* r2w, const double* r2, const double* w2)
+{
+  memcpy(R2w, r2w, sizeof(R2w));
+  memcpy(R2, r2, sizeof(R2));
+  memcpy(W2, w2, sizeof(W2));
+}
+
+/* ---------------- geometry ---------------- */
+static inline void cell_geom(const double* coords, const int32_t* v, double K[3][3], double* adet)
+{
+  double x0[3], J[3][3];
+  for (int r = 0; r < 3; ++r) x0[r] = coords[3 * (int64_t)v[0] + r];
+  for (int c = 0; c < 3; ++c)
+    for (int r = 0; r < 3; ++r) J[r][c] = coords[3 * (int64_t)v[c + 1] + r] - x0[r];
+  double c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1];
+  double c01 = J[1][2] * J[2][0] - J[1][0] * J[2][2];
+  double c02 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
+  double det = J[0][0] * c00 + J[0][1] * c01 + J[0][2] * c02;
+  double id = 1.0 / det;
+  K[0][0] = c00 * id;
+  K[1][0] = c01 * id;
+  K[2][0] = c02 * id;
+  K[0][1] = (J[0][2] * J[2][1] - J[0][1] * J[2][2]) * id;
+  K[1][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) * id;
+  K[2][1] = (J[0][1] * J[2][0] - J[0][0] * J[2][1]) * id;
+  K[0][2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) * id;
+  K[1][2] = (J[0][2] * J[1][0] - J[0][0] * J[1][2]) * id;
+  K[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) * id;
+  *adet = fabs(det);
+}
+
+static const double P1G[4][3] = {{-1, -1, -1}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+
+/* Ae is k0 x k1 row-major (k0 = k1 = 4, 10 or 30) */
+static void tabulate(int kind, const double* coords, const int32_t* v, int64_t c,
+                     const double* coeff0, const double* coeff1, double* Ae)
+{
+  double K[3][3], adet;
+  cell_geom(coords, v, K, &adet);
+  if (kind == 1) {
+    double G[4][3];
+    for (int i = 0; i < 4; ++i)
+      for (int b = 0; b < 3; ++b)
+        G[i][b] = P1G[i][0] * K[0][b] + P1G[i][1] * K[1][b] + P1G[i][2] * K[2][b];
+    double s = adet / 6.0 * (coeff0 ? coeff0[c] : 1.0);
+    for (int i = 0; i < 4; ++i)
+      for (int j = 0; j < 4; ++j)
+        Ae[i * 4 + j] = s * (G[i][0] * G[j][0] + G[i][1] * G[j][1] + G[i][2] * G[j][2]);
+  } else if (kind == 2) {
+    double Gh[3][3];
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b)
+        Gh[a][b] = adet * (K[a][0] * K[b][0] + K[a][1] * K[b][1] + K[a][2] * K[b][2]);
+    double km[4];
+    for (int m = 0; m < 4; ++m) km[m] = coeff0[v[m]];
+    for (int i = 0; i < 100; ++i) Ae[i] = 0.0;
+    for (int m = 0; m < 4; ++m)
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) {
+          double w = km[m] * Gh[a][b];
+          const double* R = &R2w[m][a][b][0][0];
+          for (int e = 0; e < 100; ++e) Ae[e] += w * R[e];
+        }
+  } else {
+    static __thread double D[3][3][100];
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b) {
+        double* Dab = D[a][b];
+        for (int e = 0; e < 100; ++e) Dab[e] = 0.0;
+        for (int p = 0; p < 3; ++p)
+          for (int q = 0; q < 3; ++q) {
+            double w = adet * K[p][a] * K[q][b];
+            const double* R = &R2[p][q][0][0];
+            for (int e = 0; e < 100; ++e) Dab[e] += w * R[e];
+          }
+      }
+    double lam = coeff0[c], mu = coeff1[c];
+    for (int i = 0; i < 10; ++i)
+      for (int a = 0; a < 3; ++a)
+        for (int j = 0; j < 10; ++j)
+          for (int b = 0; b < 3; ++b) {
+            int e = i * 10 + j;
+            double S = (a == b) ? (D[0][0][e] + D[1][1][e] + D[2][2][e]) : 0.0;
+            Ae[(3 * i + a) * 30 + 3 * j + b] = mu * (S + D[b][a][e]) + lam * D[a][b][e];
+          }
+  }
+}
+
+/* be has k0 entries */
+static void tabulate_vec(int kind, const double* coords, const int32_t* v, int64_t c,
+                         const double* f, double* be)
+{
+  double K[3][3], adet;
+  cell_geom(coords, v, K, &adet);
+  if (kind == 1) {
+    double s = f[v[0]] + f[v[1]] + f[v[2]] + f[v[3]];
+    for (int i = 0; i < 4; ++i) be[i] = adet / 120.0 * (f[v[i]] + s);
+  } else if (kind == 2) {
+    for (int i = 0; i < 10; ++i) be[i] = f[c] * adet * W2[i];
+  } else {
+    for (int i = 0; i < 10; ++i)
+      for (int a = 0; a < 3; ++a) be[3 * i + a] = f[3 * c + a] * adet * W2[i];
+  }
+}
+
+static inline int kdofs(int kind) { return kind == 1 ? 4 : 10; }
+
+/* ---------------- row-owning partition ---------------- */
+typedef struct {
+  int nthreads;
+  int64_t* row_lo; /* block-row range [row_lo[t], row_lo[t+1]) */
+  int64_t** cells; /* cells touching the range */
+  int64_t* ncells;
+} plan_t;
+
+void* cfem_plan_create(int nthreads, const int32_t* dofs, int64_t ncells, int k, int64_t nblocks)
+{
+  plan_t* p = (plan_t*)calloc(1, sizeof(plan_t));
+  p->nthreads = nthreads;
+  p->row_lo = (int64_t*)malloc(sizeof(int64_t) * (nthreads + 1));
+  for (int t = 0; t <= nthreads; ++t) p->row_lo[t] = nblocks * t / nthreads;
+  p->cells = (int64_t**)calloc(nthreads, sizeof(int64_t*));
+  p->ncells = (int64_t*)calloc(nthreads, sizeof(int64_t));
+  int64_t* count = (int64_t*)calloc(nthreads, sizeof(int64_t));
+  int* owner = (int*)malloc(sizeof(int) * (size_t)(nblocks > 0 ? nblocks : 1));
+  for (int t = 0; t < nthreads; ++t)
+    for (int64_t r = p->row_lo[t]; r < p->row_lo[t + 1]; ++r) owner[r] = t;
+  char* seen = (char*)malloc(nthreads);
+  for (int pass = 0; pass < 2; ++pass) {
+    for (int t = 0; t < nthreads; ++t) {
+      if (pass == 1) p->cells[t] = (int64_t*)malloc(sizeof(int64_t) * (count[t] ? count[t] : 1));
+      count[t] = 0;
+    }
+    for (int64_t c = 0; c < ncells; ++c) {
+      memset(seen, 0, nthreads);
+      for (int i = 0; i < k; ++i) {
+        int t = owner[dofs[c * k + i]];
+        if (!seen[t]) {
+          seen[t] = 1;
+          if (pass == 1) p->cells[t][count[t]] = c;
+          count[t]++;
+        }
+      }
+    }
+  }
+  for (int t = 0; t < nthreads; ++t) p->ncells[t] = count[t];
+  free(seen);
+  free(owner);
+  free(count);
+  return p;
+}
+
+void cfem_plan_destroy(void* vp)
+{
+  plan_t* p = (plan_t*)vp;
+  if (!p) return;
+  for (int t = 0; t < p->nthreads; ++t) free(p->cells[t]);
+  free(p->cells);
+  free(p->ncells);
+  free(p->row_lo);
+  free(p);
+}
+
+int64_t cfem_plan_total_cells(void* vp)
+{
+  plan_t* p = (plan_t*)vp;
+  int64_t s = 0;
+  for (int t = 0; t < p->nthreads; ++t) s += p->ncells[t];
+  return s;
+}
+
+/* ---------------- jobs ---------------- */
+typedef struct {
+  plan_t* plan;
+  int t, kind, bs, op;
+  const double *coords, *coeff0, *coeff1, *f, *g, *x0;
+  const int32_t *cells, *dofs, *row_ptr, *col, *bc_dofs;
+  const uint8_t* markers;
+  double *values, *b;
+  double diagonal, scale;
+  int64_t n_bc;
+} job_t;
+
+static inline int64_t find_col(const int32_t* row_ptr, const int32_t* col, int64_t row, int32_t c)
+{
+  int64_t lo = row_ptr[row], hi = row_ptr[row + 1];
+  while (lo < hi) {
+    int64_t mid = (lo + hi) >> 1;
+    if (col[mid] < c) lo = mid + 1;
+    else hi = mid;
+  }
+  return (lo < row_ptr[row + 1] && col[lo] == c) ? lo : -1;
+}
+
+static void* run_job(void* arg)
+{
+  job_t* J = (job_t*)arg;
+  plan_t* P = J->plan;
+  const int k = kdofs(J->kind), bs = J->bs, ks = k * bs;
+  const int64_t rlo = P->row_lo[J->t] * bs, rhi = P->row_lo[J->t + 1] * bs;
+  double Ae[900], be[30];
+  int64_t rows[30];
+  int32_t colsx[30];
+  const int64_t* my = P->cells[J->t];
+  const int64_t nmy = P->ncells[J->t];
+  if (J->op == 0) { /* matrix */
+    for (int64_t r = rlo; r < rhi; ++r)
+      for (int64_t s = J->row_ptr[r]; s < J->row_ptr[r + 1]; ++s) J->values[s] = 0.0;
+    for (int64_t q = 0; q < nmy; ++q) {
+      int64_t c = my[q];
+      tabulate(J->kind, J->coords, J->cells + 4 * c, c, J->coeff0, J->coeff1, Ae);
+      for (int i = 0; i < k; ++i)
+        for (int a = 0; a < bs; ++a) {
+          rows[i * bs + a] = (int64_t)J->dofs[c * k + i] * bs + a;
+          colsx[i * bs + a] = J->dofs[c * k + i] * bs + a;
+        }
+      for (int ii = 0; ii < ks; ++ii) {
+        int64_t r = rows[ii];
+        if (r < rlo || r >= rhi || J->markers[r]) continue;
+        for (int jj = 0; jj < ks; ++jj) {
+          if (J->markers[colsx[jj]]) continue;
+          int64_t s = find_col(J->row_ptr, J->col, r, colsx[jj]);
+          if (s >= 0) J->values[s] += Ae[ii * ks + jj];
+        }
+      }
+    }
+    for (int64_t q = 0; q < J->n_bc; ++q) {
+      int64_t r = J->bc_dofs[q];
+      if (r < rlo || r >= rhi) continue;
+      int64_t s = find_col(J->row_ptr, J->col, r, (int32_t)r);
+      if (s >= 0) J->values[s] = J->diagonal;
+    }
+  } else if (J->op == 1) { /* vector */
+    for (int64_t r = rlo; r < rhi; ++r) J->b[r] = 0.0;
+    for (int64_t q = 0; q < nmy; ++q) {
+      int64_t c = my[q];
+      tabulate_vec(J->kind, J->coords, J->cells + 4 * c, c, J->f, be);
+      for (int i = 0; i < k; ++i)
+        for (int a = 0; a < bs; ++a) {
+          int64_t r = (int64_t)J->dofs[c * k + i] * bs + a;
+          if (r >= rlo && r < rhi) J->b[r] += be[i * bs + a];
+        }
+    }
+  } else { /* lifting */
+    for (int64_t q = 0; q < nmy; ++q) {
+      int64_t c = my[q];
+      int any = 0;
+      for (int i = 0; i < k && !any; ++i)
+        for (int a = 0; a < bs; ++a)
+          if (J->markers[(int64_t)J->dofs[c * k + i] * bs + a]) any = 1;
+      if (!any) continue;
+      tabulate(J->kind, J->coords, J->cells + 4 * c, c, J->coeff0, J->coeff1, Ae);
+      double d[30];
+      for (int j = 0; j < k; ++j)
+        for (int b = 0; b < bs; ++b) {
+          int64_t cc = (int64_t)J->dofs[c * k + j] * bs + b;
+          d[j * bs + b] = J->markers[cc] ? (J->g[cc] - (J->x0 ? J->x0[cc] : 0.0)) : 0.0;
+        }
+      for (int ii = 0; ii < ks; ++ii) {
+        int64_t r = (int64_t)J->dofs[c * k + ii / bs] * bs + ii % bs;
+        if (r < rlo || r >= rhi) continue;
+        double s = 0.0;
+        for (int jj = 0; jj < ks; ++jj) s += Ae[ii * ks + jj] * d[jj];
+        J->b[r] -= J->scale * s;
+      }
+    }
+  }
+  return NULL;
+}
+
+static void run_all(job_t* proto)
+{
+  plan_t* P = proto->plan;
+  int T = P->nthreads;
+  pthread_t* th = (pthread_t*)malloc(sizeof(pthread_t) * T);
+  job_t* jobs = (job_t*)malloc(sizeof(job_t) * T);
+  for (int t = 0; t < T; ++t) {
+    jobs[t] = *proto;
+    jobs[t].t = t;
+    pthread_create(&th[t], NULL, run_job, &jobs[t]);
+  }
+  for (int t = 0; t < T; ++t) pthread_join(th[t], NULL);
+  free(jobs);
+  free(th);
+}
+
+void cfem_assemble_matrix(void* plan, int kind, const double* coords, const int32_t* cells,
+                          const int32_t* dofs, int bs, const double* coeff0, const double* coeff1,
+                          const int32_t* row_ptr, const int32_t* col, const uint8_t* markers,
+                          double* values, double diagonal, const int32_t* bc_dofs, int64_t n_bc)
+{
+  job_t J;
+  memset(&J, 0, sizeof(J));
+  J.plan = (plan_t*)plan;
+  J.kind = kind;
+  J.bs = bs;
+  J.op = 0;
+  J.coords = coords;
+  J.cells = cells;
+  J.dofs = dofs;
+  J.coeff0 = coeff0;
+  J.coeff1 = coeff1;
+  J.row_ptr = row_ptr;
+  J.col = col;
+  J.markers = markers;
+  J.values = values;
+  J.diagonal = diagonal;
+  J.bc_dofs = bc_dofs;
+  J.n_bc = n_bc;
+  run_all(&J);
+}
+
+void cfem_assemble_vector(void* plan, int kind, const double* coords, const int32_t* cells,
+                          const int32_t* dofs, int bs, const double* f, double* b)
+{
+  job_t J;
+  memset(&J, 0, sizeof(J));
+  J.plan = (plan_t*)plan;
+  J.kind = kind;
+  J.bs = bs;
+  J.op = 1;
+  J.coords = coords;
+  J.cells = cells;
+  J.dofs = dofs;
+  J.f = f;
+  J.b = b;
+  run_all(&J);
+}
+
+void cfem_apply_lifting(void* plan, int kind, const double* coords, const int32_t* cells,
+                        const int32_t* dofs, int bs, const double* coeff0, const double* coeff1,
+                        const uint8_t* markers, const double* g, const double* x0, double scale,
+                        double* b)
+{
+  job_t J;
+  memset(&J, 0, sizeof(J));
+  J.plan = (plan_t*)plan;
+  J.kind = kind;
+  J.bs = bs;
+  J.op = 2;
+  J.coords = coords;
+  J.cells = cells;
+  J.dofs = dofs;
+  J.coeff0 = coeff0;
+  J.coeff1 = coeff1;
+  J.markers = markers;
+  J.g = g;
+  J.x0 = x0;
+  J.scale = scale;
+  J.b = b;
+  run_all(&J);
+}
+
+void cfem_set_bc(double* b, const int32_t* bc_dofs, int64_t n_bc, const double* g,
+                 const double* x0, double scale)
+{
+  for (int64_t q = 0; q < n_bc; ++q) {
+    int64_t d = bc_dofs[q];
+    b[d] = scale * (g[d] - (x0 ? x0[d] : 0.0));
+  }
+}

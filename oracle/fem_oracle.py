@@ -1,0 +1,593 @@
+"""CPU oracle for the cudolfinx assembly hot path (TEST INFRASTRUCTURE ONLY).
+
+This module is the checker, never the product: only ``tests/``,
+``__graft_entry__.smoke()`` and the ``cpu_baseline`` leg of ``bench.py`` may
+import it.  The CUDA library must never route through it.
+
+Parity status: **parity unpinned against DOLFINx** -- the reference publishes
+no golden vectors and its own tests compare against DOLFINx at run time
+(python/test/test_cuda_assembly.py:93-209); DOLFINx, FFCx, basix and PETSc
+are not installed here, so the reference cannot be run.  The oracle is instead
+pinned to closed-form known answers (tests/test_oracle.py): the P1 reference
+stiffness matrix, exactly integrated reference tensors (rational arithmetic),
+patch tests (linear fields are reproduced exactly), rigid-body modes of the
+elasticity operator, and integral identities of the load vectors.
+
+What it restates (reference file:line):
+
+* mesh        -- unit cube, n^3 hexes x 6 tets sharing the v0-v7 diagonal, the
+                 topology DOLFINx ``create_box(CellType.tetrahedron)`` produces
+                 (python/examples/poisson.py:34-40).
+* dofmaps     -- P1 = vertex numbering; P2 = vertices + edge midpoints with the
+                 basix tetrahedron edge order (2,3),(1,3),(1,2),(0,3),(0,2),(0,1);
+                 a blocked (bs=3) map is unrolled as ``dof*bs + comp``
+                 (cpp/cudolfinx/fem/CUDADofMap.cpp:210-229).
+* sparsity    -- sorted unique columns per row, block rows unrolled to scalar
+                 AIJ (cpp/cudolfinx/la/petsc.cpp:38-65).
+* matrix      -- per cell: element tensor, skip BC rows/cols, add into CSR
+                 (cpp/cudolfinx/fem/CUDAFormIntegral.cpp:1154-1224), then set the
+                 diagonal of BC rows (cpp/cudolfinx/fem/CUDAAssembler.cpp:131-164).
+* vector      -- per cell element vector added into b
+                 (cpp/cudolfinx/fem/CUDAFormIntegral.cpp:309-355).
+* lifting     -- b[rows] -= scale * Ae[:, bc cols] (g - x0)[bc cols] for cells
+                 with a BC column (cpp/cudolfinx/fem/CUDAFormIntegral.cpp:647-715).
+* set_bc      -- b[d] = scale * (g[d] - x0[d]) for BC dofs
+                 (cpp/cudolfinx/fem/CUDAAssembler.cpp:115-124).
+
+Element tensors are computed from first principles (FFCx generates them in the
+reference; they are exact for these polynomial integrands, so any exact
+quadrature agrees up to rounding):
+
+* P1 Poisson   Ae_ij = k_c |detJ|/6 grad(phi_i).grad(phi_j)   (k DG0 or 1)
+* P2 Poisson   Ae_ij = sum_m k_m sum_ab G_ab R[m,a,b,i,j],  G = |detJ| K K^T,
+               R = int_ref lambda_m d_a phi_i d_b phi_j     (k a P1 field)
+* vector P2 elasticity (DG0 lambda, mu)
+               A[(i,a),(j,b)] = mu (delta_ab S_ij + D[b,a,i,j]) + lam D[a,b,i,j]
+               D[a,b,i,j] = int d_a phi_i d_b phi_j
+* P1 load with P1 f:   b = M f,  M_ij = |detJ| (1 + delta_ij) / 120
+* P2 load with DG0 f:  b_i = f_c |detJ| w_i, w = (-1/120 x4, 1/30 x6)
+* vector P2 load with DG0 body force f_c (3 comps): b_(i,a) = f_ca |detJ| w_i
+"""
+from __future__ import annotations
+
+from fractions import Fraction
+from functools import lru_cache
+from math import factorial
+
+import numpy as np
+
+# ---------------------------------------------------------------------------
+# Reference-element tables (exact rational arithmetic, then cast to float64)
+# ---------------------------------------------------------------------------
+
+#: basix edge numbering of the reference tetrahedron
+TET_EDGES = ((2, 3), (1, 3), (1, 2), (0, 3), (0, 2), (0, 1))
+
+
+def _mono_int(a, b, c):
+    """int over the reference tet of x^a y^b z^c = a! b! c! / (a+b+c+3)!"""
+    return Fraction(factorial(a) * factorial(b) * factorial(c), factorial(a + b + c + 3))
+
+
+def _pmul(p, q):
+    r = {}
+    for k1, v1 in p.items():
+        for k2, v2 in q.items():
+            k = (k1[0] + k2[0], k1[1] + k2[1], k1[2] + k2[2])
+            r[k] = r.get(k, 0) + v1 * v2
+    return {k: v for k, v in r.items() if v != 0}
+
+
+def _padd(p, q, s=1):
+    r = dict(p)
+    for k, v in q.items():
+        r[k] = r.get(k, 0) + s * v
+    return {k: v for k, v in r.items() if v != 0}
+
+
+def _pscale(p, s):
+    return {k: v * s for k, v in p.items()}
+
+
+def _pdiff(p, ax):
+    r = {}
+    for k, v in p.items():
+        if k[ax] > 0:
+            kk = list(k)
+            kk[ax] -= 1
+            r[tuple(kk)] = r.get(tuple(kk), 0) + v * k[ax]
+    return r
+
+
+def _pint(p):
+    return sum((v * _mono_int(*k) for k, v in p.items()), Fraction(0))
+
+
+_LAMBDA = [
+    {(0, 0, 0): Fraction(1), (1, 0, 0): Fraction(-1), (0, 1, 0): Fraction(-1), (0, 0, 1): Fraction(-1)},
+    {(1, 0, 0): Fraction(1)},
+    {(0, 1, 0): Fraction(1)},
+    {(0, 0, 1): Fraction(1)},
+]
+
+
+def _basis(degree):
+    if degree == 1:
+        return list(_LAMBDA)
+    if degree == 2:
+        vert = [_pmul(l, _padd(_pscale(l, 2), {(0, 0, 0): Fraction(1)}, -1)) for l in _LAMBDA]
+        edge = [_pscale(_pmul(_LAMBDA[a], _LAMBDA[b]), 4) for a, b in TET_EDGES]
+        return vert + edge
+    raise ValueError(degree)
+
+
+@lru_cache(maxsize=None)
+def ref_grad_tensor(degree: int, weighted: bool):
+    """R0[a,b,i,j] = int_ref d_a phi_i d_b phi_j   (weighted=False), shape (3,3,k,k)
+    R[m,a,b,i,j] = int_ref lambda_m d_a phi_i d_b phi_j (weighted=True), (4,3,3,k,k)."""
+    phi = _basis(degree)
+    k = len(phi)
+    dphi = [[_pdiff(p, ax) for ax in range(3)] for p in phi]
+    if not weighted:
+        out = np.zeros((3, 3, k, k))
+        for a in range(3):
+            for b in range(3):
+                for i in range(k):
+                    for j in range(k):
+                        out[a, b, i, j] = float(_pint(_pmul(dphi[i][a], dphi[j][b])))
+        return out
+    out = np.zeros((4, 3, 3, k, k))
+    for m in range(4):
+        for a in range(3):
+            for b in range(3):
+                for i in range(k):
+                    for j in range(k):
+                        out[m, a, b, i, j] = float(_pint(_pmul(_LAMBDA[m], _pmul(dphi[i][a], dphi[j][b]))))
+    return out
+
+
+@lru_cache(maxsize=None)
+def ref_basis_integrals(degree: int):
+    """w_i = int_ref phi_i  (reference volume 1/6)."""
+    return np.array([float(_pint(p)) for p in _basis(degree)])
+
+
+# ---------------------------------------------------------------------------
+# Mesh and dofmaps
+# ---------------------------------------------------------------------------
+
+def unit_cube_tet_mesh(n: int, jitter: float = 0.0, seed: int = 0):
+    """Unit cube split into n^3 hexes x 6 tetrahedra sharing the v0-v7 diagonal.
+
+    Vertex (ix, iy, iz) has index iz*(n+1)^2 + iy*(n+1) + ix.  With ``jitter``
+    > 0 every vertex moves by U[-jitter*h, jitter*h] per coordinate, except in
+    the directions normal to the boundary planes it lies on (the domain stays
+    the unit cube).  Returns (coords float64 [V,3], cells int32 [6 n^3, 4]).
+    """
+    n1 = n + 1
+    g = np.arange(n1, dtype=np.float64) / n
+    z, y, x = np.meshgrid(g, g, g, indexing="ij")
+    coords = np.stack([x.ravel(), y.ravel(), z.ravel()], axis=1)
+    if jitter > 0:
+        rng = np.random.default_rng(seed)
+        d = rng.uniform(-jitter / n, jitter / n, size=coords.shape)
+        idx = np.stack(np.meshgrid(np.arange(n1), np.arange(n1), np.arange(n1), indexing="ij"), -1).reshape(-1, 3)[:, ::-1]
+        on_bnd = (idx == 0) | (idx == n)
+        d[on_bnd] = 0.0
+        coords = coords + d
+    iz, iy, ix = np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij")
+    v0 = (iz * n1 * n1 + iy * n1 + ix).ravel()
+    v1 = v0 + 1
+    v2 = v0 + n1
+    v3 = v1 + n1
+    v4 = v0 + n1 * n1
+    v5 = v1 + n1 * n1
+    v6 = v2 + n1 * n1
+    v7 = v3 + n1 * n1
+    tets = [(v0, v1, v3, v7), (v0, v1, v7, v5), (v0, v5, v7, v4),
+            (v0, v3, v2, v7), (v0, v6, v4, v7), (v0, v2, v6, v7)]
+    cells = np.stack([np.stack(t, axis=1) for t in tets], axis=1).reshape(-1, 4)
+    return coords, cells.astype(np.int32)
+
+
+def vertex_grid_index(n: int):
+    """(ix, iy, iz) integer grid index of every vertex (int64 [V,3])."""
+    n1 = n + 1
+    v = np.arange(n1 ** 3)
+    return np.stack([v % n1, (v // n1) % n1, v // (n1 * n1)], axis=1)
+
+
+def p2_dofmap(n: int, cells: np.ndarray):
+    """P2 dofmap on the unit-cube mesh.
+
+    Each dof sits on a point of the doubled grid (vertex 2*idx, edge midpoint
+    idx_a + idx_b); dofs are numbered by lexicographic (z, y, x) order of those
+    points, which interleaves vertex and edge dofs spatially.  Local order per
+    cell: 4 vertices, then edges in basix order.  Returns (dofs int32 [C,10],
+    num_dofs, doubled-grid index int64 [num_dofs,3]).
+    """
+    vg = vertex_grid_index(n)
+    m = 2 * n + 1
+    pts = [2 * vg[cells[:, v]] for v in range(4)]
+    pts += [vg[cells[:, a]] + vg[cells[:, b]] for a, b in TET_EDGES]
+    P = np.stack(pts, axis=1)  # [C,10,3]
+    key = (P[..., 2] * m + P[..., 1]) * m + P[..., 0]
+    uniq, inv = np.unique(key.ravel(), return_inverse=True)
+    dofs = inv.reshape(key.shape).astype(np.int32)
+    grid = np.stack([uniq % m, (uniq // m) % m, uniq // (m * m)], axis=1)
+    return dofs, len(uniq), grid
+
+
+def boundary_dofs_from_grid(grid: np.ndarray, extent: int):
+    """Dofs lying on the boundary of the unit cube: a grid coordinate equals 0
+    or ``extent`` (exact topological marking for this structured mesh)."""
+    return np.nonzero(np.any((grid == 0) | (grid == extent), axis=1))[0].astype(np.int32)
+
+
+def dof_coordinates(coords, cells, dofs, num_dofs, degree):
+    """Physical coordinates of each dof (vertex or edge midpoint)."""
+    X = np.zeros((num_dofs, 3))
+    if degree == 1:
+        X[dofs.ravel()] = coords[cells.ravel()]
+        return X
+    cc = coords[cells]  # [C,4,3]
+    pts = [cc[:, v] for v in range(4)] + [0.5 * (cc[:, a] + cc[:, b]) for a, b in TET_EDGES]
+    P = np.stack(pts, axis=1)
+    X[dofs.ravel()] = P.reshape(-1, 3)
+    return X
+
+
+# ---------------------------------------------------------------------------
+# Sparsity (cpp/cudolfinx/la/petsc.cpp:38-65; DOLFINx SparsityPattern)
+# ---------------------------------------------------------------------------
+
+def block_sparsity(dofs0, dofs1, n0):
+    """Sorted unique block columns per block row: returns (bptr, bcol)."""
+    k0, k1 = dofs0.shape[1], dofs1.shape[1]
+    r = np.repeat(dofs0, k1, axis=1).astype(np.int64).ravel()
+    c = np.tile(dofs1, (1, k0)).astype(np.int64).ravel()
+    ncol = int(dofs1.max()) + 1 if dofs1.size else 1
+    key = np.unique(r * ncol + c)
+    rows = key // ncol
+    cols = (key % ncol).astype(np.int32)
+    bptr = np.zeros(n0 + 1, dtype=np.int64)
+    np.add.at(bptr, rows + 1, 1)
+    return np.cumsum(bptr), cols
+
+
+def sparsity(dofs0, dofs1, n0, bs0=1, bs1=1):
+    """Scalar (unrolled) CSR pattern: row bs0*R+a has columns bs1*C+b for C in
+    the sorted block columns of R and b in 0..bs1-1 (la/petsc.cpp:45-65)."""
+    bptr, bcol = block_sparsity(dofs0, dofs1, n0)
+    blen = np.diff(bptr)
+    row_len = np.repeat(blen * bs1, bs0)
+    row_ptr = np.zeros(n0 * bs0 + 1, dtype=np.int64)
+    row_ptr[1:] = np.cumsum(row_len)
+    # unrolled columns of each block row, repeated bs0 times
+    ucol = (bcol.astype(np.int64)[:, None] * bs1 + np.arange(bs1)[None, :]).ravel()
+    col = np.empty(row_ptr[-1], dtype=np.int32)
+    # each scalar row bs0*R+a copies ucol[bptr[R]*bs1 : bptr[R+1]*bs1]
+    seg_start = np.repeat(bptr[:-1] * bs1, bs0)  # start of source segment for each scalar row
+    seg_len = row_len
+    total = int(row_ptr[-1])
+    if total:
+        rid = np.repeat(np.arange(n0 * bs0), seg_len)
+        off = np.arange(total) - row_ptr[rid]
+        col[:] = ucol[seg_start[rid] + off]
+    return row_ptr.astype(np.int32), col
+
+
+def diag_positions(row_ptr, col):
+    """Slot of A[r, r] in CSR for every row (-1 if absent)."""
+    nrows = len(row_ptr) - 1
+    out = np.full(nrows, -1, dtype=np.int64)
+    rid = np.repeat(np.arange(nrows), np.diff(row_ptr))
+    hit = np.nonzero(col == rid)[0]
+    out[rid[hit]] = hit
+    return out
+
+
+def csr_slots(row_ptr, col, rows, cols):
+    """Slot index of (rows[i], cols[i]) via binary search in each CSR row
+    (the reference's ``binary_search``, CUDAFormIntegral.cpp:2572-2602)."""
+    rows = np.asarray(rows, dtype=np.int64)
+    cols = np.asarray(cols, dtype=np.int64)
+    rp = row_ptr.astype(np.int64)
+    # global key search: rows are sorted blocks, columns sorted inside a row
+    key_all = np.repeat(np.arange(len(rp) - 1, dtype=np.int64), np.diff(rp)) * (1 << 32) + col.astype(np.int64)
+    key = rows * (1 << 32) + cols
+    s = np.searchsorted(key_all, key)
+    ok = (s < len(key_all)) & (key_all[np.minimum(s, len(key_all) - 1)] == key)
+    if not np.all(ok):
+        raise KeyError("entry not in sparsity pattern")
+    return s
+
+
+# ---------------------------------------------------------------------------
+# Geometry
+# ---------------------------------------------------------------------------
+
+def cell_geometry(coords, cells):
+    """Per cell: J (C,3,3) with columns x_k - x_0, detJ (C,), K = J^{-1} (C,3,3)."""
+    x = coords[cells]  # [C,4,3]
+    J = np.stack([x[:, 1] - x[:, 0], x[:, 2] - x[:, 0], x[:, 3] - x[:, 0]], axis=2)
+    det = np.linalg.det(J)
+    K = np.linalg.inv(J)
+    return J, det, K
+
+
+# ---------------------------------------------------------------------------
+# Element tensors (first principles; FFCx tabulate_tensor in the reference)
+# ---------------------------------------------------------------------------
+
+_P1_REF_GRAD = np.array([[-1.0, -1.0, -1.0], [1.0, 0.0, 0.0], [0.0, 1.0, 0.0], [0.0, 0.0, 1.0]])
+
+
+def p1_stiffness(coords, cells, k_dg0=None):
+    """Ae [C,4,4] of k * inner(grad u, grad v) * dx with P1, k DG0 (or 1)."""
+    _, det, K = cell_geometry(coords, cells)
+    G = np.einsum("ia,cab->cib", _P1_REF_GRAD, K)  # grad phi_i = K^T ghat_i  -> (ghat K)_b
+    Ae = np.abs(det)[:, None, None] / 6.0 * np.einsum("cib,cjb->cij", G, G)
+    if k_dg0 is not None:
+        Ae = Ae * np.asarray(k_dg0)[:, None, None]
+    return Ae
+
+
+def p2_stiffness(coords, cells, k_cell_values):
+    """Ae [C,10,10] of k * inner(grad u, grad v) * dx with P2, k a P1 field
+    given by its 4 vertex values per cell ``k_cell_values`` [C,4]."""
+    _, det, K = cell_geometry(coords, cells)
+    G = np.abs(det)[:, None, None] * np.einsum("cak,cbk->cab", K, K)
+    R = ref_grad_tensor(2, True)  # [4,3,3,10,10]
+    return np.einsum("cm,cab,mabij->cij", k_cell_values, G, R, optimize=True)
+
+
+def p2_elasticity(coords, cells, lam, mu):
+    """Ae [C,30,30] (local index 3*i + a) of 2 mu eps(u):eps(v) + lam div u div v,
+    vector P2, DG0 lam and mu."""
+    _, det, K = cell_geometry(coords, cells)
+    R0 = ref_grad_tensor(2, False)  # [3,3,10,10]
+    # D[a,b,i,j] = |det| sum_{al,be} K[al,a] K[be,b] R0[al,be,i,j]
+    D = np.abs(det)[:, None, None, None, None] * np.einsum("cpa,cqb,pqij->cabij", K, K, R0, optimize=True)
+    S = np.einsum("caaij->cij", D)
+    C = len(cells)
+    A = np.zeros((C, 10, 3, 10, 3))
+    eye = np.eye(3)
+    # mu (delta_ab S_ij + D[b,a,i,j]) + lam D[a,b,i,j]
+    A += mu[:, None, None, None, None] * (eye[None, None, :, None, :] * S[:, :, None, :, None])
+    A += mu[:, None, None, None, None] * np.transpose(D, (0, 3, 2, 4, 1))   # D[b,a,i,j] at [i,a,j,b]
+    A += lam[:, None, None, None, None] * np.transpose(D, (0, 3, 1, 4, 2))  # D[a,b,i,j] at [i,a,j,b]
+    return A.reshape(C, 30, 30)
+
+
+def p1_load_p1f(coords, cells, f_vertex):
+    """be [C,4] of f*v*dx with f a P1 field (vertex values), P1 test space."""
+    _, det, _ = cell_geometry(coords, cells)
+    fc = f_vertex[cells]
+    return np.abs(det)[:, None] / 120.0 * (fc + fc.sum(axis=1, keepdims=True))
+
+
+def p2_load_dg0(coords, cells, f_cell):
+    """be [C,10] of f*v*dx with f DG0, P2 test space."""
+    _, det, _ = cell_geometry(coords, cells)
+    w = ref_basis_integrals(2)
+    return (np.abs(det) * f_cell)[:, None] * w[None, :]
+
+
+def p2_vector_load_dg0(coords, cells, f_cell3):
+    """be [C,30] (index 3*i + a) of inner(f, v)*dx, f DG0 vector [C,3]."""
+    _, det, _ = cell_geometry(coords, cells)
+    w = ref_basis_integrals(2)
+    be = np.abs(det)[:, None, None] * w[None, :, None] * f_cell3[:, None, :]
+    return be.reshape(len(cells), 30)
+
+
+# ---------------------------------------------------------------------------
+# Global assembly
+# ---------------------------------------------------------------------------
+
+def unroll(dofs, bs):
+    """dof*bs + comp (CUDADofMap.cpp:227)."""
+    if bs == 1:
+        return dofs.astype(np.int64)
+    return (dofs.astype(np.int64)[:, :, None] * bs + np.arange(bs)).reshape(len(dofs), -1)
+
+
+def assemble_matrix(Ae, dofs0, dofs1, row_ptr, col, bs0=1, bs1=1,
+                    bc0_markers=None, bc1_markers=None, diagonal=1.0, bc0_owned_dofs=None):
+    """CSR values: sum_e Ae scattered with BC rows/cols skipped
+    (CUDAFormIntegral.cpp:1195-1213), then A[d,d] = diagonal for BC rows
+    (CUDAAssembler.cpp:131-164)."""
+    u0 = unroll(dofs0, bs0)
+    u1 = unroll(dofs1, bs1)
+    C, k0 = u0.shape
+    k1 = u1.shape[1]
+    rows = np.repeat(u0, k1, axis=1).ravel()
+    cols = np.tile(u1, (1, k0)).ravel()
+    vals = Ae.reshape(C, k0 * k1).ravel()
+    keep = np.ones(rows.shape, dtype=bool)
+    if bc0_markers is not None:
+        keep &= bc0_markers[rows] == 0
+    if bc1_markers is not None:
+        keep &= bc1_markers[cols] == 0
+    slots = csr_slots(row_ptr, col, rows[keep], cols[keep])
+    values = np.zeros(len(col))
+    np.add.at(values, slots, vals[keep])
+    if bc0_owned_dofs is not None and len(bc0_owned_dofs):
+        dpos = diag_positions(row_ptr, col)
+        d = dpos[np.asarray(bc0_owned_dofs)]
+        values[d[d >= 0]] = diagonal
+    return values
+
+
+def assemble_vector(be, dofs, num_values, bs=1):
+    """b += be scattered (CUDAFormIntegral.cpp:345-354)."""
+    u = unroll(dofs, bs)
+    b = np.zeros(num_values)
+    np.add.at(b, u.ravel(), be.reshape(-1))
+    return b
+
+
+def apply_lifting(b, Ae, dofs0, dofs1, bc1_markers, g, x0=None, scale=1.0, bs0=1, bs1=1):
+    """b -= scale * A (g - x0) restricted to BC columns, for every cell with a
+    BC column (CUDAFormIntegral.cpp:647-715)."""
+    u0 = unroll(dofs0, bs0)
+    u1 = unroll(dofs1, bs1)
+    m = bc1_markers[u1] != 0
+    has = np.nonzero(m.any(axis=1))[0]
+    if len(has) == 0:
+        return b
+    u0h, u1h, mh = u0[has], u1[has], m[has]
+    d = g[u1h] - (x0[u1h] if x0 is not None else 0.0)
+    d = np.where(mh, d, 0.0)
+    be = -scale * np.einsum("cij,cj->ci", Ae[has], d)
+    np.add.at(b, u0h.ravel(), be.ravel())
+    return b
+
+
+def set_bc(b, bc_dofs, g, x0=None, scale=1.0):
+    """b[d] = scale * (g[d] - x0[d]) (CUDAAssembler.cpp:115-124)."""
+    d = np.asarray(bc_dofs)
+    b[d] = scale * (g[d] - (x0[d] if x0 is not None else 0.0))
+    return b
+
+
+# ---------------------------------------------------------------------------
+# Jacobi-preconditioned CG (the reference hands A, b to PETSc KSP cg+jacobi:
+# python/examples/poisson.py:116-125)
+# ---------------------------------------------------------------------------
+
+def pcg_jacobi(row_ptr, col, values, b, rtol=1e-8, max_iter=10000):
+    import scipy.sparse as sp
+    n = len(row_ptr) - 1
+    A = sp.csr_matrix((values, col, row_ptr), shape=(n, n))
+    dinv = 1.0 / A.diagonal()
+    x = np.zeros(n)
+    r = b - A @ x
+    z = dinv * r
+    p = z.copy()
+    rz = r @ z
+    b_norm = np.linalg.norm(b)
+    it = 0
+    while it < max_iter:
+        if np.linalg.norm(r) <= rtol * b_norm:
+            break
+        Ap = A @ p
+        alpha = rz / (p @ Ap)
+        x += alpha * p
+        r -= alpha * Ap
+        z = dinv * r
+        rz_new = r @ z
+        p = z + (rz_new / rz) * p
+        rz = rz_new
+        it += 1
+    return x, it
+
+
+# ---------------------------------------------------------------------------
+# Problem builders for the benchmark configurations
+# ---------------------------------------------------------------------------
+
+def build_problem(kind: str, n: int, seed: int = 0):
+    """Synthetic problem instances (seeded numpy inputs).
+
+    kind: 'p1'   -- P1 Poisson, k=1, f = P1 interpolant of sin(pi x)sin(pi y)sin(pi z),
+                    homogeneous Dirichlet on the whole boundary.
+          'p2'   -- P2 Poisson, k = exp(N(0,1)) per vertex (P1 field), f ~ U[-1,1]
+                    per cell (DG0), g = x + y + z on the boundary.
+          'vp2'  -- vector P2 elasticity, lam ~ U[0.5,2], mu ~ U[0.2,1] per cell,
+                    vertices jittered +-0.2h, body force (0,0,-1), u = 0 on the boundary.
+          'p1k'  -- P1 Poisson with DG0 k log-uniform in [1e-2,1e2] per cell.
+    """
+    rng = np.random.default_rng(seed)
+    P = {"kind": kind, "n": n}
+    if kind == "vp2":
+        coords, cells = unit_cube_tet_mesh(n, jitter=0.2, seed=seed)
+    else:
+        coords, cells = unit_cube_tet_mesh(n)
+    P["coords"], P["cells"] = coords, cells
+    C = len(cells)
+    if kind in ("p1", "p1k"):
+        dofs = cells.copy()
+        ndof = len(coords)
+        grid = vertex_grid_index(n)
+        bnd = boundary_dofs_from_grid(grid, n)
+        X = coords
+        P.update(dofs=dofs, ndof=ndof, bs=1, degree=1, bc_dofs=bnd)
+        if kind == "p1":
+            f = np.sin(np.pi * X[:, 0]) * np.sin(np.pi * X[:, 1]) * np.sin(np.pi * X[:, 2])
+            P.update(k=None, f=f, g=np.zeros(ndof))
+        else:
+            k = np.exp(rng.uniform(np.log(1e-2), np.log(1e2), size=C))
+            f = np.ones(ndof)
+            P.update(k=k, f=f, g=np.zeros(ndof))
+    elif kind == "p2":
+        dofs, ndof, grid = p2_dofmap(n, cells)
+        X = dof_coordinates(coords, cells, dofs, ndof, 2)
+        bnd = boundary_dofs_from_grid(grid, 2 * n)
+        kv = np.exp(rng.standard_normal(len(coords)))
+        f = rng.uniform(-1.0, 1.0, size=C)
+        g = X.sum(axis=1)
+        P.update(dofs=dofs, ndof=ndof, bs=1, degree=2, bc_dofs=bnd, k=kv, f=f, g=g)
+    elif kind == "vp2":
+        dofs, ndof, grid = p2_dofmap(n, cells)
+        bnd_nodes = boundary_dofs_from_grid(grid, 2 * n)
+        bnd = (bnd_nodes[:, None] * 3 + np.arange(3)).ravel().astype(np.int32)
+        lam = rng.uniform(0.5, 2.0, size=C)
+        mu = rng.uniform(0.2, 1.0, size=C)
+        f3 = np.tile(np.array([0.0, 0.0, -1.0]), (C, 1))
+        P.update(dofs=dofs, ndof=ndof, bs=3, degree=2, bc_dofs=bnd, lam=lam, mu=mu, f=f3,
+                 g=np.zeros(3 * ndof))
+    else:
+        raise ValueError(kind)
+    return P
+
+
+def element_matrices(P):
+    kind = P["kind"]
+    if kind in ("p1", "p1k"):
+        return p1_stiffness(P["coords"], P["cells"], P["k"])
+    if kind == "p2":
+        return p2_stiffness(P["coords"], P["cells"], P["k"][P["cells"]])
+    if kind == "vp2":
+        return p2_elasticity(P["coords"], P["cells"], P["lam"], P["mu"])
+    raise ValueError(kind)
+
+
+def element_vectors(P):
+    kind = P["kind"]
+    if kind in ("p1", "p1k"):
+        return p1_load_p1f(P["coords"], P["cells"], P["f"])
+    if kind == "p2":
+        return p2_load_dg0(P["coords"], P["cells"], P["f"])
+    if kind == "vp2":
+        return p2_vector_load_dg0(P["coords"], P["cells"], P["f"])
+    raise ValueError(kind)
+
+
+def solve_system(P):
+    """Full oracle pipeline: A with BCs, b = assemble + lifting + set_bc.
+    Returns dict(row_ptr, col, A, b)."""
+    bs = P["bs"]
+    dofs = P["dofs"]
+    nscal = P["ndof"] * bs
+    row_ptr, col = sparsity(dofs, dofs, P["ndof"], bs, bs)
+    markers = np.zeros(nscal, dtype=np.uint8)
+    markers[P["bc_dofs"]] = 1
+    Ae = element_matrices(P)
+    A = assemble_matrix(Ae, dofs, dofs, row_ptr, col, bs, bs, markers, markers, 1.0, P["bc_dofs"])
+    be = element_vectors(P)
+    b = assemble_vector(be, dofs, nscal, bs)
+    b = apply_lifting(b, Ae, dofs, dofs, markers, P["g"], None, 1.0, bs, bs)
+    b = set_bc(b, P["bc_dofs"], P["g"])
+    return {"row_ptr": row_ptr, "col": col, "A": A, "b": b, "markers": markers}
+
+
+def nnz_formula(kind: str, n: int) -> int:
+    """Closed-form nnz for the unit-cube meshes."""
+    V = (n + 1) ** 3
+    E = 3 * n * (n + 1) ** 2 + 3 * n * n * (n + 1) + n ** 3
+    if kind in ("p1", "p1k"):
+        return V + 2 * E
+    p2 = 230 * n ** 3 + 138 * n ** 2 + 24 * n + 1
+    return p2 if kind == "p2" else 9 * p2

@@ -1,0 +1,81 @@
+"""Helpers shared by the GPU tests: build a problem through the cudolfinx
+mirror API (C-ABI underneath) from the oracle's inputs, and compare."""
+import numpy as np
+
+from conftest import ensure_library
+
+
+def tolerance_check(gpu, ref, rtol=1e-12, floor=1e-13):
+    """Entrywise |gpu - ref| <= rtol*|ref| + floor*max|ref|.
+
+    FP64 atomics add contributions in a different order than the oracle; an
+    entry whose contributions cancel ends at rounding level, so a floor
+    relative to the largest entry is part of the bound."""
+    gpu = np.asarray(gpu)
+    ref = np.asarray(ref)
+    scale = max(np.abs(ref).max() if ref.size else 0.0, 1e-300)
+    err = np.abs(gpu - ref)
+    bound = rtol * np.abs(ref) + floor * scale
+    worst = np.max(err / np.maximum(np.abs(ref), floor * scale / rtol)) if ref.size else 0.0
+    return bool(np.all(err <= bound)), float(worst)
+
+
+def mirror_problem(P, precision="fp64"):
+    """Mesh/spaces/forms/BC through the mirror API for an oracle problem P."""
+    ensure_library()
+    import cudolfinx as cx
+    from cudolfinx import fem
+
+    mesh = fem.Mesh(P["coords"], P["cells"], grid_n=P["n"])
+    kind = P["kind"]
+    out = {"mesh": mesh}
+    if kind in ("p1", "p1k"):
+        V = fem.functionspace(mesh, ("P", 1))
+        assert np.array_equal(V.dofs, P["dofs"])
+        if kind == "p1":
+            k = 1.0
+        else:
+            W = fem.functionspace(mesh, ("DG", 0))
+            k = fem.Function(W, P["k"])
+        fP1 = fem.Function(V, P["f"])
+        a = fem.stiffness(V, k)
+        L = fem.load(V, fP1)
+    elif kind == "p2":
+        V = fem.functionspace(mesh, ("P", 2))
+        assert np.array_equal(V.dofs, P["dofs"])
+        V1 = fem.functionspace(mesh, ("P", 1))
+        W = fem.functionspace(mesh, ("DG", 0))
+        a = fem.stiffness(V, fem.Function(V1, P["k"]), precision=precision)
+        L = fem.load(V, fem.Function(W, P["f"]))
+    elif kind == "vp2":
+        V = fem.functionspace(mesh, ("P", 2, (3,)))
+        W = fem.functionspace(mesh, ("DG", 0))
+        a = fem.elasticity(V, fem.Function(W, P["lam"]), fem.Function(W, P["mu"]), precision=precision)
+        W3 = fem.functionspace(mesh, ("DG", 0, (3,)))
+        L = fem.load(V, fem.Function(W3, np.asarray(P["f"]).reshape(-1)))
+    else:
+        raise ValueError(kind)
+    g = fem.Function(V, P["g"])
+    bc = fem.dirichletbc(g, P["bc_dofs"])
+    out.update(V=V, a=a, L=L, bc=bc)
+    out["cx"] = cx
+    return out
+
+
+def run_system(P, deterministic=False, precision="fp64"):
+    """A (host CSR arrays) and b through the mirror API: assemble_matrix with
+    BCs, assemble_vector + apply_lifting + set_bc."""
+    M = mirror_problem(P, precision)
+    cx = M["cx"]
+    asm = cx.CUDAAssembler()
+    a = cx.form(M["a"])
+    L = cx.form(M["L"])
+    bcs = asm.pack_bcs([M["bc"]])
+    A = asm.assemble_matrix(a, bcs=bcs, deterministic=deterministic)
+    A.assemble()
+    b = asm.assemble_vector(L)
+    asm.apply_lifting(b, [a], [bcs])
+    asm.set_bc(b, bcs, M["V"])
+    rp, col = A.sparsity.to_host()
+    return {"row_ptr": rp, "col": col, "A": A.values.cpu().numpy(), "b": b.to_host(), "asm": asm, "Aobj": A,
+            "bobj": b, "forms": (a, L), "bcs": bcs, "M": M}

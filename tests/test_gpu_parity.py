@@ -1,0 +1,211 @@
+"""GPU parity: the CUDA path (through the C-ABI) against the CPU oracle.
+
+Bar: identical CSR pattern (bit-exact), CSR values and right-hand sides
+within 1e-12 relative in FP64 (entrywise, with a 1e-13*max|A| floor for
+entries that cancel to rounding level); the deterministic variant is also
+bitwise reproducible from run to run.
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from gpu_util import mirror_problem, run_system, tolerance_check
+from oracle import fem_oracle as fo
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+CASES = [("p1", 2), ("p1", 7), ("p1", 16), ("p1k", 6), ("p2", 2), ("p2", 5), ("p2", 9), ("vp2", 2), ("vp2", 4)]
+
+
+def _problem_from_golden(path):
+    G = np.load(path)
+    kind = os.path.basename(path).split("_n")[0]
+    P = {"kind": kind, "n": int(G["n"]), "coords": G["coords"], "cells": G["cells"], "dofs": G["dofs"],
+         "bc_dofs": G["bc_dofs"], "g": G["g"], "ndof": int(G["ndof"]), "bs": int(G["bs"])}
+    for k in ("k", "f", "lam", "mu"):
+        P[k] = G[k] if k in G.files else None
+    return P, G
+
+
+@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLDEN, "*.npz"))))
+@pytest.mark.parametrize("deterministic", [False, True])
+def test_golden_fixtures(path, deterministic):
+    P, G = _problem_from_golden(path)
+    R = run_system(P, deterministic=deterministic)
+    assert np.array_equal(R["row_ptr"], G["row_ptr"]) and np.array_equal(R["col"], G["col"])
+    ok, worst = tolerance_check(R["A"], G["A"])
+    assert ok, worst
+    ok, worst = tolerance_check(R["b"], G["b"])
+    assert ok, worst
+
+
+@pytest.mark.parametrize("kind,n", CASES)
+@pytest.mark.parametrize("deterministic", [False, True])
+def test_system_parity(kind, n, deterministic):
+    P = fo.build_problem(kind, n, seed=n)
+    S = fo.solve_system(P)
+    R = run_system(P, deterministic=deterministic)
+    assert np.array_equal(R["row_ptr"], S["row_ptr"]) and np.array_equal(R["col"], S["col"])
+    ok, worst = tolerance_check(R["A"], S["A"])
+    assert ok, f"A worst rel err {worst}"
+    ok, worst = tolerance_check(R["b"], S["b"])
+    assert ok, f"b worst rel err {worst}"
+
+
+@pytest.mark.parametrize("kind,n", [("p1", 8), ("p2", 5), ("vp2", 3)])
+def test_deterministic_is_bitwise_reproducible(kind, n):
+    P = fo.build_problem(kind, n, seed=3)
+    R1 = run_system(P, deterministic=True)
+    asm, A, (a, _), bcs = R1["asm"], R1["Aobj"], R1["forms"], R1["bcs"]
+    first = A.values.clone()
+    for _ in range(3):
+        asm.assemble_matrix(a, A, bcs=bcs, deterministic=True)
+        A.assemble()
+        assert bool((A.values == first).all())
+
+
+def test_matrix_without_bcs_and_zero_false_accumulates():
+    P = fo.build_problem("p2", 4, seed=1)
+    M = mirror_problem(P)
+    cx = M["cx"]
+    asm = cx.CUDAAssembler()
+    a = cx.form(M["a"])
+    A = asm.assemble_matrix(a)
+    A.assemble()
+    Ae = fo.element_matrices(P)
+    rp, col = fo.sparsity(P["dofs"], P["dofs"], P["ndof"])
+    ref = fo.assemble_matrix(Ae, P["dofs"], P["dofs"], rp, col)
+    ok, worst = tolerance_check(A.values.cpu().numpy(), ref)
+    assert ok, worst
+    for det in (False, True):
+        asm.assemble_matrix(a, A, zero=False, deterministic=det)
+        A.assemble()
+    ok, worst = tolerance_check(A.values.cpu().numpy(), 3 * ref)
+    assert ok, worst
+
+
+def test_reassembly_after_coefficient_update():
+    # the reference's test_reassembly: change a coefficient on the host, re-assemble
+    P = fo.build_problem("p2", 4, seed=2)
+    M = mirror_problem(P)
+    cx = M["cx"]
+    asm = cx.CUDAAssembler()
+    L = cx.form(M["L"])
+    fL = M["L"].coefficients[0]
+    b = asm.assemble_vector(L)
+    for d in (2.0, 3.0):
+        fL.x.array[:] = P["f"] * d
+        asm.assemble_vector(L, b)
+        ref = fo.assemble_vector(fo.p2_load_dg0(P["coords"], P["cells"], P["f"] * d), P["dofs"], P["ndof"])
+        ok, worst = tolerance_check(b.to_host(), ref)
+        assert ok, worst
+
+
+def test_lifting_with_x0_and_scale():
+    P = fo.build_problem("p2", 4, seed=4)
+    M = mirror_problem(P)
+    cx = M["cx"]
+    asm = cx.CUDAAssembler()
+    a, L = cx.form(M["a"]), cx.form(M["L"])
+    bcs = asm.pack_bcs([M["bc"]])
+    rng = np.random.default_rng(0)
+    x0h = rng.standard_normal(P["ndof"])
+    x0 = asm.create_vector(L)
+    import torch
+    x0.vector.copy_(torch.from_numpy(x0h))
+    b = asm.assemble_vector(L)
+    asm.apply_lifting(b, [a], [bcs], x0=[x0], scale=-0.7)
+    asm.set_bc(b, bcs, M["V"], x0=x0, scale=-0.7)
+    markers = np.zeros(P["ndof"], np.uint8)
+    markers[P["bc_dofs"]] = 1
+    ref = fo.assemble_vector(fo.element_vectors(P), P["dofs"], P["ndof"])
+    ref = fo.apply_lifting(ref, fo.element_matrices(P), P["dofs"], P["dofs"], markers, P["g"], x0h, -0.7)
+    ref = fo.set_bc(ref, P["bc_dofs"], P["g"], x0h, -0.7)
+    ok, worst = tolerance_check(b.to_host(), ref)
+    assert ok, worst
+
+
+def test_bc_update_changes_values_not_pattern():
+    P = fo.build_problem("p2", 3, seed=5)
+    M = mirror_problem(P)
+    cx = M["cx"]
+    asm = cx.CUDAAssembler()
+    L = cx.form(M["L"])
+    bcs = asm.pack_bcs([M["bc"]])
+    b = asm.assemble_vector(L)
+    M["bc"].value.x.array[:] *= 2.0
+    bcs.update()
+    asm.set_bc(b, bcs, M["V"])
+    out = b.to_host()
+    assert np.allclose(out[P["bc_dofs"]], 2.0 * P["g"][P["bc_dofs"]], rtol=1e-15, atol=0)
+
+
+def test_fp32_element_tensors_precision_path():
+    # FP32 contraction, FP64 accumulation: relative Frobenius error at FP32 level
+    for kind, n in (("p2", 6), ("vp2", 3)):
+        P = fo.build_problem(kind, n, seed=6)
+        S = fo.solve_system(P)
+        R = run_system(P, precision="fp32")
+        rel = np.linalg.norm(R["A"] - S["A"]) / np.linalg.norm(S["A"])
+        assert rel < 2e-6, (kind, rel)
+        assert rel > 0.0
+
+
+def test_pcg_solution_matches_direct_solve():
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spla
+
+    for kind, n in (("p1", 8), ("p2", 5), ("vp2", 3)):
+        P = fo.build_problem(kind, n, seed=7)
+        R = run_system(P)
+        N = len(R["row_ptr"]) - 1
+        A = sp.csr_matrix((R["A"], R["col"], R["row_ptr"]), shape=(N, N))
+        x_ref = spla.spsolve(A.tocsc(), R["b"])
+        x, it, res = R["asm"].solve(R["Aobj"], R["bobj"], rtol=1e-10)
+        xh = x.to_host()
+        assert res <= 1e-10 and it > 0
+        assert np.linalg.norm(xh - x_ref) <= 1e-7 * np.linalg.norm(x_ref)
+
+
+def test_pcg_reports_non_convergence():
+    P = fo.build_problem("p2", 5, seed=8)
+    R = run_system(P)
+    x, it, res = R["asm"].solve(R["Aobj"], R["bobj"], rtol=1e-12, max_iter=3, raise_on_failure=False)
+    assert it == 3 and res > 1e-12
+    with pytest.raises(RuntimeError, match="PCG stopped"):
+        R["asm"].solve(R["Aobj"], R["bobj"], rtol=1e-12, max_iter=3)
+
+
+def test_missing_coupling_is_reported_not_faulted():
+    # a pattern without the off-diagonal couplings: binding reports FE_ERR_PATTERN
+    P = fo.build_problem("p1", 2, seed=0)
+    M = mirror_problem(P)
+    cx = M["cx"]
+    a = cx.form(M["a"])
+    n = P["ndof"]
+    rp = np.arange(n + 1, dtype=np.int32)
+    col = np.arange(n, dtype=np.int32)
+    ctx = cx.get_cuda_context()
+    sp_diag = cx.Sparsity.from_csr(ctx, rp, col, n)
+    with pytest.raises(RuntimeError, match="coupling missing"):
+        a._bind(sp_diag)
+    # the context stays usable afterwards
+    asm = cx.CUDAAssembler()
+    A = asm.assemble_matrix(cx.form(M["a"]))
+    A.assemble()
+
+
+def test_empty_bc_and_empty_mesh():
+    import cudolfinx as cx
+    from cudolfinx import fem
+
+    m = fem.Mesh(np.zeros((0, 3)), np.zeros((0, 4), np.int32))
+    V = fem.functionspace(m, ("P", 1))
+    asm = cx.CUDAAssembler()
+    a = cx.form(fem.stiffness(V))
+    A = asm.assemble_matrix(a, bcs=[])
+    A.assemble()
+    assert A.sparsity.nnz == 0

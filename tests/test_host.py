@@ -1,0 +1,123 @@
+"""CPU tests of the product's host side: the C-ABI library loads and exports
+every declared entry point, the host pattern builder is bit-exact with the
+oracle (DOLFINx SparsityPattern + la/petsc.cpp:45-65 unroll), and the
+cudolfinx.fem stand-ins generate the oracle's meshes and dofmaps."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, ensure_library
+from oracle import fem_oracle as fo
+
+HEADER = os.path.join(ROOT, "include", "cudolfinx_b200.h")
+
+
+def declared_symbols():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(fe_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    path = ensure_library()
+    lib = ctypes.CDLL(path)
+    syms = declared_symbols()
+    assert len(syms) >= 25
+    missing = [s for s in syms if not hasattr(lib, s)]
+    assert not missing, missing
+
+
+def test_python_binding_declares_every_symbol():
+    ensure_library()
+    from cudolfinx import _lib
+
+    assert set(declared_symbols()) == set(_lib.EXPORTED)
+
+
+def _host_pattern(d0, d1, bs, nb):
+    from cudolfinx import _lib
+
+    nnz = ctypes.c_int64()
+    rp, cl = ctypes.c_void_p(), ctypes.c_void_p()
+    d0 = np.ascontiguousarray(d0, dtype=np.int32)
+    d1 = np.ascontiguousarray(d1, dtype=np.int32)
+    st = _lib.lib.fe_pattern_build_host(d0.ctypes.data, d1.ctypes.data, d0.shape[0], d0.shape[1], d1.shape[1], bs, bs,
+                                        nb, nb, ctypes.byref(nnz), ctypes.byref(rp), ctypes.byref(cl))
+    if st != 0:
+        return st, _lib.last_error(), None
+    nrows = nb * bs
+    row_ptr = np.ctypeslib.as_array((ctypes.c_int32 * (nrows + 1)).from_address(rp.value)).copy()
+    col = np.ctypeslib.as_array((ctypes.c_int32 * max(1, nnz.value)).from_address(cl.value))[: nnz.value].copy()
+    _lib.lib.fe_free_host(rp)
+    _lib.lib.fe_free_host(cl)
+    return st, row_ptr, col
+
+
+@pytest.mark.parametrize("kind,n", [("p1", 1), ("p1", 4), ("p2", 1), ("p2", 3), ("vp2", 2)])
+def test_host_pattern_bit_exact_with_oracle(kind, n):
+    ensure_library()
+    P = fo.build_problem(kind, n)
+    st, rp, col = _host_pattern(P["dofs"], P["dofs"], P["bs"], P["ndof"])
+    assert st == 0, rp
+    ref_rp, ref_col = fo.sparsity(P["dofs"], P["dofs"], P["ndof"], P["bs"], P["bs"])
+    assert np.array_equal(rp, ref_rp)
+    assert np.array_equal(col, ref_col)
+
+
+def test_host_pattern_rectangular_and_ragged():
+    # rows from a P1 map, columns from a P2 map on the same cells (rectangular, uneven rows)
+    ensure_library()
+    P1 = fo.build_problem("p1", 2)
+    dofs2, nd2, _ = fo.p2_dofmap(2, P1["cells"])
+    from cudolfinx import _lib
+
+    nnz = ctypes.c_int64()
+    rp, cl = ctypes.c_void_p(), ctypes.c_void_p()
+    d0 = np.ascontiguousarray(P1["dofs"], dtype=np.int32)
+    d1 = np.ascontiguousarray(dofs2, dtype=np.int32)
+    st = _lib.lib.fe_pattern_build_host(d0.ctypes.data, d1.ctypes.data, len(d0), 4, 10, 1, 1, P1["ndof"], nd2,
+                                        ctypes.byref(nnz), ctypes.byref(rp), ctypes.byref(cl))
+    assert st == 0
+    n0 = P1["ndof"]
+    row_ptr = np.ctypeslib.as_array((ctypes.c_int32 * (n0 + 1)).from_address(rp.value)).copy()
+    col = np.ctypeslib.as_array((ctypes.c_int32 * nnz.value).from_address(cl.value)).copy()
+    _lib.lib.fe_free_host(rp)
+    _lib.lib.fe_free_host(cl)
+    ref_rp, ref_col = fo.sparsity(P1["dofs"], dofs2, n0)
+    assert np.array_equal(row_ptr, ref_rp) and np.array_equal(col, ref_col)
+
+
+def test_host_pattern_empty_mesh():
+    ensure_library()
+    st, rp, col = _host_pattern(np.zeros((0, 4), np.int32), np.zeros((0, 4), np.int32), 1, 5)
+    assert st == 0 and np.array_equal(rp, np.zeros(6, np.int32)) and len(col) == 0
+
+
+def test_host_pattern_rejects_out_of_range_dofs():
+    ensure_library()
+    d = np.array([[0, 1, 2, 7]], dtype=np.int32)
+    st, msg, _ = _host_pattern(d, d, 1, 4)
+    assert st == 1 and "out of range" in msg
+
+
+@pytest.mark.parametrize("n,jitter", [(2, 0.0), (3, 0.2)])
+def test_fem_standins_match_oracle(n, jitter):
+    ensure_library()
+    from cudolfinx import fem
+
+    m = fem.create_unit_cube(n, jitter=jitter, seed=0)
+    coords, cells = fo.unit_cube_tet_mesh(n, jitter=jitter, seed=0)
+    assert np.array_equal(m.cells, cells) and np.array_equal(m.geometry_x, coords)
+    V2 = fem.functionspace(m, ("P", 2))
+    dofs, nd, grid = fo.p2_dofmap(n, cells)
+    assert V2.num_nodes == nd and np.array_equal(V2.dofs, dofs)
+    assert np.array_equal(V2.boundary_nodes(), fo.boundary_dofs_from_grid(grid, 2 * n))
+    X = fo.dof_coordinates(coords, cells, dofs, nd, 2)
+    assert np.allclose(V2.tabulate_dof_coordinates(), X)
+    V1 = fem.functionspace(m, ("P", 1))
+    assert np.array_equal(V1.boundary_nodes(), fo.boundary_dofs_from_grid(fo.vertex_grid_index(n), n))
+    Vv = fem.functionspace(m, ("P", 2, (3,)))
+    assert Vv.bs == 3 and Vv.num_dofs == 3 * nd
