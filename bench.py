@@ -48,6 +48,8 @@ import numpy as np  # noqa: E402
 WORKLOADS = {
     "p2": dict(kind="p2", n=96, precision="fp64",
                desc="P2 Poisson n=96: 5,308,416 tets, k P1 lognormal, f DG0 U[-1,1], g=x+y+z"),
+    "p2mid": dict(kind="p2", n=48, precision="fp64",
+                  desc="P2 Poisson n=48 (profiling size): 663,552 tets, k P1 lognormal, f DG0, g=x+y+z"),
     "p1": dict(kind="p1", n=32, precision="fp64",
                desc="P1 Poisson n=32: 196,608 tets, k=1, f=P1(sin sin sin), homogeneous Dirichlet"),
     "p1big": dict(kind="p1", n=128, precision="fp64",
