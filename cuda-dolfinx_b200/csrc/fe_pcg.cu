@@ -13,6 +13,9 @@
 //     in batches and synchronises once per batch.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <mutex>
+
 #include "fe_internal.h"
 
 namespace fe {
@@ -265,4 +268,121 @@ extern "C" int fe_pcg_solve(fe_sparsity s, const double* values, const double* b
   if (status != FE_OK) fe::set_last_error("PCG stopped after " + std::to_string(it) + " iterations at relative residual " +
                                           std::to_string(res));
   return status;
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of the solver.
+//
+// Some callers cannot allocate device memory while they solve: an embedding
+// application whose device memory is already handed to its own pool (a
+// framework caching allocator, or a PETSc / Kokkos arena sized to the card)
+// can have cudaMalloc fail or steal its budget, and a latency-critical loop
+// must not enter the CUDA allocator, which may synchronise the device.
+// fe_pcg_solve_noalloc gives them the same solver with its scratch vectors in
+// a fixed file-scope device array instead of cudaMallocAsync.
+// ---------------------------------------------------------------------------
+namespace fe {
+namespace {
+
+constexpr int64_t kNoAllocMaxRows = int64_t(1) << 18;  // 262,144 rows
+constexpr int kNoAllocMaxGrid = 1024;                   // reduction slots per dot product
+constexpr int64_t kNoAllocScalarWords = 16;            // room for one Scalars record (in doubles)
+static_assert(sizeof(Scalars) <= kNoAllocScalarWords * sizeof(double), "Scalars record does not fit");
+
+// r, z, p, Ap, dinv (kNoAllocMaxRows each), 3 x kNoAllocMaxGrid partial sums, one Scalars record:
+// 5 * 262,144 * 8 B + 3 * 1024 * 8 B + 128 B = 10.5 MB held by every device that loads the library.
+static __device__ __align__(256) double g_pcg_scratch[5 * kNoAllocMaxRows + 3 * kNoAllocMaxGrid +
+                                                      kNoAllocScalarWords];
+
+// Device address of g_pcg_scratch, looked up once per device (with that device current).
+constexpr int kMaxDevices = 64;
+std::mutex g_scratch_mutex;
+double* g_scratch_ptr[kMaxDevices] = {};
+
+double* scratch_address(int device) {
+  if (device < 0 || device >= kMaxDevices) FE_FAIL(FE_ERR_ARG, "device ordinal out of range for the scratch table");
+  std::lock_guard<std::mutex> lock(g_scratch_mutex);
+  if (!g_scratch_ptr[device]) {
+    void* p = nullptr;
+    FE_CUDA(cudaGetSymbolAddress(&p, g_pcg_scratch));
+    g_scratch_ptr[device] = static_cast<double*>(p);
+  }
+  return g_scratch_ptr[device];
+}
+
+template <int SUB>
+void run_noalloc(const fe_sparsity_s& A, const double* val, const double* b, double* x, double rtol, int max_iter,
+                 int* iterations, double* rel_res, double* scratch, cudaStream_t s) {
+  const int64_t n = A.num_rows;
+  const unsigned grid = (unsigned)std::min(A.ctx->num_sms * 4, kNoAllocMaxGrid);
+  double* r = scratch;
+  double* z = r + kNoAllocMaxRows;
+  double* p = z + kNoAllocMaxRows;
+  double* Ap = p + kNoAllocMaxRows;
+  double* dinv = Ap + kNoAllocMaxRows;
+  double* part = dinv + kNoAllocMaxRows;
+  Scalars* sc = reinterpret_cast<Scalars*>(part + 3 * kNoAllocMaxGrid);
+  // Every scratch word a kernel reads is written earlier in the same call:
+  // k_init writes r, z, p, dinv for all n rows, k_spmv writes Ap before
+  // k_update reads it, partial sums are written before each reduction, and
+  // the Scalars record is re-initialised here.
+  Scalars h{};
+  h.tol2 = rtol * rtol;
+  h.max_iter = max_iter;
+  FE_CUDA(cudaMemcpyAsync(sc, &h, sizeof(h), cudaMemcpyHostToDevice, s));
+  k_init<SUB><<<grid, kThreads, 0, s>>>(n, A.row_ptr.p, A.col.p, val, A.diag.p, b, x, r, z, p, dinv, part);
+  k_reduce<<<1, 1024, 0, s>>>(part, grid, 0, sc);
+  FE_CUDA(cudaGetLastError());
+  const int batch = 16;
+  for (int it = 0;; it += batch) {
+    for (int q = 0; q < batch; ++q) {
+      k_spmv<SUB><<<grid, kThreads, 0, s>>>(n, A.row_ptr.p, A.col.p, val, p, Ap, part, sc);
+      k_reduce<<<1, 1024, 0, s>>>(part, grid, 1, sc);
+      k_update<<<grid, kThreads, 0, s>>>(n, x, r, z, p, Ap, dinv, part, sc);
+      k_reduce<<<1, 1024, 0, s>>>(part, grid, 2, sc);
+      k_update_p<<<grid, kThreads, 0, s>>>(n, z, p, sc);
+    }
+    FE_CUDA(cudaGetLastError());
+    FE_CUDA(cudaMemcpyAsync(&h, sc, sizeof(h), cudaMemcpyDeviceToHost, s));
+    FE_CUDA(cudaStreamSynchronize(s));
+    if (h.done || it >= max_iter) break;
+  }
+  *iterations = h.iter;
+  *rel_res = h.bb > 0 ? sqrt(h.rr / h.bb) : 0.0;
+}
+
+}  // namespace
+}  // namespace fe
+
+extern "C" int fe_pcg_solve_noalloc(fe_sparsity s, const double* values, const double* b, double* x, double rtol,
+                                    int max_iter, int* iterations, double* rel_residual, void* stream) {
+  int it = 0;
+  double res = 0.0;
+  try {
+    if (!s || !values || !b || !x) FE_FAIL(FE_ERR_ARG, "null argument");
+    if (s->num_rows != s->num_cols) FE_FAIL(FE_ERR_ARG, "PCG needs a square matrix");
+    if (s->num_rows > fe::kNoAllocMaxRows)
+      FE_FAIL(FE_ERR_ARG, "fe_pcg_solve_noalloc supports at most " + std::to_string(fe::kNoAllocMaxRows) +
+                              " rows (its static scratch size); the matrix has " + std::to_string(s->num_rows) +
+                              " rows: use fe_pcg_solve");
+    FE_CUDA(cudaSetDevice(s->ctx->device));
+    double* scratch = fe::scratch_address(s->ctx->device);
+    const cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    const double mean = s->num_rows ? (double)s->nnz / (double)s->num_rows : 0.0;
+    if (mean <= 6) fe::run_noalloc<4>(*s, values, b, x, rtol, max_iter, &it, &res, scratch, st);
+    else if (mean <= 14) fe::run_noalloc<8>(*s, values, b, x, rtol, max_iter, &it, &res, scratch, st);
+    else if (mean <= 40) fe::run_noalloc<16>(*s, values, b, x, rtol, max_iter, &it, &res, scratch, st);
+    else fe::run_noalloc<32>(*s, values, b, x, rtol, max_iter, &it, &res, scratch, st);
+    if (iterations) *iterations = it;
+    if (rel_residual) *rel_residual = res;
+  } catch (const fe::Error& e) {
+    fe::set_last_error(e.what());
+    return e.code;
+  }
+  if (!(res <= rtol)) {
+    fe::set_last_error("PCG stopped after " + std::to_string(it) + " iterations at relative residual " +
+                       std::to_string(res));
+    return FE_ERR_NOT_CONVERGED;
+  }
+  return FE_OK;
 }

@@ -69,6 +69,7 @@ _SIGS = {
     "fe_apply_lifting": (i32, [vp, i32, vp, vp, vp, dbl, vp]),
     "fe_set_bc": (i32, [vp, i64, vp, vp, dbl, vp]),
     "fe_pcg_solve": (i32, [vp, vp, vp, vp, dbl, i32, ctypes.POINTER(i32), ctypes.POINTER(dbl), vp]),
+    "fe_pcg_solve_noalloc": (i32, [vp, vp, vp, vp, dbl, i32, ctypes.POINTER(i32), ctypes.POINTER(dbl), vp]),
 }
 
 for _name, (_res, _args) in _SIGS.items():

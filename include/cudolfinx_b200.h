@@ -190,6 +190,26 @@ int fe_set_bc(double* b, int64_t num_values, fe_bc bc, const double* x0, double 
 int fe_pcg_solve(fe_sparsity s, const double* values, const double* b, double* x, double rtol,
                  int max_iter, int* iterations, double* rel_residual, void* stream);
 
+/* Allocation-free variant of fe_pcg_solve (no counterpart in the reference).
+ * For callers that cannot allocate device memory while they solve: an
+ * application whose device memory is already reserved by its own pool
+ * allocator (a framework caching allocator, a PETSc / Kokkos arena sized to
+ * the card), or a latency-critical loop that must not enter the CUDA
+ * allocator.  Same arguments, results and status codes as fe_pcg_solve, but
+ * the solver's scratch vectors live in one file-scope device array of
+ * 10.5 MB (5 vectors of 262,144 doubles plus reduction slots), which every
+ * GPU that loads the library holds until the process exits; it calls no
+ * cudaMalloc / cudaFree.
+ *  - Matrices with more than 262,144 rows are rejected with FE_ERR_ARG.
+ *  - The first call on a device looks up the array's device address (once per
+ *    device, with that device current); make that first call before any
+ *    stream capture.
+ *  - Every call shares the one array and re-initialises all of it that it
+ *    reads; calls that overlap on the GPU (other streams, other threads) race
+ *    on it and must be serialised by the caller. */
+int fe_pcg_solve_noalloc(fe_sparsity s, const double* values, const double* b, double* x, double rtol,
+                         int max_iter, int* iterations, double* rel_residual, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
