@@ -2,7 +2,7 @@
 """Headline benchmark: FEM system assembly on one B200 (matrix nnz/s).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload p2|p1|p1big|vp2] [--variant atomic|deterministic]
+                    [--workload p2|p2mid|p1|p1big|vp2] [--variant auto|tile|atomic|sorted-slot]
 
 Default workload (the configuration the headline metric is quoted on): P2
 Poisson on the unit cube, 96^3 hexes x 6 = 5,308,416 tets, 7,189,057 dofs,
@@ -57,7 +57,20 @@ WORKLOADS = {
     "vp2": dict(kind="vp2", n=64, precision="fp32",
                 desc="vector-P2 elasticity n=64: 1,572,864 jittered tets, lam/mu DG0, FP32 element tensors"),
 }
-KERNELS_PER_STEP = 7  # zero A, matrix, set_diagonal, zero b, vector, lifting, set_bc
+# kernels of one step besides the matrix call: zero b, vector, lifting, set_bc
+VECTOR_KERNELS = 4
+
+
+def matrix_kernels(kind: str, variant: str) -> int:
+    """Kernel launches of one fe_assemble_matrix call (with BCs): 2 for the
+    single-pass variants (row gather, tile, ordered tile; + set_diagonal), 3
+    for the atomic scatter (zero + scatter + set_diagonal) and the sorted-slot
+    reduction (element tensors + gather + set_diagonal)."""
+    if variant in ("tile", "row-gather") or (variant == "deterministic" and kind in ("p1", "p2")):
+        return 2
+    return 3  # atomic, block (zero + kernel + set_diagonal), sorted-slot
+
+
 _PINNED: list = []
 
 
@@ -291,14 +304,15 @@ def run_gpu(args, rank, world, local_rank):
     nrows = A.sparsity.num_rows
     stream = torch.cuda.current_stream()
     sp = stream.cuda_stream
-    flags = _lib.ASM_DETERMINISTIC if args.variant == "deterministic" else 0
+    flags = _lib.ASM_ZERO | _lib.VARIANT_FLAGS[args.variant]
     forms = (ctypes.c_void_p * 1)(a.cuda_form)
     bcs1 = (ctypes.c_void_p * 1)(hbc)
     Lib = _lib.lib
     Ap, bp = A.values.data_ptr(), b.vector.data_ptr()
 
     def step(ev0=None, ev1=None):
-        _lib.check(Lib.fe_zero_entries(Ap, nnz, sp), "zero")
+        # the matrix call owns its zeroing: a zero pass before the atomic
+        # scatter, none for the gather variants (they write every value once)
         if ev0 is not None:
             ev0.record(stream)
         _lib.check(Lib.fe_assemble_matrix(a.cuda_form, Ap, hbc, hbc, 1.0, flags, sp), "matrix")
@@ -416,7 +430,7 @@ def run_gpu(args, rank, world, local_rank):
                      "kernel_ms": mat_ms, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"
                      if "hbm_gbs" in peaks else "fallback 6650 GB/s"},
         "matrix_nnz_per_s": nnz / (mat_ms / 1e3),
-        "gpu_launches": KERNELS_PER_STEP * args.steps + (1 if args.variant == "deterministic" else 0) * args.steps,
+        "gpu_launches": (matrix_kernels(W["kind"], args.variant) + VECTOR_KERNELS) * args.steps,
         "clocks": clk,
         "setup_s": setup_s,
     }
@@ -459,7 +473,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="p2")
-    ap.add_argument("--variant", choices=["atomic", "deterministic"], default="atomic")
+    ap.add_argument("--variant", choices=["auto", "tile", "atomic", "sorted-slot", "deterministic", "row-gather",
+                                          "block"], default="auto")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")

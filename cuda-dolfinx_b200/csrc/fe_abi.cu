@@ -204,6 +204,8 @@ int fe_mesh_create(fe_context ctx, const double* coords, int64_t num_nodes, cons
     m->num_cells = num_cells;
     upload(m->x, coords, (size_t)num_nodes * 3);
     upload(m->geom, geom_dofmap, (size_t)num_cells * 4);
+    m->host_x.assign(coords, coords + num_nodes * 3);
+    m->host_geom.assign(geom_dofmap, geom_dofmap + num_cells * 4);
     *out = m.release();
   });
 }
@@ -262,6 +264,7 @@ int fe_sparsity_build(fe_dofmap rows, fe_dofmap cols, fe_sparsity* out) {
     upload(s->row_ptr, row_ptr.data(), row_ptr.size());
     upload(s->col, col.data(), col.size());
     upload(s->diag, diag.data(), diag.size());
+    s->host_row_ptr = std::move(row_ptr);
     s->id = g_next_id++;
     *out = s.release();
   });
@@ -319,6 +322,7 @@ int fe_sparsity_create(fe_context ctx, const int32_t* row_ptr, const int32_t* co
     upload(s->row_ptr, row_ptr, (size_t)num_rows + 1);
     upload(s->col, col, (size_t)nnz);
     upload(s->diag, diag.data(), diag.size());
+    s->host_row_ptr.assign(row_ptr, row_ptr + num_rows + 1);
     s->id = g_next_id++;
     *out = s.release();
   });
@@ -526,11 +530,44 @@ int fe_assemble_matrix(fe_form a, double* values, fe_bc bc0, fe_bc bc1, double d
     if (bc0) FE_REQUIRE(bc0->num_dofs == a->sp->num_rows, "bc0 size differs from the number of rows");
     if (bc1) FE_REQUIRE(bc1->num_dofs == a->sp->num_cols, "bc1 size differs from the number of columns");
     cudaStream_t st = as_stream(stream);
-    if (flags & FE_ASM_DETERMINISTIC) {
-      assemble_matrix_gather(*a, values, bc0, bc1, diagonal, (flags & FE_ASM_ZERO) != 0, st);
+    const bool zero = (flags & FE_ASM_ZERO) != 0;
+    if (flags & FE_ASM_SORTED_SLOT) {
+      assemble_matrix_gather(*a, values, bc0, bc1, diagonal, zero, st);
       return;
     }
-    if (flags & FE_ASM_ZERO) launch_zero(values, a->sp->nnz, st);
+    if (flags & FE_ASM_DETERMINISTIC) {
+      if (tile_supported(*a)) {
+        assemble_matrix_tiled(*a, values, bc0, bc1, zero, true, st);
+        if (bc0) launch_set_diagonal(*a->sp, *bc0, diagonal, values, st);
+      } else {
+        assemble_matrix_gather(*a, values, bc0, bc1, diagonal, zero, st);
+      }
+      return;
+    }
+    if (flags & FE_ASM_TILE) {
+      FE_REQUIRE(tile_supported(*a), "the tile variant supports P1/P2 stiffness only");
+      assemble_matrix_tiled(*a, values, bc0, bc1, zero, false, st);
+      if (bc0) launch_set_diagonal(*a->sp, *bc0, diagonal, values, st);
+      return;
+    }
+    if (flags & FE_ASM_ROW_GATHER) {
+      FE_REQUIRE(rowgather_supported(*a), "the row-gather variant supports P1 stiffness only");
+      assemble_matrix_rowgather(*a, values, bc0, bc1, zero, st);
+      if (bc0) launch_set_diagonal(*a->sp, *bc0, diagonal, values, st);
+      return;
+    }
+    // default: the block variant for P1 meshes above ~1M cells (measured faster
+    // on B200 at 12.6M cells: 0.80 vs 0.86 ms), the FP64-atomic scatter otherwise
+    const bool auto_block = !(flags & FE_ASM_ATOMIC) && a->kind == FE_FORM_P1_STIFFNESS &&
+                            a->mesh->num_cells >= (int64_t(1) << 20);
+    const bool want_block = (flags & FE_ASM_BLOCK) || auto_block;
+    if (flags & FE_ASM_BLOCK) FE_REQUIRE(block_supported(*a), "the block variant supports P1/P2 stiffness only");
+    if (want_block && block_supported(*a)) {
+      assemble_matrix_block(*a, values, bc0, bc1, zero, st);
+      if (bc0) launch_set_diagonal(*a->sp, *bc0, diagonal, values, st);
+      return;
+    }
+    if (zero) launch_zero(values, a->sp->nnz, st);
     MatLaunch L{};
     L.kind = a->kind;
     L.precision = a->precision;

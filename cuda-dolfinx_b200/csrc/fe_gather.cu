@@ -20,18 +20,15 @@
 #include "fe_element_code.cuh"
 #include "fe_internal.h"
 
-struct fe_form_s::Gather {
-  fe::DevBuf<int32_t> seg;      // [nnz+1] start of each slot's contribution list
-  fe::DevBuf<int32_t> contrib;  // [num_contrib] sorted contribution ids
-  fe::DevBuf<double> E;         // [num_contrib] element tensors, entry-major
-  int64_t num_contrib = 0;
-  int K = 0;                    // scalar dofs per cell (k*bs)
-};
-
 fe_form_s::fe_form_s() = default;
 fe_form_s::~fe_form_s() = default;
 
-void fe::reset_gather_plan(fe_form_s& f) { f.gather.reset(); }
+void fe::reset_gather_plan(fe_form_s& f) {
+  f.gather.reset();
+  reset_tile_plan(f);
+  reset_row_plan(f);
+  reset_block_plan(f);
+}
 
 namespace fe {
 namespace {

@@ -87,6 +87,8 @@ struct fe_mesh_s {
   int nodes_per_cell = 4;
   fe::DevBuf<double> x;      // [num_nodes*3]
   fe::DevBuf<int32_t> geom;  // [num_cells*4]
+  std::vector<double> host_x;      // host copies (tile planning)
+  std::vector<int32_t> host_geom;
 };
 
 struct fe_dofmap_s {
@@ -104,6 +106,7 @@ struct fe_sparsity_s {
   fe::DevBuf<int32_t> row_ptr;   // [num_rows+1]
   fe::DevBuf<int32_t> col;       // [nnz]
   fe::DevBuf<int32_t> diag;      // [num_rows] slot of (r, r) or -1
+  std::vector<int32_t> host_row_ptr;  // host copy (tile planning)
   uint64_t id = 0;
 };
 
@@ -144,8 +147,63 @@ struct fe_form_s {
   // deterministic sorted-slot plan (fe_gather.cu); built on first use
   struct Gather;
   std::unique_ptr<Gather> gather;
+  // owner-computes tile plan (fe_tile.cu); built on first use
+  struct TilePlan;
+  std::unique_ptr<TilePlan> tiles;
+  // row-gather plan (fe_rowgather.cu): inverse dofmap; built on first use
+  struct RowPlan;
+  std::unique_ptr<RowPlan> rows;
+  // cell-block plan (fe_block.cu); built on first use
+  struct BlockPlan;
+  std::unique_ptr<BlockPlan> blocks;
   fe_form_s();
   ~fe_form_s();
+};
+
+// Plans owned by a form (defined here so every translation unit can destroy them)
+struct fe_form_s::Gather {
+  fe::DevBuf<int32_t> seg;      // [nnz+1] start of each slot's contribution list
+  fe::DevBuf<int32_t> contrib;  // [num_contrib] sorted contribution ids
+  fe::DevBuf<double> E;         // [num_contrib] element tensors, entry-major
+  int64_t num_contrib = 0;
+  int K = 0;                    // scalar dofs per cell (k*bs)
+};
+
+struct fe_form_s::TilePlan {
+  int64_t ntiles = 0;
+  fe::DevBuf<int32_t> tile_rows_ptr;  // [ntiles+1] into rows
+  fe::DevBuf<int32_t> rows;           // owned block rows, tile by tile
+  fe::DevBuf<int32_t> row_soff;       // offset of each owned row's segment in the tile buffer
+  fe::DevBuf<int32_t> row_tile;       // [block rows] owning tile of each row
+  fe::DevBuf<int32_t> row_local;      // [block rows] index of the row inside its tile
+  fe::DevBuf<int32_t> tile_cells_ptr; // [ntiles+1] into cells
+  fe::DevBuf<int32_t> cells;          // cells touching each tile (ascending within a tile)
+  fe::DevBuf<int32_t> tile_rec_ptr;   // [ntiles+1] into recs
+  fe::DevBuf<uint32_t> recs;          // (row_local << 16) | (lc << 8) | i
+  fe::DevBuf<int32_t> tile_goff_ptr;  // [ntiles+1] into goff
+  fe::DevBuf<int32_t> goff;           // per chunk: NG+1 offsets relative to the tile's first record
+  int64_t total_cells = 0;            // sum of tile cell lists (>= num_cells: border cells repeat)
+};
+
+struct fe_form_s::RowPlan {
+  fe::DevBuf<int32_t> inc_ptr;        // [block rows + 1]
+  fe::DevBuf<int32_t> inc;            // incidences cell*k + i, grouped by row
+};
+
+struct fe_form_s::BlockPlan {
+  int64_t nblocks = 0;
+  const fe_dofmap_s* coef_map_owner = nullptr;  // P1 coefficient dofmap the plan copied
+  fe::DevBuf<int32_t> block_ptr;      // [nblocks+1] cell ranges (block order)
+  fe::DevBuf<int32_t> brow_ptr;       // [nblocks+1] into rows/soff
+  fe::DevBuf<int32_t> rows;           // touched block rows per block (ascending)
+  fe::DevBuf<int32_t> soff;           // window offset of each touched row
+  fe::DevBuf<uint16_t> lrow;          // [cells][k] window row of each local dof
+  fe::DevBuf<int32_t> cell_id;        // block order -> original cell
+  fe::DevBuf<int32_t> geom;           // [cells][4] geometry dofmap, block order
+  fe::DevBuf<int32_t> dofs0, dofs1;   // [cells][k] form dofmaps, block order
+  fe::DevBuf<uint8_t> pos;            // [cells][k*k] slot bytes, block order
+  fe::DevBuf<int32_t> coef_map;       // [cells][4] P1 coefficient dofmap, block order
+  fe::DevBuf<double> gbound;          // [nblocks] geometric part of the element-entry bound
 };
 
 namespace fe {
@@ -220,7 +278,25 @@ void launch_set_bc(double* b, int64_t num_values, const int32_t* dofs, int64_t n
 // error word of the current context's kernels
 unsigned* device_error_word(fe_context ctx);
 
-// drops the deterministic plan of a form (fe_gather.cu)
+// drops the deterministic plans of a form (fe_gather.cu, fe_tile.cu)
 void reset_gather_plan(fe_form_s& f);
+void reset_tile_plan(fe_form_s& f);
+
+// owner-computes tile assembly (fe_tile.cu): true if the form kind has a tile kernel
+bool tile_supported(const fe_form_s& f);
+void assemble_matrix_tiled(fe_form_s& f, double* values, const fe_bc_s* bc0, const fe_bc_s* bc1, bool zero,
+                           bool deterministic, cudaStream_t s);
+
+// cell-block assembly (fe_block.cu) for P1/P2 stiffness
+bool block_supported(const fe_form_s& f);
+void reset_block_plan(fe_form_s& f);
+void assemble_matrix_block(fe_form_s& f, double* values, const fe_bc_s* bc0, const fe_bc_s* bc1, bool zero,
+                           cudaStream_t s);
+
+// row-gather assembly (fe_rowgather.cu) for P1 stiffness
+bool rowgather_supported(const fe_form_s& f);
+void reset_row_plan(fe_form_s& f);
+void assemble_matrix_rowgather(fe_form_s& f, double* values, const fe_bc_s* bc0, const fe_bc_s* bc1, bool zero,
+                               cudaStream_t s);
 
 }  // namespace fe

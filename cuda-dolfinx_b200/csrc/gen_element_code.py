@@ -78,6 +78,26 @@ def lit(x: Fraction) -> str:
     return float(x).hex()
 
 
+def sum_expr(var, terms, chains=4):
+    """sum_t var[idx_t] * c_t as up to `chains` independent fma chains added
+    by a balanced tree: the critical path is ~len/chains fmas instead of len."""
+    if not terms:
+        return "T(0)"
+    n = min(chains, len(terms))
+    parts = []
+    for k in range(n):
+        sub = terms[k::n]
+        idx, c = sub[0]
+        e = f"{var}[{idx}] * T({lit(c)})"
+        for idx, c in sub[1:]:
+            e = f"fma({var}[{idx}], T({lit(c)}), {e})"
+        parts.append(e)
+    while len(parts) > 1:
+        parts = [f"({parts[q]} + {parts[q + 1]})" if q + 1 < len(parts) else parts[q]
+                 for q in range(0, len(parts), 2)]
+    return parts[0]
+
+
 def r_weighted(m, a, b, i, j):
     return pint(pmul(LAM[m], pmul(DPHI[i][a], DPHI[j][b])))
 
@@ -113,6 +133,7 @@ def gen() -> str:
     w("template <typename T, typename Emit>\n")
     w("__device__ __forceinline__ void p2_stiffness_p1coef(const T* q, Emit&& emit) {\n")
     nterms = 0
+    maxabs_p1coef = Fraction(0)
     for (i, j) in UNIQ:
         terms = []
         for m in range(4):
@@ -120,11 +141,9 @@ def gen() -> str:
                 c = sym_pair(lambda a, b, ii, jj: r_weighted(m, a, b, ii, jj), s, i, j)
                 if c != 0:
                     terms.append((m * 6 + s, c))
+                    maxabs_p1coef = max(maxabs_p1coef, abs(c))
         nterms += len(terms)
-        expr = "T(0)"
-        for idx, c in terms:
-            expr = f"fma(q[{idx}], T({lit(c)}), {expr})"
-        w(f"  emit({i}, {j}, {expr});\n")
+        w(f"  emit({i}, {j}, {sum_expr('q', terms)});\n")
     w("}\n")
     w(f"// terms: {nterms}\n\n")
 
@@ -132,17 +151,19 @@ def gen() -> str:
     w("// P2 stiffness with a cellwise-constant coefficient: g[s] = k * Ghat_s.\n")
     w("template <typename T, typename Emit>\n")
     w("__device__ __forceinline__ void p2_stiffness_const(const T* g, Emit&& emit) {\n")
+    maxabs_const = Fraction(0)
     for (i, j) in UNIQ:
         terms = []
         for s in range(6):
             c = sym_pair(r_plain, s, i, j)
             if c != 0:
                 terms.append((s, c))
-        expr = "T(0)"
-        for idx, c in terms:
-            expr = f"fma(g[{idx}], T({lit(c)}), {expr})"
-        w(f"  emit({i}, {j}, {expr});\n")
+                maxabs_const = max(maxabs_const, abs(c))
+        w(f"  emit({i}, {j}, {sum_expr('g', terms, 2)});\n")
     w("}\n\n")
+    w("// Largest |coefficient| of the two P2 stiffness bodies: |A_ij| <= max * sum|q| bounds every entry.\n")
+    w(f"constexpr double kP2P1CoefTermMax = {lit(maxabs_p1coef)};\n")
+    w(f"constexpr double kP2ConstTermMax = {lit(maxabs_const)};\n\n")
 
     # vector P2 elasticity: block (a,b), entry (i,j): sum_pq W[p*3+q] R0[p][q][i][j]
     w("// One 10x10 block of vector-P2 elasticity: value(i,j) = sum_pq W[p*3+q] *\n")
@@ -159,10 +180,7 @@ def gen() -> str:
                         c = r_plain(p, q, i, j)
                         if c != 0:
                             terms.append((p * 3 + q, c))
-                expr = "T(0)"
-                for idx, c in terms:
-                    expr = f"fma(W[{idx}], T({lit(c)}), {expr})"
-                w(f"  emit({i}, {j}, {expr});\n")
+                w(f"  emit({i}, {j}, {sum_expr('W', terms, 2)});\n")
         w("}\n\n")
     w("}  // namespace fe\n")
     return "".join(out)

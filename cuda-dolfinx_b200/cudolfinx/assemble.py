@@ -77,8 +77,18 @@ class CUDAAssembler:
 
     # -- assembly ------------------------------------------------------------
     def assemble_matrix(self, a: CUDAForm, mat: typing.Optional[CUDAMatrix] = None, bcs=(), diagonal: float = 1.0,
-                        constants=None, coeffs=None, zero: bool = True, deterministic: bool = False) -> CUDAMatrix:
-        """Assemble a bilinear form into a device CSR matrix (not finalised)."""
+                        constants=None, coeffs=None, zero: bool = True, deterministic: bool = False,
+                        variant: str = "auto") -> CUDAMatrix:
+        """Assemble a bilinear form into a device CSR matrix (not finalised).
+
+        ``variant``: "auto" (row gather for P1, atomic scatter otherwise),
+        "deterministic" (bitwise reproducible: ordered tile gather for P1/P2,
+        sorted-slot otherwise), "atomic" (FP64-atomic scatter), "sorted-slot"
+        (global sorted-slot reduction), "tile" (owner-computes row tiles with
+        shared-memory accumulation, P1/P2), "row-gather" (P1).
+        ``deterministic=True`` is the same as variant="deterministic"."""
+        if variant not in _lib.VARIANT_FLAGS:
+            raise ValueError(f"unknown variant {variant!r}; expected one of {sorted(_lib.VARIANT_FLAGS)}")
         if not isinstance(a, CUDAForm):
             raise TypeError(f"Expected CUDAForm, got '{type(a)}'")
         if mat is None:
@@ -91,7 +101,8 @@ class CUDAAssembler:
         # as the reference (assemble.py:100-103): always copy host coefficients to the device
         a.to_device()
         self.pack_coefficients(a, coeffs)
-        flags = (_lib.ASM_ZERO if zero else 0) | (_lib.ASM_DETERMINISTIC if deterministic else 0)
+        flags = ((_lib.ASM_ZERO if zero else 0) | (_lib.ASM_DETERMINISTIC if deterministic else 0)
+                 | _lib.VARIANT_FLAGS[variant])
         _lib.check(_lib.lib.fe_assemble_matrix(a.cuda_form, mat.values.data_ptr(), bc0.handle if bc0 else None,
                                                bc1.handle if bc1 else None, float(diagonal), flags,
                                                self._ctx.stream()), "fe_assemble_matrix")

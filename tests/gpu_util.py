@@ -62,7 +62,7 @@ def mirror_problem(P, precision="fp64"):
     return out
 
 
-def run_system(P, deterministic=False, precision="fp64"):
+def run_system(P, deterministic=False, precision="fp64", variant="auto"):
     """A (host CSR arrays) and b through the mirror API: assemble_matrix with
     BCs, assemble_vector + apply_lifting + set_bc."""
     M = mirror_problem(P, precision)
@@ -71,7 +71,7 @@ def run_system(P, deterministic=False, precision="fp64"):
     a = cx.form(M["a"])
     L = cx.form(M["L"])
     bcs = asm.pack_bcs([M["bc"]])
-    A = asm.assemble_matrix(a, bcs=bcs, deterministic=deterministic)
+    A = asm.assemble_matrix(a, bcs=bcs, deterministic=deterministic, variant=variant)
     A.assemble()
     b = asm.assemble_vector(L)
     asm.apply_lifting(b, [a], [bcs])

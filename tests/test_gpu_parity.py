@@ -30,11 +30,24 @@ def _problem_from_golden(path):
     return P, G
 
 
+VARIANTS = ["auto", "atomic", "tile", "deterministic", "sorted-slot", "row-gather", "block"]
+
+
+def _supported(kind, variant):
+    if variant == "row-gather":
+        return kind in ("p1", "p1k")
+    if variant in ("tile", "block"):
+        return kind in ("p1", "p1k", "p2")
+    return True
+
+
 @pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLDEN, "*.npz"))))
-@pytest.mark.parametrize("deterministic", [False, True])
-def test_golden_fixtures(path, deterministic):
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_golden_fixtures(path, variant):
     P, G = _problem_from_golden(path)
-    R = run_system(P, deterministic=deterministic)
+    if not _supported(P["kind"], variant):
+        pytest.skip("variant not offered for this element")
+    R = run_system(P, variant=variant)
     assert np.array_equal(R["row_ptr"], G["row_ptr"]) and np.array_equal(R["col"], G["col"])
     ok, worst = tolerance_check(R["A"], G["A"])
     assert ok, worst
@@ -43,11 +56,13 @@ def test_golden_fixtures(path, deterministic):
 
 
 @pytest.mark.parametrize("kind,n", CASES)
-@pytest.mark.parametrize("deterministic", [False, True])
-def test_system_parity(kind, n, deterministic):
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_system_parity(kind, n, variant):
+    if not _supported(kind, variant):
+        pytest.skip("variant not offered for this element")
     P = fo.build_problem(kind, n, seed=n)
     S = fo.solve_system(P)
-    R = run_system(P, deterministic=deterministic)
+    R = run_system(P, variant=variant)
     assert np.array_equal(R["row_ptr"], S["row_ptr"]) and np.array_equal(R["col"], S["col"])
     ok, worst = tolerance_check(R["A"], S["A"])
     assert ok, f"A worst rel err {worst}"
@@ -55,14 +70,15 @@ def test_system_parity(kind, n, deterministic):
     assert ok, f"b worst rel err {worst}"
 
 
-@pytest.mark.parametrize("kind,n", [("p1", 8), ("p2", 5), ("vp2", 3)])
-def test_deterministic_is_bitwise_reproducible(kind, n):
+@pytest.mark.parametrize("kind,n,variant", [("p1", 8, "deterministic"), ("p2", 5, "deterministic"),
+                                            ("p1", 8, "sorted-slot"), ("vp2", 3, "deterministic")])
+def test_deterministic_is_bitwise_reproducible(kind, n, variant):
     P = fo.build_problem(kind, n, seed=3)
-    R1 = run_system(P, deterministic=True)
+    R1 = run_system(P, variant=variant)
     asm, A, (a, _), bcs = R1["asm"], R1["Aobj"], R1["forms"], R1["bcs"]
     first = A.values.clone()
     for _ in range(3):
-        asm.assemble_matrix(a, A, bcs=bcs, deterministic=True)
+        asm.assemble_matrix(a, A, bcs=bcs, variant=variant)
         A.assemble()
         assert bool((A.values == first).all())
 
@@ -80,10 +96,10 @@ def test_matrix_without_bcs_and_zero_false_accumulates():
     ref = fo.assemble_matrix(Ae, P["dofs"], P["dofs"], rp, col)
     ok, worst = tolerance_check(A.values.cpu().numpy(), ref)
     assert ok, worst
-    for det in (False, True):
-        asm.assemble_matrix(a, A, zero=False, deterministic=det)
+    for variant in ("atomic", "tile", "deterministic", "sorted-slot"):
+        asm.assemble_matrix(a, A, zero=False, variant=variant)
         A.assemble()
-    ok, worst = tolerance_check(A.values.cpu().numpy(), 3 * ref)
+    ok, worst = tolerance_check(A.values.cpu().numpy(), 5 * ref)
     assert ok, worst
 
 
