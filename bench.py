@@ -57,6 +57,13 @@ WORKLOADS = {
     "vp2": dict(kind="vp2", n=64, precision="fp32",
                 desc="vector-P2 elasticity n=64: 1,572,864 jittered tets, lam/mu DG0, FP32 element tensors"),
 }
+# batched workload: many DG0-coefficient instances on one mesh and pattern
+BATCH = dict(n=48, instances=256, cpu_sample=4,
+             desc="256 instances of P1 Poisson on one 48^3 x 6 = 663,552-tet mesh, DG0 k log-uniform "
+                  "[1e-2,1e2] per cell and instance, one shared pattern, homogeneous Dirichlet; FP32 element "
+                  "tensors, FP64 accumulation")
+# kernels of one batched call with <= 448 instances: pack, element tensors, record fill, gather
+BATCH_KERNELS = 4
 # kernels of one step besides the matrix call: zero b, vector, lifting, set_bc
 VECTOR_KERNELS = 4
 
@@ -442,7 +449,192 @@ def run_gpu(args, rank, world, local_rank):
     return out
 
 
+def batch_inputs(seed: int):
+    """P1 stiffness form with a DG0 coefficient on the batch mesh, the BC and
+    the oracle-style problem dict (host, seeded)."""
+    from cudolfinx import fem
+
+    mesh = fem.create_unit_cube(BATCH["n"])
+    V = fem.functionspace(mesh, ("P", 1))
+    W = fem.functionspace(mesh, ("DG", 0))
+    C = mesh.num_cells
+    a = fem.stiffness(V, fem.Function(W, np.ones(C)))
+    bc_dofs = fem.locate_boundary_dofs(V)
+    bc = fem.dirichletbc(fem.Function(V), bc_dofs)
+    I = {"kind": "p1", "n": BATCH["n"], "mesh": mesh, "V": V, "a": a, "bc": bc, "bc_dofs": bc_dofs,
+         "ndof": V.num_nodes, "bs": 1, "dofs": V.dofs, "coords": mesh.geometry_x, "cells": mesh.cells,
+         "g": np.zeros(V.num_nodes), "f": np.ones(V.num_nodes)}
+    return I
+
+
+def batch_coefficients(S: int, C: int, seed: int, device):
+    """k_s(c) log-uniform in [1e-2, 1e2], seeded, generated on the device."""
+    import torch
+
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    u = torch.rand((S, C), generator=g, dtype=torch.float64, device=device)
+    return torch.exp(np.log(1e-2) + u * (np.log(1e2) - np.log(1e-2)))
+
+
+def cpu_batch_baseline(I, row_ptr, col, nnz, kd, sample, reps=1):
+    """C port of the reference CPU path, one instance at a time (the reference
+    has no batch path), on `sample` instances."""
+    from oracle import cfem
+
+    threads = os.cpu_count() or 1
+    P = oracle_problem(I)
+    P["kind"] = "p1k"
+    times = []
+    for s in range(sample):
+        P["k"] = kd[s].cpu().numpy()
+        C = cfem.CpuAssembler(P, row_ptr, col, nthreads=threads)
+        C.assemble_matrix()  # warm
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            C.assemble_matrix()
+        times.append((time.perf_counter() - t0) / reps)
+        C.close()
+    t = sum(times)
+    return {"value": nnz * sample / t, "unit": "nnz/s", "cores": threads, "kind": "port",
+            "sample": f"{sample} of the {BATCH['instances']} instances, one matrix assembly each (BC skip, "
+                      f"unit diagonal), {threads} threads, C port of the reference CPU path (oracle/cfem.c)",
+            "seconds_per_instance": t / sample}
+
+
+def run_gpu_batch(args, rank, world, local_rank):
+    import torch
+
+    import cudolfinx as cx
+    from cudolfinx import _lib
+
+    torch.cuda.set_device(local_rank)
+    t_setup = time.perf_counter()
+    I = batch_inputs(args.seed)
+    S = BATCH["instances"]
+    C = len(I["cells"])
+    asm = cx.CUDAAssembler()
+    a = cx.form(I["a"])
+    A0 = asm.create_matrix(a)
+    nnz = A0.sparsity.nnz
+    nrows = A0.sparsity.num_rows
+    dbc = asm.pack_bcs([I["bc"]])
+    hbc = dbc._get_cpp_bcs(I["V"]).handle
+    kd = batch_coefficients(S, C, args.seed + 1000 * (rank + 1), "cuda")
+    vals = torch.zeros((S, nnz), dtype=torch.float64, device="cuda")
+    ktab = (ctypes.c_void_p * S)(*[kd[s].data_ptr() for s in range(S)])
+    vtab = (ctypes.c_void_p * S)(*[vals[s].data_ptr() for s in range(S)])
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+    Lib = _lib.lib
+
+    def step():
+        _lib.check(Lib.fe_assemble_matrix_batch(a.cuda_form, S, ktab, vtab, hbc, hbc, 1.0, _lib.ASM_ZERO, sp),
+                   "batch")
+
+    step()
+    torch.cuda.synchronize()
+    setup_s = time.perf_counter() - t_setup
+    for _ in range(args.warmup):
+        step()
+    dist = torch.distributed if world > 1 else None
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    time.sleep(0.3)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    e_start = torch.cuda.Event(enable_timing=True)
+    e_end = torch.cuda.Event(enable_timing=True)
+    e_start.record(stream)
+    for k in range(args.steps):
+        ev[k][0].record(stream)
+        step()
+        ev[k][1].record(stream)
+    e_end.record(stream)
+    torch.cuda.synchronize()
+    total_ms = e_start.elapsed_time(e_end)
+    call_ms = statistics.mean(x.elapsed_time(y) for x, y in ev)
+    clk = clocks.stop()
+
+    # the plain path: one FP64 fe_assemble_matrix per instance (default variant)
+    ap = cx.form(I["a"])
+    ap._bind(A0.sparsity)
+    plain_vals = torch.zeros(nnz, dtype=torch.float64, device="cuda")
+
+    def plain_all():
+        for s in range(S):
+            _lib.check(Lib.fe_form_set_coefficient(ap.cuda_form, 0, _lib.COEFF_DG0, None, kd[s].data_ptr(), C, 1,
+                                                   sp), "set_coefficient")
+            _lib.check(Lib.fe_assemble_matrix(ap.cuda_form, plain_vals.data_ptr(), hbc, hbc, 1.0, _lib.ASM_ZERO,
+                                              sp), "matrix")
+
+    plain_all()
+    torch.cuda.synchronize()
+    p0 = torch.cuda.Event(enable_timing=True)
+    p1 = torch.cuda.Event(enable_timing=True)
+    p0.record(stream)
+    plain_all()
+    p1.record(stream)
+    torch.cuda.synchronize()
+    plain_ms = p0.elapsed_time(p1)
+    # agreement of the last instance between the two paths (FP32 element tensors)
+    rel = float(torch.linalg.norm(vals[S - 1] - plain_vals) / torch.linalg.norm(plain_vals))
+    if dist:
+        t = torch.tensor([total_ms, call_ms, plain_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms, call_ms, plain_ms = (float(x) for x in t)
+
+    alg = S * (8 * nnz + 8 * C) + 16 * C + 16 * C + 16 * C + 24 * len(I["coords"]) + 4 * (nrows + 1) + nrows
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            peaks = json.load(fh)
+    except (OSError, ValueError):
+        pass
+    peak = peaks.get("hbm_gbs", 6650.0)
+    achieved = alg / (call_ms / 1e3) / 1e9
+    out = {
+        "metric": "matrix nnz/s (batched instances)",
+        "value": world * S * nnz * args.steps / (total_ms / 1e3),
+        "unit": "nnz/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32-element/f64-accumulate",
+        "data": "synthetic (seeded mesh; coefficients from a seeded device generator)",
+        "config": {"workload": BATCH["desc"], "instances": S, "cells": C, "dofs": nrows, "nnz": nnz,
+                   "step": "fe_assemble_matrix_batch: pack coefficients + unit element tensors + record fill + "
+                           "persistent gather into %d CSR value arrays" % S,
+                   "l2": "inputs larger than L2 (values %.2f GB per step)" % (8 * S * nnz / 1e9),
+                   "parallelism": f"replicas x{world}"},
+        "roofline": {"bound": "hbm", "kernel": "batched assembly call (4 launches)", "achieved": achieved,
+                     "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": load_traffic("batch"),
+                     "algorithmic_bytes": alg, "kernel_ms": call_ms,
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if "hbm_gbs" in peaks
+                     else "fallback 6650 GB/s"},
+        "plain_fp64": {"ms_per_batch": plain_ms, "nnz_per_s": S * nnz / (plain_ms / 1e3),
+                       "speedup_of_batch": plain_ms / call_ms,
+                       "path": "one fe_assemble_matrix (FP64, default variant) per instance",
+                       "rel_frobenius_last_instance": rel},
+        "gpu_launches": BATCH_KERNELS * args.steps,
+        "clocks": clk,
+        "setup_s": setup_s,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        row_ptr, col = A0.sparsity.to_host()
+        out["cpu_baseline"] = cpu_batch_baseline(I, row_ptr, col, nnz, kd, BATCH["cpu_sample"])
+    return out
+
+
 def run_reference(args):
+    if args.workload == "batch":
+        return run_reference_batch(args)
     W = WORKLOADS[args.workload]
     I = make_inputs(W["kind"], W["n"], seed=args.seed)
     row_ptr, col = host_pattern(I)
@@ -466,13 +658,54 @@ def run_reference(args):
             "e2e": {"value": v, "unit": "nnz/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+def run_reference_batch(args):
+    import torch
+
+    I = batch_inputs(args.seed)
+    row_ptr, col = host_pattern(I)
+    nnz = len(col)
+    kd = batch_coefficients(BATCH["cpu_sample"], len(I["cells"]), args.seed + 1000, "cpu")
+    from oracle import cfem
+
+    threads = os.cpu_count() or 1
+    P = oracle_problem(I)
+    P["kind"] = "p1k"
+    P["k"] = kd[0].numpy()
+    Cq = cfem.CpuAssembler(P, row_ptr, col, nthreads=threads)
+
+    def one_step():
+        t0 = time.perf_counter()
+        for s in range(BATCH["cpu_sample"]):
+            Cq.c0 = np.ascontiguousarray(kd[s].numpy())
+            Cq.assemble_matrix()
+        return time.perf_counter() - t0
+
+    for _ in range(args.warmup):
+        one_step()
+    times = [one_step() for _ in range(args.steps)]
+    Cq.close()
+    total = sum(times)
+    v = nnz * BATCH["cpu_sample"] * args.steps / total
+    del torch
+    return {"impl": "reference", "metric": "matrix nnz/s (batched instances)", "value": v, "unit": "nnz/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded)",
+            "config": {"workload": BATCH["desc"], "cells": len(I["cells"]), "nnz": nnz,
+                       "step": f"{BATCH['cpu_sample']} instances (bounded sample), one assembly each"},
+            "cpu_baseline": {"value": v, "unit": "nnz/s", "cores": threads, "kind": "port",
+                             "sample": f"{BATCH['cpu_sample']} instances per step; C port of the reference CPU "
+                                       "path (oracle/cfem.c), which has no batch path"},
+            "e2e": {"value": v, "unit": "nnz/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="p2")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batch"], default="p2")
     ap.add_argument("--variant", choices=["auto", "tile", "atomic", "sorted-slot", "deterministic", "row-gather",
                                           "block"], default="auto")
     ap.add_argument("--seed", type=int, default=0)
@@ -496,7 +729,8 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local_rank))
     try:
-        out = run_gpu(args, rank, world, local_rank)
+        runner = run_gpu_batch if args.workload == "batch" else run_gpu
+        out = runner(args, rank, world, local_rank)
         if rank == 0:
             print(json.dumps(out), flush=True)
     finally:

@@ -591,6 +591,21 @@ int fe_assemble_matrix(fe_form a, double* values, fe_bc bc0, fe_bc bc1, double d
   });
 }
 
+int fe_assemble_matrix_batch(fe_form a, int num_instances, const double* const* coefficients,
+                             double* const* values, fe_bc bc0, fe_bc bc1, double diagonal, unsigned flags,
+                             void* stream) {
+  return guard([&] {
+    FE_REQUIRE(a, "null form");
+    FE_REQUIRE(a->rank == 2, "assemble_matrix_batch needs a bilinear form");
+    FE_REQUIRE(a->sp, "bind a sparsity pattern first (fe_form_bind_sparsity)");
+    if (bc0) FE_REQUIRE(bc0->num_dofs == a->sp->num_rows, "bc0 size differs from the number of rows");
+    if (bc1) FE_REQUIRE(bc1->num_dofs == a->sp->num_cols, "bc1 size differs from the number of columns");
+    DeviceScope d(a->ctx);
+    assemble_matrix_batch(*a, num_instances, coefficients, values, bc0, bc1, diagonal, (flags & FE_ASM_ZERO) != 0,
+                          as_stream(stream));
+  });
+}
+
 int fe_zero_entries(double* values, int64_t n, void* stream) {
   return guard([&] {
     FE_REQUIRE(n >= 0 && (values || n == 0), "invalid argument");

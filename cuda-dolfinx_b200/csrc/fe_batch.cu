@@ -1,0 +1,385 @@
+// Batched assembly: many coefficient instances of one bilinear form on one
+// mesh and one sparsity pattern, written into as many caller-owned CSR value
+// arrays.
+//
+// The reference assembles one form instance per call (python/cudolfinx/
+// assemble.py:52-110, one launch of CUDAFormIntegral.cpp:1103-1226 per
+// matrix); it has no batch path.  For a cellwise-constant (DG0) coefficient k
+// the element matrix of instance s is k_s(c) * A_c, with A_c the element
+// matrix of the unit coefficient, so
+//     A_s[slot] = sum over the slot's element entries (c, e) of k_s(c) * A_c[e].
+// The batch computes A_c once per call, in FP32 (geometry, Jacobian,
+// determinant and inverse in FP64), and then forms every instance's values
+// with FP64 accumulation in one persistent launch:
+//   k_batch_pack    k_s(c) (FP64, one array per instance) -> kp[c][s] (FP32),
+//                   a tiled transpose (the batch's pack_coefficients)
+//   k_batch_elem_*  unit-coefficient element tensors E[c][i*K+j]
+//   k_batch_fill    rec[r] = {E of record r, cell of record r}, records in
+//                   slot order (the sorted-slot plan of fe_gather.cu)
+//   k_batch_gather  persistent; one warp per (32 slots x 32*IPL instances):
+//                   lane = instance while summing a slot's records (the
+//                   coefficient row kp[c][..] is one coalesced load), lane =
+//                   slot while storing (a staging tile in shared memory turns
+//                   the result so each instance's 32 slots go out as one
+//                   256-byte store).  BC rows/columns and the BC diagonal are
+//                   applied in the store.
+// Every instance's slot sum runs in the plan's fixed record order, so the
+// result is bitwise reproducible.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "fe_element_code.cuh"
+#include "fe_internal.h"
+
+namespace fe {
+namespace {
+
+constexpr int kMaxBatchLaunch = 448;  // instances per launch: the pointer tables travel as kernel
+                                       // parameters (< 4 KB); a multiple of 64 keeps chunks aligned
+constexpr int kSlotsPerItem = 32;
+
+unsigned nblocks(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
+
+// ---- plan ----------------------------------------------------------------
+__global__ void k_plan_records(const int32_t* __restrict__ contrib, int64_t nrec, int64_t num_cells,
+                               int32_t* __restrict__ rec_cell, uint8_t* __restrict__ rec_entry) {
+  const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (r >= nrec) return;
+  const int64_t id = contrib[r];  // entry * num_cells + cell
+  const int64_t e = id / num_cells;
+  rec_cell[r] = (int32_t)(id - e * num_cells);
+  rec_entry[r] = (uint8_t)e;
+}
+
+__global__ void k_plan_slot_row(const int32_t* __restrict__ row_ptr, int64_t num_rows, int32_t* __restrict__ slot_row) {
+  const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (r >= num_rows) return;
+  for (int32_t s = row_ptr[r]; s < row_ptr[r + 1]; ++s) slot_row[s] = (int32_t)r;
+}
+
+// ---- pack ----------------------------------------------------------------
+struct PackArgs {
+  int64_t num_cells;
+  int num_inst;       // instances in this launch
+  int64_t ld;         // row stride of kp (floats)
+  int col0;           // first kp column of this launch
+  float* kp;
+  const double* coef[kMaxBatchLaunch];
+};
+
+// 32 cells x 32 instances per block: coalesced reads along cells, coalesced
+// writes along instances; columns past num_inst are written as zero.
+__global__ void __launch_bounds__(256) k_batch_pack(const __grid_constant__ PackArgs a) {
+  __shared__ float t[32][33];
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  const int64_t c0 = blockIdx.x * 32ll;
+  const int s0 = blockIdx.y * 32;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int sl = ty + 8 * j, s = s0 + sl;
+    const int64_t c = c0 + tx;
+    t[sl][tx] = (s < a.num_inst && c < a.num_cells) ? (float)__ldg(a.coef[s] + c) : 0.0f;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int cl = ty + 8 * j;
+    const int64_t c = c0 + cl;
+    if (c < a.num_cells && a.col0 + s0 + tx < a.ld) a.kp[c * a.ld + a.col0 + s0 + tx] = t[tx][cl];
+  }
+}
+
+// ---- unit-coefficient element tensors (FP32 out, FP64 geometry) ----------
+struct ElemArgs {
+  int64_t num_cells;
+  const double* __restrict__ x;
+  const int32_t* __restrict__ geom;
+  float* __restrict__ E;
+};
+
+struct Geo {
+  double K[3][3];
+  double adet;
+};
+
+__device__ __forceinline__ void geometry(const double* __restrict__ x, const int32_t* __restrict__ geom, int64_t c,
+                                         Geo& g) {
+  const int4 v = __ldg(reinterpret_cast<const int4*>(geom) + c);
+  const int vv[4] = {v.x, v.y, v.z, v.w};
+  double J[3][3];
+#pragma unroll
+  for (int cc = 0; cc < 3; ++cc)
+#pragma unroll
+    for (int r = 0; r < 3; ++r) J[r][cc] = __ldg(x + 3 * (int64_t)vv[cc + 1] + r) - __ldg(x + 3 * (int64_t)vv[0] + r);
+  const double c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1];
+  const double c01 = J[1][2] * J[2][0] - J[1][0] * J[2][2];
+  const double c02 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
+  const double det = J[0][0] * c00 + J[0][1] * c01 + J[0][2] * c02;
+  const double id = 1.0 / det;
+  g.K[0][0] = c00 * id;
+  g.K[1][0] = c01 * id;
+  g.K[2][0] = c02 * id;
+  g.K[0][1] = (J[0][2] * J[2][1] - J[0][1] * J[2][2]) * id;
+  g.K[1][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) * id;
+  g.K[2][1] = (J[0][1] * J[2][0] - J[0][0] * J[2][1]) * id;
+  g.K[0][2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) * id;
+  g.K[1][2] = (J[0][2] * J[1][0] - J[0][0] * J[1][2]) * id;
+  g.K[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) * id;
+  g.adet = fabs(det);
+}
+
+__global__ void k_batch_elem_p1(const ElemArgs a) {
+  const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (c >= a.num_cells) return;
+  Geo g;
+  geometry(a.x, a.geom, c, g);
+  double G[4][3];
+#pragma unroll
+  for (int b = 0; b < 3; ++b) {
+    G[1][b] = g.K[0][b];
+    G[2][b] = g.K[1][b];
+    G[3][b] = g.K[2][b];
+    G[0][b] = -(g.K[0][b] + g.K[1][b] + g.K[2][b]);
+  }
+  const double s = g.adet * (1.0 / 6.0);
+  float v[16];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = i; j < 4; ++j) {
+      v[i * 4 + j] = (float)(s * (G[i][0] * G[j][0] + G[i][1] * G[j][1] + G[i][2] * G[j][2]));
+      v[j * 4 + i] = v[i * 4 + j];
+    }
+  float4* out = reinterpret_cast<float4*>(a.E + c * 16);
+#pragma unroll
+  for (int q = 0; q < 4; ++q) out[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+}
+
+__global__ void k_batch_elem_p2(const ElemArgs a) {
+  const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (c >= a.num_cells) return;
+  Geo g;
+  geometry(a.x, a.geom, c, g);
+  const int pa[6] = {0, 1, 2, 0, 0, 1}, pb[6] = {0, 1, 2, 1, 2, 2};
+  float gq[6];
+#pragma unroll
+  for (int s = 0; s < 6; ++s)
+    gq[s] = (float)(g.adet * (g.K[pa[s]][0] * g.K[pb[s]][0] + g.K[pa[s]][1] * g.K[pb[s]][1] +
+                              g.K[pa[s]][2] * g.K[pb[s]][2]));
+  float* __restrict__ E = a.E + c * 100;
+  p2_stiffness_const<float>(gq, [&](int i, int j, float v) {
+    E[i * 10 + j] = v;
+    if (i != j) E[j * 10 + i] = v;
+  });
+}
+
+__global__ void k_batch_fill(const int32_t* __restrict__ rec_cell, const uint8_t* __restrict__ rec_entry,
+                             int64_t nrec, int KK, const float* __restrict__ E, float2* __restrict__ rec) {
+  const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (r >= nrec) return;
+  const int32_t c = rec_cell[r];
+  rec[r] = make_float2(__ldg(E + (int64_t)c * KK + rec_entry[r]), __int_as_float(c));
+}
+
+// ---- persistent gather ---------------------------------------------------
+struct GatherArgs {
+  int64_t nnz;
+  int num_inst;        // instances in this launch
+  int col0;            // kp column of the launch's first instance
+  int64_t ld;          // kp row stride (floats)
+  int64_t num_items;   // slot groups * instance chunks
+  int num_chunks;
+  const int32_t* seg;
+  const float2* rec;
+  const float* kp;
+  const int32_t* slot_row;
+  const int32_t* col;
+  const uint8_t* bc0;
+  const uint8_t* bc1;
+  double diagonal;
+  int zero;
+  double* values[kMaxBatchLaunch];
+};
+
+template <int IPL>
+struct GatherCfg {
+  static constexpr int CHUNK = 32 * IPL;        // instances per work item
+  static constexpr int WARPS = IPL == 1 ? 8 : 4;
+  static constexpr int TSTRIDE = CHUNK + 1;     // doubles per staged slot (odd: conflict-free column reads)
+  static constexpr size_t SMEM = (size_t)WARPS * kSlotsPerItem * TSTRIDE * sizeof(double);
+};
+
+template <int IPL>
+__global__ void __launch_bounds__(32 * GatherCfg<IPL>::WARPS) k_batch_gather(const __grid_constant__ GatherArgs a) {
+  using Cfg = GatherCfg<IPL>;
+  extern __shared__ double stage_all[];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  double* __restrict__ T = stage_all + wid * (kSlotsPerItem * Cfg::TSTRIDE);
+  const int64_t nw = (int64_t)gridDim.x * Cfg::WARPS;
+  for (int64_t item = blockIdx.x * (int64_t)Cfg::WARPS + wid; item < a.num_items; item += nw) {
+    const int64_t g = item / a.num_chunks;
+    const int ioff = (int)(item - g * a.num_chunks) * Cfg::CHUNK;
+    const int64_t s0 = g * kSlotsPerItem;
+    const int ns = (int)min((int64_t)kSlotsPerItem, a.nnz - s0);
+    const float* __restrict__ kb = a.kp + a.col0 + ioff + lane * IPL;
+    int32_t r = __ldg(a.seg + s0);
+    for (int j = 0; j < ns; ++j) {
+      const int32_t r1 = __ldg(a.seg + s0 + j + 1);
+      double acc[IPL];
+#pragma unroll
+      for (int t = 0; t < IPL; ++t) acc[t] = 0.0;
+#pragma unroll 4
+      for (; r < r1; ++r) {
+        const float2 rc = __ldg(a.rec + r);
+        const double ae = (double)rc.x;
+        const float* kr = kb + (int64_t)__float_as_int(rc.y) * a.ld;
+        if constexpr (IPL == 1) {
+          acc[0] = fma(ae, (double)__ldg(kr), acc[0]);
+        } else {
+          const float2 kv = __ldg(reinterpret_cast<const float2*>(kr));
+          acc[0] = fma(ae, (double)kv.x, acc[0]);
+          acc[1] = fma(ae, (double)kv.y, acc[1]);
+        }
+      }
+#pragma unroll
+      for (int t = 0; t < IPL; ++t) T[j * Cfg::TSTRIDE + lane * IPL + t] = acc[t];
+    }
+    __syncwarp();
+    if (lane < ns) {
+      const int64_t slot = s0 + lane;
+      bool mask = false, diag = false;
+      if (a.bc0 || a.bc1) {
+        const int32_t row = __ldg(a.slot_row + slot), cl = __ldg(a.col + slot);
+        const bool rm = a.bc0 && a.bc0[row];
+        mask = rm || (a.bc1 && a.bc1[cl]);
+        diag = rm && row == cl;
+      }
+      const int nin = min(Cfg::CHUNK, a.num_inst - ioff);
+      for (int i = 0; i < nin; ++i) {
+        double* __restrict__ out = a.values[ioff + i] + slot;
+        double v = a.zero ? 0.0 : *out;
+        if (!mask) v += T[lane * Cfg::TSTRIDE + i];
+        if (diag) v = a.diagonal;
+        *out = v;
+      }
+    }
+    __syncwarp();
+  }
+}
+
+template <int IPL>
+void launch_gather(const GatherArgs& ga, int num_sms, cudaStream_t s) {
+  using Cfg = GatherCfg<IPL>;
+  // per device and cheap: set on every launch rather than cached
+  FE_CUDA(cudaFuncSetAttribute(k_batch_gather<IPL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM));
+  int per_sm = 0;
+  FE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_gather<IPL>, 32 * Cfg::WARPS, Cfg::SMEM));
+  const int64_t want = (ga.num_items + Cfg::WARPS - 1) / Cfg::WARPS;
+  const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)num_sms * std::max(1, per_sm)));
+  k_batch_gather<IPL><<<(unsigned)grid, 32 * Cfg::WARPS, Cfg::SMEM, s>>>(ga);
+  FE_CUDA(cudaGetLastError());
+}
+
+}  // namespace
+
+bool batch_supported(const fe_form_s& f) {
+  return (f.kind == FE_FORM_P1_STIFFNESS || f.kind == FE_FORM_P2_STIFFNESS) && f.V0 && f.V0->bs == 1;
+}
+
+void reset_batch_plan(fe_form_s& f) { f.batch.reset(); }
+
+void assemble_matrix_batch(fe_form_s& f, int num_instances, const double* const* coefficients,
+                           double* const* values, const fe_bc_s* bc0, const fe_bc_s* bc1, double diagonal,
+                           bool zero, cudaStream_t s) {
+  FE_REQUIRE(batch_supported(f), "batched assembly supports P1/P2 stiffness with a DG0 coefficient only");
+  FE_REQUIRE(num_instances >= 0, "negative instance count");
+  if (bc0) FE_REQUIRE(bc0->n_owned == bc0->n_bc, "batched assembly needs every BC dof owned");
+  if (num_instances == 0) return;
+  FE_REQUIRE(coefficients && values, "null coefficient or value table");
+  const int64_t C = f.mesh->num_cells;
+  const int64_t nnz = f.sp->nnz;
+  for (int i = 0; i < num_instances; ++i) {
+    FE_REQUIRE(coefficients[i] || C == 0, "null coefficient array");
+    FE_REQUIRE(values[i] || nnz == 0, "null value array");
+  }
+  const int K = f.V0->k;
+  const int KK = K * K;
+  if (!f.batch) {
+    ensure_gather_plan(f, s);
+    auto B = std::make_unique<fe_form_s::BatchPlan>();
+    B->num_records = f.gather->num_contrib;
+    B->KK = KK;
+    B->rec_cell.alloc(std::max<int64_t>(1, B->num_records));
+    B->rec_entry.alloc(std::max<int64_t>(1, B->num_records));
+    B->slot_row.alloc(std::max<int64_t>(1, nnz));
+    B->E.alloc(std::max<int64_t>(1, C * KK));
+    B->rec.alloc(std::max<int64_t>(1, B->num_records));
+    if (B->num_records) {
+      k_plan_records<<<nblocks(B->num_records, 256), 256, 0, s>>>(f.gather->contrib.p, B->num_records, C,
+                                                                  B->rec_cell.p, B->rec_entry.p);
+      FE_CUDA(cudaGetLastError());
+    }
+    if (f.sp->num_rows) {
+      k_plan_slot_row<<<nblocks(f.sp->num_rows, 256), 256, 0, s>>>(f.sp->row_ptr.p, f.sp->num_rows, B->slot_row.p);
+      FE_CUDA(cudaGetLastError());
+    }
+    f.batch = std::move(B);
+  }
+  auto& B = *f.batch;
+  // packed coefficients: one row of ld floats per cell, resized on demand
+  const int ipl = num_instances > 32 ? 2 : 1;
+  const int chunk = 32 * ipl;
+  const int64_t ld = ((int64_t)num_instances + chunk - 1) / chunk * chunk;
+  if (B.kp_ld != ld || !B.kp.p) {
+    B.kp.alloc(std::max<int64_t>(1, C * ld));
+    B.kp_ld = ld;
+  }
+  if (C) {
+    for (int i0 = 0; i0 < num_instances; i0 += kMaxBatchLaunch) {
+      PackArgs pa{};
+      pa.num_cells = C;
+      pa.num_inst = std::min(kMaxBatchLaunch, num_instances - i0);
+      pa.ld = ld;
+      pa.col0 = i0;
+      pa.kp = B.kp.p;
+      for (int i = 0; i < pa.num_inst; ++i) pa.coef[i] = coefficients[i0 + i];
+      // the last launch also zeroes the padding columns up to ld
+      const int64_t cols = (i0 + kMaxBatchLaunch >= num_instances) ? ld - i0 : pa.num_inst;
+      dim3 grid(nblocks(C, 32), nblocks(cols, 32));
+      k_batch_pack<<<grid, 256, 0, s>>>(pa);
+      FE_CUDA(cudaGetLastError());
+    }
+    ElemArgs ea{C, f.mesh->x.p, f.mesh->geom.p, B.E.p};
+    if (f.kind == FE_FORM_P1_STIFFNESS) k_batch_elem_p1<<<nblocks(C, 128), 128, 0, s>>>(ea);
+    else k_batch_elem_p2<<<nblocks(C, 128), 128, 0, s>>>(ea);
+    FE_CUDA(cudaGetLastError());
+    k_batch_fill<<<nblocks(B.num_records, 256), 256, 0, s>>>(B.rec_cell.p, B.rec_entry.p, B.num_records, KK, B.E.p,
+                                                             B.rec.p);
+    FE_CUDA(cudaGetLastError());
+  }
+  if (!nnz) return;
+  for (int i0 = 0; i0 < num_instances; i0 += kMaxBatchLaunch) {
+    GatherArgs ga{};
+    ga.nnz = nnz;
+    ga.num_inst = std::min(kMaxBatchLaunch, num_instances - i0);
+    ga.col0 = i0;
+    ga.ld = ld;
+    ga.num_chunks = (ga.num_inst + chunk - 1) / chunk;
+    ga.num_items = ((nnz + kSlotsPerItem - 1) / kSlotsPerItem) * ga.num_chunks;
+    ga.seg = f.gather->seg.p;
+    ga.rec = B.rec.p;
+    ga.kp = B.kp.p;
+    ga.slot_row = B.slot_row.p;
+    ga.col = f.sp->col.p;
+    ga.bc0 = bc0 ? bc0->markers.p : nullptr;
+    ga.bc1 = bc1 ? bc1->markers.p : nullptr;
+    ga.diagonal = diagonal;
+    ga.zero = zero ? 1 : 0;
+    for (int i = 0; i < ga.num_inst; ++i) ga.values[i] = values[i0 + i];
+    if (ipl == 2) launch_gather<2>(ga, f.ctx->num_sms, s);
+    else launch_gather<1>(ga, f.ctx->num_sms, s);
+  }
+}
+
+}  // namespace fe

@@ -28,6 +28,7 @@ void fe::reset_gather_plan(fe_form_s& f) {
   reset_tile_plan(f);
   reset_row_plan(f);
   reset_block_plan(f);
+  reset_batch_plan(f);
 }
 
 namespace fe {
@@ -327,41 +328,45 @@ unsigned blocks(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
 }  // namespace
 
-void assemble_matrix_gather(fe_form_s& f, double* values, const fe_bc_s* bc0, const fe_bc_s* bc1, double diagonal,
-                            bool zero, cudaStream_t s) {
+void ensure_gather_plan(fe_form_s& f, cudaStream_t s) {
+  if (f.gather) return;
   const int64_t C = f.mesh->num_cells;
   const int bs = f.V0->bs;
   const int K = f.V0->k * bs;
   const int64_t ncontrib = C * K * K;
-  if (ncontrib > INT32_MAX) FE_FAIL(FE_ERR_ARG, "too many element entries for the deterministic plan");
+  if (ncontrib > INT32_MAX) FE_FAIL(FE_ERR_ARG, "too many element entries for the sorted-slot plan");
   SlotArgs sa{C, f.V0->dofs.p, f.V1->dofs.p, f.V0->k, f.V1->k, bs, f.pos.p, f.sp->row_ptr.p};
-  if (!f.gather) {
-    auto G = std::make_unique<fe_form_s::Gather>();
-    const int64_t nnz = f.sp->nnz;
-    G->num_contrib = ncontrib;
-    G->K = K;
-    G->seg.alloc(nnz + 1);
-    G->contrib.alloc(std::max<int64_t>(1, ncontrib));
-    G->E.alloc(std::max<int64_t>(1, ncontrib));
-    FE_CUDA(cudaMemsetAsync(G->seg.p, 0, (nnz + 1) * sizeof(int32_t), s));
-    if (ncontrib) {
-      k_count<<<blocks(ncontrib, 256), 256, 0, s>>>(sa, G->seg.p);
-      FE_CUDA(cudaGetLastError());
-    }
-    scan_exclusive(G->seg.p, nnz + 1, s);
-    DevBuf<int32_t> cursor(nnz + 1);
-    FE_CUDA(cudaMemcpyAsync(cursor.p, G->seg.p, (nnz + 1) * sizeof(int32_t), cudaMemcpyDeviceToDevice, s));
-    if (ncontrib) {
-      k_fill<<<blocks(ncontrib, 256), 256, 0, s>>>(sa, cursor.p, G->contrib.p);
-      FE_CUDA(cudaGetLastError());
-    }
-    if (nnz) {
-      k_sort_segments<<<blocks(nnz, 256), 256, 0, s>>>(G->seg.p, nnz, G->contrib.p);
-      FE_CUDA(cudaGetLastError());
-    }
-    FE_CUDA(cudaStreamSynchronize(s));  // cursor is freed on return
-    f.gather = std::move(G);
+  auto G = std::make_unique<fe_form_s::Gather>();
+  const int64_t nnz = f.sp->nnz;
+  G->num_contrib = ncontrib;
+  G->K = K;
+  G->seg.alloc(nnz + 1);
+  G->contrib.alloc(std::max<int64_t>(1, ncontrib));
+  FE_CUDA(cudaMemsetAsync(G->seg.p, 0, (nnz + 1) * sizeof(int32_t), s));
+  if (ncontrib) {
+    k_count<<<blocks(ncontrib, 256), 256, 0, s>>>(sa, G->seg.p);
+    FE_CUDA(cudaGetLastError());
   }
+  scan_exclusive(G->seg.p, nnz + 1, s);
+  DevBuf<int32_t> cursor(nnz + 1);
+  FE_CUDA(cudaMemcpyAsync(cursor.p, G->seg.p, (nnz + 1) * sizeof(int32_t), cudaMemcpyDeviceToDevice, s));
+  if (ncontrib) {
+    k_fill<<<blocks(ncontrib, 256), 256, 0, s>>>(sa, cursor.p, G->contrib.p);
+    FE_CUDA(cudaGetLastError());
+  }
+  if (nnz) {
+    k_sort_segments<<<blocks(nnz, 256), 256, 0, s>>>(G->seg.p, nnz, G->contrib.p);
+    FE_CUDA(cudaGetLastError());
+  }
+  FE_CUDA(cudaStreamSynchronize(s));  // cursor is freed on return
+  f.gather = std::move(G);
+}
+
+void assemble_matrix_gather(fe_form_s& f, double* values, const fe_bc_s* bc0, const fe_bc_s* bc1, double diagonal,
+                            bool zero, cudaStream_t s) {
+  const int64_t C = f.mesh->num_cells;
+  ensure_gather_plan(f, s);
+  if (!f.gather->E.p) f.gather->E.alloc(std::max<int64_t>(1, f.gather->num_contrib));
   auto& G = *f.gather;
   ElemArgs ea{};
   ea.num_cells = C;

@@ -156,6 +156,9 @@ struct fe_form_s {
   // cell-block plan (fe_block.cu); built on first use
   struct BlockPlan;
   std::unique_ptr<BlockPlan> blocks;
+  // batched-instance plan (fe_batch.cu); built on first use
+  struct BatchPlan;
+  std::unique_ptr<BatchPlan> batch;
   fe_form_s();
   ~fe_form_s();
 };
@@ -204,6 +207,18 @@ struct fe_form_s::BlockPlan {
   fe::DevBuf<uint8_t> pos;            // [cells][k*k] slot bytes, block order
   fe::DevBuf<int32_t> coef_map;       // [cells][4] P1 coefficient dofmap, block order
   fe::DevBuf<double> gbound;          // [nblocks] geometric part of the element-entry bound
+};
+
+struct fe_form_s::BatchPlan {
+  int64_t num_records = 0;            // num_cells * K * K
+  int KK = 0;                         // element entries per cell
+  fe::DevBuf<int32_t> rec_cell;       // [records] cell of each slot-sorted record
+  fe::DevBuf<uint8_t> rec_entry;      // [records] local entry i*K+j of each record
+  fe::DevBuf<int32_t> slot_row;       // [nnz] CSR row of each slot
+  fe::DevBuf<float> E;                // [cells][KK] unit-coefficient element tensors (FP32)
+  fe::DevBuf<float2> rec;             // [records] {entry value, cell bits}, refreshed per call
+  fe::DevBuf<float> kp;               // [cells][ld] packed instance coefficients (FP32)
+  int64_t kp_ld = 0;
 };
 
 namespace fe {
@@ -292,6 +307,18 @@ bool block_supported(const fe_form_s& f);
 void reset_block_plan(fe_form_s& f);
 void assemble_matrix_block(fe_form_s& f, double* values, const fe_bc_s* bc0, const fe_bc_s* bc1, bool zero,
                            cudaStream_t s);
+
+// sorted-slot plan (fe_gather.cu): per CSR slot the ordered list of element
+// entries that land there; built on first use
+void ensure_gather_plan(fe_form_s& f, cudaStream_t s);
+
+// batched assembly of many DG0-coefficient instances on one mesh and pattern
+// (fe_batch.cu)
+bool batch_supported(const fe_form_s& f);
+void reset_batch_plan(fe_form_s& f);
+void assemble_matrix_batch(fe_form_s& f, int num_instances, const double* const* coefficients,
+                           double* const* values, const fe_bc_s* bc0, const fe_bc_s* bc1, double diagonal,
+                           bool zero, cudaStream_t s);
 
 // row-gather assembly (fe_rowgather.cu) for P1 stiffness
 bool rowgather_supported(const fe_form_s& f);

@@ -66,6 +66,7 @@ _SIGS = {
     "fe_bc_update": (i32, [vp, vp, vp]),
     "fe_bc_destroy": (i32, [vp]),
     "fe_assemble_matrix": (i32, [vp, vp, vp, vp, dbl, u32, vp]),
+    "fe_assemble_matrix_batch": (i32, [vp, i32, vp, vp, vp, vp, dbl, u32, vp]),
     "fe_zero_entries": (i32, [vp, i64, vp]),
     "fe_assemble_vector": (i32, [vp, vp, u32, vp]),
     "fe_apply_lifting": (i32, [vp, i32, vp, vp, vp, dbl, vp]),

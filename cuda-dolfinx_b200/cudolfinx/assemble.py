@@ -81,11 +81,12 @@ class CUDAAssembler:
                         variant: str = "auto") -> CUDAMatrix:
         """Assemble a bilinear form into a device CSR matrix (not finalised).
 
-        ``variant``: "auto" (row gather for P1, atomic scatter otherwise),
-        "deterministic" (bitwise reproducible: ordered tile gather for P1/P2,
-        sorted-slot otherwise), "atomic" (FP64-atomic scatter), "sorted-slot"
-        (global sorted-slot reduction), "tile" (owner-computes row tiles with
-        shared-memory accumulation, P1/P2), "row-gather" (P1).
+        ``variant``: "auto" (block variant for P1 on meshes of >= 2^20 cells,
+        atomic scatter otherwise), "deterministic" (bitwise reproducible:
+        ordered tile gather for P1/P2, sorted-slot otherwise), "atomic"
+        (FP64-atomic scatter), "sorted-slot" (global sorted-slot reduction),
+        "block" (Morton cell blocks combined in shared memory, P1/P2), "tile"
+        (owner-computes row tiles, P1/P2), "row-gather" (P1).
         ``deterministic=True`` is the same as variant="deterministic"."""
         if variant not in _lib.VARIANT_FLAGS:
             raise ValueError(f"unknown variant {variant!r}; expected one of {sorted(_lib.VARIANT_FLAGS)}")
@@ -108,6 +109,55 @@ class CUDAAssembler:
                                                self._ctx.stream()), "fe_assemble_matrix")
         mat._bcs = col  # keep device BC data alive while the work is queued
         return mat
+
+    def assemble_matrix_batch(self, a: CUDAForm, coefficients, mats: typing.Optional[list] = None, bcs=(),
+                              diagonal: float = 1.0, zero: bool = True) -> list:
+        """Assemble many instances of a P1/P2 stiffness form that differ only
+        in a DG0 coefficient, in one batched launch (no counterpart in the
+        reference, which assembles one form per call).
+
+        ``coefficients``: a sequence of device float64 tensors of length
+        num_cells, or one (instances, num_cells) tensor.  ``mats``: CUDAMatrix
+        objects sharing the form's pattern (created when None).  Element
+        tensors are FP32 and slot sums FP64 in a fixed order, so results are
+        bitwise reproducible; BC semantics match ``assemble_matrix``."""
+        if not isinstance(a, CUDAForm):
+            raise TypeError(f"Expected CUDAForm, got '{type(a)}'")
+        if isinstance(coefficients, torch.Tensor) and coefficients.dim() == 2:
+            coefficients = list(coefficients.unbind(0))
+        coefficients = list(coefficients)
+        if not coefficients and not mats:
+            return []
+        ncells = a._spec.mesh.num_cells
+        for k in coefficients:
+            if not (isinstance(k, torch.Tensor) and k.is_cuda and k.dtype == torch.float64 and k.is_contiguous()
+                    and k.numel() == ncells):
+                raise ValueError("each coefficient must be a contiguous float64 device tensor of num_cells values")
+        if mats is None:
+            first = self.create_matrix(a)
+            mats = [first] + [CUDAMatrix(self._ctx, first.sparsity) for _ in coefficients[1:]]
+        elif len(mats) != len(coefficients):
+            raise ValueError("need one matrix per coefficient instance")
+        if mats:
+            a._bind(mats[0].sparsity)
+            for m in mats[1:]:
+                if m.sparsity is not mats[0].sparsity:
+                    raise ValueError("all matrices of a batch must share one sparsity pattern")
+        col = self._bc_collection(bcs)
+        bc0 = col._get_cpp_bcs(a.function_spaces[0])
+        bc1 = col._get_cpp_bcs(a.function_spaces[1])
+        a.to_device()
+        import ctypes
+        n = len(coefficients)
+        ktab = (ctypes.c_void_p * max(1, n))(*[k.data_ptr() for k in coefficients])
+        vtab = (ctypes.c_void_p * max(1, n))(*[m.values.data_ptr() for m in mats])
+        _lib.check(_lib.lib.fe_assemble_matrix_batch(a.cuda_form, n, ktab, vtab, bc0.handle if bc0 else None,
+                                                     bc1.handle if bc1 else None, float(diagonal),
+                                                     _lib.ASM_ZERO if zero else 0, self._ctx.stream()),
+                   "fe_assemble_matrix_batch")
+        for m in mats:
+            m._bcs = col
+        return mats
 
     def assemble_vector(self, b: CUDAForm, vec: typing.Optional[CUDAVector] = None, constants=None, coeffs=None,
                         zero: bool = True) -> CUDAVector:

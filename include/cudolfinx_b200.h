@@ -173,6 +173,19 @@ int fe_bc_destroy(fe_bc bc);
  * owned bc0 rows get `diagonal` on the diagonal when the form is square. */
 int fe_assemble_matrix(fe_form a, double* values, fe_bc bc0, fe_bc bc1, double diagonal,
                        unsigned flags, void* stream);
+/* Batched matrix assembly; no counterpart in the reference, whose
+ * assemble_matrix (python/cudolfinx/assemble.py:52-110) takes one form
+ * instance per call.  Assembles `num_instances` instances of the P1 or P2
+ * stiffness form `a` that differ only in a DG0 coefficient:
+ * coefficients[i] (device f64[num_cells]) is instance i's k, values[i]
+ * (device f64[nnz] of a's bound pattern) receives instance i's CSR values.
+ * Both tables are host arrays of device pointers.  Element tensors are FP32,
+ * slot sums FP64 in a fixed order (bitwise reproducible).  BC handling and
+ * FE_ASM_ZERO as fe_assemble_matrix; other flags are ignored.  The form's own
+ * coefficient is not used. */
+int fe_assemble_matrix_batch(fe_form a, int num_instances, const double* const* coefficients,
+                             double* const* values, fe_bc bc0, fe_bc bc1, double diagonal,
+                             unsigned flags, void* stream);
 /* Replaces zero_matrix_entries / zero_vector_entries (wrappers/fem.cpp:212-222,
  * 256-266; kernel CUDAAssembler.cpp:38-56): values[0..n) = 0 on `stream`. */
 int fe_zero_entries(double* values, int64_t n, void* stream);
