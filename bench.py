@@ -511,7 +511,7 @@ def run_gpu_batch(args, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     t_setup = time.perf_counter()
     I = batch_inputs(args.seed)
-    S = BATCH["instances"]
+    S = args.instances or BATCH["instances"]
     C = len(I["cells"])
     asm = cx.CUDAAssembler()
     a = cx.form(I["a"])
@@ -608,7 +608,8 @@ def run_gpu_batch(args, rank, world, local_rank):
         "vs_baseline": None,
         "dtype": "f32-element/f64-accumulate",
         "data": "synthetic (seeded mesh; coefficients from a seeded device generator)",
-        "config": {"workload": BATCH["desc"], "instances": S, "cells": C, "dofs": nrows, "nnz": nnz,
+        "config": {"workload": BATCH["desc"] if S == BATCH["instances"] else
+                   BATCH["desc"].replace("256 instances", f"{S} instances"), "instances": S, "cells": C, "dofs": nrows, "nnz": nnz,
                    "step": "fe_assemble_matrix_batch: pack coefficients + unit element tensors + record fill + "
                            "persistent gather into %d CSR value arrays" % S,
                    "l2": "inputs larger than L2 (values %.2f GB per step)" % (8 * S * nnz / 1e9),
@@ -709,6 +710,8 @@ def main():
     ap.add_argument("--variant", choices=["auto", "tile", "atomic", "sorted-slot", "deterministic", "row-gather",
                                           "block"], default="auto")
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--instances", type=int, default=0,
+                    help="batch workload: number of instances (default 256; smaller for profiling)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

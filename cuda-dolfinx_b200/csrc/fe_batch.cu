@@ -16,18 +16,20 @@
 //   k_batch_elem_*  unit-coefficient element tensors E[c][i*K+j]
 //   k_batch_fill    rec[r] = {E of record r, cell of record r}, records in
 //                   slot order (the sorted-slot plan of fe_gather.cu)
-//   k_batch_gather  persistent; one warp per (32 slots x 32*IPL instances):
+//   k_batch_gather  persistent; one warp per (8 slots x 32*IPL instances):
 //                   lane = instance while summing a slot's records (the
 //                   coefficient row kp[c][..] is one coalesced load), lane =
 //                   slot while storing (a staging tile in shared memory turns
-//                   the result so each instance's 32 slots go out as one
-//                   256-byte store).  BC rows/columns and the BC diagonal are
+//                   the result so each instance's 8 slots go out as one
+//                   64-byte store, four instances per instruction).  BC rows/columns and the BC diagonal are
 //                   applied in the store.
 // Every instance's slot sum runs in the plan's fixed record order, so the
 // result is bitwise reproducible.
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
+#include <type_traits>
 
 #include "fe_element_code.cuh"
 #include "fe_internal.h"
@@ -35,11 +37,19 @@
 namespace fe {
 namespace {
 
-constexpr int kMaxBatchLaunch = 448;  // instances per launch: the pointer tables travel as kernel
-                                       // parameters (< 4 KB); a multiple of 64 keeps chunks aligned
-constexpr int kSlotsPerItem = 32;
+constexpr int kMaxBatchLaunch = 384;  // instances per launch: the pointer tables travel as kernel
+                                       // parameters (< 4 KB); a multiple of 128 keeps chunks aligned
+constexpr int kSlotsPerItem = 8;  // slots per gather work item
 
 unsigned nblocks(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
+
+// slot-sorted record: unit element-tensor entry (FP32 value, held as double)
+// and its cell
+struct alignas(16) BatchRec {
+  double ae;
+  int32_t cell;
+  int32_t pad;
+};
 
 // ---- plan ----------------------------------------------------------------
 __global__ void k_plan_records(const int32_t* __restrict__ contrib, int64_t nrec, int64_t num_cells,
@@ -175,11 +185,11 @@ __global__ void k_batch_elem_p2(const ElemArgs a) {
 }
 
 __global__ void k_batch_fill(const int32_t* __restrict__ rec_cell, const uint8_t* __restrict__ rec_entry,
-                             int64_t nrec, int KK, const float* __restrict__ E, float2* __restrict__ rec) {
+                             int64_t nrec, int KK, const float* __restrict__ E, BatchRec* __restrict__ rec) {
   const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (r >= nrec) return;
   const int32_t c = rec_cell[r];
-  rec[r] = make_float2(__ldg(E + (int64_t)c * KK + rec_entry[r]), __int_as_float(c));
+  rec[r] = BatchRec{(double)__ldg(E + (int64_t)c * KK + rec_entry[r]), c, 0};
 }
 
 // ---- persistent gather ---------------------------------------------------
@@ -191,7 +201,7 @@ struct GatherArgs {
   int64_t num_items;   // slot groups * instance chunks
   int num_chunks;
   const int32_t* seg;
-  const float2* rec;
+  const BatchRec* rec;
   const float* kp;
   const int32_t* slot_row;
   const int32_t* col;
@@ -205,63 +215,151 @@ struct GatherArgs {
 template <int IPL>
 struct GatherCfg {
   static constexpr int CHUNK = 32 * IPL;        // instances per work item
-  static constexpr int WARPS = IPL == 1 ? 8 : 4;
-  static constexpr int TSTRIDE = CHUNK + 1;     // doubles per staged slot (odd: conflict-free column reads)
-  static constexpr size_t SMEM = (size_t)WARPS * kSlotsPerItem * TSTRIDE * sizeof(double);
+  static constexpr int WARPS = 8;
+  static constexpr int TSTRIDE = CHUNK + 1;     // doubles per staged slot
+  static constexpr int MIN_BLOCKS = 3;          // 24 resident warps per SM
+  static constexpr size_t WARP_SMEM = kSlotsPerItem * TSTRIDE * sizeof(double) + 32 * sizeof(BatchRec);
+  static constexpr size_t SMEM = WARPS * WARP_SMEM;
 };
 
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kLoadBatch = 8;  // coefficient loads in flight per warp
+
 template <int IPL>
-__global__ void __launch_bounds__(32 * GatherCfg<IPL>::WARPS) k_batch_gather(const __grid_constant__ GatherArgs a) {
+struct KVec;
+template <>
+struct KVec<1> {
+  using T = float;
+  static __device__ __forceinline__ double at(const float& v, int) { return (double)v; }
+};
+template <>
+struct KVec<2> {
+  using T = float2;
+  static __device__ __forceinline__ double at(const float2& v, int t) { return (double)(t ? v.y : v.x); }
+};
+template <>
+struct KVec<4> {
+  using T = float4;
+  static __device__ __forceinline__ double at(const float4& v, int t) {
+    return (double)(t == 0 ? v.x : t == 1 ? v.y : t == 2 ? v.z : v.w);
+  }
+};
+
+// One warp per work item (kSlotsPerItem consecutive slots x CHUNK instances;
+// lane l holds instances l*IPL .. l*IPL+IPL-1 of the chunk).  The item's
+// records are a contiguous range, read 32 at a time with one coalesced load
+// into a per-warp buffer and broadcast from there, so the coefficient loads
+// (one coalesced CHUNK-wide row segment per record) do not wait on a record
+// load and kLoadBatch of them are in flight.  Staged results use column
+// (i % IPL) * 32 + i / IPL for instance i, so the per-lane writes are
+// conflict-free.
+template <int IPL>
+__global__ void __launch_bounds__(32 * GatherCfg<IPL>::WARPS, GatherCfg<IPL>::MIN_BLOCKS)
+    k_batch_gather(const __grid_constant__ GatherArgs a) {
   using Cfg = GatherCfg<IPL>;
-  extern __shared__ double stage_all[];
+  using KV = typename KVec<IPL>::T;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  double* __restrict__ T = stage_all + wid * (kSlotsPerItem * Cfg::TSTRIDE);
+  unsigned char* wbase = smem_raw + wid * Cfg::WARP_SMEM;
+  BatchRec* __restrict__ R = reinterpret_cast<BatchRec*>(wbase);
+  double* __restrict__ T = reinterpret_cast<double*>(wbase + 32 * sizeof(BatchRec));
   const int64_t nw = (int64_t)gridDim.x * Cfg::WARPS;
   for (int64_t item = blockIdx.x * (int64_t)Cfg::WARPS + wid; item < a.num_items; item += nw) {
-    const int64_t g = item / a.num_chunks;
-    const int ioff = (int)(item - g * a.num_chunks) * Cfg::CHUNK;
+    const uint32_t g32 = (uint32_t)item / (uint32_t)a.num_chunks;  // items < 2^31 (host check)
+    const int64_t g = g32;
+    const int ioff = (int)((uint32_t)item - g32 * (uint32_t)a.num_chunks) * Cfg::CHUNK;
     const int64_t s0 = g * kSlotsPerItem;
     const int ns = (int)min((int64_t)kSlotsPerItem, a.nnz - s0);
-    const float* __restrict__ kb = a.kp + a.col0 + ioff + lane * IPL;
-    int32_t r = __ldg(a.seg + s0);
-    for (int j = 0; j < ns; ++j) {
-      const int32_t r1 = __ldg(a.seg + s0 + j + 1);
-      double acc[IPL];
+    const KV* __restrict__ kb = reinterpret_cast<const KV*>(a.kp + a.col0 + ioff + lane * IPL);
+    const int64_t ldv = a.ld / IPL;
+    // lane l < ns holds the end of slot l's record list
+    const int32_t my_end = lane < ns ? __ldg(a.seg + s0 + lane + 1) : INT32_MAX;
+    const int32_t R0 = __ldg(a.seg + s0);
+    const int32_t R1 = __shfl_sync(kFull, my_end, ns - 1);
+    int j = 0;
+    int32_t cur_end = __shfl_sync(kFull, my_end, 0);
+    double acc[IPL];
 #pragma unroll
-      for (int t = 0; t < IPL; ++t) acc[t] = 0.0;
-#pragma unroll 4
-      for (; r < r1; ++r) {
-        const float2 rc = __ldg(a.rec + r);
-        const double ae = (double)rc.x;
-        const float* kr = kb + (int64_t)__float_as_int(rc.y) * a.ld;
-        if constexpr (IPL == 1) {
-          acc[0] = fma(ae, (double)__ldg(kr), acc[0]);
-        } else {
-          const float2 kv = __ldg(reinterpret_cast<const float2*>(kr));
-          acc[0] = fma(ae, (double)kv.x, acc[0]);
-          acc[1] = fma(ae, (double)kv.y, acc[1]);
+    for (int t = 0; t < IPL; ++t) acc[t] = 0.0;
+    auto flush = [&]() {
+#pragma unroll
+      for (int t = 0; t < IPL; ++t) {
+        T[j * Cfg::TSTRIDE + t * 32 + lane] = acc[t];
+        acc[t] = 0.0;
+      }
+      ++j;
+    };
+    auto consume = [&](int32_t rr, double ae, const KV& kv) {
+      while (rr >= cur_end) {  // the current slot is complete
+        flush();
+        cur_end = __shfl_sync(kFull, my_end, j);
+      }
+#pragma unroll
+      for (int t = 0; t < IPL; ++t) acc[t] = fma(ae, KVec<IPL>::at(kv, t), acc[t]);
+    };
+    for (int32_t base = R0; base < R1; base += 32) {
+      const int cnt = min(32, R1 - base);
+      __syncwarp();
+      if (lane < cnt) R[lane] = a.rec[base + lane];
+      __syncwarp();
+      int q0 = 0;
+      for (; q0 + kLoadBatch <= cnt; q0 += kLoadBatch) {
+        KV kv[kLoadBatch];
+#pragma unroll
+        for (int u = 0; u < kLoadBatch; ++u) kv[u] = __ldg(kb + (int64_t)R[q0 + u].cell * ldv);
+#pragma unroll
+        for (int u = 0; u < kLoadBatch; ++u) consume(base + q0 + u, R[q0 + u].ae, kv[u]);
+      }
+      if (q0 < cnt) {
+        KV kv[kLoadBatch];
+#pragma unroll
+        for (int u = 0; u < kLoadBatch; ++u)
+          if (q0 + u < cnt) kv[u] = __ldg(kb + (int64_t)R[q0 + u].cell * ldv);
+#pragma unroll
+        for (int u = 0; u < kLoadBatch; ++u)
+          if (q0 + u < cnt) consume(base + q0 + u, R[q0 + u].ae, kv[u]);
+      }
+    }
+    while (j < ns) flush();  // the last slot (and any slot without records)
+    __syncwarp();
+    // store: lane = pair of consecutive slots (2p, 2p+1) of the item for one
+    // instance; kSub lane groups take successive instances, so one store
+    // instruction writes kSub instances' kSlotsPerItem consecutive values
+    constexpr int kPairs = kSlotsPerItem / 2;
+    constexpr int kSub = 32 / kPairs;
+    const int p = lane % kPairs, sub = lane / kPairs;
+    const int sa = 2 * p;
+    if (sa < ns) {
+      const int64_t slot = s0 + sa;
+      const bool two = sa + 1 < ns;
+      bool mask[2] = {false, false}, diag[2] = {false, false};
+      if (a.bc0 || a.bc1) {
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          if (h == 0 || two) {
+            const int32_t row = __ldg(a.slot_row + slot + h), cl = __ldg(a.col + slot + h);
+            const bool rm = a.bc0 && a.bc0[row];
+            mask[h] = rm || (a.bc1 && a.bc1[cl]);
+            diag[h] = rm && row == cl;
+          }
         }
       }
-#pragma unroll
-      for (int t = 0; t < IPL; ++t) T[j * Cfg::TSTRIDE + lane * IPL + t] = acc[t];
-    }
-    __syncwarp();
-    if (lane < ns) {
-      const int64_t slot = s0 + lane;
-      bool mask = false, diag = false;
-      if (a.bc0 || a.bc1) {
-        const int32_t row = __ldg(a.slot_row + slot), cl = __ldg(a.col + slot);
-        const bool rm = a.bc0 && a.bc0[row];
-        mask = rm || (a.bc1 && a.bc1[cl]);
-        diag = rm && row == cl;
-      }
       const int nin = min(Cfg::CHUNK, a.num_inst - ioff);
-      for (int i = 0; i < nin; ++i) {
+      for (int i = sub; i < nin; i += kSub) {
         double* __restrict__ out = a.values[ioff + i] + slot;
-        double v = a.zero ? 0.0 : *out;
-        if (!mask) v += T[lane * Cfg::TSTRIDE + i];
-        if (diag) v = a.diagonal;
-        *out = v;
+        const int c = (i % IPL) * 32 + i / IPL;
+        double v0 = a.zero ? 0.0 : out[0];
+        double v1 = (a.zero || !two) ? 0.0 : out[1];
+        if (!mask[0]) v0 += T[sa * Cfg::TSTRIDE + c];
+        if (two && !mask[1]) v1 += T[(sa + 1) * Cfg::TSTRIDE + c];
+        if (diag[0]) v0 = a.diagonal;
+        if (diag[1]) v1 = a.diagonal;
+        if (two && ((reinterpret_cast<uintptr_t>(out) & 15) == 0)) {
+          *reinterpret_cast<double2*>(out) = make_double2(v0, v1);
+        } else {
+          out[0] = v0;
+          if (two) out[1] = v1;
+        }
       }
     }
     __syncwarp();
@@ -328,7 +426,7 @@ void assemble_matrix_batch(fe_form_s& f, int num_instances, const double* const*
   }
   auto& B = *f.batch;
   // packed coefficients: one row of ld floats per cell, resized on demand
-  const int ipl = num_instances > 32 ? 2 : 1;
+  const int ipl = num_instances > 64 ? 4 : (num_instances > 32 ? 2 : 1);
   const int chunk = 32 * ipl;
   const int64_t ld = ((int64_t)num_instances + chunk - 1) / chunk * chunk;
   if (B.kp_ld != ld || !B.kp.p) {
@@ -355,7 +453,7 @@ void assemble_matrix_batch(fe_form_s& f, int num_instances, const double* const*
     else k_batch_elem_p2<<<nblocks(C, 128), 128, 0, s>>>(ea);
     FE_CUDA(cudaGetLastError());
     k_batch_fill<<<nblocks(B.num_records, 256), 256, 0, s>>>(B.rec_cell.p, B.rec_entry.p, B.num_records, KK, B.E.p,
-                                                             B.rec.p);
+                                                             reinterpret_cast<BatchRec*>(B.rec.p));
     FE_CUDA(cudaGetLastError());
   }
   if (!nnz) return;
@@ -367,8 +465,9 @@ void assemble_matrix_batch(fe_form_s& f, int num_instances, const double* const*
     ga.ld = ld;
     ga.num_chunks = (ga.num_inst + chunk - 1) / chunk;
     ga.num_items = ((nnz + kSlotsPerItem - 1) / kSlotsPerItem) * ga.num_chunks;
+    FE_REQUIRE(ga.num_items < INT32_MAX, "batch too large for one gather launch");
     ga.seg = f.gather->seg.p;
-    ga.rec = B.rec.p;
+    ga.rec = reinterpret_cast<const BatchRec*>(B.rec.p);
     ga.kp = B.kp.p;
     ga.slot_row = B.slot_row.p;
     ga.col = f.sp->col.p;
@@ -377,7 +476,8 @@ void assemble_matrix_batch(fe_form_s& f, int num_instances, const double* const*
     ga.diagonal = diagonal;
     ga.zero = zero ? 1 : 0;
     for (int i = 0; i < ga.num_inst; ++i) ga.values[i] = values[i0 + i];
-    if (ipl == 2) launch_gather<2>(ga, f.ctx->num_sms, s);
+    if (ipl == 4) launch_gather<4>(ga, f.ctx->num_sms, s);
+    else if (ipl == 2) launch_gather<2>(ga, f.ctx->num_sms, s);
     else launch_gather<1>(ga, f.ctx->num_sms, s);
   }
 }

@@ -59,7 +59,7 @@ def _setup(kind, n):
     return P, M, a, asm, bcs, torch
 
 
-@pytest.mark.parametrize("kind,n,S", [("p1", 4, 5), ("p1", 6, 40), ("p2", 3, 7), ("p2", 4, 33)])
+@pytest.mark.parametrize("kind,n,S", [("p1", 4, 5), ("p1", 6, 40), ("p2", 3, 7), ("p2", 4, 33), ("p2", 3, 70)])
 def test_batch_matches_oracle(kind, n, S):
     P, M, a, asm, bcs, torch = _setup(kind, n)
     ks = _instances(P, S, seed=11)
@@ -123,7 +123,7 @@ def test_batch_more_instances_than_one_launch():
     kd = torch.tensor(np.stack(ks), device="cuda")
     mats = asm.assemble_matrix_batch(a, kd, bcs=bcs)
     torch.cuda.synchronize()
-    for i in (0, 63, 64, 447, 448, 449):
+    for i in (0, 63, 64, 127, 128, 383, 384, 449):
         _, _, ref = _oracle_matrix(P, ks[i])
         _check(mats[i].values.cpu().numpy(), ref)
 
