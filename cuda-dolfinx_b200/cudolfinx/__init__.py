@@ -7,10 +7,11 @@ the host-side stand-ins for the DOLFINx objects those calls consume.
 """
 from . import _lib, fem
 from .assemble import CUDAAssembler
+from .batch import AssemblyGraph, VariantTuner
 from .bcs import CUDADirichletBC
 from .context import get_cuda_context
 from .form import CUDAForm, form
 from .la import CUDAMatrix, CUDAVector, Sparsity
 
-__all__ = ["CUDAAssembler", "CUDADirichletBC", "CUDAForm", "CUDAMatrix", "CUDAVector", "Sparsity", "fem", "form",
-           "get_cuda_context"]
+__all__ = ["AssemblyGraph", "CUDAAssembler", "CUDADirichletBC", "CUDAForm", "CUDAMatrix", "CUDAVector", "Sparsity", "fem", "form",
+           "get_cuda_context", "VariantTuner"]

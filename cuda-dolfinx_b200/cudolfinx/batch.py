@@ -1,0 +1,134 @@
+"""Many independent assemblies in one CUDA graph, with a variant autotuner.
+
+No counterpart in the reference, which launches one assembly per Python call
+with a context synchronisation after every kernel (cpp/cudolfinx/fem/
+CUDAFormIntegral.cpp:2354-2361).  Here a list of (form, matrix, BCs) items --
+meshes of different sizes, P1 and P2 forms mixed -- is assembled through the
+C-ABI on one stream, captured once into a CUDA graph and replayed with a
+single launch call.  ``VariantTuner`` times the matrix variants that apply to
+each (form kind, precision, size class) on the device and keeps the fastest;
+the graph is captured with the chosen variant per item.
+"""
+from __future__ import annotations
+
+import math
+import typing
+
+import torch
+
+from . import _lib
+from .bcs import CUDADirichletBC
+from .context import get_cuda_context
+from .form import CUDAForm
+from .la import CUDAMatrix
+
+# matrix variants worth timing per form kind (all parity-tested)
+CANDIDATES = {
+    "P1_STIFFNESS": ("atomic", "block", "tile"),
+    "P2_STIFFNESS": ("atomic", "block"),
+    "VP2_ELASTICITY": ("atomic", "sorted-slot"),
+}
+
+
+class VariantTuner:
+    """Chooses the fastest matrix variant per (form kind, precision, size
+    class); size classes are powers of two of the cell count."""
+
+    def __init__(self, reps: int = 3):
+        self.reps = reps
+        self.cache: dict = {}
+        self.timings: dict = {}
+
+    @staticmethod
+    def key(a: CUDAForm) -> tuple:
+        C = a._spec.mesh.num_cells
+        return (a._spec.kind, a._spec.precision, int(math.log2(max(1, C))))
+
+    def choose(self, a: CUDAForm, mat: CUDAMatrix, bc0, bc1) -> str:
+        k = self.key(a)
+        if k in self.cache:
+            return self.cache[k]
+        stream = torch.cuda.current_stream()
+        sp = stream.cuda_stream
+        best, best_ms, times = None, float("inf"), {}
+        for v in CANDIDATES.get(a._spec.kind, ("atomic",)):
+            flags = _lib.ASM_ZERO | _lib.VARIANT_FLAGS[v]
+
+            def call():
+                _lib.check(_lib.lib.fe_assemble_matrix(a.cuda_form, mat.values.data_ptr(), bc0, bc1, 1.0, flags, sp),
+                           "fe_assemble_matrix")
+
+            call()  # plan build
+            call()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(self.reps):
+                call()
+            e1.record(stream)
+            e1.synchronize()
+            ms = e0.elapsed_time(e1) / self.reps
+            times[v] = ms
+            if ms < best_ms:
+                best, best_ms = v, ms
+        self.cache[k] = best
+        self.timings[k] = times
+        return best
+
+
+class AssemblyGraph:
+    """Matrix assemblies of many (form, matrix, BCs) items captured into one
+    CUDA graph.  ``variants``: "auto" (engine default per item), "tune" (a
+    VariantTuner picks per item) or one variant name for every item."""
+
+    def __init__(self, items: typing.Sequence[tuple], variants: str = "tune",
+                 tuner: typing.Optional[VariantTuner] = None):
+        self._ctx = get_cuda_context()
+        self.items = []
+        for a, mat, bcs in items:
+            if not isinstance(a, CUDAForm) or a.rank != 2:
+                raise TypeError("items must hold bilinear CUDAForms")
+            a._bind(mat.sparsity)
+            col = bcs if isinstance(bcs, CUDADirichletBC) or bcs is None else CUDADirichletBC(self._ctx, list(bcs))
+            bc0 = col._get_cpp_bcs(a.function_spaces[0]) if col else None
+            bc1 = col._get_cpp_bcs(a.function_spaces[1]) if col else None
+            self.items.append({"a": a, "mat": mat, "col": col, "bc0": bc0.handle if bc0 else None,
+                               "bc1": bc1.handle if bc1 else None})
+        self.tuner = tuner or VariantTuner()
+        for it in self.items:
+            if variants == "tune":
+                it["variant"] = self.tuner.choose(it["a"], it["mat"], it["bc0"], it["bc1"])
+            else:
+                it["variant"] = variants
+        self.graph = None
+        self._stream = None
+
+    def _launch_all(self, sp):
+        for it in self.items:
+            flags = _lib.ASM_ZERO | _lib.VARIANT_FLAGS[it["variant"]]
+            _lib.check(_lib.lib.fe_assemble_matrix(it["a"].cuda_form, it["mat"].values.data_ptr(), it["bc0"],
+                                                   it["bc1"], 1.0, flags, sp), "fe_assemble_matrix")
+
+    def run_eager(self):
+        """The same launches without the graph (one C-ABI call per item)."""
+        self._launch_all(torch.cuda.current_stream().cuda_stream)
+
+    def capture(self):
+        # plans and caches are built outside the capture
+        self.run_eager()
+        torch.cuda.synchronize()
+        self.graph = torch.cuda.CUDAGraph()
+        self._stream = torch.cuda.Stream()
+        with torch.cuda.graph(self.graph, stream=self._stream):
+            self._launch_all(torch.cuda.current_stream().cuda_stream)
+        torch.cuda.synchronize()
+        return self
+
+    def replay(self):
+        if self.graph is None:
+            raise RuntimeError("capture() first")
+        self.graph.replay()
+
+    @property
+    def nnz(self) -> int:
+        return sum(it["mat"].sparsity.nnz for it in self.items)
