@@ -69,6 +69,11 @@ MULTI = dict(count=64, nmin=8, nmax=64, cpu_every=8,
              desc="64 unit-cube tet meshes, n^3 x 6 cells with n ~ U{8..64} (seeded), P1 (k=1) and P2 (k P1 "
                   "lognormal) 50/50, Dirichlet on the boundary; P2 element tensors FP32, P1 FP64, FP64 "
                   "accumulation; all matrix assemblies in one CUDA graph, variant per item from the autotuner")
+# serving: assemble-and-solve requests with Poisson arrivals
+SERVE = dict(requests=120, rates=(50.0, 200.0, 1000.0), nmin=8, nmax=48, workers=4, budget_gb=60,
+             desc="assemble + Jacobi-PCG (rtol 1e-8) requests with Poisson arrivals; 35% P1 / 35% P2 Poisson "
+                  "(k DG0 lognormal, f=1, g=x+y+z), 30% vector-P2 elasticity (lam, mu DG0 lognormal, body force "
+                  "(0,0,-1), u=0); unit-cube meshes n^3 x 6 tets, n log-uniform")
 # kernels of one step besides the matrix call: zero b, vector, lifting, set_bc
 VECTOR_KERNELS = 4
 
@@ -810,7 +815,156 @@ def run_reference_multimesh(args):
             "e2e": {"value": v, "unit": "nnz/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+def serve_request_bytes(kind, n, iterations):
+    """HBM bytes one request must move: its matrix assembly (values written,
+    slot map, dofmap, geometry, coordinates, coefficients), b, and per PCG
+    iteration one SpMV (values, columns, row pointers, p, Ap) plus the
+    vector updates (x, r, z, p, Ap, dinv)."""
+    from cudolfinx import serve
+
+    sz = serve.problem_sizes(kind, n)
+    C, N, nnz, k = sz["cells"], sz["rows"], sz["nnz"], sz["k"]
+    asm = 8 * nnz + k * k * C + 4 * k * C + 16 * C + 24 * sz["vertices"] + 8 * C * (2 if kind == "vp2" else 1)
+    vec = 8 * N + 4 * k * C + 16 * C
+    per_it = 12 * nnz + 4 * N + 16 * N + 8 * 10 * N
+    return asm + vec + iterations * per_it
+
+
+def serve_launches(iterations):
+    # matrix (zero, kernel, diagonal) + vector (zero, kernel, lifting, set_bc) + PCG (2 + 80 per 16 iterations)
+    return 3 + 4 + 2 + 80 * ((iterations + 16) // 16)
+
+
+def run_gpu_serve(args, rank, world, local_rank):
+    import torch
+
+    from cudolfinx import serve
+
+    torch.cuda.set_device(local_rank)
+    count = args.serve_requests or SERVE["requests"]
+    rates = [float(r) for r in (args.serve_rates.split(",") if args.serve_rates else SERVE["rates"])]
+    nmax = args.serve_nmax or SERVE["nmax"]
+    seed = args.seed + 7919 * rank
+    t_setup = time.perf_counter()
+    base = serve.make_requests(count, rates[0], seed=seed, nmin=SERVE["nmin"], nmax=nmax)
+    srv = serve.Server(workers=SERVE["workers"], hbm_budget=SERVE["budget_gb"] << 30, precision="fp32")
+    keys = sorted({r.key for r in base})
+    srv.warm(keys)
+    setup_s = time.perf_counter() - t_setup
+    # warm-up: a few requests through the running server
+    srv.run(serve.make_requests(4, 0.0, seed=seed + 1, nmin=SERVE["nmin"], nmax=min(nmax, 16)))
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    per_rate = []
+    served_results = None
+    for rate in rates:
+        reqs = serve.make_requests(count, rate, seed=seed, nmin=SERVE["nmin"], nmax=nmax)
+        res = srv.run(reqs)
+        summ = serve.summarize(res)
+        summ["rate_rps"] = rate
+        per_rate.append(summ)
+        served_results = res
+    clk = clocks.stop()
+    # plain path: one request at a time, FP64, nothing cached, same requests at the lowest rate
+    plain_res = serve.Server(plain=True).run(serve.make_requests(count, rates[0], seed=seed, nmin=SERVE["nmin"],
+                                                                 nmax=nmax))
+    plain = serve.summarize(plain_res)
+    plain["rate_rps"] = rates[0]
+    diffs = [serve.solution_difference(a, b) for a, b in zip(served_results, plain_res)]
+    top = per_rate[-1]
+    alg = sum(serve_request_bytes(r.kind, r.n, r.iterations) for r in served_results if r.error is None)
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            peaks = json.load(fh)
+    except (OSError, ValueError):
+        pass
+    peak = peaks.get("hbm_gbs", 6650.0)
+    achieved = alg / top["makespan_s"] / 1e9
+    value = top["throughput_rps"]
+    if world > 1:
+        t = torch.tensor([value], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MIN)
+        value = float(t[0]) * world
+    out = {
+        "metric": "served assemble+solve requests/s (p50/p99 latency beside)",
+        "value": value, "unit": "req/s", "n_gpus": world, "steps": count, "warmup": 4,
+        "ms_per_step": 1e3 / top["throughput_rps"] if top["throughput_rps"] else None,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32-element(P2, vP2)/f64-accumulate, f64 PCG",
+        "data": "synthetic (seeded request stream)",
+        "config": {"workload": SERVE["desc"] + f" in [{SERVE['nmin']}, {nmax}] (bounded sample of the "
+                   f"10,000-request stream: {count} requests per rate)", "requests": count, "rates_rps": rates,
+                   "workers": SERVE["workers"], "hbm_budget_gb": SERVE["budget_gb"],
+                   "cache": f"warm: one slot per (family, n) of the stream built before the timed runs "
+                            f"({len(keys)} sizes)",
+                   "step": "one request: H2D coefficients, assemble A and b (lifting, set_bc), PCG, D2H x",
+                   "parallelism": f"replicas x{world}"},
+        "latency": {"per_rate": per_rate, "p50_ms": top["p50_ms"], "p99_ms": top["p99_ms"]},
+        "plain_fp64": {**plain, "path": "one request at a time, FP64 element tensors, mesh/pattern/forms built "
+                                        "per request", "speedup_of_served": (top["throughput_rps"] /
+                                                                             plain["throughput_rps"])
+                       if plain["throughput_rps"] else None},
+        "precision": {"max_rel_solution_diff_vs_fp64": max(diffs) if diffs else None,
+                      "median_rel_solution_diff_vs_fp64": float(np.median(diffs)) if diffs else None},
+        "roofline": {"bound": "hbm", "kernel": "served request mix (assembly + PCG)", "achieved": achieved,
+                     "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                     "algorithmic_bytes": alg, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"
+                     if "hbm_gbs" in peaks else "fallback 6650 GB/s"},
+        "gpu_launches": sum(serve_launches(r.iterations) for r in served_results if r.error is None),
+        "e2e": {"value": top["throughput_rps"], "unit": "req/s",
+                "h2d_bytes_per_step": int(np.mean([8 * sum(c.size for c in r.coef) for r in base])),
+                "d2h_bytes_per_step": int(np.mean([8 * serve.problem_sizes(r.kind, r.n)["rows"] for r in base])),
+                "note": "every request is end to end: host coefficients in, solution out"},
+        "clocks": clk, "setup_s": setup_s, "max_concurrent": srv.max_concurrent,
+        "ledger_peak_gb": srv.ledger.peak / 2 ** 30,
+    }
+    return out
+
+
+def run_reference_serve(args):
+    """C port of the reference CPU path on a bounded sample of the request
+    stream: assembly only (the reference hands the system to PETSc KSP, which
+    is not part of this build), one request at a time."""
+    from oracle import cfem
+    from cudolfinx import serve
+
+    count = min(args.serve_requests or SERVE["requests"], 24)
+    nmax = args.serve_nmax or SERVE["nmax"]
+    reqs = serve.make_requests(count, 0.0, seed=args.seed, nmin=SERVE["nmin"], nmax=nmax)
+    threads = os.cpu_count() or 1
+    t_all = 0.0
+    for r in reqs:
+        kind = {"p1": "p1", "p2": "p2", "vp2": "vp2"}[r.kind]
+        I = make_inputs(kind, r.n, seed=args.seed)
+        rp, cl = host_pattern(I)
+        P = oracle_problem(I)
+        if kind == "vp2":
+            P["lam"], P["mu"] = r.coef
+        elif kind == "p1":
+            P["kind"] = "p1k"
+            P["k"] = r.coef[0]
+        Cq = cfem.CpuAssembler(P, rp, cl, nthreads=threads)
+        t0 = time.perf_counter()
+        Cq.assemble_matrix()
+        Cq.assemble_rhs()
+        t_all += time.perf_counter() - t0
+        Cq.close()
+    v = count / t_all
+    return {"impl": "reference", "metric": "served assemble+solve requests/s (p50/p99 latency beside)", "value": v,
+            "unit": "req/s", "n_gpus": 1, "steps": count, "warmup": 0, "ms_per_step": 1e3 * t_all / count,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded request stream)",
+            "config": {"workload": SERVE["desc"], "requests_timed": count,
+                       "step": "assembly of A and b (lifting, set_bc) per request; solve not included"},
+            "cpu_baseline": {"value": v, "unit": "req/s", "cores": threads, "kind": "port",
+                             "sample": f"{count} requests, assembly only, C port of the reference CPU path"},
+            "e2e": {"value": v, "unit": "req/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
 def run_reference(args):
+    if args.workload == "serve":
+        return run_reference_serve(args)
     if args.workload == "batch":
         return run_reference_batch(args)
     if args.workload == "multimesh":
@@ -885,10 +1039,13 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batch", "multimesh"], default="p2")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batch", "multimesh", "serve"], default="p2")
     ap.add_argument("--variant", choices=["auto", "tile", "atomic", "sorted-slot", "deterministic", "row-gather",
                                           "block"], default="auto")
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--serve-requests", type=int, default=0, help="serve workload: requests per rate")
+    ap.add_argument("--serve-rates", default="", help="serve workload: comma-separated arrival rates (req/s)")
+    ap.add_argument("--serve-nmax", type=int, default=0, help="serve workload: largest n (default 48)")
     ap.add_argument("--instances", type=int, default=0,
                     help="batch workload: number of instances (default 256; smaller for profiling)")
     ap.add_argument("--no-e2e", action="store_true")
@@ -911,7 +1068,8 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local_rank))
     try:
-        runner = {"batch": run_gpu_batch, "multimesh": run_gpu_multimesh}.get(args.workload, run_gpu)
+        runner = {"batch": run_gpu_batch, "multimesh": run_gpu_multimesh,
+                  "serve": run_gpu_serve}.get(args.workload, run_gpu)
         out = runner(args, rank, world, local_rank)
         if rank == 0:
             print(json.dumps(out), flush=True)

@@ -13,5 +13,17 @@ from .context import get_cuda_context
 from .form import CUDAForm, form
 from .la import CUDAMatrix, CUDAVector, Sparsity
 
+
+
+def release_caches(mesh=None):
+    """Drop the module-level device caches (meshes, dofmaps, CSR patterns):
+    all of them, or those of `mesh`.  Long-running processes that create many
+    meshes call this to return device memory."""
+    from .assemble import release_sparsity_cache
+    from .form import release_device_caches
+    release_sparsity_cache(mesh)
+    release_device_caches(mesh)
+
+
 __all__ = ["AssemblyGraph", "CUDAAssembler", "CUDADirichletBC", "CUDAForm", "CUDAMatrix", "CUDAVector", "Sparsity", "fem", "form",
-           "get_cuda_context", "VariantTuner"]
+           "get_cuda_context", "release_caches", "VariantTuner"]

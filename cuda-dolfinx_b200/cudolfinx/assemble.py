@@ -30,6 +30,13 @@ from .la import CUDAMatrix, CUDAVector, Sparsity
 _sparsity_cache: dict = {}
 
 
+def release_sparsity_cache(mesh=None):
+    """Drop cached CSR patterns: all, or those built on `mesh`."""
+    for k, e in list(_sparsity_cache.items()):
+        if mesh is None or e[0].V.mesh is mesh:
+            _sparsity_cache.pop(k, None)
+
+
 class CUDAAssembler:
     """Class for assembly on the GPU."""
 

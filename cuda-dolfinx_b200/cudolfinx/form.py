@@ -64,6 +64,17 @@ def _create_mesh_on_device(ctx, mesh) -> DeviceMesh:
     return m
 
 
+def release_device_caches(mesh=None):
+    """Drop cached device meshes and dofmaps: all of them, or those of `mesh`.
+    Objects still referenced by live forms stay alive through those forms."""
+    for k, m in list(_mesh_cache.items()):
+        if mesh is None or m.mesh is mesh:
+            _mesh_cache.pop(k, None)
+    for k, d in list(_dofmap_cache.items()):
+        if mesh is None or d.V.mesh is mesh:
+            _dofmap_cache.pop(k, None)
+
+
 def device_dofmap(ctx, V: FunctionSpace) -> DeviceDofMap:
     d = _dofmap_cache.get(id(V))
     if d is None or d.V is not V:
