@@ -9,8 +9,10 @@
 // matrix of the unit coefficient, so
 //     A_s[slot] = sum over the slot's element entries (c, e) of k_s(c) * A_c[e].
 // The batch computes A_c once per call, in FP32 (geometry, Jacobian,
-// determinant and inverse in FP64), and then forms every instance's values
-// with FP64 accumulation in one persistent launch:
+// determinant and inverse in FP64; each diagonal entry is minus the FP64 sum
+// of its row's FP32 off-diagonal entries, so element rows sum to zero as the
+// exact ones do), and then forms every instance's values with FP64
+// accumulation in one persistent launch:
 //   k_batch_pack    k_s(c) (FP64, one array per instance) -> kp[c][s] (FP32),
 //                   a tiled transpose (the batch's pack_coefficients)
 //   k_batch_elem_*  unit-coefficient element tensors E[c][i*K+j]
@@ -105,7 +107,7 @@ struct ElemArgs {
   int64_t num_cells;
   const double* __restrict__ x;
   const int32_t* __restrict__ geom;
-  float* __restrict__ E;
+  double* __restrict__ E;
 };
 
 struct Geo {
@@ -152,18 +154,26 @@ __global__ void k_batch_elem_p1(const ElemArgs a) {
     G[3][b] = g.K[2][b];
     G[0][b] = -(g.K[0][b] + g.K[1][b] + g.K[2][b]);
   }
+  // FP32 off-diagonal entries; each diagonal entry is minus the FP64 sum of
+  // its row's off-diagonal entries, so every element row sums to zero exactly
   const double s = g.adet * (1.0 / 6.0);
-  float v[16];
+  double v[16];
+  double rs[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
-    for (int j = i; j < 4; ++j) {
-      v[i * 4 + j] = (float)(s * (G[i][0] * G[j][0] + G[i][1] * G[j][1] + G[i][2] * G[j][2]));
-      v[j * 4 + i] = v[i * 4 + j];
+    for (int j = i + 1; j < 4; ++j) {
+      const double e = (double)(float)(s * (G[i][0] * G[j][0] + G[i][1] * G[j][1] + G[i][2] * G[j][2]));
+      v[i * 4 + j] = e;
+      v[j * 4 + i] = e;
+      rs[i] += e;
+      rs[j] += e;
     }
-  float4* out = reinterpret_cast<float4*>(a.E + c * 16);
 #pragma unroll
-  for (int q = 0; q < 4; ++q) out[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+  for (int i = 0; i < 4; ++i) v[i * 5] = -rs[i];
+  double2* out = reinterpret_cast<double2*>(a.E + c * 16);
+#pragma unroll
+  for (int q = 0; q < 8; ++q) out[q] = make_double2(v[2 * q], v[2 * q + 1]);
 }
 
 __global__ void k_batch_elem_p2(const ElemArgs a) {
@@ -177,19 +187,19 @@ __global__ void k_batch_elem_p2(const ElemArgs a) {
   for (int s = 0; s < 6; ++s)
     gq[s] = (float)(g.adet * (g.K[pa[s]][0] * g.K[pb[s]][0] + g.K[pa[s]][1] * g.K[pb[s]][1] +
                               g.K[pa[s]][2] * g.K[pb[s]][2]));
-  float* __restrict__ E = a.E + c * 100;
-  p2_stiffness_const<float>(gq, [&](int i, int j, float v) {
+  double* __restrict__ E = a.E + c * 100;
+  p2_stiffness_const<float>(gq, [&](int i, int j, double v) {
     E[i * 10 + j] = v;
     if (i != j) E[j * 10 + i] = v;
   });
 }
 
 __global__ void k_batch_fill(const int32_t* __restrict__ rec_cell, const uint8_t* __restrict__ rec_entry,
-                             int64_t nrec, int KK, const float* __restrict__ E, BatchRec* __restrict__ rec) {
+                             int64_t nrec, int KK, const double* __restrict__ E, BatchRec* __restrict__ rec) {
   const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (r >= nrec) return;
   const int32_t c = rec_cell[r];
-  rec[r] = BatchRec{(double)__ldg(E + (int64_t)c * KK + rec_entry[r]), c, 0};
+  rec[r] = BatchRec{__ldg(E + (int64_t)c * KK + rec_entry[r]), c, 0};
 }
 
 // ---- persistent gather ---------------------------------------------------

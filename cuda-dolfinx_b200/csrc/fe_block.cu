@@ -138,7 +138,7 @@ __device__ __forceinline__ void cell_entries(const BlockArgs& a, int64_t cb, Emi
 #pragma unroll
     for (int s = 0; s < 6; ++s)
       Gh[s] = adet * (Km[pa[s]][0] * Km[pb[s]][0] + Km[pa[s]][1] * Km[pb[s]][1] + Km[pa[s]][2] * Km[pb[s]][2]);
-    auto emitT = [&](int i, int j, T v) { emit(i, j, (double)v); };
+    auto emitT = [&](int i, int j, double v) { emit(i, j, v); };
     if (a.coef_kind == FE_COEFF_P1) {
       const int4 km = __ldg(a.coef_map + cb);
       const double kv[4] = {__ldg(a.coef + km.x), __ldg(a.coef + km.y), __ldg(a.coef + km.z), __ldg(a.coef + km.w)};

@@ -241,8 +241,7 @@ __global__ void k_elem_p2(const ElemArgs a) {
     Gh[s] = g.adet * (g.K[pa[s]][0] * g.K[pb[s]][0] + g.K[pa[s]][1] * g.K[pb[s]][1] + g.K[pa[s]][2] * g.K[pb[s]][2]);
   const int64_t N = a.num_cells;
   double* __restrict__ E = a.E;
-  auto emit = [&](int i, int j, T vt) {
-    const double v = (double)vt;
+  auto emit = [&](int i, int j, double v) {
     E[(i * 10 + j) * N + c] = v;
     if (i != j) E[(j * 10 + i) * N + c] = v;
   };
@@ -287,8 +286,7 @@ __global__ void k_elem_vp2(const ElemArgs a) {
         if (ca == cb) kk = g.K[p][0] * g.K[q][0] + g.K[p][1] * g.K[q][1] + g.K[p][2] * g.K[q][2];
         W[p * 3 + q] = (T)(g.adet * (mu * (kk + g.K[p][cb] * g.K[q][ca]) + lam * g.K[p][ca] * g.K[q][cb]));
       }
-    auto emit = [&](int i, int j, T vt) {
-      const double v = (double)vt;
+    auto emit = [&](int i, int j, double v) {
       const int ii = 3 * i + ca, jj = 3 * j + cb;
       E[(ii * 30 + jj) * N + c] = v;
       if (ii != jj) E[(jj * 30 + ii) * N + c] = v;

@@ -215,7 +215,7 @@ struct fe_form_s::BatchPlan {
   fe::DevBuf<int32_t> rec_cell;       // [records] cell of each slot-sorted record
   fe::DevBuf<uint8_t> rec_entry;      // [records] local entry i*K+j of each record
   fe::DevBuf<int32_t> slot_row;       // [nnz] CSR row of each slot
-  fe::DevBuf<float> E;                // [cells][KK] unit-coefficient element tensors (FP32)
+  fe::DevBuf<double> E;               // [cells][KK] unit-coefficient element tensors (FP32 values)
   fe::DevBuf<double2> rec;            // [records] {entry value, cell}, refreshed per call (16 B each)
   fe::DevBuf<float> kp;               // [cells][ld] packed instance coefficients (FP32)
   int64_t kp_ld = 0;

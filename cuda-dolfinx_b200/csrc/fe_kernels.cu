@@ -204,8 +204,7 @@ __global__ void __launch_bounds__(kBlock) k_mat_p2_atomic(const MatArgs a) {
     if (a.bc1) mc |= (__ldg(a.bc1 + __ldg(d1 + i)) ? 1u : 0u) << i;
   }
   double* __restrict__ vals = a.values;
-  auto emit = [&](int i, int j, T vt) {
-    const double v = (double)vt;
+  auto emit = [&](int i, int j, double v) {
     if (!(((mr >> i) | (mc >> j)) & 1u)) atomicAdd(vals + rp[i] + p[i * 10 + j], v);
     if (i != j && !(((mr >> j) | (mc >> i)) & 1u)) atomicAdd(vals + rp[j] + p[j * 10 + i], v);
   };
@@ -254,7 +253,7 @@ __device__ __forceinline__ void elasticity_blocks(const CellGeo& g, double lam, 
     const int b = blk < 3 ? blk : (blk == 3 ? 1 : 2);
     T W[9];
     elasticity_weights<T>(g, lam, mu, a, b, W);
-    auto emit = [&](int i, int j, T v) { emit_ab(a, b, i, j, v); };
+    auto emit = [&](int i, int j, double v) { emit_ab(a, b, i, j, v); };
     if (a == b)
       p2_block_upper<T>(W, emit);
     else
@@ -295,8 +294,7 @@ __global__ void __launch_bounds__(kBlock) k_mat_vp2_atomic(const MatArgs a) {
     }
   }
   double* __restrict__ vals = a.values;
-  elasticity_blocks<T>(g, lam, mu, [&](int ca, int cb, int i, int j, T vt) {
-    const double v = (double)vt;
+  elasticity_blocks<T>(g, lam, mu, [&](int ca, int cb, int i, int j, double v) {
     if (!(((mr >> (3 * i + ca)) | (mc >> (3 * j + cb))) & 1u))
       atomicAdd(vals + rp[i] + ca * L[i] + 3 * p[i * 10 + j] + cb, v);
     if (!(ca == cb && i == j) && !(((mr >> (3 * j + cb)) | (mc >> (3 * i + ca))) & 1u))
@@ -510,8 +508,7 @@ __global__ void __launch_bounds__(kBlock) k_lift_p2(const LiftArgs a) {
     dv[j] = __ldg(a.bc1 + C) ? (__ldg(a.g + C) - (a.x0 ? __ldg(a.x0 + C) : 0.0)) : 0.0;
     be[j] = 0.0;
   }
-  auto emit = [&](int i, int j, T vt) {
-    const double v = (double)vt;
+  auto emit = [&](int i, int j, double v) {
     be[i] += v * dv[j];
     if (i != j) be[j] += v * dv[i];
   };
@@ -557,8 +554,7 @@ __global__ void __launch_bounds__(kBlock) k_lift_vp2(const LiftArgs a) {
       be[3 * j + q] = 0.0;
     }
   }
-  elasticity_blocks<T>(g, lam, mu, [&](int ca, int cb, int i, int j, T vt) {
-    const double v = (double)vt;
+  elasticity_blocks<T>(g, lam, mu, [&](int ca, int cb, int i, int j, double v) {
     be[3 * i + ca] += v * dv[3 * j + cb];
     if (!(ca == cb && i == j)) be[3 * j + cb] += v * dv[3 * i + ca];
   });

@@ -166,7 +166,7 @@ __device__ __forceinline__ void element_tensor_emit(const TileArgs& a, int64_t c
     for (int s = 0; s < 6; ++s)
       Gh[s] = g.adet * (g.K[pa[s]][0] * g.K[pb[s]][0] + g.K[pa[s]][1] * g.K[pb[s]][1] +
                         g.K[pa[s]][2] * g.K[pb[s]][2]);
-    auto emitT = [&](int i, int j, T v) { emit(i, j, (double)v); };
+    auto emitT = [&](int i, int j, double v) { emit(i, j, v); };
     if (a.coef_kind == FE_COEFF_P1) {
       const int4 km = __ldg(reinterpret_cast<const int4*>(a.coef_map) + c);
       const double k[4] = {__ldg(a.coef + km.x), __ldg(a.coef + km.y), __ldg(a.coef + km.z), __ldg(a.coef + km.w)};
@@ -214,8 +214,8 @@ __device__ __forceinline__ void element_tensor(const TileArgs& a, int64_t c, dou
     for (int s = 0; s < 6; ++s)
       Gh[s] = g.adet * (g.K[pa[s]][0] * g.K[pb[s]][0] + g.K[pa[s]][1] * g.K[pb[s]][1] +
                         g.K[pa[s]][2] * g.K[pb[s]][2]);
-    int e = 0;
-    auto emit = [&](int, int, T v) { ae[e++] = (double)v; };
+    // unique entry (i <= j) index, row by row
+    auto emit = [&](int i, int j, double v) { ae[i * 10 - (i * (i - 1)) / 2 + (j - i)] = v; };
     if (a.coef_kind == FE_COEFF_P1) {
       const int4 km = __ldg(reinterpret_cast<const int4*>(a.coef_map) + c);
       const double k[4] = {__ldg(a.coef + km.x), __ldg(a.coef + km.y), __ldg(a.coef + km.z), __ldg(a.coef + km.w)};

@@ -98,6 +98,51 @@ def sum_expr(var, terms, chains=4):
     return parts[0]
 
 
+def symmetric_body(exprs, n):
+    """Body emitting the unique entries i <= j of a symmetric element block.
+
+    FP64: every entry from its expression.  FP32: the off-diagonal entries
+    from their expressions (in T), each diagonal entry as minus the FP64 sum
+    of the row's off-diagonal entries.  The exact block has zero row sums
+    (the basis sums to one), and keeping them exact after FP32 rounding stops
+    the rounding from acting on the smooth, badly conditioned modes: on P2
+    Poisson the solution error of FP32 element tensors drops by about three
+    orders of magnitude at the same matrix error."""
+    out = ["  if constexpr (sizeof(T) == 8) {\n"]
+    for (i, j), e in exprs.items():
+        out.append(f"    emit({i}, {j}, {e});\n")
+    out.append("  } else {\n")
+    out.append(f"    double rs[{n}] = {{{', '.join(['0.0'] * n)}}};\n")
+    for (i, j), e in exprs.items():
+        if i != j:
+            out.append(f"    {{ const T v = {e}; rs[{i}] += (double)v; rs[{j}] += (double)v; emit({i}, {j}, v); }}\n")
+    for i in range(n):
+        out.append(f"    emit({i}, {i}, -rs[{i}]);\n")
+    out.append("  }\n")
+    return "".join(out)
+
+
+def full_body(exprs, n):
+    """Body emitting all entries of a coupling block between two displacement
+    components.  FP32: off-diagonal entries in T, each diagonal entry as minus
+    the mean of the FP64 row and column sums of the off-diagonal entries (the
+    exact block has zero row and column sums; the block's transpose is emitted
+    with the same values, so the mean keeps the element matrix symmetric)."""
+    out = ["  if constexpr (sizeof(T) == 8) {\n"]
+    for (i, j), e in exprs.items():
+        out.append(f"    emit({i}, {j}, {e});\n")
+    out.append("  } else {\n")
+    out.append(f"    double rs[{n}] = {{{', '.join(['0.0'] * n)}}};\n")
+    out.append(f"    double cs[{n}] = {{{', '.join(['0.0'] * n)}}};\n")
+    for (i, j), e in exprs.items():
+        if i != j:
+            out.append(f"    {{ const T v = {e}; rs[{i}] += (double)v; cs[{j}] += (double)v; emit({i}, {j}, v); }}\n")
+    for i in range(n):
+        out.append(f"    emit({i}, {i}, -0.5 * (rs[{i}] + cs[{i}]));\n")
+    out.append("  }\n")
+    return "".join(out)
+
+
 def r_weighted(m, a, b, i, j):
     return pint(pmul(LAM[m], pmul(DPHI[i][a], DPHI[j][b])))
 
@@ -129,11 +174,13 @@ def gen() -> str:
     # P2 stiffness, P1 coefficient: q[m*6+s] = k_m * Ghat_s
     w("// P2 stiffness with a P1 coefficient: q[m*6+s] = k_m * Ghat_s,\n")
     w("// Ghat = |detJ| K K^T (s over (00,11,22,01,02,12)).  Calls emit(i, j, value)\n")
-    w("// for the 55 unique entries i <= j.\n")
+    w("// for the 55 unique entries i <= j (FP32: off-diagonal entries first, then\n")
+    w("// the diagonal entries as minus their rows' FP64 sums; emit takes a double).\n")
     w("template <typename T, typename Emit>\n")
     w("__device__ __forceinline__ void p2_stiffness_p1coef(const T* q, Emit&& emit) {\n")
     nterms = 0
     maxabs_p1coef = Fraction(0)
+    exprs = {}
     for (i, j) in UNIQ:
         terms = []
         for m in range(4):
@@ -143,7 +190,8 @@ def gen() -> str:
                     terms.append((m * 6 + s, c))
                     maxabs_p1coef = max(maxabs_p1coef, abs(c))
         nterms += len(terms)
-        w(f"  emit({i}, {j}, {sum_expr('q', terms)});\n")
+        exprs[(i, j)] = sum_expr('q', terms)
+    w(symmetric_body(exprs, 10))
     w("}\n")
     w(f"// terms: {nterms}\n\n")
 
@@ -152,6 +200,7 @@ def gen() -> str:
     w("template <typename T, typename Emit>\n")
     w("__device__ __forceinline__ void p2_stiffness_const(const T* g, Emit&& emit) {\n")
     maxabs_const = Fraction(0)
+    exprs = {}
     for (i, j) in UNIQ:
         terms = []
         for s in range(6):
@@ -159,7 +208,8 @@ def gen() -> str:
             if c != 0:
                 terms.append((s, c))
                 maxabs_const = max(maxabs_const, abs(c))
-        w(f"  emit({i}, {j}, {sum_expr('g', terms, 2)});\n")
+        exprs[(i, j)] = sum_expr('g', terms, 2)
+    w(symmetric_body(exprs, 10))
     w("}\n\n")
     w("// Largest |coefficient| of the two P2 stiffness bodies: |A_ij| <= max * sum|q| bounds every entry.\n")
     w(f"constexpr double kP2P1CoefTermMax = {lit(maxabs_p1coef)};\n")
@@ -172,6 +222,7 @@ def gen() -> str:
         name = "p2_block_full" if full else "p2_block_upper"
         w("template <typename T, typename Emit>\n")
         w(f"__device__ __forceinline__ void {name}(const T* W, Emit&& emit) {{\n")
+        exprs = {}
         for i in range(10):
             for j in range(10) if full else range(i, 10):
                 terms = []
@@ -180,7 +231,8 @@ def gen() -> str:
                         c = r_plain(p, q, i, j)
                         if c != 0:
                             terms.append((p * 3 + q, c))
-                w(f"  emit({i}, {j}, {sum_expr('W', terms, 2)});\n")
+                exprs[(i, j)] = sum_expr('W', terms, 2)
+        w(full_body(exprs, 10) if full else symmetric_body(exprs, 10))
         w("}\n\n")
     w("}  // namespace fe\n")
     return "".join(out)

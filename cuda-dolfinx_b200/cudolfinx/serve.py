@@ -270,11 +270,11 @@ class _Slot:
         self.V = sh.V
 
 
-def _execute(asm, slot: _Slot, req: Request):
+def _execute(asm, slot: _Slot, req: Request, variant: str = "auto"):
     import torch
     for dev, host in zip(slot.coef, req.coef):
         dev.copy_(torch.from_numpy(np.ascontiguousarray(host, dtype=np.float64)), non_blocking=True)
-    asm.assemble_matrix(slot.a, slot.A, bcs=slot.bcs)
+    asm.assemble_matrix(slot.a, slot.A, bcs=slot.bcs, variant=variant)
     asm.assemble_vector(slot.L, slot.b)
     asm.apply_lifting(slot.b, [slot.a], [slot.bcs])
     asm.set_bc(slot.b, slot.bcs, slot.V)
@@ -290,14 +290,18 @@ class Server:
     ``workers``: concurrent requests on the device (one stream each).
     ``hbm_budget``: bytes the server may hold for slots and shared data.
     ``precision``: element tensors of the P2 and vector-P2 forms ("fp32" or
-    "fp64"; P1 is always FP64).  ``plain=True``: the one-at-a-time FP64 path
-    (one worker, nothing cached)."""
+    "fp64"; P1 is always FP64).  ``variant``: matrix assembly variant
+    ("deterministic" makes every result bitwise independent of what else
+    runs).  ``plain=True``: the one-at-a-time FP64 path (one worker, nothing
+    cached)."""
 
-    def __init__(self, workers: int = 4, hbm_budget: int = 40 << 30, precision: str = "fp32", plain: bool = False):
+    def __init__(self, workers: int = 4, hbm_budget: int = 40 << 30, precision: str = "fp32", plain: bool = False,
+                 variant: str = "auto"):
         import torch
 
         from .assemble import CUDAAssembler
         self.plain = plain
+        self.variant = variant
         self.workers = 1 if plain else int(workers)
         self.precision = "fp64" if plain else precision
         self.ledger = SlotLedger(hbm_budget)
@@ -399,7 +403,7 @@ class Server:
                                 raise
                             with cond:
                                 self.ledger.register(key, slot, nb)
-                        x, its, res = _execute(self._asm, slot, req)
+                        x, its, res = _execute(self._asm, slot, req, self.variant)
                 except Exception as e:  # the request fails, the server goes on
                     x, its, res, err = None, 0, float("nan"), f"{type(e).__name__}: {e}"
                 done = time.perf_counter() - t0
