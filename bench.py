@@ -78,14 +78,16 @@ SERVE = dict(requests=120, rates=(50.0, 200.0, 1000.0), nmin=8, nmax=48, workers
 VECTOR_KERNELS = 4
 
 
-def matrix_kernels(kind: str, variant: str) -> int:
+def matrix_kernels(kind: str, variant: str, big: bool = False) -> int:
     """Kernel launches of one fe_assemble_matrix call (with BCs): 2 for the
     single-pass variants (row gather, tile, ordered tile; + set_diagonal), 3
     for the atomic scatter (zero + scatter + set_diagonal) and the sorted-slot
     reduction (element tensors + gather + set_diagonal)."""
     if variant in ("tile", "row-gather") or (variant == "deterministic" and kind in ("p1", "p2")):
         return 2
-    return 3  # atomic, block (zero + kernel + set_diagonal), sorted-slot
+    if kind == "vp2" and variant in ("atomic", "auto"):
+        return 4  # zero + upper-triangle scatter + lower-triangle mirror + set_diagonal
+    return 3  # atomic-full, block (zero + kernel + set_diagonal), sorted-slot
 
 
 _PINNED: list = []
@@ -448,7 +450,8 @@ def run_gpu(args, rank, world, local_rank):
                      "kernel_ms": mat_ms, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"
                      if "hbm_gbs" in peaks else "fallback 6650 GB/s"},
         "matrix_nnz_per_s": nnz / (mat_ms / 1e3),
-        "gpu_launches": (matrix_kernels(W["kind"], args.variant) + VECTOR_KERNELS) * args.steps,
+        "gpu_launches": (matrix_kernels(W["kind"], args.variant, len(I["cells"]) >= (1 << 20)) + VECTOR_KERNELS)
+        * args.steps,
         "clocks": clk,
         "setup_s": setup_s,
     }
@@ -761,7 +764,7 @@ def run_gpu_multimesh(args, rank, world, local_rank):
         pass
     peak = peaks.get("hbm_gbs", 6650.0)
     achieved = alg / (ms / 1e3) / 1e9
-    launches = sum(matrix_kernels(I["kind"], it["variant"]) for I, it in zip(Is, G.items))
+    launches = sum(matrix_kernels(I["kind"], it["variant"], len(I["cells"]) >= (1 << 20)) for I, it in zip(Is, G.items))
     chosen = {}
     for it in G.items:
         chosen[it["variant"]] = chosen.get(it["variant"], 0) + 1
@@ -1093,7 +1096,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batch", "multimesh", "serve"], default="p2")
-    ap.add_argument("--variant", choices=["auto", "tile", "atomic", "sorted-slot", "deterministic", "row-gather",
+    ap.add_argument("--variant", choices=["auto", "tile", "atomic", "atomic-full", "sorted-slot", "deterministic",
+                                          "row-gather",
                                           "block"], default="auto")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--serve-requests", type=int, default=0, help="serve workload: requests per rate")

@@ -262,6 +262,137 @@ __global__ void __launch_bounds__(BlockTraits<KIND>::NT, BlockTraits<KIND>::MINB
   }
 }
 
+// P1 specialisation (constant or DG0 coefficient): the same window
+// combine, with the per-cell reads vectorised (window rows as one 8-byte
+// load, slot bytes as one 16-byte load), BC column masks of square forms
+// taken from the window rows instead of global reads, the cells of a warp
+// spread over the block (fewer lanes adding into the same window slot at
+// once), and a flat flush over the window (a per-slot row table in shared
+// memory keeps all lanes busy on 15-slot rows).
+// window arithmetic of the P1 kernel: FP64 shared-memory atomics (true) or
+// the exact fixed-point combine (false)
+constexpr bool kP1BlockFp64Window = false;
+
+struct P1Smem {
+  using Tr = BlockTraits<FE_FORM_P1_STIFFNESS>;
+  static constexpr size_t OFF_SOFF = sizeof(uint32_t) * 2 * (Tr::WCAP + 2);
+  static constexpr size_t OFF_GBASE = OFF_SOFF + sizeof(int32_t) * (Tr::RCAP + 1);
+  static constexpr size_t OFF_WROW = OFF_GBASE + sizeof(int32_t) * Tr::RCAP;
+  static constexpr size_t OFF_RMASK = OFF_WROW + sizeof(uint16_t) * Tr::WCAP;
+  static constexpr size_t OFF_CMASK = OFF_RMASK + Tr::RCAP;
+  static constexpr size_t SMEM = OFF_CMASK + Tr::RCAP;
+};
+
+template <bool FP64ACC>
+__global__ void __launch_bounds__(BlockTraits<FE_FORM_P1_STIFFNESS>::NT, 4) k_block_p1(const BlockArgs a,
+                                                                                    int square) {
+  using Tr = BlockTraits<FE_FORM_P1_STIFFNESS>;
+  using S = P1Smem;
+  constexpr int NT = Tr::NT, NW = NT / 32;
+  extern __shared__ __align__(16) unsigned char smem[];
+  uint32_t* win = reinterpret_cast<uint32_t*>(smem);
+  int32_t* s_soff = reinterpret_cast<int32_t*>(smem + S::OFF_SOFF);
+  int32_t* s_gbase = reinterpret_cast<int32_t*>(smem + S::OFF_GBASE);
+  uint16_t* s_wrow = reinterpret_cast<uint16_t*>(smem + S::OFF_WROW);
+  uint8_t* s_rmask = smem + S::OFF_RMASK;
+  uint8_t* s_cmask = smem + S::OFF_CMASK;
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int32_t b = blockIdx.x;
+  const int32_t r0 = a.brow_ptr[b], nrows = a.brow_ptr[b + 1] - r0;
+  const int32_t c0 = a.block_ptr[b], ncells = a.block_ptr[b + 1] - c0;
+  for (int r = tid; r < nrows; r += NT) {
+    const int32_t R = a.rows[r0 + r];
+    const int32_t lo = __ldg(a.row_ptr + R), len = __ldg(a.row_ptr + R + 1) - lo;
+    const int32_t so = a.soff[r0 + r];
+    s_gbase[r] = lo;
+    s_soff[r] = so;
+    if (r == nrows - 1) s_soff[nrows] = so + len;
+    s_rmask[r] = a.bc0 ? a.bc0[R] : 0;
+    s_cmask[r] = (square && a.bc1) ? a.bc1[R] : 0;
+    for (int e = 0; e < len; ++e) s_wrow[so + e] = (uint16_t)r;
+  }
+  __shared__ unsigned s_bmax;
+  if (tid == 0) s_bmax = 0u;
+  __syncthreads();
+  const int32_t wtot = nrows ? s_soff[nrows] : 0;
+  for (int q = tid; q < 2 * wtot; q += NT) win[q] = 0u;
+  double kfac = fabs(a.coef_const);
+  if (!FP64ACC && a.coef_kind != FE_COEFF_CONSTANT) {
+    for (int q = tid; q < ncells; q += NT)
+      atomicMax(&s_bmax, __float_as_uint((float)(cell_coef_factor(a, c0 + q) * 1.0625)));
+  }
+  __syncthreads();
+  if (!FP64ACC && a.coef_kind != FE_COEFF_CONSTANT) kfac = (double)__uint_as_float(s_bmax);
+  const double bmax = 1.25 * a.gbound[b] * kfac;
+  int ex = 0;
+  frexp(bmax, &ex);
+  const double scale = (bmax > 0.0 && bmax < 1e300) ? ldexp(1.0, 50 - ex) : 1.0;
+  const double inv_scale = 1.0 / scale;
+  double* wind = reinterpret_cast<double*>(smem);
+  constexpr double kMagic = 6755399441055744.0;  // 1.5 * 2^52
+
+  // lane l of warp w takes cells l*span + w, l*span + w + NW, ...: the 32
+  // cells of one warp instruction lie span cells apart along the curve
+  const int span = (ncells + 31) / 32;
+  for (int slot = warp; slot < span; slot += NW) {
+    const int q = lane * span + slot;
+    if (q >= ncells) continue;
+    const int64_t cb = c0 + q;
+    const uint2 lrw = __ldg(reinterpret_cast<const uint2*>(a.lrow) + cb);
+    const int lr[4] = {(int)(lrw.x & 0xffffu), (int)(lrw.x >> 16), (int)(lrw.y & 0xffffu), (int)(lrw.y >> 16)};
+    const uint4 pq = __ldg(reinterpret_cast<const uint4*>(a.pos) + cb);
+    const uint32_t pw[4] = {pq.x, pq.y, pq.z, pq.w};
+    int wbase[4];
+    unsigned own = 0, cmask = 0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      wbase[i] = s_soff[lr[i]];
+      own |= (s_rmask[lr[i]] ? 0u : 1u) << i;
+      if (square) cmask |= (unsigned)s_cmask[lr[i]] << i;
+      else if (a.bc1) cmask |= (a.bc1[__ldg(a.dofs1 + cb * 4 + i)] ? 1u : 0u) << i;
+    }
+    auto add_fixed = [&](int idx, long long w) {
+      const uint32_t lo = (uint32_t)(unsigned long long)w;
+      const uint32_t hi = (uint32_t)((unsigned long long)w >> 32);
+      const uint32_t old = atomicAdd(win + 2 * idx, lo);
+      atomicAdd(win + 2 * idx + 1, hi + ((old + lo < old) ? 1u : 0u));
+    };
+    auto add = [&](int idx, double v) {
+      if constexpr (FP64ACC) {
+        atomicAdd(wind + idx, v);
+      } else {
+        constexpr double kMagic = 6755399441055744.0;  // 1.5 * 2^52
+        add_fixed(idx, __double_as_longlong(fma(v, scale, kMagic)) - __double_as_longlong(kMagic));
+      }
+    };
+    auto emit = [&](int i, int j, double v) {
+      const bool ok_ij = ((own >> i) & 1u) && !((cmask >> j) & 1u);
+      add(ok_ij ? wbase[i] + (int)((pw[i] >> (8 * j)) & 0xffu) : Tr::WCAP, v);
+      if (i != j) {
+        const bool ok_ji = ((own >> j) & 1u) && !((cmask >> i) & 1u);
+        add(ok_ji ? wbase[j] + (int)((pw[j] >> (8 * i)) & 0xffu) : Tr::WCAP, v);
+      }
+    };
+    cell_entries<FE_FORM_P1_STIFFNESS, double>(a, cb, emit);
+  }
+  __syncthreads();
+  // flat flush: consecutive lanes take consecutive window slots
+  for (int w = tid; w < wtot; w += NT) {
+    double v;
+    if constexpr (FP64ACC) {
+      v = wind[w];
+    } else {
+      const uint32_t lo = win[2 * w], hi = win[2 * w + 1];
+      v = fma((double)(int32_t)hi, 4294967296.0, (double)lo) * inv_scale;
+    }
+    if (v != 0.0) {
+      const int r = s_wrow[w];
+      atomicAdd(a.values + s_gbase[r] + (w - s_soff[r]), v);
+    }
+  }
+}
+
 uint64_t spread3b(uint64_t v) {
   v &= 0x1fffff;
   v = (v | v << 32) & 0x1f00000000ffffull;
@@ -484,6 +615,14 @@ void launch_block(const fe_form_s& f, const fe_form_s::BlockPlan& P, double* val
   else a.term_max = (a.coef_kind == FE_COEFF_P1) ? kP2P1CoefTermMax : kP2ConstTermMax;
   a.values = values;
   if (P.nblocks == 0) return;
+  if constexpr (KIND == FE_FORM_P1_STIFFNESS) {
+    constexpr size_t smem = P1Smem::SMEM;
+    auto kern = k_block_p1<kP1BlockFp64Window>;
+    FE_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kern<<<(unsigned)P.nblocks, BlockTraits<KIND>::NT, smem, s>>>(a, f.V0 == f.V1 ? 1 : 0);
+    FE_CUDA(cudaGetLastError());
+    return;
+  }
   auto kern = k_block<KIND, T>;
   constexpr size_t smem = BlockSmem<KIND>::SMEM;
   FE_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

@@ -108,6 +108,15 @@ struct fe_sparsity_s {
   fe::DevBuf<int32_t> diag;      // [num_rows] slot of (r, r) or -1
   std::vector<int32_t> host_row_ptr;  // host copy (tile planning)
   uint64_t id = 0;
+  // transpose map of the strictly lower triangle (symmetric patterns): one
+  // {lower slot, slot of its transpose} pair per strictly-lower slot, in slot
+  // order; built on first use
+  struct Mirror {
+    fe::DevBuf<int2> pairs;         // [lower slots]
+    int64_t nlower = 0;
+    bool ok = false;                // pattern symmetric with every diagonal present
+  };
+  std::unique_ptr<Mirror> mirror;
 };
 
 struct fe_bc_s {
@@ -246,8 +255,14 @@ struct MatLaunch {
   const Coefficient* c0;
   const Coefficient* c1;
   double* values;
+  int upper = 0;  // reduce only into the upper triangle and the diagonal
 };
 void launch_zero(double* v, int64_t n, cudaStream_t s);
+// symmetric-pattern transpose map (built once per pattern); false if the
+// pattern is not symmetric or lacks a diagonal entry
+bool ensure_mirror(fe_sparsity_s& sp, cudaStream_t s);
+// values[lower slot] = values[its transpose] for every strictly-lower slot
+void launch_mirror_lower(const fe_sparsity_s& sp, double* values, cudaStream_t s);
 void launch_build_slotmap(const fe_form_s& f, cudaStream_t s);
 void launch_matrix_atomic(const MatLaunch& a, cudaStream_t s);
 void launch_set_diagonal(const fe_sparsity_s& sp, const fe_bc_s& bc, double diagonal, double* values,

@@ -14,6 +14,8 @@
 // only, and coefficients are gathered in-kernel (no separate packing pass).
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "fe_element_code.cuh"
 #include "fe_internal.h"
 
@@ -131,6 +133,7 @@ struct MatArgs {
   const uint8_t* __restrict__ bc1;
   CoefDev c0, c1;
   double* __restrict__ values;
+  int upper;  // symmetric form + pattern: one reduction per unique entry, into the upper triangle
 };
 
 // ---------------------------------------------------------------------------
@@ -165,8 +168,13 @@ __global__ void __launch_bounds__(kBlock) k_mat_p1_atomic(const MatArgs a) {
 #pragma unroll
     for (int j = i; j < 4; ++j) {
       const double v = s * (G[i][0] * G[j][0] + G[i][1] * G[j][1] + G[i][2] * G[j][2]);
-      if (!(((mr >> i) | (mc >> j)) & 1u)) atomicAdd(a.values + rp[i] + ((pws[i] >> (8 * j)) & 0xffu), v);
-      if (i != j && !(((mr >> j) | (mc >> i)) & 1u))
+      // upper mode: only the entry whose row is below its column (the lower
+      // one is filled from it afterwards)
+      const bool do_ij = !a.upper || i == j || r[i] < r[j];
+      const bool do_ji = i != j && (!a.upper || r[j] < r[i]);
+      if (do_ij && !(((mr >> i) | (mc >> j)) & 1u))
+        atomicAdd(a.values + rp[i] + ((pws[i] >> (8 * j)) & 0xffu), v);
+      if (do_ji && !(((mr >> j) | (mc >> i)) & 1u))
         atomicAdd(a.values + rp[j] + ((pws[j] >> (8 * i)) & 0xffu), v);
     }
 }
@@ -192,21 +200,25 @@ __global__ void __launch_bounds__(kBlock) k_mat_p2_atomic(const MatArgs a) {
   double Gh[6];
   ghat(g, Gh);
 
-  int rp[10];
+  int rp[10], rd[10];
   unsigned mr = 0, mc = 0;
   const int32_t* d0 = a.dofs0 + c * 10;
   const int32_t* d1 = a.dofs1 + c * 10;
 #pragma unroll
   for (int i = 0; i < 10; ++i) {
     const int r = __ldg(d0 + i);
+    rd[i] = r;
     rp[i] = __ldg(a.row_ptr + r);
     if (a.bc0) mr |= (__ldg(a.bc0 + r) ? 1u : 0u) << i;
     if (a.bc1) mc |= (__ldg(a.bc1 + __ldg(d1 + i)) ? 1u : 0u) << i;
   }
   double* __restrict__ vals = a.values;
+  const bool upper = a.upper != 0;
   auto emit = [&](int i, int j, double v) {
-    if (!(((mr >> i) | (mc >> j)) & 1u)) atomicAdd(vals + rp[i] + p[i * 10 + j], v);
-    if (i != j && !(((mr >> j) | (mc >> i)) & 1u)) atomicAdd(vals + rp[j] + p[j * 10 + i], v);
+    const bool do_ij = !upper || i == j || rd[i] < rd[j];
+    const bool do_ji = i != j && (!upper || rd[j] < rd[i]);
+    if (do_ij && !(((mr >> i) | (mc >> j)) & 1u)) atomicAdd(vals + rp[i] + p[i * 10 + j], v);
+    if (do_ji && !(((mr >> j) | (mc >> i)) & 1u)) atomicAdd(vals + rp[j] + p[j * 10 + i], v);
   };
   if constexpr (COEF == FE_COEFF_P1) {
     const int4 km = __ldg(reinterpret_cast<const int4*>(a.c0.map) + c);
@@ -277,13 +289,14 @@ __global__ void __launch_bounds__(kBlock) k_mat_vp2_atomic(const MatArgs a) {
   cell_geometry(a.x, load_geom(a.geom, c), g);
   const double lam = coef_cell(a.c0, c), mu = coef_cell(a.c1, c);
 
-  int rp[10], L[10];
+  int rp[10], L[10], rd[10];
   unsigned mr = 0, mc = 0;
   const int32_t* d0 = a.dofs0 + c * 10;
   const int32_t* d1 = a.dofs1 + c * 10;
 #pragma unroll
   for (int i = 0; i < 10; ++i) {
     const int R = __ldg(d0 + i);
+    rd[i] = R;
     rp[i] = __ldg(a.row_ptr + 3 * R);
     L[i] = __ldg(a.row_ptr + 3 * R + 1) - rp[i];
     const int C = __ldg(d1 + i);
@@ -294,10 +307,17 @@ __global__ void __launch_bounds__(kBlock) k_mat_vp2_atomic(const MatArgs a) {
     }
   }
   double* __restrict__ vals = a.values;
+  const bool upper = a.upper != 0;
   elasticity_blocks<T>(g, lam, mu, [&](int ca, int cb, int i, int j, double v) {
-    if (!(((mr >> (3 * i + ca)) | (mc >> (3 * j + cb))) & 1u))
+    // scalar rows 3*rd[i]+ca and 3*rd[j]+cb; upper mode keeps the entry in the
+    // upper triangle (the diagonal entry when they coincide)
+    const int ri = 3 * rd[i] + ca, rj = 3 * rd[j] + cb;
+    const bool same = ca == cb && i == j;
+    const bool do_ij = !upper || ri <= rj;
+    const bool do_ji = !same && (!upper || rj < ri);
+    if (do_ij && !(((mr >> (3 * i + ca)) | (mc >> (3 * j + cb))) & 1u))
       atomicAdd(vals + rp[i] + ca * L[i] + 3 * p[i * 10 + j] + cb, v);
-    if (!(ca == cb && i == j) && !(((mr >> (3 * j + cb)) | (mc >> (3 * i + ca))) & 1u))
+    if (do_ji && !(((mr >> (3 * j + cb)) | (mc >> (3 * i + ca))) & 1u))
       atomicAdd(vals + rp[j] + cb * L[j] + 3 * p[j * 10 + i] + ca, v);
   });
 }
@@ -328,6 +348,53 @@ __global__ void k_set_diagonal(const int32_t* __restrict__ dofs, int64_t n_owned
   if (r < 0 || r >= num_rows) return;
   const int32_t s = diag[r];
   if (s >= 0) values[s] = value;
+}
+
+// Strictly-lower slot counts per row (diag[r] - row_ptr[r]); -1 when a row
+// has no diagonal entry.
+__global__ void k_lower_count(const int32_t* __restrict__ row_ptr, const int32_t* __restrict__ diag,
+                              int64_t num_rows, int32_t* __restrict__ cnt) {
+  const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (r >= num_rows) return;
+  const int32_t d = diag[r];
+  cnt[r] = d < 0 ? -1 : d - row_ptr[r];
+}
+
+// One pair per strictly-lower slot (r, c), c < r: {the slot, the slot of
+// (c, r)}, the latter by binary search in row c; a missing transpose entry
+// sets *bad.
+__global__ void k_lower_pairs(const int32_t* __restrict__ row_ptr, const int32_t* __restrict__ col,
+                              const int32_t* __restrict__ lower_ptr, int64_t num_rows, int2* __restrict__ pairs,
+                              int* __restrict__ bad) {
+  const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (r >= num_rows) return;
+  const int32_t lo = row_ptr[r], n = lower_ptr[r + 1] - lower_ptr[r], base = lower_ptr[r];
+  for (int32_t t = 0; t < n; ++t) {
+    const int32_t c = col[lo + t];
+    int32_t a = row_ptr[c], b = row_ptr[c + 1] - 1, hit = -1;
+    while (a <= b) {
+      const int32_t m = (a + b) >> 1;
+      const int32_t v = col[m];
+      if (v == (int32_t)r) {
+        hit = m;
+        break;
+      }
+      if (v < (int32_t)r) a = m + 1;
+      else b = m - 1;
+    }
+    if (hit < 0) atomicOr(bad, 1);
+    pairs[base + t] = make_int2(lo + t, hit < 0 ? lo + t : hit);
+  }
+}
+
+// values[pair.x] = values[pair.y] for every strictly-lower slot: one slot per
+// thread, pairs read coalesced, the mirror reads are the only scattered ones.
+__global__ void k_mirror_pairs(const int2* __restrict__ pairs, int64_t n, double* __restrict__ values) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += stride) {
+    const int2 p = __ldg(pairs + k);
+    values[p.x] = values[p.y];
+  }
 }
 
 // Cell-to-slot map: block position of dofs1[c,j] inside block row dofs0[c,i].
@@ -633,6 +700,7 @@ void launch_matrix_atomic(const MatLaunch& L, cudaStream_t s) {
   a.c0 = to_dev(L.c0);
   a.c1 = to_dev(L.c1);
   a.values = L.values;
+  a.upper = L.upper;
   const unsigned grid = grid_for(L.num_cells, kBlock);
   const bool f32 = L.precision == FE_PREC_FP32;
   switch (L.kind) {
@@ -655,6 +723,60 @@ void launch_matrix_atomic(const MatLaunch& L, cudaStream_t s) {
     default:
       FE_FAIL(FE_ERR_ARG, "not a bilinear form kind: " + std::to_string(L.kind));
   }
+  FE_CUDA(cudaGetLastError());
+}
+
+bool ensure_mirror(fe_sparsity_s& sp, cudaStream_t s) {
+  if (sp.mirror) return sp.mirror->ok;
+  auto M = std::make_unique<fe_sparsity_s::Mirror>();
+  const int64_t R = sp.num_rows;
+  if (R == 0 || sp.num_rows != sp.num_cols) {
+    sp.mirror = std::move(M);
+    return false;
+  }
+  DevBuf<int32_t> cnt(R);
+  k_lower_count<<<grid_for(R, 256), 256, 0, s>>>(sp.row_ptr.p, sp.diag.p, R, cnt.p);
+  FE_CUDA(cudaGetLastError());
+  std::vector<int32_t> h(R);
+  FE_CUDA(cudaMemcpyAsync(h.data(), cnt.p, R * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  FE_CUDA(cudaStreamSynchronize(s));
+  std::vector<int32_t> lp(R + 1, 0);
+  bool ok = true;
+  int64_t tot = 0;
+  for (int64_t r = 0; r < R; ++r) {
+    if (h[r] < 0) ok = false;
+    tot += h[r] < 0 ? 0 : h[r];
+    if (tot > INT32_MAX) ok = false;
+    lp[r + 1] = (int32_t)std::min<int64_t>(tot, INT32_MAX);
+  }
+  if (ok) {
+    M->nlower = tot;
+    M->pairs.alloc(std::max<int64_t>(1, tot));
+    DevBuf<int32_t> lower_ptr(R + 1);
+    FE_CUDA(cudaMemcpyAsync(lower_ptr.p, lp.data(), (R + 1) * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+    DevBuf<int> bad(1);
+    FE_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(int), s));
+    k_lower_pairs<<<grid_for(R, 128), 128, 0, s>>>(sp.row_ptr.p, sp.col.p, lower_ptr.p, R, M->pairs.p, bad.p);
+    FE_CUDA(cudaGetLastError());
+    int hb = 0;
+    FE_CUDA(cudaMemcpyAsync(&hb, bad.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    FE_CUDA(cudaStreamSynchronize(s));  // lower_ptr and bad are freed on return
+    ok = hb == 0;
+  }
+  M->ok = ok;
+  if (!ok) M->pairs.release();
+  sp.mirror = std::move(M);
+  return ok;
+}
+
+void launch_mirror_lower(const fe_sparsity_s& sp, double* values, cudaStream_t s) {
+  const auto& M = *sp.mirror;
+  if (!M.ok || M.nlower == 0) return;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const unsigned grid = (unsigned)std::min<int64_t>((M.nlower + 255) / 256, (int64_t)sms * 16);
+  k_mirror_pairs<<<grid, 256, 0, s>>>(M.pairs.p, M.nlower, values);
   FE_CUDA(cudaGetLastError());
 }
 

@@ -93,7 +93,8 @@ class CUDAAssembler:
         ordered tile gather for P1/P2, sorted-slot otherwise), "atomic"
         (FP64-atomic scatter), "sorted-slot" (global sorted-slot reduction),
         "block" (Morton cell blocks combined in shared memory, P1/P2), "tile"
-        (owner-computes row tiles, P1/P2), "row-gather" (P1).
+        (owner-computes row tiles, P1/P2), "row-gather" (P1), "atomic-full"
+        (atomic scatter into both triangles, the reference's scheme).
         ``deterministic=True`` is the same as variant="deterministic"."""
         if variant not in _lib.VARIANT_FLAGS:
             raise ValueError(f"unknown variant {variant!r}; expected one of {sorted(_lib.VARIANT_FLAGS)}")

@@ -26,7 +26,7 @@ from .la import CUDAMatrix
 CANDIDATES = {
     "P1_STIFFNESS": ("atomic", "block", "tile"),
     "P2_STIFFNESS": ("atomic", "block"),
-    "VP2_ELASTICITY": ("atomic", "sorted-slot"),
+    "VP2_ELASTICITY": ("atomic", "atomic-full"),
 }
 
 

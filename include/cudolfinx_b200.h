@@ -77,12 +77,16 @@ enum fe_precision {
  * scatter otherwise (the fastest measured on B200 for each case). */
 #define FE_ASM_ZERO 1u            /* overwrite instead of accumulating (assemble.py:52 zero=True)   */
 #define FE_ASM_DETERMINISTIC 2u   /* bitwise reproducible: ordered tile gather (P1/P2), else sorted-slot */
-#define FE_ASM_ATOMIC 4u          /* FP64-atomic scatter through the slot map (zero pass first)     */
+#define FE_ASM_ATOMIC 4u          /* FP64-atomic scatter through the slot map (zero pass first); for
+                                     vector-P2 elasticity on a symmetric pattern with equal row/column
+                                     BCs each unique entry is reduced once into the upper triangle
+                                     and a pass copies it to the lower triangle                      */
 #define FE_ASM_SORTED_SLOT 8u     /* global sorted-slot segmented reduction (reproducible)          */
 #define FE_ASM_TILE 16u           /* owner-computes row tiles, shared-memory accumulation (P1/P2)   */
 #define FE_ASM_ROW_GATHER 32u     /* one warp per CSR row over the row's cells (P1)                 */
 #define FE_ASM_BLOCK 64u          /* Morton cell blocks combined in shared memory, then coalesced
                                      reductions (P1/P2)                                              */
+#define FE_ASM_FULL_SCATTER 128u  /* atomic scatter into both triangles, as the reference does      */
 
 /* ---- errors / context --------------------------------------------------- */
 const char* fe_last_error(void);

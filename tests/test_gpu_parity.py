@@ -30,7 +30,7 @@ def _problem_from_golden(path):
     return P, G
 
 
-VARIANTS = ["auto", "atomic", "tile", "deterministic", "sorted-slot", "row-gather", "block"]
+VARIANTS = ["auto", "atomic", "atomic-full", "tile", "deterministic", "sorted-slot", "row-gather", "block"]
 
 
 def _supported(kind, variant):
