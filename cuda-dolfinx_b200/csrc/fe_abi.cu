@@ -570,8 +570,8 @@ int fe_assemble_matrix(fe_form a, double* values, fe_bc bc0, fe_bc bc1, double d
     // every built-in bilinear form is symmetric: on a symmetric pattern with
     // the same BCs on rows and columns, vector-P2 elasticity reduces each
     // unique entry once into the upper triangle and a gather pass fills the
-    // lower triangle from it (measured on B200 at n=64: 7.6 ms instead of
-    // 12.4 ms).  For P1/P2 the pass costs what the halved reductions save
+    // lower triangle from it (vector P2 n=64 on B200: 7.6 ms instead of about
+    // 12 ms).  For P1/P2 the pass costs what the halved reductions save
     // (P2 n=96: 1.58 + 0.95 ms vs 2.55 ms), so they keep both reductions, as
     // does FE_ASM_FULL_SCATTER for every form.
     const bool upper = zero && !(flags & FE_ASM_FULL_SCATTER) && a->kind == FE_FORM_VP2_ELASTICITY &&

@@ -36,11 +36,11 @@ struct BlockTraits;
 // WCAP: window slots (8 bytes each); RCAP: touched rows per block; MINB: CTAs per SM to fit
 template <>
 struct BlockTraits<FE_FORM_P1_STIFFNESS> {
-  static constexpr int K = 4, NT = 256, BMAX = 512, WCAP = 4096, RCAP = 512, MINB = 4;
+  static constexpr int K = 4, NT = 256, BMAX = 512, WCAP = 3072, RCAP = 512, MINB = 4, VCAP = 512;
 };
 template <>
 struct BlockTraits<FE_FORM_P2_STIFFNESS> {
-  static constexpr int K = 10, NT = 128, BMAX = 128, WCAP = 8192, RCAP = 768, MINB = 3;
+  static constexpr int K = 10, NT = 128, BMAX = 128, WCAP = 8192, RCAP = 768, MINB = 3, VCAP = 1 << 30;
 };
 
 template <int KIND>
@@ -75,6 +75,9 @@ struct BlockArgs {
   const double* __restrict__ gbound;       // [nblocks] geometric part of the entry bound
   double term_max;                         // reference-tensor part of the entry bound
   double* __restrict__ values;
+  const int32_t* __restrict__ gvert_ptr;   // P1: [nblocks+1] block geometry nodes
+  const double* __restrict__ gx;           // P1: their coordinates, block by block
+  const uint16_t* __restrict__ glocal;     // P1: [cells][4] block-local node of each vertex
 };
 
 __device__ __forceinline__ void block_geom(const double* __restrict__ x, int4 v, double K[3][3], double& adet) {
@@ -269,33 +272,40 @@ __global__ void __launch_bounds__(BlockTraits<KIND>::NT, BlockTraits<KIND>::MINB
 // spread over the block (fewer lanes adding into the same window slot at
 // once), and a flat flush over the window (a per-slot row table in shared
 // memory keeps all lanes busy on 15-slot rows).
-// window arithmetic of the P1 kernel: FP64 shared-memory atomics (true) or
-// the exact fixed-point combine (false)
-constexpr bool kP1BlockFp64Window = false;
+// P1 window: a contribution's 64-bit fixed-point value w (|w| < 2^50) is
+// kept as two 32-bit shared words (low and high half, two planes); the low
+// word's atomic returns its old value, from which the carry into the high
+// word is added exactly once per wrap.  (Three carry-free 21-bit fields were
+// measured too: the kernel is bound by shared-memory wavefronts, so the third
+// atomic per contribution cost more than the carry dependency.)
+constexpr int kP1Wcap = BlockTraits<FE_FORM_P1_STIFFNESS>::WCAP;
 
 struct P1Smem {
   using Tr = BlockTraits<FE_FORM_P1_STIFFNESS>;
-  static constexpr size_t OFF_SOFF = sizeof(uint32_t) * 2 * (Tr::WCAP + 2);
+  static constexpr int PLANE = kP1Wcap + 1;  // + the spare slot
+  static constexpr size_t OFF_SOFF = sizeof(uint32_t) * 2 * PLANE + 8;
   static constexpr size_t OFF_GBASE = OFF_SOFF + sizeof(int32_t) * (Tr::RCAP + 1);
   static constexpr size_t OFF_WROW = OFF_GBASE + sizeof(int32_t) * Tr::RCAP;
-  static constexpr size_t OFF_RMASK = OFF_WROW + sizeof(uint16_t) * Tr::WCAP;
+  static constexpr size_t OFF_RMASK = OFF_WROW + sizeof(uint16_t) * kP1Wcap;
   static constexpr size_t OFF_CMASK = OFF_RMASK + Tr::RCAP;
-  static constexpr size_t SMEM = OFF_CMASK + Tr::RCAP;
+  static constexpr size_t OFF_X = (OFF_CMASK + Tr::RCAP + 15) / 16 * 16;
+  static constexpr size_t SMEM = OFF_X + sizeof(double) * 3 * Tr::VCAP;
 };
 
-template <bool FP64ACC>
 __global__ void __launch_bounds__(BlockTraits<FE_FORM_P1_STIFFNESS>::NT, 4) k_block_p1(const BlockArgs a,
                                                                                     int square) {
   using Tr = BlockTraits<FE_FORM_P1_STIFFNESS>;
   using S = P1Smem;
-  constexpr int NT = Tr::NT, NW = NT / 32;
+  constexpr int NT = Tr::NT, NW = NT / 32, PLANE = S::PLANE;
   extern __shared__ __align__(16) unsigned char smem[];
-  uint32_t* win = reinterpret_cast<uint32_t*>(smem);
+  uint32_t* w0 = reinterpret_cast<uint32_t*>(smem);  // low words
+  uint32_t* w1 = w0 + PLANE;                         // high words
   int32_t* s_soff = reinterpret_cast<int32_t*>(smem + S::OFF_SOFF);
   int32_t* s_gbase = reinterpret_cast<int32_t*>(smem + S::OFF_GBASE);
   uint16_t* s_wrow = reinterpret_cast<uint16_t*>(smem + S::OFF_WROW);
   uint8_t* s_rmask = smem + S::OFF_RMASK;
   uint8_t* s_cmask = smem + S::OFF_CMASK;
+  double* s_x = reinterpret_cast<double*>(smem + S::OFF_X);
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int32_t b = blockIdx.x;
@@ -312,25 +322,32 @@ __global__ void __launch_bounds__(BlockTraits<FE_FORM_P1_STIFFNESS>::NT, 4) k_bl
     s_cmask[r] = (square && a.bc1) ? a.bc1[R] : 0;
     for (int e = 0; e < len; ++e) s_wrow[so + e] = (uint16_t)r;
   }
+  {
+    // the block's geometry nodes: one coalesced copy into shared memory
+    const int32_t g0 = a.gvert_ptr[b], ng = a.gvert_ptr[b + 1] - g0;
+    const double* src = a.gx + 3 * (int64_t)g0;
+    for (int q = tid; q < 3 * ng; q += NT) s_x[q] = __ldg(src + q);
+  }
   __shared__ unsigned s_bmax;
   if (tid == 0) s_bmax = 0u;
   __syncthreads();
   const int32_t wtot = nrows ? s_soff[nrows] : 0;
-  for (int q = tid; q < 2 * wtot; q += NT) win[q] = 0u;
-  double kfac = fabs(a.coef_const);
-  if (!FP64ACC && a.coef_kind != FE_COEFF_CONSTANT) {
+  for (int q = tid; q < wtot; q += NT) {
+    w0[q] = 0u;
+    w1[q] = 0u;
+  }
+  if (a.coef_kind != FE_COEFF_CONSTANT) {
     for (int q = tid; q < ncells; q += NT)
       atomicMax(&s_bmax, __float_as_uint((float)(cell_coef_factor(a, c0 + q) * 1.0625)));
   }
   __syncthreads();
-  if (!FP64ACC && a.coef_kind != FE_COEFF_CONSTANT) kfac = (double)__uint_as_float(s_bmax);
+  const double kfac = a.coef_kind != FE_COEFF_CONSTANT ? (double)__uint_as_float(s_bmax) : fabs(a.coef_const);
   const double bmax = 1.25 * a.gbound[b] * kfac;
   int ex = 0;
   frexp(bmax, &ex);
   const double scale = (bmax > 0.0 && bmax < 1e300) ? ldexp(1.0, 50 - ex) : 1.0;
   const double inv_scale = 1.0 / scale;
-  double* wind = reinterpret_cast<double*>(smem);
-  constexpr double kMagic = 6755399441055744.0;  // 1.5 * 2^52
+  constexpr double kMagic = 6755399441055744.0;  // 1.5 * 2^52: v + kMagic holds round(v) in its low bits
 
   // lane l of warp w takes cells l*span + w, l*span + w + NW, ...: the 32
   // cells of one warp instruction lie span cells apart along the curve
@@ -352,43 +369,63 @@ __global__ void __launch_bounds__(BlockTraits<FE_FORM_P1_STIFFNESS>::NT, 4) k_bl
       if (square) cmask |= (unsigned)s_cmask[lr[i]] << i;
       else if (a.bc1) cmask |= (a.bc1[__ldg(a.dofs1 + cb * 4 + i)] ? 1u : 0u) << i;
     }
-    auto add_fixed = [&](int idx, long long w) {
+    auto add = [&](int idx, long long w) {
       const uint32_t lo = (uint32_t)(unsigned long long)w;
       const uint32_t hi = (uint32_t)((unsigned long long)w >> 32);
-      const uint32_t old = atomicAdd(win + 2 * idx, lo);
-      atomicAdd(win + 2 * idx + 1, hi + ((old + lo < old) ? 1u : 0u));
-    };
-    auto add = [&](int idx, double v) {
-      if constexpr (FP64ACC) {
-        atomicAdd(wind + idx, v);
-      } else {
-        constexpr double kMagic = 6755399441055744.0;  // 1.5 * 2^52
-        add_fixed(idx, __double_as_longlong(fma(v, scale, kMagic)) - __double_as_longlong(kMagic));
-      }
+      const uint32_t old = atomicAdd(w0 + idx, lo);
+      atomicAdd(w1 + idx, hi + ((old + lo < old) ? 1u : 0u));
     };
     auto emit = [&](int i, int j, double v) {
+      const long long w = __double_as_longlong(fma(v, scale, kMagic)) - __double_as_longlong(kMagic);
       const bool ok_ij = ((own >> i) & 1u) && !((cmask >> j) & 1u);
-      add(ok_ij ? wbase[i] + (int)((pw[i] >> (8 * j)) & 0xffu) : Tr::WCAP, v);
+      add(ok_ij ? wbase[i] + (int)((pw[i] >> (8 * j)) & 0xffu) : kP1Wcap, w);
       if (i != j) {
         const bool ok_ji = ((own >> j) & 1u) && !((cmask >> i) & 1u);
-        add(ok_ji ? wbase[j] + (int)((pw[j] >> (8 * i)) & 0xffu) : Tr::WCAP, v);
+        add(ok_ji ? wbase[j] + (int)((pw[j] >> (8 * i)) & 0xffu) : kP1Wcap, w);
       }
     };
-    cell_entries<FE_FORM_P1_STIFFNESS, double>(a, cb, emit);
+    // P1 element from the staged coordinates: grad phi_i = K^T ghat_i,
+    // A_ij = k |det J| / 6 grad phi_i . grad phi_j
+    const uint2 glw = __ldg(reinterpret_cast<const uint2*>(a.glocal) + cb);
+    const int gl[4] = {(int)(glw.x & 0xffffu), (int)(glw.x >> 16), (int)(glw.y & 0xffffu), (int)(glw.y >> 16)};
+    double J[3][3];
+#pragma unroll
+    for (int cc = 0; cc < 3; ++cc)
+#pragma unroll
+      for (int r = 0; r < 3; ++r) J[r][cc] = s_x[3 * gl[cc + 1] + r] - s_x[3 * gl[0] + r];
+    const double c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1];
+    const double c01 = J[1][2] * J[2][0] - J[1][0] * J[2][2];
+    const double c02 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
+    const double det = J[0][0] * c00 + J[0][1] * c01 + J[0][2] * c02;
+    const double id = 1.0 / det;
+    double G[4][3];
+    G[1][0] = c00 * id;
+    G[1][1] = (J[0][2] * J[2][1] - J[0][1] * J[2][2]) * id;
+    G[1][2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) * id;
+    G[2][0] = c01 * id;
+    G[2][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) * id;
+    G[2][2] = (J[0][2] * J[1][0] - J[0][0] * J[1][2]) * id;
+    G[3][0] = c02 * id;
+    G[3][1] = (J[0][1] * J[2][0] - J[0][0] * J[2][1]) * id;
+    G[3][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) * id;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) G[0][d] = -(G[1][d] + G[2][d] + G[3][d]);
+    const double kc = a.coef_kind == FE_COEFF_DG0 ? __ldg(a.coef + __ldg(a.cell_id + cb)) : a.coef_const;
+    const double sc = fabs(det) * (1.0 / 6.0) * kc;
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = i; j < 4; ++j) emit(i, j, sc * (G[i][0] * G[j][0] + G[i][1] * G[j][1] + G[i][2] * G[j][2]));
   }
   __syncthreads();
   // flat flush: consecutive lanes take consecutive window slots
   for (int w = tid; w < wtot; w += NT) {
-    double v;
-    if constexpr (FP64ACC) {
-      v = wind[w];
-    } else {
-      const uint32_t lo = win[2 * w], hi = win[2 * w + 1];
-      v = fma((double)(int32_t)hi, 4294967296.0, (double)lo) * inv_scale;
-    }
-    if (v != 0.0) {
+    const uint32_t lo = w0[w], hi = w1[w];
+    if (lo | hi) {
       const int r = s_wrow[w];
-      atomicAdd(a.values + s_gbase[r] + (w - s_soff[r]), v);
+      // hi * 2^32 + lo, rounded once to double (both halves convert exactly)
+      const double v = fma((double)(int32_t)hi, 4294967296.0, (double)lo);
+      atomicAdd(a.values + s_gbase[r] + (w - s_soff[r]), v * inv_scale);
     }
   }
 }
@@ -446,13 +483,25 @@ std::unique_ptr<fe_form_s::BlockPlan> build_block_plan(const fe_form_s& f) {
   std::vector<int32_t> block_ptr(1, 0), brow_ptr(1, 0), rows, soff;
   std::vector<uint16_t> lrow(C * K);
   std::vector<int32_t> mark(V0.num_blocks, -1), local(V0.num_blocks, 0);
+  // geometry nodes per block (the P1 kernel stages their coordinates)
+  const int64_t nnodes = (int64_t)X.size() / 3;
+  std::vector<int32_t> gmark(nnodes, -1), glocal_of(nnodes, 0), gvert_ptr(1, 0), gverts;
+  std::vector<uint16_t> glocal(C * 4);
   int64_t q = 0;
   while (q < C) {
     const int32_t bid = (int32_t)block_ptr.size() - 1;
-    std::vector<int32_t> brows;
+    std::vector<int32_t> brows, bverts;
     int64_t wsize = 0, start = q;
     while (q < C && q - start < Tr::BMAX) {
       const int64_t c = key[q].second;
+      int64_t addv = 0;
+      for (int v = 0; v < 4; ++v) {
+        const int32_t g = G[c * 4 + v];
+        bool dup = gmark[g] == bid;
+        for (int u = 0; u < v; ++u) dup |= G[c * 4 + u] == g;
+        if (!dup) ++addv;
+      }
+      if (q > start && (int64_t)bverts.size() + addv > Tr::VCAP) break;
       int64_t add = 0, addr = 0;
       for (int i = 0; i < K; ++i) {
         const int32_t R = V0.host[c * K + i];
@@ -474,9 +523,23 @@ std::unique_ptr<fe_form_s::BlockPlan> build_block_plan(const fe_form_s& f) {
           brows.push_back(R);
         }
       }
+      for (int v = 0; v < 4; ++v) {
+        const int32_t g = G[c * 4 + v];
+        if (gmark[g] != bid) {
+          gmark[g] = bid;
+          glocal_of[g] = (int32_t)bverts.size();
+          bverts.push_back(g);
+        }
+      }
       wsize += add;
       ++q;
     }
+    for (int64_t p = start; p < q; ++p) {
+      const int64_t c = key[p].second;
+      for (int v = 0; v < 4; ++v) glocal[p * 4 + v] = (uint16_t)glocal_of[G[c * 4 + v]];
+    }
+    gverts.insert(gverts.end(), bverts.begin(), bverts.end());
+    gvert_ptr.push_back((int32_t)gverts.size());
     std::sort(brows.begin(), brows.end());
     int32_t off = 0;
     for (size_t u = 0; u < brows.size(); ++u) {
@@ -584,6 +647,14 @@ std::unique_ptr<fe_form_s::BlockPlan> build_block_plan(const fe_form_s& f) {
   up(P->pos, pos);
   if (p1coef) up(P->coef_map, cmap);
   up(P->gbound, gbound);
+  if (KIND == FE_FORM_P1_STIFFNESS) {
+    std::vector<double> gx(gverts.size() * 3);
+    for (size_t u = 0; u < gverts.size(); ++u)
+      for (int d = 0; d < 3; ++d) gx[3 * u + d] = X[3 * (int64_t)gverts[u] + d];
+    up(P->gvert_ptr, gvert_ptr);
+    up(P->gx, gx);
+    up(P->glocal, glocal);
+  }
   return P;
 }
 
@@ -614,12 +685,14 @@ void launch_block(const fe_form_s& f, const fe_form_s::BlockPlan& P, double* val
   if (KIND == FE_FORM_P1_STIFFNESS) a.term_max = 1.0;
   else a.term_max = (a.coef_kind == FE_COEFF_P1) ? kP2P1CoefTermMax : kP2ConstTermMax;
   a.values = values;
+  a.gvert_ptr = P.gvert_ptr.p;
+  a.gx = P.gx.p;
+  a.glocal = P.glocal.p;
   if (P.nblocks == 0) return;
   if constexpr (KIND == FE_FORM_P1_STIFFNESS) {
     constexpr size_t smem = P1Smem::SMEM;
-    auto kern = k_block_p1<kP1BlockFp64Window>;
-    FE_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    kern<<<(unsigned)P.nblocks, BlockTraits<KIND>::NT, smem, s>>>(a, f.V0 == f.V1 ? 1 : 0);
+    FE_CUDA(cudaFuncSetAttribute(k_block_p1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_block_p1<<<(unsigned)P.nblocks, BlockTraits<KIND>::NT, smem, s>>>(a, f.V0 == f.V1 ? 1 : 0);
     FE_CUDA(cudaGetLastError());
     return;
   }
