@@ -93,6 +93,26 @@ def matrix_kernels(kind: str, variant: str, big: bool = False) -> int:
 _PINNED: list = []
 
 
+def reduce_over_ranks(values, op: str = "max", device: str = "cuda"):
+    """Element-wise max (timings) or min (throughputs) of per-rank values;
+    every rank gets the result; the identity without a process group."""
+    import torch
+    import torch.distributed as dist
+
+    vals = [float(v) for v in values]
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return vals
+    t = torch.tensor(vals, dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.MIN)
+    return [float(x) for x in t]
+
+
+def replica_rate(units_per_rank: float, steps: int, max_ms: float, world: int) -> float:
+    """Whole-job throughput of N replicas: all ranks' units over the slowest
+    rank's time."""
+    return world * units_per_rank * steps / (max_ms / 1e3)
+
+
 # ---------------------------------------------------------------------------
 # problem construction (host, seeded)
 # ---------------------------------------------------------------------------
@@ -365,10 +385,7 @@ def run_gpu(args, rank, world, local_rank):
     total_ms = e_start.elapsed_time(e_end)
     mat_ms = statistics.mean(m0.elapsed_time(m1) for m0, m1 in mats)
     clk = clocks.stop()
-    if dist:
-        t = torch.tensor([total_ms, mat_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms, mat_ms = float(t[0]), float(t[1])
+    total_ms, mat_ms = reduce_over_ranks([total_ms, mat_ms])
     ms_per_step = total_ms / args.steps
     cx.get_cuda_context().synchronize()
 
@@ -405,13 +422,10 @@ def run_gpu(args, rank, world, local_rank):
         s1.record(stream)
         torch.cuda.synchronize()
         e2e_ms = s0.elapsed_time(s1)
-        if dist:
-            t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_ms = float(t[0])
+        (e2e_ms,) = reduce_over_ranks([e2e_ms])
         # parity of the two legs (same seeded inputs)
         same = bool(torch.allclose(bhost.to(b.vector.device), b.vector, rtol=1e-12, atol=1e-13))
-        e2e = {"value": world * nnz * args.steps / (e2e_ms / 1e3), "unit": "nnz/s",
+        e2e = {"value": replica_rate(nnz, args.steps, e2e_ms, world), "unit": "nnz/s",
                "h2d_bytes_per_step": int(coef_bytes), "d2h_bytes_per_step": int(nrows * 8),
                "ms_per_step": e2e_ms / args.steps, "path": "cudolfinx.CUDAAssembler (Python API -> C-ABI)",
                "matches_device_leg": same}
@@ -429,7 +443,7 @@ def run_gpu(args, rank, world, local_rank):
     traffic = load_traffic(kernel_key)
     out = {
         "metric": "matrix nnz/s",
-        "value": world * nnz * args.steps / (total_ms / 1e3),
+        "value": replica_rate(nnz, args.steps, total_ms, world),
         "unit": "nnz/s",
         "n_gpus": world,
         "steps": args.steps,
@@ -625,10 +639,7 @@ def run_gpu_batch(args, rank, world, local_rank):
     plain_ms = p0.elapsed_time(p1)
     # agreement of the last instance between the two paths (FP32 element tensors)
     rel = float(torch.linalg.norm(vals[S - 1] - plain_vals) / torch.linalg.norm(plain_vals))
-    if dist:
-        t = torch.tensor([total_ms, call_ms, plain_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms, call_ms, plain_ms = (float(x) for x in t)
+    total_ms, call_ms, plain_ms = reduce_over_ranks([total_ms, call_ms, plain_ms])
 
     alg = S * (8 * nnz + 8 * C) + 16 * C + 16 * C + 16 * C + 24 * len(I["coords"]) + 4 * (nrows + 1) + nrows
     peaks = {}
@@ -641,7 +652,7 @@ def run_gpu_batch(args, rank, world, local_rank):
     achieved = alg / (call_ms / 1e3) / 1e9
     out = {
         "metric": "matrix nnz/s (batched instances)",
-        "value": world * S * nnz * args.steps / (total_ms / 1e3),
+        "value": replica_rate(S * nnz, args.steps, total_ms, world),
         "unit": "nnz/s",
         "n_gpus": world,
         "steps": args.steps,
@@ -750,10 +761,7 @@ def run_gpu_multimesh(args, rank, world, local_rank):
             fp64_items.append((a, mat, bcs))
     plain = cx.AssemblyGraph(fp64_items, variants="auto")
     plain_ms = timed(plain.run_eager, max(1, args.steps // 2))
-    if dist:
-        t = torch.tensor([total_ms, eager_ms, plain_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms, eager_ms, plain_ms = (float(x) for x in t)
+    total_ms, eager_ms, plain_ms = reduce_over_ranks([total_ms, eager_ms, plain_ms])
     ms = total_ms / args.steps
     alg = sum(algorithmic_matrix_bytes(I, it[1].sparsity.nnz) for I, it in zip(Is, items))
     peaks = {}
@@ -770,7 +778,7 @@ def run_gpu_multimesh(args, rank, world, local_rank):
         chosen[it["variant"]] = chosen.get(it["variant"], 0) + 1
     out = {
         "metric": "matrix nnz/s (multi-mesh graph)",
-        "value": world * nnz * args.steps / (total_ms / 1e3),
+        "value": replica_rate(nnz, args.steps, total_ms, world),
         "unit": "nnz/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32-element(P2)/f64-accumulate",
@@ -937,10 +945,8 @@ def run_gpu_serve(args, rank, world, local_rank):
     peak = peaks.get("hbm_gbs", 6650.0)
     achieved = alg / top["makespan_s"] / 1e9
     value = top["throughput_rps"]
-    if world > 1:
-        t = torch.tensor([value], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MIN)
-        value = float(t[0]) * world
+    (value,) = reduce_over_ranks([value], op="min")
+    value *= world
     out = {
         "metric": "served assemble+solve requests/s (p50/p99 latency beside)",
         "value": value, "unit": "req/s", "n_gpus": world, "steps": count, "warmup": 4,
