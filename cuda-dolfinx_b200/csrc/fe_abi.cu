@@ -270,6 +270,20 @@ int fe_sparsity_build(fe_dofmap rows, fe_dofmap cols, fe_sparsity* out) {
   });
 }
 
+int fe_sparsity_build_device(fe_dofmap rows, fe_dofmap cols, void* stream, fe_sparsity* out) {
+  return guard([&] {
+    FE_REQUIRE(rows && cols && out, "null argument");
+    FE_REQUIRE(rows->ctx == cols->ctx, "dofmaps belong to different contexts");
+    FE_REQUIRE(rows->num_cells == cols->num_cells, "dofmaps cover different cell counts");
+    DeviceScope d(rows->ctx);
+    auto s = std::make_unique<fe_sparsity_s>();
+    s->ctx = rows->ctx;
+    build_pattern_device(*rows, *cols, as_stream(stream), *s);
+    s->id = g_next_id++;
+    *out = s.release();
+  });
+}
+
 int fe_pattern_build_host(const int32_t* dofs0, const int32_t* dofs1, int64_t num_cells, int k0, int k1, int bs0,
                           int bs1, int64_t num_blocks0, int64_t num_blocks1, int64_t* nnz, int32_t** row_ptr_out,
                           int32_t** col_out) {

@@ -326,6 +326,10 @@ void reset_block_plan(fe_form_s& f);
 void assemble_matrix_block(fe_form_s& f, double* values, const fe_bc_s* bc0, const fe_bc_s* bc1, bool zero,
                            cudaStream_t s);
 
+// device pattern build (fe_sparsity_dev.cu): fills num_rows/num_cols/nnz,
+// row_ptr, col, diag and host_row_ptr of `sp`
+void build_pattern_device(const fe_dofmap_s& rows, const fe_dofmap_s& cols, cudaStream_t s, fe_sparsity_s& sp);
+
 // sorted-slot plan (fe_gather.cu): per CSR slot the ordered list of element
 // entries that land there; built on first use
 void ensure_gather_plan(fe_form_s& f, cudaStream_t s);

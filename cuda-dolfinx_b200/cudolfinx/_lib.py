@@ -51,6 +51,7 @@ _SIGS = {
     "fe_dofmap_create": (i32, [vp, vp, i64, i32, i32, i64, PP]),
     "fe_dofmap_destroy": (i32, [vp]),
     "fe_sparsity_build": (i32, [vp, vp, PP]),
+    "fe_sparsity_build_device": (i32, [vp, vp, vp, PP]),
     "fe_sparsity_create": (i32, [vp, vp, vp, i64, i64, PP]),
     "fe_sparsity_info": (i32, [vp, ctypes.POINTER(i64), ctypes.POINTER(i64), ctypes.POINTER(i64)]),
     "fe_sparsity_copy_to_host": (i32, [vp, vp, vp]),

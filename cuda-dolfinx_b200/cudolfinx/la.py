@@ -31,9 +31,16 @@ class Sparsity:
         self.num_rows, self.num_cols, self.nnz = r.value, c.value, n.value
 
     @classmethod
-    def build(cls, ctx, dofmap0, dofmap1):
+    def build(cls, ctx, dofmap0, dofmap1, on_device: bool = True):
+        """CSR pattern of the cell integral (create_cuda_matrix, la/petsc.cpp:14-151);
+        built on the device by default, on the host with ``on_device=False``
+        (the same arrays, bit for bit)."""
         h = _lib.out_handle()
-        _lib.check(_lib.lib.fe_sparsity_build(dofmap0.handle, dofmap1.handle, h), "fe_sparsity_build")
+        if on_device:
+            _lib.check(_lib.lib.fe_sparsity_build_device(dofmap0.handle, dofmap1.handle, ctx.stream(), h),
+                       "fe_sparsity_build_device")
+        else:
+            _lib.check(_lib.lib.fe_sparsity_build(dofmap0.handle, dofmap1.handle, h), "fe_sparsity_build")
         return cls(ctx, h.value)
 
     @classmethod

@@ -121,6 +121,10 @@ int fe_dofmap_destroy(fe_dofmap d);
  * unique block columns per block row) unrolled to scalar AIJ exactly as
  * la/petsc.cpp:45-65 does.  Built on the host from the dofmaps. */
 int fe_sparsity_build(fe_dofmap rows, fe_dofmap cols, fe_sparsity* out);
+/* The same pattern built on the device (radix sort + unique of the cell
+ * couplings, then the same unroll), bit-exact with fe_sparsity_build; for
+ * callers that create many meshes.  Synchronises `stream`. */
+int fe_sparsity_build_device(fe_dofmap rows, fe_dofmap cols, void* stream, fe_sparsity* out);
 /* Adopt an existing pattern (e.g. the arrays of a PETSc AIJ matrix); host arrays. */
 int fe_sparsity_create(fe_context ctx, const int32_t* row_ptr, const int32_t* col,
                        int64_t num_rows, int64_t num_cols, fe_sparsity* out);
