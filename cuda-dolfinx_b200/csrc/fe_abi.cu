@@ -69,10 +69,15 @@ int form_rank(int kind) {
     case FE_FORM_P1_STIFFNESS:
     case FE_FORM_P2_STIFFNESS:
     case FE_FORM_VP2_ELASTICITY:
+    case FE_FORM_P1_FACET_MASS:
+    case FE_FORM_P2_FACET_MASS:
       return 2;
     case FE_FORM_P1_LOAD:
     case FE_FORM_P2_LOAD:
     case FE_FORM_VP2_LOAD:
+    case FE_FORM_P1_FACET_LOAD:
+    case FE_FORM_P2_FACET_LOAD:
+    case FE_FORM_VP2_FACET_LOAD:
       return 1;
     default:
       return 0;
@@ -84,10 +89,14 @@ void form_space(int kind, int& k, int& bs) {
   switch (kind) {
     case FE_FORM_P1_STIFFNESS:
     case FE_FORM_P1_LOAD:
+    case FE_FORM_P1_FACET_MASS:
+    case FE_FORM_P1_FACET_LOAD:
       k = 4, bs = 1;
       return;
     case FE_FORM_P2_STIFFNESS:
     case FE_FORM_P2_LOAD:
+    case FE_FORM_P2_FACET_MASS:
+    case FE_FORM_P2_FACET_LOAD:
       k = 10, bs = 1;
       return;
     default:
@@ -408,7 +417,7 @@ int fe_form_set_coefficient(fe_form f, int index, int coeff_kind, fe_dofmap cmap
     const int ncoef = (f->kind == FE_FORM_VP2_ELASTICITY) ? 2 : 1;
     FE_REQUIRE(index >= 0 && index < ncoef, "coefficient index out of range");
     FE_REQUIRE(values, "null values");
-    const int ncomp = (f->kind == FE_FORM_VP2_LOAD) ? 3 : 1;
+    const int ncomp = (f->kind == FE_FORM_VP2_LOAD || f->kind == FE_FORM_VP2_FACET_LOAD) ? 3 : 1;
     Coefficient& c = f->coeff[index];
     const int64_t C = f->mesh->num_cells;
     if (coeff_kind == FE_COEFF_CONSTANT) {
@@ -425,13 +434,15 @@ int fe_form_set_coefficient(fe_form f, int index, int coeff_kind, fe_dofmap cmap
     } else if (coeff_kind == FE_COEFF_P1) {
       FE_REQUIRE(cmap && cmap->k == 4 && cmap->bs == 1 && cmap->num_cells == C, "P1 coefficient needs a P1 dofmap");
       FE_REQUIRE(n >= cmap->num_blocks, "P1 coefficient has fewer values than dofs");
-      FE_REQUIRE(f->kind == FE_FORM_P2_STIFFNESS || f->kind == FE_FORM_P1_LOAD,
-                 "P1 coefficients are supported by P2 stiffness and P1 load forms");
+      FE_REQUIRE(f->kind == FE_FORM_P2_STIFFNESS || f->kind == FE_FORM_P1_LOAD ||
+                     f->kind == FE_FORM_P1_FACET_LOAD || f->kind == FE_FORM_P2_FACET_LOAD,
+                 "P1 coefficients are supported by P2 stiffness, P1 load and facet load forms");
     } else {
       FE_FAIL(FE_ERR_ARG, "unknown coefficient kind " + std::to_string(coeff_kind));
     }
     if (f->kind == FE_FORM_P1_STIFFNESS || f->kind == FE_FORM_VP2_ELASTICITY || f->kind == FE_FORM_P2_LOAD ||
-        f->kind == FE_FORM_VP2_LOAD)
+        f->kind == FE_FORM_VP2_LOAD || f->kind == FE_FORM_P1_FACET_MASS || f->kind == FE_FORM_P2_FACET_MASS ||
+        f->kind == FE_FORM_VP2_FACET_LOAD)
       FE_REQUIRE(coeff_kind != FE_COEFF_P1, "this form takes constant or DG0 coefficients");
     c.kind = coeff_kind;
     c.map = (coeff_kind == FE_COEFF_P1) ? cmap : nullptr;
@@ -444,6 +455,21 @@ int fe_form_set_coefficient(fe_form f, int index, int coeff_kind, fe_dofmap cmap
       FE_CUDA(cudaMemcpyAsync(c.own.p, values, n * sizeof(double), cudaMemcpyHostToDevice, as_stream(stream)));
       c.values = c.own.p;
     }
+  });
+}
+
+int fe_form_set_facets(fe_form f, const int32_t* pairs, int64_t num_facets) {
+  return guard([&] {
+    FE_REQUIRE(f, "null form");
+    FE_REQUIRE(is_facet_kind(f->kind), "not an exterior-facet form");
+    FE_REQUIRE(num_facets >= 0 && (pairs || num_facets == 0), "invalid facet list");
+    DeviceScope d(f->ctx);
+    const int64_t C = f->mesh->num_cells;
+    for (int64_t q = 0; q < num_facets; ++q)
+      if (pairs[2 * q] < 0 || pairs[2 * q] >= C || pairs[2 * q + 1] < 0 || pairs[2 * q + 1] > 3)
+        FE_FAIL(FE_ERR_ARG, "facet " + std::to_string(q) + " is not a (cell, local facet 0..3) pair of the mesh");
+    upload(f->facets, pairs, (size_t)(2 * num_facets));
+    f->num_facets = num_facets;
   });
 }
 
@@ -545,6 +571,16 @@ int fe_assemble_matrix(fe_form a, double* values, fe_bc bc0, fe_bc bc1, double d
     if (bc1) FE_REQUIRE(bc1->num_dofs == a->sp->num_cols, "bc1 size differs from the number of columns");
     cudaStream_t st = as_stream(stream);
     const bool zero = (flags & FE_ASM_ZERO) != 0;
+    if (is_facet_kind(a->kind)) {
+      FE_REQUIRE(!(flags & (FE_ASM_DETERMINISTIC | FE_ASM_SORTED_SLOT | FE_ASM_TILE | FE_ASM_ROW_GATHER |
+                            FE_ASM_BLOCK)),
+                 "exterior-facet forms assemble with the atomic scatter only");
+      FE_REQUIRE(a->V0 == a->V1, "exterior-facet mass forms need the same test and trial dofmap");
+      if (zero) launch_zero(values, a->sp->nnz, st);
+      assemble_matrix_facets(*a, values, bc0, bc1, st);
+      if (bc0) launch_set_diagonal(*a->sp, *bc0, diagonal, values, st);
+      return;
+    }
     if (flags & FE_ASM_SORTED_SLOT) {
       assemble_matrix_gather(*a, values, bc0, bc1, diagonal, zero, st);
       return;
@@ -648,6 +684,10 @@ int fe_assemble_vector(fe_form Lf, double* b, unsigned flags, void* stream) {
     cudaStream_t st = as_stream(stream);
     const int64_t n = scalar_size(Lf->V0);
     if (flags & FE_ASM_ZERO) launch_zero(b, n, st);
+    if (is_facet_kind(Lf->kind)) {
+      assemble_vector_facets(*Lf, b, n, st);
+      return;
+    }
     VecLaunch L{};
     L.kind = Lf->kind;
     L.num_cells = Lf->mesh->num_cells;
@@ -677,6 +717,10 @@ int fe_apply_lifting(double* b, int num_forms, const fe_form* a, const fe_bc* bc
       if (!bc) continue;
       DeviceScope d(f->ctx);
       FE_REQUIRE(bc->num_dofs == scalar_size(f->V1), "bc size differs from the trial space size");
+      if (is_facet_kind(f->kind)) {
+        lifting_facets(*f, *bc, x0 ? x0[i] : nullptr, scale, b, scalar_size(f->V0), st);
+        continue;
+      }
       const int need = (f->kind == FE_FORM_VP2_ELASTICITY) ? 2 : (f->kind == FE_FORM_P2_STIFFNESS ? 1 : 0);
       for (int q = 0; q < need; ++q) FE_REQUIRE(f->coeff[q].kind >= 0, "coefficient not set");
       auto& cells = lift_cells(*bc, *f->V1, st);

@@ -153,6 +153,8 @@ struct fe_form_s {
   fe::Coefficient coeff[2];
   fe_sparsity sp = nullptr;
   fe::DevBuf<uint8_t> pos;       // [num_cells * k0 * k1] block column positions (padded to 16 B)
+  fe::DevBuf<int32_t> facets;    // exterior-facet forms: [num_facets][2] (cell, local facet)
+  int64_t num_facets = 0;
   // deterministic sorted-slot plan (fe_gather.cu); built on first use
   struct Gather;
   std::unique_ptr<Gather> gather;
@@ -325,6 +327,14 @@ bool block_supported(const fe_form_s& f);
 void reset_block_plan(fe_form_s& f);
 void assemble_matrix_block(fe_form_s& f, double* values, const fe_bc_s* bc0, const fe_bc_s* bc1, bool zero,
                            cudaStream_t s);
+
+// exterior-facet forms (fe_facet.cu)
+bool is_facet_kind(int kind);
+void assemble_matrix_facets(const fe_form_s& f, double* values, const fe_bc_s* bc0, const fe_bc_s* bc1,
+                            cudaStream_t s);
+void assemble_vector_facets(const fe_form_s& f, double* b, int64_t num_values, cudaStream_t s);
+void lifting_facets(const fe_form_s& f, const fe_bc_s& bc, const double* x0, double scale, double* b,
+                    int64_t num_values, cudaStream_t s);
 
 // device pattern build (fe_sparsity_dev.cu): fills num_rows/num_cols/nnz,
 // row_ptr, col, diag and host_row_ptr of `sp`

@@ -159,6 +159,83 @@ def sym_pair(fn, s, i, j):
     return v
 
 
+FACETS = ((1, 2, 3), (0, 2, 3), (0, 1, 3), (0, 1, 2))  # facet f opposite vertex f
+
+
+def bary_basis(degree):
+    """Basis functions as polynomials in the four barycentric coordinates."""
+    lam = [{tuple(1 if q == m else 0 for q in range(4)): Fraction(1)} for m in range(4)]
+
+    def mul(p, q):
+        r = {}
+        for k1, v1 in p.items():
+            for k2, v2 in q.items():
+                k = tuple(a + b for a, b in zip(k1, k2))
+                r[k] = r.get(k, 0) + v1 * v2
+        return {k: v for k, v in r.items() if v != 0}
+
+    if degree == 1:
+        return lam, lam, mul
+    vert = []
+    for m in range(4):
+        p = {k: 2 * v for k, v in mul(lam[m], lam[m]).items()}
+        for k, v in lam[m].items():
+            p[k] = p.get(k, 0) - v
+        vert.append(p)
+    edge = [{k: 4 * v for k, v in mul(lam[a], lam[b]).items()} for a, b in EDGES]
+    return vert + edge, lam, mul
+
+
+def bary_facet_int(p, f):
+    """int_F p / |F| for p in barycentric monomials: 2 a! b! c! / (a+b+c+2)!,
+    lambda_f = 0 on facet f."""
+    tot = Fraction(0)
+    for k, v in p.items():
+        if k[f]:
+            continue
+        e = [k[m] for m in range(4) if m != f]
+        tot += v * Fraction(2 * factorial(e[0]) * factorial(e[1]) * factorial(e[2]), factorial(sum(e) + 2))
+    return tot
+
+
+def facet_tables() -> str:
+    """Exterior-facet reference tensors, per local facet f, over the cell-local
+    dofs that lie on f (the others vanish there): mass int phi_i phi_j / |F|,
+    load int phi_i / |F| and P1-weighted load int lambda_m phi_i / |F|.
+    Compiled only where FE_FACET_TABLES is defined."""
+    out = ["#ifdef FE_FACET_TABLES\n"]
+    for degree in (1, 2):
+        phi, lam, mul = bary_basis(degree)
+        k = len(phi)
+        on = []
+        for f in range(4):
+            verts = [v for v in range(4) if v != f]
+            dofs = list(verts)
+            if degree == 2:
+                dofs += [4 + e for e, (a, b) in enumerate(EDGES) if f not in (a, b)]
+            on.append(dofs)
+        nd = len(on[0])
+        P = f"P{degree}"
+        out.append(f"// cell-local dofs on each facet ({P})\n")
+        out.append(f"static __constant__ int kFacetDofs{P}[4][{nd}] = {{" +
+                   ", ".join("{" + ", ".join(str(d) for d in on[f]) + "}" for f in range(4)) + "};\n")
+        mass = [[[bary_facet_int(mul(phi[on[f][a]], phi[on[f][b]]), f) for b in range(nd)] for a in range(nd)]
+                for f in range(4)]
+        load = [[bary_facet_int(phi[on[f][a]], f) for a in range(nd)] for f in range(4)]
+        wl = [[[bary_facet_int(mul(lam[m], phi[on[f][a]]), f) for a in range(nd)] for m in range(4)]
+              for f in range(4)]
+        out.append(f"static __constant__ double kFacetMass{P}[4][{nd}][{nd}] = {{" +
+                   ", ".join("{" + ", ".join("{" + ", ".join(lit(x) for x in row) + "}" for row in mass[f]) + "}"
+                             for f in range(4)) + "};\n")
+        out.append(f"static __constant__ double kFacetLoad{P}[4][{nd}] = {{" +
+                   ", ".join("{" + ", ".join(lit(x) for x in load[f]) + "}" for f in range(4)) + "};\n")
+        out.append(f"static __constant__ double kFacetLoadW{P}[4][4][{nd}] = {{" +
+                   ", ".join("{" + ", ".join("{" + ", ".join(lit(x) for x in row) + "}" for row in wl[f]) + "}"
+                             for f in range(4)) + "};\n")
+    out.append("#endif  // FE_FACET_TABLES\n\n")
+    return "".join(out)
+
+
 def gen() -> str:
     out = []
     w = out.append
@@ -234,6 +311,7 @@ def gen() -> str:
                 exprs[(i, j)] = sum_expr('W', terms, 2)
         w(full_body(exprs, 10) if full else symmetric_body(exprs, 10))
         w("}\n\n")
+    w(facet_tables())
     w("}  // namespace fe\n")
     return "".join(out)
 

@@ -235,6 +235,7 @@ class FormSpec:
     coefficients: list = field(default_factory=list)
     rank: int = 2
     precision: str = "fp64"
+    facets: Optional[np.ndarray] = None  # exterior-facet forms: [F, 2] (cell, local facet)
 
     @property
     def function_spaces(self):
@@ -258,6 +259,42 @@ def elasticity(V: FunctionSpace, lam: Coefficient, mu: Coefficient, precision: s
     if V.bs != 3 or V.degree != 2:
         raise ValueError("elasticity needs a vector P2 space")
     return FormSpec("VP2_ELASTICITY", V, [lam, mu], 2, precision)
+
+
+# facet f of a tetrahedron is the one opposite vertex f (basix / DOLFINx)
+_TET_FACETS = np.array([[1, 2, 3], [0, 2, 3], [0, 1, 3], [0, 1, 2]])
+
+
+def exterior_facets(mesh: "Mesh") -> np.ndarray:
+    """(cell, local facet) pairs of the boundary facets -- the facets that
+    belong to one cell only -- ordered by cell then local facet (the
+    exterior-facet integration domain DOLFINx hands the reference,
+    CUDAFormIntegral.cpp:361-447)."""
+    cells = mesh.cells
+    F = np.sort(cells[:, _TET_FACETS], axis=2).reshape(-1, 3)
+    _, inv, cnt = np.unique(F, axis=0, return_inverse=True, return_counts=True)
+    ext = np.nonzero(cnt[inv.ravel()] == 1)[0]
+    return np.ascontiguousarray(np.stack([ext // 4, ext % 4], axis=1).astype(np.int32))
+
+
+def facet_mass(V: FunctionSpace, alpha: Coefficient = 1.0, facets: Optional[np.ndarray] = None) -> FormSpec:
+    """alpha * u * v * ds over exterior facets (Robin term) on scalar P1/P2;
+    alpha constant or DG0 (the value of the facet's cell)."""
+    if V.bs != 1 or V.family != "P":
+        raise ValueError("facet_mass needs a scalar Lagrange space")
+    facets = exterior_facets(V.mesh) if facets is None else np.ascontiguousarray(facets, dtype=np.int32)
+    return FormSpec("P1_FACET_MASS" if V.degree == 1 else "P2_FACET_MASS", V, [alpha], 2, "fp64", facets)
+
+
+def facet_load(V: FunctionSpace, g: Coefficient, facets: Optional[np.ndarray] = None) -> FormSpec:
+    """inner(g, v) * ds over exterior facets (Neumann / traction term) on P1,
+    P2 or vector P2; g constant, DG0 or (scalar) P1."""
+    facets = exterior_facets(V.mesh) if facets is None else np.ascontiguousarray(facets, dtype=np.int32)
+    if V.bs == 3:
+        kind = "VP2_FACET_LOAD"
+    else:
+        kind = "P1_FACET_LOAD" if V.degree == 1 else "P2_FACET_LOAD"
+    return FormSpec(kind, V, [g], 1, "fp64", facets)
 
 
 def load(V: FunctionSpace, f: Coefficient) -> FormSpec:

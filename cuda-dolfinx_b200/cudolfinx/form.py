@@ -99,6 +99,10 @@ class CUDAForm:
         _lib.check(_lib.lib.fe_form_create(self._ctx.handle, _lib.FORM[form.kind], self._cuda_mesh.handle,
                                            self._dofmaps[0].handle, trial, h), "fe_form_create")
         self._handle = h.value
+        if form.facets is not None:
+            fc = np.ascontiguousarray(form.facets, dtype=np.int32)
+            self._facets = fc
+            _lib.check(_lib.lib.fe_form_set_facets(self._handle, fc.ctypes.data, len(fc)), "fe_form_set_facets")
         if form.precision == "fp32":
             _lib.check(_lib.lib.fe_form_set_precision(self._handle, _lib.PREC_FP32), "fe_form_set_precision")
         self._bound_sparsity = None
@@ -109,7 +113,7 @@ class CUDAForm:
     # -- coefficients -------------------------------------------------------
     def _set_coefficient(self, i: int, c):
         ctx = self._ctx
-        ncomp = 3 if self._spec.kind == "VP2_LOAD" else 1
+        ncomp = 3 if self._spec.kind in ("VP2_LOAD", "VP2_FACET_LOAD") else 1
         C = self._spec.mesh.num_cells
         if isinstance(c, Function):
             V = c.function_space

@@ -55,7 +55,14 @@ enum fe_form_kind {
                                   coeff 0 = lam, coeff 1 = mu                       */
   FE_FORM_P1_LOAD = 11,        /* f*v*dx, P1;        coeff 0 = f                    */
   FE_FORM_P2_LOAD = 12,        /* f*v*dx, P2;        coeff 0 = f                    */
-  FE_FORM_VP2_LOAD = 13        /* inner(f, v)*dx, vector P2; coeff 0 = f (3 comps)  */
+  FE_FORM_VP2_LOAD = 13,       /* inner(f, v)*dx, vector P2; coeff 0 = f (3 comps)  */
+  /* exterior-facet (ds) forms over the facets given by fe_form_set_facets
+   * (CUDAFormIntegral.cpp:361-447 vector, :1667-1793 matrix, :721-837 lifting) */
+  FE_FORM_P1_FACET_MASS = 4,   /* alpha*u*v*ds, P1;  coeff 0 = alpha (constant / DG0 of the facet's cell) */
+  FE_FORM_P2_FACET_MASS = 5,   /* alpha*u*v*ds, P2;  coeff 0 = alpha                 */
+  FE_FORM_P1_FACET_LOAD = 14,  /* g*v*ds, P1;        coeff 0 = g (constant / DG0 / P1) */
+  FE_FORM_P2_FACET_LOAD = 15,  /* g*v*ds, P2;        coeff 0 = g (constant / DG0 / P1) */
+  FE_FORM_VP2_FACET_LOAD = 16  /* inner(t, v)*ds, vector P2; coeff 0 = t (3 comps)   */
 };
 
 /* Coefficient representations (CUDAFormCoefficients.h:352-365 packs these
@@ -156,6 +163,11 @@ int fe_form_set_coefficient(fe_form f, int index, int coeff_kind, fe_dofmap cmap
                             const double* values, int64_t n, int values_on_device,
                             void* stream);
 int fe_form_set_precision(fe_form f, int precision);
+/* Integration domain of an exterior-facet form: num_facets (cell, local
+ * facet) pairs, int32[2*num_facets] host array; local facet f is the facet
+ * opposite vertex f of the cell (the pairs DOLFINx packs for the reference's
+ * active_mesh_entities, CUDAFormIntegral.cpp:361-447). */
+int fe_form_set_facets(fe_form f, const int32_t* cell_facet_pairs, int64_t num_facets);
 /* Bind the matrix pattern and build the cell-to-slot map once (the reference's
  * unused lookup-table prototype, CUDAFormIntegral.cpp:1230-1407, made the
  * default).  Fails with FE_ERR_PATTERN if a cell coupling is missing. */

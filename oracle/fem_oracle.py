@@ -153,6 +153,122 @@ def ref_basis_integrals(degree: int):
 
 
 # ---------------------------------------------------------------------------
+# Exterior-facet reference tensors (ds integrals)
+# ---------------------------------------------------------------------------
+# facet i of a tetrahedron is the one opposite vertex i (basix / DOLFINx
+# sub-entity numbering); the reference passes exterior facets as (cell, local
+# facet) pairs (CUDAFormIntegral.cpp:361-447, active_mesh_entities).
+TET_FACETS = ((1, 2, 3), (0, 2, 3), (0, 1, 3), (0, 1, 2))
+
+
+def _bary_basis(degree):
+    """Basis functions as polynomials in the four barycentric coordinates:
+    dict {(e0, e1, e2, e3): coefficient}."""
+    lam = [{tuple(1 if q == m else 0 for q in range(4)): Fraction(1)} for m in range(4)]
+
+    def mul(p, q):
+        r = {}
+        for k1, v1 in p.items():
+            for k2, v2 in q.items():
+                k = tuple(a + b for a, b in zip(k1, k2))
+                r[k] = r.get(k, 0) + v1 * v2
+        return {k: v for k, v in r.items() if v != 0}
+
+    if degree == 1:
+        return lam, mul
+    vert = []
+    for m in range(4):
+        p = {k: 2 * v for k, v in mul(lam[m], lam[m]).items()}
+        for k, v in lam[m].items():
+            p[k] = p.get(k, 0) - v
+        vert.append(p)
+    edge = [{k: 4 * v for k, v in mul(lam[a], lam[b]).items()} for a, b in TET_EDGES]
+    return vert + edge, mul
+
+
+def _facet_int(p, f):
+    """int over facet f of p, divided by the facet area: barycentric monomials
+    integrate to 2 a! b! c! / (a + b + c + 2)! on a triangle; lambda_f = 0 there."""
+    tot = Fraction(0)
+    for k, v in p.items():
+        if k[f]:
+            continue
+        e = [k[m] for m in range(4) if m != f]
+        tot += v * Fraction(2 * factorial(e[0]) * factorial(e[1]) * factorial(e[2]), factorial(sum(e) + 2))
+    return tot
+
+
+@lru_cache(maxsize=None)
+def facet_ref_tensors(degree: int):
+    """For each local facet f: mass M[f,i,j] = int_F phi_i phi_j / |F|,
+    load l[f,i] = int_F phi_i / |F|, weighted load w[f,m,i] = int_F lambda_m phi_i / |F|."""
+    phi, mul = _bary_basis(degree)
+    lam = [{tuple(1 if q == m else 0 for q in range(4)): Fraction(1)} for m in range(4)]
+    k = len(phi)
+    M = np.zeros((4, k, k))
+    l = np.zeros((4, k))
+    w = np.zeros((4, 4, k))
+    for f in range(4):
+        for i in range(k):
+            l[f, i] = float(_facet_int(phi[i], f))
+            for j in range(k):
+                M[f, i, j] = float(_facet_int(mul(phi[i], phi[j]), f))
+            for m in range(4):
+                w[f, m, i] = float(_facet_int(mul(lam[m], phi[i]), f))
+    return M, l, w
+
+
+def exterior_facets(cells):
+    """(cell, local facet) pairs of the facets that belong to one cell only,
+    ordered by cell then local facet."""
+    F = np.sort(cells[:, np.array(TET_FACETS)], axis=2).reshape(-1, 3)
+    _, inv, cnt = np.unique(F, axis=0, return_inverse=True, return_counts=True)
+    ext = np.nonzero(cnt[inv.ravel()] == 1)[0]
+    return np.stack([ext // 4, ext % 4], axis=1).astype(np.int32)
+
+
+def facet_areas(coords, cells, facets):
+    v = cells[facets[:, 0][:, None], np.array(TET_FACETS)[facets[:, 1]]]  # [F, 3]
+    a, b, c = coords[v[:, 0]], coords[v[:, 1]], coords[v[:, 2]]
+    return 0.5 * np.linalg.norm(np.cross(b - a, c - a), axis=1)
+
+
+def facet_mass(coords, cells, facets, degree, alpha=None):
+    """Element matrices [F, k, k] of alpha * u * v * ds on cell-local dofs
+    (alpha constant or one value per cell of the facet)."""
+    M, _, _ = facet_ref_tensors(degree)
+    area = facet_areas(coords, cells, facets)
+    s = area if alpha is None else area * np.broadcast_to(np.asarray(alpha, dtype=float), area.shape)
+    return s[:, None, None] * M[facets[:, 1]]
+
+
+def facet_load(coords, cells, facets, degree, g=None, g_kind="constant", p1_cells=None):
+    """Element vectors [F, k] of g * v * ds; g: constant, 'dg0' (one value per
+    cell, indexed by the facet's cell) or 'p1' (vertex values; p1_cells gives
+    the cells' P1 dofs)."""
+    _, l, w = facet_ref_tensors(degree)
+    area = facet_areas(coords, cells, facets)
+    f = facets[:, 1]
+    if g_kind == "p1":
+        gv = np.asarray(g)[p1_cells[facets[:, 0]]]  # [F, 4]
+        return area[:, None] * np.einsum("fm,fmi->fi", gv, w[f])
+    if g_kind == "dg0":
+        gc = np.asarray(g)[facets[:, 0]]
+    else:
+        gc = np.full(len(facets), 1.0 if g is None else float(g))
+    return (area * gc)[:, None] * l[f]
+
+
+def facet_vector_load(coords, cells, facets, t):
+    """Element vectors [F, 30] (interleaved dof*3 + comp) of t . v ds on vector
+    P2, t a constant 3-vector."""
+    _, l, _ = facet_ref_tensors(2)
+    area = facet_areas(coords, cells, facets)
+    be = (area[:, None] * l[facets[:, 1]])[:, :, None] * np.asarray(t, dtype=float)[None, None, :]
+    return be.reshape(len(facets), 30)
+
+
+# ---------------------------------------------------------------------------
 # Mesh and dofmaps
 # ---------------------------------------------------------------------------
 

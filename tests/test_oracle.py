@@ -161,3 +161,35 @@ def test_c_port_matches_numpy_oracle(kind, n):
     C.close()
     assert np.abs(v - S["A"]).max() <= 1e-13 * np.abs(S["A"]).max()
     assert np.abs(b - S["b"]).max() <= 1e-13 * max(1.0, np.abs(S["b"]).max())
+
+
+def test_exterior_facets_and_facet_tensors():
+    for n in (1, 2, 3):
+        coords, cells = fo.unit_cube_tet_mesh(n)
+        F = fo.exterior_facets(cells)
+        assert len(F) == 12 * n * n
+        assert abs(fo.facet_areas(coords, cells, F).sum() - 6.0) < 1e-12
+    coords, cells = fo.unit_cube_tet_mesh(3)
+    F = fo.exterior_facets(cells)
+    # sum of the facet mass = boundary area; P1 / P2 loads integrate g exactly
+    for deg in (1, 2):
+        M = fo.facet_mass(coords, cells, F, deg)
+        assert abs(M.sum() - 6.0) < 1e-12
+        assert np.allclose(M, np.transpose(M, (0, 2, 1)))
+        assert abs(fo.facet_load(coords, cells, F, deg, 2.0).sum() - 12.0) < 1e-12
+    # g = x + y + z as a P1 field: int_boundary g ds = 9 on the unit cube
+    g = coords.sum(axis=1)
+    for deg in (1, 2):
+        b = fo.facet_load(coords, cells, F, deg, g, "p1", p1_cells=cells)
+        assert abs(b.sum() - 9.0) < 1e-12
+    t = fo.facet_vector_load(coords, cells, F, (1.0, -2.0, 0.5))
+    assert np.allclose(t.reshape(len(F), 10, 3).sum(axis=(0, 1)), 6.0 * np.array([1.0, -2.0, 0.5]))
+
+
+def test_exterior_facets_match_mirror_helper():
+    from conftest import ensure_library  # noqa: F401
+    from cudolfinx import fem
+    for n in (2, 3):
+        coords, cells = fo.unit_cube_tet_mesh(n)
+        mesh = fem.create_unit_cube(n)
+        assert np.array_equal(fem.exterior_facets(mesh), fo.exterior_facets(cells))
