@@ -79,8 +79,13 @@ int form_rank(int kind) {
     case FE_FORM_P2_FACET_LOAD:
     case FE_FORM_VP2_FACET_LOAD:
       return 1;
-    default:
+    case FE_FORM_INTEGRAL:
+    case FE_FORM_P1_ENERGY:
+    case FE_FORM_P2_ENERGY:
+    case FE_FORM_FACET_INTEGRAL:
       return 0;
+    default:
+      return -1;
   }
 }
 
@@ -385,10 +390,11 @@ int fe_sparsity_destroy(fe_sparsity s) {
 int fe_form_create(fe_context ctx, int form_kind, fe_mesh mesh, fe_dofmap test, fe_dofmap trial, fe_form* out) {
   return guard([&] {
     DeviceScope d(ctx);
-    FE_REQUIRE(out && mesh && test, "null argument");
     const int rank = form_rank(form_kind);
-    FE_REQUIRE(rank > 0, "unknown form kind " + std::to_string(form_kind));
-    FE_REQUIRE((rank == 2) == (trial != nullptr), "bilinear forms need a trial dofmap, linear forms none");
+    FE_REQUIRE(rank >= 0, "unknown form kind " + std::to_string(form_kind));
+    FE_REQUIRE(out && mesh && (test || rank == 0), "null argument");
+    FE_REQUIRE((rank == 2) == (trial != nullptr), "bilinear forms need a trial dofmap, others none");
+    FE_REQUIRE(rank > 0 || test == nullptr, "functionals take no test dofmap");
     int k = 0, bs = 0;
     form_space(form_kind, k, bs);
     for (fe_dofmap V : {test, trial}) {
@@ -414,7 +420,8 @@ int fe_form_set_coefficient(fe_form f, int index, int coeff_kind, fe_dofmap cmap
   return guard([&] {
     FE_REQUIRE(f, "null form");
     DeviceScope d(f->ctx);
-    const int ncoef = (f->kind == FE_FORM_VP2_ELASTICITY) ? 2 : 1;
+    const int ncoef =
+        (f->kind == FE_FORM_VP2_ELASTICITY || f->kind == FE_FORM_P1_ENERGY || f->kind == FE_FORM_P2_ENERGY) ? 2 : 1;
     FE_REQUIRE(index >= 0 && index < ncoef, "coefficient index out of range");
     FE_REQUIRE(values, "null values");
     const int ncomp = (f->kind == FE_FORM_VP2_LOAD || f->kind == FE_FORM_VP2_FACET_LOAD) ? 3 : 1;
@@ -435,8 +442,14 @@ int fe_form_set_coefficient(fe_form f, int index, int coeff_kind, fe_dofmap cmap
       FE_REQUIRE(cmap && cmap->k == 4 && cmap->bs == 1 && cmap->num_cells == C, "P1 coefficient needs a P1 dofmap");
       FE_REQUIRE(n >= cmap->num_blocks, "P1 coefficient has fewer values than dofs");
       FE_REQUIRE(f->kind == FE_FORM_P2_STIFFNESS || f->kind == FE_FORM_P1_LOAD ||
-                     f->kind == FE_FORM_P1_FACET_LOAD || f->kind == FE_FORM_P2_FACET_LOAD,
-                 "P1 coefficients are supported by P2 stiffness, P1 load and facet load forms");
+                     f->kind == FE_FORM_P1_FACET_LOAD || f->kind == FE_FORM_P2_FACET_LOAD ||
+                     f->kind == FE_FORM_INTEGRAL || f->kind == FE_FORM_FACET_INTEGRAL ||
+                     (f->kind == FE_FORM_P1_ENERGY && index == 1),
+                 "P1 coefficients are supported by P2 stiffness, P1 load, facet load and functional forms");
+    } else if (coeff_kind == FE_COEFF_P2) {
+      FE_REQUIRE(f->kind == FE_FORM_P2_ENERGY && index == 1, "P2 coefficients are the u of FE_FORM_P2_ENERGY");
+      FE_REQUIRE(cmap && cmap->k == 10 && cmap->bs == 1 && cmap->num_cells == C, "P2 coefficient needs a P2 dofmap");
+      FE_REQUIRE(n >= cmap->num_blocks, "P2 coefficient has fewer values than dofs");
     } else {
       FE_FAIL(FE_ERR_ARG, "unknown coefficient kind " + std::to_string(coeff_kind));
     }
@@ -444,8 +457,11 @@ int fe_form_set_coefficient(fe_form f, int index, int coeff_kind, fe_dofmap cmap
         f->kind == FE_FORM_VP2_LOAD || f->kind == FE_FORM_P1_FACET_MASS || f->kind == FE_FORM_P2_FACET_MASS ||
         f->kind == FE_FORM_VP2_FACET_LOAD)
       FE_REQUIRE(coeff_kind != FE_COEFF_P1, "this form takes constant or DG0 coefficients");
+    if ((f->kind == FE_FORM_P1_ENERGY || f->kind == FE_FORM_P2_ENERGY) && index == 1)
+      FE_REQUIRE(coeff_kind == (f->kind == FE_FORM_P1_ENERGY ? FE_COEFF_P1 : FE_COEFF_P2),
+                 "u of an energy functional is a P1 / P2 field");
     c.kind = coeff_kind;
-    c.map = (coeff_kind == FE_COEFF_P1) ? cmap : nullptr;
+    c.map = (coeff_kind == FE_COEFF_P1 || coeff_kind == FE_COEFF_P2) ? cmap : nullptr;
     c.n = n;
     if (values_on_device) {
       c.own.release();
@@ -461,7 +477,7 @@ int fe_form_set_coefficient(fe_form f, int index, int coeff_kind, fe_dofmap cmap
 int fe_form_set_facets(fe_form f, const int32_t* pairs, int64_t num_facets) {
   return guard([&] {
     FE_REQUIRE(f, "null form");
-    FE_REQUIRE(is_facet_kind(f->kind), "not an exterior-facet form");
+    FE_REQUIRE(is_facet_kind(f->kind) || f->kind == FE_FORM_FACET_INTEGRAL, "not an exterior-facet form");
     FE_REQUIRE(num_facets >= 0 && (pairs || num_facets == 0), "invalid facet list");
     DeviceScope d(f->ctx);
     const int64_t C = f->mesh->num_cells;
@@ -664,6 +680,19 @@ int fe_assemble_matrix_batch(fe_form a, int num_instances, const double* const* 
     DeviceScope d(a->ctx);
     assemble_matrix_batch(*a, num_instances, coefficients, values, bc0, bc1, diagonal, (flags & FE_ASM_ZERO) != 0,
                           as_stream(stream));
+  });
+}
+
+int fe_assemble_scalar(fe_form M, double* result, void* stream) {
+  return guard([&] {
+    FE_REQUIRE(M && result, "null argument");
+    FE_REQUIRE(M->rank == 0 && is_scalar_kind(M->kind), "assemble_scalar needs a functional");
+    if (M->kind == FE_FORM_INTEGRAL || M->kind == FE_FORM_FACET_INTEGRAL)
+      FE_REQUIRE(M->coeff[0].kind >= 0, "coefficient 0 is not set");
+    if (M->kind == FE_FORM_P1_ENERGY || M->kind == FE_FORM_P2_ENERGY)
+      FE_REQUIRE(M->coeff[1].kind >= 0, "coefficient 1 (u) is not set");
+    DeviceScope d(M->ctx);
+    *result = assemble_scalar(*M, as_stream(stream));
   });
 }
 

@@ -155,6 +155,7 @@ struct fe_form_s {
   fe::DevBuf<uint8_t> pos;       // [num_cells * k0 * k1] block column positions (padded to 16 B)
   fe::DevBuf<int32_t> facets;    // exterior-facet forms: [num_facets][2] (cell, local facet)
   int64_t num_facets = 0;
+  fe::DevBuf<double> scalar_partial;  // functionals: per-block partial sums + the result
   // deterministic sorted-slot plan (fe_gather.cu); built on first use
   struct Gather;
   std::unique_ptr<Gather> gather;
@@ -335,6 +336,10 @@ void assemble_matrix_facets(const fe_form_s& f, double* values, const fe_bc_s* b
 void assemble_vector_facets(const fe_form_s& f, double* b, int64_t num_values, cudaStream_t s);
 void lifting_facets(const fe_form_s& f, const fe_bc_s& bc, const double* x0, double scale, double* b,
                     int64_t num_values, cudaStream_t s);
+
+// functionals (fe_scalar.cu)
+bool is_scalar_kind(int kind);
+double assemble_scalar(fe_form_s& f, cudaStream_t s);
 
 // device pattern build (fe_sparsity_dev.cu): fills num_rows/num_cols/nnz,
 // row_ptr, col, diag and host_row_ptr of `sp`

@@ -33,8 +33,9 @@ FE_ERR_NOT_CONVERGED = 6
 
 # enum values (include/cudolfinx_b200.h)
 FORM = {"P1_STIFFNESS": 1, "P2_STIFFNESS": 2, "VP2_ELASTICITY": 3, "P1_LOAD": 11, "P2_LOAD": 12, "VP2_LOAD": 13,
-        "P1_FACET_MASS": 4, "P2_FACET_MASS": 5, "P1_FACET_LOAD": 14, "P2_FACET_LOAD": 15, "VP2_FACET_LOAD": 16}
-COEFF_CONSTANT, COEFF_DG0, COEFF_P1 = 0, 1, 2
+        "P1_FACET_MASS": 4, "P2_FACET_MASS": 5, "P1_FACET_LOAD": 14, "P2_FACET_LOAD": 15, "VP2_FACET_LOAD": 16,
+        "INTEGRAL": 31, "P1_ENERGY": 32, "P2_ENERGY": 33, "FACET_INTEGRAL": 34}
+COEFF_CONSTANT, COEFF_DG0, COEFF_P1, COEFF_P2 = 0, 1, 2, 3
 PREC_FP64, PREC_FP32 = 0, 1
 ASM_ZERO, ASM_DETERMINISTIC, ASM_ATOMIC, ASM_SORTED_SLOT, ASM_TILE, ASM_ROW_GATHER, ASM_BLOCK = 1, 2, 4, 8, 16, 32, 64
 ASM_FULL_SCATTER = 128
@@ -64,6 +65,7 @@ _SIGS = {
     "fe_form_set_coefficient": (i32, [vp, i32, i32, vp, vp, i64, i32, vp]),
     "fe_form_set_precision": (i32, [vp, i32]),
     "fe_form_set_facets": (i32, [vp, vp, i64]),
+    "fe_assemble_scalar": (i32, [vp, ctypes.POINTER(dbl), vp]),
     "fe_form_bind_sparsity": (i32, [vp, vp, vp]),
     "fe_form_destroy": (i32, [vp]),
     "fe_bc_create": (i32, [vp, i64, vp, vp, i64, i64, vp, PP]),

@@ -8,10 +8,11 @@ rows/columns skipped and sets ``diagonal`` on owned BC rows;
 current stream (the reference synchronises after every kernel);
 ``diagonal`` is honoured (the reference's binding always uses 1.0,
 wrappers/fem.cpp:274); ``scale`` stays double (the reference's binding
-takes a C float, wrappers/fem.cpp:335, 361); block/restricted and scalar
-assembly are outside this engine.  Additions: ``deterministic=True`` selects
-the bitwise-reproducible sorted-slot reduction, and ``solve`` runs the
-on-device Jacobi-PCG.
+takes a C float, wrappers/fem.cpp:335, 361); block/restricted assembly is outside
+this engine.  ``assemble_scalar`` returns the functional's value with a
+fixed-order reduction.  Additions: ``deterministic=True`` selects a
+bitwise-reproducible matrix variant, ``assemble_matrix_batch`` assembles many
+coefficient instances at once, and ``solve`` runs the on-device Jacobi-PCG.
 """
 from __future__ import annotations
 
@@ -166,6 +167,21 @@ class CUDAAssembler:
         for m in mats:
             m._bcs = col
         return mats
+
+    def assemble_scalar(self, b: CUDAForm, constants=None, coeffs=None) -> float:
+        """Value of a functional (assemble.py:204-226); the reduction runs in a
+        fixed order, so the value is reproducible bit for bit."""
+        if not isinstance(b, CUDAForm):
+            raise TypeError(f"Expected CUDAForm, got '{type(b)}'")
+        if b.rank != 0:
+            raise ValueError("assemble_scalar needs a functional")
+        import ctypes
+        b.to_device()  # assemble.py:220-222
+        self.pack_coefficients(b, coeffs)
+        out = ctypes.c_double(0.0)
+        _lib.check(_lib.lib.fe_assemble_scalar(b.cuda_form, ctypes.byref(out), self._ctx.stream()),
+                   "fe_assemble_scalar")
+        return out.value
 
     def assemble_vector(self, b: CUDAForm, vec: typing.Optional[CUDAVector] = None, constants=None, coeffs=None,
                         zero: bool = True) -> CUDAVector:

@@ -236,14 +236,17 @@ class FormSpec:
     rank: int = 2
     precision: str = "fp64"
     facets: Optional[np.ndarray] = None  # exterior-facet forms: [F, 2] (cell, local facet)
+    domain: Optional["Mesh"] = None      # functionals: the mesh (V may be None)
 
     @property
     def function_spaces(self):
+        if self.rank == 0:
+            return []
         return [self.V, self.V] if self.rank == 2 else [self.V]
 
     @property
     def mesh(self):
-        return self.V.mesh
+        return self.domain if self.domain is not None else self.V.mesh
 
 
 def stiffness(V: FunctionSpace, k: Coefficient = 1.0, precision: str = "fp64") -> FormSpec:
@@ -295,6 +298,27 @@ def facet_load(V: FunctionSpace, g: Coefficient, facets: Optional[np.ndarray] = 
     else:
         kind = "P1_FACET_LOAD" if V.degree == 1 else "P2_FACET_LOAD"
     return FormSpec(kind, V, [g], 1, "fp64", facets)
+
+
+def integral(f: Coefficient, mesh: Optional["Mesh"] = None) -> FormSpec:
+    """The functional int f dx; f constant (give the mesh), DG0 or P1."""
+    mesh = mesh if mesh is not None else f.function_space.mesh
+    return FormSpec("INTEGRAL", None, [f], 0, "fp64", None, mesh)
+
+
+def energy(u: "Function", k: Coefficient = 1.0) -> FormSpec:
+    """The functional int k |grad u|^2 dx for a scalar P1 or P2 Function u
+    (k constant or DG0); equals u^T A u for the stiffness matrix A."""
+    V = u.function_space
+    if V.bs != 1 or V.family != "P" or V.degree not in (1, 2):
+        raise ValueError("energy needs a scalar P1 or P2 Function")
+    return FormSpec("P1_ENERGY" if V.degree == 1 else "P2_ENERGY", None, [k, u], 0, "fp64", None, V.mesh)
+
+
+def facet_integral(g: Coefficient, mesh: "Mesh", facets: Optional[np.ndarray] = None) -> FormSpec:
+    """The functional int g ds over exterior facets; g constant, DG0 or P1."""
+    facets = exterior_facets(mesh) if facets is None else np.ascontiguousarray(facets, dtype=np.int32)
+    return FormSpec("FACET_INTEGRAL", None, [g], 0, "fp64", facets, mesh)
 
 
 def load(V: FunctionSpace, f: Coefficient) -> FormSpec:

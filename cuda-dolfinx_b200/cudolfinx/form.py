@@ -96,8 +96,9 @@ class CUDAForm:
         self._jit_args = dict(DEFAULT_CUDA_JIT_ARGS, **(jit_args or {}))
         h = _lib.out_handle()
         trial = self._dofmaps[1].handle if form.rank == 2 else None
+        test = self._dofmaps[0].handle if form.rank >= 1 else None
         _lib.check(_lib.lib.fe_form_create(self._ctx.handle, _lib.FORM[form.kind], self._cuda_mesh.handle,
-                                           self._dofmaps[0].handle, trial, h), "fe_form_create")
+                                           test, trial, h), "fe_form_create")
         self._handle = h.value
         if form.facets is not None:
             fc = np.ascontiguousarray(form.facets, dtype=np.int32)
@@ -122,6 +123,9 @@ class CUDAForm:
                 kind, cmap = _lib.COEFF_DG0, None
             elif V.degree == 1 and V.bs == 1:
                 kind, cmap = _lib.COEFF_P1, device_dofmap(ctx, V)
+                self._aux_dofmaps[i] = cmap
+            elif V.degree == 2 and V.bs == 1 and self._spec.kind == "P2_ENERGY":
+                kind, cmap = _lib.COEFF_P2, device_dofmap(ctx, V)
                 self._aux_dofmaps[i] = cmap
             else:
                 raise ValueError("coefficients must be constants, DG0 or scalar P1 Functions")

@@ -62,7 +62,13 @@ enum fe_form_kind {
   FE_FORM_P2_FACET_MASS = 5,   /* alpha*u*v*ds, P2;  coeff 0 = alpha                 */
   FE_FORM_P1_FACET_LOAD = 14,  /* g*v*ds, P1;        coeff 0 = g (constant / DG0 / P1) */
   FE_FORM_P2_FACET_LOAD = 15,  /* g*v*ds, P2;        coeff 0 = g (constant / DG0 / P1) */
-  FE_FORM_VP2_FACET_LOAD = 16  /* inner(t, v)*ds, vector P2; coeff 0 = t (3 comps)   */
+  FE_FORM_VP2_FACET_LOAD = 16, /* inner(t, v)*ds, vector P2; coeff 0 = t (3 comps)   */
+  /* functionals (rank 0, fe_assemble_scalar; CUDAFormIntegral.cpp:66-266) */
+  FE_FORM_INTEGRAL = 31,       /* int f dx;          coeff 0 = f (constant / DG0 / P1) */
+  FE_FORM_P1_ENERGY = 32,      /* int k |grad u|^2 dx; coeff 0 = k (constant / DG0),
+                                  coeff 1 = u (P1, through its P1 dofmap)           */
+  FE_FORM_P2_ENERGY = 33,      /* as P1_ENERGY with u a P2 field (FE_COEFF_P2)      */
+  FE_FORM_FACET_INTEGRAL = 34  /* int g ds over fe_form_set_facets; coeff 0 = g     */
 };
 
 /* Coefficient representations (CUDAFormCoefficients.h:352-365 packs these
@@ -70,7 +76,8 @@ enum fe_form_kind {
 enum fe_coeff_kind {
   FE_COEFF_CONSTANT = 0, /* one value (or 3 for a vector load) for all cells */
   FE_COEFF_DG0 = 1,      /* one value per cell (3 per cell for a vector load) */
-  FE_COEFF_P1 = 2        /* vertex values through a P1 dofmap                 */
+  FE_COEFF_P1 = 2,       /* vertex values through a P1 dofmap                 */
+  FE_COEFF_P2 = 3        /* P2 node values through a P2 dofmap (energy functional) */
 };
 
 /* Element-tensor precision of a matrix form. */
@@ -163,7 +170,8 @@ int fe_form_set_coefficient(fe_form f, int index, int coeff_kind, fe_dofmap cmap
                             const double* values, int64_t n, int values_on_device,
                             void* stream);
 int fe_form_set_precision(fe_form f, int precision);
-/* Integration domain of an exterior-facet form: num_facets (cell, local
+/* Integration domain of an exterior-facet form (facet kinds and
+ * FE_FORM_FACET_INTEGRAL): num_facets (cell, local
  * facet) pairs, int32[2*num_facets] host array; local facet f is the facet
  * opposite vertex f of the cell (the pairs DOLFINx packs for the reference's
  * active_mesh_entities, CUDAFormIntegral.cpp:361-447). */
@@ -206,6 +214,12 @@ int fe_assemble_matrix(fe_form a, double* values, fe_bc bc0, fe_bc bc1, double d
 int fe_assemble_matrix_batch(fe_form a, int num_instances, const double* const* coefficients,
                              double* const* values, fe_bc bc0, fe_bc bc1, double diagonal,
                              unsigned flags, void* stream);
+/* Replaces assemble_scalar_on_device (python/cudolfinx/assemble.py:204-226):
+ * the value of a functional (FE_FORM_INTEGRAL, *_ENERGY, FE_FORM_FACET_INTEGRAL)
+ * into *result (host).  The sum runs in a fixed order, so the value is
+ * bitwise reproducible on a given GPU (the reference adds per-thread partials
+ * with atomicAdd).  Synchronises `stream`. */
+int fe_assemble_scalar(fe_form M, double* result, void* stream);
 /* Replaces zero_matrix_entries / zero_vector_entries (wrappers/fem.cpp:212-222,
  * 256-266; kernel CUDAAssembler.cpp:38-56): values[0..n) = 0 on `stream`. */
 int fe_zero_entries(double* values, int64_t n, void* stream);

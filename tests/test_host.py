@@ -121,3 +121,17 @@ def test_fem_standins_match_oracle(n, jitter):
     assert np.array_equal(V1.boundary_nodes(), fo.boundary_dofs_from_grid(fo.vertex_grid_index(n), n))
     Vv = fem.functionspace(m, ("P", 2, (3,)))
     assert Vv.bs == 3 and Vv.num_dofs == 3 * nd
+
+
+def test_functional_specs_build_without_gpu():
+    from cudolfinx import fem
+    mesh = fem.create_unit_cube(2)
+    V2 = fem.functionspace(mesh, ("P", 2))
+    u = fem.Function(V2, np.ones(V2.num_dofs))
+    s = fem.energy(u, 2.0)
+    assert s.rank == 0 and s.kind == "P2_ENERGY" and s.mesh is mesh and s.function_spaces == []
+    assert fem.integral(1.0, mesh).kind == "INTEGRAL"
+    fi = fem.facet_integral(1.0, mesh)
+    assert fi.kind == "FACET_INTEGRAL" and len(fi.facets) == 12 * 4
+    with pytest.raises(ValueError):
+        fem.energy(fem.Function(fem.functionspace(mesh, ("P", 2, (3,)))))
