@@ -2,7 +2,7 @@
 """Headline benchmark: FEM system assembly on one B200 (matrix nnz/s).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload p2|p2mid|p1|p1big|vp2] [--variant auto|tile|atomic|sorted-slot]
+                    [--workload p2|p2mid|p1|p1big|vp2|p3|batch|multimesh|serve] [--variant auto|tile|atomic|sorted-slot]
 
 Default workload (the configuration the headline metric is quoted on): P2
 Poisson on the unit cube, 96^3 hexes x 6 = 5,308,416 tets, 7,189,057 dofs,
@@ -19,7 +19,7 @@ assemble call and the read-back of b (D2H) are inside the timed region.
 The CSR value array (1.64 GB) exceeds the 126 MB L2, so no flush is needed
 between steps.
 
-Multi-GPU: replicas only (the north-star path is one GPU with no ghost
+Multi-GPU: replicas only (the assembly path runs on one GPU with no ghost
 exchange); each rank assembles its own copy, value = N * nnz / max step time.
 ``--impl reference`` times the C restatement of the reference's CPU path
 (oracle/cfem.c: per-cell tabulation, binary-search CSR insertion, row-owning
@@ -56,6 +56,9 @@ WORKLOADS = {
                   desc="P1 Poisson n=128: 12,582,912 tets, k=1, f=P1(sin sin sin), homogeneous Dirichlet"),
     "vp2": dict(kind="vp2", n=64, precision="fp32",
                 desc="vector-P2 elasticity n=64: 1,572,864 jittered tets, lam/mu DG0, FP32 element tensors"),
+    "p3": dict(kind="p3", n=48, precision="fp64",
+               desc="equispaced P3 Poisson n=48: 663,552 tets, 3,048,625 dofs, k DG0 lognormal, f DG0 U[-1,1], "
+                    "g=x+y+z"),
 }
 # batched workload: many DG0-coefficient instances on one mesh and pattern
 BATCH = dict(n=48, instances=256, cpu_sample=4,
@@ -85,7 +88,7 @@ def matrix_kernels(kind: str, variant: str, big: bool = False) -> int:
     reduction (element tensors + gather + set_diagonal)."""
     if variant in ("tile", "row-gather") or (variant == "deterministic" and kind in ("p1", "p2")):
         return 2
-    if kind == "vp2" and variant in ("atomic", "auto"):
+    if kind in ("vp2", "p3") and variant in ("atomic", "auto"):
         return 4  # zero + upper-triangle scatter + lower-triangle mirror + set_diagonal
     return 3  # atomic-full, block (zero + kernel + set_diagonal), sorted-slot
 
@@ -152,6 +155,18 @@ def make_inputs(kind: str, n: int, seed: int = 0, pinned: bool = False, precisio
         W = fem.functionspace(mesh, ("DG", 0))
         k = fem.Function(V1)
         k.x.array = host(np.exp(rng.standard_normal(V1.num_dofs)))
+        f = fem.Function(W)
+        f.x.array = host(rng.uniform(-1.0, 1.0, size=C))
+        g = fem.Function(V)
+        g.x.array[:] = V.tabulate_dof_coordinates().sum(axis=1)
+        a = fem.stiffness(V, k, precision=precision)
+        L = fem.load(V, f)
+        I.update(k=k.x.array, f=f.x.array, g=g.x.array)
+    elif kind == "p3":
+        V = fem.functionspace(mesh, ("P", 3))
+        W = fem.functionspace(mesh, ("DG", 0))
+        k = fem.Function(W)
+        k.x.array = host(np.exp(rng.standard_normal(C)))
         f = fem.Function(W)
         f.x.array = host(rng.uniform(-1.0, 1.0, size=C))
         g = fem.Function(V)
@@ -311,6 +326,8 @@ def algorithmic_matrix_bytes(I, nnz):
         b += 16 * C + 8 * nnodes  # P1 coefficient: its dofmap + vertex values
     elif I["kind"] == "vp2":
         b += 16 * C  # lam, mu DG0
+    elif I["kind"] == "p3":
+        b += 8 * C  # k DG0
     return b
 
 

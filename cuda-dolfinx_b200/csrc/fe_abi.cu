@@ -71,6 +71,7 @@ int form_rank(int kind) {
     case FE_FORM_VP2_ELASTICITY:
     case FE_FORM_P1_FACET_MASS:
     case FE_FORM_P2_FACET_MASS:
+    case FE_FORM_P3_STIFFNESS:
       return 2;
     case FE_FORM_P1_LOAD:
     case FE_FORM_P2_LOAD:
@@ -78,6 +79,7 @@ int form_rank(int kind) {
     case FE_FORM_P1_FACET_LOAD:
     case FE_FORM_P2_FACET_LOAD:
     case FE_FORM_VP2_FACET_LOAD:
+    case FE_FORM_P3_LOAD:
       return 1;
     case FE_FORM_INTEGRAL:
     case FE_FORM_P1_ENERGY:
@@ -103,6 +105,10 @@ void form_space(int kind, int& k, int& bs) {
     case FE_FORM_P2_FACET_MASS:
     case FE_FORM_P2_FACET_LOAD:
       k = 10, bs = 1;
+      return;
+    case FE_FORM_P3_STIFFNESS:
+    case FE_FORM_P3_LOAD:
+      k = 20, bs = 1;
       return;
     default:
       k = 10, bs = 3;
@@ -455,7 +461,7 @@ int fe_form_set_coefficient(fe_form f, int index, int coeff_kind, fe_dofmap cmap
     }
     if (f->kind == FE_FORM_P1_STIFFNESS || f->kind == FE_FORM_VP2_ELASTICITY || f->kind == FE_FORM_P2_LOAD ||
         f->kind == FE_FORM_VP2_LOAD || f->kind == FE_FORM_P1_FACET_MASS || f->kind == FE_FORM_P2_FACET_MASS ||
-        f->kind == FE_FORM_VP2_FACET_LOAD)
+        f->kind == FE_FORM_VP2_FACET_LOAD || f->kind == FE_FORM_P3_STIFFNESS || f->kind == FE_FORM_P3_LOAD)
       FE_REQUIRE(coeff_kind != FE_COEFF_P1, "this form takes constant or DG0 coefficients");
     if ((f->kind == FE_FORM_P1_ENERGY || f->kind == FE_FORM_P2_ENERGY) && index == 1)
       FE_REQUIRE(coeff_kind == (f->kind == FE_FORM_P1_ENERGY ? FE_COEFF_P1 : FE_COEFF_P2),
@@ -493,8 +499,9 @@ int fe_form_set_precision(fe_form f, int precision) {
   return guard([&] {
     FE_REQUIRE(f, "null form");
     FE_REQUIRE(precision == FE_PREC_FP64 || precision == FE_PREC_FP32, "unknown precision");
-    FE_REQUIRE(precision == FE_PREC_FP64 || f->kind == FE_FORM_P2_STIFFNESS || f->kind == FE_FORM_VP2_ELASTICITY,
-               "FP32 element tensors are offered for P2 stiffness and vector-P2 elasticity");
+    FE_REQUIRE(precision == FE_PREC_FP64 || f->kind == FE_FORM_P2_STIFFNESS || f->kind == FE_FORM_P3_STIFFNESS ||
+                   f->kind == FE_FORM_VP2_ELASTICITY,
+               "FP32 element tensors are offered for P2 / P3 stiffness and vector-P2 elasticity");
     f->precision = precision;
   });
 }
@@ -634,14 +641,16 @@ int fe_assemble_matrix(fe_form a, double* values, fe_bc bc0, fe_bc bc1, double d
       return;
     }
     // every built-in bilinear form is symmetric: on a symmetric pattern with
-    // the same BCs on rows and columns, vector-P2 elasticity reduces each
-    // unique entry once into the upper triangle and a gather pass fills the
-    // lower triangle from it (vector P2 n=64 on B200: 7.6 ms instead of about
-    // 12 ms).  For P1/P2 the pass costs what the halved reductions save
-    // (P2 n=96: 1.58 + 0.95 ms vs 2.55 ms), so they keep both reductions, as
-    // does FE_ASM_FULL_SCATTER for every form.
-    const bool upper = zero && !(flags & FE_ASM_FULL_SCATTER) && a->kind == FE_FORM_VP2_ELASTICITY &&
-                       a->V0 == a->V1 && bc0 == bc1 && ensure_mirror(*a->sp, st);
+    // the same BCs on rows and columns, vector-P2 elasticity and P3 reduce
+    // each unique entry once into the upper triangle and a gather pass fills
+    // the lower triangle from it (on B200, vector P2 n=64: 7.6 ms instead of
+    // about 12 ms; P3 n=48: 1.79 ms instead of 2.23 ms).  For P1/P2 the pass
+    // costs what the halved reductions save (P2 n=96: 1.58 + 0.95 ms vs
+    // 2.55 ms), so they keep both reductions, as does FE_ASM_FULL_SCATTER for
+    // every form.
+    const bool upper = zero && !(flags & FE_ASM_FULL_SCATTER) &&
+                       (a->kind == FE_FORM_VP2_ELASTICITY || a->kind == FE_FORM_P3_STIFFNESS) && a->V0 == a->V1 &&
+                       bc0 == bc1 && ensure_mirror(*a->sp, st);
     if (zero) launch_zero(values, a->sp->nnz, st);
     MatLaunch L{};
     L.kind = a->kind;

@@ -264,6 +264,29 @@ __global__ void k_elem_p2(const ElemArgs a) {
 }
 
 template <typename T>
+__global__ void k_elem_p3(const ElemArgs a) {
+  const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (c >= a.num_cells) return;
+  Geo g;
+  geo(a.x, a.geom, c, g);
+  const int pa[6] = {0, 1, 2, 0, 0, 1}, pb[6] = {0, 1, 2, 1, 2, 2};
+  const double k = cellcoef(a.coef0_kind, a.c0, a.c0const, c);
+  T gq[6];
+#pragma unroll
+  for (int s = 0; s < 6; ++s) {
+    const double gh =
+        g.adet * (g.K[pa[s]][0] * g.K[pb[s]][0] + g.K[pa[s]][1] * g.K[pb[s]][1] + g.K[pa[s]][2] * g.K[pb[s]][2]);
+    gq[s] = (T)(k * gh);
+  }
+  const int64_t N = a.num_cells;
+  double* __restrict__ E = a.E;
+  p3_stiffness_const<T>(gq, [&](int i, int j, double v) {
+    E[(i * 20 + j) * N + c] = v;
+    if (i != j) E[(j * 20 + i) * N + c] = v;
+  });
+}
+
+template <typename T>
 __global__ void k_elem_vp2(const ElemArgs a) {
   const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (c >= a.num_cells) return;
@@ -398,6 +421,10 @@ void assemble_matrix_gather(fe_form_s& f, double* values, const fe_bc_s* bc0, co
       case FE_FORM_VP2_ELASTICITY:
         if (f.precision == FE_PREC_FP32) k_elem_vp2<float><<<grid, 128, 0, s>>>(ea);
         else k_elem_vp2<double><<<grid, 128, 0, s>>>(ea);
+        break;
+      case FE_FORM_P3_STIFFNESS:
+        if (f.precision == FE_PREC_FP32) k_elem_p3<float><<<grid, 128, 0, s>>>(ea);
+        else k_elem_p3<double><<<grid, 128, 0, s>>>(ea);
         break;
       default:
         FE_FAIL(FE_ERR_ARG, "not a bilinear form");

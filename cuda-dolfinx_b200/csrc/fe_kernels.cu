@@ -240,6 +240,62 @@ __global__ void __launch_bounds__(kBlock) k_mat_p2_atomic(const MatArgs a) {
 }
 
 // ---------------------------------------------------------------------------
+// P3 stiffness (20 dofs, 210 unique entries), one thread per cell, FP64
+// atomics.  The 400-byte map rows of a 64-cell tile are staged in shared
+// memory with a one-word pad per cell (101 words apart: consecutive threads
+// read different banks).
+// ---------------------------------------------------------------------------
+constexpr int kBlockP3 = 64;
+constexpr int kP3Words = 101;  // 100 map words + 1 pad word per cell
+
+template <typename T>
+__global__ void __launch_bounds__(kBlockP3) k_mat_p3_atomic(const MatArgs a) {
+  __shared__ uint32_t spw[kBlockP3 * kP3Words];
+  const int64_t c0 = blockIdx.x * (int64_t)kBlockP3;
+  const int64_t left = a.num_cells - c0;
+  const int ncell = left < kBlockP3 ? (int)left : kBlockP3;
+  {
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(a.pos + c0 * 400);
+    for (int w = threadIdx.x; w < ncell * 100; w += kBlockP3) spw[(w / 100) * kP3Words + w % 100] = __ldg(src + w);
+  }
+  __syncthreads();
+  if ((int)threadIdx.x >= ncell) return;
+  const int64_t c = c0 + threadIdx.x;
+  const uint8_t* p = reinterpret_cast<const uint8_t*>(spw + threadIdx.x * kP3Words);
+
+  CellGeo g;
+  cell_geometry(a.x, load_geom(a.geom, c), g);
+  double Gh[6];
+  ghat(g, Gh);
+
+  int rp[20], rd[20];
+  unsigned mr = 0, mc = 0;
+  const int32_t* d0 = a.dofs0 + c * 20;
+  const int32_t* d1 = a.dofs1 + c * 20;
+#pragma unroll
+  for (int i = 0; i < 20; ++i) {
+    const int r = __ldg(d0 + i);
+    rd[i] = r;
+    rp[i] = __ldg(a.row_ptr + r);
+    if (a.bc0) mr |= (__ldg(a.bc0 + r) ? 1u : 0u) << i;
+    if (a.bc1) mc |= (__ldg(a.bc1 + __ldg(d1 + i)) ? 1u : 0u) << i;
+  }
+  double* __restrict__ vals = a.values;
+  const bool upper = a.upper != 0;
+  auto emit = [&](int i, int j, double v) {
+    const bool do_ij = !upper || i == j || rd[i] < rd[j];
+    const bool do_ji = i != j && (!upper || rd[j] < rd[i]);
+    if (do_ij && !(((mr >> i) | (mc >> j)) & 1u)) atomicAdd(vals + rp[i] + p[i * 20 + j], v);
+    if (do_ji && !(((mr >> j) | (mc >> i)) & 1u)) atomicAdd(vals + rp[j] + p[j * 20 + i], v);
+  };
+  const double k = coef_cell(a.c0, c);
+  T gq[6];
+#pragma unroll
+  for (int s = 0; s < 6; ++s) gq[s] = (T)(k * Gh[s]);
+  p3_stiffness_const<T>(gq, emit);
+}
+
+// ---------------------------------------------------------------------------
 // Vector-P2 elasticity (bs = 3), one thread per cell, FP64 atomics
 // A[(i,a),(j,b)] = sum_pq W_ab[p][q] R0[p][q][i][j],
 // W_ab[p][q] = |det| (mu (delta_ab (KK^T)_pq + K_pb K_qa) + lam K_pa K_qb)
@@ -493,6 +549,21 @@ __global__ void __launch_bounds__(kBlock) k_vec_p2(const VecArgs a) {
   for (int i = 0; i < 10; ++i) add_guarded(a.b, __ldg(d + i), a.num_values, s * p2_basis_integral(i));
 }
 
+// P3 load with a DG0 / constant f: |det J| f int_ref phi_i.  The edge basis
+// functions of the equispaced cubic element integrate to exactly zero, so only
+// the vertex and face rows receive a contribution.
+__global__ void __launch_bounds__(kBlock) k_vec_p3(const VecArgs a) {
+  const int64_t c = blockIdx.x * (int64_t)kBlock + threadIdx.x;
+  if (c >= a.num_cells) return;
+  CellGeo g;
+  cell_geometry(a.x, load_geom(a.geom, c), g);
+  const double s = coef_cell(a.f, c) * g.adet;
+  const int32_t* d = a.dofs + c * 20;
+#pragma unroll
+  for (int i = 0; i < 20; ++i)
+    if (i < 4 || i >= 16) add_guarded(a.b, __ldg(d + i), a.num_values, s * p3_basis_integral(i));
+}
+
 __global__ void __launch_bounds__(kBlock) k_vec_vp2(const VecArgs a) {
   const int64_t c = blockIdx.x * (int64_t)kBlock + threadIdx.x;
   if (c >= a.num_cells) return;
@@ -601,6 +672,36 @@ __global__ void __launch_bounds__(kBlock) k_lift_p2(const LiftArgs a) {
 }
 
 template <typename T>
+__global__ void __launch_bounds__(kBlockP3) k_lift_p3(const LiftArgs a) {
+  const int64_t t = blockIdx.x * (int64_t)kBlockP3 + threadIdx.x;
+  if (t >= a.num_list) return;
+  const int64_t c = a.cells[t];
+  CellGeo g;
+  cell_geometry(a.x, load_geom(a.geom, c), g);
+  double Gh[6];
+  ghat(g, Gh);
+  double dv[20], be[20];
+  const int32_t* d0 = a.dofs0 + c * 20;
+  const int32_t* d1 = a.dofs1 + c * 20;
+#pragma unroll
+  for (int j = 0; j < 20; ++j) {
+    const int C = __ldg(d1 + j);
+    dv[j] = __ldg(a.bc1 + C) ? (__ldg(a.g + C) - (a.x0 ? __ldg(a.x0 + C) : 0.0)) : 0.0;
+    be[j] = 0.0;
+  }
+  const double k = coef_cell(a.c0, c);
+  T gq[6];
+#pragma unroll
+  for (int s = 0; s < 6; ++s) gq[s] = (T)(k * Gh[s]);
+  p3_stiffness_const<T>(gq, [&](int i, int j, double v) {
+    be[i] += v * dv[j];
+    if (i != j) be[j] += v * dv[i];
+  });
+#pragma unroll
+  for (int i = 0; i < 20; ++i) add_guarded(a.b, __ldg(d0 + i), a.num_values, -a.scale * be[i]);
+}
+
+template <typename T>
 __global__ void __launch_bounds__(kBlock) k_lift_vp2(const LiftArgs a) {
   const int64_t t = blockIdx.x * (int64_t)kBlock + threadIdx.x;
   if (t >= a.num_list) return;
@@ -657,6 +758,7 @@ __global__ void k_set_bc(double* __restrict__ b, int64_t num_values, const int32
 }
 
 unsigned grid_for(int64_t n, int block) { return (unsigned)((n + block - 1) / block); }
+
 
 }  // namespace
 
@@ -720,6 +822,15 @@ void launch_matrix_atomic(const MatLaunch& L, cudaStream_t s) {
       if (f32) k_mat_vp2_atomic<float><<<grid, kBlock, 0, s>>>(a);
       else k_mat_vp2_atomic<double><<<grid, kBlock, 0, s>>>(a);
       break;
+    case FE_FORM_P3_STIFFNESS: {
+      // one thread per cell: splitting a cell's 210 entries over 2, 4 or 8
+      // warps measured the same or slower on B200 (P3 n=48: 1.75-2.12 ms vs
+      // 1.79 ms), the reductions themselves bound the kernel
+      const unsigned g3 = grid_for(L.num_cells, kBlockP3);
+      if (f32) k_mat_p3_atomic<float><<<g3, kBlockP3, 0, s>>>(a);
+      else k_mat_p3_atomic<double><<<g3, kBlockP3, 0, s>>>(a);
+      break;
+    }
     default:
       FE_FAIL(FE_ERR_ARG, "not a bilinear form kind: " + std::to_string(L.kind));
   }
@@ -809,6 +920,9 @@ void launch_vector(const VecLaunch& L, cudaStream_t s) {
     case FE_FORM_VP2_LOAD:
       k_vec_vp2<<<grid, kBlock, 0, s>>>(a);
       break;
+    case FE_FORM_P3_LOAD:
+      k_vec_p3<<<grid, kBlock, 0, s>>>(a);
+      break;
     default:
       FE_FAIL(FE_ERR_ARG, "not a linear form kind: " + std::to_string(L.kind));
   }
@@ -851,6 +965,12 @@ void launch_lifting(const LiftLaunch& L, cudaStream_t s) {
       if (f32) k_lift_vp2<float><<<grid, kBlock, 0, s>>>(a);
       else k_lift_vp2<double><<<grid, kBlock, 0, s>>>(a);
       break;
+    case FE_FORM_P3_STIFFNESS: {
+      const unsigned g3 = grid_for(L.num_list, kBlockP3);
+      if (f32) k_lift_p3<float><<<g3, kBlockP3, 0, s>>>(a);
+      else k_lift_p3<double><<<g3, kBlockP3, 0, s>>>(a);
+      break;
+    }
     default:
       FE_FAIL(FE_ERR_ARG, "lifting needs a bilinear form, got kind " + std::to_string(L.kind));
   }

@@ -73,6 +73,32 @@ DPHI = [[pdiff(p, ax) for ax in range(3)] for p in PHI]
 UNIQ = [(i, j) for i in range(10) for j in range(i, 10)]
 
 
+def _scale(p, c):
+    return {k: c * v for k, v in p.items()}
+
+
+def _const(c):
+    return {(0, 0, 0): Fraction(c)}
+
+
+# P3 Lagrange, equispaced points (basix's "equispaced" variant): vertices,
+# then two dofs per edge in the basix edge order (the point nearer the edge's
+# first vertex first), then one dof per face (face f opposite vertex f)
+FACES = ((1, 2, 3), (0, 2, 3), (0, 1, 3), (0, 1, 2))
+PHI3 = ([_scale(pmul(l, pmul(padd(_scale(l, 3), _const(1), -1), padd(_scale(l, 3), _const(2), -1))),
+                Fraction(1, 2)) for l in LAM]
+        + [q for a, b in EDGES
+           for q in (_scale(pmul(pmul(LAM[a], LAM[b]), padd(_scale(LAM[a], 3), _const(1), -1)), Fraction(9, 2)),
+                     _scale(pmul(pmul(LAM[a], LAM[b]), padd(_scale(LAM[b], 3), _const(1), -1)), Fraction(9, 2)))]
+        + [_scale(pmul(pmul(LAM[a], LAM[b]), LAM[c]), 27) for a, b, c in FACES])
+DPHI3 = [[pdiff(p, ax) for ax in range(3)] for p in PHI3]
+UNIQ3 = [(i, j) for i in range(20) for j in range(i, 20)]
+
+
+def r3_plain(a, b, i, j):
+    return pint(pmul(DPHI3[i][a], DPHI3[j][b]))
+
+
 def lit(x: Fraction) -> str:
     """Exact-as-possible C double literal (hex float of the rounded value)."""
     return float(x).hex()
@@ -247,6 +273,29 @@ def gen() -> str:
     w("// int_ref phi_i (reference volume 1/6)\n")
     w("__device__ __forceinline__ double p2_basis_integral(int i) {\n")
     w("  return i < 4 ? " + lit(ints[0]) + " : " + lit(ints[4]) + ";\n}\n\n")
+
+    # P3: basis integrals and stiffness with a cellwise-constant coefficient
+    ints3 = [pint(p) for p in PHI3]
+    w("// int_ref phi_i of the equispaced P3 element (vertices, edge pairs, faces)\n")
+    w("__device__ __forceinline__ double p3_basis_integral(int i) {\n")
+    w("  return i < 4 ? " + lit(ints3[0]) + " : (i < 16 ? " + lit(ints3[4]) + " : " + lit(ints3[16]) + ");\n}\n\n")
+    w("// P3 stiffness with a cellwise-constant coefficient: g[s] = k * Ghat_s;\n")
+    w("// emit(i, j, value) for the 210 unique entries i <= j.\n")
+    w("template <typename T, typename Emit>\n")
+    w("__device__ __forceinline__ void p3_stiffness_const(const T* g, Emit&& emit) {\n")
+    exprs3 = {}
+    maxabs3 = Fraction(0)
+    for (i, j) in UNIQ3:
+        terms = []
+        for s_ in range(6):
+            c = sym_pair(r3_plain, s_, i, j)
+            if c != 0:
+                terms.append((s_, c))
+                maxabs3 = max(maxabs3, abs(c))
+        exprs3[(i, j)] = sum_expr('g', terms, 2)
+    w(symmetric_body(exprs3, 20))
+    w("}\n")
+    w(f"constexpr double kP3ConstTermMax = {lit(maxabs3)};\n\n")
 
     # P2 stiffness, P1 coefficient: q[m*6+s] = k_m * Ghat_s
     w("// P2 stiffness with a P1 coefficient: q[m*6+s] = k_m * Ghat_s,\n")

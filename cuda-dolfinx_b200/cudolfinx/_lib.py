@@ -34,7 +34,8 @@ FE_ERR_NOT_CONVERGED = 6
 # enum values (include/cudolfinx_b200.h)
 FORM = {"P1_STIFFNESS": 1, "P2_STIFFNESS": 2, "VP2_ELASTICITY": 3, "P1_LOAD": 11, "P2_LOAD": 12, "VP2_LOAD": 13,
         "P1_FACET_MASS": 4, "P2_FACET_MASS": 5, "P1_FACET_LOAD": 14, "P2_FACET_LOAD": 15, "VP2_FACET_LOAD": 16,
-        "INTEGRAL": 31, "P1_ENERGY": 32, "P2_ENERGY": 33, "FACET_INTEGRAL": 34}
+        "INTEGRAL": 31, "P1_ENERGY": 32, "P2_ENERGY": 33, "FACET_INTEGRAL": 34,
+        "P3_STIFFNESS": 6, "P3_LOAD": 17}
 COEFF_CONSTANT, COEFF_DG0, COEFF_P1, COEFF_P2 = 0, 1, 2, 3
 PREC_FP64, PREC_FP32 = 0, 1
 ASM_ZERO, ASM_DETERMINISTIC, ASM_ATOMIC, ASM_SORTED_SLOT, ASM_TILE, ASM_ROW_GATHER, ASM_BLOCK = 1, 2, 4, 8, 16, 32, 64

@@ -31,6 +31,16 @@ import numpy as np
 
 TET_EDGES = ((2, 3), (1, 3), (1, 2), (0, 3), (0, 2), (0, 1))
 
+# barycentric weights (in thirds) of the 20 equispaced P3 nodes in basix's
+# local order: vertices; per edge (a, b) the point nearer a, then the one
+# nearer b; per face f (opposite vertex f) its centroid
+_P3_WEIGHTS = np.array(
+    [[3 if q == v else 0 for q in range(4)] for v in range(4)]
+    + [w for a, b in TET_EDGES
+       for w in ([2 if q == a else (1 if q == b else 0) for q in range(4)],
+                 [1 if q == a else (2 if q == b else 0) for q in range(4)])]
+    + [[0 if q == f else 1 for q in range(4)] for f in range(4)], dtype=np.int64)
+
 
 class Mesh:
     """Affine tetrahedral mesh: coordinates (N,3) float64 and cells (C,4) int32."""
@@ -78,7 +88,9 @@ def create_unit_cube(n: int, jitter: float = 0.0, seed: int = 0) -> Mesh:
 
 
 class FunctionSpace:
-    """Lagrange space of degree 1 or 2 (scalar or 3-vector) on a Mesh."""
+    """Lagrange space of degree 1, 2 or 3 (scalar; degree 2 also as a
+    3-vector) on a Mesh.  Degree 3 uses equispaced points (basix's
+    "equispaced" Lagrange variant)."""
 
     def __init__(self, mesh: Mesh, element):
         family, degree = element[0], int(element[1])
@@ -104,8 +116,12 @@ class FunctionSpace:
             self._grid = None
         elif degree == 2:
             self._build_p2()
+        elif degree == 3:
+            if self.bs != 1:
+                raise ValueError("degree 3 is offered for scalar spaces")
+            self._build_p3()
         else:
-            raise ValueError("degree must be 1 or 2")
+            raise ValueError("degree must be 1, 2 or 3")
         self._uid = id(self)
 
     def _build_p2(self):
@@ -118,6 +134,22 @@ class FunctionSpace:
         g = np.stack([v % n1, (v // n1) % n1, v // (n1 * n1)], axis=-1)  # [C,4,3]
         pts = [2 * g[:, a] for a in range(4)] + [g[:, a] + g[:, b] for a, b in TET_EDGES]
         P = np.stack(pts, axis=1)
+        self.dofs = ((P[..., 2] * M + P[..., 1]) * M + P[..., 0]).astype(np.int32)
+        self.num_nodes = M ** 3
+        self._grid = (n, M)
+
+    def _build_p3(self):
+        # every point of the tripled (3n+1)^3 grid is a P3 node of this mesh
+        # (each Kuhn tet's 20 nodes are grid points, and the tets cover every
+        # point), numbered like the P2 nodes: dof = (Z*(3n+1) + Y)*(3n+1) + X
+        m = self.mesh
+        if m.grid_n is None:
+            raise ValueError("P3 spaces are built for structured unit-cube meshes")
+        n = m.grid_n
+        n1, M = n + 1, 3 * n + 1
+        v = m.cells.astype(np.int64)
+        g = np.stack([v % n1, (v // n1) % n1, v // (n1 * n1)], axis=-1)  # [C,4,3]
+        P = np.einsum("lv,cvd->cld", _P3_WEIGHTS, g)  # tripled-grid coordinates [C,20,3]
         self.dofs = ((P[..., 2] * M + P[..., 1]) * M + P[..., 0]).astype(np.int32)
         self.num_nodes = M ** 3
         self._grid = (n, M)
@@ -142,6 +174,10 @@ class FunctionSpace:
         if self.degree == 1:
             X[self.dofs.ravel()] = m.geometry_x[m.cells.ravel()]
             return X
+        if self.degree == 3:
+            P = np.einsum("lv,cvd->cld", _P3_WEIGHTS / 3.0, cx)
+            X[self.dofs.ravel()] = P.reshape(-1, 3)
+            return X
         pts = [cx[:, a] for a in range(4)] + [0.5 * (cx[:, a] + cx[:, b]) for a, b in TET_EDGES]
         X[self.dofs.ravel()] = np.stack(pts, axis=1).reshape(-1, 3)
         return X
@@ -152,10 +188,8 @@ class FunctionSpace:
         if m.grid_n is None:
             raise ValueError("boundary location needs a structured unit-cube mesh")
         n = m.grid_n
-        if self.degree == 1:
-            ext, N = n, n + 1
-        else:
-            ext, N = 2 * n, 2 * n + 1
+        ext = self.degree * n
+        N = ext + 1
         k = np.arange(N ** 3)
         ijk = np.stack([k % N, (k // N) % N, k // (N * N)], axis=1)
         return np.nonzero(np.any((ijk == 0) | (ijk == ext), axis=1))[0].astype(np.int32)
@@ -253,7 +287,7 @@ def stiffness(V: FunctionSpace, k: Coefficient = 1.0, precision: str = "fp64") -
     """k * inner(grad(u), grad(v)) * dx on a scalar P1/P2 space."""
     if V.bs != 1 or V.family != "P":
         raise ValueError("stiffness needs a scalar Lagrange space")
-    kind = "P1_STIFFNESS" if V.degree == 1 else "P2_STIFFNESS"
+    kind = {1: "P1_STIFFNESS", 2: "P2_STIFFNESS", 3: "P3_STIFFNESS"}[V.degree]
     return FormSpec(kind, V, [k], 2, precision)
 
 
@@ -283,8 +317,8 @@ def exterior_facets(mesh: "Mesh") -> np.ndarray:
 def facet_mass(V: FunctionSpace, alpha: Coefficient = 1.0, facets: Optional[np.ndarray] = None) -> FormSpec:
     """alpha * u * v * ds over exterior facets (Robin term) on scalar P1/P2;
     alpha constant or DG0 (the value of the facet's cell)."""
-    if V.bs != 1 or V.family != "P":
-        raise ValueError("facet_mass needs a scalar Lagrange space")
+    if V.bs != 1 or V.family != "P" or V.degree not in (1, 2):
+        raise ValueError("facet_mass needs a scalar P1 or P2 space")
     facets = exterior_facets(V.mesh) if facets is None else np.ascontiguousarray(facets, dtype=np.int32)
     return FormSpec("P1_FACET_MASS" if V.degree == 1 else "P2_FACET_MASS", V, [alpha], 2, "fp64", facets)
 
@@ -292,6 +326,8 @@ def facet_mass(V: FunctionSpace, alpha: Coefficient = 1.0, facets: Optional[np.n
 def facet_load(V: FunctionSpace, g: Coefficient, facets: Optional[np.ndarray] = None) -> FormSpec:
     """inner(g, v) * ds over exterior facets (Neumann / traction term) on P1,
     P2 or vector P2; g constant, DG0 or (scalar) P1."""
+    if V.family != "P" or V.degree not in (1, 2):
+        raise ValueError("facet_load needs a P1, P2 or vector-P2 space")
     facets = exterior_facets(V.mesh) if facets is None else np.ascontiguousarray(facets, dtype=np.int32)
     if V.bs == 3:
         kind = "VP2_FACET_LOAD"
@@ -322,9 +358,9 @@ def facet_integral(g: Coefficient, mesh: "Mesh", facets: Optional[np.ndarray] = 
 
 
 def load(V: FunctionSpace, f: Coefficient) -> FormSpec:
-    """inner(f, v) * dx on P1 / P2 / vector P2."""
+    """inner(f, v) * dx on P1 / P2 / P3 / vector P2."""
     if V.bs == 3:
         kind = "VP2_LOAD"
     else:
-        kind = "P1_LOAD" if V.degree == 1 else "P2_LOAD"
+        kind = {1: "P1_LOAD", 2: "P2_LOAD", 3: "P3_LOAD"}[V.degree]
     return FormSpec(kind, V, [f], 1)

@@ -56,6 +56,10 @@ enum fe_form_kind {
   FE_FORM_P1_LOAD = 11,        /* f*v*dx, P1;        coeff 0 = f                    */
   FE_FORM_P2_LOAD = 12,        /* f*v*dx, P2;        coeff 0 = f                    */
   FE_FORM_VP2_LOAD = 13,       /* inner(f, v)*dx, vector P2; coeff 0 = f (3 comps)  */
+  /* P3 Lagrange on equispaced points (20 dofs per cell: vertices, two per
+   * edge, one per face) */
+  FE_FORM_P3_STIFFNESS = 6,    /* k*inner(grad u, grad v)*dx, P3;   coeff 0 = k (constant / DG0) */
+  FE_FORM_P3_LOAD = 17,        /* f*v*dx, P3;        coeff 0 = f (constant / DG0)   */
   /* exterior-facet (ds) forms over the facets given by fe_form_set_facets
    * (CUDAFormIntegral.cpp:361-447 vector, :1667-1793 matrix, :721-837 lifting) */
   FE_FORM_P1_FACET_MASS = 4,   /* alpha*u*v*ds, P1;  coeff 0 = alpha (constant / DG0 of the facet's cell) */

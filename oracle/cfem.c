@@ -24,8 +24,9 @@
  * own rows (no atomics; shared cells are recomputed).
  *
  * Element kinds: 1 = P1 Poisson (k DG0 or 1), 2 = P2 Poisson (k P1 field),
- * 3 = vector P2 elasticity (lam, mu DG0).  Reference tensors are passed in
- * by cfem_set_tables() from the exact rational tables of fem_oracle.py.
+ * 3 = vector P2 elasticity (lam, mu DG0), 4 = equispaced P3 Poisson (k DG0).
+ * Reference tensors are passed in by cfem_set_tables() / cfem_set_tables_p3()
+ * from the exact rational tables of fem_oracle.py.
  */
 #include <math.h>
 #include <pthread.h>
@@ -36,12 +37,20 @@
 static double R2w[4][3][3][10][10]; /* int lambda_m d_a phi_i d_b phi_j */
 static double R2[3][3][10][10];     /* int d_a phi_i d_b phi_j          */
 static double W2[10];               /* int phi_i                         */
+static double R3[3][3][20][20];     /* int d_a psi_i d_b psi_j (P3)      */
+static double W3[20];               /* int psi_i (P3)                    */
 
 void cfem_set_tables(const double* r2w, const double* r2, const double* w2)
 {
   memcpy(R2w, r2w, sizeof(R2w));
   memcpy(R2, r2, sizeof(R2));
   memcpy(W2, w2, sizeof(W2));
+}
+
+void cfem_set_tables_p3(const double* r3, const double* w3)
+{
+  memcpy(R3, r3, sizeof(R3));
+  memcpy(W3, w3, sizeof(W3));
 }
 
 /* ---------------- geometry ---------------- */
@@ -70,7 +79,7 @@ static inline void cell_geom(const double* coords, const int32_t* v, double K[3]
 
 static const double P1G[4][3] = {{-1, -1, -1}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
 
-/* Ae is k0 x k1 row-major (k0 = k1 = 4, 10 or 30) */
+/* Ae is k0 x k1 row-major (k0 = k1 = 4, 10, 20 or 30) */
 static void tabulate(int kind, const double* coords, const int32_t* v, int64_t c,
                      const double* coeff0, const double* coeff1, double* Ae)
 {
@@ -100,6 +109,15 @@ static void tabulate(int kind, const double* coords, const int32_t* v, int64_t c
           const double* R = &R2w[m][a][b][0][0];
           for (int e = 0; e < 100; ++e) Ae[e] += w * R[e];
         }
+  } else if (kind == 4) {
+    double s = coeff0 ? coeff0[c] : 1.0;
+    for (int i = 0; i < 400; ++i) Ae[i] = 0.0;
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b) {
+        double w = s * adet * (K[a][0] * K[b][0] + K[a][1] * K[b][1] + K[a][2] * K[b][2]);
+        const double* R = &R3[a][b][0][0];
+        for (int e = 0; e < 400; ++e) Ae[e] += w * R[e];
+      }
   } else {
     static __thread double D[3][3][100];
     for (int a = 0; a < 3; ++a)
@@ -136,13 +154,15 @@ static void tabulate_vec(int kind, const double* coords, const int32_t* v, int64
     for (int i = 0; i < 4; ++i) be[i] = adet / 120.0 * (f[v[i]] + s);
   } else if (kind == 2) {
     for (int i = 0; i < 10; ++i) be[i] = f[c] * adet * W2[i];
+  } else if (kind == 4) {
+    for (int i = 0; i < 20; ++i) be[i] = f[c] * adet * W3[i];
   } else {
     for (int i = 0; i < 10; ++i)
       for (int a = 0; a < 3; ++a) be[3 * i + a] = f[3 * c + a] * adet * W2[i];
   }
 }
 
-static inline int kdofs(int kind) { return kind == 1 ? 4 : 10; }
+static inline int kdofs(int kind) { return kind == 1 ? 4 : (kind == 4 ? 20 : 10); }
 
 /* ---------------- row-owning partition ---------------- */
 typedef struct {

@@ -22,7 +22,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 _SRC = os.path.join(_HERE, "cfem.c")
 _lib = None
 
-KIND = {"p1": 1, "p1k": 1, "p2": 2, "vp2": 3}
+KIND = {"p1": 1, "p1k": 1, "p2": 2, "vp2": 3, "p3": 4}
 
 
 def _cpu_fingerprint() -> str:
@@ -63,6 +63,7 @@ def lib():
         L.cfem_plan_total_cells.restype = i64
         L.cfem_plan_total_cells.argtypes = [vp]
         L.cfem_set_tables.argtypes = [vp, vp, vp]
+        L.cfem_set_tables_p3.argtypes = [vp, vp]
         L.cfem_assemble_matrix.argtypes = [vp, i32, vp, vp, vp, i32, vp, vp, vp, vp, vp, vp, dbl, vp, i64]
         L.cfem_assemble_vector.argtypes = [vp, i32, vp, vp, vp, i32, vp, vp]
         L.cfem_apply_lifting.argtypes = [vp, i32, vp, vp, vp, i32, vp, vp, vp, vp, vp, dbl, vp]
@@ -70,8 +71,11 @@ def lib():
         r2w = np.ascontiguousarray(fo.ref_grad_tensor(2, True))
         r2 = np.ascontiguousarray(fo.ref_grad_tensor(2, False))
         w2 = np.ascontiguousarray(fo.ref_basis_integrals(2))
-        L._tables = (r2w, r2, w2)
+        r3 = np.ascontiguousarray(fo.ref_grad_tensor(3, False))
+        w3 = np.ascontiguousarray(fo.ref_basis_integrals(3))
+        L._tables = (r2w, r2, w2, r3, w3)
         L.cfem_set_tables(r2w.ctypes.data, r2.ctypes.data, w2.ctypes.data)
+        L.cfem_set_tables_p3(r3.ctypes.data, w3.ctypes.data)
         _lib = L
     return _lib
 

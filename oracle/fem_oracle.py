@@ -118,6 +118,21 @@ def _basis(degree):
         vert = [_pmul(l, _padd(_pscale(l, 2), {(0, 0, 0): Fraction(1)}, -1)) for l in _LAMBDA]
         edge = [_pscale(_pmul(_LAMBDA[a], _LAMBDA[b]), 4) for a, b in TET_EDGES]
         return vert + edge
+    if degree == 3:
+        # equispaced P3 Lagrange: vertices, two dofs per edge (basix edge
+        # order, the point nearer the edge's first vertex first), face centroids
+        one = {(0, 0, 0): Fraction(1)}
+        two = {(0, 0, 0): Fraction(2)}
+        vert = [_pscale(_pmul(l, _pmul(_padd(_pscale(l, 3), one, -1), _padd(_pscale(l, 3), two, -1))),
+                        Fraction(1, 2)) for l in _LAMBDA]
+        edge = []
+        for a, b in TET_EDGES:
+            ab = _pmul(_LAMBDA[a], _LAMBDA[b])
+            edge.append(_pscale(_pmul(ab, _padd(_pscale(_LAMBDA[a], 3), one, -1)), Fraction(9, 2)))
+            edge.append(_pscale(_pmul(ab, _padd(_pscale(_LAMBDA[b], 3), one, -1)), Fraction(9, 2)))
+        face = [_pscale(_pmul(_pmul(_LAMBDA[a], _LAMBDA[b]), _LAMBDA[c]), 27)
+                for a, b, c in ((1, 2, 3), (0, 2, 3), (0, 1, 3), (0, 1, 2))]
+        return vert + edge + face
     raise ValueError(degree)
 
 
@@ -334,6 +349,34 @@ def p2_dofmap(n: int, cells: np.ndarray):
     return dofs, len(uniq), grid
 
 
+def p3_local_points():
+    """Barycentric weights (in thirds) of the 20 P3 nodes in local order."""
+    w = [tuple(3 if q == v else 0 for q in range(4)) for v in range(4)]
+    for a, b in TET_EDGES:
+        w.append(tuple(2 if q == a else (1 if q == b else 0) for q in range(4)))
+        w.append(tuple(1 if q == a else (2 if q == b else 0) for q in range(4)))
+    for f in range(4):
+        w.append(tuple(0 if q == f else 1 for q in range(4)))
+    return np.array(w, dtype=np.int64)
+
+
+def p3_dofmap(n: int, cells: np.ndarray):
+    """Equispaced P3 dofmap on the unit-cube mesh: every node sits on the
+    tripled grid (3x vertex index); dofs are numbered by lexicographic (z, y, x)
+    order of the points that are nodes.  Returns (dofs int32 [C,20], num_dofs,
+    tripled-grid index [num_dofs,3])."""
+    vg = vertex_grid_index(n)
+    m = 3 * n + 1
+    W = p3_local_points()  # [20, 4]
+    V = np.stack([vg[cells[:, v]] for v in range(4)], axis=1)  # [C,4,3]
+    P = np.einsum("lv,cvd->cld", W, V)  # [C,20,3] tripled-grid coordinates
+    key = (P[..., 2] * m + P[..., 1]) * m + P[..., 0]
+    uniq, inv = np.unique(key.ravel(), return_inverse=True)
+    dofs = inv.reshape(key.shape).astype(np.int32)
+    grid = np.stack([uniq % m, (uniq // m) % m, uniq // (m * m)], axis=1)
+    return dofs, len(uniq), grid
+
+
 def boundary_dofs_from_grid(grid: np.ndarray, extent: int):
     """Dofs lying on the boundary of the unit cube: a grid coordinate equals 0
     or ``extent`` (exact topological marking for this structured mesh)."""
@@ -347,6 +390,10 @@ def dof_coordinates(coords, cells, dofs, num_dofs, degree):
         X[dofs.ravel()] = coords[cells.ravel()]
         return X
     cc = coords[cells]  # [C,4,3]
+    if degree == 3:
+        P = np.einsum("lv,cvd->cld", p3_local_points() / 3.0, cc)
+        X[dofs.ravel()] = P.reshape(-1, 3)
+        return X
     pts = [cc[:, v] for v in range(4)] + [0.5 * (cc[:, a] + cc[:, b]) for a, b in TET_EDGES]
     P = np.stack(pts, axis=1)
     X[dofs.ravel()] = P.reshape(-1, 3)
@@ -456,6 +503,23 @@ def p2_stiffness(coords, cells, k_cell_values):
     G = np.abs(det)[:, None, None] * np.einsum("cak,cbk->cab", K, K)
     R = ref_grad_tensor(2, True)  # [4,3,3,10,10]
     return np.einsum("cm,cab,mabij->cij", k_cell_values, G, R, optimize=True)
+
+
+def p3_stiffness(coords, cells, k_dg0=None):
+    """Ae [C,20,20] of k * inner(grad u, grad v) * dx with equispaced P3, k DG0 (or 1)."""
+    _, det, K = cell_geometry(coords, cells)
+    G = np.abs(det)[:, None, None] * np.einsum("cak,cbk->cab", K, K)
+    R0 = ref_grad_tensor(3, False)  # [3,3,20,20]
+    Ae = np.einsum("cab,abij->cij", G, R0, optimize=True)
+    if k_dg0 is not None:
+        Ae = Ae * np.asarray(k_dg0)[:, None, None]
+    return Ae
+
+
+def p3_load_dg0(coords, cells, f_cell):
+    """be [C,20] of f * v * dx with f DG0: |det| f int_ref phi_i."""
+    _, det, _ = cell_geometry(coords, cells)
+    return (np.abs(det) * np.asarray(f_cell))[:, None] * ref_basis_integrals(3)[None, :]
 
 
 def p2_elasticity(coords, cells, lam, mu):
@@ -614,6 +678,8 @@ def build_problem(kind: str, n: int, seed: int = 0):
           'vp2'  -- vector P2 elasticity, lam ~ U[0.5,2], mu ~ U[0.2,1] per cell,
                     vertices jittered +-0.2h, body force (0,0,-1), u = 0 on the boundary.
           'p1k'  -- P1 Poisson with DG0 k log-uniform in [1e-2,1e2] per cell.
+          'p3'   -- equispaced P3 Poisson, k = exp(N(0,1)) and f ~ U[-1,1] per cell
+                    (DG0), g = x + y + z on the boundary.
     """
     rng = np.random.default_rng(seed)
     P = {"kind": kind, "n": n}
@@ -645,6 +711,13 @@ def build_problem(kind: str, n: int, seed: int = 0):
         f = rng.uniform(-1.0, 1.0, size=C)
         g = X.sum(axis=1)
         P.update(dofs=dofs, ndof=ndof, bs=1, degree=2, bc_dofs=bnd, k=kv, f=f, g=g)
+    elif kind == "p3":
+        dofs, ndof, grid = p3_dofmap(n, cells)
+        X = dof_coordinates(coords, cells, dofs, ndof, 3)
+        bnd = boundary_dofs_from_grid(grid, 3 * n)
+        k = np.exp(rng.standard_normal(C))
+        f = rng.uniform(-1.0, 1.0, size=C)
+        P.update(dofs=dofs, ndof=ndof, bs=1, degree=3, bc_dofs=bnd, k=k, f=f, g=X.sum(axis=1))
     elif kind == "vp2":
         dofs, ndof, grid = p2_dofmap(n, cells)
         bnd_nodes = boundary_dofs_from_grid(grid, 2 * n)
@@ -665,6 +738,8 @@ def element_matrices(P):
         return p1_stiffness(P["coords"], P["cells"], P["k"])
     if kind == "p2":
         return p2_stiffness(P["coords"], P["cells"], P["k"][P["cells"]])
+    if kind == "p3":
+        return p3_stiffness(P["coords"], P["cells"], P["k"])
     if kind == "vp2":
         return p2_elasticity(P["coords"], P["cells"], P["lam"], P["mu"])
     raise ValueError(kind)
@@ -676,6 +751,8 @@ def element_vectors(P):
         return p1_load_p1f(P["coords"], P["cells"], P["f"])
     if kind == "p2":
         return p2_load_dg0(P["coords"], P["cells"], P["f"])
+    if kind == "p3":
+        return p3_load_dg0(P["coords"], P["cells"], P["f"])
     if kind == "vp2":
         return p2_vector_load_dg0(P["coords"], P["cells"], P["f"])
     raise ValueError(kind)
@@ -705,5 +782,9 @@ def nnz_formula(kind: str, n: int) -> int:
     E = 3 * n * (n + 1) ** 2 + 3 * n * n * (n + 1) + n ** 3
     if kind in ("p1", "p1k"):
         return V + 2 * E
+    if kind == "p3":
+        # cubic in n through the counts at n = 1..4 (1816, 12415, 39664,
+        # 91429); row widths are fixed per node class away from the boundary
+        return 1311 * n ** 3 + 459 * n ** 2 + 45 * n + 1
     p2 = 230 * n ** 3 + 138 * n ** 2 + 24 * n + 1
     return p2 if kind == "p2" else 9 * p2

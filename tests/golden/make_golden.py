@@ -20,7 +20,7 @@ sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 
 from oracle import fem_oracle as fo  # noqa: E402
 
-CASES = [("p1", 2), ("p1", 3), ("p1k", 2), ("p2", 2), ("vp2", 2)]
+CASES = [("p1", 2), ("p1", 3), ("p1k", 2), ("p2", 2), ("vp2", 2), ("p3", 2)]
 
 
 def make(kind, n):

@@ -47,6 +47,12 @@ def mirror_problem(P, precision="fp64"):
         W = fem.functionspace(mesh, ("DG", 0))
         a = fem.stiffness(V, fem.Function(V1, P["k"]), precision=precision)
         L = fem.load(V, fem.Function(W, P["f"]))
+    elif kind == "p3":
+        V = fem.functionspace(mesh, ("P", 3))
+        assert np.array_equal(V.dofs, P["dofs"])
+        W = fem.functionspace(mesh, ("DG", 0))
+        a = fem.stiffness(V, fem.Function(W, P["k"]), precision=precision)
+        L = fem.load(V, fem.Function(W, P["f"]))
     elif kind == "vp2":
         V = fem.functionspace(mesh, ("P", 2, (3,)))
         W = fem.functionspace(mesh, ("DG", 0))

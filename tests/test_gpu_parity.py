@@ -17,7 +17,8 @@ from oracle import fem_oracle as fo
 pytestmark = pytest.mark.gpu
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
-CASES = [("p1", 2), ("p1", 7), ("p1", 16), ("p1k", 6), ("p2", 2), ("p2", 5), ("p2", 9), ("vp2", 2), ("vp2", 4)]
+CASES = [("p1", 2), ("p1", 7), ("p1", 16), ("p1k", 6), ("p2", 2), ("p2", 5), ("p2", 9), ("vp2", 2), ("vp2", 4),
+         ("p3", 2), ("p3", 4)]
 
 
 def _problem_from_golden(path):
@@ -71,7 +72,8 @@ def test_system_parity(kind, n, variant):
 
 
 @pytest.mark.parametrize("kind,n,variant", [("p1", 8, "deterministic"), ("p2", 5, "deterministic"),
-                                            ("p1", 8, "sorted-slot"), ("vp2", 3, "deterministic")])
+                                            ("p1", 8, "sorted-slot"), ("vp2", 3, "deterministic"),
+                                            ("p3", 3, "deterministic")])
 def test_deterministic_is_bitwise_reproducible(kind, n, variant):
     P = fo.build_problem(kind, n, seed=3)
     R1 = run_system(P, variant=variant)
@@ -161,7 +163,7 @@ def test_bc_update_changes_values_not_pattern():
 
 def test_fp32_element_tensors_precision_path():
     # FP32 contraction, FP64 accumulation: relative Frobenius error at FP32 level
-    for kind, n in (("p2", 6), ("vp2", 3)):
+    for kind, n in (("p2", 6), ("vp2", 3), ("p3", 3)):
         P = fo.build_problem(kind, n, seed=6)
         S = fo.solve_system(P)
         R = run_system(P, precision="fp32")
@@ -174,7 +176,7 @@ def test_pcg_solution_matches_direct_solve():
     import scipy.sparse as sp
     import scipy.sparse.linalg as spla
 
-    for kind, n in (("p1", 8), ("p2", 5), ("vp2", 3)):
+    for kind, n in (("p1", 8), ("p2", 5), ("vp2", 3), ("p3", 3)):
         P = fo.build_problem(kind, n, seed=7)
         R = run_system(P)
         N = len(R["row_ptr"]) - 1

@@ -121,6 +121,25 @@ def test_fem_standins_match_oracle(n, jitter):
     assert np.array_equal(V1.boundary_nodes(), fo.boundary_dofs_from_grid(fo.vertex_grid_index(n), n))
     Vv = fem.functionspace(m, ("P", 2, (3,)))
     assert Vv.bs == 3 and Vv.num_dofs == 3 * nd
+    V3 = fem.functionspace(m, ("P", 3))
+    d3, nd3, grid3 = fo.p3_dofmap(n, cells)
+    assert V3.num_nodes == nd3 and np.array_equal(V3.dofs, d3)
+    assert np.array_equal(V3.boundary_nodes(), fo.boundary_dofs_from_grid(grid3, 3 * n))
+    assert np.allclose(V3.tabulate_dof_coordinates(), fo.dof_coordinates(coords, cells, d3, nd3, 3))
+
+
+def test_p3_form_specs_build_without_gpu():
+    from cudolfinx import fem
+    mesh = fem.create_unit_cube(2)
+    V3 = fem.functionspace(mesh, ("P", 3))
+    assert fem.stiffness(V3, 2.0).kind == "P3_STIFFNESS"
+    assert fem.stiffness(V3, 2.0, precision="fp32").precision == "fp32"
+    assert fem.load(V3, 1.0).kind == "P3_LOAD"
+    for bad in (lambda: fem.facet_mass(V3), lambda: fem.facet_load(V3, 1.0),
+                lambda: fem.energy(fem.Function(V3)), lambda: fem.functionspace(mesh, ("P", 3, (3,))),
+                lambda: fem.functionspace(mesh, ("P", 4))):
+        with pytest.raises(ValueError):
+            bad()
 
 
 def test_functional_specs_build_without_gpu():

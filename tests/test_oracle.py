@@ -151,7 +151,7 @@ def test_oracle_reproduces_golden_fixtures(path):
     assert np.abs(S["b"] - G["b"]).max() <= 1e-14 * max(1.0, np.abs(G["b"]).max())
 
 
-@pytest.mark.parametrize("kind,n", [("p1", 5), ("p1k", 4), ("p2", 4), ("vp2", 3)])
+@pytest.mark.parametrize("kind,n", [("p1", 5), ("p1k", 4), ("p2", 4), ("vp2", 3), ("p3", 3)])
 def test_c_port_matches_numpy_oracle(kind, n):
     P = fo.build_problem(kind, n)
     S = fo.solve_system(P)
@@ -193,3 +193,83 @@ def test_exterior_facets_match_mirror_helper():
         coords, cells = fo.unit_cube_tet_mesh(n)
         mesh = fem.create_unit_cube(n)
         assert np.array_equal(fem.exterior_facets(mesh), fo.exterior_facets(cells))
+
+
+# --- equispaced P3 -----------------------------------------------------------
+def _cube_gauss(fun, q=4):
+    """Tensor Gauss-Legendre rule on [0,1]^3 (exact for degree 2q-1 per axis)."""
+    t, w = np.polynomial.legendre.leggauss(q)
+    t, w = 0.5 * (t + 1.0), 0.5 * w
+    Z, Y, X = np.meshgrid(t, t, t, indexing="ij")
+    W = (w[:, None, None] * w[None, :, None] * w[None, None, :]).ravel()
+    return float(np.sum(W * fun(X.ravel(), Y.ravel(), Z.ravel())))
+
+
+def _cubic(X):
+    x, y, z = X[:, 0], X[:, 1], X[:, 2]
+    return x ** 3 + y ** 2 * z + x * y * z - 2.0 * z ** 3
+
+
+def _cubic_grad2(x, y, z):
+    gx = 3 * x ** 2 + y * z
+    gy = 2 * y * z + x * z
+    gz = y ** 2 + x * y - 6 * z ** 2
+    return gx * gx + gy * gy + gz * gz
+
+
+def test_p3_basis_is_lagrange_and_integrals_known_answer():
+    # phi_i(node_j) = delta_ij on the reference tet; int phi = |T|/40 (vertex),
+    # 0 (edge), 9|T|/40 (face), |T| = 1/6
+    B = fo._basis(3)
+    W = fo.p3_local_points() / 3.0  # barycentric
+    pts = W[:, 1:]  # reference coordinates (x, y, z) = (l1, l2, l3)
+    V = np.array([[sum(float(c) * p[0] ** e[0] * p[1] ** e[1] * p[2] ** e[2] for e, c in phi.items())
+                   for phi in B] for p in pts])
+    assert np.abs(V - np.eye(20)).max() < 1e-14
+    w3 = fo.ref_basis_integrals(3)
+    assert np.allclose(w3[:4], 1.0 / 240) and np.allclose(w3[4:16], 0.0, atol=1e-17)
+    assert np.allclose(w3[16:], 9.0 / 240)
+
+
+@pytest.mark.parametrize("jitter", [0.0, 0.2])
+def test_p3_energy_and_load_reproduce_cubic_integrals(jitter):
+    # a cubic u is interpolated exactly: u^T A u = int |grad u|^2 and
+    # sum_i b_i u_i = int u (f = 1) over the unit cube, on any affine mesh of it
+    n = 3
+    coords, cells = fo.unit_cube_tet_mesh(n, jitter=jitter, seed=4)
+    dofs, ndof, _ = fo.p3_dofmap(n, cells)
+    X = fo.dof_coordinates(coords, cells, dofs, ndof, 3)
+    u = _cubic(X)
+    Ae = fo.p3_stiffness(coords, cells)
+    energy = np.einsum("ci,cij,cj->", u[dofs], Ae, u[dofs])
+    assert abs(energy - _cube_gauss(_cubic_grad2)) < 1e-11 * energy
+    be = fo.p3_load_dg0(coords, cells, np.ones(len(cells)))
+    mean = np.einsum("ci,ci->", be, u[dofs])
+    assert abs(mean - _cube_gauss(lambda x, y, z: x ** 3 + y ** 2 * z + x * y * z - 2 * z ** 3)) < 1e-13
+    # constants are in the kernel of every element matrix
+    assert np.abs(Ae.sum(axis=2)).max() < 1e-12 * np.abs(Ae).max()
+
+
+def test_p3_patch_test_harmonic_cubic_is_exact():
+    # -div grad u = 0 with a harmonic cubic on the boundary: P3 reproduces it
+    P = fo.build_problem("p3", 2, seed=1)
+    P["k"] = np.ones_like(P["k"])
+    P["f"] = np.zeros_like(P["f"])
+    X = fo.dof_coordinates(P["coords"], P["cells"], P["dofs"], P["ndof"], 3)
+    P["g"] = X[:, 0] ** 3 - 3 * X[:, 0] * X[:, 1] ** 2 + X[:, 1] * X[:, 2]
+    S = fo.solve_system(P)
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spla
+    m = len(S["row_ptr"]) - 1
+    A = sp.csr_matrix((S["A"], S["col"], S["row_ptr"]), shape=(m, m))
+    u = spla.spsolve(A.tocsc(), S["b"])
+    assert np.abs(u - P["g"]).max() < 1e-11
+
+
+def test_p3_nnz_closed_form_and_dof_count():
+    for n in (1, 2, 3):
+        P = fo.build_problem("p3", n)
+        assert P["ndof"] == (3 * n + 1) ** 3
+        rp, col = fo.sparsity(P["dofs"], P["dofs"], P["ndof"])
+        assert len(col) == fo.nnz_formula("p3", n)
+        assert np.diff(rp).max() <= 256  # block positions fit the byte map
