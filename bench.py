@@ -88,7 +88,8 @@ def matrix_kernels(kind: str, variant: str, big: bool = False) -> int:
     reduction (element tensors + gather + set_diagonal)."""
     if variant in ("tile", "row-gather") or (variant == "deterministic" and kind in ("p1", "p2")):
         return 2
-    if kind in ("vp2", "p3") and variant in ("atomic", "auto"):
+    atomic = variant == "atomic" or (variant == "auto" and not (kind == "p1" and big))
+    if kind in ("p1", "vp2", "p3") and atomic:
         return 4  # zero + upper-triangle scatter + lower-triangle mirror + set_diagonal
     return 3  # atomic-full, block (zero + kernel + set_diagonal), sorted-slot
 

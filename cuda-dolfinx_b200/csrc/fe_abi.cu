@@ -641,15 +641,16 @@ int fe_assemble_matrix(fe_form a, double* values, fe_bc bc0, fe_bc bc1, double d
       return;
     }
     // every built-in bilinear form is symmetric: on a symmetric pattern with
-    // the same BCs on rows and columns, vector-P2 elasticity and P3 reduce
-    // each unique entry once into the upper triangle and a gather pass fills
-    // the lower triangle from it (on B200, vector P2 n=64: 7.6 ms instead of
-    // about 12 ms; P3 n=48: 1.79 ms instead of 2.23 ms).  For P1/P2 the pass
-    // costs what the halved reductions save (P2 n=96: 1.58 + 0.95 ms vs
-    // 2.55 ms), so they keep both reductions, as does FE_ASM_FULL_SCATTER for
-    // every form.
+    // the same BCs on rows and columns, P1, P3 and vector-P2 elasticity
+    // reduce each unique entry once into the upper triangle and a gather pass
+    // fills the lower triangle from it (on B200, vector P2 n=64: 7.6 ms
+    // instead of about 12 ms; P3 n=48: 1.79 instead of 2.23 ms; P1 n=128 on
+    // the atomic path: 0.73 instead of 0.85 ms; P1 n=32: equal).  For P2 the
+    // pass costs what the halved reductions save (n=96: 2.80 ms either way),
+    // so it keeps both reductions, as does FE_ASM_FULL_SCATTER for every form.
     const bool upper = zero && !(flags & FE_ASM_FULL_SCATTER) &&
-                       (a->kind == FE_FORM_VP2_ELASTICITY || a->kind == FE_FORM_P3_STIFFNESS) && a->V0 == a->V1 &&
+                       (a->kind == FE_FORM_VP2_ELASTICITY || a->kind == FE_FORM_P3_STIFFNESS ||
+                        a->kind == FE_FORM_P1_STIFFNESS) && a->V0 == a->V1 &&
                        bc0 == bc1 && ensure_mirror(*a->sp, st);
     if (zero) launch_zero(values, a->sp->nnz, st);
     MatLaunch L{};

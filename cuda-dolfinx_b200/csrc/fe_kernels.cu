@@ -168,14 +168,18 @@ __global__ void __launch_bounds__(kBlock) k_mat_p1_atomic(const MatArgs a) {
 #pragma unroll
     for (int j = i; j < 4; ++j) {
       const double v = s * (G[i][0] * G[j][0] + G[i][1] * G[j][1] + G[i][2] * G[j][2]);
-      // upper mode: only the entry whose row is below its column (the lower
-      // one is filled from it afterwards)
-      const bool do_ij = !a.upper || i == j || r[i] < r[j];
-      const bool do_ji = i != j && (!a.upper || r[j] < r[i]);
-      if (do_ij && !(((mr >> i) | (mc >> j)) & 1u))
-        atomicAdd(a.values + rp[i] + ((pws[i] >> (8 * j)) & 0xffu), v);
-      if (do_ji && !(((mr >> j) | (mc >> i)) & 1u))
-        atomicAdd(a.values + rp[j] + ((pws[j] >> (8 * i)) & 0xffu), v);
+      const int sij = rp[i] + ((pws[i] >> (8 * j)) & 0xffu), sji = rp[j] + ((pws[j] >> (8 * i)) & 0xffu);
+      const unsigned mij = (mr >> i) | (mc >> j), mji = (mr >> j) | (mc >> i);
+      if (a.upper) {
+        // one reduction per unique entry, into the upper triangle (the lower
+        // one is filled from it afterwards); the target is a select, so the
+        // warp issues one RED instead of two half-masked ones
+        const bool lo = i == j || r[i] < r[j];
+        if (!((lo ? mij : mji) & 1u)) atomicAdd(a.values + (lo ? sij : sji), v);
+        continue;
+      }
+      if (!(mij & 1u)) atomicAdd(a.values + sij, v);
+      if (i != j && !(mji & 1u)) atomicAdd(a.values + sji, v);
     }
 }
 
@@ -215,10 +219,16 @@ __global__ void __launch_bounds__(kBlock) k_mat_p2_atomic(const MatArgs a) {
   double* __restrict__ vals = a.values;
   const bool upper = a.upper != 0;
   auto emit = [&](int i, int j, double v) {
-    const bool do_ij = !upper || i == j || rd[i] < rd[j];
-    const bool do_ji = i != j && (!upper || rd[j] < rd[i]);
-    if (do_ij && !(((mr >> i) | (mc >> j)) & 1u)) atomicAdd(vals + rp[i] + p[i * 10 + j], v);
-    if (do_ji && !(((mr >> j) | (mc >> i)) & 1u)) atomicAdd(vals + rp[j] + p[j * 10 + i], v);
+    const unsigned mij = (mr >> i) | (mc >> j), mji = (mr >> j) | (mc >> i);
+    if (upper) {
+      // one RED per unique entry, target chosen by a select (no divergence)
+      const bool lo = i == j || rd[i] < rd[j];
+      const int slot = lo ? rp[i] + p[i * 10 + j] : rp[j] + p[j * 10 + i];
+      if (!((lo ? mij : mji) & 1u)) atomicAdd(vals + slot, v);
+      return;
+    }
+    if (!(mij & 1u)) atomicAdd(vals + rp[i] + p[i * 10 + j], v);
+    if (i != j && !(mji & 1u)) atomicAdd(vals + rp[j] + p[j * 10 + i], v);
   };
   if constexpr (COEF == FE_COEFF_P1) {
     const int4 km = __ldg(reinterpret_cast<const int4*>(a.c0.map) + c);
@@ -282,6 +292,9 @@ __global__ void __launch_bounds__(kBlockP3) k_mat_p3_atomic(const MatArgs a) {
   }
   double* __restrict__ vals = a.values;
   const bool upper = a.upper != 0;
+  // upper mode keeps the two predicated REDs per entry (one of them active
+  // in each lane): choosing the slot by a select, as the other kernels do,
+  // measured slower for P3 on B200 (P3 n=48: 2.23 vs 1.79 ms)
   auto emit = [&](int i, int j, double v) {
     const bool do_ij = !upper || i == j || rd[i] < rd[j];
     const bool do_ji = i != j && (!upper || rd[j] < rd[i]);
@@ -368,13 +381,17 @@ __global__ void __launch_bounds__(kBlock) k_mat_vp2_atomic(const MatArgs a) {
     // scalar rows 3*rd[i]+ca and 3*rd[j]+cb; upper mode keeps the entry in the
     // upper triangle (the diagonal entry when they coincide)
     const int ri = 3 * rd[i] + ca, rj = 3 * rd[j] + cb;
-    const bool same = ca == cb && i == j;
-    const bool do_ij = !upper || ri <= rj;
-    const bool do_ji = !same && (!upper || rj < ri);
-    if (do_ij && !(((mr >> (3 * i + ca)) | (mc >> (3 * j + cb))) & 1u))
-      atomicAdd(vals + rp[i] + ca * L[i] + 3 * p[i * 10 + j] + cb, v);
-    if (do_ji && !(((mr >> (3 * j + cb)) | (mc >> (3 * i + ca))) & 1u))
-      atomicAdd(vals + rp[j] + cb * L[j] + 3 * p[j * 10 + i] + ca, v);
+    const unsigned mij = (mr >> (3 * i + ca)) | (mc >> (3 * j + cb));
+    const unsigned mji = (mr >> (3 * j + cb)) | (mc >> (3 * i + ca));
+    if (upper) {
+      // one RED per unique entry, target chosen by a select (no divergence)
+      const bool lo = ri <= rj;
+      const int slot = lo ? rp[i] + ca * L[i] + 3 * p[i * 10 + j] + cb : rp[j] + cb * L[j] + 3 * p[j * 10 + i] + ca;
+      if (!((lo ? mij : mji) & 1u)) atomicAdd(vals + slot, v);
+      return;
+    }
+    if (!(mij & 1u)) atomicAdd(vals + rp[i] + ca * L[i] + 3 * p[i * 10 + j] + cb, v);
+    if (!(ca == cb && i == j) && !(mji & 1u)) atomicAdd(vals + rp[j] + cb * L[j] + 3 * p[j * 10 + i] + ca, v);
   });
 }
 
