@@ -460,13 +460,32 @@ __global__ void k_lower_pairs(const int32_t* __restrict__ row_ptr, const int32_t
   }
 }
 
-// values[pair.x] = values[pair.y] for every strictly-lower slot: one slot per
-// thread, pairs read coalesced, the mirror reads are the only scattered ones.
-__global__ void k_mirror_pairs(const int2* __restrict__ pairs, int64_t n, double* __restrict__ values) {
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += stride) {
-    const int2 p = __ldg(pairs + k);
-    values[p.x] = values[p.y];
+// values[pair.x] = values[pair.y] for every strictly-lower slot.  Pairs and
+// stores are coalesced; the mirror reads are the only scattered accesses and
+// the kernel is bound by their latency, so each thread takes kMirrorUnroll
+// pairs 32 apart (every load and store instruction of a warp still covers
+// consecutive pairs) and issues all of its gathers before its stores.
+constexpr int kMirrorUnroll = 4;
+
+__global__ void __launch_bounds__(256) k_mirror_pairs(const int2* __restrict__ pairs, int64_t n,
+                                                      double* __restrict__ values) {
+  constexpr int U = kMirrorUnroll;
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t base = warp * 32 * U; base < n; base += nwarps * 32 * U) {
+    int2 p[U];
+    double v[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int64_t k = base + u * 32 + lane;
+      p[u] = k < n ? __ldg(pairs + k) : make_int2(-1, -1);
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) v[u] = p[u].x >= 0 ? values[p[u].y] : 0.0;
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+      if (p[u].x >= 0) values[p[u].x] = v[u];
   }
 }
 
@@ -903,7 +922,8 @@ void launch_mirror_lower(const fe_sparsity_s& sp, double* values, cudaStream_t s
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const unsigned grid = (unsigned)std::min<int64_t>((M.nlower + 255) / 256, (int64_t)sms * 16);
+  const unsigned grid =
+      (unsigned)std::min<int64_t>((M.nlower + 256 * kMirrorUnroll - 1) / (256 * kMirrorUnroll), (int64_t)sms * 16);
   k_mirror_pairs<<<grid, 256, 0, s>>>(M.pairs.p, M.nlower, values);
   FE_CUDA(cudaGetLastError());
 }
