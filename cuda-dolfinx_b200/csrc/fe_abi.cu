@@ -261,6 +261,37 @@ int fe_dofmap_create(fe_context ctx, const int32_t* cell_dofs, int64_t num_cells
   });
 }
 
+int fe_dofmap_create_restricted(fe_context ctx, const int32_t* cell_dofs, int64_t num_cells, int dofs_per_cell,
+                                int bs, int64_t num_blocks, fe_dofmap* out) {
+  return guard([&] {
+    DeviceScope d(ctx);
+    FE_REQUIRE(out, "null output pointer");
+    FE_REQUIRE(dofs_per_cell > 0 && dofs_per_cell <= 32, "dofs_per_cell must be in 1..32");
+    FE_REQUIRE(bs >= 1 && bs <= 3, "block size must be 1..3");
+    FE_REQUIRE(num_cells >= 0 && num_blocks >= 0, "negative size");
+    FE_REQUIRE(num_blocks * bs <= INT32_MAX, "too many dofs for int32 indices");
+    FE_REQUIRE(cell_dofs || !num_cells, "null dofmap");
+    const int64_t n = num_cells * dofs_per_cell;
+    bool excluded = false;
+    for (int64_t q = 0; q < n; ++q) {
+      if (cell_dofs[q] < -1 || cell_dofs[q] >= num_blocks)
+        FE_FAIL(FE_ERR_ARG, "restricted dofmap entry out of range at " + std::to_string(q));
+      excluded |= cell_dofs[q] == -1;
+    }
+    auto m = std::make_unique<fe_dofmap_s>();
+    m->ctx = ctx;
+    m->num_cells = num_cells;
+    m->num_blocks = num_blocks;
+    m->k = dofs_per_cell;
+    m->bs = bs;
+    m->excluded = excluded;
+    m->host.assign(cell_dofs, cell_dofs + n);
+    upload(m->dofs, cell_dofs, (size_t)n);
+    m->id = g_next_id++;
+    *out = m.release();
+  });
+}
+
 int fe_dofmap_destroy(fe_dofmap d) {
   return guard([&] { delete d; });
 }
@@ -287,6 +318,35 @@ int fe_sparsity_build(fe_dofmap rows, fe_dofmap cols, fe_sparsity* out) {
     s->host_row_ptr = std::move(row_ptr);
     s->id = g_next_id++;
     *out = s.release();
+  });
+}
+
+int fe_sparsity_build_block(fe_context ctx, int num_parts, const fe_dofmap* rows, const fe_dofmap* cols,
+                            const int64_t* row_offsets, const int64_t* col_offsets, int64_t num_rows,
+                            int64_t num_cols, fe_sparsity* out) {
+  return guard([&] {
+    FE_REQUIRE(ctx && out, "null argument");
+    FE_REQUIRE(num_parts >= 0 && (num_parts == 0 || (rows && cols && row_offsets && col_offsets)), "null part table");
+    DeviceScope d(ctx);
+    std::vector<SystemPart> parts;
+    for (int p = 0; p < num_parts; ++p) {
+      FE_REQUIRE(rows[p] && cols[p], "null dofmap in part " + std::to_string(p));
+      FE_REQUIRE(rows[p]->ctx == ctx && cols[p]->ctx == ctx, "part " + std::to_string(p) + " belongs to another context");
+      parts.push_back(SystemPart{rows[p], cols[p], row_offsets[p], col_offsets[p]});
+    }
+    std::vector<int32_t> row_ptr, col, diag;
+    build_system_pattern(parts, num_rows, num_cols, row_ptr, col, diag);
+    auto sp = std::make_unique<fe_sparsity_s>();
+    sp->ctx = ctx;
+    sp->num_rows = num_rows;
+    sp->num_cols = num_cols;
+    sp->nnz = (int64_t)col.size();
+    upload(sp->row_ptr, row_ptr.data(), row_ptr.size());
+    upload(sp->col, col.data(), col.size());
+    upload(sp->diag, diag.data(), diag.size());
+    sp->host_row_ptr = std::move(row_ptr);
+    sp->id = g_next_id++;
+    *out = sp.release();
   });
 }
 
@@ -409,6 +469,7 @@ int fe_form_create(fe_context ctx, int form_kind, fe_mesh mesh, fe_dofmap test, 
                                                std::to_string(V->bs) + "; form kind " + std::to_string(form_kind) +
                                                " needs " + std::to_string(k) + " bs " + std::to_string(bs));
       FE_REQUIRE(V->num_cells == mesh->num_cells, "dofmap and mesh cell counts differ");
+      FE_REQUIRE(!V->excluded || !is_facet_kind(form_kind), "exterior-facet forms take unrestricted dofmaps");
     }
     auto f = std::make_unique<fe_form_s>();
     f->ctx = ctx;
@@ -445,7 +506,8 @@ int fe_form_set_coefficient(fe_form f, int index, int coeff_kind, fe_dofmap cmap
     if (coeff_kind == FE_COEFF_DG0) {
       FE_REQUIRE(n == C * ncomp, "DG0 coefficient needs num_cells*" + std::to_string(ncomp) + " values");
     } else if (coeff_kind == FE_COEFF_P1) {
-      FE_REQUIRE(cmap && cmap->k == 4 && cmap->bs == 1 && cmap->num_cells == C, "P1 coefficient needs a P1 dofmap");
+      FE_REQUIRE(cmap && cmap->k == 4 && cmap->bs == 1 && cmap->num_cells == C && !cmap->excluded,
+                 "P1 coefficient needs an unrestricted P1 dofmap");
       FE_REQUIRE(n >= cmap->num_blocks, "P1 coefficient has fewer values than dofs");
       FE_REQUIRE(f->kind == FE_FORM_P2_STIFFNESS || f->kind == FE_FORM_P1_LOAD ||
                      f->kind == FE_FORM_P1_FACET_LOAD || f->kind == FE_FORM_P2_FACET_LOAD ||
@@ -454,7 +516,8 @@ int fe_form_set_coefficient(fe_form f, int index, int coeff_kind, fe_dofmap cmap
                  "P1 coefficients are supported by P2 stiffness, P1 load, facet load and functional forms");
     } else if (coeff_kind == FE_COEFF_P2) {
       FE_REQUIRE(f->kind == FE_FORM_P2_ENERGY && index == 1, "P2 coefficients are the u of FE_FORM_P2_ENERGY");
-      FE_REQUIRE(cmap && cmap->k == 10 && cmap->bs == 1 && cmap->num_cells == C, "P2 coefficient needs a P2 dofmap");
+      FE_REQUIRE(cmap && cmap->k == 10 && cmap->bs == 1 && cmap->num_cells == C && !cmap->excluded,
+                 "P2 coefficient needs an unrestricted P2 dofmap");
       FE_REQUIRE(n >= cmap->num_blocks, "P2 coefficient has fewer values than dofs");
     } else {
       FE_FAIL(FE_ERR_ARG, "unknown coefficient kind " + std::to_string(coeff_kind));
@@ -511,6 +574,9 @@ int fe_form_bind_sparsity(fe_form f, fe_sparsity s, void* stream) {
     FE_REQUIRE(f && s, "null argument");
     FE_REQUIRE(f->rank == 2, "only bilinear forms bind a matrix pattern");
     FE_REQUIRE(s->ctx == f->ctx, "pattern belongs to another context");
+    FE_REQUIRE(!f->V0->excluded && !f->V1->excluded,
+               "forms on restricted dofmaps bind to a block pattern (fe_form_bind_sparsity_block)");
+    FE_REQUIRE(!s->parent, "a block view cannot be bound directly");
     FE_REQUIRE(s->num_rows == scalar_size(f->V0) && s->num_cols == scalar_size(f->V1),
                "pattern shape does not match the form's spaces");
     DeviceScope d(f->ctx);
@@ -519,6 +585,7 @@ int fe_form_bind_sparsity(fe_form f, fe_sparsity s, void* stream) {
     f->pos.alloc((bytes + 15) / 16 * 16 + 16);
     FE_CUDA(cudaMemsetAsync(f->pos.p, 0, f->pos.bytes(), st));
     f->sp = s;
+    f->view.reset();
     reset_gather_plan(*f);
     try {
       launch_build_slotmap(*f, st);
@@ -527,6 +594,37 @@ int fe_form_bind_sparsity(fe_form f, fe_sparsity s, void* stream) {
       f->sp = nullptr;  // the byte map is incomplete: the form stays unbound
       throw;
     }
+  });
+}
+
+int fe_form_bind_sparsity_block(fe_form f, fe_sparsity s, int64_t row_offset, int64_t col_offset, void* stream) {
+  return guard([&] {
+    FE_REQUIRE(f && s, "null argument");
+    FE_REQUIRE(f->rank == 2, "only bilinear forms bind a matrix pattern");
+    FE_REQUIRE(s->ctx == f->ctx, "pattern belongs to another context");
+    FE_REQUIRE(!s->parent, "bind to the monolithic pattern, not to a view");
+    FE_REQUIRE(row_offset >= 0 && col_offset >= 0 && row_offset + scalar_size(f->V0) <= s->num_rows &&
+                   col_offset + scalar_size(f->V1) <= s->num_cols,
+               "the form's block does not fit the pattern at these offsets");
+    DeviceScope d(f->ctx);
+    cudaStream_t st = as_stream(stream);
+    const size_t bytes = (size_t)f->mesh->num_cells * f->V0->k * f->V1->k;
+    f->pos.alloc((bytes + 15) / 16 * 16 + 16);
+    FE_CUDA(cudaMemsetAsync(f->pos.p, 0, f->pos.bytes(), st));
+    auto v = std::make_unique<fe_sparsity_s>();
+    v->ctx = f->ctx;
+    v->num_rows = scalar_size(f->V0);
+    v->num_cols = scalar_size(f->V1);
+    v->nnz = s->nnz;
+    v->parent = s;
+    v->id = g_next_id++;
+    f->sp = nullptr;
+    f->view.reset();
+    reset_gather_plan(*f);
+    launch_build_view(*f, *s, row_offset, col_offset, *v, st);
+    check_device_errors(f->ctx, st, FE_ERR_PATTERN);  // the form stays unbound on a missing coupling
+    f->view = std::move(v);
+    f->sp = f->view.get();
   });
 }
 
@@ -594,6 +692,11 @@ int fe_assemble_matrix(fe_form a, double* values, fe_bc bc0, fe_bc bc1, double d
     if (bc1) FE_REQUIRE(bc1->num_dofs == a->sp->num_cols, "bc1 size differs from the number of columns");
     cudaStream_t st = as_stream(stream);
     const bool zero = (flags & FE_ASM_ZERO) != 0;
+    const bool view = a->sp->parent != nullptr;
+    if (view)
+      FE_REQUIRE(!(flags & (FE_ASM_DETERMINISTIC | FE_ASM_SORTED_SLOT | FE_ASM_TILE | FE_ASM_ROW_GATHER |
+                            FE_ASM_BLOCK)),
+                 "a form bound to a block pattern assembles with the atomic scatter only");
     if (is_facet_kind(a->kind)) {
       FE_REQUIRE(!(flags & (FE_ASM_DETERMINISTIC | FE_ASM_SORTED_SLOT | FE_ASM_TILE | FE_ASM_ROW_GATHER |
                             FE_ASM_BLOCK)),
@@ -631,7 +734,7 @@ int fe_assemble_matrix(fe_form a, double* values, fe_bc bc0, fe_bc bc1, double d
     }
     // default: the block variant for P1 meshes above ~1M cells (measured faster
     // on B200 at 12.6M cells: 0.80 vs 0.86 ms), the FP64-atomic scatter otherwise
-    const bool auto_block = !(flags & FE_ASM_ATOMIC) && a->kind == FE_FORM_P1_STIFFNESS &&
+    const bool auto_block = !(flags & FE_ASM_ATOMIC) && !view && a->kind == FE_FORM_P1_STIFFNESS &&
                             a->mesh->num_cells >= (int64_t(1) << 20);
     const bool want_block = (flags & FE_ASM_BLOCK) || auto_block;
     if (flags & FE_ASM_BLOCK) FE_REQUIRE(block_supported(*a), "the block variant supports P1/P2 stiffness only");
@@ -648,7 +751,7 @@ int fe_assemble_matrix(fe_form a, double* values, fe_bc bc0, fe_bc bc1, double d
     // the atomic path: 0.73 instead of 0.85 ms; P1 n=32: equal).  For P2 the
     // pass costs what the halved reductions save (n=96: 2.80 ms either way),
     // so it keeps both reductions, as does FE_ASM_FULL_SCATTER for every form.
-    const bool upper = zero && !(flags & FE_ASM_FULL_SCATTER) &&
+    const bool upper = zero && !view && !(flags & FE_ASM_FULL_SCATTER) &&
                        (a->kind == FE_FORM_VP2_ELASTICITY || a->kind == FE_FORM_P3_STIFFNESS ||
                         a->kind == FE_FORM_P1_STIFFNESS) && a->V0 == a->V1 &&
                        bc0 == bc1 && ensure_mirror(*a->sp, st);
@@ -685,6 +788,7 @@ int fe_assemble_matrix_batch(fe_form a, int num_instances, const double* const* 
     FE_REQUIRE(a, "null form");
     FE_REQUIRE(a->rank == 2, "assemble_matrix_batch needs a bilinear form");
     FE_REQUIRE(a->sp, "bind a sparsity pattern first (fe_form_bind_sparsity)");
+    FE_REQUIRE(!a->sp->parent, "batched assembly does not take block-bound forms");
     if (bc0) FE_REQUIRE(bc0->num_dofs == a->sp->num_rows, "bc0 size differs from the number of rows");
     if (bc1) FE_REQUIRE(bc1->num_dofs == a->sp->num_cols, "bc1 size differs from the number of columns");
     DeviceScope d(a->ctx);

@@ -98,6 +98,7 @@ struct fe_dofmap_s {
   fe::DevBuf<int32_t> dofs;      // [num_cells*k] block dofs
   std::vector<int32_t> host;     // host copy (sparsity build)
   uint64_t id = 0;               // unique id for caches
+  bool excluded = false;         // some entries are -1: dofs outside a restriction
 };
 
 struct fe_sparsity_s {
@@ -117,6 +118,12 @@ struct fe_sparsity_s {
     bool ok = false;                // pattern symmetric with every diagonal present
   };
   std::unique_ptr<Mirror> mirror;
+  // block view (fe_form_bind_sparsity_block): the rows of one block form
+  // inside a monolithic pattern.  row_ptr[r] is then the first slot of the
+  // block's column segment in monolithic row offset + r (nnz = the monolithic
+  // count, so zeroing covers the whole value array), diag[r] the slot of the
+  // monolithic diagonal entry of that row; col is empty.
+  fe_sparsity parent = nullptr;
 };
 
 struct fe_bc_s {
@@ -152,6 +159,7 @@ struct fe_form_s {
   fe_dofmap V0 = nullptr, V1 = nullptr;
   fe::Coefficient coeff[2];
   fe_sparsity sp = nullptr;
+  std::unique_ptr<fe_sparsity_s> view;  // block view that sp points to (fe_form_bind_sparsity_block)
   fe::DevBuf<uint8_t> pos;       // [num_cells * k0 * k1] block column positions (padded to 16 B)
   fe::DevBuf<int32_t> facets;    // exterior-facet forms: [num_facets][2] (cell, local facet)
   int64_t num_facets = 0;
@@ -244,6 +252,18 @@ void build_block_pattern(const int32_t* dofs0, const int32_t* dofs1, int64_t num
                          std::vector<int32_t>& bcol);
 void unroll_pattern(const std::vector<int64_t>& bptr, const std::vector<int32_t>& bcol, int bs0, int bs1,
                     std::vector<int32_t>& row_ptr, std::vector<int32_t>& col, std::vector<int32_t>& diag);
+// one coupling of a block system: the cell couplings of (rows, cols) placed
+// at scalar offsets of the monolithic matrix; -1 entries are skipped
+struct SystemPart {
+  const fe_dofmap_s* rows;
+  const fe_dofmap_s* cols;
+  int64_t row_offset, col_offset;
+};
+// monolithic scalar pattern: the union of the parts' unrolled couplings, each
+// row's columns sorted and unique (DOLFINx's block SparsityPattern, block
+// size 1, as create_cuda_matrix_block builds it)
+void build_system_pattern(const std::vector<SystemPart>& parts, int64_t num_rows, int64_t num_cols,
+                          std::vector<int32_t>& row_ptr, std::vector<int32_t>& col, std::vector<int32_t>& diag);
 
 // ---- kernels (fe_kernels.cu) ----
 struct MatLaunch {
@@ -270,6 +290,10 @@ bool ensure_mirror(fe_sparsity_s& sp, cudaStream_t s);
 // values[lower slot] = values[its transpose] for every strictly-lower slot
 void launch_mirror_lower(const fe_sparsity_s& sp, double* values, cudaStream_t s);
 void launch_build_slotmap(const fe_form_s& f, cudaStream_t s);
+// block view of a monolithic pattern for form f at the given scalar offsets:
+// fills view.row_ptr (segment starts), view.diag and f.pos
+void launch_build_view(const fe_form_s& f, const fe_sparsity_s& mono, int64_t row_offset, int64_t col_offset,
+                       fe_sparsity_s& view, cudaStream_t s);
 void launch_matrix_atomic(const MatLaunch& a, cudaStream_t s);
 void launch_set_diagonal(const fe_sparsity_s& sp, const fe_bc_s& bc, double diagonal, double* values,
                          cudaStream_t s);

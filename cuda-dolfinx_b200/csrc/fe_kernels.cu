@@ -153,16 +153,16 @@ __global__ void __launch_bounds__(kBlock) k_mat_p1_atomic(const MatArgs a) {
   const int cl[4] = {d1.x, d1.y, d1.z, d1.w};
   const uint4 pw = __ldg(reinterpret_cast<const uint4*>(a.pos) + c);
   const uint32_t pws[4] = {pw.x, pw.y, pw.z, pw.w};
+  // masked rows / columns: BC dofs and dofs outside a restriction (-1)
   unsigned mr = 0, mc = 0;
-  if (a.bc0)
 #pragma unroll
-    for (int i = 0; i < 4; ++i) mr |= (__ldg(a.bc0 + r[i]) ? 1u : 0u) << i;
-  if (a.bc1)
-#pragma unroll
-    for (int i = 0; i < 4; ++i) mc |= (__ldg(a.bc1 + cl[i]) ? 1u : 0u) << i;
+  for (int i = 0; i < 4; ++i) {
+    mr |= (r[i] < 0 || (a.bc0 && __ldg(a.bc0 + r[i])) ? 1u : 0u) << i;
+    mc |= (cl[i] < 0 || (a.bc1 && __ldg(a.bc1 + cl[i])) ? 1u : 0u) << i;
+  }
   int rp[4];
 #pragma unroll
-  for (int i = 0; i < 4; ++i) rp[i] = __ldg(a.row_ptr + r[i]);
+  for (int i = 0; i < 4; ++i) rp[i] = r[i] < 0 ? 0 : __ldg(a.row_ptr + r[i]);
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
@@ -210,11 +210,12 @@ __global__ void __launch_bounds__(kBlock) k_mat_p2_atomic(const MatArgs a) {
   const int32_t* d1 = a.dofs1 + c * 10;
 #pragma unroll
   for (int i = 0; i < 10; ++i) {
-    const int r = __ldg(d0 + i);
+    // masked rows / columns: BC dofs and dofs outside a restriction (-1)
+    const int r = __ldg(d0 + i), cc = __ldg(d1 + i);
     rd[i] = r;
-    rp[i] = __ldg(a.row_ptr + r);
-    if (a.bc0) mr |= (__ldg(a.bc0 + r) ? 1u : 0u) << i;
-    if (a.bc1) mc |= (__ldg(a.bc1 + __ldg(d1 + i)) ? 1u : 0u) << i;
+    rp[i] = r < 0 ? 0 : __ldg(a.row_ptr + r);
+    mr |= (r < 0 || (a.bc0 && __ldg(a.bc0 + r)) ? 1u : 0u) << i;
+    mc |= (cc < 0 || (a.bc1 && __ldg(a.bc1 + cc)) ? 1u : 0u) << i;
   }
   double* __restrict__ vals = a.values;
   const bool upper = a.upper != 0;
@@ -284,11 +285,12 @@ __global__ void __launch_bounds__(kBlockP3) k_mat_p3_atomic(const MatArgs a) {
   const int32_t* d1 = a.dofs1 + c * 20;
 #pragma unroll
   for (int i = 0; i < 20; ++i) {
-    const int r = __ldg(d0 + i);
+    // masked rows / columns: BC dofs and dofs outside a restriction (-1)
+    const int r = __ldg(d0 + i), cc = __ldg(d1 + i);
     rd[i] = r;
-    rp[i] = __ldg(a.row_ptr + r);
-    if (a.bc0) mr |= (__ldg(a.bc0 + r) ? 1u : 0u) << i;
-    if (a.bc1) mc |= (__ldg(a.bc1 + __ldg(d1 + i)) ? 1u : 0u) << i;
+    rp[i] = r < 0 ? 0 : __ldg(a.row_ptr + r);
+    mr |= (r < 0 || (a.bc0 && __ldg(a.bc0 + r)) ? 1u : 0u) << i;
+    mc |= (cc < 0 || (a.bc1 && __ldg(a.bc1 + cc)) ? 1u : 0u) << i;
   }
   double* __restrict__ vals = a.values;
   const bool upper = a.upper != 0;
@@ -364,15 +366,16 @@ __global__ void __launch_bounds__(kBlock) k_mat_vp2_atomic(const MatArgs a) {
   const int32_t* d1 = a.dofs1 + c * 10;
 #pragma unroll
   for (int i = 0; i < 10; ++i) {
+    // masked rows / columns: BC dofs and nodes outside a restriction (-1)
     const int R = __ldg(d0 + i);
-    rd[i] = R;
-    rp[i] = __ldg(a.row_ptr + 3 * R);
-    L[i] = __ldg(a.row_ptr + 3 * R + 1) - rp[i];
     const int C = __ldg(d1 + i);
+    rd[i] = R;
+    rp[i] = R < 0 ? 0 : __ldg(a.row_ptr + 3 * R);
+    L[i] = R < 0 ? 0 : __ldg(a.row_ptr + 3 * R + 1) - rp[i];
 #pragma unroll
     for (int q = 0; q < 3; ++q) {
-      if (a.bc0) mr |= (__ldg(a.bc0 + 3 * R + q) ? 1u : 0u) << (3 * i + q);
-      if (a.bc1) mc |= (__ldg(a.bc1 + 3 * C + q) ? 1u : 0u) << (3 * i + q);
+      mr |= (R < 0 || (a.bc0 && __ldg(a.bc0 + 3 * R + q)) ? 1u : 0u) << (3 * i + q);
+      mc |= (C < 0 || (a.bc1 && __ldg(a.bc1 + 3 * C + q)) ? 1u : 0u) << (3 * i + q);
     }
   }
   double* __restrict__ vals = a.values;
@@ -533,6 +536,77 @@ __global__ void k_build_slotmap(const int32_t* __restrict__ dofs0, const int32_t
   }
 }
 
+// Block view of a monolithic pattern: for local scalar row rl of a block form
+// placed at (row_offset, col_offset), the first slot of monolithic row
+// row_offset + rl whose column is >= col_offset (the block's column segment),
+// and that row's diagonal slot.
+__global__ void k_view_rows(const int32_t* __restrict__ row_ptr, const int32_t* __restrict__ col,
+                            const int32_t* __restrict__ diag, int64_t row_offset, int64_t col_offset,
+                            int64_t num_local_rows, int32_t* __restrict__ seg, int32_t* __restrict__ vdiag) {
+  const int64_t rl = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (rl >= num_local_rows) return;
+  const int64_t r = row_offset + rl;
+  int32_t a = row_ptr[r], b = row_ptr[r + 1];
+  while (a < b) {
+    const int32_t m = (a + b) >> 1;
+    if (col[m] < col_offset) a = m + 1;
+    else b = m;
+  }
+  seg[rl] = a;
+  vdiag[rl] = diag[r];
+}
+
+// Cell-to-slot map of a block form through its view: block position of
+// dofs1[c,j] inside the column segment of block row dofs0[c,i]; entries of
+// excluded dofs (-1) are 0 and never used.
+__global__ void k_build_slotmap_view(const int32_t* __restrict__ dofs0, const int32_t* __restrict__ dofs1,
+                                     int64_t num_cells, int k0, int k1, int bs0, int bs1,
+                                     const int32_t* __restrict__ row_ptr, const int32_t* __restrict__ col,
+                                     const int32_t* __restrict__ seg, int64_t row_offset, int64_t col_offset,
+                                     uint8_t* __restrict__ pos, unsigned* err) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= num_cells * k0) return;
+  const int64_t c = t / k0;
+  const int64_t R = dofs0[t];
+  if (R < 0) {
+    for (int j = 0; j < k1; ++j) pos[t * k1 + j] = 0;
+    return;
+  }
+  const int64_t rl = R * bs0;
+  const int32_t lo = seg[rl], hi = row_ptr[row_offset + rl + 1];
+  const int32_t L = bs0 > 1 ? seg[rl + 1] - lo : 0;
+  for (int j = 0; j < k1; ++j) {
+    const int64_t C = dofs1[c * k1 + j];
+    uint8_t out = 0;
+    if (C >= 0) {
+      const int64_t key = col_offset + C * bs1;
+      int32_t a = lo, b = hi;
+      while (a < b) {
+        const int32_t m = (a + b) >> 1;
+        if (col[m] < key) a = m + 1;
+        else b = m;
+      }
+      if (a >= hi || col[a] != key) {
+        raise_err(err, DEV_ERR_PATTERN);
+      } else {
+        const int32_t off = a - lo;
+        if (off % bs1) raise_err(err, DEV_ERR_BLOCK);
+        const int32_t pb = off / bs1;
+        if (pb > 255) raise_err(err, DEV_ERR_ROW_WIDE);
+        else out = (uint8_t)pb;
+        for (int q = 1; q < bs1; ++q)
+          if (a + q >= hi || col[a + q] != key + q) raise_err(err, DEV_ERR_BLOCK);
+        // the component rows of a block row: equal lengths, same segment layout
+        for (int q = 1; q < bs0; ++q) {
+          const int32_t sq = seg[rl + q], eq = row_ptr[row_offset + rl + q + 1];
+          if (sq - lo != q * L || sq + off >= eq || col[sq + off] != key) raise_err(err, DEV_ERR_BLOCK);
+        }
+      }
+    }
+    pos[t * k1 + j] = out;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Vector assembly (element vector -> atomicAdd), CUDAFormIntegral.cpp:270-357
 // ---------------------------------------------------------------------------
@@ -654,7 +728,7 @@ __global__ void __launch_bounds__(kBlock) k_lift_p1(const LiftArgs a) {
   double dv[4];
 #pragma unroll
   for (int j = 0; j < 4; ++j)
-    dv[j] = __ldg(a.bc1 + cl[j]) ? (__ldg(a.g + cl[j]) - (a.x0 ? __ldg(a.x0 + cl[j]) : 0.0)) : 0.0;
+    dv[j] = cl[j] >= 0 && __ldg(a.bc1 + cl[j]) ? (__ldg(a.g + cl[j]) - (a.x0 ? __ldg(a.x0 + cl[j]) : 0.0)) : 0.0;
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
     double acc = 0.0;
@@ -679,7 +753,7 @@ __global__ void __launch_bounds__(kBlock) k_lift_p2(const LiftArgs a) {
 #pragma unroll
   for (int j = 0; j < 10; ++j) {
     const int C = __ldg(d1 + j);
-    dv[j] = __ldg(a.bc1 + C) ? (__ldg(a.g + C) - (a.x0 ? __ldg(a.x0 + C) : 0.0)) : 0.0;
+    dv[j] = C >= 0 && __ldg(a.bc1 + C) ? (__ldg(a.g + C) - (a.x0 ? __ldg(a.x0 + C) : 0.0)) : 0.0;
     be[j] = 0.0;
   }
   auto emit = [&](int i, int j, double v) {
@@ -722,7 +796,7 @@ __global__ void __launch_bounds__(kBlockP3) k_lift_p3(const LiftArgs a) {
 #pragma unroll
   for (int j = 0; j < 20; ++j) {
     const int C = __ldg(d1 + j);
-    dv[j] = __ldg(a.bc1 + C) ? (__ldg(a.g + C) - (a.x0 ? __ldg(a.x0 + C) : 0.0)) : 0.0;
+    dv[j] = C >= 0 && __ldg(a.bc1 + C) ? (__ldg(a.g + C) - (a.x0 ? __ldg(a.x0 + C) : 0.0)) : 0.0;
     be[j] = 0.0;
   }
   const double k = coef_cell(a.c0, c);
@@ -754,7 +828,7 @@ __global__ void __launch_bounds__(kBlock) k_lift_vp2(const LiftArgs a) {
 #pragma unroll
     for (int q = 0; q < 3; ++q) {
       const int64_t s = 3 * C + q;
-      dv[3 * j + q] = __ldg(a.bc1 + s) ? (__ldg(a.g + s) - (a.x0 ? __ldg(a.x0 + s) : 0.0)) : 0.0;
+      dv[3 * j + q] = C >= 0 && __ldg(a.bc1 + s) ? (__ldg(a.g + s) - (a.x0 ? __ldg(a.x0 + s) : 0.0)) : 0.0;
       be[3 * j + q] = 0.0;
     }
   }
@@ -778,6 +852,7 @@ __global__ void k_mark_cells(const int32_t* __restrict__ dofs, int64_t num_cells
   bool any = false;
   for (int i = 0; i < k && !any; ++i) {
     const int64_t D = dofs[c * k + i];
+    if (D < 0) continue;  // outside a restriction
     for (int q = 0; q < bs; ++q) any |= markers[D * bs + q] != 0;
   }
   if (any) out[atomicAdd(count, 1ull)] = (int32_t)c;
@@ -820,6 +895,26 @@ void launch_build_slotmap(const fe_form_s& f, cudaStream_t s) {
   k_build_slotmap<<<grid_for(n, 256), 256, 0, s>>>(V0.dofs.p, V1.dofs.p, V0.num_cells, V0.k, V1.k, V0.bs,
                                                    V1.bs, f.sp->row_ptr.p, f.sp->col.p, f.sp->num_rows,
                                                    f.pos.p, device_error_word(f.ctx));
+  FE_CUDA(cudaGetLastError());
+}
+
+void launch_build_view(const fe_form_s& f, const fe_sparsity_s& mono, int64_t row_offset, int64_t col_offset,
+                       fe_sparsity_s& view, cudaStream_t s) {
+  const fe_dofmap_s& V0 = *f.V0;
+  const fe_dofmap_s& V1 = *f.V1;
+  const int64_t nrows = V0.num_blocks * V0.bs;
+  view.row_ptr.alloc(nrows + 1);
+  view.diag.alloc(std::max<int64_t>(1, nrows));
+  FE_CUDA(cudaMemsetAsync(view.row_ptr.p, 0, (nrows + 1) * sizeof(int32_t), s));
+  if (nrows)
+    k_view_rows<<<grid_for(nrows, 256), 256, 0, s>>>(mono.row_ptr.p, mono.col.p, mono.diag.p, row_offset, col_offset,
+                                                     nrows, view.row_ptr.p, view.diag.p);
+  FE_CUDA(cudaGetLastError());
+  const int64_t n = V0.num_cells * V0.k;
+  if (n)
+    k_build_slotmap_view<<<grid_for(n, 256), 256, 0, s>>>(V0.dofs.p, V1.dofs.p, V0.num_cells, V0.k, V1.k, V0.bs, V1.bs,
+                                                          mono.row_ptr.p, mono.col.p, view.row_ptr.p, row_offset,
+                                                          col_offset, f.pos.p, device_error_word(f.ctx));
   FE_CUDA(cudaGetLastError());
 }
 

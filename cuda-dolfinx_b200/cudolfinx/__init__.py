@@ -10,7 +10,7 @@ from .assemble import CUDAAssembler
 from .batch import AssemblyGraph, VariantTuner
 from .bcs import CUDADirichletBC
 from .context import get_cuda_context
-from .form import CUDAForm, form
+from .form import BlockCUDAForm, CUDAForm, form
 from .la import CUDAMatrix, CUDAVector, Sparsity
 
 
@@ -25,5 +25,5 @@ def release_caches(mesh=None):
     release_device_caches(mesh)
 
 
-__all__ = ["AssemblyGraph", "CUDAAssembler", "CUDADirichletBC", "CUDAForm", "CUDAMatrix", "CUDAVector", "Sparsity", "fem", "form",
+__all__ = ["AssemblyGraph", "BlockCUDAForm", "CUDAAssembler", "CUDADirichletBC", "CUDAForm", "CUDAMatrix", "CUDAVector", "Sparsity", "fem", "form",
            "get_cuda_context", "release_caches", "VariantTuner"]

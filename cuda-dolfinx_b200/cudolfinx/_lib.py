@@ -52,9 +52,11 @@ _SIGS = {
     "fe_mesh_create": (i32, [vp, vp, i64, vp, i64, i32, PP]),
     "fe_mesh_destroy": (i32, [vp]),
     "fe_dofmap_create": (i32, [vp, vp, i64, i32, i32, i64, PP]),
+    "fe_dofmap_create_restricted": (i32, [vp, vp, i64, i32, i32, i64, PP]),
     "fe_dofmap_destroy": (i32, [vp]),
     "fe_sparsity_build": (i32, [vp, vp, PP]),
     "fe_sparsity_build_device": (i32, [vp, vp, vp, PP]),
+    "fe_sparsity_build_block": (i32, [vp, i32, vp, vp, vp, vp, i64, i64, PP]),
     "fe_sparsity_create": (i32, [vp, vp, vp, i64, i64, PP]),
     "fe_sparsity_info": (i32, [vp, ctypes.POINTER(i64), ctypes.POINTER(i64), ctypes.POINTER(i64)]),
     "fe_sparsity_copy_to_host": (i32, [vp, vp, vp]),
@@ -68,6 +70,7 @@ _SIGS = {
     "fe_form_set_facets": (i32, [vp, vp, i64]),
     "fe_assemble_scalar": (i32, [vp, ctypes.POINTER(dbl), vp]),
     "fe_form_bind_sparsity": (i32, [vp, vp, vp]),
+    "fe_form_bind_sparsity_block": (i32, [vp, vp, i64, i64, vp]),
     "fe_form_destroy": (i32, [vp]),
     "fe_bc_create": (i32, [vp, i64, vp, vp, i64, i64, vp, PP]),
     "fe_bc_update": (i32, [vp, vp, vp]),

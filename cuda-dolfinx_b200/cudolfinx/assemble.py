@@ -8,9 +8,11 @@ rows/columns skipped and sets ``diagonal`` on owned BC rows;
 current stream (the reference synchronises after every kernel);
 ``diagonal`` is honoured (the reference's binding always uses 1.0,
 wrappers/fem.cpp:274); ``scale`` stays double (the reference's binding
-takes a C float, wrappers/fem.cpp:335, 361); block/restricted assembly is outside
-this engine.  ``assemble_scalar`` returns the functional's value with a
-fixed-order reduction.  Additions: ``deterministic=True`` selects a
+takes a C float, wrappers/fem.cpp:335, 361).  Block forms (``cudolfinx.form``
+of a list / list of lists, optionally restricted) assemble into one monolithic
+matrix / vector with ``assemble_matrix_block`` / ``assemble_vector_block``
+(assemble.py:112-202).  ``assemble_scalar`` returns the functional's value with
+a fixed-order reduction.  Additions: ``deterministic=True`` selects a
 bitwise-reproducible matrix variant, ``assemble_matrix_batch`` assembles many
 coefficient instances at once, and ``solve`` runs the on-device Jacobi-PCG.
 """
@@ -25,7 +27,7 @@ from . import _lib
 from .bcs import CUDADirichletBC
 from .context import get_cuda_context
 from .fem import DirichletBC, FunctionSpace
-from .form import CUDAForm
+from .form import BlockCUDAForm, CUDAForm
 from .la import CUDAMatrix, CUDAVector, Sparsity
 
 _sparsity_cache: dict = {}
@@ -50,6 +52,13 @@ class CUDAAssembler:
             raise TypeError(f"Expected CUDAForm, got type '{type(a)}'.")
         if a.rank != 2:
             raise ValueError("create_matrix needs a bilinear form")
+        if a.restriction(0) is not None or a.restriction(1) is not None:
+            # a restricted form is a one-block system
+            sp = Sparsity.build_block(self._ctx, [(a._dofmaps[0], a._dofmaps[1], 0, 0)], a.space_size(0),
+                                      a.space_size(1))
+            mat = CUDAMatrix(self._ctx, sp)
+            a._bind_block(sp, 0, 0)
+            return mat
         key = (id(a._dofmaps[0]), id(a._dofmaps[1]))
         entry = _sparsity_cache.get(key)
         if entry is None or entry[0] is not a._dofmaps[0] or entry[1] is not a._dofmaps[1]:
@@ -63,7 +72,32 @@ class CUDAAssembler:
     def create_vector(self, b: CUDAForm) -> CUDAVector:
         if not isinstance(b, CUDAForm):
             raise TypeError(f"Expected CUDAForm, got type '{type(b)}'.")
-        return CUDAVector(self._ctx, b.function_spaces[0].num_dofs)
+        return CUDAVector(self._ctx, b.space_size(0))
+
+    def create_matrix_block(self, a: BlockCUDAForm) -> CUDAMatrix:
+        """Monolithic matrix of a block form (create_matrix_block,
+        assemble.py:236-243 -> cpp/cudolfinx/fem/petsc.h:39-107); every block
+        form is bound to it at its offsets."""
+        if not isinstance(a, BlockCUDAForm):
+            raise TypeError(f"Expected BlockCUDAForm, got type '{type(a)}'")
+        parts = [(f._dofmaps[0], f._dofmaps[1], a.row_offsets[i], a.col_offsets[j])
+                 for i, row in enumerate(a.forms) for j, f in enumerate(row) if f is not None]
+        sp = Sparsity.build_block(self._ctx, parts, a.row_offsets[-1], a.col_offsets[-1])
+        mat = CUDAMatrix(self._ctx, sp)
+        self._bind_blocks(a, mat)
+        return mat
+
+    def _bind_blocks(self, a: BlockCUDAForm, mat: CUDAMatrix):
+        for i, row in enumerate(a.forms):
+            for j, f in enumerate(row):
+                if f is not None:
+                    f._bind_block(mat.sparsity, a.row_offsets[i], a.col_offsets[j])
+
+    def create_vector_block(self, b: BlockCUDAForm) -> CUDAVector:
+        """Monolithic vector of a block linear form (assemble.py:255-262)."""
+        if not isinstance(b, BlockCUDAForm):
+            raise TypeError(f"Expected BlockCUDAForm, got type '{type(b)}')")
+        return CUDAVector(self._ctx, b.local_size)
 
     def pack_bcs(self, bcs: list[DirichletBC]) -> CUDADirichletBC:
         return CUDADirichletBC(self._ctx, bcs)
@@ -106,8 +140,8 @@ class CUDAAssembler:
         else:
             a._bind(mat.sparsity)
         col = self._bc_collection(bcs)
-        bc0 = col._get_cpp_bcs(a.function_spaces[0])
-        bc1 = col._get_cpp_bcs(a.function_spaces[1])
+        bc0 = col._get_cpp_bcs(a.function_spaces[0], a.restriction(0))
+        bc1 = col._get_cpp_bcs(a.function_spaces[1], a.restriction(1))
         # as the reference (assemble.py:100-103): always copy host coefficients to the device
         a.to_device()
         self.pack_coefficients(a, coeffs)
@@ -168,6 +202,57 @@ class CUDAAssembler:
             m._bcs = col
         return mats
 
+    def assemble_matrix_block(self, a: BlockCUDAForm, mat: typing.Optional[CUDAMatrix] = None, bcs=None,
+                              coeffs=None, constants=None, zero: bool = True, diagonal: float = 1.0) -> CUDAMatrix:
+        """Assemble a block form into one monolithic matrix (assemble.py:112-134):
+        zero it once, then add every block at its offsets.  ``bcs``: a list of
+        lists (the BCs of block (i, j), as the reference takes them) or one flat
+        list of DirichletBCs applied to every block by function space (rows on
+        the block's test space, columns on its trial space); owned BC rows get
+        ``diagonal`` on the monolithic diagonal."""
+        if not isinstance(a, BlockCUDAForm):
+            raise TypeError(f"Expected BlockCUDAForm, got '{type(a)}'")
+        if mat is None:
+            mat = self.create_matrix_block(a)
+        else:
+            self._bind_blocks(a, mat)
+        if zero:
+            _lib.check(_lib.lib.fe_zero_entries(mat.values.data_ptr(), mat.sparsity.nnz, self._ctx.stream()),
+                       "fe_zero_entries")
+        nested = bcs is not None and len(bcs) and isinstance(bcs[0], (list, tuple))
+        flat = None if (bcs is None or nested) else self._bc_collection(bcs)
+        for i, row in enumerate(a.forms):
+            for j, f in enumerate(row):
+                if f is None:
+                    continue
+                _bcs = (bcs[i][j] if nested else flat) if bcs is not None else []
+                _coeffs = coeffs[i][j] if coeffs is not None else None
+                self.assemble_matrix(f, mat, bcs=_bcs, coeffs=_coeffs, zero=False, diagonal=diagonal,
+                                     variant="atomic")
+        return mat
+
+    def assemble_vector_block(self, b: BlockCUDAForm, vec: typing.Optional[CUDAVector] = None, constants=None,
+                              coeffs=None, zero: bool = True) -> CUDAVector:
+        """Assemble a block linear form into one vector, block i at offsets[i]
+        (assemble.py:168-202)."""
+        if not isinstance(b, BlockCUDAForm):
+            raise TypeError(f"Expected BlockCUDAForm, got '{type(b)}'")
+        if vec is None:
+            vec = self.create_vector_block(b)
+        n = len(b.forms)
+        _coeffs = [None] * n if coeffs is None else coeffs
+        if len(_coeffs) != n:
+            raise ValueError(f"Expected coeffs to be None or a list of length: '{n}', got '{len(_coeffs)}' instead!")
+        if zero:
+            vec.vector.zero_()
+        base = vec.vector.data_ptr()
+        for f, off, c in zip(b.forms, b.offsets, _coeffs):
+            f.to_device()
+            self.pack_coefficients(f, c)
+            _lib.check(_lib.lib.fe_assemble_vector(f.cuda_form, base + 8 * off, 0, self._ctx.stream()),
+                       "fe_assemble_vector")
+        return vec
+
     def assemble_scalar(self, b: CUDAForm, constants=None, coeffs=None) -> float:
         """Value of a functional (assemble.py:204-226); the reduction runs in a
         fixed order, so the value is reproducible bit for bit."""
@@ -217,7 +302,7 @@ class CUDAAssembler:
             self.pack_coefficients(f, c)
             col = self._bc_collection(bc)
             keep.append(col)
-            d = col._get_cpp_bcs(f.function_spaces[1])
+            d = col._get_cpp_bcs(f.function_spaces[1], f.restriction(1))
             forms[i] = f.cuda_form
             hbcs[i] = d.handle if d else None
             hx0[i] = x0[i].vector.data_ptr() if (x0 is not None and x0[i] is not None) else None
@@ -226,10 +311,11 @@ class CUDAAssembler:
         b._keep = keep
 
     def set_bc(self, b: CUDAVector, bcs, V: FunctionSpace, x0: typing.Optional[CUDAVector] = None,
-               scale: float = 1.0):
-        """b[bc dofs] = scale * (g - x0) on the BCs of V."""
+               scale: float = 1.0, restriction: typing.Optional[np.ndarray] = None):
+        """b[bc dofs] = scale * (g - x0) on the BCs of V (in the numbering of
+        `restriction`, the kept dofs of V, when b lives on a restricted space)."""
         col = self._bc_collection(bcs)
-        d = col._get_cpp_bcs(V)
+        d = col._get_cpp_bcs(V, restriction)
         if d is None:
             return
         _lib.check(_lib.lib.fe_set_bc(b.vector.data_ptr(), b.size, d.handle,

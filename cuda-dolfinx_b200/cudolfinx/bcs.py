@@ -44,6 +44,47 @@ class _DeviceBC:
             vals = bc.values()
             self.g[bc.dofs] = vals[bc.dofs]
         _lib.check(_lib.lib.fe_bc_update(self.handle, self.g.ctypes.data, self.ctx.stream()), "fe_bc_update")
+        for r in getattr(self, "_restricted", {}).values():
+            r.refresh()
+
+    def restricted(self, restriction: np.ndarray) -> "_RestrictedBC":
+        """The same BCs in the numbering of a restricted space (kept block
+        dofs `restriction`, sorted): BC dofs outside it are dropped."""
+        if not hasattr(self, "_restricted"):
+            self._restricted = {}
+        key = np.ascontiguousarray(restriction, dtype=np.int32).tobytes()
+        r = self._restricted.get(key)
+        if r is None:
+            r = _RestrictedBC(self, np.frombuffer(key, dtype=np.int32))
+            self._restricted[key] = r
+        return r
+
+    def __del__(self):
+        if getattr(self, "handle", None):
+            _lib.lib.fe_bc_destroy(self.handle)
+            self.handle = None
+
+
+class _RestrictedBC:
+    """Device BC object of a restricted space, derived from a _DeviceBC."""
+
+    def __init__(self, parent: _DeviceBC, restriction: np.ndarray):
+        self.parent = parent
+        bs = parent.V.bs
+        self.kept = (restriction.astype(np.int64)[:, None] * bs + np.arange(bs)).ravel()
+        self.markers = np.ascontiguousarray(parent.markers[self.kept])
+        self.dofs = np.ascontiguousarray(np.nonzero(self.markers)[0].astype(np.int32))
+        self.g = np.ascontiguousarray(parent.g[self.kept])
+        h = _lib.out_handle()
+        n = len(self.kept)
+        _lib.check(_lib.lib.fe_bc_create(parent.ctx.handle, n, self.markers.ctypes.data,
+                                         self.dofs.ctypes.data if len(self.dofs) else None, len(self.dofs),
+                                         len(self.dofs), self.g.ctypes.data, h), "fe_bc_create")
+        self.handle = h.value
+
+    def refresh(self):
+        self.g[:] = self.parent.g[self.kept]
+        _lib.check(_lib.lib.fe_bc_update(self.handle, self.g.ctypes.data, self.parent.ctx.stream()), "fe_bc_update")
 
     def __del__(self):
         if getattr(self, "handle", None):
@@ -70,11 +111,12 @@ class CUDADirichletBC:
                 self._bc_lists.append([bc])
         self._device_bcs = [_DeviceBC(ctx, V, L) for V, L in zip(self._function_spaces, self._bc_lists)]
 
-    def _get_cpp_bcs(self, V: FunctionSpace):
-        """Device BC object for V, or None (no BCs on V) like the reference's empty collection."""
+    def _get_cpp_bcs(self, V: FunctionSpace, restriction: typing.Optional[np.ndarray] = None):
+        """Device BC object for V (in the numbering of `restriction` when
+        given), or None (no BCs on V) like the reference's empty collection."""
         for W, d in zip(self._function_spaces, self._device_bcs):
             if W is V:
-                return d
+                return d if restriction is None else d.restricted(restriction)
         return None
 
     def update(self, bcs: typing.Optional[typing.List[DirichletBC]] = None):

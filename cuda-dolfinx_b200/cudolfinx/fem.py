@@ -271,31 +271,46 @@ class FormSpec:
     precision: str = "fp64"
     facets: Optional[np.ndarray] = None  # exterior-facet forms: [F, 2] (cell, local facet)
     domain: Optional["Mesh"] = None      # functionals: the mesh (V may be None)
+    W: Optional[FunctionSpace] = None    # bilinear forms: trial space when it is not V
 
     @property
     def function_spaces(self):
         if self.rank == 0:
             return []
-        return [self.V, self.V] if self.rank == 2 else [self.V]
+        return [self.V, self.W if self.W is not None else self.V] if self.rank == 2 else [self.V]
 
     @property
     def mesh(self):
         return self.domain if self.domain is not None else self.V.mesh
 
 
-def stiffness(V: FunctionSpace, k: Coefficient = 1.0, precision: str = "fp64") -> FormSpec:
-    """k * inner(grad(u), grad(v)) * dx on a scalar P1/P2 space."""
+def _trial(V: FunctionSpace, trial: Optional[FunctionSpace]) -> Optional[FunctionSpace]:
+    if trial is None or trial is V:
+        return None
+    if (trial.mesh is not V.mesh or trial.family != V.family or trial.degree != V.degree or trial.bs != V.bs
+            or not np.array_equal(trial.dofs, V.dofs)):
+        raise ValueError("the trial space must be another copy of the test space's element on the same mesh")
+    return trial
+
+
+def stiffness(V: FunctionSpace, k: Coefficient = 1.0, precision: str = "fp64",
+              trial: Optional[FunctionSpace] = None) -> FormSpec:
+    """k * inner(grad(u), grad(v)) * dx on a scalar P1/P2/P3 space; u from
+    ``trial`` (another space of the same element, e.g. the second field of a
+    block system) when given."""
     if V.bs != 1 or V.family != "P":
         raise ValueError("stiffness needs a scalar Lagrange space")
     kind = {1: "P1_STIFFNESS", 2: "P2_STIFFNESS", 3: "P3_STIFFNESS"}[V.degree]
-    return FormSpec(kind, V, [k], 2, precision)
+    return FormSpec(kind, V, [k], 2, precision, W=_trial(V, trial))
 
 
-def elasticity(V: FunctionSpace, lam: Coefficient, mu: Coefficient, precision: str = "fp64") -> FormSpec:
-    """2 mu eps(u):eps(v) + lam div(u) div(v) on a vector P2 space."""
+def elasticity(V: FunctionSpace, lam: Coefficient, mu: Coefficient, precision: str = "fp64",
+               trial: Optional[FunctionSpace] = None) -> FormSpec:
+    """2 mu eps(u):eps(v) + lam div(u) div(v) on a vector P2 space (u from
+    ``trial`` when given, as for ``stiffness``)."""
     if V.bs != 3 or V.degree != 2:
         raise ValueError("elasticity needs a vector P2 space")
-    return FormSpec("VP2_ELASTICITY", V, [lam, mu], 2, precision)
+    return FormSpec("VP2_ELASTICITY", V, [lam, mu], 2, precision, W=_trial(V, trial))
 
 
 # facet f of a tetrahedron is the one opposite vertex f (basix / DOLFINx)

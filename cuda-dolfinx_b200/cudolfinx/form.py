@@ -41,14 +41,37 @@ class DeviceMesh:
 
 
 class DeviceDofMap:
-    def __init__(self, ctx, V: FunctionSpace):
+    """Device dofmap of V; with ``restriction`` (sorted block dofs of V that
+    are kept) the cell dofs are renumbered to positions in the restriction and
+    dofs outside it become -1 (CUDADofMap::update with a restriction map,
+    cpp/cudolfinx/fem/CUDADofMap.cpp:199-236)."""
+
+    def __init__(self, ctx, V: FunctionSpace, restriction: typing.Optional[np.ndarray] = None):
         self.ctx = ctx
         self.V = V
+        self.restriction = None if restriction is None else np.ascontiguousarray(restriction, dtype=np.int32)
         h = _lib.out_handle()
-        d = np.ascontiguousarray(V.dofs, dtype=np.int32)
-        _lib.check(_lib.lib.fe_dofmap_create(ctx.handle, d.ctypes.data, d.shape[0], d.shape[1], V.bs,
-                                             V.num_nodes, h), "fe_dofmap_create")
+        if self.restriction is None:
+            d = np.ascontiguousarray(V.dofs, dtype=np.int32)
+            self.num_blocks = V.num_nodes
+            _lib.check(_lib.lib.fe_dofmap_create(ctx.handle, d.ctypes.data, d.shape[0], d.shape[1], V.bs,
+                                                 V.num_nodes, h), "fe_dofmap_create")
+        else:
+            r = self.restriction
+            if r.size and (r.min() < 0 or r.max() >= V.num_nodes or np.any(np.diff(r) <= 0)):
+                raise ValueError("a restriction is a sorted list of distinct dofs of the space")
+            remap = np.full(V.num_nodes, -1, dtype=np.int32)
+            remap[r] = np.arange(len(r), dtype=np.int32)
+            d = np.ascontiguousarray(remap[V.dofs])
+            self.num_blocks = len(r)
+            _lib.check(_lib.lib.fe_dofmap_create_restricted(ctx.handle, d.ctypes.data, d.shape[0], d.shape[1],
+                                                            V.bs, len(r), h), "fe_dofmap_create_restricted")
         self.handle = h.value
+
+    @property
+    def size(self) -> int:
+        """Scalar dofs of the (restricted) space."""
+        return self.num_blocks * self.V.bs
 
     def __del__(self):
         if getattr(self, "handle", None):
@@ -94,6 +117,15 @@ class CUDAForm:
         self._cuda_mesh = _create_mesh_on_device(self._ctx, form.mesh)
         self._dofmaps = [device_dofmap(self._ctx, V) for V in form.function_spaces]
         self._jit_args = dict(DEFAULT_CUDA_JIT_ARGS, **(jit_args or {}))
+        self._handle = None
+        self._create_handle()
+
+    def _create_handle(self):
+        """(Re)create the engine form on the current dofmaps."""
+        form = self._spec
+        if self._handle:
+            _lib.lib.fe_form_destroy(self._handle)
+            self._handle = None
         h = _lib.out_handle()
         trial = self._dofmaps[1].handle if form.rank == 2 else None
         test = self._dofmaps[0].handle if form.rank >= 1 else None
@@ -110,6 +142,30 @@ class CUDAForm:
         self._coef_refs: list = [None] * len(form.coefficients)
         self._aux_dofmaps: dict = {}
         self.to_device()
+
+    # -- restriction (CUDAForm::set_restriction, cpp/cudolfinx/fem/CUDAForm.h:201-232) --
+    def set_restriction(self, restrictions: typing.Sequence[typing.Optional[np.ndarray]]):
+        """Restrict the form's spaces (one entry per argument, None = the whole
+        space): cell dofs outside a restriction take no entries and the kept
+        dofs are numbered by their position in it."""
+        if len(restrictions) != self.rank:
+            raise ValueError("Number of restrictions must equal arity of form (1 for vector, 2 for matrix)!")
+        old = [dm.restriction for dm in self._dofmaps]
+        new = [None if r is None else np.ascontiguousarray(r, dtype=np.int32) for r in restrictions]
+        if all((o is None and n is None) or (o is not None and n is not None and np.array_equal(o, n))
+               for o, n in zip(old, new)):
+            return
+        self._dofmaps = [device_dofmap(self._ctx, V) if r is None else DeviceDofMap(self._ctx, V, r)
+                         for V, r in zip(self._spec.function_spaces, new)]
+        self._create_handle()
+
+    def restriction(self, i: int):
+        """Restriction of argument i (None: the whole space)."""
+        return self._dofmaps[i].restriction
+
+    def space_size(self, i: int) -> int:
+        """Scalar size of argument i's (restricted) space."""
+        return self._dofmaps[i].size
 
     # -- coefficients -------------------------------------------------------
     def _set_coefficient(self, i: int, c):
@@ -168,6 +224,16 @@ class CUDAForm:
                        "fe_form_bind_sparsity")
             self._bound_sparsity = sparsity
 
+    def _bind_block(self, sparsity, row_offset: int, col_offset: int):
+        """Bind as block (i, j) of a monolithic pattern at scalar offsets."""
+        key = (row_offset, col_offset)
+        if self._bound_sparsity is not sparsity or getattr(self, "_block_offsets", None) != key:
+            _lib.check(_lib.lib.fe_form_bind_sparsity_block(self._handle, sparsity.handle, int(row_offset),
+                                                            int(col_offset), self._ctx.stream()),
+                       "fe_form_bind_sparsity_block")
+            self._bound_sparsity = sparsity
+            self._block_offsets = key
+
     # -- properties mirroring the reference --------------------------------
     @property
     def cuda_form(self):
@@ -195,13 +261,121 @@ class CUDAForm:
             self._handle = None
 
 
-def form(form: typing.Union[FormSpec, typing.Iterable[FormSpec]], restriction=None,
+class BlockCUDAForm:
+    """Forms of a block system (mirrors python/cudolfinx/form.py:107-225).
+
+    A list of linear forms is a block vector; a list of lists of bilinear
+    forms (None for an empty block) is a block matrix.  Block i occupies the
+    scalar range [offsets[i], offsets[i+1]) of the monolithic vector / matrix,
+    its size that of its (restricted) space.  ``restrictions``: for a vector
+    one array (or None) per form; for a matrix a pair (row restrictions,
+    column restrictions).  Each array lists the kept block dofs of the space,
+    sorted; kept dofs are numbered by their position in it."""
+
+    def __init__(self, forms, restrictions=None):
+        self._forms = forms
+        self._restrictions = restrictions
+        if not len(forms):
+            raise ValueError("Must provide at least one form!")
+        if isinstance(forms[0], CUDAForm):
+            self._init_vector()
+        else:
+            self._init_matrix()
+
+    @staticmethod
+    def _offsets(sizes):
+        off = [0]
+        for n in sizes:
+            off.append(off[-1] + n)
+        return off
+
+    def _init_vector(self):
+        for i, f in enumerate(self._forms):
+            if f.rank != 1:
+                raise ValueError("a block vector takes linear forms")
+            r = None if self._restrictions is None else self._restrictions[i]
+            f.set_restriction([r])
+        self._offsets_list = self._offsets([f.space_size(0) for f in self._forms])
+        self._row_offsets = self._col_offsets = self._offsets_list
+
+    def _init_matrix(self):
+        rows, cols = len(self._forms), len(self._forms[0])
+        if any(len(r) != cols for r in self._forms):
+            raise ValueError("a block matrix needs rows of equal length")
+        rr = [None] * rows if self._restrictions is None else list(self._restrictions[0])
+        cr = [None] * cols if self._restrictions is None else list(self._restrictions[1])
+        if len(rr) != rows or len(cr) != cols:
+            raise ValueError("one restriction per block row and per block column")
+        rsize, csize = [None] * rows, [None] * cols
+        for i, row in enumerate(self._forms):
+            for j, f in enumerate(row):
+                if f is None:
+                    continue
+                if f.rank != 2:
+                    raise ValueError("a block matrix takes bilinear forms")
+                f.set_restriction([rr[i], cr[j]])
+                for sizes, k, idx in ((rsize, 0, i), (csize, 1, j)):
+                    n = f.space_size(k)
+                    if sizes[idx] is not None and sizes[idx] != n:
+                        raise ValueError("the forms of a block row / column act on spaces of different sizes")
+                    sizes[idx] = n
+        if any(n is None for n in rsize) or any(n is None for n in csize):
+            raise ValueError("every block row and column needs at least one form")
+        self._row_offsets = self._offsets(rsize)
+        self._col_offsets = self._offsets(csize)
+        self._offsets_list = self._row_offsets
+
+    @property
+    def forms(self):
+        """Return the list of forms."""
+        return self._forms
+
+    @property
+    def dolfinx_forms(self):
+        return [f.dolfinx_form if isinstance(f, CUDAForm) else [g.dolfinx_form if g else None for g in f]
+                for f in self._forms]
+
+    @property
+    def offsets(self):
+        """Scalar offsets of the blocks (rows for a block matrix)."""
+        return self._offsets_list
+
+    @property
+    def row_offsets(self):
+        return self._row_offsets
+
+    @property
+    def col_offsets(self):
+        return self._col_offsets
+
+    @property
+    def local_size(self):
+        """Size of the monolithic vector (rows of the block matrix)."""
+        return self._offsets_list[-1]
+
+    @property
+    def global_size(self):
+        return self.local_size
+
+
+def form(form: typing.Union[FormSpec, typing.Iterable], restriction=None,
          cuda_jit_args: typing.Optional[dict] = None, **kwargs):
-    """Create a CUDAForm (or a list of them) from built-in form specs
-    (mirrors cudolfinx.form, python/cudolfinx/form.py:227-249).  Block forms
-    and restrictions are not part of this engine."""
-    if restriction is not None:
-        raise NotImplementedError("restricted/block forms are outside this engine")
+    """Create a CUDAForm from a built-in form spec, or a BlockCUDAForm from a
+    list of them (block vector) or a list of lists (block matrix, None for an
+    empty block) with optional restrictions (mirrors cudolfinx.form,
+    python/cudolfinx/form.py:227-249)."""
     if isinstance(form, FormSpec):
+        if restriction is not None:
+            f = CUDAForm(form, cuda_jit_args)
+            f.set_restriction(restriction)
+            return f
         return CUDAForm(form, cuda_jit_args)
-    return [CUDAForm(f, cuda_jit_args) for f in form]
+
+    def _create(x):
+        if x is None:
+            return None
+        if isinstance(x, FormSpec):
+            return CUDAForm(x, cuda_jit_args)
+        return [_create(y) for y in x]
+
+    return BlockCUDAForm(_create(form), restriction)

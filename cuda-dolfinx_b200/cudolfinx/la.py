@@ -44,6 +44,21 @@ class Sparsity:
         return cls(ctx, h.value)
 
     @classmethod
+    def build_block(cls, ctx, parts, num_rows: int, num_cols: int):
+        """Monolithic pattern of a block form (create_cuda_matrix_block,
+        cpp/cudolfinx/fem/petsc.h:39-107): ``parts`` = [(row dofmap, column
+        dofmap, row offset, column offset)], one per non-empty block."""
+        n = len(parts)
+        rows = (ctypes.c_void_p * max(1, n))(*[p[0].handle for p in parts])
+        cols = (ctypes.c_void_p * max(1, n))(*[p[1].handle for p in parts])
+        roff = np.ascontiguousarray([p[2] for p in parts] or [0], dtype=np.int64)
+        coff = np.ascontiguousarray([p[3] for p in parts] or [0], dtype=np.int64)
+        h = _lib.out_handle()
+        _lib.check(_lib.lib.fe_sparsity_build_block(ctx.handle, n, rows, cols, roff.ctypes.data, coff.ctypes.data,
+                                                    int(num_rows), int(num_cols), h), "fe_sparsity_build_block")
+        return cls(ctx, h.value)
+
+    @classmethod
     def from_csr(cls, ctx, row_ptr, col, num_cols):
         rp = np.ascontiguousarray(row_ptr, dtype=np.int32)
         cl = np.ascontiguousarray(col, dtype=np.int32)

@@ -131,6 +131,16 @@ int fe_mesh_destroy(fe_mesh m);
  * is derived in the kernels instead of storing the unrolled map. */
 int fe_dofmap_create(fe_context ctx, const int32_t* cell_dofs, int64_t num_cells,
                      int dofs_per_cell, int bs, int64_t num_blocks, fe_dofmap* out);
+/* A restricted dofmap (CUDADofMap::update with a restriction map,
+ * cpp/cudolfinx/fem/CUDADofMap.cpp:199-236, set by CUDAForm::set_restriction,
+ * cpp/cudolfinx/fem/CUDAForm.h:201-232): entries are block dofs of the
+ * restricted numbering 0..num_blocks-1, or -1 for a cell dof outside the
+ * restriction, which then takes no matrix, vector or lifting entry.  Forms on
+ * such dofmaps bind with fe_form_bind_sparsity_block and assemble with the
+ * atomic scatter; exterior-facet forms and coefficients take unrestricted
+ * dofmaps. */
+int fe_dofmap_create_restricted(fe_context ctx, const int32_t* cell_dofs, int64_t num_cells,
+                                int dofs_per_cell, int bs, int64_t num_blocks, fe_dofmap* out);
 int fe_dofmap_destroy(fe_dofmap d);
 
 /* ---- sparsity ------------------------------------------------------------ */
@@ -143,6 +153,16 @@ int fe_sparsity_build(fe_dofmap rows, fe_dofmap cols, fe_sparsity* out);
  * couplings, then the same unroll), bit-exact with fe_sparsity_build; for
  * callers that create many meshes.  Synchronises `stream`. */
 int fe_sparsity_build_device(fe_dofmap rows, fe_dofmap cols, void* stream, fe_sparsity* out);
+/* Replaces create_cuda_matrix_block (cpp/cudolfinx/fem/petsc.h:39-107): the
+ * monolithic scalar pattern of a block form.  Part p contributes the cell
+ * couplings of (rows[p], cols[p]) unrolled and shifted to scalar row
+ * row_offsets[p] and column col_offsets[p] (the offsets of BlockCUDAForm,
+ * python/cudolfinx/form.py:127-160); -1 entries of restricted dofmaps couple
+ * nothing.  Columns are sorted and unique per row (DOLFINx's block
+ * SparsityPattern at block size 1).  Built on the host. */
+int fe_sparsity_build_block(fe_context ctx, int num_parts, const fe_dofmap* rows, const fe_dofmap* cols,
+                            const int64_t* row_offsets, const int64_t* col_offsets, int64_t num_rows,
+                            int64_t num_cols, fe_sparsity* out);
 /* Adopt an existing pattern (e.g. the arrays of a PETSc AIJ matrix); host arrays. */
 int fe_sparsity_create(fe_context ctx, const int32_t* row_ptr, const int32_t* col,
                        int64_t num_rows, int64_t num_cols, fe_sparsity* out);
@@ -184,6 +204,16 @@ int fe_form_set_facets(fe_form f, const int32_t* cell_facet_pairs, int64_t num_f
  * unused lookup-table prototype, CUDAFormIntegral.cpp:1230-1407, made the
  * default).  Fails with FE_ERR_PATTERN if a cell coupling is missing. */
 int fe_form_bind_sparsity(fe_form f, fe_sparsity s, void* stream);
+/* Bind form (i, j) of a block form to a monolithic pattern with its rows at
+ * scalar row_offset and its columns at col_offset (set_restriction offsets,
+ * cpp/cudolfinx/fem/CUDAForm.h:201-232).  fe_assemble_matrix then adds the
+ * block into the monolithic value array: FE_ASM_ZERO zeroes all of it, owned
+ * BC rows of bc0 get the diagonal on the monolithic diagonal; the atomic
+ * scatter only (assemble_matrix_block, python/cudolfinx/assemble.py:112-134,
+ * calls it per block with zero=False).  Fails with FE_ERR_PATTERN if a
+ * coupling is missing from the pattern. */
+int fe_form_bind_sparsity_block(fe_form f, fe_sparsity s, int64_t row_offset, int64_t col_offset,
+                                void* stream);
 int fe_form_destroy(fe_form f);
 
 /* ---- Dirichlet BCs ------------------------------------------------------- */

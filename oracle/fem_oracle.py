@@ -633,6 +633,92 @@ def set_bc(b, bc_dofs, g, x0=None, scale=1.0):
 
 
 # ---------------------------------------------------------------------------
+# Block / restricted systems (python/cudolfinx/form.py:107-225,
+# assemble.py:112-202, cpp/cudolfinx/fem/petsc.h:39-107, fem/utils.h:14-98)
+# ---------------------------------------------------------------------------
+
+def restricted_dofmap(dofs, restriction, num_blocks):
+    """Cell dofs renumbered to their position in `restriction` (sorted kept
+    block dofs), -1 outside it (CUDADofMap::update with a restriction map,
+    cpp/cudolfinx/fem/CUDADofMap.cpp:199-236)."""
+    remap = np.full(num_blocks, -1, dtype=np.int64)
+    remap[np.asarray(restriction)] = np.arange(len(restriction))
+    return remap[np.asarray(dofs)]
+
+
+def scalar_cell_dofs(dofs, bs):
+    """[C, k*bs] scalar dofs dof*bs + comp, -1 where the block dof is -1."""
+    d = np.asarray(dofs, dtype=np.int64)
+    s = (d[:, :, None] * bs + np.arange(bs)).reshape(d.shape[0], -1)
+    s[np.repeat(d < 0, bs, axis=1)] = -1
+    return s
+
+
+def _couplings(d0, d1, bs0, bs1):
+    s0, s1 = scalar_cell_dofs(d0, bs0), scalar_cell_dofs(d1, bs1)
+    R = np.broadcast_to(s0[:, :, None], (s0.shape[0], s0.shape[1], s1.shape[1]))
+    C = np.broadcast_to(s1[:, None, :], R.shape)
+    return R, C, (R >= 0) & (C >= 0)
+
+
+def block_pattern(parts, num_rows, num_cols):
+    """Monolithic scalar CSR of a block system: the union of every part's cell
+    couplings placed at its offsets, sorted unique columns per row (DOLFINx's
+    block SparsityPattern at block size 1, as create_cuda_matrix_block builds
+    it, cpp/cudolfinx/fem/petsc.h:39-107; restricted couplings as in
+    compute_restricted_sparsity_pattern, fem/utils.h:14-98).
+    parts = [(dofs0, dofs1, bs0, bs1, row_offset, col_offset)], -1 = excluded."""
+    keys = [np.zeros(0, dtype=np.int64)]
+    for d0, d1, bs0, bs1, ro, co in parts:
+        R, C, m = _couplings(d0, d1, bs0, bs1)
+        keys.append((ro + R[m]) * num_cols + (co + C[m]))
+    k = np.unique(np.concatenate(keys))
+    rows, cols = k // num_cols, k % num_cols
+    row_ptr = np.zeros(num_rows + 1, dtype=np.int64)
+    np.add.at(row_ptr, rows + 1, 1)
+    return np.cumsum(row_ptr).astype(np.int32), cols.astype(np.int32)
+
+
+def assemble_block_matrix(blocks, row_ptr, col, diagonal=1.0):
+    """Monolithic values of a block system: each block (a dict with Ae
+    [C, k0*bs0, k1*bs1], dofs0, dofs1, bs0, bs1, row_offset, col_offset and
+    optional markers0 / markers1 / bc_rows in its own, restricted numbering)
+    adds its element matrices at its offsets, skipping excluded dofs and
+    BC-marked rows / columns (the per-block assemble_matrix calls of
+    assemble_matrix_block, assemble.py:112-134, each a
+    CUDAFormIntegral.cpp:1154-1224 scatter); then every block's BC rows get
+    `diagonal` on the monolithic diagonal (CUDAAssembler.cpp:131-164)."""
+    values = np.zeros(len(col))
+    dpos = diag_positions(row_ptr, col)
+    for B in blocks:
+        R, C, m = _couplings(B["dofs0"], B["dofs1"], B["bs0"], B["bs1"])
+        m = m.copy()
+        if B.get("markers0") is not None:
+            m &= np.asarray(B["markers0"])[np.maximum(R, 0)] == 0
+        if B.get("markers1") is not None:
+            m &= np.asarray(B["markers1"])[np.maximum(C, 0)] == 0
+        slots = csr_slots(row_ptr, col, B["row_offset"] + R[m], B["col_offset"] + C[m])
+        np.add.at(values, slots, np.asarray(B["Ae"])[m])
+    for B in blocks:
+        if B.get("bc_rows") is not None and len(B["bc_rows"]):
+            d = dpos[B["row_offset"] + np.asarray(B["bc_rows"], dtype=np.int64)]
+            values[d[d >= 0]] = diagonal
+    return values
+
+
+def assemble_block_vector(parts, size):
+    """Monolithic vector: part (be [C, k*bs], dofs, bs, offset) adds its element
+    vectors at its offset, skipping excluded dofs (assemble_vector_block,
+    assemble.py:168-202)."""
+    b = np.zeros(size)
+    for be, dofs, bs, off in parts:
+        s = scalar_cell_dofs(dofs, bs)
+        m = s >= 0
+        np.add.at(b, off + s[m], np.asarray(be).reshape(s.shape)[m])
+    return b
+
+
+# ---------------------------------------------------------------------------
 # Jacobi-preconditioned CG (the reference hands A, b to PETSc KSP cg+jacobi:
 # python/examples/poisson.py:116-125)
 # ---------------------------------------------------------------------------

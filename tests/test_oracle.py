@@ -273,3 +273,109 @@ def test_p3_nnz_closed_form_and_dof_count():
         rp, col = fo.sparsity(P["dofs"], P["dofs"], P["ndof"])
         assert len(col) == fo.nnz_formula("p3", n)
         assert np.diff(rp).max() <= 256  # block positions fit the byte map
+
+
+# --- block / restricted systems ----------------------------------------------
+def _csr(rp, col, vals, shape):
+    import scipy.sparse as sp
+    return sp.csr_matrix((vals, col, rp), shape=shape)
+
+
+def _structural_submatrix(rp, col, rows, cols):
+    """Pattern of A[rows][:, cols] (structural entries kept, explicit zeros too)."""
+    import scipy.sparse as sp
+    n = len(rp) - 1
+    S = sp.csr_matrix((np.ones(len(col)), col, rp), shape=(n, n))[rows][:, cols].tocsr()
+    S.sort_indices()
+    return S.indptr.astype(np.int32), S.indices.astype(np.int32)
+
+
+def test_block_system_block_diagonal_matches_separate_systems():
+    import scipy.sparse as sp
+    P1 = fo.build_problem("p1k", 3, seed=2)
+    P2 = fo.build_problem("p2", 3, seed=2)
+    S1, S2 = fo.solve_system(P1), fo.solve_system(P2)
+    n1, n2 = P1["ndof"], P2["ndof"]
+    parts = [(P1["dofs"], P1["dofs"], 1, 1, 0, 0), (P2["dofs"], P2["dofs"], 1, 1, n1, n1)]
+    rp, col = fo.block_pattern(parts, n1 + n2, n1 + n2)
+    blocks = []
+    for P, off in ((P1, 0), (P2, n1)):
+        mk = np.zeros(P["ndof"], dtype=np.uint8)
+        mk[P["bc_dofs"]] = 1
+        blocks.append(dict(Ae=fo.element_matrices(P), dofs0=P["dofs"], dofs1=P["dofs"], bs0=1, bs1=1, row_offset=off,
+                           col_offset=off, markers0=mk, markers1=mk, bc_rows=P["bc_dofs"]))
+    v = fo.assemble_block_matrix(blocks, rp, col)
+    ref = sp.block_diag([_csr(S1["row_ptr"], S1["col"], S1["A"], (n1, n1)),
+                         _csr(S2["row_ptr"], S2["col"], S2["A"], (n2, n2))]).tocsr()
+    ref.sort_indices()
+    assert np.array_equal(rp, ref.indptr) and np.array_equal(col, ref.indices)
+    assert np.array_equal(v, ref.data)
+
+
+@pytest.mark.parametrize("kind,bs", [("p2", 1), ("vp2", 3)])
+def test_restricted_system_is_the_submatrix_of_the_full_system(kind, bs):
+    # dofs outside a restriction take no entries: the restricted matrix is
+    # A_full[R, R] (pattern and values), for any restriction
+    P = fo.build_problem(kind, 3, seed=5)
+    dofs, nd = P["dofs"], P["ndof"]
+    X = fo.dof_coordinates(P["coords"], P["cells"], dofs, nd, 2)
+    R = np.nonzero(X[:, 0] <= 0.5 + 1e-12)[0]
+    Ae = fo.element_matrices(P)
+    rp_f, col_f = fo.sparsity(dofs, dofs, nd, bs, bs)
+    A_f = fo.assemble_matrix(Ae, dofs, dofs, rp_f, col_f, bs, bs)
+    dr = fo.restricted_dofmap(dofs, R, nd)
+    nr = len(R) * bs
+    rp, col = fo.block_pattern([(dr, dr, bs, bs, 0, 0)], nr, nr)
+    v = fo.assemble_block_matrix([dict(Ae=Ae, dofs0=dr, dofs1=dr, bs0=bs, bs1=bs, row_offset=0, col_offset=0)],
+                                 rp, col)
+    keep = (R[:, None] * bs + np.arange(bs)).ravel()
+    srp, scol = _structural_submatrix(rp_f, col_f, keep, keep)
+    assert np.array_equal(rp, srp) and np.array_equal(col, scol)
+    sub = _csr(rp_f, col_f, A_f, (nd * bs, nd * bs))[keep][:, keep].tocsr()
+    sub.sort_indices()
+    assert np.allclose(v, sub.data, rtol=0, atol=1e-14 * np.abs(A_f).max())
+    # restricted load vector = the kept entries of the full one
+    if kind == "p2":
+        be = fo.element_vectors(P)
+        b_full = fo.assemble_vector(be, dofs, nd)
+        b = fo.assemble_block_vector([(be, dr, 1, 0)], len(R))
+        assert np.allclose(b, b_full[R], rtol=0, atol=1e-15)
+
+
+def test_coupled_restricted_block_system_is_a_submatrix():
+    # [[K, -K], [-K, 2K]] on (V, V_R): the second field restricted to x <= 1/2;
+    # equals the unrestricted 2x2 system with the excluded rows / columns of
+    # the second field removed, BC rows included
+    import scipy.sparse as sp
+    P = fo.build_problem("p2", 3, seed=9)
+    dofs, nd = P["dofs"], P["ndof"]
+    X = fo.dof_coordinates(P["coords"], P["cells"], dofs, nd, 2)
+    R = np.nonzero(X[:, 0] <= 0.5 + 1e-12)[0]
+    K = fo.element_matrices(P)
+    mk = np.zeros(nd, dtype=np.uint8)
+    mk[P["bc_dofs"]] = 1
+
+    def system(d1, n1, mk1, bc1):
+        parts = [(dofs, dofs, 1, 1, 0, 0), (dofs, d1, 1, 1, 0, nd), (d1, dofs, 1, 1, nd, 0), (d1, d1, 1, 1, nd, nd)]
+        rp, col = fo.block_pattern(parts, nd + n1, nd + n1)
+        B = [dict(Ae=K, dofs0=dofs, dofs1=dofs, row_offset=0, col_offset=0, markers0=mk, markers1=mk,
+                  bc_rows=P["bc_dofs"]),
+             dict(Ae=-K, dofs0=dofs, dofs1=d1, row_offset=0, col_offset=nd, markers0=mk, markers1=mk1,
+                  bc_rows=P["bc_dofs"]),
+             dict(Ae=-K, dofs0=d1, dofs1=dofs, row_offset=nd, col_offset=0, markers0=mk1, markers1=mk, bc_rows=bc1),
+             dict(Ae=2 * K, dofs0=d1, dofs1=d1, row_offset=nd, col_offset=nd, markers0=mk1, markers1=mk1,
+                  bc_rows=bc1)]
+        for b in B:
+            b.update(bs0=1, bs1=1)
+        return rp, col, fo.assemble_block_matrix(B, rp, col)
+
+    rp_f, col_f, v_f = system(dofs, nd, mk, P["bc_dofs"])
+    dr = fo.restricted_dofmap(dofs, R, nd)
+    mkr = mk[R]
+    rp, col, v = system(dr, len(R), mkr, np.nonzero(mkr)[0])
+    keep = np.concatenate([np.arange(nd), nd + R])
+    srp, scol = _structural_submatrix(rp_f, col_f, keep, keep)
+    assert np.array_equal(rp, srp) and np.array_equal(col, scol)
+    sub = _csr(rp_f, col_f, v_f, (2 * nd, 2 * nd))[keep][:, keep].tocsr()
+    sub.sort_indices()
+    assert np.allclose(v, sub.data, rtol=0, atol=1e-14 * np.abs(v_f).max())
