@@ -2,7 +2,7 @@
 """Headline benchmark: FEM system assembly on one B200 (matrix nnz/s).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload p2|p2mid|p1|p1big|vp2|p3|batch|multimesh|serve] [--variant auto|tile|atomic|sorted-slot]
+                    [--workload p2|p2mid|p1|p1big|vp2|p3|batch|multimesh|serve|blocksys] [--variant auto|tile|atomic|sorted-slot]
 
 Default workload (the configuration the headline metric is quoted on): P2
 Poisson on the unit cube, 96^3 hexes x 6 = 5,308,416 tets, 7,189,057 dofs,
@@ -706,6 +706,266 @@ def run_gpu_batch(args, rank, world, local_rank):
     return out
 
 
+# two-field block system with a restricted second field
+BLOCKSYS = dict(n=64, cpu_n=16,
+                desc="two-field P2 block system on the unit cube, n=64 (1,572,864 tets): [[K, -K], [-K, 2K]] with "
+                     "K = k grad.grad, k P1 lognormal, the second field restricted to the dofs with x <= 1/2, "
+                     "Dirichlet g=x+y+z (2g) on the boundary of both fields, loads f DG0 U[-1,1]; FP64")
+# launches of one block step: zero A + 4 x (scatter + set_diagonal) + zero b + 2 loads
+BLOCKSYS_KERNELS = 12
+
+
+def blocksys_inputs(n: int, seed: int, pinned: bool = False):
+    """Forms, BCs and oracle-side arrays of the two-field block system."""
+    from cudolfinx import fem
+
+    rng = np.random.default_rng(seed)
+    mesh = fem.create_unit_cube(n)
+    C = mesh.num_cells
+    V = fem.functionspace(mesh, ("P", 2))
+    W = fem.functionspace(mesh, ("P", 2))
+    V1 = fem.functionspace(mesh, ("P", 1))
+    DG = fem.functionspace(mesh, ("DG", 0))
+
+    def host(a):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        if not pinned:
+            return a
+        import torch
+        t = torch.empty(a.shape, dtype=torch.float64, pin_memory=True)
+        _PINNED.append(t)
+        out = t.numpy()
+        out[...] = a
+        return out
+
+    k = np.exp(rng.standard_normal(V1.num_dofs))
+    f = rng.uniform(-1.0, 1.0, size=C)
+    X = V.tabulate_dof_coordinates()
+    R = np.nonzero(X[:, 0] <= 0.5 + 1e-12)[0].astype(np.int32)
+    kf = [fem.Function(V1, host(k)), fem.Function(V1, host(-k)), fem.Function(V1, host(-k)),
+          fem.Function(V1, host(2 * k))]
+    a = [[fem.stiffness(V, kf[0]), fem.stiffness(V, kf[1], trial=W)],
+         [fem.stiffness(W, kf[2], trial=V), fem.stiffness(W, kf[3])]]
+    L = [fem.load(V, fem.Function(DG, host(f))), fem.load(W, fem.Function(DG, host(f)))]
+    g = X.sum(axis=1)
+    bnd = fem.locate_boundary_dofs(V)
+    bcs = [fem.dirichletbc(fem.Function(V, g), bnd), fem.dirichletbc(fem.Function(W, 2 * g), bnd)]
+    return dict(mesh=mesh, V=V, W=W, a=a, L=L, bcs=bcs, R=R, k=k, f=f, bnd=bnd, cells=mesh.cells,
+                coords=mesh.geometry_x, dofs=V.dofs, ndof=V.num_nodes)
+
+
+def blocksys_alg_bytes(I, nnz, rows):
+    """Algorithmic bytes of the block matrix assembly: values written once
+    (8/nnz) and, per block, its byte map (100/cell), test and trial dofmaps
+    (80/cell), geometry dofmap (16/cell), coordinates (24/node), the P1
+    coefficient (16/cell + 8/node), segment starts (4/row) and BC markers
+    (1/row + 1/column)."""
+    C, nv = len(I["cells"]), len(I["coords"])
+    nV, nW = I["ndof"], len(I["R"])
+    b = 8 * nnz
+    for r, c in ((nV, nV), (nV, nW), (nW, nV), (nW, nW)):
+        b += 100 * C + 80 * C + 16 * C + 24 * nv + 16 * C + 8 * nv + 4 * (r + 1) + r + c
+    return b
+
+
+def blocksys_cpu_sample(n: int, seed: int, steps: int = 1):
+    """Oracle (numpy) restatement of the block system on the n-sized mesh:
+    element tensors + block matrix + block vector per step; returns
+    (seconds per step, monolithic nnz)."""
+    from oracle import fem_oracle as fo
+
+    coords, cells = fo.unit_cube_tet_mesh(n)
+    dofs, nd, grid = fo.p2_dofmap(n, cells)
+    rng = np.random.default_rng(seed)
+    k = np.exp(rng.standard_normal((n + 1) ** 3))
+    f = rng.uniform(-1.0, 1.0, size=len(cells))
+    X = fo.dof_coordinates(coords, cells, dofs, nd, 2)
+    R = np.nonzero(X[:, 0] <= 0.5 + 1e-12)[0]
+    bnd = fo.boundary_dofs_from_grid(grid, 2 * n)
+    mk = np.zeros(nd, dtype=np.uint8)
+    mk[bnd] = 1
+    dr = fo.restricted_dofmap(dofs, R, nd)
+    mkr = mk[R]
+    bcr = np.nonzero(mkr)[0]
+    parts = [(dofs, dofs, 1, 1, 0, 0), (dofs, dr, 1, 1, 0, nd), (dr, dofs, 1, 1, nd, 0), (dr, dr, 1, 1, nd, nd)]
+    rp, col = fo.block_pattern(parts, nd + len(R), nd + len(R))
+    times = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        K = fo.p2_stiffness(coords, cells, k[cells])
+        B = [dict(Ae=K, dofs0=dofs, dofs1=dofs, row_offset=0, col_offset=0, markers0=mk, markers1=mk, bc_rows=bnd),
+             dict(Ae=-K, dofs0=dofs, dofs1=dr, row_offset=0, col_offset=nd, markers0=mk, markers1=mkr, bc_rows=bnd),
+             dict(Ae=-K, dofs0=dr, dofs1=dofs, row_offset=nd, col_offset=0, markers0=mkr, markers1=mk, bc_rows=bcr),
+             dict(Ae=2 * K, dofs0=dr, dofs1=dr, row_offset=nd, col_offset=nd, markers0=mkr, markers1=mkr,
+                  bc_rows=bcr)]
+        for b in B:
+            b.update(bs0=1, bs1=1)
+        fo.assemble_block_matrix(B, rp, col)
+        be = fo.p2_load_dg0(coords, cells, f)
+        fo.assemble_block_vector([(be, dofs, 1, 0), (be, dr, 1, nd)], nd + len(R))
+        times.append(time.perf_counter() - t0)
+    return statistics.median(times), len(col)
+
+
+def run_gpu_blocksys(args, rank, world, local_rank):
+    import torch
+
+    import cudolfinx as cx
+    from cudolfinx import _lib
+
+    torch.cuda.set_device(local_rank)
+    t_setup = time.perf_counter()
+    I = blocksys_inputs(BLOCKSYS["n"], args.seed)
+    asm = cx.CUDAAssembler()
+    A = cx.form(I["a"], restriction=([None, I["R"]], [None, I["R"]]))
+    Lb = cx.form(I["L"], restriction=[None, I["R"]])
+    M = asm.create_matrix_block(A)
+    b = asm.create_vector_block(Lb)
+    dbc = asm.pack_bcs(I["bcs"])
+    nnz, nrows = M.sparsity.nnz, M.sparsity.num_rows
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+    Lib = _lib.lib
+    blocks = []
+    for i, row in enumerate(A.forms):
+        for j, f in enumerate(row):
+            h0 = dbc._get_cpp_bcs(f.function_spaces[0], f.restriction(0))
+            h1 = dbc._get_cpp_bcs(f.function_spaces[1], f.restriction(1))
+            blocks.append((f.cuda_form, h0.handle if h0 else None, h1.handle if h1 else None))
+    vforms = [(f.cuda_form, off) for f, off in zip(Lb.forms, Lb.offsets)]
+    Mp, bp = M.values.data_ptr(), b.vector.data_ptr()
+
+    def step(ev0=None, ev1=None):
+        if ev0 is not None:
+            ev0.record(stream)
+        _lib.check(Lib.fe_zero_entries(Mp, nnz, sp), "zero")
+        for h, b0, b1 in blocks:
+            _lib.check(Lib.fe_assemble_matrix(h, Mp, b0, b1, 1.0, 0, sp), "matrix block")
+        if ev1 is not None:
+            ev1.record(stream)
+        _lib.check(Lib.fe_zero_entries(bp, nrows, sp), "zero b")
+        for h, off in vforms:
+            _lib.check(Lib.fe_assemble_vector(h, bp + 8 * off, 0, sp), "vector block")
+
+    step()
+    torch.cuda.synchronize()
+    setup_s = time.perf_counter() - t_setup
+    for _ in range(args.warmup):
+        step()
+    dist = torch.distributed if world > 1 else None
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    time.sleep(0.3)
+    mats = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for k in range(args.steps):
+        step(*mats[k])
+    e1.record(stream)
+    torch.cuda.synchronize()
+    total_ms = e0.elapsed_time(e1)
+    mat_ms = statistics.mean(x.elapsed_time(y) for x, y in mats)
+    clk = clocks.stop()
+    total_ms, mat_ms = reduce_over_ranks([total_ms, mat_ms])
+
+    e2e = None
+    if not args.no_e2e:
+        I2 = blocksys_inputs(BLOCKSYS["n"], args.seed, pinned=True)
+        A2 = cx.form(I2["a"], restriction=([None, I2["R"]], [None, I2["R"]]))
+        L2 = cx.form(I2["L"], restriction=[None, I2["R"]])
+        M2 = cx.CUDAMatrix(asm._ctx, M.sparsity)
+        b2 = asm.create_vector_block(L2)
+        dbc2 = asm.pack_bcs(I2["bcs"])
+        bhost = torch.empty(nrows, dtype=torch.float64, pin_memory=True)
+        coef_bytes = sum(np.asarray(c.x.array).nbytes for row in I2["a"] for f in row for c in f.coefficients) + \
+            sum(np.asarray(c.x.array).nbytes for f in I2["L"] for c in f.coefficients)
+
+        def e2e_step():
+            asm.assemble_matrix_block(A2, M2, bcs=dbc2)
+            asm.assemble_vector_block(L2, b2)
+            bhost.copy_(b2.vector, non_blocking=True)
+
+        for _ in range(max(1, args.warmup)):
+            e2e_step()
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        s0 = torch.cuda.Event(enable_timing=True)
+        s1 = torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        for _ in range(args.steps):
+            e2e_step()
+        s1.record(stream)
+        torch.cuda.synchronize()
+        (e2e_ms,) = reduce_over_ranks([s0.elapsed_time(s1)])
+        same = bool(torch.allclose(M2.values, M.values, rtol=1e-12, atol=1e-13 * float(M.values.abs().max())))
+        e2e = {"value": replica_rate(nnz, args.steps, e2e_ms, world), "unit": "nnz/s",
+               "h2d_bytes_per_step": int(coef_bytes), "d2h_bytes_per_step": int(nrows * 8),
+               "ms_per_step": e2e_ms / args.steps,
+               "path": "cudolfinx.CUDAAssembler.assemble_matrix_block + assemble_vector_block (Python API -> C-ABI)",
+               "matches_device_leg": same}
+
+    alg = blocksys_alg_bytes(I, nnz, nrows)
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            peaks = json.load(fh)
+    except (OSError, ValueError):
+        pass
+    peak = peaks.get("hbm_gbs", 6650.0)
+    achieved = alg / (mat_ms / 1e3) / 1e9
+    out = {
+        "metric": "matrix nnz/s (block system)", "value": replica_rate(nnz, args.steps, total_ms, world),
+        "unit": "nnz/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded numpy inputs)",
+        "config": {"workload": BLOCKSYS["desc"], "cells": len(I["cells"]), "dofs": nrows, "nnz": nnz,
+                   "kept_dofs_second_field": int(len(I["R"])),
+                   "step": "zero A + 4 block scatters (BC skip, unit diagonal) + zero b + 2 block loads",
+                   "l2": "inputs larger than L2 (values %.2f GB)" % (8 * nnz / 1e9),
+                   "parallelism": f"replicas x{world}"},
+        "roofline": {"bound": "hbm", "kernel": "block matrix assembly (zero + 4 blocks)", "achieved": achieved,
+                     "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": load_traffic("blocksys"),
+                     "algorithmic_bytes": alg, "kernel_ms": mat_ms,
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if "hbm_gbs" in peaks
+                     else "fallback 6650 GB/s"},
+        "matrix_nnz_per_s": nnz / (mat_ms / 1e3),
+        "gpu_launches": BLOCKSYS_KERNELS * args.steps,
+        "clocks": clk,
+        "setup_s": setup_s,
+    }
+    if e2e:
+        out["e2e"] = e2e
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        t, nnz_s = blocksys_cpu_sample(BLOCKSYS["cpu_n"], args.seed, steps=2)
+        out["cpu_baseline"] = {"value": nnz_s / t, "unit": "nnz/s", "cores": 1, "kind": "port",
+                               "sample": f"the same block system at n={BLOCKSYS['cpu_n']} "
+                                         f"({6 * BLOCKSYS['cpu_n'] ** 3} cells, nnz {nnz_s}): element tensors + "
+                                         "block matrix + block vector with the numpy oracle (oracle/fem_oracle.py), "
+                                         "median of 2, one thread", "seconds_per_step": t}
+    return out
+
+
+def run_reference_blocksys(args):
+    steps = max(1, args.steps)
+    for _ in range(args.warmup):
+        blocksys_cpu_sample(BLOCKSYS["cpu_n"], args.seed, 1)
+    t, nnz = blocksys_cpu_sample(BLOCKSYS["cpu_n"], args.seed, steps)
+    v = nnz / t
+    return {"impl": "reference", "metric": "matrix nnz/s (block system)", "value": v, "unit": "nnz/s",
+            "n_gpus": 1, "steps": steps, "warmup": args.warmup, "ms_per_step": 1e3 * t, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": {"workload": BLOCKSYS["desc"], "sample_n": BLOCKSYS["cpu_n"], "nnz": nnz},
+            "cpu_baseline": {"value": v, "unit": "nnz/s", "cores": 1, "kind": "port",
+                             "sample": f"n={BLOCKSYS['cpu_n']} block system per step, numpy oracle "
+                                       "(the reference's block path needs DOLFINx + PETSc)"},
+            "e2e": {"value": v, "unit": "nnz/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
 def multimesh_inputs(seed: int):
     rng = np.random.default_rng(seed)
     ns = rng.integers(MULTI["nmin"], MULTI["nmax"] + 1, size=MULTI["count"])
@@ -1049,6 +1309,8 @@ def run_reference(args):
         return run_reference_batch(args)
     if args.workload == "multimesh":
         return run_reference_multimesh(args)
+    if args.workload == "blocksys":
+        return run_reference_blocksys(args)
     W = WORKLOADS[args.workload]
     I = make_inputs(W["kind"], W["n"], seed=args.seed)
     row_ptr, col = host_pattern(I)
@@ -1119,7 +1381,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batch", "multimesh", "serve"], default="p2")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batch", "multimesh", "serve", "blocksys"], default="p2")
     ap.add_argument("--variant", choices=["auto", "tile", "atomic", "atomic-full", "sorted-slot", "deterministic",
                                           "row-gather",
                                           "block"], default="auto")
@@ -1152,8 +1414,8 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local_rank))
     try:
-        runner = {"batch": run_gpu_batch, "multimesh": run_gpu_multimesh,
-                  "serve": run_gpu_serve}.get(args.workload, run_gpu)
+        runner = {"batch": run_gpu_batch, "multimesh": run_gpu_multimesh, "serve": run_gpu_serve,
+                  "blocksys": run_gpu_blocksys}.get(args.workload, run_gpu)
         out = runner(args, rank, world, local_rank)
         if rank == 0:
             print(json.dumps(out), flush=True)

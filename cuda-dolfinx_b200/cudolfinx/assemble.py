@@ -206,10 +206,10 @@ class CUDAAssembler:
                               coeffs=None, constants=None, zero: bool = True, diagonal: float = 1.0) -> CUDAMatrix:
         """Assemble a block form into one monolithic matrix (assemble.py:112-134):
         zero it once, then add every block at its offsets.  ``bcs``: a list of
-        lists (the BCs of block (i, j), as the reference takes them) or one flat
-        list of DirichletBCs applied to every block by function space (rows on
-        the block's test space, columns on its trial space); owned BC rows get
-        ``diagonal`` on the monolithic diagonal."""
+        lists (the BCs of block (i, j), as the reference takes them), or one flat
+        list of DirichletBCs (or a CUDADirichletBC) applied to every block by
+        function space (rows on the block's test space, columns on its trial
+        space); owned BC rows get ``diagonal`` on the monolithic diagonal."""
         if not isinstance(a, BlockCUDAForm):
             raise TypeError(f"Expected BlockCUDAForm, got '{type(a)}'")
         if mat is None:
@@ -219,7 +219,7 @@ class CUDAAssembler:
         if zero:
             _lib.check(_lib.lib.fe_zero_entries(mat.values.data_ptr(), mat.sparsity.nnz, self._ctx.stream()),
                        "fe_zero_entries")
-        nested = bcs is not None and len(bcs) and isinstance(bcs[0], (list, tuple))
+        nested = isinstance(bcs, (list, tuple)) and len(bcs) > 0 and isinstance(bcs[0], (list, tuple))
         flat = None if (bcs is None or nested) else self._bc_collection(bcs)
         for i, row in enumerate(a.forms):
             for j, f in enumerate(row):

@@ -52,11 +52,18 @@ class _DeviceBC:
         dofs `restriction`, sorted): BC dofs outside it are dropped."""
         if not hasattr(self, "_restricted"):
             self._restricted = {}
+            self._by_id = {}
+        # a form hands out the same restriction array on every call: look it up
+        # by identity first, by content (hashing the whole array) only once
+        hit = self._by_id.get(id(restriction))
+        if hit is not None and hit[0] is restriction:
+            return hit[1]
         key = np.ascontiguousarray(restriction, dtype=np.int32).tobytes()
         r = self._restricted.get(key)
         if r is None:
             r = _RestrictedBC(self, np.frombuffer(key, dtype=np.int32))
             self._restricted[key] = r
+        self._by_id[id(restriction)] = (restriction, r)
         return r
 
     def __del__(self):

@@ -96,9 +96,10 @@ enum fe_precision {
 #define FE_ASM_ZERO 1u            /* overwrite instead of accumulating (assemble.py:52 zero=True)   */
 #define FE_ASM_DETERMINISTIC 2u   /* bitwise reproducible: ordered tile gather (P1/P2), else sorted-slot */
 #define FE_ASM_ATOMIC 4u          /* FP64-atomic scatter through the slot map (zero pass first); for
-                                     vector-P2 elasticity on a symmetric pattern with equal row/column
-                                     BCs each unique entry is reduced once into the upper triangle
-                                     and a pass copies it to the lower triangle                      */
+                                     P1, P3 and vector-P2 forms on a symmetric pattern with equal
+                                     row/column BCs (and FE_ASM_ZERO) each unique entry is reduced
+                                     once into the upper triangle and a pass copies it to the lower
+                                     triangle                                                        */
 #define FE_ASM_SORTED_SLOT 8u     /* global sorted-slot segmented reduction (reproducible)          */
 #define FE_ASM_TILE 16u           /* owner-computes row tiles, shared-memory accumulation (P1/P2)   */
 #define FE_ASM_ROW_GATHER 32u     /* one warp per CSR row over the row's cells (P1)                 */

@@ -175,3 +175,15 @@ def test_block_forms_reject_other_variants_and_restricted_facets():
     V = fem.functionspace(mesh, ("P", 2))
     with pytest.raises(RuntimeError, match="unrestricted"):
         cx.form(fem.facet_mass(V, 1.0), restriction=[R, R])
+
+
+def test_block_matrix_takes_a_packed_bc_collection():
+    cx, fem, P, mesh = _setup(2, 3)
+    A, bcs, R = _coupled_system(cx, fem, P, mesh, True)
+    asm = cx.CUDAAssembler()
+    M1 = asm.assemble_matrix_block(A, bcs=bcs)
+    M2 = asm.assemble_matrix_block(A, bcs=asm.pack_bcs(bcs))
+    M1.assemble()
+    M2.assemble()
+    ok, worst = tolerance_check(M2.values.cpu().numpy(), M1.values.cpu().numpy())
+    assert ok, worst
