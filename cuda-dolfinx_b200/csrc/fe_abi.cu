@@ -892,6 +892,20 @@ int fe_apply_lifting(double* b, int num_forms, const fe_form* a, const fe_bc* bc
   });
 }
 
+int fe_interpolate(fe_dofmap target, double* u1, fe_dofmap source, const double* u0, const double* matrix,
+                   void* stream) {
+  return guard([&] {
+    FE_REQUIRE(target && source && matrix, "null argument");
+    FE_REQUIRE(target->ctx == source->ctx, "dofmaps belong to different contexts");
+    FE_REQUIRE(target->num_cells == source->num_cells, "the spaces are on different meshes (cell counts differ)");
+    FE_REQUIRE(target->bs == source->bs, "interpolation maps between spaces of the same block size");
+    FE_REQUIRE(!source->excluded, "the source space must be unrestricted");
+    FE_REQUIRE((u1 || !target->num_blocks) && (u0 || !source->num_blocks), "null coefficient array");
+    DeviceScope d(target->ctx);
+    interpolate(*target, u1, *source, u0, matrix, as_stream(stream));
+  });
+}
+
 int fe_set_bc(double* b, int64_t num_values, fe_bc bc, const double* x0, double scale, void* stream) {
   return guard([&] {
     FE_REQUIRE(bc, "null bc");

@@ -99,6 +99,7 @@ struct fe_dofmap_s {
   std::vector<int32_t> host;     // host copy (sparsity build)
   uint64_t id = 0;               // unique id for caches
   bool excluded = false;         // some entries are -1: dofs outside a restriction
+  fe::DevBuf<int32_t> owner;     // [num_blocks] lowest cell*k + i listing each dof (interpolation), on first use
 };
 
 struct fe_sparsity_s {
@@ -334,6 +335,11 @@ void launch_mark_cells(const int32_t* dofs, int64_t num_cells, int k, int bs, co
                        int32_t* out_cells, unsigned long long* out_count, cudaStream_t s);
 void launch_set_bc(double* b, int64_t num_values, const int32_t* dofs, int64_t n_bc, const double* g,
                    const double* x0, double scale, cudaStream_t s);
+
+// same-map interpolation u1 = I u0 (fe_interp.cu); im is the host
+// [target.k][source.k] matrix; one owner cell per target dof
+void interpolate(fe_dofmap_s& target, double* u1, const fe_dofmap_s& source, const double* u0, const double* im,
+                 cudaStream_t s);
 
 // error word of the current context's kernels
 unsigned* device_error_word(fe_context ctx);

@@ -198,6 +198,49 @@ class FunctionSpace:
         return other is self
 
 
+def reference_nodes(V: FunctionSpace) -> np.ndarray:
+    """Reference coordinates [k, 3] of the element's nodes in local order
+    (DG0: the centroid)."""
+    if V.family == "DG":
+        return np.full((1, 3), 0.25)
+    if V.degree == 1:
+        W = np.eye(4)
+    elif V.degree == 2:
+        W = np.array([np.eye(4)[v] for v in range(4)] + [0.5 * (np.eye(4)[a] + np.eye(4)[b]) for a, b in TET_EDGES])
+    else:
+        W = _P3_WEIGHTS / 3.0
+    return W[:, 1:].copy()  # (x, y, z) = (l1, l2, l3)
+
+
+def lagrange_basis(V: FunctionSpace, X: np.ndarray) -> np.ndarray:
+    """Values [npts, k] of the element's basis functions at reference points X
+    (barycentric formulas of the equispaced Lagrange elements, basix local order)."""
+    X = np.atleast_2d(np.asarray(X, dtype=np.float64))
+    lam = np.column_stack([1.0 - X.sum(axis=1), X[:, 0], X[:, 1], X[:, 2]])
+    if V.family == "DG":
+        return np.ones((len(X), 1))
+    if V.degree == 1:
+        return lam
+    if V.degree == 2:
+        vert = [lam[:, v] * (2 * lam[:, v] - 1) for v in range(4)]
+        edge = [4 * lam[:, a] * lam[:, b] for a, b in TET_EDGES]
+        return np.column_stack(vert + edge)
+    vert = [0.5 * lam[:, v] * (3 * lam[:, v] - 1) * (3 * lam[:, v] - 2) for v in range(4)]
+    edge = []
+    for a, b in TET_EDGES:
+        edge.append(4.5 * lam[:, a] * lam[:, b] * (3 * lam[:, a] - 1))
+        edge.append(4.5 * lam[:, a] * lam[:, b] * (3 * lam[:, b] - 1))
+    face = [27 * np.prod(lam[:, [q for q in range(4) if q != f]], axis=1) for f in range(4)]
+    return np.column_stack(vert + edge + face)
+
+
+def interpolation_matrix(V: FunctionSpace, V0: FunctionSpace) -> np.ndarray:
+    """Interpolation operator [k, k0] from V0 into V on the same reference map:
+    V's nodes evaluated in V0's basis (create_interpolation_operator of
+    Lagrange elements)."""
+    return np.ascontiguousarray(lagrange_basis(V0, reference_nodes(V)))
+
+
 def functionspace(mesh: Mesh, element) -> FunctionSpace:
     return FunctionSpace(mesh, element)
 

@@ -271,6 +271,19 @@ int fe_apply_lifting(double* b, int num_forms, const fe_form* a, const fe_bc* bc
 int fe_set_bc(double* b, int64_t num_values, fe_bc bc, const double* x0, double scale,
               void* stream);
 
+/* ---- interpolation ------------------------------------------------------- */
+/* Replaces CUDACoefficient::interpolate (cpp/cudolfinx/fem/CUDACoefficient.h:64-83
+ * -> interpolate_same_map, cpp/cudolfinx/fem/CUDAInterpolate.cu): u1 = I u0 for
+ * two spaces on the same mesh and reference map.  `matrix` (host, row-major
+ * target.k x source.k) is the interpolation operator: the target element's
+ * nodes evaluated in the source element's basis (create_interpolation_operator).
+ * u0 / u1 are device arrays of num_blocks*bs values; block spaces interpolate
+ * component by component.  Each target dof is computed once, from the lowest
+ * (cell, local dof) that lists it (the reference lets the last writer win);
+ * dofs listed by no cell keep their values. */
+int fe_interpolate(fe_dofmap target, double* u1, fe_dofmap source, const double* u0, const double* matrix,
+                   void* stream);
+
 /* ---- solver (the reference hands A, b to PETSc KSP cg + jacobi:
  * python/examples/poisson.py:116-125) ------------------------------------ */
 /* Jacobi-preconditioned CG on device.  x is the initial guess and the result

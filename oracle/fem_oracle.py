@@ -719,6 +719,50 @@ def assemble_block_vector(parts, size):
 
 
 # ---------------------------------------------------------------------------
+# Same-map interpolation (cpp/cudolfinx/fem/CUDACoefficient.h:64-83,
+# cpp/cudolfinx/fem/CUDAInterpolate.cu)
+# ---------------------------------------------------------------------------
+
+def element_nodes(degree):
+    """Reference coordinates [k, 3] of the Lagrange nodes in local order;
+    degree 0 = DG0 (the centroid)."""
+    if degree == 0:
+        return np.full((1, 3), 0.25)
+    if degree == 1:
+        B = np.eye(4)
+    elif degree == 2:
+        B = np.array([np.eye(4)[v] for v in range(4)] + [0.5 * (np.eye(4)[a] + np.eye(4)[b]) for a, b in TET_EDGES])
+    else:
+        B = p3_local_points() / 3.0
+    return B[:, 1:]
+
+
+def interpolation_operator(degree_target, degree_source):
+    """[k1, k0]: the target nodes evaluated in the source basis (the exact
+    rational basis of this module; create_interpolation_operator for Lagrange
+    elements)."""
+    X = element_nodes(degree_target)
+    if degree_source == 0:
+        return np.ones((len(X), 1))
+    B = _basis(degree_source)
+    return np.array([[sum(float(c) * x[0] ** e[0] * x[1] ** e[1] * x[2] ** e[2] for e, c in phi.items())
+                      for phi in B] for x in X])
+
+
+def interpolate_same_map(u0, dofs0, dofs1, im, n_target_blocks, bs=1, u1=None):
+    """The reference algorithm (interpolate_same_map, CUDAInterpolate.cu):
+    gather each cell's source values X0 = u0[M0], X1 = IM X0, scatter
+    u1[M1] = X1 with cells in order (a later cell overwrites a shared dof)."""
+    u1 = np.zeros(n_target_blocks * bs) if u1 is None else u1.copy()
+    d0, d1 = np.asarray(dofs0, dtype=np.int64), np.asarray(dofs1, dtype=np.int64)
+    for q in range(bs):
+        X1 = np.asarray(u0)[d0 * bs + q] @ np.asarray(im).T
+        for c in range(len(d1)):
+            u1[d1[c] * bs + q] = X1[c]
+    return u1
+
+
+# ---------------------------------------------------------------------------
 # Jacobi-preconditioned CG (the reference hands A, b to PETSc KSP cg+jacobi:
 # python/examples/poisson.py:116-125)
 # ---------------------------------------------------------------------------

@@ -154,3 +154,19 @@ def test_functional_specs_build_without_gpu():
     assert fi.kind == "FACET_INTEGRAL" and len(fi.facets) == 12 * 4
     with pytest.raises(ValueError):
         fem.energy(fem.Function(fem.functionspace(mesh, ("P", 2, (3,)))))
+
+
+def test_reference_nodes_and_basis_are_lagrange_and_match_the_oracle():
+    from cudolfinx import fem
+    m = fem.create_unit_cube(1)
+    spaces = {0: fem.functionspace(m, ("DG", 0)), 1: fem.functionspace(m, ("P", 1)),
+              2: fem.functionspace(m, ("P", 2)), 3: fem.functionspace(m, ("P", 3))}
+    for d, V in spaces.items():
+        X = fem.reference_nodes(V)
+        assert np.allclose(X, fo.element_nodes(d))
+        if d:
+            assert np.allclose(fem.lagrange_basis(V, X), np.eye(len(X)), atol=1e-14)
+    for dt in spaces:
+        for ds in (1, 2, 3):
+            assert np.allclose(fem.interpolation_matrix(spaces[dt], spaces[ds]), fo.interpolation_operator(dt, ds),
+                               atol=1e-14)

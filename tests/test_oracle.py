@@ -379,3 +379,37 @@ def test_coupled_restricted_block_system_is_a_submatrix():
     sub = _csr(rp_f, col_f, v_f, (2 * nd, 2 * nd))[keep][:, keep].tocsr()
     sub.sort_indices()
     assert np.allclose(v, sub.data, rtol=0, atol=1e-14 * np.abs(v_f).max())
+
+
+# --- interpolation ------------------------------------------------------------
+@pytest.mark.parametrize("dt,ds", [(1, 1), (2, 1), (3, 1), (3, 2), (1, 2), (2, 3), (0, 1), (0, 2)])
+def test_interpolation_operator_reproduces_the_source_polynomials(dt, ds):
+    # IM maps the source nodal values of any polynomial of the source degree to
+    # its values at the target nodes
+    rng = np.random.default_rng(dt * 7 + ds)
+    c = rng.standard_normal(10)
+
+    def poly(X):  # a quadratic (exact in P2 / P3, its linear part in P1)
+        x, y, z = X[:, 0], X[:, 1], X[:, 2]
+        q = c[0] + c[1] * x + c[2] * y + c[3] * z
+        if ds >= 2:
+            q = q + c[4] * x * x + c[5] * x * y + c[6] * y * z + c[7] * z * z + c[8] * x * z + c[9] * y * y
+        return q
+
+    im = fo.interpolation_operator(dt, ds)
+    got = im @ poly(fo.element_nodes(ds))
+    assert np.allclose(got, poly(fo.element_nodes(dt)), atol=1e-13)
+
+
+def test_oracle_interpolation_is_exact_for_polynomials_on_the_mesh():
+    n = 3
+    coords, cells = fo.unit_cube_tet_mesh(n, jitter=0.2, seed=3)
+    d2, n2, _ = fo.p2_dofmap(n, cells)
+    d3, n3, _ = fo.p3_dofmap(n, cells)
+    X2 = fo.dof_coordinates(coords, cells, d2, n2, 2)
+    X3 = fo.dof_coordinates(coords, cells, d3, n3, 3)
+    q = lambda X: 1 + X[:, 0] - 2 * X[:, 1] * X[:, 2] + X[:, 2] ** 2
+    u3 = fo.interpolate_same_map(q(X2), d2, d3, fo.interpolation_operator(3, 2), n3)
+    assert np.abs(u3 - q(X3)).max() < 1e-13
+    u2 = fo.interpolate_same_map(u3, d3, d2, fo.interpolation_operator(2, 3), n2)
+    assert np.abs(u2 - q(X2)).max() < 1e-13
