@@ -2,7 +2,7 @@
 """Headline benchmark: FEM system assembly on one B200 (matrix nnz/s).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload p2|p2mid|p1|p1big|vp2|p3|batch|multimesh|serve|blocksys] [--variant auto|tile|atomic|sorted-slot]
+                    [--workload p2|p2mid|p1|p1big|vp2|p3|batch|multimesh|serve|blocksys|interp] [--variant auto|tile|atomic|sorted-slot]
 
 Default workload (the configuration the headline metric is quoted on): P2
 Poisson on the unit cube, 96^3 hexes x 6 = 5,308,416 tets, 7,189,057 dofs,
@@ -966,6 +966,137 @@ def run_reference_blocksys(args):
             "e2e": {"value": v, "unit": "nnz/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+# device interpolation: a P2 field into P3 on one mesh
+INTERP = dict(n=64, cpu_n=24,
+              desc="same-map interpolation P2 -> P3 on the unit cube, n=64 (1,572,864 tets; 2,146,689 source "
+                   "and 7,189,057 target dofs), source values N(0,1); FP64")
+
+
+def run_gpu_interp(args, rank, world, local_rank):
+    import torch
+
+    import cudolfinx as cx
+    from cudolfinx import _lib, fem
+
+    torch.cuda.set_device(local_rank)
+    n = INTERP["n"]
+    mesh = fem.create_unit_cube(n)
+    V0 = fem.functionspace(mesh, ("P", 2))
+    V1 = fem.functionspace(mesh, ("P", 3))
+    rng = np.random.default_rng(args.seed)
+    c0 = cx.Coefficient(fem.Function(V0, rng.standard_normal(V0.num_dofs)))
+    c1 = cx.Coefficient(fem.Function(V1))
+    im = fem.interpolation_matrix(V1, V0)
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+    h1, h0 = c1._dofmap.handle, c0._dofmap.handle
+    p1, p0 = c1.device_values.data_ptr(), c0.device_values.data_ptr()
+
+    def step():
+        _lib.check(_lib.lib.fe_interpolate(h1, p1, h0, p0, im.ctypes.data, sp), "interpolate")
+
+    step()
+    torch.cuda.synchronize()
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    time.sleep(0.3)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    (ms,) = reduce_over_ranks([e0.elapsed_time(e1)])
+    ms_step = ms / args.steps
+    n1, n0, C = V1.num_dofs, V0.num_dofs, mesh.num_cells
+    # per target dof: owner entry (4) + value written (8); the source values
+    # (8 per source dof) and the source dofmap (4 * 10 per cell) read once
+    alg = 12 * n1 + 8 * n0 + 40 * C
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            peaks = json.load(fh)
+    except (OSError, ValueError):
+        pass
+    peak = peaks.get("hbm_gbs", 6650.0)
+    achieved = alg / (ms_step / 1e3) / 1e9
+    e2e = None
+    if not args.no_e2e:
+        host_u0 = torch.from_numpy(c0.values()).pin_memory()
+        host_u1 = torch.empty(n1, dtype=torch.float64, pin_memory=True)
+
+        def e2e_step():
+            c0.device_values.copy_(host_u0, non_blocking=True)
+            step()
+            host_u1.copy_(c1.device_values, non_blocking=True)
+
+        for _ in range(max(1, args.warmup)):
+            e2e_step()
+        torch.cuda.synchronize()
+        s0 = torch.cuda.Event(enable_timing=True)
+        s1 = torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        for _ in range(args.steps):
+            e2e_step()
+        s1.record(stream)
+        torch.cuda.synchronize()
+        (e2e_ms,) = reduce_over_ranks([s0.elapsed_time(s1)])
+        e2e = {"value": replica_rate(n1, args.steps, e2e_ms, world), "unit": "target dofs/s",
+               "h2d_bytes_per_step": 8 * n0, "d2h_bytes_per_step": 8 * n1, "ms_per_step": e2e_ms / args.steps,
+               "path": "fe_interpolate with the source uploaded from pinned host memory and the result read back"}
+    out = {"metric": "interpolated target dofs/s", "value": replica_rate(n1, args.steps, ms, world),
+           "unit": "target dofs/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f64", "data": "synthetic (seeded)",
+           "config": {"workload": INTERP["desc"], "cells": C, "source_dofs": n0, "target_dofs": n1,
+                      "l2": "working set %.2f GB (> L2)" % (alg / 1e9), "parallelism": f"replicas x{world}"},
+           "roofline": {"bound": "hbm", "kernel": "k_interpolate", "achieved": achieved, "peak": peak,
+                        "unit": "GB/s", "frac": achieved / peak, "traffic": load_traffic("interp"),
+                        "algorithmic_bytes": alg, "kernel_ms": ms_step,
+                        "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if "hbm_gbs" in peaks
+                        else "fallback 6650 GB/s"},
+           "gpu_launches": args.steps, "clocks": clk}
+    if e2e:
+        out["e2e"] = e2e
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = interp_cpu_sample(INTERP["cpu_n"], args.seed)
+    return out
+
+
+def interp_cpu_sample(n: int, seed: int):
+    """The oracle's restatement of the reference algorithm (gather, multiply,
+    scatter cell by cell) on the n-sized mesh."""
+    from oracle import fem_oracle as fo
+
+    coords, cells = fo.unit_cube_tet_mesh(n)
+    d2, n2, _ = fo.p2_dofmap(n, cells)
+    d3, n3, _ = fo.p3_dofmap(n, cells)
+    u0 = np.random.default_rng(seed).standard_normal(n2)
+    im = fo.interpolation_operator(3, 2)
+    t0 = time.perf_counter()
+    fo.interpolate_same_map(u0, d2, d3, im, n3)
+    t = time.perf_counter() - t0
+    return {"value": n3 / t, "unit": "target dofs/s", "cores": 1, "kind": "port",
+            "sample": f"P2 -> P3 at n={n} ({6 * n ** 3} cells, {n3} target dofs): oracle interpolate_same_map "
+                      "(numpy, cell loop in the reference's order), one thread", "seconds_per_step": t}
+
+
+def run_reference_interp(args):
+    r = interp_cpu_sample(INTERP["cpu_n"], args.seed)
+    v = r["value"]
+    return {"impl": "reference", "metric": "interpolated target dofs/s", "value": v, "unit": "target dofs/s",
+            "n_gpus": 1, "steps": 1, "warmup": 0, "ms_per_step": 1e3 * r["seconds_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded)", "config": {"workload": INTERP["desc"], "sample_n": INTERP["cpu_n"]},
+            "cpu_baseline": r, "e2e": {"value": v, "unit": "target dofs/s", "h2d_bytes_per_step": 0,
+                                       "d2h_bytes_per_step": 0}}
+
+
 def multimesh_inputs(seed: int):
     rng = np.random.default_rng(seed)
     ns = rng.integers(MULTI["nmin"], MULTI["nmax"] + 1, size=MULTI["count"])
@@ -1311,6 +1442,8 @@ def run_reference(args):
         return run_reference_multimesh(args)
     if args.workload == "blocksys":
         return run_reference_blocksys(args)
+    if args.workload == "interp":
+        return run_reference_interp(args)
     W = WORKLOADS[args.workload]
     I = make_inputs(W["kind"], W["n"], seed=args.seed)
     row_ptr, col = host_pattern(I)
@@ -1381,7 +1514,8 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batch", "multimesh", "serve", "blocksys"], default="p2")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batch", "multimesh", "serve", "blocksys", "interp"],
+                    default="p2")
     ap.add_argument("--variant", choices=["auto", "tile", "atomic", "atomic-full", "sorted-slot", "deterministic",
                                           "row-gather",
                                           "block"], default="auto")
@@ -1415,7 +1549,7 @@ def main():
                                 device_id=torch.device("cuda", local_rank))
     try:
         runner = {"batch": run_gpu_batch, "multimesh": run_gpu_multimesh, "serve": run_gpu_serve,
-                  "blocksys": run_gpu_blocksys}.get(args.workload, run_gpu)
+                  "blocksys": run_gpu_blocksys, "interp": run_gpu_interp}.get(args.workload, run_gpu)
         out = runner(args, rank, world, local_rank)
         if rank == 0:
             print(json.dumps(out), flush=True)
