@@ -49,6 +49,7 @@ std::string decode_device_error(unsigned w) {
   if (w & DEV_ERR_ROW_WIDE) s += " [block row wider than 255 block columns]";
   if (w & DEV_ERR_BLOCK) s += " [CSR rows of a block row are not block-structured]";
   if (w & DEV_ERR_INDEX) s += " [index out of range]";
+  if (w & DEV_ERR_FACET) s += " [the two sides of an interior facet are different triangles]";
   return s;
 }
 
@@ -72,6 +73,8 @@ int form_rank(int kind) {
     case FE_FORM_P1_FACET_MASS:
     case FE_FORM_P2_FACET_MASS:
     case FE_FORM_P3_STIFFNESS:
+    case FE_FORM_DG0_JUMP:
+    case FE_FORM_DG1_JUMP:
       return 2;
     case FE_FORM_P1_LOAD:
     case FE_FORM_P2_LOAD:
@@ -80,11 +83,14 @@ int form_rank(int kind) {
     case FE_FORM_P2_FACET_LOAD:
     case FE_FORM_VP2_FACET_LOAD:
     case FE_FORM_P3_LOAD:
+    case FE_FORM_DG0_AVG_LOAD:
+    case FE_FORM_DG1_AVG_LOAD:
       return 1;
     case FE_FORM_INTEGRAL:
     case FE_FORM_P1_ENERGY:
     case FE_FORM_P2_ENERGY:
     case FE_FORM_FACET_INTEGRAL:
+    case FE_FORM_JUMP_NORM:
       return 0;
     default:
       return -1;
@@ -109,6 +115,14 @@ void form_space(int kind, int& k, int& bs) {
     case FE_FORM_P3_STIFFNESS:
     case FE_FORM_P3_LOAD:
       k = 20, bs = 1;
+      return;
+    case FE_FORM_DG0_JUMP:
+    case FE_FORM_DG0_AVG_LOAD:
+      k = 1, bs = 1;
+      return;
+    case FE_FORM_DG1_JUMP:
+    case FE_FORM_DG1_AVG_LOAD:
+      k = 4, bs = 1;
       return;
     default:
       k = 10, bs = 3;
@@ -350,6 +364,62 @@ int fe_sparsity_build_block(fe_context ctx, int num_parts, const fe_dofmap* rows
   });
 }
 
+int fe_sparsity_build_forms(int num_forms, const fe_form* forms, fe_sparsity* out) {
+  return guard([&] {
+    FE_REQUIRE(out && num_forms > 0 && forms, "need at least one form");
+    const fe_form f0 = forms[0];
+    FE_REQUIRE(f0 && f0->rank == 2, "the forms must be bilinear");
+    DeviceScope d(f0->ctx);
+    std::vector<std::unique_ptr<fe_dofmap_s>> macro;  // host-only macro dofmaps of interior-facet forms
+    std::vector<SystemPart> parts;
+    for (int q = 0; q < num_forms; ++q) {
+      const fe_form f = forms[q];
+      FE_REQUIRE(f && f->rank == 2 && f->ctx == f0->ctx, "form " + std::to_string(q) + " is not a bilinear form of "
+                                                          "the same context");
+      FE_REQUIRE(f->V0->num_blocks == f0->V0->num_blocks && f->V0->bs == f0->V0->bs &&
+                     f->V1->num_blocks == f0->V1->num_blocks && f->V1->bs == f0->V1->bs,
+                 "form " + std::to_string(q) + " acts on spaces of other sizes");
+      if (!is_ifacet_kind(f->kind)) {
+        parts.push_back(SystemPart{f->V0, f->V1, 0, 0});
+        continue;
+      }
+      FE_REQUIRE(f->facets_set, "form " + std::to_string(q) + ": set the interior facets first");
+      const int64_t F = f->num_facets;
+      fe_dofmap_s* side[2];
+      for (int t = 0; t < 2; ++t) {
+        const fe_dofmap_s* V = t == 0 ? f->V0 : f->V1;
+        auto m = std::make_unique<fe_dofmap_s>();
+        m->num_cells = F;
+        m->k = 2 * V->k;
+        m->bs = V->bs;
+        m->num_blocks = V->num_blocks;
+        m->host.resize((size_t)F * m->k);
+        for (int64_t e = 0; e < F; ++e)
+          for (int i = 0; i < V->k; ++i) {
+            m->host[e * m->k + i] = V->host[(int64_t)f->host_facets[4 * e] * V->k + i];
+            m->host[e * m->k + V->k + i] = V->host[(int64_t)f->host_facets[4 * e + 2] * V->k + i];
+          }
+        side[t] = m.get();
+        macro.push_back(std::move(m));
+      }
+      parts.push_back(SystemPart{side[0], side[1], 0, 0});
+    }
+    std::vector<int32_t> row_ptr, col, diag;
+    build_system_pattern(parts, scalar_size(f0->V0), scalar_size(f0->V1), row_ptr, col, diag);
+    auto sp = std::make_unique<fe_sparsity_s>();
+    sp->ctx = f0->ctx;
+    sp->num_rows = scalar_size(f0->V0);
+    sp->num_cols = scalar_size(f0->V1);
+    sp->nnz = (int64_t)col.size();
+    upload(sp->row_ptr, row_ptr.data(), row_ptr.size());
+    upload(sp->col, col.data(), col.size());
+    upload(sp->diag, diag.data(), diag.size());
+    sp->host_row_ptr = std::move(row_ptr);
+    sp->id = g_next_id++;
+    *out = sp.release();
+  });
+}
+
 int fe_sparsity_build_device(fe_dofmap rows, fe_dofmap cols, void* stream, fe_sparsity* out) {
   return guard([&] {
     FE_REQUIRE(rows && cols && out, "null argument");
@@ -470,6 +540,7 @@ int fe_form_create(fe_context ctx, int form_kind, fe_mesh mesh, fe_dofmap test, 
                                                " needs " + std::to_string(k) + " bs " + std::to_string(bs));
       FE_REQUIRE(V->num_cells == mesh->num_cells, "dofmap and mesh cell counts differ");
       FE_REQUIRE(!V->excluded || !is_facet_kind(form_kind), "exterior-facet forms take unrestricted dofmaps");
+      FE_REQUIRE(!V->excluded || !is_ifacet_kind(form_kind), "interior-facet forms take unrestricted dofmaps");
     }
     auto f = std::make_unique<fe_form_s>();
     f->ctx = ctx;
@@ -512,7 +583,7 @@ int fe_form_set_coefficient(fe_form f, int index, int coeff_kind, fe_dofmap cmap
       FE_REQUIRE(f->kind == FE_FORM_P2_STIFFNESS || f->kind == FE_FORM_P1_LOAD ||
                      f->kind == FE_FORM_P1_FACET_LOAD || f->kind == FE_FORM_P2_FACET_LOAD ||
                      f->kind == FE_FORM_INTEGRAL || f->kind == FE_FORM_FACET_INTEGRAL ||
-                     (f->kind == FE_FORM_P1_ENERGY && index == 1),
+                     f->kind == FE_FORM_JUMP_NORM || (f->kind == FE_FORM_P1_ENERGY && index == 1),
                  "P1 coefficients are supported by P2 stiffness, P1 load, facet load and functional forms");
     } else if (coeff_kind == FE_COEFF_P2) {
       FE_REQUIRE(f->kind == FE_FORM_P2_ENERGY && index == 1, "P2 coefficients are the u of FE_FORM_P2_ENERGY");
@@ -524,7 +595,8 @@ int fe_form_set_coefficient(fe_form f, int index, int coeff_kind, fe_dofmap cmap
     }
     if (f->kind == FE_FORM_P1_STIFFNESS || f->kind == FE_FORM_VP2_ELASTICITY || f->kind == FE_FORM_P2_LOAD ||
         f->kind == FE_FORM_VP2_LOAD || f->kind == FE_FORM_P1_FACET_MASS || f->kind == FE_FORM_P2_FACET_MASS ||
-        f->kind == FE_FORM_VP2_FACET_LOAD || f->kind == FE_FORM_P3_STIFFNESS || f->kind == FE_FORM_P3_LOAD)
+        f->kind == FE_FORM_VP2_FACET_LOAD || f->kind == FE_FORM_P3_STIFFNESS || f->kind == FE_FORM_P3_LOAD ||
+        is_ifacet_kind(f->kind))
       FE_REQUIRE(coeff_kind != FE_COEFF_P1, "this form takes constant or DG0 coefficients");
     if ((f->kind == FE_FORM_P1_ENERGY || f->kind == FE_FORM_P2_ENERGY) && index == 1)
       FE_REQUIRE(coeff_kind == (f->kind == FE_FORM_P1_ENERGY ? FE_COEFF_P1 : FE_COEFF_P2),
@@ -558,6 +630,55 @@ int fe_form_set_facets(fe_form f, const int32_t* pairs, int64_t num_facets) {
   });
 }
 
+int fe_form_set_interior_facets(fe_form f, const int32_t* quads, int64_t num_facets) {
+  return guard([&] {
+    FE_REQUIRE(f, "null form");
+    FE_REQUIRE(is_ifacet_kind(f->kind) || f->kind == FE_FORM_JUMP_NORM, "not an interior-facet form");
+    FE_REQUIRE(num_facets >= 0 && (quads || num_facets == 0), "invalid facet list");
+    DeviceScope d(f->ctx);
+    const int64_t C = f->mesh->num_cells;
+    const std::vector<int32_t>& G = f->mesh->host_geom;
+    for (int64_t q = 0; q < num_facets; ++q) {
+      const int32_t c0 = quads[4 * q], l0 = quads[4 * q + 1], c1 = quads[4 * q + 2], l1 = quads[4 * q + 3];
+      if (c0 < 0 || c0 >= C || c1 < 0 || c1 >= C || l0 < 0 || l0 > 3 || l1 < 0 || l1 > 3 || c0 == c1)
+        FE_FAIL(FE_ERR_ARG, "interior facet " + std::to_string(q) + " is not a (cell, facet, cell, facet) quadruple "
+                            "of two different cells of the mesh");
+      // the two local facets must be the same triangle
+      for (int t = 0; t < 4; ++t) {
+        if (t == l0) continue;
+        bool found = false;
+        for (int u = 0; u < 4; ++u)
+          if (u != l1 && G[4 * (int64_t)c1 + u] == G[4 * (int64_t)c0 + t]) found = true;
+        if (!found)
+          FE_FAIL(FE_ERR_ARG, "interior facet " + std::to_string(q) + ": the two local facets are different triangles");
+      }
+    }
+    f->host_facets.assign(quads, quads + 4 * num_facets);
+    upload(f->facets, quads, (size_t)(4 * num_facets));
+    f->num_facets = num_facets;
+    f->facets_set = true;
+    // macro dofmaps: cell0's dofs then cell1's, per facet
+    for (int side = 0; side < 2; ++side) {
+      const fe_dofmap_s* V = side == 0 ? f->V0 : f->V1;
+      fe::DevBuf<int32_t>& dst = side == 0 ? f->macro0 : f->macro1;
+      if (!V || (side == 1 && f->V1 == f->V0)) {
+        dst.release();
+        continue;
+      }
+      const int k = V->k;
+      std::vector<int32_t> m((size_t)num_facets * 2 * k);
+      for (int64_t q = 0; q < num_facets; ++q)
+        for (int i = 0; i < k; ++i) {
+          m[q * 2 * k + i] = V->host[(int64_t)quads[4 * q] * k + i];
+          m[q * 2 * k + k + i] = V->host[(int64_t)quads[4 * q + 2] * k + i];
+        }
+      upload(dst, m.data(), m.size());
+    }
+    f->sp = nullptr;  // the byte map depends on the facets: bind again
+    f->view.reset();
+  });
+}
+
 int fe_form_set_precision(fe_form f, int precision) {
   return guard([&] {
     FE_REQUIRE(f, "null form");
@@ -579,9 +700,13 @@ int fe_form_bind_sparsity(fe_form f, fe_sparsity s, void* stream) {
     FE_REQUIRE(!s->parent, "a block view cannot be bound directly");
     FE_REQUIRE(s->num_rows == scalar_size(f->V0) && s->num_cols == scalar_size(f->V1),
                "pattern shape does not match the form's spaces");
+    FE_REQUIRE(!is_ifacet_kind(f->kind) || f->facets_set,
+               "set the interior facets first (fe_form_set_interior_facets)");
     DeviceScope d(f->ctx);
     cudaStream_t st = as_stream(stream);
-    const size_t bytes = (size_t)f->mesh->num_cells * f->V0->k * f->V1->k;
+    const size_t bytes = is_ifacet_kind(f->kind)
+                             ? (size_t)f->num_facets * (2 * f->V0->k) * (2 * f->V1->k)
+                             : (size_t)f->mesh->num_cells * f->V0->k * f->V1->k;
     f->pos.alloc((bytes + 15) / 16 * 16 + 16);
     FE_CUDA(cudaMemsetAsync(f->pos.p, 0, f->pos.bytes(), st));
     f->sp = s;
@@ -603,6 +728,7 @@ int fe_form_bind_sparsity_block(fe_form f, fe_sparsity s, int64_t row_offset, in
     FE_REQUIRE(f->rank == 2, "only bilinear forms bind a matrix pattern");
     FE_REQUIRE(s->ctx == f->ctx, "pattern belongs to another context");
     FE_REQUIRE(!s->parent, "bind to the monolithic pattern, not to a view");
+    FE_REQUIRE(!is_ifacet_kind(f->kind), "interior-facet forms bind with fe_form_bind_sparsity");
     FE_REQUIRE(row_offset >= 0 && col_offset >= 0 && row_offset + scalar_size(f->V0) <= s->num_rows &&
                    col_offset + scalar_size(f->V1) <= s->num_cols,
                "the form's block does not fit the pattern at these offsets");
@@ -697,6 +823,15 @@ int fe_assemble_matrix(fe_form a, double* values, fe_bc bc0, fe_bc bc1, double d
       FE_REQUIRE(!(flags & (FE_ASM_DETERMINISTIC | FE_ASM_SORTED_SLOT | FE_ASM_TILE | FE_ASM_ROW_GATHER |
                             FE_ASM_BLOCK)),
                  "a form bound to a block pattern assembles with the atomic scatter only");
+    if (is_ifacet_kind(a->kind)) {
+      FE_REQUIRE(!(flags & (FE_ASM_DETERMINISTIC | FE_ASM_SORTED_SLOT | FE_ASM_TILE | FE_ASM_ROW_GATHER |
+                            FE_ASM_BLOCK)),
+                 "interior-facet forms assemble with the atomic scatter only");
+      if (zero) launch_zero(values, a->sp->nnz, st);
+      assemble_matrix_ifacets(*a, values, bc0, bc1, st);
+      if (bc0) launch_set_diagonal(*a->sp, *bc0, diagonal, values, st);
+      return;
+    }
     if (is_facet_kind(a->kind)) {
       FE_REQUIRE(!(flags & (FE_ASM_DETERMINISTIC | FE_ASM_SORTED_SLOT | FE_ASM_TILE | FE_ASM_ROW_GATHER |
                             FE_ASM_BLOCK)),
@@ -801,8 +936,10 @@ int fe_assemble_scalar(fe_form M, double* result, void* stream) {
   return guard([&] {
     FE_REQUIRE(M && result, "null argument");
     FE_REQUIRE(M->rank == 0 && is_scalar_kind(M->kind), "assemble_scalar needs a functional");
-    if (M->kind == FE_FORM_INTEGRAL || M->kind == FE_FORM_FACET_INTEGRAL)
+    if (M->kind == FE_FORM_INTEGRAL || M->kind == FE_FORM_FACET_INTEGRAL || M->kind == FE_FORM_JUMP_NORM)
       FE_REQUIRE(M->coeff[0].kind >= 0, "coefficient 0 is not set");
+    if (M->kind == FE_FORM_JUMP_NORM)
+      FE_REQUIRE(M->facets_set, "set the interior facets first (fe_form_set_interior_facets)");
     if (M->kind == FE_FORM_P1_ENERGY || M->kind == FE_FORM_P2_ENERGY)
       FE_REQUIRE(M->coeff[1].kind >= 0, "coefficient 1 (u) is not set");
     DeviceScope d(M->ctx);
@@ -829,6 +966,11 @@ int fe_assemble_vector(fe_form Lf, double* b, unsigned flags, void* stream) {
     if (flags & FE_ASM_ZERO) launch_zero(b, n, st);
     if (is_facet_kind(Lf->kind)) {
       assemble_vector_facets(*Lf, b, n, st);
+      return;
+    }
+    if (is_ifacet_kind(Lf->kind)) {
+      FE_REQUIRE(Lf->facets_set, "set the interior facets first (fe_form_set_interior_facets)");
+      assemble_vector_ifacets(*Lf, b, n, st);
       return;
     }
     VecLaunch L{};
@@ -862,6 +1004,11 @@ int fe_apply_lifting(double* b, int num_forms, const fe_form* a, const fe_bc* bc
       FE_REQUIRE(bc->num_dofs == scalar_size(f->V1), "bc size differs from the trial space size");
       if (is_facet_kind(f->kind)) {
         lifting_facets(*f, *bc, x0 ? x0[i] : nullptr, scale, b, scalar_size(f->V0), st);
+        continue;
+      }
+      if (is_ifacet_kind(f->kind)) {
+        FE_REQUIRE(f->facets_set, "set the interior facets first (fe_form_set_interior_facets)");
+        lifting_ifacets(*f, *bc, x0 ? x0[i] : nullptr, scale, b, scalar_size(f->V0), st);
         continue;
       }
       const int need = (f->kind == FE_FORM_VP2_ELASTICITY) ? 2 : (f->kind == FE_FORM_P2_STIFFNESS ? 1 : 0);

@@ -38,7 +38,8 @@ enum DeviceError : unsigned {
   DEV_ERR_PATTERN = 1u,    // a cell coupling was not found in the CSR row
   DEV_ERR_ROW_WIDE = 2u,   // a block row has more than 255 block columns
   DEV_ERR_BLOCK = 4u,      // the CSR rows of one block row differ
-  DEV_ERR_INDEX = 8u       // an index outside its array
+  DEV_ERR_INDEX = 8u,      // an index outside its array
+  DEV_ERR_FACET = 16u      // the two local facets of an interior facet are not the same triangle
 };
 
 // RAII device buffer.
@@ -162,8 +163,13 @@ struct fe_form_s {
   fe_sparsity sp = nullptr;
   std::unique_ptr<fe_sparsity_s> view;  // block view that sp points to (fe_form_bind_sparsity_block)
   fe::DevBuf<uint8_t> pos;       // [num_cells * k0 * k1] block column positions (padded to 16 B)
-  fe::DevBuf<int32_t> facets;    // exterior-facet forms: [num_facets][2] (cell, local facet)
+  fe::DevBuf<int32_t> facets;    // exterior-facet forms: [num_facets][2] (cell, local facet);
+                                 // interior-facet forms: [num_facets][4] (cell0, facet0, cell1, facet1)
   int64_t num_facets = 0;
+  std::vector<int32_t> host_facets;        // interior-facet forms: host copy (pattern construction)
+  bool facets_set = false;                 // fe_form_set_facets / fe_form_set_interior_facets was called
+  fe::DevBuf<int32_t> macro0, macro1;      // interior-facet forms: [num_facets][2k] test / trial dofs
+                                           // of the two cells (cell0's, then cell1's)
   fe::DevBuf<double> scalar_partial;  // functionals: per-block partial sums + the result
   // deterministic sorted-slot plan (fe_gather.cu); built on first use
   struct Gather;
@@ -361,6 +367,13 @@ void assemble_matrix_block(fe_form_s& f, double* values, const fe_bc_s* bc0, con
 
 // exterior-facet forms (fe_facet.cu)
 bool is_facet_kind(int kind);
+// interior-facet (dS) forms of discontinuous spaces (fe_ifacet.cu)
+bool is_ifacet_kind(int kind);
+void assemble_matrix_ifacets(const fe_form_s& f, double* values, const fe_bc_s* bc0, const fe_bc_s* bc1,
+                             cudaStream_t s);
+void assemble_vector_ifacets(const fe_form_s& f, double* b, int64_t num_values, cudaStream_t s);
+void lifting_ifacets(const fe_form_s& f, const fe_bc_s& bc, const double* x0, double scale, double* b,
+                     int64_t num_values, cudaStream_t s);
 void assemble_matrix_facets(const fe_form_s& f, double* values, const fe_bc_s* bc0, const fe_bc_s* bc1,
                             cudaStream_t s);
 void assemble_vector_facets(const fe_form_s& f, double* b, int64_t num_values, cudaStream_t s);

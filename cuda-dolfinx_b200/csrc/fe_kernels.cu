@@ -890,6 +890,17 @@ void launch_zero(double* v, int64_t n, cudaStream_t s) {
 void launch_build_slotmap(const fe_form_s& f, cudaStream_t s) {
   const fe_dofmap_s& V0 = *f.V0;
   const fe_dofmap_s& V1 = *f.V1;
+  if (is_ifacet_kind(f.kind)) {
+    // interior facets: the macro couplings of the two cells of every facet
+    const int64_t n = f.num_facets * 2 * V0.k;
+    if (n == 0) return;
+    k_build_slotmap<<<grid_for(n, 256), 256, 0, s>>>(f.macro0.p, f.macro1.p ? f.macro1.p : f.macro0.p,
+                                                     f.num_facets, 2 * V0.k, 2 * V1.k, V0.bs, V1.bs,
+                                                     f.sp->row_ptr.p, f.sp->col.p, f.sp->num_rows, f.pos.p,
+                                                     device_error_word(f.ctx));
+    FE_CUDA(cudaGetLastError());
+    return;
+  }
   const int64_t n = V0.num_cells * V0.k;
   if (n == 0) return;
   k_build_slotmap<<<grid_for(n, 256), 256, 0, s>>>(V0.dofs.p, V1.dofs.p, V0.num_cells, V0.k, V1.k, V0.bs,

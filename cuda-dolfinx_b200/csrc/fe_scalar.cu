@@ -1,5 +1,5 @@
 // Scalar assembly (functionals): int f dx, int k |grad u|^2 dx for P1 / P2 u,
-// int g ds over exterior facets.
+// int g ds over exterior facets, int jump(u)^2 dS over interior facets.
 //
 // The reference generates cell / exterior-facet / interior-facet scalar
 // kernels that add every thread's partial value into the result with one
@@ -34,8 +34,9 @@ struct ScalarArgs {
   // coefficient 1 (u of the energy functionals)
   const double* __restrict__ u;
   const int32_t* __restrict__ umap;
-  // facets
+  // facets ((cell, facet) pairs; interior facets: (cell0, facet0, cell1, facet1))
   const int2* __restrict__ facets;
+  const int4* __restrict__ quads;
   double* __restrict__ partial;
 };
 
@@ -102,8 +103,56 @@ __device__ double facet_value(const ScalarArgs& a, int64_t t) {
   return area * coef0_cell(a, c);
 }
 
+// int jump(u)^2 dS over interior facet t: DG0 u: |F| (u0 - u1)^2; a vertex
+// field (DG1 / P1 through a 4-dof map): the jump is linear on the facet with
+// vertex values d_p, and int (sum_p d_p lambda_p)^2 = |F| (sum d_p^2 + (sum d_p)^2) / 12
+__device__ double jump_value(const ScalarArgs& a, int64_t t) {
+  const int4 q = __ldg(a.quads + t);
+  const int4 g0 = __ldg(reinterpret_cast<const int4*>(a.geom) + q.x);
+  const int4 g1 = __ldg(reinterpret_cast<const int4*>(a.geom) + q.z);
+  const int v0[4] = {g0.x, g0.y, g0.z, g0.w}, v1[4] = {g1.x, g1.y, g1.z, g1.w};
+  int loc0[3], loc1[3], n = 0;
+#pragma unroll
+  for (int u = 0; u < 4; ++u)
+    if (u != q.y) loc0[n++] = u;
+#pragma unroll
+  for (int p = 0; p < 3; ++p) {
+    loc1[p] = 0;
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (u != q.w && v1[u] == v0[loc0[p]]) loc1[p] = u;
+  }
+  double P[3][3];
+#pragma unroll
+  for (int p = 0; p < 3; ++p)
+#pragma unroll
+    for (int d = 0; d < 3; ++d) P[p][d] = __ldg(a.x + 3 * (int64_t)v0[loc0[p]] + d);
+  const double e1[3] = {P[1][0] - P[0][0], P[1][1] - P[0][1], P[1][2] - P[0][2]};
+  const double e2[3] = {P[2][0] - P[0][0], P[2][1] - P[0][1], P[2][2] - P[0][2]};
+  const double cx = e1[1] * e2[2] - e1[2] * e2[1], cy = e1[2] * e2[0] - e1[0] * e2[2],
+               cz = e1[0] * e2[1] - e1[1] * e2[0];
+  const double area = 0.5 * sqrt(cx * cx + cy * cy + cz * cz);
+  if (a.c0kind == FE_COEFF_P1) {
+    double s1 = 0.0, s2 = 0.0;
+#pragma unroll
+    for (int p = 0; p < 3; ++p) {
+      const double d = __ldg(a.c0v + __ldg(a.c0map + 4 * (int64_t)q.x + loc0[p])) -
+                       __ldg(a.c0v + __ldg(a.c0map + 4 * (int64_t)q.z + loc1[p]));
+      s1 += d;
+      s2 += d * d;
+    }
+    return area * (s2 + s1 * s1) * (1.0 / 12.0);
+  }
+  if (a.c0kind == FE_COEFF_DG0) {
+    const double d = __ldg(a.c0v + q.x) - __ldg(a.c0v + q.z);
+    return area * d * d;
+  }
+  return 0.0;  // a constant has no jump
+}
+
 __device__ double cell_value(const ScalarArgs& a, int64_t c) {
   if (a.kind == FE_FORM_FACET_INTEGRAL) return facet_value(a, c);
+  if (a.kind == FE_FORM_JUMP_NORM) return jump_value(a, c);
   Geo g;
   tet_geometry(a.x, __ldg(reinterpret_cast<const int4*>(a.geom) + c), g);
   const double vol = g.adet * (1.0 / 6.0);
@@ -174,7 +223,7 @@ __global__ void __launch_bounds__(kScalarThreads) k_scalar_final(double* __restr
 
 bool is_scalar_kind(int kind) {
   return kind == FE_FORM_INTEGRAL || kind == FE_FORM_P1_ENERGY || kind == FE_FORM_P2_ENERGY ||
-         kind == FE_FORM_FACET_INTEGRAL;
+         kind == FE_FORM_FACET_INTEGRAL || kind == FE_FORM_JUMP_NORM;
 }
 
 double assemble_scalar(fe_form_s& f, cudaStream_t s) {
@@ -182,7 +231,8 @@ double assemble_scalar(fe_form_s& f, cudaStream_t s) {
   if (f.scalar_partial.n < (size_t)grid + 1) f.scalar_partial.alloc(grid + 1);
   ScalarArgs a{};
   a.kind = f.kind;
-  a.num_items = f.kind == FE_FORM_FACET_INTEGRAL ? f.num_facets : f.mesh->num_cells;
+  a.num_items =
+      (f.kind == FE_FORM_FACET_INTEGRAL || f.kind == FE_FORM_JUMP_NORM) ? f.num_facets : f.mesh->num_cells;
   a.x = f.mesh->x.p;
   a.geom = f.mesh->geom.p;
   const Coefficient& c0 = f.coeff[0];
@@ -194,6 +244,7 @@ double assemble_scalar(fe_form_s& f, cudaStream_t s) {
   a.u = c1.values;
   a.umap = c1.map ? c1.map->dofs.p : nullptr;
   a.facets = reinterpret_cast<const int2*>(f.facets.p);
+  a.quads = reinterpret_cast<const int4*>(f.facets.p);
   a.partial = f.scalar_partial.p;
   k_scalar<<<grid, kScalarThreads, 0, s>>>(a);
   FE_CUDA(cudaGetLastError());

@@ -35,7 +35,9 @@ FE_ERR_NOT_CONVERGED = 6
 FORM = {"P1_STIFFNESS": 1, "P2_STIFFNESS": 2, "VP2_ELASTICITY": 3, "P1_LOAD": 11, "P2_LOAD": 12, "VP2_LOAD": 13,
         "P1_FACET_MASS": 4, "P2_FACET_MASS": 5, "P1_FACET_LOAD": 14, "P2_FACET_LOAD": 15, "VP2_FACET_LOAD": 16,
         "INTEGRAL": 31, "P1_ENERGY": 32, "P2_ENERGY": 33, "FACET_INTEGRAL": 34,
-        "P3_STIFFNESS": 6, "P3_LOAD": 17}
+        "P3_STIFFNESS": 6, "P3_LOAD": 17, "DG0_JUMP": 7, "DG1_JUMP": 8, "DG0_AVG_LOAD": 18, "DG1_AVG_LOAD": 19,
+        "JUMP_NORM": 35}
+INTERIOR_FACET_KINDS = ("DG0_JUMP", "DG1_JUMP", "DG0_AVG_LOAD", "DG1_AVG_LOAD", "JUMP_NORM")
 COEFF_CONSTANT, COEFF_DG0, COEFF_P1, COEFF_P2 = 0, 1, 2, 3
 PREC_FP64, PREC_FP32 = 0, 1
 ASM_ZERO, ASM_DETERMINISTIC, ASM_ATOMIC, ASM_SORTED_SLOT, ASM_TILE, ASM_ROW_GATHER, ASM_BLOCK = 1, 2, 4, 8, 16, 32, 64
@@ -57,6 +59,7 @@ _SIGS = {
     "fe_sparsity_build": (i32, [vp, vp, PP]),
     "fe_sparsity_build_device": (i32, [vp, vp, vp, PP]),
     "fe_sparsity_build_block": (i32, [vp, i32, vp, vp, vp, vp, i64, i64, PP]),
+    "fe_sparsity_build_forms": (i32, [i32, vp, PP]),
     "fe_sparsity_create": (i32, [vp, vp, vp, i64, i64, PP]),
     "fe_sparsity_info": (i32, [vp, ctypes.POINTER(i64), ctypes.POINTER(i64), ctypes.POINTER(i64)]),
     "fe_sparsity_copy_to_host": (i32, [vp, vp, vp]),
@@ -68,6 +71,7 @@ _SIGS = {
     "fe_form_set_coefficient": (i32, [vp, i32, i32, vp, vp, i64, i32, vp]),
     "fe_form_set_precision": (i32, [vp, i32]),
     "fe_form_set_facets": (i32, [vp, vp, i64]),
+    "fe_form_set_interior_facets": (i32, [vp, vp, i64]),
     "fe_assemble_scalar": (i32, [vp, ctypes.POINTER(dbl), vp]),
     "fe_form_bind_sparsity": (i32, [vp, vp, vp]),
     "fe_form_bind_sparsity_block": (i32, [vp, vp, i64, i64, vp]),

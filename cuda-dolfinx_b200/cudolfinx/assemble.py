@@ -47,11 +47,32 @@ class CUDAAssembler:
         self._ctx = get_cuda_context()
 
     # -- creation ------------------------------------------------------------
-    def create_matrix(self, a: CUDAForm) -> CUDAMatrix:
+    def create_matrix(self, a) -> CUDAMatrix:
+        """Device CSR matrix for a bilinear form (create_cuda_matrix,
+        assemble.py:228-234).  ``a`` may also be a list of bilinear forms on
+        the same spaces whose sum is to be assembled into one matrix (the
+        integrals of one DOLFINx form, e.g. a DG cell term and its
+        interior-facet jump term): the pattern is the union of their
+        couplings and every form is bound to it."""
+        if isinstance(a, (list, tuple)):
+            forms = list(a)
+            if not forms or not all(isinstance(f, CUDAForm) and f.rank == 2 for f in forms):
+                raise TypeError("Expected a list of bilinear CUDAForms")
+            sp = Sparsity.build_forms(self._ctx, forms)
+            mat = CUDAMatrix(self._ctx, sp)
+            for f in forms:
+                f._bind(sp)
+            return mat
         if not isinstance(a, CUDAForm):
             raise TypeError(f"Expected CUDAForm, got type '{type(a)}'.")
         if a.rank != 2:
             raise ValueError("create_matrix needs a bilinear form")
+        if a.dolfinx_form.kind in _lib.INTERIOR_FACET_KINDS:
+            # interior-facet couplings join the two cells of every facet
+            sp = Sparsity.build_forms(self._ctx, [a])
+            mat = CUDAMatrix(self._ctx, sp)
+            a._bind(sp)
+            return mat
         if a.restriction(0) is not None or a.restriction(1) is not None:
             # a restricted form is a one-block system
             sp = Sparsity.build_block(self._ctx, [(a._dofmaps[0], a._dofmaps[1], 0, 0)], a.space_size(0),

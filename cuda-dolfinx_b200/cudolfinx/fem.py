@@ -104,10 +104,13 @@ class FunctionSpace:
         if self.bs not in (1, 3):
             raise ValueError("value shape must be () or (3,)")
         if self.family == "DG":
-            if degree != 0:
-                raise ValueError("only DG0 is supported")
-            self.dofs = np.arange(mesh.num_cells, dtype=np.int32).reshape(-1, 1)
-            self.num_nodes = mesh.num_cells
+            if degree not in (0, 1) or self.bs != 1 and degree != 0:
+                raise ValueError("DG0 (scalar or vector) and scalar DG1 are supported")
+            # discontinuous: every cell owns its dofs (DG1: one per vertex, in
+            # the cell's vertex order)
+            k = 1 if degree == 0 else 4
+            self.dofs = np.arange(mesh.num_cells * k, dtype=np.int32).reshape(-1, k)
+            self.num_nodes = mesh.num_cells * k
             self._node_x = None
             self._grid = None
         elif degree == 1:
@@ -170,7 +173,7 @@ class FunctionSpace:
         X = np.zeros((self.num_nodes, 3))
         cx = m.geometry_x[m.cells]
         if self.family == "DG":
-            return cx.mean(axis=1)
+            return cx.mean(axis=1) if self.degree == 0 else cx.reshape(-1, 3).copy()
         if self.degree == 1:
             X[self.dofs.ravel()] = m.geometry_x[m.cells.ravel()]
             return X
@@ -201,7 +204,7 @@ class FunctionSpace:
 def reference_nodes(V: FunctionSpace) -> np.ndarray:
     """Reference coordinates [k, 3] of the element's nodes in local order
     (DG0: the centroid)."""
-    if V.family == "DG":
+    if V.family == "DG" and V.degree == 0:
         return np.full((1, 3), 0.25)
     if V.degree == 1:
         W = np.eye(4)
@@ -217,7 +220,7 @@ def lagrange_basis(V: FunctionSpace, X: np.ndarray) -> np.ndarray:
     (barycentric formulas of the equispaced Lagrange elements, basix local order)."""
     X = np.atleast_2d(np.asarray(X, dtype=np.float64))
     lam = np.column_stack([1.0 - X.sum(axis=1), X[:, 0], X[:, 1], X[:, 2]])
-    if V.family == "DG":
+    if V.family == "DG" and V.degree == 0:
         return np.ones((len(X), 1))
     if V.degree == 1:
         return lam
@@ -413,6 +416,54 @@ def facet_integral(g: Coefficient, mesh: "Mesh", facets: Optional[np.ndarray] = 
     """The functional int g ds over exterior facets; g constant, DG0 or P1."""
     facets = exterior_facets(mesh) if facets is None else np.ascontiguousarray(facets, dtype=np.int32)
     return FormSpec("FACET_INTEGRAL", None, [g], 0, "fp64", facets, mesh)
+
+
+def interior_facets(mesh: "Mesh") -> np.ndarray:
+    """(cell0, local facet0, cell1, local facet1) of every facet shared by two
+    cells, cell0 < cell1, ordered by the facet's sorted vertex triple (the
+    interior-facet integration domain DOLFINx hands the reference,
+    CUDAFormIntegral.cpp:451-522)."""
+    F = np.sort(mesh.cells[:, _TET_FACETS], axis=2).reshape(-1, 3)
+    _, inv, cnt = np.unique(F, axis=0, return_inverse=True, return_counts=True)
+    inv = inv.ravel()
+    order = np.argsort(inv, kind="stable")
+    start = np.concatenate([[0], np.cumsum(cnt)[:-1]])
+    two = np.nonzero(cnt == 2)[0]
+    e0, e1 = order[start[two]], order[start[two] + 1]
+    return np.ascontiguousarray(np.stack([e0 // 4, e0 % 4, e1 // 4, e1 % 4], axis=1).astype(np.int32))
+
+
+def _dg(V: FunctionSpace) -> int:
+    if V.family != "DG" or V.bs != 1 or V.degree not in (0, 1):
+        raise ValueError("interior-facet forms act on scalar DG0 / DG1 spaces")
+    return V.degree
+
+
+def jump_penalty(V: FunctionSpace, alpha: Coefficient = 1.0, facets: Optional[np.ndarray] = None) -> FormSpec:
+    """alpha * jump(u) * jump(v) * dS over interior facets on DG0 / DG1
+    (jump = value from cell0 minus value from cell1); alpha constant or DG0,
+    averaged over the two cells of a facet."""
+    kind = "DG0_JUMP" if _dg(V) == 0 else "DG1_JUMP"
+    facets = interior_facets(V.mesh) if facets is None else np.ascontiguousarray(facets, dtype=np.int32)
+    return FormSpec(kind, V, [alpha], 2, "fp64", facets)
+
+
+def facet_average_load(V: FunctionSpace, g: Coefficient = 1.0, facets: Optional[np.ndarray] = None) -> FormSpec:
+    """g * avg(v) * dS over interior facets on DG0 / DG1; g constant or DG0
+    (averaged over the two cells)."""
+    kind = "DG0_AVG_LOAD" if _dg(V) == 0 else "DG1_AVG_LOAD"
+    facets = interior_facets(V.mesh) if facets is None else np.ascontiguousarray(facets, dtype=np.int32)
+    return FormSpec(kind, V, [g], 1, "fp64", facets)
+
+
+def jump_norm(u: "Function", facets: Optional[np.ndarray] = None) -> FormSpec:
+    """The functional int jump(u)^2 dS over interior facets for a DG0, DG1 or
+    P1 Function u (zero for a continuous u)."""
+    V = u.function_space
+    if V.bs != 1 or V.degree not in (0, 1) or (V.family == "P" and V.degree != 1):
+        raise ValueError("jump_norm needs a scalar DG0, DG1 or P1 Function")
+    facets = interior_facets(V.mesh) if facets is None else np.ascontiguousarray(facets, dtype=np.int32)
+    return FormSpec("JUMP_NORM", None, [u], 0, "fp64", facets, V.mesh)
 
 
 def load(V: FunctionSpace, f: Coefficient) -> FormSpec:

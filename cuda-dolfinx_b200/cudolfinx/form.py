@@ -135,7 +135,11 @@ class CUDAForm:
         if form.facets is not None:
             fc = np.ascontiguousarray(form.facets, dtype=np.int32)
             self._facets = fc
-            _lib.check(_lib.lib.fe_form_set_facets(self._handle, fc.ctypes.data, len(fc)), "fe_form_set_facets")
+            if form.kind in _lib.INTERIOR_FACET_KINDS:
+                _lib.check(_lib.lib.fe_form_set_interior_facets(self._handle, fc.ctypes.data, len(fc)),
+                           "fe_form_set_interior_facets")
+            else:
+                _lib.check(_lib.lib.fe_form_set_facets(self._handle, fc.ctypes.data, len(fc)), "fe_form_set_facets")
         if form.precision == "fp32":
             _lib.check(_lib.lib.fe_form_set_precision(self._handle, _lib.PREC_FP32), "fe_form_set_precision")
         self._bound_sparsity = None
@@ -175,8 +179,13 @@ class CUDAForm:
         if isinstance(c, Function):
             V = c.function_space
             vals = np.ascontiguousarray(c.x.array, dtype=np.float64)
-            if V.family == "DG":
+            if V.family == "DG" and V.degree == 0:
                 kind, cmap = _lib.COEFF_DG0, None
+            elif V.family == "DG" and V.degree == 1:
+                # vertex values through the DG1 dofmap: the engine's 4-dof
+                # vertex-field coefficient (FE_COEFF_P1)
+                kind, cmap = _lib.COEFF_P1, device_dofmap(ctx, V)
+                self._aux_dofmaps[i] = cmap
             elif V.degree == 1 and V.bs == 1:
                 kind, cmap = _lib.COEFF_P1, device_dofmap(ctx, V)
                 self._aux_dofmaps[i] = cmap

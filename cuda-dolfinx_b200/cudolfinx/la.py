@@ -59,6 +59,17 @@ class Sparsity:
         return cls(ctx, h.value)
 
     @classmethod
+    def build_forms(cls, ctx, forms):
+        """Pattern of a sum of bilinear forms on the same spaces: the union of
+        their cell / interior-facet couplings (create_sparsity_pattern of a
+        form with several integrals)."""
+        n = len(forms)
+        tab = (ctypes.c_void_p * n)(*[f.cuda_form for f in forms])
+        h = _lib.out_handle()
+        _lib.check(_lib.lib.fe_sparsity_build_forms(n, tab, h), "fe_sparsity_build_forms")
+        return cls(ctx, h.value)
+
+    @classmethod
     def from_csr(cls, ctx, row_ptr, col, num_cols):
         rp = np.ascontiguousarray(row_ptr, dtype=np.int32)
         cl = np.ascontiguousarray(col, dtype=np.int32)

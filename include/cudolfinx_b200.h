@@ -67,12 +67,23 @@ enum fe_form_kind {
   FE_FORM_P1_FACET_LOAD = 14,  /* g*v*ds, P1;        coeff 0 = g (constant / DG0 / P1) */
   FE_FORM_P2_FACET_LOAD = 15,  /* g*v*ds, P2;        coeff 0 = g (constant / DG0 / P1) */
   FE_FORM_VP2_FACET_LOAD = 16, /* inner(t, v)*ds, vector P2; coeff 0 = t (3 comps)   */
+  /* interior-facet (dS) forms of discontinuous spaces over the facets given by
+   * fe_form_set_interior_facets (CUDAFormIntegral.cpp:451-522 vector,
+   * :1988-2103 matrix); jump(u) = u(cell0) - u(cell1), avg(v) = (v(cell0) +
+   * v(cell1))/2; a DG0 coefficient enters as the average of the two cells */
+  FE_FORM_DG0_JUMP = 7,        /* alpha*jump(u)*jump(v)*dS, DG0 (1 dof/cell); coeff 0 = alpha */
+  FE_FORM_DG1_JUMP = 8,        /* the same on DG1 (4 dofs/cell, one per vertex)  */
+  FE_FORM_DG0_AVG_LOAD = 18,   /* g*avg(v)*dS, DG0;  coeff 0 = g (constant / DG0) */
+  FE_FORM_DG1_AVG_LOAD = 19,   /* g*avg(v)*dS, DG1                                */
   /* functionals (rank 0, fe_assemble_scalar; CUDAFormIntegral.cpp:66-266) */
   FE_FORM_INTEGRAL = 31,       /* int f dx;          coeff 0 = f (constant / DG0 / P1) */
   FE_FORM_P1_ENERGY = 32,      /* int k |grad u|^2 dx; coeff 0 = k (constant / DG0),
                                   coeff 1 = u (P1, through its P1 dofmap)           */
   FE_FORM_P2_ENERGY = 33,      /* as P1_ENERGY with u a P2 field (FE_COEFF_P2)      */
-  FE_FORM_FACET_INTEGRAL = 34  /* int g ds over fe_form_set_facets; coeff 0 = g     */
+  FE_FORM_FACET_INTEGRAL = 34, /* int g ds over fe_form_set_facets; coeff 0 = g     */
+  FE_FORM_JUMP_NORM = 35       /* int jump(u)^2 dS over fe_form_set_interior_facets;
+                                  coeff 0 = u: DG0 (FE_COEFF_DG0) or DG1 / P1 through
+                                  its 4-dof dofmap (FE_COEFF_P1)                    */
 };
 
 /* Coefficient representations (CUDAFormCoefficients.h:352-365 packs these
@@ -154,6 +165,13 @@ int fe_sparsity_build(fe_dofmap rows, fe_dofmap cols, fe_sparsity* out);
  * couplings, then the same unroll), bit-exact with fe_sparsity_build; for
  * callers that create many meshes.  Synchronises `stream`. */
 int fe_sparsity_build_device(fe_dofmap rows, fe_dofmap cols, void* stream, fe_sparsity* out);
+/* The pattern of a sum of bilinear forms on the same spaces, as DOLFINx's
+ * create_sparsity_pattern builds it for a form with several integrals: the
+ * union of the cell couplings of cell and exterior-facet forms and of the
+ * couplings of both cells of every facet of interior-facet forms
+ * (cpp/cudolfinx/fem/utils.h:61-83 inserts the same macro-cell dofs).
+ * Built on the host. */
+int fe_sparsity_build_forms(int num_forms, const fe_form* forms, fe_sparsity* out);
 /* Replaces create_cuda_matrix_block (cpp/cudolfinx/fem/petsc.h:39-107): the
  * monolithic scalar pattern of a block form.  Part p contributes the cell
  * couplings of (rows[p], cols[p]) unrolled and shifted to scalar row
@@ -201,6 +219,14 @@ int fe_form_set_precision(fe_form f, int precision);
  * opposite vertex f of the cell (the pairs DOLFINx packs for the reference's
  * active_mesh_entities, CUDAFormIntegral.cpp:361-447). */
 int fe_form_set_facets(fe_form f, const int32_t* cell_facet_pairs, int64_t num_facets);
+/* Integration domain of an interior-facet form (FE_FORM_DG*_JUMP,
+ * FE_FORM_DG*_AVG_LOAD, FE_FORM_JUMP_NORM): num_facets quadruples (cell0,
+ * local facet0, cell1, local facet1), host int32, where the two local facets
+ * are the same triangle (the interior-facet entities DOLFINx packs for the
+ * reference, CUDAFormIntegral.cpp:451-522).  The element tensors couple the
+ * dofs of both cells.  A facet whose two sides differ is reported as
+ * FE_ERR_DEVICE by the next synchronising call and contributes nothing. */
+int fe_form_set_interior_facets(fe_form f, const int32_t* quads, int64_t num_facets);
 /* Bind the matrix pattern and build the cell-to-slot map once (the reference's
  * unused lookup-table prototype, CUDAFormIntegral.cpp:1230-1407, made the
  * default).  Fails with FE_ERR_PATTERN if a cell coupling is missing. */

@@ -719,6 +719,92 @@ def assemble_block_vector(parts, size):
 
 
 # ---------------------------------------------------------------------------
+# Interior-facet (dS) integrals of discontinuous spaces
+# (CUDAFormIntegral.cpp:451-522 vector, :1988-2103 matrix)
+# ---------------------------------------------------------------------------
+
+def interior_facets(cells):
+    """(cell0, local facet0, cell1, local facet1) of every facet shared by two
+    cells, cell0 < cell1, ordered by the facet's sorted vertex triple."""
+    F = np.sort(cells[:, np.array(TET_FACETS)], axis=2).reshape(-1, 3)
+    _, inv, cnt = np.unique(F, axis=0, return_inverse=True, return_counts=True)
+    inv = inv.ravel()
+    order = np.argsort(inv, kind="stable")
+    start = np.concatenate([[0], np.cumsum(cnt)[:-1]])
+    two = np.nonzero(cnt == 2)[0]
+    e0, e1 = order[start[two]], order[start[two] + 1]
+    return np.stack([e0 // 4, e0 % 4, e1 // 4, e1 % 4], axis=1).astype(np.int32)
+
+
+def dg_dofmap(num_cells, degree):
+    """Discontinuous Lagrange dofmap: each cell owns its dofs (DG0: one, DG1:
+    one per vertex in the cell's vertex order)."""
+    k = 1 if degree == 0 else 4
+    return np.arange(num_cells * k, dtype=np.int32).reshape(num_cells, k)
+
+
+def _barycentric(coords, cells, c, X):
+    """Barycentric coordinates [F, q, 4] of points X [F, q, 3] in cells c [F]."""
+    x = coords[cells[c]]  # [F,4,3]
+    J = np.transpose(x[:, 1:] - x[:, :1], (0, 2, 1))  # columns x_k - x_0
+    l = np.linalg.solve(J[:, None], (X - x[:, :1])[..., None])[..., 0]
+    return np.concatenate([1.0 - l.sum(axis=2, keepdims=True), l], axis=2)
+
+
+def _facet_traces(coords, cells, quads, degree):
+    """Quadrature (the 3 edge midpoints of the facet, weight area/3 each:
+    exact for quadratics) and the traces of both cells' bases there:
+    returns w [F, 3], T0 [F, 3, k], T1 [F, 3, k]."""
+    quads = np.asarray(quads)
+    c0, f0, c1 = quads[:, 0], quads[:, 1], quads[:, 2]
+    v = cells[c0[:, None], np.array(TET_FACETS)[f0]]  # [F,3] facet vertices
+    P = coords[v]  # [F,3,3]
+    X = 0.5 * (P + P[:, [1, 2, 0]])  # edge midpoints
+    area = 0.5 * np.linalg.norm(np.cross(P[:, 1] - P[:, 0], P[:, 2] - P[:, 0]), axis=1)
+    w = np.repeat(area[:, None] / 3.0, 3, axis=1)
+    if degree == 0:
+        one = np.ones((len(quads), 3, 1))
+        return w, one, one
+    return w, _barycentric(coords, cells, c0, X), _barycentric(coords, cells, c1, X)
+
+
+def interior_jump_tensors(coords, cells, quads, degree, alpha=None):
+    """[F, 2k, 2k] of alpha * jump(u) * jump(v) * dS: macro dofs = cell0's
+    then cell1's, jump = trace from cell0 minus trace from cell1; alpha per
+    facet (the DG0 average of the two cells, or 1)."""
+    w, T0, T1 = _facet_traces(coords, cells, quads, degree)
+    S = np.concatenate([T0, -T1], axis=2)  # [F,3,2k]
+    A = np.einsum("fq,fqi,fqj->fij", w, S, S)
+    return A if alpha is None else A * np.asarray(alpha)[:, None, None]
+
+
+def interior_avg_load(coords, cells, quads, degree, g=None):
+    """[F, 2k] of g * avg(v) * dS (g per facet, or 1)."""
+    w, T0, T1 = _facet_traces(coords, cells, quads, degree)
+    be = 0.5 * np.einsum("fq,fqi->fi", w, np.concatenate([T0, T1], axis=2))
+    return be if g is None else be * np.asarray(g)[:, None]
+
+
+def interior_jump_norm(coords, cells, quads, degree, u_macro):
+    """sum over the facets of int jump(u)^2 dS, u_macro [F, 2k] the macro dof values."""
+    w, T0, T1 = _facet_traces(coords, cells, quads, degree)
+    S = np.concatenate([T0, -T1], axis=2)
+    return float(np.einsum("fq,fq->", w, np.einsum("fqi,fi->fq", S, u_macro) ** 2))
+
+
+def macro_dofmap(dofs, quads):
+    """[F, 2k]: cell0's dofs then cell1's for every interior facet."""
+    quads = np.asarray(quads)
+    return np.concatenate([dofs[quads[:, 0]], dofs[quads[:, 2]]], axis=1)
+
+
+def facet_average(values_per_cell, quads):
+    """The average of a DG0 field over the two cells of each interior facet."""
+    v = np.asarray(values_per_cell)
+    return 0.5 * (v[quads[:, 0]] + v[quads[:, 2]])
+
+
+# ---------------------------------------------------------------------------
 # Same-map interpolation (cpp/cudolfinx/fem/CUDACoefficient.h:64-83,
 # cpp/cudolfinx/fem/CUDAInterpolate.cu)
 # ---------------------------------------------------------------------------

@@ -413,3 +413,69 @@ def test_oracle_interpolation_is_exact_for_polynomials_on_the_mesh():
     assert np.abs(u3 - q(X3)).max() < 1e-13
     u2 = fo.interpolate_same_map(u3, d3, d2, fo.interpolation_operator(2, 3), n2)
     assert np.abs(u2 - q(X2)).max() < 1e-13
+
+
+# --- interior-facet (DG) integrals ----------------------------------------------
+def _dg_problem(n=3, jitter=0.2, seed=1):
+    coords, cells = fo.unit_cube_tet_mesh(n, jitter=jitter, seed=seed)
+    return coords, cells, fo.interior_facets(cells)
+
+
+def test_interior_facets_pair_matching_faces():
+    coords, cells, q = _dg_problem(3)
+    n = 3
+    # every facet is interior or exterior; 4 facets per cell
+    ext = fo.exterior_facets(cells)
+    assert 2 * len(q) + len(ext) == 4 * len(cells)
+    assert len(ext) == 2 * 6 * n * n  # two triangles per boundary square
+    F = np.array(fo.TET_FACETS)
+    a = np.sort(cells[q[:, 0][:, None], F[q[:, 1]]], axis=1)
+    b = np.sort(cells[q[:, 2][:, None], F[q[:, 3]]], axis=1)
+    assert np.array_equal(a, b) and np.all(q[:, 0] < q[:, 2])
+
+
+def test_dg0_jump_matrix_is_the_area_weighted_cell_graph_laplacian():
+    coords, cells, q = _dg_problem(2)
+    C = len(cells)
+    alpha = np.random.default_rng(0).uniform(0.5, 2.0, C)
+    af = fo.facet_average(alpha, q)
+    Ae = fo.interior_jump_tensors(coords, cells, q, 0, af)
+    d = fo.dg_dofmap(C, 0)
+    A = np.zeros((C, C))
+    for f, (c0, _, c1, _) in enumerate(q):
+        m = fo.macro_dofmap(d, q[f:f + 1])[0]
+        A[np.ix_(m, m)] += Ae[f]
+    area = fo.facet_areas(coords, cells, q[:, :2])
+    L = np.zeros((C, C))
+    for f, (c0, _, c1, _) in enumerate(q):
+        w = af[f] * area[f]
+        L[c0, c0] += w
+        L[c1, c1] += w
+        L[c0, c1] -= w
+        L[c1, c0] -= w
+    assert np.allclose(A, L, rtol=1e-13, atol=1e-15)
+
+
+def test_dg1_jump_vanishes_on_continuous_fields_and_is_the_jump_norm():
+    coords, cells, q = _dg_problem(3)
+    C = len(cells)
+    d = fo.dg_dofmap(C, 1)
+    m = fo.macro_dofmap(d, q)
+    Ae = fo.interior_jump_tensors(coords, cells, q, 1)
+    rng = np.random.default_rng(4)
+    # a continuous P1 field written into DG1 has no jump
+    uc = rng.standard_normal(len(coords))[cells].ravel()
+    assert np.abs(np.einsum("fij,fj->fi", Ae, uc[m])).max() < 1e-14
+    assert abs(fo.interior_jump_norm(coords, cells, q, 1, uc[m])) < 1e-28
+    # for any DG1 field, u^T A u is the jump norm
+    u = rng.standard_normal(4 * C)
+    uAu = np.einsum("fi,fij,fj->", u[m], Ae, u[m])
+    assert abs(uAu - fo.interior_jump_norm(coords, cells, q, 1, u[m])) < 1e-12 * uAu
+
+
+def test_interior_average_load_sums_to_the_interior_facet_area():
+    coords, cells, q = _dg_problem(3)
+    area = fo.facet_areas(coords, cells, q[:, :2]).sum()
+    for degree in (0, 1):
+        be = fo.interior_avg_load(coords, cells, q, degree)
+        assert abs(be.sum() - area) < 1e-13 * area
