@@ -2,7 +2,7 @@
 """Headline benchmark: FEM system assembly on one B200 (matrix nnz/s).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload p2|p2mid|p1|p1big|vp2|p3|batch|multimesh|serve|blocksys|interp] [--variant auto|tile|atomic|sorted-slot]
+                    [--workload p2|p2mid|p1|p1big|vp2|p3|batch|multimesh|serve|blocksys|interp|dg] [--variant auto|tile|atomic|sorted-slot]
 
 Default workload (the configuration the headline metric is quoted on): P2
 Poisson on the unit cube, 96^3 hexes x 6 = 5,308,416 tets, 7,189,057 dofs,
@@ -1097,6 +1097,200 @@ def run_reference_interp(args):
                                        "d2h_bytes_per_step": 0}}
 
 
+# interior-penalty DG1 system: broken P1 stiffness + jump penalty + facet load
+DGSYS = dict(n=64, alpha=10.0, cpu_n=16,
+             desc="DG1 interior-penalty system on the unit cube, n=64 (1,572,864 tets, 6,291,456 dofs, 3,121,152 "
+                  "interior facets): broken P1 stiffness + 10*jump(u)*jump(v)*dS on one union pattern, load "
+                  "g*avg(v)*dS with g DG0 U[-1,1]; FP64")
+# zero + cell scatter + mirror + jump scatter + vector zero + facet load
+DGSYS_KERNELS = 6
+
+
+def dg_inputs(n: int, seed: int, pinned: bool = False):
+    from cudolfinx import fem
+
+    mesh = fem.create_unit_cube(n)
+    V = fem.functionspace(mesh, ("DG", 1))
+    W = fem.functionspace(mesh, ("DG", 0))
+    g = np.random.default_rng(seed).uniform(-1.0, 1.0, mesh.num_cells)
+    if pinned:
+        import torch
+        t = torch.empty(g.shape, dtype=torch.float64, pin_memory=True)
+        _PINNED.append(t)
+        t.numpy()[:] = g
+        g = t.numpy()
+    q = fem.interior_facets(mesh)
+    a_cell = fem.FormSpec("P1_STIFFNESS", V, [1.0], 2)
+    a_jump = fem.jump_penalty(V, DGSYS["alpha"], facets=q)
+    L = fem.facet_average_load(V, fem.Function(W, g), facets=q)
+    return dict(mesh=mesh, V=V, a_cell=a_cell, a_jump=a_jump, L=L, facets=q, g=g)
+
+
+def dg_cpu_sample(n: int, seed: int):
+    """The oracle on the n-sized DG1 system: element tensors (cells and
+    facets) + monolithic matrix + facet load."""
+    from oracle import fem_oracle as fo
+
+    coords, cells = fo.unit_cube_tet_mesh(n)
+    q = fo.interior_facets(cells)
+    C = len(cells)
+    d = fo.dg_dofmap(C, 1)
+    m = fo.macro_dofmap(d, q)
+    N = 4 * C
+    g = np.random.default_rng(seed).uniform(-1.0, 1.0, C)
+    rp, col = fo.block_pattern([(d, d, 1, 1, 0, 0), (m, m, 1, 1, 0, 0)], N, N)
+    t0 = time.perf_counter()
+    fo.assemble_block_matrix([
+        dict(Ae=fo.p1_stiffness(coords, cells), dofs0=d, dofs1=d, bs0=1, bs1=1, row_offset=0, col_offset=0),
+        dict(Ae=fo.interior_jump_tensors(coords, cells, q, 1, np.full(len(q), DGSYS["alpha"])), dofs0=m, dofs1=m,
+             bs0=1, bs1=1, row_offset=0, col_offset=0)], rp, col)
+    fo.assemble_vector(fo.interior_avg_load(coords, cells, q, 1, fo.facet_average(g, q)), m, N)
+    t = time.perf_counter() - t0
+    return t, len(col)
+
+
+def run_gpu_dg(args, rank, world, local_rank):
+    import torch
+
+    import cudolfinx as cx
+    from cudolfinx import _lib
+
+    torch.cuda.set_device(local_rank)
+    t_setup = time.perf_counter()
+    I = dg_inputs(DGSYS["n"], args.seed)
+    asm = cx.CUDAAssembler()
+    a_cell, a_jump, L = cx.form(I["a_cell"]), cx.form(I["a_jump"]), cx.form(I["L"])
+    A = asm.create_matrix([a_cell, a_jump])
+    b = asm.create_vector(L)
+    nnz, nrows = A.sparsity.nnz, A.sparsity.num_rows
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+    Lib = _lib.lib
+    Ap, bp = A.values.data_ptr(), b.vector.data_ptr()
+
+    def step(ev0=None, ev1=None):
+        if ev0 is not None:
+            ev0.record(stream)
+        _lib.check(Lib.fe_assemble_matrix(a_cell.cuda_form, Ap, None, None, 1.0, _lib.ASM_ZERO, sp), "cell")
+        _lib.check(Lib.fe_assemble_matrix(a_jump.cuda_form, Ap, None, None, 1.0, 0, sp), "jump")
+        if ev1 is not None:
+            ev1.record(stream)
+        _lib.check(Lib.fe_assemble_vector(L.cuda_form, bp, _lib.ASM_ZERO, sp), "load")
+
+    step()
+    torch.cuda.synchronize()
+    setup_s = time.perf_counter() - t_setup
+    for _ in range(args.warmup):
+        step()
+    dist = torch.distributed if world > 1 else None
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    time.sleep(0.3)
+    mats = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for k in range(args.steps):
+        step(*mats[k])
+    e1.record(stream)
+    torch.cuda.synchronize()
+    total_ms = e0.elapsed_time(e1)
+    mat_ms = statistics.mean(x.elapsed_time(y) for x, y in mats)
+    clk = clocks.stop()
+    total_ms, mat_ms = reduce_over_ranks([total_ms, mat_ms])
+
+    e2e = None
+    if not args.no_e2e:
+        I2 = dg_inputs(DGSYS["n"], args.seed, pinned=True)
+        c2, j2, L2 = cx.form(I2["a_cell"]), cx.form(I2["a_jump"]), cx.form(I2["L"])
+        for f in (c2, j2):
+            f._bind(A.sparsity)
+        A2 = cx.CUDAMatrix(asm._ctx, A.sparsity)
+        b2 = asm.create_vector(L2)
+        bhost = torch.empty(nrows, dtype=torch.float64, pin_memory=True)
+
+        def e2e_step():
+            asm.assemble_matrix(c2, A2)
+            asm.assemble_matrix(j2, A2, zero=False)
+            asm.assemble_vector(L2, b2)
+            bhost.copy_(b2.vector, non_blocking=True)
+
+        for _ in range(max(1, args.warmup)):
+            e2e_step()
+        torch.cuda.synchronize()
+        s0 = torch.cuda.Event(enable_timing=True)
+        s1 = torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        for _ in range(args.steps):
+            e2e_step()
+        s1.record(stream)
+        torch.cuda.synchronize()
+        (e2e_ms,) = reduce_over_ranks([s0.elapsed_time(s1)])
+        same = bool(torch.allclose(A2.values, A.values, rtol=1e-12, atol=1e-13 * float(A.values.abs().max())))
+        e2e = {"value": replica_rate(nnz, args.steps, e2e_ms, world), "unit": "nnz/s",
+               "h2d_bytes_per_step": int(I2["g"].nbytes), "d2h_bytes_per_step": int(nrows * 8),
+               "ms_per_step": e2e_ms / args.steps,
+               "path": "cudolfinx.CUDAAssembler.assemble_matrix x2 + assemble_vector (Python API -> C-ABI)",
+               "matches_device_leg": same}
+
+    C, nv, F = I["mesh"].num_cells, I["mesh"].num_vertices, len(I["facets"])
+    # values once (8/nnz); cell term: byte map 16 + dofmap 16 + geometry 16 per
+    # cell, coordinates 24 per vertex; jump term per facet: quad 16, macro dofs
+    # 32, byte map 64, both cells' geometry 32; row_ptr 4 per row per launch
+    alg = 8 * nnz + 48 * C + 24 * nv + 144 * F + 8 * (nrows + 1)
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            peaks = json.load(fh)
+    except (OSError, ValueError):
+        pass
+    peak = peaks.get("hbm_gbs", 6650.0)
+    achieved = alg / (mat_ms / 1e3) / 1e9
+    out = {
+        "metric": "matrix nnz/s (DG1 interior penalty)", "value": replica_rate(nnz, args.steps, total_ms, world),
+        "unit": "nnz/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded)",
+        "config": {"workload": DGSYS["desc"], "cells": C, "dofs": nrows, "nnz": nnz, "interior_facets": F,
+                   "step": "cell term (zero + upper-triangle scatter + mirror) + jump term + facet load",
+                   "l2": "inputs larger than L2 (values %.2f GB)" % (8 * nnz / 1e9),
+                   "parallelism": f"replicas x{world}"},
+        "roofline": {"bound": "hbm", "kernel": "cell + jump matrix assembly", "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "traffic": load_traffic("dg"),
+                     "algorithmic_bytes": alg, "kernel_ms": mat_ms,
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if "hbm_gbs" in peaks
+                     else "fallback 6650 GB/s"},
+        "matrix_nnz_per_s": nnz / (mat_ms / 1e3),
+        "gpu_launches": DGSYS_KERNELS * args.steps,
+        "clocks": clk,
+        "setup_s": setup_s,
+    }
+    if e2e:
+        out["e2e"] = e2e
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        t, nnz_s = dg_cpu_sample(DGSYS["cpu_n"], args.seed)
+        out["cpu_baseline"] = {"value": nnz_s / t, "unit": "nnz/s", "cores": 1, "kind": "port",
+                               "sample": f"the same DG1 system at n={DGSYS['cpu_n']} ({6 * DGSYS['cpu_n'] ** 3} "
+                                         f"cells, nnz {nnz_s}): element tensors + matrix + facet load with the numpy "
+                                         "oracle, one thread", "seconds_per_step": t}
+    return out
+
+
+def run_reference_dg(args):
+    t, nnz = dg_cpu_sample(DGSYS["cpu_n"], args.seed)
+    v = nnz / t
+    return {"impl": "reference", "metric": "matrix nnz/s (DG1 interior penalty)", "value": v, "unit": "nnz/s",
+            "n_gpus": 1, "steps": 1, "warmup": 0, "ms_per_step": 1e3 * t, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": {"workload": DGSYS["desc"], "sample_n": DGSYS["cpu_n"], "nnz": nnz},
+            "cpu_baseline": {"value": v, "unit": "nnz/s", "cores": 1, "kind": "port",
+                             "sample": f"n={DGSYS['cpu_n']} DG1 system, numpy oracle (the reference needs DOLFINx)"},
+            "e2e": {"value": v, "unit": "nnz/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
 def multimesh_inputs(seed: int):
     rng = np.random.default_rng(seed)
     ns = rng.integers(MULTI["nmin"], MULTI["nmax"] + 1, size=MULTI["count"])
@@ -1444,6 +1638,8 @@ def run_reference(args):
         return run_reference_blocksys(args)
     if args.workload == "interp":
         return run_reference_interp(args)
+    if args.workload == "dg":
+        return run_reference_dg(args)
     W = WORKLOADS[args.workload]
     I = make_inputs(W["kind"], W["n"], seed=args.seed)
     row_ptr, col = host_pattern(I)
@@ -1514,7 +1710,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batch", "multimesh", "serve", "blocksys", "interp"],
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batch", "multimesh", "serve", "blocksys", "interp", "dg"],
                     default="p2")
     ap.add_argument("--variant", choices=["auto", "tile", "atomic", "atomic-full", "sorted-slot", "deterministic",
                                           "row-gather",
@@ -1549,7 +1745,8 @@ def main():
                                 device_id=torch.device("cuda", local_rank))
     try:
         runner = {"batch": run_gpu_batch, "multimesh": run_gpu_multimesh, "serve": run_gpu_serve,
-                  "blocksys": run_gpu_blocksys, "interp": run_gpu_interp}.get(args.workload, run_gpu)
+                  "blocksys": run_gpu_blocksys, "interp": run_gpu_interp,
+                  "dg": run_gpu_dg}.get(args.workload, run_gpu)
         out = runner(args, rank, world, local_rank)
         if rank == 0:
             print(json.dumps(out), flush=True)
