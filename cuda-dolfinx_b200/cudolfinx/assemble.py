@@ -168,9 +168,10 @@ class CUDAAssembler:
         self.pack_coefficients(a, coeffs)
         flags = ((_lib.ASM_ZERO if zero else 0) | (_lib.ASM_DETERMINISTIC if deterministic else 0)
                  | _lib.VARIANT_FLAGS[variant])
-        _lib.check(_lib.lib.fe_assemble_matrix(a.cuda_form, mat.values.data_ptr(), bc0.handle if bc0 else None,
+        _lib.check(_lib.lib.fe_assemble_matrix(a._handle, mat.values.data_ptr(), bc0.handle if bc0 else None,
                                                bc1.handle if bc1 else None, float(diagonal), flags,
                                                self._ctx.stream()), "fe_assemble_matrix")
+        a._mark_used()
         mat._bcs = col  # keep device BC data alive while the work is queued
         return mat
 
@@ -264,14 +265,16 @@ class CUDAAssembler:
         _coeffs = [None] * n if coeffs is None else coeffs
         if len(_coeffs) != n:
             raise ValueError(f"Expected coeffs to be None or a list of length: '{n}', got '{len(_coeffs)}' instead!")
+        vec._before_write()
         if zero:
             vec.vector.zero_()
         base = vec.vector.data_ptr()
         for f, off, c in zip(b.forms, b.offsets, _coeffs):
             f.to_device()
             self.pack_coefficients(f, c)
-            _lib.check(_lib.lib.fe_assemble_vector(f.cuda_form, base + 8 * off, 0, self._ctx.stream()),
+            _lib.check(_lib.lib.fe_assemble_vector(f._handle, base + 8 * off, 0, self._ctx.stream()),
                        "fe_assemble_vector")
+            f._mark_used()
         return vec
 
     def assemble_scalar(self, b: CUDAForm, constants=None, coeffs=None) -> float:
@@ -285,8 +288,9 @@ class CUDAAssembler:
         b.to_device()  # assemble.py:220-222
         self.pack_coefficients(b, coeffs)
         out = ctypes.c_double(0.0)
-        _lib.check(_lib.lib.fe_assemble_scalar(b.cuda_form, ctypes.byref(out), self._ctx.stream()),
+        _lib.check(_lib.lib.fe_assemble_scalar(b._handle, ctypes.byref(out), self._ctx.stream()),
                    "fe_assemble_scalar")
+        b._mark_used()
         return out.value
 
     def assemble_vector(self, b: CUDAForm, vec: typing.Optional[CUDAVector] = None, constants=None, coeffs=None,
@@ -298,8 +302,10 @@ class CUDAAssembler:
             vec = self.create_vector(b)
         b.to_device()  # assemble.py:156-158
         self.pack_coefficients(b, coeffs)
-        _lib.check(_lib.lib.fe_assemble_vector(b.cuda_form, vec.vector.data_ptr(), _lib.ASM_ZERO if zero else 0,
+        vec._before_write()
+        _lib.check(_lib.lib.fe_assemble_vector(b._handle, vec.vector.data_ptr(), _lib.ASM_ZERO if zero else 0,
                                                self._ctx.stream()), "fe_assemble_vector")
+        b._mark_used()
         return vec
 
     def apply_lifting(self, b: CUDAVector, a: list[CUDAForm], bcs: list, x0: typing.Optional[list] = None,
@@ -324,11 +330,14 @@ class CUDAAssembler:
             col = self._bc_collection(bc)
             keep.append(col)
             d = col._get_cpp_bcs(f.function_spaces[1], f.restriction(1))
-            forms[i] = f.cuda_form
+            forms[i] = f._handle
             hbcs[i] = d.handle if d else None
             hx0[i] = x0[i].vector.data_ptr() if (x0 is not None and x0[i] is not None) else None
+        b._before_write()
         _lib.check(_lib.lib.fe_apply_lifting(b.vector.data_ptr(), n, forms, hbcs, hx0 if x0 is not None else None,
                                              float(scale), self._ctx.stream()), "fe_apply_lifting")
+        for f in a:
+            f._mark_used()
         b._keep = keep
 
     def set_bc(self, b: CUDAVector, bcs, V: FunctionSpace, x0: typing.Optional[CUDAVector] = None,
@@ -339,6 +348,7 @@ class CUDAAssembler:
         d = col._get_cpp_bcs(V, restriction)
         if d is None:
             return
+        b._before_write()
         _lib.check(_lib.lib.fe_set_bc(b.vector.data_ptr(), b.size, d.handle,
                                       x0.vector.data_ptr() if x0 is not None else None, float(scale),
                                       self._ctx.stream()), "fe_set_bc")
@@ -351,6 +361,7 @@ class CUDAAssembler:
         import ctypes
         if x is None:
             x = CUDAVector(self._ctx, b.size)
+        x._before_write()
         it, res = ctypes.c_int(0), ctypes.c_double(0.0)
         st = _lib.lib.fe_pcg_solve(A.sparsity.handle, A.values.data_ptr(), b.vector.data_ptr(), x.vector.data_ptr(),
                                    float(rtol), int(max_iter), ctypes.byref(it), ctypes.byref(res), self._ctx.stream())

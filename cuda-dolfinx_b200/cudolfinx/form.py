@@ -13,6 +13,7 @@ import ctypes
 import typing
 
 import numpy as np
+import torch
 
 from . import _lib
 from .context import get_cuda_context
@@ -144,6 +145,8 @@ class CUDAForm:
             _lib.check(_lib.lib.fe_form_set_precision(self._handle, _lib.PREC_FP32), "fe_form_set_precision")
         self._bound_sparsity = None
         self._coef_refs: list = [None] * len(form.coefficients)
+        self._coef_free: list = [None] * len(form.coefficients)  # event after the last tracked read
+        self._external = getattr(self, "_external", False)
         self._aux_dofmaps: dict = {}
         self.to_device()
 
@@ -195,17 +198,14 @@ class CUDAForm:
             else:
                 raise ValueError("coefficients must be constants, DG0 or scalar P1 Functions")
             self._coef_refs[i] = vals
-            _lib.check(_lib.lib.fe_form_set_coefficient(self._handle, i, kind, cmap.handle if cmap else None,
-                                                        vals.ctypes.data, len(vals), 0, ctx.stream()),
-                       "fe_form_set_coefficient")
-            return
+            return self._upload(i, kind, cmap.handle if cmap else None, vals)
         if hasattr(c, "data_ptr"):  # device tensor: DG0 values read in place
             if c.numel() != C * ncomp:
                 raise ValueError("device coefficient arrays must hold one value per cell (DG0)")
             self._coef_refs[i] = c
             _lib.check(_lib.lib.fe_form_set_coefficient(self._handle, i, _lib.COEFF_DG0, None, c.data_ptr(),
                                                         c.numel(), 1, ctx.stream()), "fe_form_set_coefficient")
-            return
+            return None
         arr = np.atleast_1d(np.asarray(c, dtype=np.float64)).ravel()
         if arr.size == ncomp:
             kind = _lib.COEFF_CONSTANT
@@ -216,15 +216,49 @@ class CUDAForm:
                              f"{C * ncomp} (DG0) values")
         arr = np.ascontiguousarray(arr)
         self._coef_refs[i] = arr
-        _lib.check(_lib.lib.fe_form_set_coefficient(self._handle, i, kind, None, arr.ctypes.data, arr.size, 0,
-                                                    ctx.stream()), "fe_form_set_coefficient")
+        if kind == _lib.COEFF_CONSTANT:
+            _lib.check(_lib.lib.fe_form_set_coefficient(self._handle, i, kind, None, arr.ctypes.data, arr.size, 0,
+                                                        ctx.stream()), "fe_form_set_coefficient")
+            return None
+        return self._upload(i, kind, None, arr)
+
+    def _upload(self, i: int, kind: int, cmap, arr: np.ndarray):
+        """Host -> device copy of coefficient i on the context's upload stream.
+        It waits only for the last tracked kernel that read the same device
+        buffer (so it overlaps other work still running on the compute stream),
+        or for all work queued on the current stream when that is unknown."""
+        ctx = self._ctx
+        up = ctx.upload_stream()
+        free = self._coef_free[i]
+        if self._external or free is None:
+            up.wait_stream(ctx.torch_stream())
+        else:
+            up.wait_event(free)
+        _lib.check(_lib.lib.fe_form_set_coefficient(self._handle, i, kind, cmap, arr.ctypes.data, arr.size, 0,
+                                                    up.cuda_stream), "fe_form_set_coefficient")
+        ev = torch.cuda.Event()
+        ev.record(up)
+        return ev
 
     def to_device(self, coefficients: typing.Optional[list] = None):
         """Copy host-side coefficient values to the device (CUDAForm.h:195-199).
-        With ``coefficients`` given, only those Functions are re-uploaded."""
+        With ``coefficients`` given, only those Functions are re-uploaded.  The
+        copies run on the context's upload stream; work enqueued afterwards on
+        the current stream waits for them."""
+        cur = self._ctx.torch_stream()
         for i, c in enumerate(self._spec.coefficients):
             if coefficients is None or any(c is q for q in coefficients):
-                self._set_coefficient(i, c)
+                ev = self._set_coefficient(i, c)
+                if ev is not None:
+                    cur.wait_event(ev)
+
+    def _mark_used(self):
+        """Record that the kernels enqueued so far on the current stream read
+        this form's coefficient buffers (the next upload into them waits)."""
+        ev = torch.cuda.Event()
+        ev.record(self._ctx.torch_stream())
+        for i in range(len(self._coef_free)):
+            self._coef_free[i] = ev
 
     # -- pattern binding ----------------------------------------------------
     def _bind(self, sparsity):
@@ -246,6 +280,10 @@ class CUDAForm:
     # -- properties mirroring the reference --------------------------------
     @property
     def cuda_form(self):
+        """The engine form handle, for direct C-ABI calls.  Once handed out,
+        coefficient uploads wait for everything queued on the current stream
+        (kernels launched through the handle are not tracked)."""
+        self._external = True
         return self._handle
 
     @property

@@ -64,7 +64,7 @@ class Sparsity:
         their cell / interior-facet couplings (create_sparsity_pattern of a
         form with several integrals)."""
         n = len(forms)
-        tab = (ctypes.c_void_p * n)(*[f.cuda_form for f in forms])
+        tab = (ctypes.c_void_p * n)(*[f._handle for f in forms])
         h = _lib.out_handle()
         _lib.check(_lib.lib.fe_sparsity_build_forms(n, tab, h), "fe_sparsity_build_forms")
         return cls(ctx, h.value)
@@ -119,6 +119,33 @@ class CUDAVector:
         self.size = n
         self._values = values if values is not None else torch.zeros(n, dtype=torch.float64,
                                                                       device=ctx.torch_device)
+        self._read_done = None  # event of a pending copy_to_host
+
+    def copy_to_host(self, out: torch.Tensor | None = None) -> torch.Tensor:
+        """Asynchronous device -> host copy into `out` (a pinned CPU float64
+        tensor of `size` values; allocated pinned when None), on the context's
+        download stream once the work already queued on the current stream is
+        done; it overlaps work queued afterwards.  The assembler's next writes
+        into this vector wait for it; synchronise before reading `out` (e.g.
+        torch.cuda.synchronize()), and order other writes to ``vector`` after
+        ctx.join_transfers()."""
+        if out is None:
+            out = torch.empty(self.size, dtype=torch.float64, pin_memory=True)
+        dn = self._ctx.download_stream()
+        dn.wait_stream(self._ctx.torch_stream())
+        with torch.cuda.stream(dn):
+            out.copy_(self._values, non_blocking=True)
+        self._values.record_stream(dn)
+        ev = torch.cuda.Event()
+        ev.record(dn)
+        self._read_done = ev
+        return out
+
+    def _before_write(self):
+        """Order a write on the current stream after a pending copy_to_host."""
+        if self._read_done is not None:
+            self._ctx.torch_stream().wait_event(self._read_done)
+            self._read_done = None
 
     @property
     def vector(self) -> torch.Tensor:
@@ -131,6 +158,7 @@ class CUDAVector:
 
     def to_host(self) -> np.ndarray:
         """Copy device values to a host array (CUDAVector::copy_vector_values_to_host)."""
+        self._ctx.join_transfers()
         torch.cuda.current_stream(self._ctx.device).synchronize()
         return self._values.cpu().numpy()
 
