@@ -56,6 +56,9 @@ WORKLOADS = {
                   desc="P1 Poisson n=128: 12,582,912 tets, k=1, f=P1(sin sin sin), homogeneous Dirichlet"),
     "vp2": dict(kind="vp2", n=64, precision="fp32",
                 desc="vector-P2 elasticity n=64: 1,572,864 jittered tets, lam/mu DG0, FP32 element tensors"),
+    "vp2mid": dict(kind="vp2", n=32, precision="fp32",
+                   desc="vector-P2 elasticity n=32 (profiling size): 196,608 jittered tets, lam/mu DG0, FP32 element "
+                        "tensors"),
     "p3": dict(kind="p3", n=48, precision="fp64",
                desc="equispaced P3 Poisson n=48: 663,552 tets, 3,048,625 dofs, k DG0 lognormal, f DG0 U[-1,1], "
                     "g=x+y+z"),

@@ -20,6 +20,10 @@ from .context import get_cuda_context
 from .fem import FormSpec, Function, FunctionSpace
 
 DEFAULT_CUDA_JIT_ARGS = {"max_threads_per_block": 1024, "min_blocks_per_multiprocessor": 1}
+# transfers of at least this size run on the context's side streams (below it
+# on the current stream: for a few hundred kB the extra event round trip costs
+# more than the overlap gains)
+OVERLAP_MIN_BYTES = 1 << 20
 
 _mesh_cache: dict[int, "DeviceMesh"] = {}
 _dofmap_cache: dict[int, "DeviceDofMap"] = {}
@@ -228,6 +232,12 @@ class CUDAForm:
         buffer (so it overlaps other work still running on the compute stream),
         or for all work queued on the current stream when that is unknown."""
         ctx = self._ctx
+        if arr.nbytes < OVERLAP_MIN_BYTES:
+            # small copies: the event round trip would cost more than the overlap
+            _lib.check(_lib.lib.fe_form_set_coefficient(self._handle, i, kind, cmap, arr.ctypes.data, arr.size, 0,
+                                                        ctx.stream()), "fe_form_set_coefficient")
+            return None
+        self._overlapped = True
         up = ctx.upload_stream()
         free = self._coef_free[i]
         if self._external or free is None:
@@ -254,7 +264,10 @@ class CUDAForm:
 
     def _mark_used(self):
         """Record that the kernels enqueued so far on the current stream read
-        this form's coefficient buffers (the next upload into them waits)."""
+        this form's coefficient buffers (the next upload into them waits).
+        Only forms with side-stream uploads need it."""
+        if not getattr(self, "_overlapped", False):
+            return
         ev = torch.cuda.Event()
         ev.record(self._ctx.torch_stream())
         for i in range(len(self._coef_free)):

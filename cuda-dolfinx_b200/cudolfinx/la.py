@@ -131,6 +131,11 @@ class CUDAVector:
         ctx.join_transfers()."""
         if out is None:
             out = torch.empty(self.size, dtype=torch.float64, pin_memory=True)
+        if 8 * self.size < (1 << 20):
+            # small vectors: on the current stream (an event round trip would
+            # cost more than the overlap)
+            out.copy_(self._values, non_blocking=True)
+            return out
         dn = self._ctx.download_stream()
         dn.wait_stream(self._ctx.torch_stream())
         with torch.cuda.stream(dn):
