@@ -889,7 +889,7 @@ int fe_assemble_matrix(fe_form a, double* values, fe_bc bc0, fe_bc bc1, double d
     const bool upper = zero && !view && !(flags & FE_ASM_FULL_SCATTER) &&
                        (a->kind == FE_FORM_VP2_ELASTICITY || a->kind == FE_FORM_P3_STIFFNESS ||
                         a->kind == FE_FORM_P1_STIFFNESS) && a->V0 == a->V1 &&
-                       bc0 == bc1 && ensure_mirror(*a->sp, st);
+                       bc0 == bc1 && ensure_mirror(*a->sp, st, a->V0->bs);
     if (zero) launch_zero(values, a->sp->nnz, st);
     MatLaunch L{};
     L.kind = a->kind;

@@ -117,6 +117,12 @@ struct fe_sparsity_s {
   struct Mirror {
     fe::DevBuf<int2> pairs;         // [lower slots]
     int64_t nlower = 0;
+    // block size 3 (vector P2): one record per node block on or below the
+    // block diagonal, {lower base, lower row length, upper base, upper row
+    // length}; a diagonal block has upper base == lower base
+    int bs = 1;
+    fe::DevBuf<int4> blocks;
+    int64_t nblocks = 0;
     bool ok = false;                // pattern symmetric with every diagonal present
   };
   std::unique_ptr<Mirror> mirror;
@@ -293,7 +299,7 @@ struct MatLaunch {
 void launch_zero(double* v, int64_t n, cudaStream_t s);
 // symmetric-pattern transpose map (built once per pattern); false if the
 // pattern is not symmetric or lacks a diagonal entry
-bool ensure_mirror(fe_sparsity_s& sp, cudaStream_t s);
+bool ensure_mirror(fe_sparsity_s& sp, cudaStream_t s, int bs = 1);
 // values[lower slot] = values[its transpose] for every strictly-lower slot
 void launch_mirror_lower(const fe_sparsity_s& sp, double* values, cudaStream_t s);
 void launch_build_slotmap(const fe_form_s& f, cudaStream_t s);

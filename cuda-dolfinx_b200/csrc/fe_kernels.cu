@@ -492,6 +492,97 @@ __global__ void __launch_bounds__(256) k_mirror_pairs(const int2* __restrict__ p
   }
 }
 
+// Block size 3: per block row I, the number of node blocks on or below the
+// diagonal (block position of column 3I in row 3I, plus one); -1 if the three
+// rows of the block row differ in length or the diagonal is missing.
+__global__ void k_lower_count3(const int32_t* __restrict__ row_ptr, const int32_t* __restrict__ diag,
+                               int64_t num_block_rows, int32_t* __restrict__ cnt) {
+  const int64_t I = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (I >= num_block_rows) return;
+  const int64_t r = 3 * I;
+  const int32_t lo = row_ptr[r], len = row_ptr[r + 1] - lo;
+  const int32_t d = diag[r];
+  const bool same = row_ptr[r + 2] - row_ptr[r + 1] == len && row_ptr[r + 3] - row_ptr[r + 2] == len;
+  cnt[I] = (d < 0 || !same || len % 3 || (d - lo) % 3) ? -1 : (d - lo) / 3 + 1;
+}
+
+// One record per node block (I, J), J <= I: {slot of (3I, 3J), row length of
+// 3I, slot of (3J, 3I), row length of 3J}; the transposed block is found by a
+// binary search in row 3J, a missing one sets *bad.
+__global__ void k_lower_blocks3(const int32_t* __restrict__ row_ptr, const int32_t* __restrict__ col,
+                                const int32_t* __restrict__ lower_ptr, int64_t num_block_rows,
+                                int4* __restrict__ blocks, int* __restrict__ bad) {
+  const int64_t I = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (I >= num_block_rows) return;
+  const int64_t r = 3 * I;
+  const int32_t lo = row_ptr[r], len = row_ptr[r + 1] - lo;
+  const int32_t base = lower_ptr[I], n = lower_ptr[I + 1] - base;
+  for (int32_t t = 0; t < n; ++t) {
+    const int32_t l0 = lo + 3 * t;
+    const int32_t c = col[l0];
+    // the block's three columns are c, c+1, c+2 (l0 + 2 is inside the row: t
+    // is at most the diagonal block's position and the row length is a
+    // multiple of 3)
+    if (c % 3 || col[l0 + 1] != c + 1 || col[l0 + 2] != c + 2) {
+      atomicOr(bad, 1);
+      blocks[base + t] = make_int4(l0, len, l0, len);
+      continue;
+    }
+    if (t == n - 1) {  // the diagonal block
+      blocks[base + t] = make_int4(l0, len, l0, len);
+      continue;
+    }
+    const int64_t rj = c;  // row 3J
+    int32_t a = row_ptr[rj], b = row_ptr[rj + 1] - 1, hit = -1;
+    while (a <= b) {
+      const int32_t m = (a + b) >> 1;
+      const int32_t v = col[m];
+      if (v == (int32_t)r) {
+        hit = m;
+        break;
+      }
+      if (v < (int32_t)r) a = m + 1;
+      else b = m - 1;
+    }
+    const int32_t lenj = row_ptr[rj + 1] - row_ptr[rj];
+    if (hit < 0 || hit + 2 >= row_ptr[rj + 1] || col[hit + 1] != (int32_t)r + 1 || col[hit + 2] != (int32_t)r + 2) {
+      atomicOr(bad, 1);
+      blocks[base + t] = make_int4(l0, len, l0, len);  // harmless diagonal-style record
+      continue;
+    }
+    blocks[base + t] = make_int4(l0, len, hit, lenj);
+  }
+}
+
+// Strictly-lower part from the upper part, node block by node block (block
+// size 3): the 9 entries of a block below the diagonal are 3 rows of 3
+// contiguous slots, read from the transposed block's 3 rows of 3 contiguous
+// slots; a diagonal block copies its 3 entries below the diagonal.  One
+// 16-byte record per block replaces nine 8-byte slot pairs.
+__global__ void __launch_bounds__(256) k_mirror_blocks3(const int4* __restrict__ blocks, int64_t n,
+                                                        double* __restrict__ values) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += stride) {
+    const int4 b = __ldg(blocks + k);
+    if (b.z == b.x) {
+      const double v10 = values[b.x + 1], v20 = values[b.x + 2], v21 = values[b.x + b.y + 2];
+      values[b.x + b.y] = v10;
+      values[b.x + 2 * b.y] = v20;
+      values[b.x + 2 * b.y + 1] = v21;
+      continue;
+    }
+    double v[3][3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int a = 0; a < 3; ++a) v[c][a] = values[b.z + c * b.w + a];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) values[b.x + a * b.y + c] = v[c][a];
+  }
+}
+
 // Cell-to-slot map: block position of dofs1[c,j] inside block row dofs0[c,i].
 __global__ void k_build_slotmap(const int32_t* __restrict__ dofs0, const int32_t* __restrict__ dofs1,
                                 int64_t num_cells, int k0, int k1, int bs0, int bs1,
@@ -979,13 +1070,54 @@ void launch_matrix_atomic(const MatLaunch& L, cudaStream_t s) {
   FE_CUDA(cudaGetLastError());
 }
 
-bool ensure_mirror(fe_sparsity_s& sp, cudaStream_t s) {
-  if (sp.mirror) return sp.mirror->ok;
+namespace {
+// node-block mirror of a block-size-3 pattern; false if the pattern is not
+// block-structured or not symmetric
+bool build_mirror3(fe_sparsity_s& sp, fe_sparsity_s::Mirror& M, cudaStream_t s) {
+  const int64_t NB = sp.num_rows / 3;
+  DevBuf<int32_t> cnt(NB);
+  k_lower_count3<<<grid_for(NB, 256), 256, 0, s>>>(sp.row_ptr.p, sp.diag.p, NB, cnt.p);
+  FE_CUDA(cudaGetLastError());
+  std::vector<int32_t> h(NB);
+  FE_CUDA(cudaMemcpyAsync(h.data(), cnt.p, NB * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  FE_CUDA(cudaStreamSynchronize(s));
+  std::vector<int32_t> lp(NB + 1, 0);
+  int64_t tot = 0;
+  for (int64_t I = 0; I < NB; ++I) {
+    if (h[I] < 0) return false;
+    tot += h[I];
+    if (tot > INT32_MAX) return false;
+    lp[I + 1] = (int32_t)tot;
+  }
+  M.nblocks = tot;
+  M.blocks.alloc(std::max<int64_t>(1, tot));
+  DevBuf<int32_t> lower_ptr(NB + 1);
+  FE_CUDA(cudaMemcpyAsync(lower_ptr.p, lp.data(), (NB + 1) * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+  DevBuf<int> bad(1);
+  FE_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(int), s));
+  k_lower_blocks3<<<grid_for(NB, 128), 128, 0, s>>>(sp.row_ptr.p, sp.col.p, lower_ptr.p, NB, M.blocks.p, bad.p);
+  FE_CUDA(cudaGetLastError());
+  int hb = 0;
+  FE_CUDA(cudaMemcpyAsync(&hb, bad.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+  FE_CUDA(cudaStreamSynchronize(s));  // lower_ptr and bad are freed on return
+  return hb == 0;
+}
+}  // namespace
+
+bool ensure_mirror(fe_sparsity_s& sp, cudaStream_t s, int bs) {
+  if (sp.mirror && sp.mirror->bs == bs) return sp.mirror->ok;
   auto M = std::make_unique<fe_sparsity_s::Mirror>();
+  M->bs = bs;
   const int64_t R = sp.num_rows;
-  if (R == 0 || sp.num_rows != sp.num_cols) {
+  if (R == 0 || sp.num_rows != sp.num_cols || (bs == 3 && R % 3)) {
     sp.mirror = std::move(M);
     return false;
+  }
+  if (bs == 3) {
+    M->ok = build_mirror3(sp, *M, s);
+    if (!M->ok) M->blocks.release();
+    sp.mirror = std::move(M);
+    return sp.mirror->ok;
   }
   DevBuf<int32_t> cnt(R);
   k_lower_count<<<grid_for(R, 256), 256, 0, s>>>(sp.row_ptr.p, sp.diag.p, R, cnt.p);
@@ -1024,10 +1156,18 @@ bool ensure_mirror(fe_sparsity_s& sp, cudaStream_t s) {
 
 void launch_mirror_lower(const fe_sparsity_s& sp, double* values, cudaStream_t s) {
   const auto& M = *sp.mirror;
-  if (!M.ok || M.nlower == 0) return;
+  if (!M.ok) return;
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (M.bs == 3) {
+    if (M.nblocks == 0) return;
+    const unsigned g3 = (unsigned)std::min<int64_t>((M.nblocks + 255) / 256, (int64_t)sms * 16);
+    k_mirror_blocks3<<<g3, 256, 0, s>>>(M.blocks.p, M.nblocks, values);
+    FE_CUDA(cudaGetLastError());
+    return;
+  }
+  if (M.nlower == 0) return;
   const unsigned grid =
       (unsigned)std::min<int64_t>((M.nlower + 256 * kMirrorUnroll - 1) / (256 * kMirrorUnroll), (int64_t)sms * 16);
   k_mirror_pairs<<<grid, 256, 0, s>>>(M.pairs.p, M.nlower, values);
