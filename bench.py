@@ -371,17 +371,18 @@ def run_gpu(args, rank, world, local_rank):
     Lib = _lib.lib
     Ap, bp = A.values.data_ptr(), b.vector.data_ptr()
 
-    def step(ev0=None, ev1=None):
+    def step(ev0=None, ev1=None, st=None):
         # the matrix call owns its zeroing: a zero pass before the atomic
         # scatter, none for the gather variants (they write every value once)
+        h = sp if st is None else st
         if ev0 is not None:
             ev0.record(stream)
-        _lib.check(Lib.fe_assemble_matrix(a.cuda_form, Ap, hbc, hbc, 1.0, flags, sp), "matrix")
+        _lib.check(Lib.fe_assemble_matrix(a.cuda_form, Ap, hbc, hbc, 1.0, flags, h), "matrix")
         if ev1 is not None:
             ev1.record(stream)
-        _lib.check(Lib.fe_assemble_vector(L.cuda_form, bp, _lib.ASM_ZERO, sp), "vector")
-        _lib.check(Lib.fe_apply_lifting(bp, 1, forms, bcs1, None, 1.0, sp), "lifting")
-        _lib.check(Lib.fe_set_bc(bp, nrows, hbc, None, 1.0, sp), "set_bc")
+        _lib.check(Lib.fe_assemble_vector(L.cuda_form, bp, _lib.ASM_ZERO, h), "vector")
+        _lib.check(Lib.fe_apply_lifting(bp, 1, forms, bcs1, None, 1.0, h), "lifting")
+        _lib.check(Lib.fe_set_bc(bp, nrows, hbc, None, 1.0, h), "set_bc")
 
     step()  # plan build (deterministic), lift-cell list
     torch.cuda.synchronize()
@@ -398,13 +399,38 @@ def run_gpu(args, rank, world, local_rank):
     e_start = torch.cuda.Event(enable_timing=True)
     e_end = torch.cuda.Event(enable_timing=True)
     mats = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    e_start.record(stream)
+    # matrix-call time (roofline basis): eager steps with events around the call
     for k in range(args.steps):
         step(*mats[k])
+    torch.cuda.synchronize()
+    mat_ms = statistics.mean(m0.elapsed_time(m1) for m0, m1 in mats)
+    # whole steps: the step's engine calls captured once in a CUDA graph and
+    # replayed (every plan and cache exists after the warm-up, so the calls
+    # are pure kernel launches); eager steps if the capture is refused
+    graph = None
+    if not args.no_graph:
+        try:
+            graph = torch.cuda.CUDAGraph()
+            cs = torch.cuda.Stream()
+            cs.wait_stream(stream)
+            with torch.cuda.graph(graph, stream=cs):
+                step(st=cs.cuda_stream)
+            stream.wait_stream(cs)
+            graph.replay()
+            torch.cuda.synchronize()
+        except Exception as exc:  # noqa: BLE001 - report and fall back to eager steps
+            graph = None
+            print(f"graph capture refused ({exc}); timing eager steps", file=sys.stderr)
+            torch.cuda.synchronize()
+    e_start.record(stream)
+    for k in range(args.steps):
+        if graph is not None:
+            graph.replay()
+        else:
+            step()
     e_end.record(stream)
     torch.cuda.synchronize()
     total_ms = e_start.elapsed_time(e_end)
-    mat_ms = statistics.mean(m0.elapsed_time(m1) for m0, m1 in mats)
     clk = clocks.stop()
     total_ms, mat_ms = reduce_over_ranks([total_ms, mat_ms])
     ms_per_step = total_ms / args.steps
@@ -478,6 +504,7 @@ def run_gpu(args, rank, world, local_rank):
         "data": "synthetic (seeded numpy inputs with the configuration's shapes and distributions)",
         "config": {"workload": W["desc"], "cells": len(I["cells"]), "dofs": nrows, "nnz": nnz,
                    "step": "zero A + assemble A (BC skip, unit diagonal) + assemble b + lifting + set_bc",
+                   "timing": "replays of the step captured in a CUDA graph" if graph is not None else "eager steps",
                    "variant": args.variant, "l2": "inputs larger than L2 (CSR values %.2f GB)" % (8 * nnz / 1e9),
                    "parallelism": f"replicas x{world}"},
         "roofline": {"bound": "hbm", "kernel": "matrix assembly (%s)" % args.variant,
@@ -1728,6 +1755,7 @@ def main():
     ap.add_argument("--instances", type=int, default=0,
                     help="batch workload: number of instances (default 256; smaller for profiling)")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-graph", action="store_true", help="time eager steps instead of replaying a CUDA graph")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-precision", action="store_true", help="skip the FP32-vs-FP64 precision report")
     ap.add_argument("--precision-rtol", type=float, default=1e-10,
