@@ -1531,6 +1531,8 @@ def run_gpu_serve(args, rank, world, local_rank):
     seed = args.seed + 7919 * rank
     t_setup = time.perf_counter()
     base = serve.make_requests(count, rates[0], seed=seed, nmin=SERVE["nmin"], nmax=nmax)
+    if args.serve_workers:
+        SERVE["workers"] = args.serve_workers
     srv = serve.Server(workers=SERVE["workers"], hbm_budget=SERVE["budget_gb"] << 30, precision="fp32")
     keys = sorted({r.key for r in base})
     srv.warm(keys)
@@ -1759,6 +1761,7 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=0, help="serve workload: requests per rate")
     ap.add_argument("--serve-rates", default="", help="serve workload: comma-separated arrival rates (req/s)")
     ap.add_argument("--serve-nmax", type=int, default=0, help="serve workload: largest n (default 48)")
+    ap.add_argument("--serve-workers", type=int, default=0, help="serve workload: worker streams (default 4)")
     ap.add_argument("--instances", type=int, default=0,
                     help="batch workload: number of instances (default 256; smaller for profiling)")
     ap.add_argument("--no-e2e", action="store_true")
