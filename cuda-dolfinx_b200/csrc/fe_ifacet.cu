@@ -15,6 +15,8 @@
 // scatters through a per-facet byte map of the macro couplings.
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include "fe_internal.h"
 
 namespace fe {
@@ -85,26 +87,31 @@ __device__ bool shared_facet(const IFArgs& a, int4 q, double& area, int loc0[3],
   return true;
 }
 
-// Calls emit(I, J, value) for the nonzero entries of the macro jump tensor
-// (I, J < 2K; K = 1 for DG0, 4 for DG1).
-template <int K, typename Emit>
-__device__ __forceinline__ void jump_tensor(double s, const int loc0[3], const int loc1[3], Emit&& emit) {
+// The jump tensor entry (I, J) of the macro dofs, written for compile-time I
+// and J: fp[I] is the facet vertex that macro dof I sits on (-1 for the
+// vertex opposite the facet; DG0: 0 for both cells), the sign is + for cell0's
+// dofs and - for cell1's.  Keeping every index compile-time keeps the
+// per-facet arrays in registers.
+template <int K, int I, int J>
+__device__ __forceinline__ double jump_entry(double s, const int fp[2 * K]) {
+  constexpr double sign = ((I < K) == (J < K)) ? 1.0 : -1.0;
   if constexpr (K == 1) {
-    emit(0, 0, s);
-    emit(0, 1, -s);
-    emit(1, 0, -s);
-    emit(1, 1, s);
+    return sign * s;
   } else {
-#pragma unroll
-    for (int p = 0; p < 3; ++p)
-#pragma unroll
-      for (int r = 0; r < 3; ++r) {
-        const double m = s * (p == r ? (2.0 / 12.0) : (1.0 / 12.0));
-        emit(loc0[p], loc0[r], m);
-        emit(loc0[p], K + loc1[r], -m);
-        emit(K + loc1[p], loc0[r], -m);
-        emit(K + loc1[p], K + loc1[r], m);
-      }
+    if (fp[I] < 0 || fp[J] < 0) return 0.0;
+    return sign * s * (fp[I] == fp[J] ? (2.0 / 12.0) : (1.0 / 12.0));
+  }
+}
+
+template <int K, int I, int J, typename F>
+__device__ __forceinline__ void for_each_entry(F&& f) {
+  if constexpr (I < 2 * K) {
+    if constexpr (J < 2 * K) {
+      f(std::integral_constant<int, I>{}, std::integral_constant<int, J>{});
+      for_each_entry<K, I, J + 1>(f);
+    } else {
+      for_each_entry<K, I + 1, 0>(f);
+    }
   }
 }
 
@@ -118,6 +125,19 @@ __global__ void __launch_bounds__(128) k_ifacet_jump(const IFArgs a) {
   int loc0[3], loc1[3];
   if (!shared_facet(a, q, area, loc0, loc1)) return;
   const double s = area * facet_coef(a, q);
+  // facet vertex of each macro dof
+  int fp[M];
+#pragma unroll
+  for (int I = 0; I < M; ++I) fp[I] = K == 1 ? 0 : -1;
+  if constexpr (K == 4) {
+#pragma unroll
+    for (int v = 0; v < 4; ++v)
+#pragma unroll
+      for (int p = 0; p < 3; ++p) {
+        if (loc0[p] == v) fp[v] = p;
+        if (loc1[p] == v) fp[K + v] = p;
+      }
+  }
   int rp[M];
   unsigned mr = 0, mc = 0;
 #pragma unroll
@@ -129,8 +149,10 @@ __global__ void __launch_bounds__(128) k_ifacet_jump(const IFArgs a) {
   }
   const uint8_t* p = a.pos + t * (M * M);
   double* __restrict__ vals = a.values;
-  jump_tensor<K>(s, loc0, loc1, [&](int I, int J, double v) {
-    if (!(((mr >> I) | (mc >> J)) & 1u)) atomicAdd(vals + rp[I] + __ldg(p + I * M + J), v);
+  for_each_entry<K, 0, 0>([&](auto ic, auto jc) {
+    constexpr int I = decltype(ic)::value, J = decltype(jc)::value;
+    const double v = jump_entry<K, I, J>(s, fp);
+    if (v != 0.0 && !(((mr >> I) | (mc >> J)) & 1u)) atomicAdd(vals + rp[I] + __ldg(p + I * M + J), v);
   });
 }
 
@@ -155,7 +177,22 @@ __global__ void __launch_bounds__(128) k_ifacet_lift(const IFArgs a) {
   int loc0[3], loc1[3];
   if (!shared_facet(a, q, area, loc0, loc1)) return;
   const double s = area * facet_coef(a, q);
-  jump_tensor<K>(s, loc0, loc1, [&](int I, int J, double v) { be[I] += v * dv[J]; });
+  int fp[M];
+#pragma unroll
+  for (int I = 0; I < M; ++I) fp[I] = K == 1 ? 0 : -1;
+  if constexpr (K == 4) {
+#pragma unroll
+    for (int v = 0; v < 4; ++v)
+#pragma unroll
+      for (int p = 0; p < 3; ++p) {
+        if (loc0[p] == v) fp[v] = p;
+        if (loc1[p] == v) fp[K + v] = p;
+      }
+  }
+  for_each_entry<K, 0, 0>([&](auto ic, auto jc) {
+    constexpr int I = decltype(ic)::value, J = decltype(jc)::value;
+    be[I] += jump_entry<K, I, J>(s, fp) * dv[J];
+  });
 #pragma unroll
   for (int I = 0; I < M; ++I) {
     const int64_t r = __ldg(a.macro0 + t * M + I);
