@@ -988,6 +988,37 @@ int fe_assemble_vector(fe_form Lf, double* b, unsigned flags, void* stream) {
   });
 }
 
+int fe_assemble_diagonal(fe_form a, double* b, unsigned flags, void* stream) {
+  return guard([&] {
+    FE_REQUIRE(a, "null form");
+    FE_REQUIRE(a->rank == 2, "the diagonal is taken of a bilinear form");
+    FE_REQUIRE(a->V0 && a->V1 && a->V0->num_blocks == a->V1->num_blocks && a->V0->bs == a->V1->bs &&
+                   a->V0->k == a->V1->k,
+               "the diagonal needs the same test and trial space");
+    FE_REQUIRE(b || scalar_size(a->V0) == 0, "null vector");
+    const int need = (a->kind == FE_FORM_VP2_ELASTICITY) ? 2 : (a->kind == FE_FORM_P2_STIFFNESS ? 1 : 0);
+    for (int q = 0; q < need; ++q) FE_REQUIRE(a->coeff[q].kind >= 0, "coefficient not set");
+    DeviceScope d(a->ctx);
+    cudaStream_t st = as_stream(stream);
+    const int64_t n = scalar_size(a->V0);
+    if (flags & FE_ASM_ZERO) launch_zero(b, n, st);
+    MatLaunch L{};
+    L.kind = a->kind;
+    L.precision = a->precision;
+    L.num_cells = a->mesh->num_cells;
+    L.x = a->mesh->x.p;
+    L.geom = a->mesh->geom.p;
+    L.dofs0 = a->V0->dofs.p;
+    L.dofs1 = a->V1->dofs.p;
+    L.k0 = a->V0->k;
+    L.k1 = a->V1->k;
+    L.bs = a->V0->bs;
+    L.c0 = &a->coeff[0];
+    L.c1 = &a->coeff[1];
+    launch_diagonal(L, b, n, st);
+  });
+}
+
 int fe_apply_lifting(double* b, int num_forms, const fe_form* a, const fe_bc* bc1, const double* const* x0,
                      double scale, void* stream) {
   return guard([&] {

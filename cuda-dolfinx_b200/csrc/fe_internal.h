@@ -308,6 +308,8 @@ void launch_build_slotmap(const fe_form_s& f, cudaStream_t s);
 void launch_build_view(const fe_form_s& f, const fe_sparsity_s& mono, int64_t row_offset, int64_t col_offset,
                        fe_sparsity_s& view, cudaStream_t s);
 void launch_matrix_atomic(const MatLaunch& a, cudaStream_t s);
+// diagonal of a cell bilinear form into b (no BCs)
+void launch_diagonal(const MatLaunch& a, double* b, int64_t num_values, cudaStream_t s);
 void launch_set_diagonal(const fe_sparsity_s& sp, const fe_bc_s& bc, double diagonal, double* values,
                          cudaStream_t s);
 

@@ -935,6 +935,99 @@ __global__ void __launch_bounds__(kBlock) k_lift_vp2(const LiftArgs a) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Diagonal of a bilinear form as a vector (the "part": "diagonal" forms FFCx
+// generates, python/test/test_cuda_assembly.py:199-208): b[r] += A_e[r][r]
+// over the cells, no BCs.  The element code is the matrix kernels'; the emit
+// keeps the diagonal entries only (for FP64 the others are dead code).
+// ---------------------------------------------------------------------------
+struct DiagArgs {
+  int64_t num_cells;
+  const double* __restrict__ x;
+  const int32_t* __restrict__ geom;
+  const int32_t* __restrict__ dofs;
+  CoefDev c0, c1;
+  double* __restrict__ b;
+  int64_t num_values;
+};
+
+__global__ void __launch_bounds__(kBlock) k_diag_p1(const DiagArgs a) {
+  const int64_t c = blockIdx.x * (int64_t)kBlock + threadIdx.x;
+  if (c >= a.num_cells) return;
+  CellGeo g;
+  cell_geometry(a.x, load_geom(a.geom, c), g);
+  double G[4][3];
+  p1_grads(g, G);
+  const double s = g.adet * (1.0 / 6.0) * coef_cell(a.c0, c);
+  const int4 d = __ldg(reinterpret_cast<const int4*>(a.dofs) + c);
+  const int r[4] = {d.x, d.y, d.z, d.w};
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+    add_guarded(a.b, r[i], a.num_values, s * (G[i][0] * G[i][0] + G[i][1] * G[i][1] + G[i][2] * G[i][2]));
+}
+
+template <int COEF, typename T>
+__global__ void __launch_bounds__(kBlock) k_diag_p2(const DiagArgs a) {
+  const int64_t c = blockIdx.x * (int64_t)kBlock + threadIdx.x;
+  if (c >= a.num_cells) return;
+  CellGeo g;
+  cell_geometry(a.x, load_geom(a.geom, c), g);
+  double Gh[6];
+  ghat(g, Gh);
+  const int32_t* d = a.dofs + c * 10;
+  auto emit = [&](int i, int j, double v) {
+    if (i == j) add_guarded(a.b, __ldg(d + i), a.num_values, v);
+  };
+  if constexpr (COEF == FE_COEFF_P1) {
+    const int4 km = __ldg(reinterpret_cast<const int4*>(a.c0.map) + c);
+    const double k[4] = {__ldg(a.c0.v + km.x), __ldg(a.c0.v + km.y), __ldg(a.c0.v + km.z),
+                         __ldg(a.c0.v + km.w)};
+    T q[24];
+#pragma unroll
+    for (int m = 0; m < 4; ++m)
+#pragma unroll
+      for (int s = 0; s < 6; ++s) q[m * 6 + s] = (T)(k[m] * Gh[s]);
+    p2_stiffness_p1coef<T>(q, emit);
+  } else {
+    const double k = coef_cell(a.c0, c);
+    T gq[6];
+#pragma unroll
+    for (int s = 0; s < 6; ++s) gq[s] = (T)(k * Gh[s]);
+    p2_stiffness_const<T>(gq, emit);
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kBlockP3) k_diag_p3(const DiagArgs a) {
+  const int64_t c = blockIdx.x * (int64_t)kBlockP3 + threadIdx.x;
+  if (c >= a.num_cells) return;
+  CellGeo g;
+  cell_geometry(a.x, load_geom(a.geom, c), g);
+  double Gh[6];
+  ghat(g, Gh);
+  const double k = coef_cell(a.c0, c);
+  T gq[6];
+#pragma unroll
+  for (int s = 0; s < 6; ++s) gq[s] = (T)(k * Gh[s]);
+  const int32_t* d = a.dofs + c * 20;
+  p3_stiffness_const<T>(gq, [&](int i, int j, double v) {
+    if (i == j) add_guarded(a.b, __ldg(d + i), a.num_values, v);
+  });
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kBlock) k_diag_vp2(const DiagArgs a) {
+  const int64_t c = blockIdx.x * (int64_t)kBlock + threadIdx.x;
+  if (c >= a.num_cells) return;
+  CellGeo g;
+  cell_geometry(a.x, load_geom(a.geom, c), g);
+  const double lam = coef_cell(a.c0, c), mu = coef_cell(a.c1, c);
+  const int32_t* d = a.dofs + c * 10;
+  elasticity_blocks<T>(g, lam, mu, [&](int ca, int cb, int i, int j, double v) {
+    if (ca == cb && i == j) add_guarded(a.b, 3 * (int64_t)__ldg(d + i) + ca, a.num_values, v);
+  });
+}
+
 __global__ void k_mark_cells(const int32_t* __restrict__ dofs, int64_t num_cells, int k, int bs,
                              const uint8_t* __restrict__ markers, int32_t* __restrict__ out,
                              unsigned long long* count) {
@@ -1256,6 +1349,49 @@ void launch_lifting(const LiftLaunch& L, cudaStream_t s) {
     }
     default:
       FE_FAIL(FE_ERR_ARG, "lifting needs a bilinear form, got kind " + std::to_string(L.kind));
+  }
+  FE_CUDA(cudaGetLastError());
+}
+
+void launch_diagonal(const MatLaunch& L, double* b, int64_t num_values, cudaStream_t s) {
+  if (L.num_cells == 0) return;
+  DiagArgs a{};
+  a.num_cells = L.num_cells;
+  a.x = L.x;
+  a.geom = L.geom;
+  a.dofs = L.dofs0;
+  a.c0 = to_dev(L.c0);
+  a.c1 = to_dev(L.c1);
+  a.b = b;
+  a.num_values = num_values;
+  const unsigned grid = grid_for(L.num_cells, kBlock);
+  const bool f32 = L.precision == FE_PREC_FP32;
+  switch (L.kind) {
+    case FE_FORM_P1_STIFFNESS:
+      k_diag_p1<<<grid, kBlock, 0, s>>>(a);
+      break;
+    case FE_FORM_P2_STIFFNESS:
+      if (a.c0.kind == FE_COEFF_P1) {
+        if (f32) k_diag_p2<FE_COEFF_P1, float><<<grid, kBlock, 0, s>>>(a);
+        else k_diag_p2<FE_COEFF_P1, double><<<grid, kBlock, 0, s>>>(a);
+      } else {
+        if (f32) k_diag_p2<FE_COEFF_DG0, float><<<grid, kBlock, 0, s>>>(a);
+        else k_diag_p2<FE_COEFF_DG0, double><<<grid, kBlock, 0, s>>>(a);
+      }
+      break;
+    case FE_FORM_P3_STIFFNESS: {
+      const unsigned g3 = grid_for(L.num_cells, kBlockP3);
+      if (f32) k_diag_p3<float><<<g3, kBlockP3, 0, s>>>(a);
+      else k_diag_p3<double><<<g3, kBlockP3, 0, s>>>(a);
+      break;
+    }
+    case FE_FORM_VP2_ELASTICITY:
+      if (f32) k_diag_vp2<float><<<grid, kBlock, 0, s>>>(a);
+      else k_diag_vp2<double><<<grid, kBlock, 0, s>>>(a);
+      break;
+    default:
+      FE_FAIL(FE_ERR_ARG, "the diagonal is offered for the cell bilinear forms (P1/P2/P3 stiffness, vector-P2 "
+                          "elasticity), not kind " + std::to_string(L.kind));
   }
   FE_CUDA(cudaGetLastError());
 }

@@ -82,6 +82,7 @@ _SIGS = {
     "fe_assemble_matrix": (i32, [vp, vp, vp, vp, dbl, u32, vp]),
     "fe_assemble_matrix_batch": (i32, [vp, i32, vp, vp, vp, vp, dbl, u32, vp]),
     "fe_zero_entries": (i32, [vp, i64, vp]),
+    "fe_assemble_diagonal": (i32, [vp, vp, u32, vp]),
     "fe_interpolate": (i32, [vp, vp, vp, vp, vp, vp]),
     "fe_assemble_vector": (i32, [vp, vp, u32, vp]),
     "fe_apply_lifting": (i32, [vp, i32, vp, vp, vp, dbl, vp]),

@@ -303,8 +303,12 @@ class CUDAAssembler:
         b.to_device()  # assemble.py:156-158
         self.pack_coefficients(b, coeffs)
         vec._before_write()
-        _lib.check(_lib.lib.fe_assemble_vector(b._handle, vec.vector.data_ptr(), _lib.ASM_ZERO if zero else 0,
-                                               self._ctx.stream()), "fe_assemble_vector")
+        if b.part == "diagonal":
+            _lib.check(_lib.lib.fe_assemble_diagonal(b._handle, vec.vector.data_ptr(), _lib.ASM_ZERO if zero else 0,
+                                                     self._ctx.stream()), "fe_assemble_diagonal")
+        else:
+            _lib.check(_lib.lib.fe_assemble_vector(b._handle, vec.vector.data_ptr(), _lib.ASM_ZERO if zero else 0,
+                                                   self._ctx.stream()), "fe_assemble_vector")
         b._mark_used()
         return vec
 

@@ -114,11 +114,20 @@ def device_dofmap(ctx, V: FunctionSpace) -> DeviceDofMap:
 class CUDAForm:
     """CUDA wrapper of a built-in form (the reference wraps a dolfinx.fem.Form)."""
 
-    def __init__(self, form: FormSpec, jit_args: typing.Optional[dict] = None):
+    def __init__(self, form: FormSpec, jit_args: typing.Optional[dict] = None, part: typing.Optional[str] = None):
         if not isinstance(form, FormSpec):
             raise TypeError(f"Expected a cudolfinx.fem.FormSpec, got '{type(form)}'")
+        if part not in (None, "full", "diagonal"):
+            raise ValueError(f"unknown form part '{part}' (expected 'full' or 'diagonal')")
+        if part == "diagonal" and (form.rank != 2 or form.facets is not None
+                                   or form.function_spaces[0] is not form.function_spaces[1]):
+            raise ValueError("the diagonal part is offered for cell bilinear forms on one space")
         self._ctx = get_cuda_context()
         self._spec = form
+        # "diagonal": the form is the matrix diagonal as a linear form on the
+        # test space (FFCx's "part" option, as passed by the reference through
+        # form_compiler_options)
+        self._part = "diagonal" if part == "diagonal" else "full"
         self._cuda_mesh = _create_mesh_on_device(self._ctx, form.mesh)
         self._dofmaps = [device_dofmap(self._ctx, V) for V in form.function_spaces]
         self._jit_args = dict(DEFAULT_CUDA_JIT_ARGS, **(jit_args or {}))
@@ -161,6 +170,8 @@ class CUDAForm:
         dofs are numbered by their position in it."""
         if len(restrictions) != self.rank:
             raise ValueError("Number of restrictions must equal arity of form (1 for vector, 2 for matrix)!")
+        if self._part == "diagonal":  # one space: the test restriction is the trial one
+            restrictions = [restrictions[0], restrictions[0]]
         old = [dm.restriction for dm in self._dofmaps]
         new = [None if r is None else np.ascontiguousarray(r, dtype=np.int32) for r in restrictions]
         if all((o is None and n is None) or (o is not None and n is not None and np.array_equal(o, n))
@@ -309,11 +320,16 @@ class CUDAForm:
 
     @property
     def function_spaces(self):
-        return self._spec.function_spaces
+        return self._spec.function_spaces[:self.rank]
 
     @property
     def rank(self) -> int:
-        return self._spec.rank
+        return 1 if self._part == "diagonal" else self._spec.rank
+
+    @property
+    def part(self) -> str:
+        """'full', or 'diagonal' for the diagonal of a bilinear form."""
+        return self._part
 
     def __del__(self):
         if getattr(self, "_handle", None):
@@ -423,19 +439,22 @@ def form(form: typing.Union[FormSpec, typing.Iterable], restriction=None,
     """Create a CUDAForm from a built-in form spec, or a BlockCUDAForm from a
     list of them (block vector) or a list of lists (block matrix, None for an
     empty block) with optional restrictions (mirrors cudolfinx.form,
-    python/cudolfinx/form.py:227-249)."""
+    python/cudolfinx/form.py:227-249).  Of the keyword arguments the reference
+    forwards to dolfinx.fem.form, ``form_compiler_options={"part": "diagonal"}``
+    is honoured: the bilinear form's diagonal becomes a linear form."""
+    fco = kwargs.get("form_compiler_options") or {}
+    part = fco.get("part")
     if isinstance(form, FormSpec):
+        f = CUDAForm(form, cuda_jit_args, part)
         if restriction is not None:
-            f = CUDAForm(form, cuda_jit_args)
             f.set_restriction(restriction)
-            return f
-        return CUDAForm(form, cuda_jit_args)
+        return f
 
     def _create(x):
         if x is None:
             return None
         if isinstance(x, FormSpec):
-            return CUDAForm(x, cuda_jit_args)
+            return CUDAForm(x, cuda_jit_args, part)
         return [_create(y) for y in x]
 
     return BlockCUDAForm(_create(form), restriction)

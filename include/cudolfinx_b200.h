@@ -292,6 +292,12 @@ int fe_assemble_vector(fe_form L, double* b, unsigned flags, void* stream);
  * on the columns of bc1[i]; x0 may be NULL or hold NULL entries. */
 int fe_apply_lifting(double* b, int num_forms, const fe_form* a, const fe_bc* bc1,
                      const double* const* x0, double scale, void* stream);
+/* The diagonal of a cell bilinear form (P1 / P2 / P3 stiffness, vector-P2
+ * elasticity) as a vector, b[r] += A_e[r][r] over the cells with no BCs: what
+ * the reference assembles from a form compiled with the FFCx option
+ * "part": "diagonal" (python/test/test_cuda_assembly.py:199-208), e.g. for a
+ * Jacobi preconditioner.  FE_ASM_ZERO zeroes b first. */
+int fe_assemble_diagonal(fe_form a, double* b, unsigned flags, void* stream);
 /* Replaces set_bc_on_device (wrappers/fem.cpp:357-383, CUDAAssembler.h:443-529):
  * b[d] = scale * (g[d] - x0[d]) for the BC dofs; x0 may be NULL. */
 int fe_set_bc(double* b, int64_t num_values, fe_bc bc, const double* x0, double scale,

@@ -608,6 +608,14 @@ def assemble_vector(be, dofs, num_values, bs=1):
     return b
 
 
+def assemble_diagonal(Ae, dofs, num_values, bs=1):
+    """Vector of the bilinear form's diagonal, b[r] += Ae[r][r] over the cells,
+    no BCs: what a form compiled with FFCx's ``"part": "diagonal"`` assembles
+    (python/test/test_cuda_assembly.py:199-208).  It equals the diagonal of
+    the matrix assembled without BCs."""
+    return assemble_vector(np.diagonal(Ae, axis1=1, axis2=2), dofs, num_values, bs)
+
+
 def apply_lifting(b, Ae, dofs0, dofs1, bc1_markers, g, x0=None, scale=1.0, bs0=1, bs1=1):
     """b -= scale * A (g - x0) restricted to BC columns, for every cell with a
     BC column (CUDAFormIntegral.cpp:647-715)."""

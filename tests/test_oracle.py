@@ -479,3 +479,15 @@ def test_interior_average_load_sums_to_the_interior_facet_area():
     for degree in (0, 1):
         be = fo.interior_avg_load(coords, cells, q, degree)
         assert abs(be.sum() - area) < 1e-13 * area
+
+
+@pytest.mark.parametrize("kind", ["p1k", "p2", "p3", "vp2"])
+def test_diagonal_part_is_the_diagonal_of_the_matrix_without_bcs(kind):
+    P = fo.build_problem(kind, 2, seed=3)
+    bs, dofs = P["bs"], P["dofs"]
+    rp, col = fo.sparsity(dofs, dofs, P["ndof"], bs, bs)
+    Ae = fo.element_matrices(P)
+    A = fo.assemble_matrix(Ae, dofs, dofs, rp, col, bs, bs)
+    d = fo.assemble_diagonal(Ae, dofs, P["ndof"] * bs, bs)
+    assert np.allclose(d, A[fo.diag_positions(rp, col)], rtol=1e-14, atol=0)
+    assert np.all(d > 0)  # an SPD operator's diagonal
