@@ -114,6 +114,14 @@ def out_handle():
     return ctypes.c_void_p()
 
 
+def release(destroy: str, handle) -> None:
+    """Destroy an engine handle from a finalizer.  A no-op when the library
+    object is already gone (interpreter shutdown clears module globals)."""
+    L = globals().get("lib")
+    if L is not None and handle:
+        getattr(L, destroy)(handle)
+
+
 def ptr(x) -> int | None:
     """Device/host address of a torch tensor, numpy array or int (None passes NULL)."""
     if x is None:

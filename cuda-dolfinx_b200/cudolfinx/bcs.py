@@ -68,7 +68,7 @@ class _DeviceBC:
 
     def __del__(self):
         if getattr(self, "handle", None):
-            _lib.lib.fe_bc_destroy(self.handle)
+            _lib.release("fe_bc_destroy", self.handle)
             self.handle = None
 
 
@@ -95,7 +95,7 @@ class _RestrictedBC:
 
     def __del__(self):
         if getattr(self, "handle", None):
-            _lib.lib.fe_bc_destroy(self.handle)
+            _lib.release("fe_bc_destroy", self.handle)
             self.handle = None
 
 

@@ -41,7 +41,7 @@ class DeviceMesh:
 
     def __del__(self):
         if getattr(self, "handle", None):
-            _lib.lib.fe_mesh_destroy(self.handle)
+            _lib.release("fe_mesh_destroy", self.handle)
             self.handle = None
 
 
@@ -80,7 +80,7 @@ class DeviceDofMap:
 
     def __del__(self):
         if getattr(self, "handle", None):
-            _lib.lib.fe_dofmap_destroy(self.handle)
+            _lib.release("fe_dofmap_destroy", self.handle)
             self.handle = None
 
 
@@ -333,7 +333,7 @@ class CUDAForm:
 
     def __del__(self):
         if getattr(self, "_handle", None):
-            _lib.lib.fe_form_destroy(self._handle)
+            _lib.release("fe_form_destroy", self._handle)
             self._handle = None
 
 

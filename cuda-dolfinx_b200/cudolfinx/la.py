@@ -95,7 +95,7 @@ class Sparsity:
 
     def __del__(self):
         if getattr(self, "handle", None):
-            _lib.lib.fe_sparsity_destroy(self.handle)
+            _lib.release("fe_sparsity_destroy", self.handle)
             self.handle = None
 
 
