@@ -69,6 +69,8 @@ int form_rank(int kind) {
   switch (kind) {
     case FE_FORM_P1_STIFFNESS:
     case FE_FORM_P2_STIFFNESS:
+    case FE_FORM_P1_MASS:
+    case FE_FORM_P2_MASS:
     case FE_FORM_VP2_ELASTICITY:
     case FE_FORM_P1_FACET_MASS:
     case FE_FORM_P2_FACET_MASS:
@@ -101,12 +103,14 @@ int form_rank(int kind) {
 void form_space(int kind, int& k, int& bs) {
   switch (kind) {
     case FE_FORM_P1_STIFFNESS:
+    case FE_FORM_P1_MASS:
     case FE_FORM_P1_LOAD:
     case FE_FORM_P1_FACET_MASS:
     case FE_FORM_P1_FACET_LOAD:
       k = 4, bs = 1;
       return;
     case FE_FORM_P2_STIFFNESS:
+    case FE_FORM_P2_MASS:
     case FE_FORM_P2_LOAD:
     case FE_FORM_P2_FACET_MASS:
     case FE_FORM_P2_FACET_LOAD:
@@ -580,11 +584,12 @@ int fe_form_set_coefficient(fe_form f, int index, int coeff_kind, fe_dofmap cmap
       FE_REQUIRE(cmap && cmap->k == 4 && cmap->bs == 1 && cmap->num_cells == C && !cmap->excluded,
                  "P1 coefficient needs an unrestricted P1 dofmap");
       FE_REQUIRE(n >= cmap->num_blocks, "P1 coefficient has fewer values than dofs");
-      FE_REQUIRE(f->kind == FE_FORM_P2_STIFFNESS || f->kind == FE_FORM_P1_LOAD ||
+      FE_REQUIRE(f->kind == FE_FORM_P2_STIFFNESS || f->kind == FE_FORM_P1_LOAD || f->kind == FE_FORM_P1_MASS ||
+                     f->kind == FE_FORM_P2_MASS ||
                      f->kind == FE_FORM_P1_FACET_LOAD || f->kind == FE_FORM_P2_FACET_LOAD ||
                      f->kind == FE_FORM_INTEGRAL || f->kind == FE_FORM_FACET_INTEGRAL ||
                      f->kind == FE_FORM_JUMP_NORM || (f->kind == FE_FORM_P1_ENERGY && index == 1),
-                 "P1 coefficients are supported by P2 stiffness, P1 load, facet load and functional forms");
+                 "P1 coefficients are supported by P2 stiffness, mass, P1 load, facet load and functional forms");
     } else if (coeff_kind == FE_COEFF_P2) {
       FE_REQUIRE(f->kind == FE_FORM_P2_ENERGY && index == 1, "P2 coefficients are the u of FE_FORM_P2_ENERGY");
       FE_REQUIRE(cmap && cmap->k == 10 && cmap->bs == 1 && cmap->num_cells == C && !cmap->excluded,
@@ -888,7 +893,7 @@ int fe_assemble_matrix(fe_form a, double* values, fe_bc bc0, fe_bc bc1, double d
     // so it keeps both reductions, as does FE_ASM_FULL_SCATTER for every form.
     const bool upper = zero && !view && !(flags & FE_ASM_FULL_SCATTER) &&
                        (a->kind == FE_FORM_VP2_ELASTICITY || a->kind == FE_FORM_P3_STIFFNESS ||
-                        a->kind == FE_FORM_P1_STIFFNESS) && a->V0 == a->V1 &&
+                        a->kind == FE_FORM_P1_STIFFNESS || a->kind == FE_FORM_P1_MASS) && a->V0 == a->V1 &&
                        bc0 == bc1 && ensure_mirror(*a->sp, st, a->V0->bs);
     if (zero) launch_zero(values, a->sp->nnz, st);
     MatLaunch L{};

@@ -1019,6 +1019,154 @@ __device__ __forceinline__ void p2_block_upper(const T* W, Emit&& emit) {
   }
 }
 
+// P1 mass, cellwise-constant coefficient: s = c * |det J|; emit(i, j, value), i <= j.
+template <typename T, typename Emit>
+__device__ __forceinline__ void p1_mass_const(T s, Emit&& emit) {
+  emit(0, 0, s * T(0x1.1111111111111p-6));
+  emit(0, 1, s * T(0x1.1111111111111p-7));
+  emit(0, 2, s * T(0x1.1111111111111p-7));
+  emit(0, 3, s * T(0x1.1111111111111p-7));
+  emit(1, 1, s * T(0x1.1111111111111p-6));
+  emit(1, 2, s * T(0x1.1111111111111p-7));
+  emit(1, 3, s * T(0x1.1111111111111p-7));
+  emit(2, 2, s * T(0x1.1111111111111p-6));
+  emit(2, 3, s * T(0x1.1111111111111p-7));
+  emit(3, 3, s * T(0x1.1111111111111p-6));
+}
+// P1 mass, P1 coefficient: cq[m] = c_m * |det J|.
+template <typename T, typename Emit>
+__device__ __forceinline__ void p1_mass_p1coef(const T* cq, Emit&& emit) {
+  emit(0, 0, (fma(cq[2], T(0x1.6c16c16c16c17p-9), cq[0] * T(0x1.1111111111111p-7)) + fma(cq[3], T(0x1.6c16c16c16c17p-9), cq[1] * T(0x1.6c16c16c16c17p-9))));
+  emit(0, 1, (fma(cq[2], T(0x1.6c16c16c16c17p-10), cq[0] * T(0x1.6c16c16c16c17p-9)) + fma(cq[3], T(0x1.6c16c16c16c17p-10), cq[1] * T(0x1.6c16c16c16c17p-9))));
+  emit(0, 2, (fma(cq[2], T(0x1.6c16c16c16c17p-9), cq[0] * T(0x1.6c16c16c16c17p-9)) + fma(cq[3], T(0x1.6c16c16c16c17p-10), cq[1] * T(0x1.6c16c16c16c17p-10))));
+  emit(0, 3, (fma(cq[2], T(0x1.6c16c16c16c17p-10), cq[0] * T(0x1.6c16c16c16c17p-9)) + fma(cq[3], T(0x1.6c16c16c16c17p-9), cq[1] * T(0x1.6c16c16c16c17p-10))));
+  emit(1, 1, (fma(cq[2], T(0x1.6c16c16c16c17p-9), cq[0] * T(0x1.6c16c16c16c17p-9)) + fma(cq[3], T(0x1.6c16c16c16c17p-9), cq[1] * T(0x1.1111111111111p-7))));
+  emit(1, 2, (fma(cq[2], T(0x1.6c16c16c16c17p-9), cq[0] * T(0x1.6c16c16c16c17p-10)) + fma(cq[3], T(0x1.6c16c16c16c17p-10), cq[1] * T(0x1.6c16c16c16c17p-9))));
+  emit(1, 3, (fma(cq[2], T(0x1.6c16c16c16c17p-10), cq[0] * T(0x1.6c16c16c16c17p-10)) + fma(cq[3], T(0x1.6c16c16c16c17p-9), cq[1] * T(0x1.6c16c16c16c17p-9))));
+  emit(2, 2, (fma(cq[2], T(0x1.1111111111111p-7), cq[0] * T(0x1.6c16c16c16c17p-9)) + fma(cq[3], T(0x1.6c16c16c16c17p-9), cq[1] * T(0x1.6c16c16c16c17p-9))));
+  emit(2, 3, (fma(cq[2], T(0x1.6c16c16c16c17p-9), cq[0] * T(0x1.6c16c16c16c17p-10)) + fma(cq[3], T(0x1.6c16c16c16c17p-9), cq[1] * T(0x1.6c16c16c16c17p-10))));
+  emit(3, 3, (fma(cq[2], T(0x1.6c16c16c16c17p-9), cq[0] * T(0x1.6c16c16c16c17p-9)) + fma(cq[3], T(0x1.1111111111111p-7), cq[1] * T(0x1.6c16c16c16c17p-9))));
+}
+
+// P2 mass, cellwise-constant coefficient: s = c * |det J|; emit(i, j, value), i <= j.
+template <typename T, typename Emit>
+__device__ __forceinline__ void p2_mass_const(T s, Emit&& emit) {
+  emit(0, 0, s * T(0x1.3813813813814p-9));
+  emit(0, 1, s * T(0x1.a01a01a01a01ap-12));
+  emit(0, 2, s * T(0x1.a01a01a01a01ap-12));
+  emit(0, 3, s * T(0x1.a01a01a01a01ap-12));
+  emit(0, 4, s * T(-0x1.3813813813814p-9));
+  emit(0, 5, s * T(-0x1.3813813813814p-9));
+  emit(0, 6, s * T(-0x1.3813813813814p-9));
+  emit(0, 7, s * T(-0x1.a01a01a01a01ap-10));
+  emit(0, 8, s * T(-0x1.a01a01a01a01ap-10));
+  emit(0, 9, s * T(-0x1.a01a01a01a01ap-10));
+  emit(1, 1, s * T(0x1.3813813813814p-9));
+  emit(1, 2, s * T(0x1.a01a01a01a01ap-12));
+  emit(1, 3, s * T(0x1.a01a01a01a01ap-12));
+  emit(1, 4, s * T(-0x1.3813813813814p-9));
+  emit(1, 5, s * T(-0x1.a01a01a01a01ap-10));
+  emit(1, 6, s * T(-0x1.a01a01a01a01ap-10));
+  emit(1, 7, s * T(-0x1.3813813813814p-9));
+  emit(1, 8, s * T(-0x1.3813813813814p-9));
+  emit(1, 9, s * T(-0x1.a01a01a01a01ap-10));
+  emit(2, 2, s * T(0x1.3813813813814p-9));
+  emit(2, 3, s * T(0x1.a01a01a01a01ap-12));
+  emit(2, 4, s * T(-0x1.a01a01a01a01ap-10));
+  emit(2, 5, s * T(-0x1.3813813813814p-9));
+  emit(2, 6, s * T(-0x1.a01a01a01a01ap-10));
+  emit(2, 7, s * T(-0x1.3813813813814p-9));
+  emit(2, 8, s * T(-0x1.a01a01a01a01ap-10));
+  emit(2, 9, s * T(-0x1.3813813813814p-9));
+  emit(3, 3, s * T(0x1.3813813813814p-9));
+  emit(3, 4, s * T(-0x1.a01a01a01a01ap-10));
+  emit(3, 5, s * T(-0x1.a01a01a01a01ap-10));
+  emit(3, 6, s * T(-0x1.3813813813814p-9));
+  emit(3, 7, s * T(-0x1.a01a01a01a01ap-10));
+  emit(3, 8, s * T(-0x1.3813813813814p-9));
+  emit(3, 9, s * T(-0x1.3813813813814p-9));
+  emit(4, 4, s * T(0x1.a01a01a01a01ap-7));
+  emit(4, 5, s * T(0x1.a01a01a01a01ap-8));
+  emit(4, 6, s * T(0x1.a01a01a01a01ap-8));
+  emit(4, 7, s * T(0x1.a01a01a01a01ap-8));
+  emit(4, 8, s * T(0x1.a01a01a01a01ap-8));
+  emit(4, 9, s * T(0x1.a01a01a01a01ap-9));
+  emit(5, 5, s * T(0x1.a01a01a01a01ap-7));
+  emit(5, 6, s * T(0x1.a01a01a01a01ap-8));
+  emit(5, 7, s * T(0x1.a01a01a01a01ap-8));
+  emit(5, 8, s * T(0x1.a01a01a01a01ap-9));
+  emit(5, 9, s * T(0x1.a01a01a01a01ap-8));
+  emit(6, 6, s * T(0x1.a01a01a01a01ap-7));
+  emit(6, 7, s * T(0x1.a01a01a01a01ap-9));
+  emit(6, 8, s * T(0x1.a01a01a01a01ap-8));
+  emit(6, 9, s * T(0x1.a01a01a01a01ap-8));
+  emit(7, 7, s * T(0x1.a01a01a01a01ap-7));
+  emit(7, 8, s * T(0x1.a01a01a01a01ap-8));
+  emit(7, 9, s * T(0x1.a01a01a01a01ap-8));
+  emit(8, 8, s * T(0x1.a01a01a01a01ap-7));
+  emit(8, 9, s * T(0x1.a01a01a01a01ap-8));
+  emit(9, 9, s * T(0x1.a01a01a01a01ap-7));
+}
+// P2 mass, P1 coefficient: cq[m] = c_m * |det J|.
+template <typename T, typename Emit>
+__device__ __forceinline__ void p2_mass_p1coef(const T* cq, Emit&& emit) {
+  emit(0, 0, (fma(cq[2], T(0x1.a01a01a01a01ap-12), cq[0] * T(0x1.3813813813814p-10)) + fma(cq[3], T(0x1.a01a01a01a01ap-12), cq[1] * T(0x1.a01a01a01a01ap-12))));
+  emit(0, 1, (cq[2] * T(0x1.a01a01a01a01ap-13) + cq[3] * T(0x1.a01a01a01a01ap-13)));
+  emit(0, 2, (cq[1] * T(0x1.a01a01a01a01ap-13) + cq[3] * T(0x1.a01a01a01a01ap-13)));
+  emit(0, 3, (cq[1] * T(0x1.a01a01a01a01ap-13) + cq[2] * T(0x1.a01a01a01a01ap-13)));
+  emit(0, 4, (fma(cq[2], T(-0x1.a01a01a01a01ap-11), cq[0] * T(-0x1.a01a01a01a01ap-12)) + fma(cq[3], T(-0x1.a01a01a01a01ap-11), cq[1] * T(-0x1.a01a01a01a01ap-12))));
+  emit(0, 5, (fma(cq[2], T(-0x1.a01a01a01a01ap-12), cq[0] * T(-0x1.a01a01a01a01ap-12)) + fma(cq[3], T(-0x1.a01a01a01a01ap-11), cq[1] * T(-0x1.a01a01a01a01ap-11))));
+  emit(0, 6, (fma(cq[2], T(-0x1.a01a01a01a01ap-11), cq[0] * T(-0x1.a01a01a01a01ap-12)) + fma(cq[3], T(-0x1.a01a01a01a01ap-12), cq[1] * T(-0x1.a01a01a01a01ap-11))));
+  emit(0, 7, (fma(cq[3], T(-0x1.a01a01a01a01ap-11), cq[1] * T(-0x1.a01a01a01a01ap-12)) + cq[2] * T(-0x1.a01a01a01a01ap-12)));
+  emit(0, 8, (fma(cq[3], T(-0x1.a01a01a01a01ap-12), cq[1] * T(-0x1.a01a01a01a01ap-12)) + cq[2] * T(-0x1.a01a01a01a01ap-11)));
+  emit(0, 9, (fma(cq[3], T(-0x1.a01a01a01a01ap-12), cq[1] * T(-0x1.a01a01a01a01ap-11)) + cq[2] * T(-0x1.a01a01a01a01ap-12)));
+  emit(1, 1, (fma(cq[2], T(0x1.a01a01a01a01ap-12), cq[0] * T(0x1.a01a01a01a01ap-12)) + fma(cq[3], T(0x1.a01a01a01a01ap-12), cq[1] * T(0x1.3813813813814p-10))));
+  emit(1, 2, (cq[0] * T(0x1.a01a01a01a01ap-13) + cq[3] * T(0x1.a01a01a01a01ap-13)));
+  emit(1, 3, (cq[0] * T(0x1.a01a01a01a01ap-13) + cq[2] * T(0x1.a01a01a01a01ap-13)));
+  emit(1, 4, (fma(cq[2], T(-0x1.a01a01a01a01ap-11), cq[0] * T(-0x1.a01a01a01a01ap-12)) + fma(cq[3], T(-0x1.a01a01a01a01ap-11), cq[1] * T(-0x1.a01a01a01a01ap-12))));
+  emit(1, 5, (fma(cq[3], T(-0x1.a01a01a01a01ap-11), cq[0] * T(-0x1.a01a01a01a01ap-12)) + cq[2] * T(-0x1.a01a01a01a01ap-12)));
+  emit(1, 6, (fma(cq[3], T(-0x1.a01a01a01a01ap-12), cq[0] * T(-0x1.a01a01a01a01ap-12)) + cq[2] * T(-0x1.a01a01a01a01ap-11)));
+  emit(1, 7, (fma(cq[2], T(-0x1.a01a01a01a01ap-12), cq[0] * T(-0x1.a01a01a01a01ap-11)) + fma(cq[3], T(-0x1.a01a01a01a01ap-11), cq[1] * T(-0x1.a01a01a01a01ap-12))));
+  emit(1, 8, (fma(cq[2], T(-0x1.a01a01a01a01ap-11), cq[0] * T(-0x1.a01a01a01a01ap-11)) + fma(cq[3], T(-0x1.a01a01a01a01ap-12), cq[1] * T(-0x1.a01a01a01a01ap-12))));
+  emit(1, 9, (fma(cq[3], T(-0x1.a01a01a01a01ap-12), cq[0] * T(-0x1.a01a01a01a01ap-11)) + cq[2] * T(-0x1.a01a01a01a01ap-12)));
+  emit(2, 2, (fma(cq[2], T(0x1.3813813813814p-10), cq[0] * T(0x1.a01a01a01a01ap-12)) + fma(cq[3], T(0x1.a01a01a01a01ap-12), cq[1] * T(0x1.a01a01a01a01ap-12))));
+  emit(2, 3, (cq[0] * T(0x1.a01a01a01a01ap-13) + cq[1] * T(0x1.a01a01a01a01ap-13)));
+  emit(2, 4, (fma(cq[3], T(-0x1.a01a01a01a01ap-11), cq[0] * T(-0x1.a01a01a01a01ap-12)) + cq[1] * T(-0x1.a01a01a01a01ap-12)));
+  emit(2, 5, (fma(cq[2], T(-0x1.a01a01a01a01ap-12), cq[0] * T(-0x1.a01a01a01a01ap-12)) + fma(cq[3], T(-0x1.a01a01a01a01ap-11), cq[1] * T(-0x1.a01a01a01a01ap-11))));
+  emit(2, 6, (fma(cq[3], T(-0x1.a01a01a01a01ap-12), cq[0] * T(-0x1.a01a01a01a01ap-12)) + cq[1] * T(-0x1.a01a01a01a01ap-11)));
+  emit(2, 7, (fma(cq[2], T(-0x1.a01a01a01a01ap-12), cq[0] * T(-0x1.a01a01a01a01ap-11)) + fma(cq[3], T(-0x1.a01a01a01a01ap-11), cq[1] * T(-0x1.a01a01a01a01ap-12))));
+  emit(2, 8, (fma(cq[3], T(-0x1.a01a01a01a01ap-12), cq[0] * T(-0x1.a01a01a01a01ap-11)) + cq[1] * T(-0x1.a01a01a01a01ap-12)));
+  emit(2, 9, (fma(cq[2], T(-0x1.a01a01a01a01ap-12), cq[0] * T(-0x1.a01a01a01a01ap-11)) + fma(cq[3], T(-0x1.a01a01a01a01ap-12), cq[1] * T(-0x1.a01a01a01a01ap-11))));
+  emit(3, 3, (fma(cq[2], T(0x1.a01a01a01a01ap-12), cq[0] * T(0x1.a01a01a01a01ap-12)) + fma(cq[3], T(0x1.3813813813814p-10), cq[1] * T(0x1.a01a01a01a01ap-12))));
+  emit(3, 4, (fma(cq[2], T(-0x1.a01a01a01a01ap-11), cq[0] * T(-0x1.a01a01a01a01ap-12)) + cq[1] * T(-0x1.a01a01a01a01ap-12)));
+  emit(3, 5, (fma(cq[2], T(-0x1.a01a01a01a01ap-12), cq[0] * T(-0x1.a01a01a01a01ap-12)) + cq[1] * T(-0x1.a01a01a01a01ap-11)));
+  emit(3, 6, (fma(cq[2], T(-0x1.a01a01a01a01ap-11), cq[0] * T(-0x1.a01a01a01a01ap-12)) + fma(cq[3], T(-0x1.a01a01a01a01ap-12), cq[1] * T(-0x1.a01a01a01a01ap-11))));
+  emit(3, 7, (fma(cq[2], T(-0x1.a01a01a01a01ap-12), cq[0] * T(-0x1.a01a01a01a01ap-11)) + cq[1] * T(-0x1.a01a01a01a01ap-12)));
+  emit(3, 8, (fma(cq[2], T(-0x1.a01a01a01a01ap-11), cq[0] * T(-0x1.a01a01a01a01ap-11)) + fma(cq[3], T(-0x1.a01a01a01a01ap-12), cq[1] * T(-0x1.a01a01a01a01ap-12))));
+  emit(3, 9, (fma(cq[2], T(-0x1.a01a01a01a01ap-12), cq[0] * T(-0x1.a01a01a01a01ap-11)) + fma(cq[3], T(-0x1.a01a01a01a01ap-12), cq[1] * T(-0x1.a01a01a01a01ap-11))));
+  emit(4, 4, (fma(cq[2], T(0x1.3813813813814p-8), cq[0] * T(0x1.a01a01a01a01ap-10)) + fma(cq[3], T(0x1.3813813813814p-8), cq[1] * T(0x1.a01a01a01a01ap-10))));
+  emit(4, 5, (fma(cq[2], T(0x1.a01a01a01a01ap-10), cq[0] * T(0x1.a01a01a01a01ap-11)) + fma(cq[3], T(0x1.3813813813814p-9), cq[1] * T(0x1.a01a01a01a01ap-10))));
+  emit(4, 6, (fma(cq[2], T(0x1.3813813813814p-9), cq[0] * T(0x1.a01a01a01a01ap-11)) + fma(cq[3], T(0x1.a01a01a01a01ap-10), cq[1] * T(0x1.a01a01a01a01ap-10))));
+  emit(4, 7, (fma(cq[2], T(0x1.a01a01a01a01ap-10), cq[0] * T(0x1.a01a01a01a01ap-10)) + fma(cq[3], T(0x1.3813813813814p-9), cq[1] * T(0x1.a01a01a01a01ap-11))));
+  emit(4, 8, (fma(cq[2], T(0x1.3813813813814p-9), cq[0] * T(0x1.a01a01a01a01ap-10)) + fma(cq[3], T(0x1.a01a01a01a01ap-10), cq[1] * T(0x1.a01a01a01a01ap-11))));
+  emit(4, 9, (fma(cq[2], T(0x1.a01a01a01a01ap-11), cq[0] * T(0x1.a01a01a01a01ap-11)) + fma(cq[3], T(0x1.a01a01a01a01ap-11), cq[1] * T(0x1.a01a01a01a01ap-11))));
+  emit(5, 5, (fma(cq[2], T(0x1.a01a01a01a01ap-10), cq[0] * T(0x1.a01a01a01a01ap-10)) + fma(cq[3], T(0x1.3813813813814p-8), cq[1] * T(0x1.3813813813814p-8))));
+  emit(5, 6, (fma(cq[2], T(0x1.a01a01a01a01ap-10), cq[0] * T(0x1.a01a01a01a01ap-11)) + fma(cq[3], T(0x1.a01a01a01a01ap-10), cq[1] * T(0x1.3813813813814p-9))));
+  emit(5, 7, (fma(cq[2], T(0x1.a01a01a01a01ap-11), cq[0] * T(0x1.a01a01a01a01ap-10)) + fma(cq[3], T(0x1.3813813813814p-9), cq[1] * T(0x1.a01a01a01a01ap-10))));
+  emit(5, 8, (fma(cq[2], T(0x1.a01a01a01a01ap-11), cq[0] * T(0x1.a01a01a01a01ap-11)) + fma(cq[3], T(0x1.a01a01a01a01ap-11), cq[1] * T(0x1.a01a01a01a01ap-11))));
+  emit(5, 9, (fma(cq[2], T(0x1.a01a01a01a01ap-11), cq[0] * T(0x1.a01a01a01a01ap-10)) + fma(cq[3], T(0x1.a01a01a01a01ap-10), cq[1] * T(0x1.3813813813814p-9))));
+  emit(6, 6, (fma(cq[2], T(0x1.3813813813814p-8), cq[0] * T(0x1.a01a01a01a01ap-10)) + fma(cq[3], T(0x1.a01a01a01a01ap-10), cq[1] * T(0x1.3813813813814p-8))));
+  emit(6, 7, (fma(cq[2], T(0x1.a01a01a01a01ap-11), cq[0] * T(0x1.a01a01a01a01ap-11)) + fma(cq[3], T(0x1.a01a01a01a01ap-11), cq[1] * T(0x1.a01a01a01a01ap-11))));
+  emit(6, 8, (fma(cq[2], T(0x1.3813813813814p-9), cq[0] * T(0x1.a01a01a01a01ap-10)) + fma(cq[3], T(0x1.a01a01a01a01ap-11), cq[1] * T(0x1.a01a01a01a01ap-10))));
+  emit(6, 9, (fma(cq[2], T(0x1.a01a01a01a01ap-10), cq[0] * T(0x1.a01a01a01a01ap-10)) + fma(cq[3], T(0x1.a01a01a01a01ap-11), cq[1] * T(0x1.3813813813814p-9))));
+  emit(7, 7, (fma(cq[2], T(0x1.a01a01a01a01ap-10), cq[0] * T(0x1.3813813813814p-8)) + fma(cq[3], T(0x1.3813813813814p-8), cq[1] * T(0x1.a01a01a01a01ap-10))));
+  emit(7, 8, (fma(cq[2], T(0x1.a01a01a01a01ap-10), cq[0] * T(0x1.3813813813814p-9)) + fma(cq[3], T(0x1.a01a01a01a01ap-10), cq[1] * T(0x1.a01a01a01a01ap-11))));
+  emit(7, 9, (fma(cq[2], T(0x1.a01a01a01a01ap-11), cq[0] * T(0x1.3813813813814p-9)) + fma(cq[3], T(0x1.a01a01a01a01ap-10), cq[1] * T(0x1.a01a01a01a01ap-10))));
+  emit(8, 8, (fma(cq[2], T(0x1.3813813813814p-8), cq[0] * T(0x1.3813813813814p-8)) + fma(cq[3], T(0x1.a01a01a01a01ap-10), cq[1] * T(0x1.a01a01a01a01ap-10))));
+  emit(8, 9, (fma(cq[2], T(0x1.a01a01a01a01ap-10), cq[0] * T(0x1.3813813813814p-9)) + fma(cq[3], T(0x1.a01a01a01a01ap-11), cq[1] * T(0x1.a01a01a01a01ap-10))));
+  emit(9, 9, (fma(cq[2], T(0x1.a01a01a01a01ap-10), cq[0] * T(0x1.3813813813814p-8)) + fma(cq[3], T(0x1.a01a01a01a01ap-10), cq[1] * T(0x1.3813813813814p-8))));
+}
+
 #ifdef FE_FACET_TABLES
 // cell-local dofs on each facet (P1)
 static __constant__ int kFacetDofsP1[4][3] = {{1, 2, 3}, {0, 2, 3}, {0, 1, 3}, {0, 1, 2}};

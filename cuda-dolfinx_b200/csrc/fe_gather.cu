@@ -228,6 +228,32 @@ __global__ void k_elem_p1(const ElemArgs a) {
     }
 }
 
+// mass matrices (P1: K = 4, P2: K = 10) with a constant / DG0 / P1 coefficient
+template <int K, int COEF>
+__global__ void k_elem_mass(const ElemArgs a) {
+  const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (c >= a.num_cells) return;
+  Geo g;
+  geo(a.x, a.geom, c, g);
+  const int64_t N = a.num_cells;
+  double* __restrict__ E = a.E;
+  auto emit = [&](int i, int j, double v) {
+    E[(i * K + j) * N + c] = v;
+    if (i != j) E[(j * K + i) * N + c] = v;
+  };
+  if constexpr (COEF == FE_COEFF_P1) {
+    const int4 km = __ldg(reinterpret_cast<const int4*>(a.c0map) + c);
+    const double cq[4] = {g.adet * __ldg(a.c0 + km.x), g.adet * __ldg(a.c0 + km.y), g.adet * __ldg(a.c0 + km.z),
+                          g.adet * __ldg(a.c0 + km.w)};
+    if constexpr (K == 4) p1_mass_p1coef<double>(cq, emit);
+    else p2_mass_p1coef<double>(cq, emit);
+  } else {
+    const double sc = g.adet * cellcoef(a.coef0_kind, a.c0, a.c0const, c);
+    if constexpr (K == 4) p1_mass_const<double>(sc, emit);
+    else p2_mass_const<double>(sc, emit);
+  }
+}
+
 template <int COEF, typename T>
 __global__ void k_elem_p2(const ElemArgs a) {
   const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -421,6 +447,14 @@ void assemble_matrix_gather(fe_form_s& f, double* values, const fe_bc_s* bc0, co
       case FE_FORM_VP2_ELASTICITY:
         if (f.precision == FE_PREC_FP32) k_elem_vp2<float><<<grid, 128, 0, s>>>(ea);
         else k_elem_vp2<double><<<grid, 128, 0, s>>>(ea);
+        break;
+      case FE_FORM_P1_MASS:
+        if (ea.coef0_kind == FE_COEFF_P1) k_elem_mass<4, FE_COEFF_P1><<<grid, 128, 0, s>>>(ea);
+        else k_elem_mass<4, FE_COEFF_DG0><<<grid, 128, 0, s>>>(ea);
+        break;
+      case FE_FORM_P2_MASS:
+        if (ea.coef0_kind == FE_COEFF_P1) k_elem_mass<10, FE_COEFF_P1><<<grid, 128, 0, s>>>(ea);
+        else k_elem_mass<10, FE_COEFF_DG0><<<grid, 128, 0, s>>>(ea);
         break;
       case FE_FORM_P3_STIFFNESS:
         if (f.precision == FE_PREC_FP32) k_elem_p3<float><<<grid, 128, 0, s>>>(ea);

@@ -251,6 +251,81 @@ __global__ void __launch_bounds__(kBlock) k_mat_p2_atomic(const MatArgs a) {
 }
 
 // ---------------------------------------------------------------------------
+// Mass matrices c*u*v*dx (P1: K = 4, P2: K = 10), one thread per cell, FP64
+// atomics.  Only |det J| and the coefficient enter the element tensor.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double cell_adet(const double* __restrict__ x, int4 v) {
+  double x0[3], J[3][3];
+  const int vv[3] = {v.y, v.z, v.w};
+#pragma unroll
+  for (int r = 0; r < 3; ++r) x0[r] = __ldg(x + 3 * (int64_t)v.x + r);
+#pragma unroll
+  for (int cc = 0; cc < 3; ++cc)
+#pragma unroll
+    for (int r = 0; r < 3; ++r) J[r][cc] = __ldg(x + 3 * (int64_t)vv[cc] + r) - x0[r];
+  return fabs(J[0][0] * (J[1][1] * J[2][2] - J[1][2] * J[2][1]) +
+              J[0][1] * (J[1][2] * J[2][0] - J[1][0] * J[2][2]) +
+              J[0][2] * (J[1][0] * J[2][1] - J[1][1] * J[2][0]));
+}
+
+// emit(i, j, value) for the unique entries i <= j of cell c's mass matrix
+template <int K, int COEF, typename Emit>
+__device__ __forceinline__ void mass_element(const CoefDev& k, int64_t c, double adet, Emit&& emit) {
+  static_assert(K == 4 || K == 10, "P1 or P2 mass");
+  if constexpr (COEF == FE_COEFF_P1) {
+    const int4 km = __ldg(reinterpret_cast<const int4*>(k.map) + c);
+    const double cq[4] = {adet * __ldg(k.v + km.x), adet * __ldg(k.v + km.y), adet * __ldg(k.v + km.z),
+                          adet * __ldg(k.v + km.w)};
+    if constexpr (K == 4) p1_mass_p1coef<double>(cq, emit);
+    else p2_mass_p1coef<double>(cq, emit);
+  } else {
+    const double sc = adet * coef_cell(k, c);
+    if constexpr (K == 4) p1_mass_const<double>(sc, emit);
+    else p2_mass_const<double>(sc, emit);
+  }
+}
+
+template <int K, int COEF>
+__global__ void __launch_bounds__(kBlock) k_mat_mass(const MatArgs a) {
+  __shared__ __align__(16) uint8_t spos[kBlock * K * K];
+  const int64_t c0 = blockIdx.x * (int64_t)kBlock;
+  const int64_t left = a.num_cells - c0;
+  const int ncell = left < kBlock ? (int)left : kBlock;
+  stage_pos<K * K>(spos, a.pos, c0, ncell);
+  __syncthreads();
+  if ((int)threadIdx.x >= ncell) return;
+  const int64_t c = c0 + threadIdx.x;
+  const uint8_t* p = spos + threadIdx.x * K * K;
+  const double adet = cell_adet(a.x, load_geom(a.geom, c));
+  int rp[K], rd[K];
+  unsigned mr = 0, mc = 0;
+  const int32_t* d0 = a.dofs0 + c * K;
+  const int32_t* d1 = a.dofs1 + c * K;
+#pragma unroll
+  for (int i = 0; i < K; ++i) {
+    // masked rows / columns: BC dofs and dofs outside a restriction (-1)
+    const int r = __ldg(d0 + i), cc = __ldg(d1 + i);
+    rd[i] = r;
+    rp[i] = r < 0 ? 0 : __ldg(a.row_ptr + r);
+    mr |= (r < 0 || (a.bc0 && __ldg(a.bc0 + r)) ? 1u : 0u) << i;
+    mc |= (cc < 0 || (a.bc1 && __ldg(a.bc1 + cc)) ? 1u : 0u) << i;
+  }
+  double* __restrict__ vals = a.values;
+  const bool upper = a.upper != 0;
+  mass_element<K, COEF>(a.c0, c, adet, [&](int i, int j, double v) {
+    const unsigned mij = (mr >> i) | (mc >> j), mji = (mr >> j) | (mc >> i);
+    if (upper) {
+      const bool lo = i == j || rd[i] < rd[j];
+      const int slot = lo ? rp[i] + p[i * K + j] : rp[j] + p[j * K + i];
+      if (!((lo ? mij : mji) & 1u)) atomicAdd(vals + slot, v);
+      return;
+    }
+    if (!(mij & 1u)) atomicAdd(vals + rp[i] + p[i * K + j], v);
+    if (i != j && !(mji & 1u)) atomicAdd(vals + rp[j] + p[j * K + i], v);
+  });
+}
+
+// ---------------------------------------------------------------------------
 // P3 stiffness (20 dofs, 210 unique entries), one thread per cell, FP64
 // atomics.  The 400-byte map rows of a 64-cell tile are staged in shared
 // memory with a one-word pad per cell (101 words apart: consecutive threads
@@ -902,6 +977,29 @@ __global__ void __launch_bounds__(kBlockP3) k_lift_p3(const LiftArgs a) {
   for (int i = 0; i < 20; ++i) add_guarded(a.b, __ldg(d0 + i), a.num_values, -a.scale * be[i]);
 }
 
+template <int K, int COEF>
+__global__ void __launch_bounds__(kBlock) k_lift_mass(const LiftArgs a) {
+  const int64_t t = blockIdx.x * (int64_t)kBlock + threadIdx.x;
+  if (t >= a.num_list) return;
+  const int64_t c = a.cells[t];
+  const double adet = cell_adet(a.x, load_geom(a.geom, c));
+  double dv[K], be[K];
+  const int32_t* d0 = a.dofs0 + c * K;
+  const int32_t* d1 = a.dofs1 + c * K;
+#pragma unroll
+  for (int j = 0; j < K; ++j) {
+    const int C = __ldg(d1 + j);
+    dv[j] = C >= 0 && __ldg(a.bc1 + C) ? (__ldg(a.g + C) - (a.x0 ? __ldg(a.x0 + C) : 0.0)) : 0.0;
+    be[j] = 0.0;
+  }
+  mass_element<K, COEF>(a.c0, c, adet, [&](int i, int j, double v) {
+    be[i] += v * dv[j];
+    if (i != j) be[j] += v * dv[i];
+  });
+#pragma unroll
+  for (int i = 0; i < K; ++i) add_guarded(a.b, __ldg(d0 + i), a.num_values, -a.scale * be[i]);
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kBlock) k_lift_vp2(const LiftArgs a) {
   const int64_t t = blockIdx.x * (int64_t)kBlock + threadIdx.x;
@@ -1028,6 +1126,17 @@ __global__ void __launch_bounds__(kBlock) k_diag_vp2(const DiagArgs a) {
   });
 }
 
+template <int K, int COEF>
+__global__ void __launch_bounds__(kBlock) k_diag_mass(const DiagArgs a) {
+  const int64_t c = blockIdx.x * (int64_t)kBlock + threadIdx.x;
+  if (c >= a.num_cells) return;
+  const double adet = cell_adet(a.x, load_geom(a.geom, c));
+  const int32_t* d = a.dofs + c * K;
+  mass_element<K, COEF>(a.c0, c, adet, [&](int i, int j, double v) {
+    if (i == j) add_guarded(a.b, __ldg(d + i), a.num_values, v);
+  });
+}
+
 __global__ void k_mark_cells(const int32_t* __restrict__ dofs, int64_t num_cells, int k, int bs,
                              const uint8_t* __restrict__ markers, int32_t* __restrict__ out,
                              unsigned long long* count) {
@@ -1147,6 +1256,14 @@ void launch_matrix_atomic(const MatLaunch& L, cudaStream_t s) {
     case FE_FORM_VP2_ELASTICITY:
       if (f32) k_mat_vp2_atomic<float><<<grid, kBlock, 0, s>>>(a);
       else k_mat_vp2_atomic<double><<<grid, kBlock, 0, s>>>(a);
+      break;
+    case FE_FORM_P1_MASS:
+      if (a.c0.kind == FE_COEFF_P1) k_mat_mass<4, FE_COEFF_P1><<<grid, kBlock, 0, s>>>(a);
+      else k_mat_mass<4, FE_COEFF_DG0><<<grid, kBlock, 0, s>>>(a);
+      break;
+    case FE_FORM_P2_MASS:
+      if (a.c0.kind == FE_COEFF_P1) k_mat_mass<10, FE_COEFF_P1><<<grid, kBlock, 0, s>>>(a);
+      else k_mat_mass<10, FE_COEFF_DG0><<<grid, kBlock, 0, s>>>(a);
       break;
     case FE_FORM_P3_STIFFNESS: {
       // one thread per cell: splitting a cell's 210 entries over 2, 4 or 8
@@ -1341,6 +1458,14 @@ void launch_lifting(const LiftLaunch& L, cudaStream_t s) {
       if (f32) k_lift_vp2<float><<<grid, kBlock, 0, s>>>(a);
       else k_lift_vp2<double><<<grid, kBlock, 0, s>>>(a);
       break;
+    case FE_FORM_P1_MASS:
+      if (a.c0.kind == FE_COEFF_P1) k_lift_mass<4, FE_COEFF_P1><<<grid, kBlock, 0, s>>>(a);
+      else k_lift_mass<4, FE_COEFF_DG0><<<grid, kBlock, 0, s>>>(a);
+      break;
+    case FE_FORM_P2_MASS:
+      if (a.c0.kind == FE_COEFF_P1) k_lift_mass<10, FE_COEFF_P1><<<grid, kBlock, 0, s>>>(a);
+      else k_lift_mass<10, FE_COEFF_DG0><<<grid, kBlock, 0, s>>>(a);
+      break;
     case FE_FORM_P3_STIFFNESS: {
       const unsigned g3 = grid_for(L.num_list, kBlockP3);
       if (f32) k_lift_p3<float><<<g3, kBlockP3, 0, s>>>(a);
@@ -1389,9 +1514,17 @@ void launch_diagonal(const MatLaunch& L, double* b, int64_t num_values, cudaStre
       if (f32) k_diag_vp2<float><<<grid, kBlock, 0, s>>>(a);
       else k_diag_vp2<double><<<grid, kBlock, 0, s>>>(a);
       break;
+    case FE_FORM_P1_MASS:
+      if (a.c0.kind == FE_COEFF_P1) k_diag_mass<4, FE_COEFF_P1><<<grid, kBlock, 0, s>>>(a);
+      else k_diag_mass<4, FE_COEFF_DG0><<<grid, kBlock, 0, s>>>(a);
+      break;
+    case FE_FORM_P2_MASS:
+      if (a.c0.kind == FE_COEFF_P1) k_diag_mass<10, FE_COEFF_P1><<<grid, kBlock, 0, s>>>(a);
+      else k_diag_mass<10, FE_COEFF_DG0><<<grid, kBlock, 0, s>>>(a);
+      break;
     default:
-      FE_FAIL(FE_ERR_ARG, "the diagonal is offered for the cell bilinear forms (P1/P2/P3 stiffness, vector-P2 "
-                          "elasticity), not kind " + std::to_string(L.kind));
+      FE_FAIL(FE_ERR_ARG, "the diagonal is offered for the cell bilinear forms (P1/P2/P3 stiffness, P1/P2 mass, "
+                          "vector-P2 elasticity), not kind " + std::to_string(L.kind));
   }
   FE_CUDA(cudaGetLastError());
 }

@@ -360,8 +360,50 @@ def gen() -> str:
                 exprs[(i, j)] = sum_expr('W', terms, 2)
         w(full_body(exprs, 10) if full else symmetric_body(exprs, 10))
         w("}\n\n")
+    w(mass_tables())
     w(facet_tables())
     w("}  // namespace fe\n")
+    return "".join(out)
+
+
+def plain_symmetric_body(exprs):
+    """Body emitting the unique entries i <= j from their expressions in
+    every precision (mass blocks have no zero row sums to preserve)."""
+    return "".join(f"  emit({i}, {j}, {e});\n" for (i, j), e in exprs.items())
+
+
+def mass_tables() -> str:
+    """Mass matrices c*u*v*dx of P1 and P2 with a cellwise-constant or a P1
+    coefficient, from the exact reference integrals (reference volume 1/6):
+    const: s = c |det J|, entry = s int_ref phi_i phi_j;
+    P1:    cq[m] = c_m |det J|, entry = sum_m cq[m] int_ref lambda_m phi_i phi_j."""
+    out = []
+    w = out.append
+    for name, basis in (("p1", LAM), ("p2", PHI)):
+        n = len(basis)
+        uniq = [(i, j) for i in range(n) for j in range(i, n)]
+        w(f"// {name.upper()} mass, cellwise-constant coefficient: s = c * |det J|; emit(i, j, value), i <= j.\n")
+        w("template <typename T, typename Emit>\n")
+        w(f"__device__ __forceinline__ void {name}_mass_const(T s, Emit&& emit) {{\n")
+        exprs = {}
+        for (i, j) in uniq:
+            c = pint(pmul(basis[i], basis[j]))
+            exprs[(i, j)] = f"s * T({lit(c)})" if c != 0 else "T(0)"
+        w(plain_symmetric_body(exprs))
+        w("}\n")
+        w(f"// {name.upper()} mass, P1 coefficient: cq[m] = c_m * |det J|.\n")
+        w("template <typename T, typename Emit>\n")
+        w(f"__device__ __forceinline__ void {name}_mass_p1coef(const T* cq, Emit&& emit) {{\n")
+        exprs = {}
+        for (i, j) in uniq:
+            terms = []
+            for m in range(4):
+                c = pint(pmul(LAM[m], pmul(basis[i], basis[j])))
+                if c != 0:
+                    terms.append((m, c))
+            exprs[(i, j)] = sum_expr("cq", terms, 2)
+        w(plain_symmetric_body(exprs))
+        w("}\n\n")
     return "".join(out)
 
 

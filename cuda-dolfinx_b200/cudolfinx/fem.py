@@ -350,6 +350,16 @@ def stiffness(V: FunctionSpace, k: Coefficient = 1.0, precision: str = "fp64",
     return FormSpec(kind, V, [k], 2, precision, W=_trial(V, trial))
 
 
+def mass(V: FunctionSpace, c: Coefficient = 1.0, trial: Optional[FunctionSpace] = None) -> FormSpec:
+    """c * u * v * dx on a scalar P1/P2 space; c constant, DG0 or a scalar P1
+    Function (FP64 element tensors; u from ``trial`` as for ``stiffness``).
+    The P1 mass and stiffness share their pattern, so M + dt K assembles into
+    one matrix (the second call with zero=False)."""
+    if V.bs != 1 or V.family != "P" or V.degree not in (1, 2):
+        raise ValueError("mass needs a scalar P1 or P2 space")
+    return FormSpec("P1_MASS" if V.degree == 1 else "P2_MASS", V, [c], 2, "fp64", W=_trial(V, trial))
+
+
 def elasticity(V: FunctionSpace, lam: Coefficient, mu: Coefficient, precision: str = "fp64",
                trial: Optional[FunctionSpace] = None) -> FormSpec:
     """2 mu eps(u):eps(v) + lam div(u) div(v) on a vector P2 space (u from

@@ -162,6 +162,18 @@ def ref_grad_tensor(degree: int, weighted: bool):
 
 
 @lru_cache(maxsize=None)
+def ref_mass_tensor(degree: int, weighted: bool):
+    """M0[i,j] = int_ref phi_i phi_j (weighted=False), shape (k,k);
+    M[m,i,j] = int_ref lambda_m phi_i phi_j (weighted=True), (4,k,k)."""
+    phi = _basis(degree)
+    k = len(phi)
+    if not weighted:
+        return np.array([[float(_pint(_pmul(phi[i], phi[j]))) for j in range(k)] for i in range(k)])
+    return np.array([[[float(_pint(_pmul(_LAMBDA[m], _pmul(phi[i], phi[j])))) for j in range(k)]
+                      for i in range(k)] for m in range(4)])
+
+
+@lru_cache(maxsize=None)
 def ref_basis_integrals(degree: int):
     """w_i = int_ref phi_i  (reference volume 1/6)."""
     return np.array([float(_pint(p)) for p in _basis(degree)])
@@ -514,6 +526,20 @@ def p3_stiffness(coords, cells, k_dg0=None):
     if k_dg0 is not None:
         Ae = Ae * np.asarray(k_dg0)[:, None, None]
     return Ae
+
+
+def mass_matrices(coords, cells, degree, c_dg0=None, c_vertex=None):
+    """Ae [C,k,k] of c * u * v * dx on P1/P2: c = 1, DG0 per cell (``c_dg0``) or
+    a P1 field given by its 4 vertex values per cell (``c_vertex`` [C,4]).
+    The reference assembles such forms from FFCx kernels
+    (CUDAFormIntegral.cpp:1103-1226); here the reference mass tensors are
+    integrated exactly."""
+    _, det, _ = cell_geometry(coords, cells)
+    adet = np.abs(det)
+    if c_vertex is not None:
+        return np.einsum("c,cm,mij->cij", adet, np.asarray(c_vertex), ref_mass_tensor(degree, True), optimize=True)
+    c = adet if c_dg0 is None else adet * np.asarray(c_dg0)
+    return c[:, None, None] * ref_mass_tensor(degree, False)[None]
 
 
 def p3_load_dg0(coords, cells, f_cell):

@@ -491,3 +491,52 @@ def test_diagonal_part_is_the_diagonal_of_the_matrix_without_bcs(kind):
     d = fo.assemble_diagonal(Ae, dofs, P["ndof"] * bs, bs)
     assert np.allclose(d, A[fo.diag_positions(rp, col)], rtol=1e-14, atol=0)
     assert np.all(d > 0)  # an SPD operator's diagonal
+
+
+def _collapsed_gauss(q=6):
+    """Points/weights on the reference tet from a tensor Gauss rule on the cube
+    (x = u, y = v (1-u), z = w (1-u)(1-v)), exact for polynomials of degree
+    <= 2q - 3 -- independent of the exact monomial integration."""
+    t, w = np.polynomial.legendre.leggauss(q)
+    t, w = 0.5 * (t + 1.0), 0.5 * w
+    U, V, W = np.meshgrid(t, t, t, indexing="ij")
+    WU, WV, WW = np.meshgrid(w, w, w, indexing="ij")
+    x = U
+    y = V * (1 - U)
+    z = W * (1 - U) * (1 - V)
+    wt = WU * WV * WW * (1 - U) ** 2 * (1 - V)
+    return np.stack([x.ravel(), y.ravel(), z.ravel()], axis=1), wt.ravel()
+
+
+def _eval_poly(p, X):
+    return sum(float(v) * X[:, 0] ** k[0] * X[:, 1] ** k[1] * X[:, 2] ** k[2] for k, v in p.items())
+
+
+@pytest.mark.parametrize("degree", [1, 2])
+def test_mass_tensors_match_an_independent_quadrature(degree):
+    X, w = _collapsed_gauss()
+    phi = np.array([_eval_poly(p, X) for p in fo._basis(degree)])
+    lam = np.array([_eval_poly(p, X) for p in fo._LAMBDA])
+    M0 = np.einsum("iq,jq,q->ij", phi, phi, w)
+    M = np.einsum("mq,iq,jq,q->mij", lam, phi, phi, w)
+    assert np.allclose(fo.ref_mass_tensor(degree, False), M0, rtol=0, atol=1e-15)
+    assert np.allclose(fo.ref_mass_tensor(degree, True), M, rtol=0, atol=1e-15)
+    assert abs(fo.ref_mass_tensor(degree, False).sum() - 1.0 / 6.0) < 1e-15  # partition of unity
+    if degree == 1:
+        expect = (np.ones((4, 4)) + np.eye(4)) / 120.0  # int lambda_i lambda_j = (1 + delta_ij) |T| / 20
+        assert np.allclose(fo.ref_mass_tensor(1, False), expect, rtol=0, atol=1e-17)
+
+
+def test_mass_matrix_reproduces_l2_norms_of_polynomials():
+    # u in the space: u^T M u = int u^2 over the unit cube, on a jittered mesh
+    coords, cells = fo.unit_cube_tet_mesh(3, jitter=0.2, seed=4)
+    x, y, z = coords[:, 0], coords[:, 1], coords[:, 2]
+    u = 1.0 + x - 2.0 * y + 3.0 * z
+    Ae = fo.mass_matrices(coords, cells, 1)
+    rp, col = fo.sparsity(cells, cells, len(coords))
+    M = fo.assemble_matrix(Ae, cells, cells, rp, col)
+    import scipy.sparse as sp
+    Ms = sp.csr_matrix((M, col, rp), shape=(len(coords), len(coords)))
+    # int_[0,1]^3 (1 + x - 2y + 3z)^2 = 1 + (1+4+9)/3 + 2*(1-2+3)/2 + 2*(-2+3-6)/4 = 6.4166...
+    exact = 1 + 14 / 3 + 2 + 2 * (1 * -2 + 1 * 3 + -2 * 3) / 4
+    assert abs(u @ (Ms @ u) - exact) < 1e-12 * exact
