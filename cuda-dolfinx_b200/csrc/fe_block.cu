@@ -77,7 +77,9 @@ struct BlockArgs {
   double* __restrict__ values;
   const int32_t* __restrict__ gvert_ptr;   // P1: [nblocks+1] block geometry nodes
   const double* __restrict__ gx;           // P1: their coordinates, block by block
-  const uint16_t* __restrict__ glocal;     // P1: [cells][4] block-local node of each vertex
+  const uint16_t* __restrict__ glocal;     // P1: [records][4] block-local node of each vertex
+  const int32_t* __restrict__ rec_ptr;     // P1: [nblocks+1] record offsets (lrow, pos, glocal,
+                                           // cell_id and dofs1 are indexed by record)
 };
 
 __device__ __forceinline__ void block_geom(const double* __restrict__ x, int4 v, double K[3][3], double& adet) {
@@ -289,7 +291,10 @@ struct P1Smem {
   static constexpr size_t OFF_RMASK = OFF_WROW + sizeof(uint16_t) * kP1Wcap;
   static constexpr size_t OFF_CMASK = OFF_RMASK + Tr::RCAP;
   static constexpr size_t OFF_X = (OFF_CMASK + Tr::RCAP + 15) / 16 * 16;
-  static constexpr size_t SMEM = OFF_X + sizeof(double) * 3 * Tr::VCAP;
+  // per window row: window offset | row BC bit 30 | column BC bit 31 (one
+  // shared-memory load per local dof instead of three)
+  static constexpr size_t OFF_RINFO = OFF_X + sizeof(double) * 3 * Tr::VCAP;
+  static constexpr size_t SMEM = OFF_RINFO + sizeof(uint32_t) * Tr::RCAP;
 };
 
 __global__ void __launch_bounds__(BlockTraits<FE_FORM_P1_STIFFNESS>::NT, 4) k_block_p1(const BlockArgs a,
@@ -306,6 +311,7 @@ __global__ void __launch_bounds__(BlockTraits<FE_FORM_P1_STIFFNESS>::NT, 4) k_bl
   uint8_t* s_rmask = smem + S::OFF_RMASK;
   uint8_t* s_cmask = smem + S::OFF_CMASK;
   double* s_x = reinterpret_cast<double*>(smem + S::OFF_X);
+  uint32_t* s_rinfo = reinterpret_cast<uint32_t*>(smem + S::OFF_RINFO);
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int32_t b = blockIdx.x;
@@ -320,6 +326,7 @@ __global__ void __launch_bounds__(BlockTraits<FE_FORM_P1_STIFFNESS>::NT, 4) k_bl
     if (r == nrows - 1) s_soff[nrows] = so + len;
     s_rmask[r] = a.bc0 ? a.bc0[R] : 0;
     s_cmask[r] = (square && a.bc1) ? a.bc1[R] : 0;
+    s_rinfo[r] = (uint32_t)so | (s_rmask[r] ? 1u << 30 : 0u) | (s_cmask[r] ? 1u << 31 : 0u);
     for (int e = 0; e < len; ++e) s_wrow[so + e] = (uint16_t)r;
   }
   {
@@ -336,9 +343,13 @@ __global__ void __launch_bounds__(BlockTraits<FE_FORM_P1_STIFFNESS>::NT, 4) k_bl
     w0[q] = 0u;
     w1[q] = 0u;
   }
+  // records of this block: cell q = lane*span + slot sits at rec0 + slot*32 + lane
+  const int span = (ncells + 31) / 32;
+  const int32_t rec0 = a.rec_ptr[b];
   if (a.coef_kind != FE_COEFF_CONSTANT) {
-    for (int q = tid; q < ncells; q += NT)
-      atomicMax(&s_bmax, __float_as_uint((float)(cell_coef_factor(a, c0 + q) * 1.0625)));
+    for (int t = tid; t < span * 32; t += NT)
+      if ((t & 31) * span + (t >> 5) < ncells)
+        atomicMax(&s_bmax, __float_as_uint((float)(cell_coef_factor(a, rec0 + t) * 1.0625)));
   }
   __syncthreads();
   const double kfac = a.coef_kind != FE_COEFF_CONSTANT ? (double)__uint_as_float(s_bmax) : fabs(a.coef_const);
@@ -350,12 +361,12 @@ __global__ void __launch_bounds__(BlockTraits<FE_FORM_P1_STIFFNESS>::NT, 4) k_bl
   constexpr double kMagic = 6755399441055744.0;  // 1.5 * 2^52: v + kMagic holds round(v) in its low bits
 
   // lane l of warp w takes cells l*span + w, l*span + w + NW, ...: the 32
-  // cells of one warp instruction lie span cells apart along the curve
-  const int span = (ncells + 31) / 32;
+  // cells of one warp instruction lie span cells apart along the curve, and
+  // their records are consecutive
   for (int slot = warp; slot < span; slot += NW) {
     const int q = lane * span + slot;
     if (q >= ncells) continue;
-    const int64_t cb = c0 + q;
+    const int64_t cb = rec0 + slot * 32 + lane;
     const uint2 lrw = __ldg(reinterpret_cast<const uint2*>(a.lrow) + cb);
     const int lr[4] = {(int)(lrw.x & 0xffffu), (int)(lrw.x >> 16), (int)(lrw.y & 0xffffu), (int)(lrw.y >> 16)};
     const uint4 pq = __ldg(reinterpret_cast<const uint4*>(a.pos) + cb);
@@ -364,9 +375,10 @@ __global__ void __launch_bounds__(BlockTraits<FE_FORM_P1_STIFFNESS>::NT, 4) k_bl
     unsigned own = 0, cmask = 0;
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-      wbase[i] = s_soff[lr[i]];
-      own |= (s_rmask[lr[i]] ? 0u : 1u) << i;
-      if (square) cmask |= (unsigned)s_cmask[lr[i]] << i;
+      const uint32_t ri = s_rinfo[lr[i]];
+      wbase[i] = (int)(ri & 0x3fffffffu);
+      own |= (((ri >> 30) & 1u) ^ 1u) << i;
+      if (square) cmask |= (ri >> 31) << i;
       else if (a.bc1) cmask |= (a.bc1[__ldg(a.dofs1 + cb * 4 + i)] ? 1u : 0u) << i;
     }
     auto add = [&](int idx, long long w) {
@@ -627,6 +639,41 @@ std::unique_ptr<fe_form_s::BlockPlan> build_block_plan(const fe_form_s& f) {
       for (int v = 0; v < 4; ++v) cmap[p * 4 + v] = kc.map->host[c * 4 + v];
   }
 
+  // P1: the kernel's lane l takes the block's cells l*span + slot (32 cells
+  // span apart per instruction, so their window rows rarely collide); the
+  // per-cell records are stored at slot*32 + lane of the block's padded range
+  // so that each of those loads is one coalesced warp access
+  std::vector<int32_t> rec_ptr;
+  if (KIND == FE_FORM_P1_STIFFNESS) {
+    const int64_t nb = (int64_t)block_ptr.size() - 1;
+    rec_ptr.assign(nb + 1, 0);
+    for (int64_t b = 0; b < nb; ++b) {
+      const int64_t n = block_ptr[b + 1] - block_ptr[b], span = (n + 31) / 32;
+      rec_ptr[b + 1] = rec_ptr[b] + (int32_t)(span * 32);
+    }
+    const int64_t NR = rec_ptr[nb];
+    std::vector<uint16_t> lrow_r(NR * K, 0), glocal_r(NR * 4, 0);
+    std::vector<int32_t> cell_r(NR, 0), d1_r(NR * K, 0);
+    std::vector<uint8_t> pos_r(NR * KK, 0);
+    for (int64_t b = 0; b < nb; ++b) {
+      const int64_t n = block_ptr[b + 1] - block_ptr[b], span = (n + 31) / 32;
+      for (int64_t qq = 0; qq < n; ++qq) {
+        const int64_t p = block_ptr[b] + qq;
+        const int64_t r = rec_ptr[b] + (qq % span) * 32 + qq / span;
+        std::copy(lrow.begin() + p * K, lrow.begin() + (p + 1) * K, lrow_r.begin() + r * K);
+        std::copy(glocal.begin() + p * 4, glocal.begin() + (p + 1) * 4, glocal_r.begin() + r * 4);
+        std::copy(pos.begin() + p * KK, pos.begin() + (p + 1) * KK, pos_r.begin() + r * KK);
+        std::copy(d1.begin() + p * K, d1.begin() + (p + 1) * K, d1_r.begin() + r * K);
+        cell_r[r] = cell_id[p];
+      }
+    }
+    lrow.swap(lrow_r);
+    glocal.swap(glocal_r);
+    pos.swap(pos_r);
+    d1.swap(d1_r);
+    cell_id.swap(cell_r);
+  }
+
   auto P = std::make_unique<fe_form_s::BlockPlan>();
   P->nblocks = (int64_t)block_ptr.size() - 1;
   P->coef_map_owner = p1coef ? kc.map : nullptr;
@@ -654,6 +701,7 @@ std::unique_ptr<fe_form_s::BlockPlan> build_block_plan(const fe_form_s& f) {
     up(P->gvert_ptr, gvert_ptr);
     up(P->gx, gx);
     up(P->glocal, glocal);
+    up(P->rec_ptr, rec_ptr);
   }
   return P;
 }
@@ -688,6 +736,7 @@ void launch_block(const fe_form_s& f, const fe_form_s::BlockPlan& P, double* val
   a.gvert_ptr = P.gvert_ptr.p;
   a.gx = P.gx.p;
   a.glocal = P.glocal.p;
+  a.rec_ptr = P.rec_ptr.p;
   if (P.nblocks == 0) return;
   if constexpr (KIND == FE_FORM_P1_STIFFNESS) {
     constexpr size_t smem = P1Smem::SMEM;

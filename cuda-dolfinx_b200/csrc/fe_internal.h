@@ -243,6 +243,8 @@ struct fe_form_s::BlockPlan {
   fe::DevBuf<int32_t> gvert_ptr;      // [nblocks+1] into gx: each block's geometry nodes
   fe::DevBuf<double> gx;              // [block nodes][3] coordinates, block by block
   fe::DevBuf<uint16_t> glocal;        // [cells][4] block-local geometry node of each cell vertex
+  fe::DevBuf<int32_t> rec_ptr;        // P1: [nblocks+1] per-cell records of each block, padded to
+                                      // whole warps and stored in the kernel's lane order
 };
 
 struct fe_form_s::BatchPlan {
