@@ -493,7 +493,12 @@ def run_gpu(args, rank, world, local_rank):
         pass
     peak = peaks.get("hbm_gbs", 6650.0)
     achieved = alg / (mat_ms / 1e3) / 1e9
-    kernel_key = f"{args.workload}:{args.variant}"
+    # the variant "auto" resolves to (fe_assemble_matrix's default): the block
+    # kernel for P1 meshes of >= 2^20 cells, the atomic scatter otherwise
+    resolved = args.variant
+    if resolved == "auto":
+        resolved = "block" if (W["kind"] == "p1" and len(I["cells"]) >= (1 << 20)) else "atomic"
+    kernel_key = f"{args.workload}:{resolved}"
     traffic = load_traffic(kernel_key)
     out = {
         "metric": "matrix nnz/s",
@@ -514,7 +519,7 @@ def run_gpu(args, rank, world, local_rank):
                    if graph is not None else "eager steps",
                    "variant": args.variant, "l2": "inputs larger than L2 (CSR values %.2f GB)" % (8 * nnz / 1e9),
                    "parallelism": f"replicas x{world}"},
-        "roofline": {"bound": "hbm", "kernel": "matrix assembly (%s)" % args.variant,
+        "roofline": {"bound": "hbm", "kernel": "matrix assembly (%s%s)" % (args.variant, "" if resolved == args.variant else " = " + resolved),
                      "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "algorithmic_bytes": alg,
                      "kernel_ms": mat_ms, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"
