@@ -584,12 +584,13 @@ int fe_form_set_coefficient(fe_form f, int index, int coeff_kind, fe_dofmap cmap
       FE_REQUIRE(cmap && cmap->k == 4 && cmap->bs == 1 && cmap->num_cells == C && !cmap->excluded,
                  "P1 coefficient needs an unrestricted P1 dofmap");
       FE_REQUIRE(n >= cmap->num_blocks, "P1 coefficient has fewer values than dofs");
-      FE_REQUIRE(f->kind == FE_FORM_P2_STIFFNESS || f->kind == FE_FORM_P1_LOAD || f->kind == FE_FORM_P1_MASS ||
+      FE_REQUIRE(f->kind == FE_FORM_P2_STIFFNESS || f->kind == FE_FORM_P1_STIFFNESS || f->kind == FE_FORM_P1_LOAD ||
+                     f->kind == FE_FORM_P1_MASS ||
                      f->kind == FE_FORM_P2_MASS ||
                      f->kind == FE_FORM_P1_FACET_LOAD || f->kind == FE_FORM_P2_FACET_LOAD ||
                      f->kind == FE_FORM_INTEGRAL || f->kind == FE_FORM_FACET_INTEGRAL ||
                      f->kind == FE_FORM_JUMP_NORM || (f->kind == FE_FORM_P1_ENERGY && index == 1),
-                 "P1 coefficients are supported by P2 stiffness, mass, P1 load, facet load and functional forms");
+                 "P1 coefficients are supported by P1/P2 stiffness, mass, P1 load, facet load and functional forms");
     } else if (coeff_kind == FE_COEFF_P2) {
       FE_REQUIRE(f->kind == FE_FORM_P2_ENERGY && index == 1, "P2 coefficients are the u of FE_FORM_P2_ENERGY");
       FE_REQUIRE(cmap && cmap->k == 10 && cmap->bs == 1 && cmap->num_cells == C && !cmap->excluded,
@@ -598,7 +599,7 @@ int fe_form_set_coefficient(fe_form f, int index, int coeff_kind, fe_dofmap cmap
     } else {
       FE_FAIL(FE_ERR_ARG, "unknown coefficient kind " + std::to_string(coeff_kind));
     }
-    if (f->kind == FE_FORM_P1_STIFFNESS || f->kind == FE_FORM_VP2_ELASTICITY || f->kind == FE_FORM_P2_LOAD ||
+    if (f->kind == FE_FORM_VP2_ELASTICITY || f->kind == FE_FORM_P2_LOAD ||
         f->kind == FE_FORM_VP2_LOAD || f->kind == FE_FORM_P1_FACET_MASS || f->kind == FE_FORM_P2_FACET_MASS ||
         f->kind == FE_FORM_VP2_FACET_LOAD || f->kind == FE_FORM_P3_STIFFNESS || f->kind == FE_FORM_P3_LOAD ||
         is_ifacet_kind(f->kind))

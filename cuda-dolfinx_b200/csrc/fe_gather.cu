@@ -216,7 +216,14 @@ __global__ void k_elem_p1(const ElemArgs a) {
     G[3][b] = g.K[2][b];
     G[0][b] = -(g.K[0][b] + g.K[1][b] + g.K[2][b]);
   }
-  const double s = g.adet * (1.0 / 6.0) * cellcoef(a.coef0_kind, a.c0, a.c0const, c);
+  double kc;
+  if (a.coef0_kind == FE_COEFF_P1) {  // P1 coefficient: its cell mean (constant gradients)
+    const int4 km = __ldg(reinterpret_cast<const int4*>(a.c0map) + c);
+    kc = 0.25 * ((__ldg(a.c0 + km.x) + __ldg(a.c0 + km.y)) + (__ldg(a.c0 + km.z) + __ldg(a.c0 + km.w)));
+  } else {
+    kc = cellcoef(a.coef0_kind, a.c0, a.c0const, c);
+  }
+  const double s = g.adet * (1.0 / 6.0) * kc;
   const int64_t N = a.num_cells;
 #pragma unroll
   for (int i = 0; i < 4; ++i)

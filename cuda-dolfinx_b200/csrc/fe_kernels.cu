@@ -52,6 +52,16 @@ __device__ __forceinline__ double coef_cell(const CoefDev& k, int64_t c) {
   return k.kind == FE_COEFF_DG0 ? __ldg(k.v + c) : k.c[0];
 }
 
+// mean over the cell of a constant / DG0 / P1 coefficient (the exact factor of
+// a P1 stiffness entry: the gradients are constant on the cell)
+__device__ __forceinline__ double coef_mean(const CoefDev& k, int64_t c) {
+  if (k.kind == FE_COEFF_P1) {
+    const int4 m = __ldg(reinterpret_cast<const int4*>(k.map) + c);
+    return 0.25 * ((__ldg(k.v + m.x) + __ldg(k.v + m.y)) + (__ldg(k.v + m.z) + __ldg(k.v + m.w)));
+  }
+  return coef_cell(k, c);
+}
+
 // ---------------------------------------------------------------------------
 // Geometry of an affine tetrahedron: K = J^{-1}, |det J|
 // ---------------------------------------------------------------------------
@@ -146,7 +156,7 @@ __global__ void __launch_bounds__(kBlock) k_mat_p1_atomic(const MatArgs a) {
   cell_geometry(a.x, load_geom(a.geom, c), g);
   double G[4][3];
   p1_grads(g, G);
-  const double s = g.adet * (1.0 / 6.0) * coef_cell(a.c0, c);
+  const double s = g.adet * (1.0 / 6.0) * coef_mean(a.c0, c);
   const int4 d0 = __ldg(reinterpret_cast<const int4*>(a.dofs0) + c);
   const int4 d1 = (a.dofs1 == a.dofs0) ? d0 : __ldg(reinterpret_cast<const int4*>(a.dofs1) + c);
   const int r[4] = {d0.x, d0.y, d0.z, d0.w};
@@ -886,7 +896,7 @@ __global__ void __launch_bounds__(kBlock) k_lift_p1(const LiftArgs a) {
   cell_geometry(a.x, load_geom(a.geom, c), g);
   double G[4][3];
   p1_grads(g, G);
-  const double s = g.adet * (1.0 / 6.0) * coef_cell(a.c0, c);
+  const double s = g.adet * (1.0 / 6.0) * coef_mean(a.c0, c);
   const int4 d0 = __ldg(reinterpret_cast<const int4*>(a.dofs0) + c);
   const int4 d1 = __ldg(reinterpret_cast<const int4*>(a.dofs1) + c);
   const int r[4] = {d0.x, d0.y, d0.z, d0.w};
@@ -1056,7 +1066,7 @@ __global__ void __launch_bounds__(kBlock) k_diag_p1(const DiagArgs a) {
   cell_geometry(a.x, load_geom(a.geom, c), g);
   double G[4][3];
   p1_grads(g, G);
-  const double s = g.adet * (1.0 / 6.0) * coef_cell(a.c0, c);
+  const double s = g.adet * (1.0 / 6.0) * coef_mean(a.c0, c);
   const int4 d = __ldg(reinterpret_cast<const int4*>(a.dofs) + c);
   const int r[4] = {d.x, d.y, d.z, d.w};
 #pragma unroll

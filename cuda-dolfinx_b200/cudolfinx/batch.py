@@ -42,7 +42,9 @@ class VariantTuner:
     @staticmethod
     def key(a: CUDAForm) -> tuple:
         C = a._spec.mesh.num_cells
-        return (a._spec.kind, a._spec.precision, int(math.log2(max(1, C))))
+        coef = tuple(type(c).__name__ + (str(c.function_space.degree) if hasattr(c, "function_space") else "")
+                     for c in a._spec.coefficients)
+        return (a._spec.kind, a._spec.precision, coef, int(math.log2(max(1, C))))
 
     def choose(self, a: CUDAForm, mat: CUDAMatrix, bc0, bc1) -> str:
         k = self.key(a)
@@ -58,7 +60,10 @@ class VariantTuner:
                 _lib.check(_lib.lib.fe_assemble_matrix(a.cuda_form, mat.values.data_ptr(), bc0, bc1, 1.0, flags, sp),
                            "fe_assemble_matrix")
 
-            call()  # plan build
+            try:
+                call()  # plan build
+            except RuntimeError:
+                continue  # variant not offered for this form (e.g. a P1 coefficient in the block kernel)
             call()
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)

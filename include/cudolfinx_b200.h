@@ -49,7 +49,8 @@ typedef struct fe_form_s* fe_form;
 /* Built-in forms (element tensors written from the mathematics; replaces the
  * FFCx tabulate_tensor bodies wrapped by python/cudolfinx/jit.py:61-114). */
 enum fe_form_kind {
-  FE_FORM_P1_STIFFNESS = 1,    /* k*inner(grad u, grad v)*dx, P1;   coeff 0 = k    */
+  FE_FORM_P1_STIFFNESS = 1,    /* k*inner(grad u, grad v)*dx, P1;   coeff 0 = k (constant / DG0 / P1;
+                                  a P1 k enters through its cell mean, exact)      */
   FE_FORM_P2_STIFFNESS = 2,    /* k*inner(grad u, grad v)*dx, P2;   coeff 0 = k    */
   FE_FORM_VP2_ELASTICITY = 3,  /* 2mu eps(u):eps(v) + lam div u div v, vector P2;
                                   coeff 0 = lam, coeff 1 = mu                       */
