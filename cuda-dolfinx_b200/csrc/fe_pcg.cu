@@ -197,7 +197,12 @@ template <int SUB>
 void run(const fe_sparsity_s& A, const double* val, const double* b, double* x, double rtol, int max_iter,
          int* iterations, double* rel_res, cudaStream_t s) {
   const int64_t n = A.num_rows;
+  // the row kernels (k_init, k_spmv: 32 registers) wait on dependent loads
+  // (row bounds -> columns and values -> gathered entries): they run 8 CTAs
+  // per SM, the vector updates (40 registers) 4; each reduction sums the
+  // partials of the launch that wrote them
   const unsigned grid = (unsigned)(A.ctx->num_sms * 4);
+  const unsigned grid_rows = (unsigned)(A.ctx->num_sms * 8);
   double *r, *z, *p, *Ap, *dinv, *part;
   Scalars* sc;
   FE_CUDA(cudaMallocAsync((void**)&r, n * sizeof(double), s));
@@ -205,20 +210,20 @@ void run(const fe_sparsity_s& A, const double* val, const double* b, double* x, 
   FE_CUDA(cudaMallocAsync((void**)&p, n * sizeof(double), s));
   FE_CUDA(cudaMallocAsync((void**)&Ap, n * sizeof(double), s));
   FE_CUDA(cudaMallocAsync((void**)&dinv, n * sizeof(double), s));
-  FE_CUDA(cudaMallocAsync((void**)&part, 3 * grid * sizeof(double), s));
+  FE_CUDA(cudaMallocAsync((void**)&part, 3 * grid_rows * sizeof(double), s));
   FE_CUDA(cudaMallocAsync((void**)&sc, sizeof(Scalars), s));
   Scalars h{};
   h.tol2 = rtol * rtol;
   h.max_iter = max_iter;
   FE_CUDA(cudaMemcpyAsync(sc, &h, sizeof(h), cudaMemcpyHostToDevice, s));
-  k_init<SUB><<<grid, kThreads, 0, s>>>(n, A.row_ptr.p, A.col.p, val, A.diag.p, b, x, r, z, p, dinv, part);
-  k_reduce<<<1, 1024, 0, s>>>(part, grid, 0, sc);
+  k_init<SUB><<<grid_rows, kThreads, 0, s>>>(n, A.row_ptr.p, A.col.p, val, A.diag.p, b, x, r, z, p, dinv, part);
+  k_reduce<<<1, 1024, 0, s>>>(part, grid_rows, 0, sc);
   FE_CUDA(cudaGetLastError());
   const int batch = 16;
   for (int it = 0;; it += batch) {
     for (int q = 0; q < batch; ++q) {
-      k_spmv<SUB><<<grid, kThreads, 0, s>>>(n, A.row_ptr.p, A.col.p, val, p, Ap, part, sc);
-      k_reduce<<<1, 1024, 0, s>>>(part, grid, 1, sc);
+      k_spmv<SUB><<<grid_rows, kThreads, 0, s>>>(n, A.row_ptr.p, A.col.p, val, p, Ap, part, sc);
+      k_reduce<<<1, 1024, 0, s>>>(part, grid_rows, 1, sc);
       k_update<<<grid, kThreads, 0, s>>>(n, x, r, z, p, Ap, dinv, part, sc);
       k_reduce<<<1, 1024, 0, s>>>(part, grid, 2, sc);
       k_update_p<<<grid, kThreads, 0, s>>>(n, z, p, sc);

@@ -67,9 +67,12 @@ class _DeviceBC:
         return r
 
     def __del__(self):
-        if getattr(self, "handle", None):
-            _lib.release("fe_bc_destroy", self.handle)
+        h = getattr(self, "handle", None)
+        if h:
             self.handle = None
+            release = getattr(_lib, "release", None)  # None during interpreter teardown
+            if release is not None:
+                release("fe_bc_destroy", h)
 
 
 class _RestrictedBC:
@@ -94,9 +97,12 @@ class _RestrictedBC:
         _lib.check(_lib.lib.fe_bc_update(self.handle, self.g.ctypes.data, self.parent.ctx.stream()), "fe_bc_update")
 
     def __del__(self):
-        if getattr(self, "handle", None):
-            _lib.release("fe_bc_destroy", self.handle)
+        h = getattr(self, "handle", None)
+        if h:
             self.handle = None
+            release = getattr(_lib, "release", None)  # None during interpreter teardown
+            if release is not None:
+                release("fe_bc_destroy", h)
 
 
 class CUDADirichletBC:

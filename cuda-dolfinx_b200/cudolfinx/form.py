@@ -40,9 +40,12 @@ class DeviceMesh:
         self.handle = h.value
 
     def __del__(self):
-        if getattr(self, "handle", None):
-            _lib.release("fe_mesh_destroy", self.handle)
+        h = getattr(self, "handle", None)
+        if h:
             self.handle = None
+            release = getattr(_lib, "release", None)  # None during interpreter teardown
+            if release is not None:
+                release("fe_mesh_destroy", h)
 
 
 class DeviceDofMap:
@@ -79,9 +82,12 @@ class DeviceDofMap:
         return self.num_blocks * self.V.bs
 
     def __del__(self):
-        if getattr(self, "handle", None):
-            _lib.release("fe_dofmap_destroy", self.handle)
+        h = getattr(self, "handle", None)
+        if h:
             self.handle = None
+            release = getattr(_lib, "release", None)  # None during interpreter teardown
+            if release is not None:
+                release("fe_dofmap_destroy", h)
 
 
 def _create_mesh_on_device(ctx, mesh) -> DeviceMesh:
@@ -332,9 +338,12 @@ class CUDAForm:
         return self._part
 
     def __del__(self):
-        if getattr(self, "_handle", None):
-            _lib.release("fe_form_destroy", self._handle)
+        h = getattr(self, "_handle", None)
+        if h:
             self._handle = None
+            release = getattr(_lib, "release", None)  # None during interpreter teardown
+            if release is not None:
+                release("fe_form_destroy", h)
 
 
 class BlockCUDAForm:

@@ -94,9 +94,12 @@ class Sparsity:
                 _DeviceView(cl.value, self.nnz, "<i4", self).tensor())
 
     def __del__(self):
-        if getattr(self, "handle", None):
-            _lib.release("fe_sparsity_destroy", self.handle)
+        h = getattr(self, "handle", None)
+        if h:
             self.handle = None
+            release = getattr(_lib, "release", None)  # None during interpreter teardown
+            if release is not None:
+                release("fe_sparsity_destroy", h)
 
 
 class _DeviceView:
