@@ -71,6 +71,7 @@ int form_rank(int kind) {
     case FE_FORM_P2_STIFFNESS:
     case FE_FORM_P1_MASS:
     case FE_FORM_P2_MASS:
+    case FE_FORM_VP2_MASS:
     case FE_FORM_VP2_ELASTICITY:
     case FE_FORM_P1_FACET_MASS:
     case FE_FORM_P2_FACET_MASS:
@@ -586,7 +587,7 @@ int fe_form_set_coefficient(fe_form f, int index, int coeff_kind, fe_dofmap cmap
       FE_REQUIRE(n >= cmap->num_blocks, "P1 coefficient has fewer values than dofs");
       FE_REQUIRE(f->kind == FE_FORM_P2_STIFFNESS || f->kind == FE_FORM_P1_STIFFNESS || f->kind == FE_FORM_P1_LOAD ||
                      f->kind == FE_FORM_P1_MASS ||
-                     f->kind == FE_FORM_P2_MASS ||
+                     f->kind == FE_FORM_P2_MASS || f->kind == FE_FORM_VP2_MASS ||
                      f->kind == FE_FORM_P1_FACET_LOAD || f->kind == FE_FORM_P2_FACET_LOAD ||
                      f->kind == FE_FORM_INTEGRAL || f->kind == FE_FORM_FACET_INTEGRAL ||
                      f->kind == FE_FORM_JUMP_NORM || (f->kind == FE_FORM_P1_ENERGY && index == 1),
@@ -874,7 +875,7 @@ int fe_assemble_matrix(fe_form a, double* values, fe_bc bc0, fe_bc bc1, double d
       return;
     }
     // default: the block variant for P1 meshes above ~1M cells (measured faster
-    // on B200 at 12.6M cells: 0.80 vs 0.86 ms), the FP64-atomic scatter otherwise
+    // on B200 at 12.6M cells: 0.54 vs 0.73 ms), the FP64-atomic scatter otherwise
     const bool auto_block = !(flags & FE_ASM_ATOMIC) && !view && a->kind == FE_FORM_P1_STIFFNESS &&
                             a->mesh->num_cells >= (int64_t(1) << 20);
     const bool want_block = (flags & FE_ASM_BLOCK) || auto_block;
@@ -894,7 +895,8 @@ int fe_assemble_matrix(fe_form a, double* values, fe_bc bc0, fe_bc bc1, double d
     // so it keeps both reductions, as does FE_ASM_FULL_SCATTER for every form.
     const bool upper = zero && !view && !(flags & FE_ASM_FULL_SCATTER) &&
                        (a->kind == FE_FORM_VP2_ELASTICITY || a->kind == FE_FORM_P3_STIFFNESS ||
-                        a->kind == FE_FORM_P1_STIFFNESS || a->kind == FE_FORM_P1_MASS) && a->V0 == a->V1 &&
+                        a->kind == FE_FORM_P1_STIFFNESS || a->kind == FE_FORM_P1_MASS ||
+                        a->kind == FE_FORM_VP2_MASS) && a->V0 == a->V1 &&
                        bc0 == bc1 && ensure_mirror(*a->sp, st, a->V0->bs);
     if (zero) launch_zero(values, a->sp->nnz, st);
     MatLaunch L{};

@@ -261,6 +261,35 @@ __global__ void k_elem_mass(const ElemArgs a) {
   }
 }
 
+// vector-P2 mass: all 900 entries (the gather reads every entry), zero
+// between different components
+template <int COEF>
+__global__ void k_elem_vmass(const ElemArgs a) {
+  const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (c >= a.num_cells) return;
+  Geo g;
+  geo(a.x, a.geom, c, g);
+  const int64_t N = a.num_cells;
+  double* __restrict__ E = a.E;
+  for (int e = 0; e < 900; ++e) E[e * N + c] = 0.0;
+  auto emit = [&](int i, int j, double v) {
+#pragma unroll
+    for (int ca = 0; ca < 3; ++ca) {
+      const int ii = 3 * i + ca, jj = 3 * j + ca;
+      E[(ii * 30 + jj) * N + c] = v;
+      if (ii != jj) E[(jj * 30 + ii) * N + c] = v;
+    }
+  };
+  if constexpr (COEF == FE_COEFF_P1) {
+    const int4 km = __ldg(reinterpret_cast<const int4*>(a.c0map) + c);
+    const double cq[4] = {g.adet * __ldg(a.c0 + km.x), g.adet * __ldg(a.c0 + km.y), g.adet * __ldg(a.c0 + km.z),
+                          g.adet * __ldg(a.c0 + km.w)};
+    p2_mass_p1coef<double>(cq, emit);
+  } else {
+    p2_mass_const<double>(g.adet * cellcoef(a.coef0_kind, a.c0, a.c0const, c), emit);
+  }
+}
+
 template <int COEF, typename T>
 __global__ void k_elem_p2(const ElemArgs a) {
   const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -462,6 +491,10 @@ void assemble_matrix_gather(fe_form_s& f, double* values, const fe_bc_s* bc0, co
       case FE_FORM_P2_MASS:
         if (ea.coef0_kind == FE_COEFF_P1) k_elem_mass<10, FE_COEFF_P1><<<grid, 128, 0, s>>>(ea);
         else k_elem_mass<10, FE_COEFF_DG0><<<grid, 128, 0, s>>>(ea);
+        break;
+      case FE_FORM_VP2_MASS:
+        if (ea.coef0_kind == FE_COEFF_P1) k_elem_vmass<FE_COEFF_P1><<<grid, 128, 0, s>>>(ea);
+        else k_elem_vmass<FE_COEFF_DG0><<<grid, 128, 0, s>>>(ea);
         break;
       case FE_FORM_P3_STIFFNESS:
         if (f.precision == FE_PREC_FP32) k_elem_p3<float><<<grid, 128, 0, s>>>(ea);

@@ -335,6 +335,57 @@ __global__ void __launch_bounds__(kBlock) k_mat_mass(const MatArgs a) {
   });
 }
 
+// vector-P2 mass rho*inner(u, v)*dx: component a of node i couples with
+// component a of node j only, by the scalar P2 mass entry
+template <int COEF>
+__global__ void __launch_bounds__(kBlock) k_mat_vmass(const MatArgs a) {
+  __shared__ __align__(16) uint8_t spos[kBlock * 100];
+  const int64_t c0 = blockIdx.x * (int64_t)kBlock;
+  const int64_t left = a.num_cells - c0;
+  const int ncell = left < kBlock ? (int)left : kBlock;
+  stage_pos<100>(spos, a.pos, c0, ncell);
+  __syncthreads();
+  if ((int)threadIdx.x >= ncell) return;
+  const int64_t c = c0 + threadIdx.x;
+  const uint8_t* p = spos + threadIdx.x * 100;
+  const double adet = cell_adet(a.x, load_geom(a.geom, c));
+  int rp[10], L[10], rd[10];
+  unsigned mr = 0, mc = 0;
+  const int32_t* d0 = a.dofs0 + c * 10;
+  const int32_t* d1 = a.dofs1 + c * 10;
+#pragma unroll
+  for (int i = 0; i < 10; ++i) {
+    const int R = __ldg(d0 + i);
+    const int C = __ldg(d1 + i);
+    rd[i] = R;
+    rp[i] = R < 0 ? 0 : __ldg(a.row_ptr + 3 * R);
+    L[i] = R < 0 ? 0 : __ldg(a.row_ptr + 3 * R + 1) - rp[i];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      mr |= (R < 0 || (a.bc0 && __ldg(a.bc0 + 3 * R + q)) ? 1u : 0u) << (3 * i + q);
+      mc |= (C < 0 || (a.bc1 && __ldg(a.bc1 + 3 * C + q)) ? 1u : 0u) << (3 * i + q);
+    }
+  }
+  double* __restrict__ vals = a.values;
+  const bool upper = a.upper != 0;
+  mass_element<10, COEF>(a.c0, c, adet, [&](int i, int j, double v) {
+#pragma unroll
+    for (int ca = 0; ca < 3; ++ca) {
+      const int ri = 3 * rd[i] + ca, rj = 3 * rd[j] + ca;
+      const unsigned mij = (mr >> (3 * i + ca)) | (mc >> (3 * j + ca));
+      const unsigned mji = (mr >> (3 * j + ca)) | (mc >> (3 * i + ca));
+      if (upper) {
+        const bool lo = ri <= rj;
+        const int slot = lo ? rp[i] + ca * L[i] + 3 * p[i * 10 + j] + ca : rp[j] + ca * L[j] + 3 * p[j * 10 + i] + ca;
+        if (!((lo ? mij : mji) & 1u)) atomicAdd(vals + slot, v);
+        continue;
+      }
+      if (!(mij & 1u)) atomicAdd(vals + rp[i] + ca * L[i] + 3 * p[i * 10 + j] + ca, v);
+      if (i != j && !(mji & 1u)) atomicAdd(vals + rp[j] + ca * L[j] + 3 * p[j * 10 + i] + ca, v);
+    }
+  });
+}
+
 // ---------------------------------------------------------------------------
 // P3 stiffness (20 dofs, 210 unique entries), one thread per cell, FP64
 // atomics.  The 400-byte map rows of a 64-cell tile are staged in shared
@@ -1010,6 +1061,40 @@ __global__ void __launch_bounds__(kBlock) k_lift_mass(const LiftArgs a) {
   for (int i = 0; i < K; ++i) add_guarded(a.b, __ldg(d0 + i), a.num_values, -a.scale * be[i]);
 }
 
+template <int COEF>
+__global__ void __launch_bounds__(kBlock) k_lift_vmass(const LiftArgs a) {
+  const int64_t t = blockIdx.x * (int64_t)kBlock + threadIdx.x;
+  if (t >= a.num_list) return;
+  const int64_t c = a.cells[t];
+  const double adet = cell_adet(a.x, load_geom(a.geom, c));
+  double dv[30], be[30];
+  const int32_t* d0 = a.dofs0 + c * 10;
+  const int32_t* d1 = a.dofs1 + c * 10;
+#pragma unroll
+  for (int j = 0; j < 10; ++j) {
+    const int64_t C = __ldg(d1 + j);
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      const int64_t s = 3 * C + q;
+      dv[3 * j + q] = C >= 0 && __ldg(a.bc1 + s) ? (__ldg(a.g + s) - (a.x0 ? __ldg(a.x0 + s) : 0.0)) : 0.0;
+      be[3 * j + q] = 0.0;
+    }
+  }
+  mass_element<10, COEF>(a.c0, c, adet, [&](int i, int j, double v) {
+#pragma unroll
+    for (int ca = 0; ca < 3; ++ca) {
+      be[3 * i + ca] += v * dv[3 * j + ca];
+      if (i != j) be[3 * j + ca] += v * dv[3 * i + ca];
+    }
+  });
+#pragma unroll
+  for (int i = 0; i < 10; ++i) {
+    const int64_t R = __ldg(d0 + i);
+#pragma unroll
+    for (int q = 0; q < 3; ++q) add_guarded(a.b, 3 * R + q, a.num_values, -a.scale * be[3 * i + q]);
+  }
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kBlock) k_lift_vp2(const LiftArgs a) {
   const int64_t t = blockIdx.x * (int64_t)kBlock + threadIdx.x;
@@ -1147,6 +1232,20 @@ __global__ void __launch_bounds__(kBlock) k_diag_mass(const DiagArgs a) {
   });
 }
 
+template <int COEF>
+__global__ void __launch_bounds__(kBlock) k_diag_vmass(const DiagArgs a) {
+  const int64_t c = blockIdx.x * (int64_t)kBlock + threadIdx.x;
+  if (c >= a.num_cells) return;
+  const double adet = cell_adet(a.x, load_geom(a.geom, c));
+  const int32_t* d = a.dofs + c * 10;
+  mass_element<10, COEF>(a.c0, c, adet, [&](int i, int j, double v) {
+    if (i != j) return;
+    const int64_t R = __ldg(d + i);
+#pragma unroll
+    for (int ca = 0; ca < 3; ++ca) add_guarded(a.b, 3 * R + ca, a.num_values, v);
+  });
+}
+
 __global__ void k_mark_cells(const int32_t* __restrict__ dofs, int64_t num_cells, int k, int bs,
                              const uint8_t* __restrict__ markers, int32_t* __restrict__ out,
                              unsigned long long* count) {
@@ -1274,6 +1373,10 @@ void launch_matrix_atomic(const MatLaunch& L, cudaStream_t s) {
     case FE_FORM_P2_MASS:
       if (a.c0.kind == FE_COEFF_P1) k_mat_mass<10, FE_COEFF_P1><<<grid, kBlock, 0, s>>>(a);
       else k_mat_mass<10, FE_COEFF_DG0><<<grid, kBlock, 0, s>>>(a);
+      break;
+    case FE_FORM_VP2_MASS:
+      if (a.c0.kind == FE_COEFF_P1) k_mat_vmass<FE_COEFF_P1><<<grid, kBlock, 0, s>>>(a);
+      else k_mat_vmass<FE_COEFF_DG0><<<grid, kBlock, 0, s>>>(a);
       break;
     case FE_FORM_P3_STIFFNESS: {
       // one thread per cell: splitting a cell's 210 entries over 2, 4 or 8
@@ -1476,6 +1579,10 @@ void launch_lifting(const LiftLaunch& L, cudaStream_t s) {
       if (a.c0.kind == FE_COEFF_P1) k_lift_mass<10, FE_COEFF_P1><<<grid, kBlock, 0, s>>>(a);
       else k_lift_mass<10, FE_COEFF_DG0><<<grid, kBlock, 0, s>>>(a);
       break;
+    case FE_FORM_VP2_MASS:
+      if (a.c0.kind == FE_COEFF_P1) k_lift_vmass<FE_COEFF_P1><<<grid, kBlock, 0, s>>>(a);
+      else k_lift_vmass<FE_COEFF_DG0><<<grid, kBlock, 0, s>>>(a);
+      break;
     case FE_FORM_P3_STIFFNESS: {
       const unsigned g3 = grid_for(L.num_list, kBlockP3);
       if (f32) k_lift_p3<float><<<g3, kBlockP3, 0, s>>>(a);
@@ -1532,8 +1639,12 @@ void launch_diagonal(const MatLaunch& L, double* b, int64_t num_values, cudaStre
       if (a.c0.kind == FE_COEFF_P1) k_diag_mass<10, FE_COEFF_P1><<<grid, kBlock, 0, s>>>(a);
       else k_diag_mass<10, FE_COEFF_DG0><<<grid, kBlock, 0, s>>>(a);
       break;
+    case FE_FORM_VP2_MASS:
+      if (a.c0.kind == FE_COEFF_P1) k_diag_vmass<FE_COEFF_P1><<<grid, kBlock, 0, s>>>(a);
+      else k_diag_vmass<FE_COEFF_DG0><<<grid, kBlock, 0, s>>>(a);
+      break;
     default:
-      FE_FAIL(FE_ERR_ARG, "the diagonal is offered for the cell bilinear forms (P1/P2/P3 stiffness, P1/P2 mass, "
+      FE_FAIL(FE_ERR_ARG, "the diagonal is offered for the cell bilinear forms (P1/P2/P3 stiffness, P1/P2/vector-P2 mass, "
                           "vector-P2 elasticity), not kind " + std::to_string(L.kind));
   }
   FE_CUDA(cudaGetLastError());

@@ -32,7 +32,7 @@ FE_OK = 0
 FE_ERR_NOT_CONVERGED = 6
 
 # enum values (include/cudolfinx_b200.h)
-FORM = {"P1_STIFFNESS": 1, "P2_STIFFNESS": 2, "VP2_ELASTICITY": 3, "P1_MASS": 9, "P2_MASS": 10, "P1_LOAD": 11, "P2_LOAD": 12, "VP2_LOAD": 13,
+FORM = {"P1_STIFFNESS": 1, "P2_STIFFNESS": 2, "VP2_ELASTICITY": 3, "P1_MASS": 9, "P2_MASS": 10, "VP2_MASS": 20, "P1_LOAD": 11, "P2_LOAD": 12, "VP2_LOAD": 13,
         "P1_FACET_MASS": 4, "P2_FACET_MASS": 5, "P1_FACET_LOAD": 14, "P2_FACET_LOAD": 15, "VP2_FACET_LOAD": 16,
         "INTEGRAL": 31, "P1_ENERGY": 32, "P2_ENERGY": 33, "FACET_INTEGRAL": 34,
         "P3_STIFFNESS": 6, "P3_LOAD": 17, "DG0_JUMP": 7, "DG1_JUMP": 8, "DG0_AVG_LOAD": 18, "DG1_AVG_LOAD": 19,

@@ -351,13 +351,14 @@ def stiffness(V: FunctionSpace, k: Coefficient = 1.0, precision: str = "fp64",
 
 
 def mass(V: FunctionSpace, c: Coefficient = 1.0, trial: Optional[FunctionSpace] = None) -> FormSpec:
-    """c * u * v * dx on a scalar P1/P2 space; c constant, DG0 or a scalar P1
-    Function (FP64 element tensors; u from ``trial`` as for ``stiffness``).
-    The P1 mass and stiffness share their pattern, so M + dt K assembles into
-    one matrix (the second call with zero=False)."""
-    if V.bs != 1 or V.family != "P" or V.degree not in (1, 2):
-        raise ValueError("mass needs a scalar P1 or P2 space")
-    return FormSpec("P1_MASS" if V.degree == 1 else "P2_MASS", V, [c], 2, "fp64", W=_trial(V, trial))
+    """c * inner(u, v) * dx on a scalar P1/P2 or a vector P2 space; c constant,
+    DG0 or a scalar P1 Function (FP64 element tensors; u from ``trial`` as for
+    ``stiffness``).  Mass and stiffness (or elasticity) share their pattern, so
+    M + dt K assembles into one matrix (the second call with zero=False)."""
+    if V.family != "P" or not ((V.bs == 1 and V.degree in (1, 2)) or (V.bs == 3 and V.degree == 2)):
+        raise ValueError("mass needs a scalar P1 / P2 or a vector P2 space")
+    kind = "VP2_MASS" if V.bs == 3 else ("P1_MASS" if V.degree == 1 else "P2_MASS")
+    return FormSpec(kind, V, [c], 2, "fp64", W=_trial(V, trial))
 
 
 def elasticity(V: FunctionSpace, lam: Coefficient, mu: Coefficient, precision: str = "fp64",

@@ -56,6 +56,7 @@ enum fe_form_kind {
                                   coeff 0 = lam, coeff 1 = mu                       */
   FE_FORM_P1_MASS = 9,         /* c*u*v*dx, P1;      coeff 0 = c (constant / DG0 / P1) */
   FE_FORM_P2_MASS = 10,        /* c*u*v*dx, P2;      coeff 0 = c (constant / DG0 / P1) */
+  FE_FORM_VP2_MASS = 20,       /* rho*inner(u, v)*dx, vector P2; coeff 0 = rho (constant / DG0 / P1) */
   FE_FORM_P1_LOAD = 11,        /* f*v*dx, P1;        coeff 0 = f                    */
   FE_FORM_P2_LOAD = 12,        /* f*v*dx, P2;        coeff 0 = f                    */
   FE_FORM_VP2_LOAD = 13,       /* inner(f, v)*dx, vector P2; coeff 0 = f (3 comps)  */
@@ -110,7 +111,7 @@ enum fe_precision {
 #define FE_ASM_ZERO 1u            /* overwrite instead of accumulating (assemble.py:52 zero=True)   */
 #define FE_ASM_DETERMINISTIC 2u   /* bitwise reproducible: ordered tile gather (P1/P2), else sorted-slot */
 #define FE_ASM_ATOMIC 4u          /* FP64-atomic scatter through the slot map (zero pass first); for
-                                     P1 (stiffness, mass), P3 and vector-P2 forms on a symmetric pattern with equal
+                                     P1 (stiffness, mass), P3 and vector-P2 (elasticity, mass) forms on a symmetric pattern with equal
                                      row/column BCs (and FE_ASM_ZERO) each unique entry is reduced
                                      once into the upper triangle and a pass copies it to the lower
                                      triangle                                                        */

@@ -542,6 +542,16 @@ def mass_matrices(coords, cells, degree, c_dg0=None, c_vertex=None):
     return c[:, None, None] * ref_mass_tensor(degree, False)[None]
 
 
+def vector_mass(Ae_scalar, bs=3):
+    """Ae [C, k*bs, k*bs] of rho * inner(u, v) * dx from the scalar mass
+    matrices: local index i*bs + a couples with j*bs + a only."""
+    C, k, _ = Ae_scalar.shape
+    out = np.zeros((C, k, bs, k, bs))
+    for a in range(bs):
+        out[:, :, a, :, a] = Ae_scalar
+    return out.reshape(C, k * bs, k * bs)
+
+
 def p3_load_dg0(coords, cells, f_cell):
     """be [C,20] of f * v * dx with f DG0: |det| f int_ref phi_i."""
     _, det, _ = cell_geometry(coords, cells)

@@ -1,4 +1,4 @@
-"""Cell mass matrices c*u*v*dx (FE_FORM_P1_MASS / FE_FORM_P2_MASS) on the GPU.
+"""Cell mass matrices c*inner(u, v)*dx (FE_FORM_P1_MASS / P2_MASS / VP2_MASS) on the GPU.
 
 Checked against the oracle (exact reference mass tensors): values with BC
 rows/columns skipped and a unit diagonal, entrywise within 1e-12 relative with
@@ -135,3 +135,70 @@ def test_mass_rejects_the_stiffness_only_variants():
                 asm.assemble_matrix(a, variant=variant)
     with pytest.raises(ValueError):
         fem.mass(fem.functionspace(mesh, ("P", 3)))
+
+
+@pytest.mark.parametrize("coef", ["const", "dg0", "p1"])
+@pytest.mark.parametrize("variant", ["auto", "atomic-full", "deterministic"])
+def test_vector_p2_mass_matches_oracle(coef, variant):
+    ensure_library()
+    import cudolfinx as cx
+    from cudolfinx import fem
+
+    n = 3
+    P = fo.build_problem("vp2", n, seed=5)
+    mesh = fem.Mesh(P["coords"], P["cells"], grid_n=n)
+    V = fem.functionspace(mesh, ("P", 2, (3,)))
+    rng = np.random.default_rng(8)
+    C = len(P["cells"])
+    if coef == "const":
+        c, kw = 1.7, dict(c_dg0=np.full(C, 1.7))
+    elif coef == "dg0":
+        vals = rng.uniform(0.5, 3.0, C)
+        c, kw = fem.Function(fem.functionspace(mesh, ("DG", 0)), vals), dict(c_dg0=vals)
+    else:
+        vals = rng.uniform(0.5, 3.0, len(P["coords"]))
+        c, kw = fem.Function(fem.functionspace(mesh, ("P", 1)), vals), dict(c_vertex=vals[P["cells"]])
+    Ae = fo.vector_mass(fo.mass_matrices(P["coords"], P["cells"], 2, **kw))
+    asm = cx.CUDAAssembler()
+    m = cx.form(fem.mass(V, c))
+    bc = fem.dirichletbc(fem.Function(V, np.linspace(-1.0, 1.0, 3 * P["ndof"])), P["bc_dofs"])
+    bcs = asm.pack_bcs([bc])
+    A = asm.assemble_matrix(m, bcs=bcs, variant=variant)
+    A.assemble()
+    rp, col = A.sparsity.to_host()
+    nscal = 3 * P["ndof"]
+    markers = np.zeros(nscal, dtype=np.uint8)
+    markers[P["bc_dofs"]] = 1
+    ref = fo.assemble_matrix(Ae, P["dofs"], P["dofs"], rp, col, 3, 3, markers, markers, 1.0, P["bc_dofs"])
+    ok, worst = tolerance_check(A.values.cpu().numpy(), ref)
+    assert ok, worst
+    if variant == "auto":
+        L0 = cx.form(fem.load(V, np.zeros(3)))
+        b = asm.assemble_vector(L0)
+        asm.apply_lifting(b, [m], [bcs])
+        g = np.linspace(-1.0, 1.0, nscal)
+        ok, worst = tolerance_check(b.to_host(), fo.apply_lifting(np.zeros(nscal), Ae, P["dofs"], P["dofs"],
+                                                                  markers, g, bs0=3, bs1=3))
+        assert ok, worst
+        d = asm.assemble_vector(cx.form(fem.mass(V, c), form_compiler_options={"part": "diagonal"})).to_host()
+        ok, worst = tolerance_check(d, fo.assemble_diagonal(Ae, P["dofs"], nscal, 3))
+        assert ok, worst
+
+
+def test_vector_p2_mass_reproduces_the_l2_norm_of_a_quadratic_field():
+    ensure_library()
+    import cudolfinx as cx
+    from cudolfinx import fem
+    import scipy.sparse as sp
+
+    mesh = fem.create_unit_cube(5, jitter=0.2, seed=6)
+    V = fem.functionspace(mesh, ("P", 2, (3,)))
+    X = V.tabulate_dof_coordinates()
+    x, y, z = X[:, 0], X[:, 1], X[:, 2]
+    u = np.stack([x * x, y * z, np.ones_like(x)], axis=1).ravel()  # (x^2, yz, 1)
+    exact = 1 / 5 + 1 / 9 + 1.0
+    A = cx.CUDAAssembler().assemble_matrix(cx.form(fem.mass(V, 2.0)))
+    A.assemble()
+    rp, col = A.sparsity.to_host()
+    M = sp.csr_matrix((A.values.cpu().numpy(), col, rp), shape=(u.size, u.size))
+    assert abs(u @ (M @ u) - 2.0 * exact) <= 1e-12 * exact

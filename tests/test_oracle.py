@@ -540,3 +540,18 @@ def test_mass_matrix_reproduces_l2_norms_of_polynomials():
     # int_[0,1]^3 (1 + x - 2y + 3z)^2 = 1 + (1+4+9)/3 + 2*(1-2+3)/2 + 2*(-2+3-6)/4 = 6.4166...
     exact = 1 + 14 / 3 + 2 + 2 * (1 * -2 + 1 * 3 + -2 * 3) / 4
     assert abs(u @ (Ms @ u) - exact) < 1e-12 * exact
+
+
+def test_vector_mass_reproduces_the_l2_norm_of_a_quadratic_vector_field():
+    import scipy.sparse as sp
+    n = 3
+    coords, cells = fo.unit_cube_tet_mesh(n, jitter=0.2, seed=9)
+    dofs, ndof, _ = fo.p2_dofmap(n, cells)
+    X = fo.dof_coordinates(coords, cells, dofs, ndof, 2)
+    x, y, z = X[:, 0], X[:, 1], X[:, 2]
+    u = np.stack([x * x, y * z, np.ones_like(x)], axis=1).ravel()
+    Ae = fo.vector_mass(fo.mass_matrices(coords, cells, 2, c_dg0=np.full(len(cells), 2.0)))
+    rp, col = fo.sparsity(dofs, dofs, ndof, 3, 3)
+    M = sp.csr_matrix((fo.assemble_matrix(Ae, dofs, dofs, rp, col, 3, 3), col, rp), shape=(3 * ndof, 3 * ndof))
+    exact = 2.0 * (1 / 5 + 1 / 9 + 1.0)
+    assert abs(u @ (M @ u) - exact) < 1e-12 * exact
