@@ -170,3 +170,43 @@ def test_reference_nodes_and_basis_are_lagrange_and_match_the_oracle():
         for ds in (1, 2, 3):
             assert np.allclose(fem.interpolation_matrix(spaces[dt], spaces[ds]), fo.interpolation_operator(dt, ds),
                                atol=1e-14)
+
+
+def test_mass_specs_and_form_part_validation_without_gpu():
+    import cudolfinx as cx
+    from cudolfinx import fem
+    from cudolfinx import _lib
+    mesh = fem.create_unit_cube(2)
+    V1, V2 = fem.functionspace(mesh, ("P", 1)), fem.functionspace(mesh, ("P", 2))
+    V2v = fem.functionspace(mesh, ("P", 2, (3,)))
+    for V, kind in ((V1, "P1_MASS"), (V2, "P2_MASS"), (V2v, "VP2_MASS")):
+        s = fem.mass(V, 2.0)
+        assert s.kind == kind and s.rank == 2 and s.precision == "fp64" and kind in _lib.FORM
+    for bad in (lambda: fem.mass(fem.functionspace(mesh, ("P", 3))),
+                lambda: fem.mass(fem.functionspace(mesh, ("DG", 1)))):
+        with pytest.raises(ValueError):
+            bad()
+    # the "part" option is checked before any device work
+    opts = {"form_compiler_options": {"part": "diagonal"}}
+    with pytest.raises(ValueError, match="one space"):
+        cx.form(fem.load(V2, 1.0), **opts)
+    with pytest.raises(ValueError, match="one space"):
+        cx.form(fem.facet_mass(V1, 1.0, fem.exterior_facets(mesh)), **opts)
+    with pytest.raises(ValueError, match="unknown form part"):
+        cx.form(fem.stiffness(V2, 1.0), form_compiler_options={"part": "lower"})
+
+
+def test_variant_tuner_key_separates_coefficient_kinds():
+    from cudolfinx import fem
+    from cudolfinx.batch import VariantTuner
+    mesh = fem.create_unit_cube(2)
+    V1 = fem.functionspace(mesh, ("P", 1))
+    W = fem.functionspace(mesh, ("DG", 0))
+
+    class _Form:  # the tuner keys on the form spec only
+        def __init__(self, spec):
+            self._spec = spec
+
+    keys = {VariantTuner.key(_Form(fem.stiffness(V1, k)))
+            for k in (1.0, fem.Function(W, np.ones(mesh.num_cells)), fem.Function(V1, np.ones(V1.num_dofs)))}
+    assert len(keys) == 3
