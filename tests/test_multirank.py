@@ -58,3 +58,26 @@ def test_single_process_identity():
     import bench
     assert bench.reduce_over_ranks([3.0, 4.0], device="cpu") == [3.0, 4.0]
     assert bench.replica_rate(10, 2, 1000.0, 1) == pytest.approx(20.0)
+
+
+def _bench(env_extra, *args):
+    import subprocess
+    import sys
+    env = dict(os.environ, **env_extra)
+    return subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), *args], cwd=ROOT, env=env,
+                          capture_output=True, text=True, timeout=600)
+
+
+def test_reference_arm_runs_on_rank_zero_only():
+    import json
+    args = ("--impl", "reference", "--workload", "p1", "--steps", "1", "--warmup", "1")
+    other = _bench({"RANK": "1", "WORLD_SIZE": "2", "LOCAL_RANK": "1"}, *args)
+    assert other.returncode == 0 and other.stdout.strip() == ""
+    first = _bench({"RANK": "0", "WORLD_SIZE": "2", "LOCAL_RANK": "0"}, *args)
+    assert first.returncode == 0, first.stderr[-2000:]
+    lines = [ln for ln in first.stdout.splitlines() if ln.strip()]
+    assert len(lines) == 1
+    out = json.loads(lines[0])
+    assert out["impl"] == "reference" and out["value"] > 0 and out["unit"] == "nnz/s"
+    assert out["cpu_baseline"]["value"] == out["value"] and out["cpu_baseline"]["kind"] in ("port", "reference")
+    assert out["e2e"]["h2d_bytes_per_step"] == 0 and out["e2e"]["d2h_bytes_per_step"] == 0
