@@ -210,3 +210,49 @@ def test_variant_tuner_key_separates_coefficient_kinds():
     keys = {VariantTuner.key(_Form(fem.stiffness(V1, k)))
             for k in (1.0, fem.Function(W, np.ones(mesh.num_cells)), fem.Function(V1, np.ones(V1.num_dofs)))}
     assert len(keys) == 3
+
+
+def test_interior_facets_and_dg_specs_without_gpu():
+    from cudolfinx import fem
+    mesh = fem.create_unit_cube(3, jitter=0.1, seed=2)
+    q = fem.interior_facets(mesh)
+    ext = fem.exterior_facets(mesh)
+    C = mesh.num_cells
+    assert 2 * len(q) + len(ext) == 4 * C                      # every facet once, interior ones twice
+    assert np.all(q[:, 0] < q[:, 2]) and q[:, [1, 3]].min() >= 0 and q[:, [1, 3]].max() <= 3
+    tri = np.array([[1, 2, 3], [0, 2, 3], [0, 1, 3], [0, 1, 2]])
+    v0 = np.sort(mesh.cells[q[:, 0][:, None], tri[q[:, 1]]], axis=1)
+    v1 = np.sort(mesh.cells[q[:, 2][:, None], tri[q[:, 3]]], axis=1)
+    assert np.array_equal(v0, v1)                               # the two sides name the same facet
+    ref = fo.interior_facets(mesh.cells)
+    assert sorted(map(tuple, q.tolist())) == sorted(map(tuple, np.asarray(ref).tolist()))
+    V0, V1 = fem.functionspace(mesh, ("DG", 0)), fem.functionspace(mesh, ("DG", 1))
+    assert fem.jump_penalty(V0, 2.0).kind == "DG0_JUMP" and fem.jump_penalty(V1).kind == "DG1_JUMP"
+    assert np.array_equal(fem.jump_penalty(V1).facets, q)
+    L = fem.facet_average_load(V1, 1.0, q[:5])
+    assert L.kind == "DG1_AVG_LOAD" and L.rank == 1 and len(L.facets) == 5
+    Vp = fem.functionspace(mesh, ("P", 1))
+    assert fem.jump_norm(fem.Function(Vp)).kind == "JUMP_NORM"
+    for bad in (lambda: fem.jump_norm(fem.Function(fem.functionspace(mesh, ("P", 2)))),
+                lambda: fem.jump_norm(fem.Function(fem.functionspace(mesh, ("P", 2, (3,)))))):
+        with pytest.raises(ValueError):
+            bad()
+
+
+def test_boundary_dofs_bcs_and_elasticity_specs_without_gpu():
+    from cudolfinx import fem
+    mesh = fem.create_unit_cube(2)
+    V = fem.functionspace(mesh, ("P", 2))
+    Vv = fem.functionspace(mesh, ("P", 2, (3,)))
+    s = fem.locate_boundary_dofs(V)
+    v = fem.locate_boundary_dofs(Vv)
+    assert np.array_equal(v, (s[:, None] * 3 + np.arange(3)).ravel())
+    X = V.tabulate_dof_coordinates()
+    on = np.any((X < 1e-12) | (X > 1 - 1e-12), axis=1)
+    assert np.array_equal(np.sort(s), np.nonzero(on)[0])
+    bc = fem.dirichletbc(0.5, s, V)
+    bcv = fem.dirichletbc(fem.Function(Vv, np.ones(Vv.num_dofs)), v)
+    assert bc is not None and bcv is not None
+    assert fem.elasticity(Vv, 1.0, 2.0).kind == "VP2_ELASTICITY"
+    with pytest.raises(ValueError):
+        fem.elasticity(V, 1.0, 2.0)
