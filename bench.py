@@ -80,6 +80,7 @@ SERVE = dict(requests=120, rates=(50.0, 200.0, 1000.0), nmin=8, nmax=48, workers
              desc="assemble + Jacobi-PCG (rtol 1e-8) requests with Poisson arrivals; 35% P1 / 35% P2 Poisson "
                   "(k DG0 lognormal, f=1, g=x+y+z), 30% vector-P2 elasticity (lam, mu DG0 lognormal, body force "
                   "(0,0,-1), u=0); unit-cube meshes n^3 x 6 tets, n log-uniform")
+L2_BYTES = 126 * 1024 * 1024
 # kernels of one step besides the matrix call: zero b, vector, lifting, set_bc
 VECTOR_KERNELS = 4
 
@@ -233,6 +234,16 @@ def oracle_problem(I):
 # ---------------------------------------------------------------------------
 # CPU legs (C restatement of the reference algorithm)
 # ---------------------------------------------------------------------------
+def workload_config(W, cells, dofs, nnz, world):
+    """The `config` object of both arms (identical for the same workload)."""
+    return {"workload": W["desc"], "cells": int(cells), "dofs": int(dofs), "nnz": int(nnz),
+            "step": "zero A + assemble A (BC skip, unit diagonal) + assemble b + lifting + set_bc",
+            "l2": ("inputs larger than L2 (CSR values %.2f GB), no flush between steps" % (8 * nnz / 1e9))
+            if 8 * nnz > L2_BYTES else ("working set fits in L2 (CSR values %.1f MB), no flush: steps time "
+                                        "L2-resident latency" % (8 * nnz / 1e6)),
+            "parallelism": f"replicas x{world}"}
+
+
 def cpu_assembler(I, row_ptr, col):
     from oracle import cfem
 
@@ -248,15 +259,75 @@ def cpu_step(C):
 
 
 def cpu_baseline(I, row_ptr, col, nnz, reps=2):
+    """Times the C restatement on the full workload; returns the baseline
+    object and the assembler, which holds the last step's A and b (the
+    parity check reads them)."""
     C, threads = cpu_assembler(I, row_ptr, col)
     cpu_step(C)  # warm (page-in, thread start)
     times = [cpu_step(C) for _ in range(reps)]
-    C.close()
     t = statistics.median(times)
     return {"value": nnz / t, "unit": "nnz/s", "cores": threads, "kind": "port",
             "sample": f"full workload ({len(I['cells'])} cells, nnz {nnz}): matrix + vector + lifting + set_bc, "
                       f"median of {reps} after 1 warm-up, {threads} threads, C port of the reference CPU "
-                      "path (oracle/cfem.c)", "seconds_per_step": t}
+                      "path (oracle/cfem.c)", "seconds_per_step": t}, C
+
+
+def parity_report(I, W, A, b, C, row_ptr, col, asm=None, dbc=None):
+    """The engine's system at the benchmark size against the C restatement's
+    (the cpu_baseline run, same inputs): the CSR pattern against the oracle's
+    own builder (bit-exact), A and b entrywise against the per-entry bound
+    (1e-12 of the sum of an entry's |contributions| plus 1e-14 of each
+    contributing element's largest |entry|; 0 where set_diagonal / set_bc
+    write).  FP32 element tensors are reported as the relative Frobenius
+    error of A and the Jacobi-PCG solution error against the oracle's FP64
+    matrix instead."""
+    from oracle import cfem
+    from oracle import fem_oracle as fo
+
+    t0 = time.perf_counter()
+    rp_o, col_o = cfem.pattern(I["dofs"], I["ndof"], I["bs"])
+    pattern_ok = bool(np.array_equal(rp_o, row_ptr) and np.array_equal(col_o, col))
+    del rp_o, col_o
+    A_gpu = A.values.cpu().numpy()
+    b_gpu = b.to_host().copy()
+    out = {"oracle": "oracle/cfem.c (C restatement of the reference path), full workload, same inputs",
+           "pattern_bit_exact": pattern_ok}
+    if W["precision"] == "fp64":
+        A_bound = C.matrix_bound()
+        okA, wA = fo.within_bound(A_gpu, C.values, A_bound)
+        del A_bound
+        b_bound = C.rhs_bound()
+        okb, wb = fo.within_bound(b_gpu, C.b, b_bound)
+        rel = lambda x, y: float(np.max(np.abs(x - y)) / max(np.max(np.abs(y)), 1e-300)) if y.size else 0.0
+        out.update({"bound": "per entry: 1e-12 * sum |contributions| + 1e-14 * max|element entry| per "
+                             "contributing element; exact where set_diagonal / set_bc write",
+                    "A_worst_err_over_bound": wA, "b_worst_err_over_bound": wb,
+                    "A_max_abs_err_over_max_abs": rel(A_gpu, C.values), "b_max_abs_err_over_max_abs": rel(b_gpu, C.b),
+                    "pass": bool(pattern_ok and okA and okb)})
+    else:
+        import torch
+
+        import cudolfinx as cx
+
+        ref = torch.from_numpy(C.values).to(A.values.device)
+        frob = float(torch.linalg.norm(A.values - ref) / torch.linalg.norm(ref))
+        # the oracle's FP64 matrix in the same pattern, both solved on the device
+        A64 = cx.CUDAMatrix(asm._ctx, A.sparsity)
+        A64.values.copy_(ref)
+        del ref
+        rtol = 1e-10
+        x32, it32, r32 = asm.solve(A, b, rtol=rtol, max_iter=200000, raise_on_failure=False)
+        x64, it64, r64 = asm.solve(A64, b, rtol=rtol, max_iter=200000, raise_on_failure=False)
+        torch.cuda.synchronize()
+        err = float(torch.linalg.norm(x32.vector - x64.vector) / torch.linalg.norm(x64.vector))
+        okb, wb = fo.within_bound(b_gpu, C.b, C.rhs_bound())
+        out.update({"A_rel_frobenius_vs_oracle_fp64": frob, "solution_rel_error_vs_oracle_fp64": err,
+                    "pcg_rtol": rtol, "pcg_iterations": [it32, it64], "b_worst_err_over_bound": wb,
+                    "pass": bool(pattern_ok and frob <= 2e-6 and err <= 1e-6 and okb),
+                    "bound": "FP32 element tensors: relative Frobenius error <= 2e-6, PCG solution error <= 1e-6 "
+                             "(b in FP64 within the per-entry bound)"})
+    out["seconds"] = time.perf_counter() - t0
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -513,12 +584,10 @@ def run_gpu(args, rank, world, local_rank):
         "vs_baseline": None,
         "dtype": "f64" if W["precision"] == "fp64" else "f32-element/f64-accumulate",
         "data": "synthetic (seeded numpy inputs with the configuration's shapes and distributions)",
-        "config": {"workload": W["desc"], "cells": len(I["cells"]), "dofs": nrows, "nnz": nnz,
-                   "step": "zero A + assemble A (BC skip, unit diagonal) + assemble b + lifting + set_bc",
-                   "timing": "replays of the step captured in a CUDA graph (matrix and vector branches concurrent)"
-                   if graph is not None else "eager steps",
-                   "variant": args.variant, "l2": "inputs larger than L2 (CSR values %.2f GB)" % (8 * nnz / 1e9),
-                   "parallelism": f"replicas x{world}"},
+        "config": workload_config(W, len(I["cells"]), nrows, nnz, world),
+        "timing": "replays of the step captured in a CUDA graph (matrix and vector branches concurrent)"
+        if graph is not None else "eager steps",
+        "variant": args.variant,
         "roofline": {"bound": "hbm", "kernel": "matrix assembly (%s%s)" % (args.variant, "" if resolved == args.variant else " = " + resolved),
                      "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "algorithmic_bytes": alg,
@@ -536,7 +605,10 @@ def run_gpu(args, rank, world, local_rank):
         out["precision"] = precision_report(I, asm, a, A, b, dbc, args.precision_rtol)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         row_ptr, col = A.sparsity.to_host()
-        out["cpu_baseline"] = cpu_baseline(I, row_ptr, col, nnz)
+        out["cpu_baseline"], C = cpu_baseline(I, row_ptr, col, nnz)
+        if not args.no_parity:
+            out["parity"] = parity_report(I, W, A, b, C, row_ptr, col, asm, dbc)
+        C.close()
     return out
 
 
@@ -1687,23 +1759,30 @@ def run_reference(args):
         return run_reference_interp(args)
     if args.workload == "dg":
         return run_reference_dg(args)
+    # the CPU path alone: problem, pattern and assembly from oracle/ (numpy
+    # builders + the C restatement); nothing of the engine is loaded
+    from oracle import cfem
+    from oracle import fem_oracle as fo
+
     W = WORKLOADS[args.workload]
-    I = make_inputs(W["kind"], W["n"], seed=args.seed)
-    row_ptr, col = host_pattern(I)
+    P = fo.build_problem(W["kind"], W["n"], seed=args.seed)
+    threads = os.cpu_count() or 1
+    row_ptr, col = cfem.pattern(P["dofs"], P["ndof"], P["bs"], nthreads=threads)
     nnz = len(col)
-    C, threads = cpu_assembler(I, row_ptr, col)
+    C = cfem.CpuAssembler(P, row_ptr, col, nthreads=threads)
     for _ in range(args.warmup):
         cpu_step(C)
     times = [cpu_step(C) for _ in range(args.steps)]
     C.close()
     total = sum(times)
     v = nnz * args.steps / total
-    return {"impl": "reference", "metric": "matrix nnz/s", "value": v, "unit": "nnz/s", "n_gpus": 1,
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    return {"impl": "reference", "metric": "matrix nnz/s", "value": v, "unit": "nnz/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded)",
-            "config": {"workload": W["desc"], "cells": len(I["cells"]), "nnz": nnz,
-                       "step": "zero A + assemble A + assemble b + lifting + set_bc"},
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64",
+            "data": "synthetic (seeded numpy inputs with the configuration's shapes and distributions)",
+            "config": workload_config(W, len(P["cells"]), P["ndof"] * P["bs"], nnz, world),
             "cpu_baseline": {"value": v, "unit": "nnz/s", "cores": threads, "kind": "port",
                              "sample": "full workload each step; C port of the reference CPU path "
                                        "(oracle/cfem.c); the reference itself needs DOLFINx + PETSc"},
@@ -1772,6 +1851,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-graph", action="store_true", help="time eager steps instead of replaying a CUDA graph")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-parity", action="store_true", help="skip the full-size parity check against the oracle")
     ap.add_argument("--no-precision", action="store_true", help="skip the FP32-vs-FP64 precision report")
     ap.add_argument("--precision-rtol", type=float, default=1e-10,
                     help="PCG tolerance of the precision report's two solves")

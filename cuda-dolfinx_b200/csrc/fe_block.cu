@@ -74,6 +74,7 @@ struct BlockArgs {
   double coef_const;
   const double* __restrict__ gbound;       // [nblocks] geometric part of the entry bound
   double term_max;                         // reference-tensor part of the entry bound
+  int fx_bits;                             // fixed-point bits S (50..57)
   double* __restrict__ values;
   const int32_t* __restrict__ gvert_ptr;   // P1: [nblocks+1] block geometry nodes
   const double* __restrict__ gx;           // P1: their coordinates, block by block
@@ -117,9 +118,39 @@ __device__ __forceinline__ double cell_coef_factor(const BlockArgs& a, int64_t c
   return a.coef_kind == FE_COEFF_DG0 ? fabs(__ldg(a.coef + __ldg(a.cell_id + cb))) : fabs(a.coef_const);
 }
 
-// element tensor of block-ordered cell cb: emit(i, j, value) for i <= j
-template <int KIND, typename T, typename Emit>
-__device__ __forceinline__ void cell_entries(const BlockArgs& a, int64_t cb, Emit&& emit) {
+// Fixed-point scale of a block.  Every entry of the block lies below bmax <
+// 2^ex; it is kept as w = round(v * 2^(S - ex)), |w| < 2^S, S = fx_bits,
+// rounded to nearest by one 64-bit conversion.  Quantisation is at most
+// 2^(ex - S - 1) per contribution, so a cell whose entries lie 2^kDirect
+// below 2^ex would lose precision relative to its own size: such cells add
+// their entries with FP64 reductions instead.
+struct FixedScale {
+  double scale, direct_below;
+};
+
+__device__ __forceinline__ FixedScale fixed_scale(double bmax, int fx_bits, int direct_bits) {
+  int ex = 0;
+  frexp(bmax, &ex);
+  const bool ok = bmax > 0.0 && bmax < 1e300;
+  FixedScale f;
+  f.scale = ok ? ldexp(1.0, fx_bits - ex) : 1.0;
+  f.direct_below = ok ? ldexp(1.0, ex - direct_bits) : 0.0;
+  return f;
+}
+
+__device__ __forceinline__ long long to_fixed(double v, const FixedScale& f) { return __double2ll_rn(v * f.scale); }
+
+// cells whose entry bound lies below 2^(ex - kDirect*) take the FP64 path:
+// the P1 bound is the cell's largest entry itself, the P2 one an upper bound
+constexpr int kDirectP1 = 8;
+constexpr int kDirectP2 = 6;
+
+// element tensor of block-ordered cell cb, entries (i, j, value) for i <= j
+// passed to emit, or to emit_direct when an upper bound of the cell's
+// |entries| lies below direct_below
+template <int KIND, typename T, typename Emit, typename EmitDirect>
+__device__ __forceinline__ void cell_entries(const BlockArgs& a, int64_t cb, double direct_below, Emit&& emit,
+                                             EmitDirect&& emit_direct) {
   double Km[3][3], adet;
   block_geom(a.x, __ldg(a.geom + cb), Km, adet);
   if constexpr (KIND == FE_FORM_P1_STIFFNESS) {
@@ -133,17 +164,28 @@ __device__ __forceinline__ void cell_entries(const BlockArgs& a, int64_t cb, Emi
     }
     const double k = a.coef_kind == FE_COEFF_DG0 ? __ldg(a.coef + __ldg(a.cell_id + cb)) : a.coef_const;
     const double s = adet * (1.0 / 6.0) * k;
+    double g2 = 0.0;
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+    for (int i = 0; i < 4; ++i) g2 = fmax(g2, G[i][0] * G[i][0] + G[i][1] * G[i][1] + G[i][2] * G[i][2]);
+    auto run = [&](auto&& e) {
 #pragma unroll
-      for (int j = i; j < 4; ++j) emit(i, j, s * (G[i][0] * G[j][0] + G[i][1] * G[j][1] + G[i][2] * G[j][2]));
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = i; j < 4; ++j) e(i, j, s * (G[i][0] * G[j][0] + G[i][1] * G[j][1] + G[i][2] * G[j][2]));
+    };
+    if (!(fabs(s) * g2 < direct_below)) run(emit);
+    else run(emit_direct);
   } else {
     const int pa[6] = {0, 1, 2, 0, 0, 1}, pb[6] = {0, 1, 2, 1, 2, 2};
-    double Gh[6];
+    double Gh[6], gsum = 0.0;
 #pragma unroll
-    for (int s = 0; s < 6; ++s)
+    for (int s = 0; s < 6; ++s) {
       Gh[s] = adet * (Km[pa[s]][0] * Km[pb[s]][0] + Km[pa[s]][1] * Km[pb[s]][1] + Km[pa[s]][2] * Km[pb[s]][2]);
+      gsum += fabs(Gh[s]);
+    }
+    const bool direct = gsum * cell_coef_factor(a, cb) * a.term_max < direct_below;
     auto emitT = [&](int i, int j, double v) { emit(i, j, v); };
+    auto emitD = [&](int i, int j, double v) { emit_direct(i, j, v); };
     if (a.coef_kind == FE_COEFF_P1) {
       const int4 km = __ldg(a.coef_map + cb);
       const double kv[4] = {__ldg(a.coef + km.x), __ldg(a.coef + km.y), __ldg(a.coef + km.z), __ldg(a.coef + km.w)};
@@ -152,13 +194,15 @@ __device__ __forceinline__ void cell_entries(const BlockArgs& a, int64_t cb, Emi
       for (int m = 0; m < 4; ++m)
 #pragma unroll
         for (int s = 0; s < 6; ++s) qv[m * 6 + s] = (T)(kv[m] * Gh[s]);
-      p2_stiffness_p1coef<T>(qv, emitT);
+      if (!direct) p2_stiffness_p1coef<T>(qv, emitT);
+      else p2_stiffness_p1coef<T>(qv, emitD);
     } else {
       const double k = a.coef_kind == FE_COEFF_DG0 ? __ldg(a.coef + __ldg(a.cell_id + cb)) : a.coef_const;
       T gq[6];
 #pragma unroll
       for (int s = 0; s < 6; ++s) gq[s] = (T)(k * Gh[s]);
-      p2_stiffness_const<T>(gq, emitT);
+      if (!direct) p2_stiffness_const<T>(gq, emitT);
+      else p2_stiffness_const<T>(gq, emitD);
     }
   }
 }
@@ -205,13 +249,7 @@ __global__ void __launch_bounds__(BlockTraits<KIND>::NT, BlockTraits<KIND>::MINB
     kfac = (double)__uint_as_float(s_bmax);
   }
   const double bmax = 1.25 * a.gbound[b] * kfac * a.term_max;
-  int ex = 0;
-  frexp(bmax, &ex);
-  // |entry * scale| < 2^50 keeps the magic-number rounding exact, and up to
-  // 255 contributions per slot stay below 2^58
-  const double scale = (bmax > 0.0 && bmax < 1e300) ? ldexp(1.0, 50 - ex) : 1.0;
-  const double inv_scale = 1.0 / scale;
-  constexpr double kMagic = 6755399441055744.0;  // 1.5 * 2^52: v + kMagic holds round(v) in its low bits
+  const FixedScale fs = fixed_scale(bmax, a.fx_bits, kDirectP2);
 
   // pass 2: entries accumulate as 64-bit fixed-point integers, kept as two
   // 32-bit words so both updates are native shared-memory atomics; integer
@@ -241,7 +279,7 @@ __global__ void __launch_bounds__(BlockTraits<KIND>::NT, BlockTraits<KIND>::MINB
       atomicAdd(win + 2 * idx + 1, hi + ((old + lo < old) ? 1u : 0u));
     };
     auto emit = [&](int i, int j, double v) {
-      const long long w = __double_as_longlong(fma(v, scale, kMagic)) - __double_as_longlong(kMagic);
+      const long long w = to_fixed(v, fs);
       const bool ok_ij = ((own >> i) & 1u) && !((cmask >> j) & 1u);
       add_fixed(ok_ij ? wbase[i] + posb(i, j) : Tr::WCAP, w);
       if (i != j) {
@@ -249,9 +287,18 @@ __global__ void __launch_bounds__(BlockTraits<KIND>::NT, BlockTraits<KIND>::MINB
         add_fixed(ok_ji ? wbase[j] + posb(j, i) : Tr::WCAP, w);
       }
     };
-    cell_entries<KIND, T>(a, cb, emit);
+    // a cell small next to the block's largest entries: FP64 reductions
+    // straight into the values
+    auto emit_direct = [&](int i, int j, double v) {
+      auto lrow = [&](int u) { return (int)__ldg(a.lrow + cb * K + u); };  // rare path: re-read
+      if (((own >> i) & 1u) && !((cmask >> j) & 1u)) atomicAdd(a.values + s_gbase[lrow(i)] + posb(i, j), v);
+      if (i != j && ((own >> j) & 1u) && !((cmask >> i) & 1u))
+        atomicAdd(a.values + s_gbase[lrow(j)] + posb(j, i), v);
+    };
+    cell_entries<KIND, T>(a, cb, fs.direct_below, emit, emit_direct);
   }
   __syncthreads();
+  const double inv = 1.0 / fs.scale;  // exact: a power of two
   // flush: one warp per touched row, lanes over consecutive slots
   const int warp = tid >> 5, lane = tid & 31;
   for (int r = warp; r < nrows; r += NT / 32) {
@@ -261,7 +308,7 @@ __global__ void __launch_bounds__(BlockTraits<KIND>::NT, BlockTraits<KIND>::MINB
       if (lo | hi) {
         // hi * 2^32 + lo, rounded once to double (both halves convert exactly)
         const double v = fma((double)(int32_t)hi, 4294967296.0, (double)lo);
-        atomicAdd(a.values + gb + e, v * inv_scale);
+        atomicAdd(a.values + gb + e, v * inv);
       }
     }
   }
@@ -354,11 +401,7 @@ __global__ void __launch_bounds__(BlockTraits<FE_FORM_P1_STIFFNESS>::NT, 4) k_bl
   __syncthreads();
   const double kfac = a.coef_kind != FE_COEFF_CONSTANT ? (double)__uint_as_float(s_bmax) : fabs(a.coef_const);
   const double bmax = 1.25 * a.gbound[b] * kfac;
-  int ex = 0;
-  frexp(bmax, &ex);
-  const double scale = (bmax > 0.0 && bmax < 1e300) ? ldexp(1.0, 50 - ex) : 1.0;
-  const double inv_scale = 1.0 / scale;
-  constexpr double kMagic = 6755399441055744.0;  // 1.5 * 2^52: v + kMagic holds round(v) in its low bits
+  const FixedScale fs = fixed_scale(bmax, a.fx_bits, kDirectP1);
 
   // lane l of warp w takes cells l*span + w, l*span + w + NW, ...: the 32
   // cells of one warp instruction lie span cells apart along the curve, and
@@ -388,13 +431,23 @@ __global__ void __launch_bounds__(BlockTraits<FE_FORM_P1_STIFFNESS>::NT, 4) k_bl
       atomicAdd(w1 + idx, hi + ((old + lo < old) ? 1u : 0u));
     };
     auto emit = [&](int i, int j, double v) {
-      const long long w = __double_as_longlong(fma(v, scale, kMagic)) - __double_as_longlong(kMagic);
+      const long long w = to_fixed(v, fs);
       const bool ok_ij = ((own >> i) & 1u) && !((cmask >> j) & 1u);
       add(ok_ij ? wbase[i] + (int)((pw[i] >> (8 * j)) & 0xffu) : kP1Wcap, w);
       if (i != j) {
         const bool ok_ji = ((own >> j) & 1u) && !((cmask >> i) & 1u);
         add(ok_ji ? wbase[j] + (int)((pw[j] >> (8 * i)) & 0xffu) : kP1Wcap, w);
       }
+    };
+    // a cell small next to the block's largest entries: FP64 reductions
+    // straight into the values (window slot -> global slot as in the flush)
+    auto emit_direct = [&](int i, int j, double v) {
+      auto red = [&](int w) {
+        const int r = s_wrow[w];
+        atomicAdd(a.values + s_gbase[r] + (w - s_soff[r]), v);
+      };
+      if (((own >> i) & 1u) && !((cmask >> j) & 1u)) red(wbase[i] + (int)((pw[i] >> (8 * j)) & 0xffu));
+      if (i != j && ((own >> j) & 1u) && !((cmask >> i) & 1u)) red(wbase[j] + (int)((pw[j] >> (8 * i)) & 0xffu));
     };
     // P1 element from the staged coordinates: grad phi_i = K^T ghat_i,
     // A_ij = k |det J| / 6 grad phi_i . grad phi_j
@@ -424,12 +477,24 @@ __global__ void __launch_bounds__(BlockTraits<FE_FORM_P1_STIFFNESS>::NT, 4) k_bl
     for (int d = 0; d < 3; ++d) G[0][d] = -(G[1][d] + G[2][d] + G[3][d]);
     const double kc = a.coef_kind == FE_COEFF_DG0 ? __ldg(a.coef + __ldg(a.cell_id + cb)) : a.coef_const;
     const double sc = fabs(det) * (1.0 / 6.0) * kc;
+    double g2 = 0.0;
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+    for (int i = 0; i < 4; ++i) g2 = fmax(g2, G[i][0] * G[i][0] + G[i][1] * G[i][1] + G[i][2] * G[i][2]);
+    if (!(fabs(sc) * g2 < fs.direct_below)) {
 #pragma unroll
-      for (int j = i; j < 4; ++j) emit(i, j, sc * (G[i][0] * G[j][0] + G[i][1] * G[j][1] + G[i][2] * G[j][2]));
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = i; j < 4; ++j) emit(i, j, sc * (G[i][0] * G[j][0] + G[i][1] * G[j][1] + G[i][2] * G[j][2]));
+    } else {
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = i; j < 4; ++j)
+          emit_direct(i, j, sc * (G[i][0] * G[j][0] + G[i][1] * G[j][1] + G[i][2] * G[j][2]));
+    }
   }
   __syncthreads();
+  const double inv = 1.0 / fs.scale;  // exact: a power of two
   // flat flush: consecutive lanes take consecutive window slots
   for (int w = tid; w < wtot; w += NT) {
     const uint32_t lo = w0[w], hi = w1[w];
@@ -437,7 +502,7 @@ __global__ void __launch_bounds__(BlockTraits<FE_FORM_P1_STIFFNESS>::NT, 4) k_bl
       const int r = s_wrow[w];
       // hi * 2^32 + lo, rounded once to double (both halves convert exactly)
       const double v = fma((double)(int32_t)hi, 4294967296.0, (double)lo);
-      atomicAdd(a.values + s_gbase[r] + (w - s_soff[r]), v * inv_scale);
+      atomicAdd(a.values + s_gbase[r] + (w - s_soff[r]), v * inv);
     }
   }
 }
@@ -463,12 +528,21 @@ std::unique_ptr<fe_form_s::BlockPlan> build_block_plan(const fe_form_s& f) {
   const std::vector<double>& X = f.mesh->host_x;
   const std::vector<int32_t>& G = f.mesh->host_geom;
 
-  // a slot collects at most one contribution per cell of its row: the
-  // fixed-point window holds up to 255 of them without overflow
+  // a slot collects at most one contribution per cell of its row: with
+  // |w| < 2^S per contribution and at most maxcnt of them, S = 62 -
+  // ceil(log2(maxcnt + 1)) keeps every slot sum below 2^62 (S <= 57; at least
+  // 54 for the 255-cell limit)
+  int fx_bits = 57;
   {
     std::vector<int32_t> cnt(V0.num_blocks, 0);
-    for (int64_t q = 0; q < C * K; ++q)
+    int32_t maxcnt = 0;
+    for (int64_t q = 0; q < C * K; ++q) {
       if (++cnt[V0.host[q]] > 255) FE_FAIL(FE_ERR_ARG, "a dof lies in more than 255 cells (block variant limit)");
+      maxcnt = std::max(maxcnt, cnt[V0.host[q]]);
+    }
+    int bits = 0;
+    while ((1 << bits) < maxcnt + 1) ++bits;
+    fx_bits = std::min(57, 62 - bits);
   }
 
   // 1. Morton order of cell centroids
@@ -676,6 +750,7 @@ std::unique_ptr<fe_form_s::BlockPlan> build_block_plan(const fe_form_s& f) {
 
   auto P = std::make_unique<fe_form_s::BlockPlan>();
   P->nblocks = (int64_t)block_ptr.size() - 1;
+  P->fx_bits = fx_bits;
   P->coef_map_owner = p1coef ? kc.map : nullptr;
   auto up = [](auto& d, const auto& h) {
     using E = typename std::decay_t<decltype(h)>::value_type;
@@ -730,6 +805,7 @@ void launch_block(const fe_form_s& f, const fe_form_s::BlockPlan& P, double* val
   a.coef = k.values;
   a.coef_const = k.kind < 0 ? 1.0 : k.constant[0];
   a.gbound = P.gbound.p;
+  a.fx_bits = P.fx_bits;
   if (KIND == FE_FORM_P1_STIFFNESS) a.term_max = 1.0;
   else a.term_max = (a.coef_kind == FE_COEFF_P1) ? kP2P1CoefTermMax : kP2ConstTermMax;
   a.values = values;

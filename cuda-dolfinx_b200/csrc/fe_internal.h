@@ -240,6 +240,8 @@ struct fe_form_s::BlockPlan {
   fe::DevBuf<uint8_t> pos;            // [cells][k*k] slot bytes, block order
   fe::DevBuf<int32_t> coef_map;       // [cells][4] P1 coefficient dofmap, block order
   fe::DevBuf<double> gbound;          // [nblocks] geometric part of the element-entry bound
+  int fx_bits = 50;                   // fixed-point bits S of the block bound: slot sums of up to
+                                      // max cells-per-dof contributions of |w| < 2^S fit in 63 bits
   fe::DevBuf<int32_t> gvert_ptr;      // [nblocks+1] into gx: each block's geometry nodes
   fe::DevBuf<double> gx;              // [block nodes][3] coordinates, block by block
   fe::DevBuf<uint16_t> glocal;        // [cells][4] block-local geometry node of each cell vertex

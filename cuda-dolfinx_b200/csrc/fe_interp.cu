@@ -66,6 +66,9 @@ unsigned blocks_for(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 void interpolate(fe_dofmap_s& target, double* u1, const fe_dofmap_s& source, const double* u0, const double* im,
                  cudaStream_t s) {
   if (target.k * source.k > kInterpMax) FE_FAIL(FE_ERR_ARG, "interpolation matrix larger than 20 x 20");
+  // owners are int32 (cell, local dof) entry indices
+  FE_REQUIRE(target.num_cells * (int64_t)target.k <= (int64_t)INT_MAX,
+             "interpolation target dofmap has more than 2^31-1 (cell, dof) entries");
   if (!target.owner.p && target.num_blocks) {
     target.owner.alloc(target.num_blocks);
     k_owner_fill<<<blocks_for(target.num_blocks, 256), 256, 0, s>>>(target.owner.p, target.num_blocks);

@@ -15,6 +15,7 @@
 
 #include <algorithm>
 #include <mutex>
+#include <vector>
 
 #include "fe_internal.h"
 
@@ -193,6 +194,34 @@ __global__ void __launch_bounds__(kThreads) k_update_p(int64_t n, const double* 
     p[i] = z[i] + beta * p[i];
 }
 
+// cudaMallocAsync'd buffers freed with cudaFreeAsync on the same stream when
+// the scope ends, normally or by an exception.
+struct StreamScratch {
+  cudaStream_t s;
+  std::vector<void*> ptrs;
+  explicit StreamScratch(cudaStream_t st) : s(st) {}
+  StreamScratch(const StreamScratch&) = delete;
+  StreamScratch& operator=(const StreamScratch&) = delete;
+  template <typename T>
+  T* get(int64_t count) {
+    void* q = nullptr;
+    FE_CUDA(cudaMallocAsync(&q, (size_t)std::max<int64_t>(count, 1) * sizeof(T), s));
+    ptrs.push_back(q);
+    return static_cast<T*>(q);
+  }
+  void release() {
+    while (!ptrs.empty()) {
+      void* q = ptrs.back();
+      ptrs.pop_back();
+      FE_CUDA(cudaFreeAsync(q, s));
+    }
+  }
+  ~StreamScratch() {
+    for (void* q : ptrs) (void)cudaFreeAsync(q, s);
+    if (!ptrs.empty()) (void)cudaGetLastError();
+  }
+};
+
 template <int SUB>
 void run(const fe_sparsity_s& A, const double* val, const double* b, double* x, double rtol, int max_iter,
          int* iterations, double* rel_res, cudaStream_t s) {
@@ -203,15 +232,16 @@ void run(const fe_sparsity_s& A, const double* val, const double* b, double* x, 
   // partials of the launch that wrote them
   const unsigned grid = (unsigned)(A.ctx->num_sms * 4);
   const unsigned grid_rows = (unsigned)(A.ctx->num_sms * 8);
-  double *r, *z, *p, *Ap, *dinv, *part;
-  Scalars* sc;
-  FE_CUDA(cudaMallocAsync((void**)&r, n * sizeof(double), s));
-  FE_CUDA(cudaMallocAsync((void**)&z, n * sizeof(double), s));
-  FE_CUDA(cudaMallocAsync((void**)&p, n * sizeof(double), s));
-  FE_CUDA(cudaMallocAsync((void**)&Ap, n * sizeof(double), s));
-  FE_CUDA(cudaMallocAsync((void**)&dinv, n * sizeof(double), s));
-  FE_CUDA(cudaMallocAsync((void**)&part, 3 * grid_rows * sizeof(double), s));
-  FE_CUDA(cudaMallocAsync((void**)&sc, sizeof(Scalars), s));
+  // stream-ordered scratch, released on every exit path (a launch or
+  // synchronisation error inside the loop throws)
+  StreamScratch buf(s);
+  double* r = buf.get<double>(n);
+  double* z = buf.get<double>(n);
+  double* p = buf.get<double>(n);
+  double* Ap = buf.get<double>(n);
+  double* dinv = buf.get<double>(n);
+  double* part = buf.get<double>(3 * (int64_t)grid_rows);
+  Scalars* sc = buf.get<Scalars>(1);
   Scalars h{};
   h.tol2 = rtol * rtol;
   h.max_iter = max_iter;
@@ -233,8 +263,7 @@ void run(const fe_sparsity_s& A, const double* val, const double* b, double* x, 
     FE_CUDA(cudaStreamSynchronize(s));
     if (h.done || it >= max_iter) break;
   }
-  for (void* q : {(void*)r, (void*)z, (void*)p, (void*)Ap, (void*)dinv, (void*)part, (void*)sc})
-    FE_CUDA(cudaFreeAsync(q, s));
+  buf.release();
   *iterations = h.iter;
   *rel_res = h.bb > 0 ? sqrt(h.rr / h.bb) : 0.0;
 }
@@ -290,12 +319,12 @@ namespace fe {
 namespace {
 
 constexpr int64_t kNoAllocMaxRows = int64_t(1) << 18;  // 262,144 rows
-constexpr int kNoAllocMaxGrid = 1024;                   // reduction slots per dot product
+constexpr int kNoAllocMaxGrid = 2048;                   // reduction slots per dot product
 constexpr int64_t kNoAllocScalarWords = 16;            // room for one Scalars record (in doubles)
 static_assert(sizeof(Scalars) <= kNoAllocScalarWords * sizeof(double), "Scalars record does not fit");
 
 // r, z, p, Ap, dinv (kNoAllocMaxRows each), 3 x kNoAllocMaxGrid partial sums, one Scalars record:
-// 5 * 262,144 * 8 B + 3 * 1024 * 8 B + 128 B = 10.5 MB held by every device that loads the library.
+// 5 * 262,144 * 8 B + 3 * 2048 * 8 B + 128 B = 10.5 MB held by every device that loads the library.
 static __device__ __align__(256) double g_pcg_scratch[5 * kNoAllocMaxRows + 3 * kNoAllocMaxGrid +
                                                       kNoAllocScalarWords];
 
@@ -319,7 +348,11 @@ template <int SUB>
 void run_noalloc(const fe_sparsity_s& A, const double* val, const double* b, double* x, double rtol, int max_iter,
                  int* iterations, double* rel_res, double* scratch, cudaStream_t s) {
   const int64_t n = A.num_rows;
+  // the launch shapes of fe_pcg_solve (8 CTAs per SM for the row kernels, 4
+  // for the vector updates), so the partial sums are grouped identically and
+  // the two solvers give bitwise-equal results on the same GPU
   const unsigned grid = (unsigned)std::min(A.ctx->num_sms * 4, kNoAllocMaxGrid);
+  const unsigned grid_rows = (unsigned)std::min(A.ctx->num_sms * 8, kNoAllocMaxGrid);
   double* r = scratch;
   double* z = r + kNoAllocMaxRows;
   double* p = z + kNoAllocMaxRows;
@@ -335,14 +368,14 @@ void run_noalloc(const fe_sparsity_s& A, const double* val, const double* b, dou
   h.tol2 = rtol * rtol;
   h.max_iter = max_iter;
   FE_CUDA(cudaMemcpyAsync(sc, &h, sizeof(h), cudaMemcpyHostToDevice, s));
-  k_init<SUB><<<grid, kThreads, 0, s>>>(n, A.row_ptr.p, A.col.p, val, A.diag.p, b, x, r, z, p, dinv, part);
-  k_reduce<<<1, 1024, 0, s>>>(part, grid, 0, sc);
+  k_init<SUB><<<grid_rows, kThreads, 0, s>>>(n, A.row_ptr.p, A.col.p, val, A.diag.p, b, x, r, z, p, dinv, part);
+  k_reduce<<<1, 1024, 0, s>>>(part, grid_rows, 0, sc);
   FE_CUDA(cudaGetLastError());
   const int batch = 16;
   for (int it = 0;; it += batch) {
     for (int q = 0; q < batch; ++q) {
-      k_spmv<SUB><<<grid, kThreads, 0, s>>>(n, A.row_ptr.p, A.col.p, val, p, Ap, part, sc);
-      k_reduce<<<1, 1024, 0, s>>>(part, grid, 1, sc);
+      k_spmv<SUB><<<grid_rows, kThreads, 0, s>>>(n, A.row_ptr.p, A.col.p, val, p, Ap, part, sc);
+      k_reduce<<<1, 1024, 0, s>>>(part, grid_rows, 1, sc);
       k_update<<<grid, kThreads, 0, s>>>(n, x, r, z, p, Ap, dinv, part, sc);
       k_reduce<<<1, 1024, 0, s>>>(part, grid, 2, sc);
       k_update_p<<<grid, kThreads, 0, s>>>(n, z, p, sc);

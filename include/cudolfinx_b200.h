@@ -334,15 +334,18 @@ int fe_pcg_solve(fe_sparsity s, const double* values, const double* b, double* x
  * application whose device memory is already reserved by its own pool
  * allocator (a framework caching allocator, a PETSc / Kokkos arena sized to
  * the card), or a latency-critical loop that must not enter the CUDA
- * allocator.  Same arguments, results and status codes as fe_pcg_solve, but
- * the solver's scratch vectors live in one file-scope device array of
- * 10.5 MB (5 vectors of 262,144 doubles plus reduction slots), which every
- * GPU that loads the library holds until the process exits; it calls no
- * cudaMalloc / cudaFree.
+ * allocator.  Same arguments and status codes as fe_pcg_solve, and on one
+ * GPU bitwise the same results (same kernels, same launch shapes), but the
+ * solver's scratch vectors live in one file-scope device array of 10.5 MB
+ * (5 vectors of 262,144 doubles plus reduction slots), which every GPU that
+ * loads the library holds until the process exits; it calls no cudaMalloc /
+ * cudaFree.
  *  - Matrices with more than 262,144 rows are rejected with FE_ERR_ARG.
  *  - The first call on a device looks up the array's device address (once per
- *    device, with that device current); make that first call before any
- *    stream capture.
+ *    device, with that device current) and keeps it; make that first call
+ *    before any stream capture, and do not reset the device
+ *    (cudaDeviceReset) while the library is loaded, which would leave the
+ *    kept address stale.
  *  - Every call shares the one array and re-initialises all of it that it
  *    reads; calls that overlap on the GPU (other streams, other threads) race
  *    on it and must be serialised by the caller. */

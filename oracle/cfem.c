@@ -238,7 +238,18 @@ typedef struct {
   double *values, *b;
   double diagonal, scale;
   int64_t n_bc;
+  /* bound mode: accumulate the per-entry parity bound (fem_oracle.py
+   * matrix_bound / vector_bound / lifting_bound) instead of the values */
+  int bound;
+  double rtol, frel;
 } job_t;
+
+static inline double absmax(const double* a, int n)
+{
+  double m = 0.0;
+  for (int i = 0; i < n; ++i) m = fmax(m, fabs(a[i]));
+  return m;
+}
 
 static inline int64_t find_col(const int32_t* row_ptr, const int32_t* col, int64_t row, int32_t c)
 {
@@ -273,6 +284,10 @@ static void* run_job(void* arg)
           rows[i * bs + a] = (int64_t)J->dofs[c * k + i] * bs + a;
           colsx[i * bs + a] = J->dofs[c * k + i] * bs + a;
         }
+      if (J->bound) {
+        const double f = J->frel * absmax(Ae, ks * ks);
+        for (int e = 0; e < ks * ks; ++e) Ae[e] = J->rtol * fabs(Ae[e]) + f;
+      }
       for (int ii = 0; ii < ks; ++ii) {
         int64_t r = rows[ii];
         if (r < rlo || r >= rhi || J->markers[r]) continue;
@@ -283,17 +298,23 @@ static void* run_job(void* arg)
         }
       }
     }
-    for (int64_t q = 0; q < J->n_bc; ++q) {
-      int64_t r = J->bc_dofs[q];
-      if (r < rlo || r >= rhi) continue;
-      int64_t s = find_col(J->row_ptr, J->col, r, (int32_t)r);
-      if (s >= 0) J->values[s] = J->diagonal;
-    }
+    /* the diagonal of BC rows is written, not summed: bound 0 */
+    if (!J->bound)
+      for (int64_t q = 0; q < J->n_bc; ++q) {
+        int64_t r = J->bc_dofs[q];
+        if (r < rlo || r >= rhi) continue;
+        int64_t s = find_col(J->row_ptr, J->col, r, (int32_t)r);
+        if (s >= 0) J->values[s] = J->diagonal;
+      }
   } else if (J->op == 1) { /* vector */
     for (int64_t r = rlo; r < rhi; ++r) J->b[r] = 0.0;
     for (int64_t q = 0; q < nmy; ++q) {
       int64_t c = my[q];
       tabulate_vec(J->kind, J->coords, J->cells + 4 * c, c, J->f, be);
+      if (J->bound) {
+        const double f = J->frel * absmax(be, ks);
+        for (int e = 0; e < ks; ++e) be[e] = J->rtol * fabs(be[e]) + f;
+      }
       for (int i = 0; i < k; ++i)
         for (int a = 0; a < bs; ++a) {
           int64_t r = (int64_t)J->dofs[c * k + i] * bs + a;
@@ -315,12 +336,26 @@ static void* run_job(void* arg)
           int64_t cc = (int64_t)J->dofs[c * k + j] * bs + b;
           d[j * bs + b] = J->markers[cc] ? (J->g[cc] - (J->x0 ? J->x0[cc] : 0.0)) : 0.0;
         }
+      double fl = 0.0;
+      if (J->bound) {
+        double dsum = 0.0;
+        for (int jj = 0; jj < ks; ++jj) {
+          d[jj] = fabs(d[jj]);
+          dsum += d[jj];
+        }
+        fl = J->frel * absmax(Ae, ks * ks) * dsum;
+      }
       for (int ii = 0; ii < ks; ++ii) {
         int64_t r = (int64_t)J->dofs[c * k + ii / bs] * bs + ii % bs;
         if (r < rlo || r >= rhi) continue;
         double s = 0.0;
-        for (int jj = 0; jj < ks; ++jj) s += Ae[ii * ks + jj] * d[jj];
-        J->b[r] -= J->scale * s;
+        if (J->bound) {
+          for (int jj = 0; jj < ks; ++jj) s += fabs(Ae[ii * ks + jj]) * d[jj];
+          J->b[r] += fabs(J->scale) * (J->rtol * s + fl);
+        } else {
+          for (int jj = 0; jj < ks; ++jj) s += Ae[ii * ks + jj] * d[jj];
+          J->b[r] -= J->scale * s;
+        }
       }
     }
   }
@@ -409,6 +444,210 @@ void cfem_apply_lifting(void* plan, int kind, const double* coords, const int32_
   J.b = b;
   run_all(&J);
 }
+
+/* Parity bounds of cfem_assemble_matrix and of cfem_assemble_vector +
+ * cfem_apply_lifting (per entry: rtol * sum |contributions| + frel * the
+ * largest |entry| of each contributing element; fem_oracle.py matrix_bound,
+ * vector_bound, lifting_bound); bound[] is overwritten, the set_bc rows are
+ * left to the caller (their bound is 0). */
+void cfem_matrix_bound(void* plan, int kind, const double* coords, const int32_t* cells, const int32_t* dofs,
+                       int bs, const double* coeff0, const double* coeff1, const int32_t* row_ptr,
+                       const int32_t* col, const uint8_t* markers, double* bound, double rtol, double frel)
+{
+  job_t J;
+  memset(&J, 0, sizeof(J));
+  J.plan = (plan_t*)plan;
+  J.kind = kind;
+  J.bs = bs;
+  J.op = 0;
+  J.coords = coords;
+  J.cells = cells;
+  J.dofs = dofs;
+  J.coeff0 = coeff0;
+  J.coeff1 = coeff1;
+  J.row_ptr = row_ptr;
+  J.col = col;
+  J.markers = markers;
+  J.values = bound;
+  J.bound = 1;
+  J.rtol = rtol;
+  J.frel = frel;
+  run_all(&J);
+}
+
+void cfem_rhs_bound(void* plan, int kind, const double* coords, const int32_t* cells, const int32_t* dofs, int bs,
+                    const double* f, const double* coeff0, const double* coeff1, const uint8_t* markers,
+                    const double* g, const double* x0, double scale, double* bound, double rtol, double frel)
+{
+  job_t J;
+  memset(&J, 0, sizeof(J));
+  J.plan = (plan_t*)plan;
+  J.kind = kind;
+  J.bs = bs;
+  J.coords = coords;
+  J.cells = cells;
+  J.dofs = dofs;
+  J.f = f;
+  J.b = bound;
+  J.bound = 1;
+  J.rtol = rtol;
+  J.frel = frel;
+  J.op = 1; /* zeroes the thread's rows, then the load vector's bound */
+  run_all(&J);
+  J.op = 2;
+  J.coeff0 = coeff0;
+  J.coeff1 = coeff1;
+  J.markers = markers;
+  J.g = g;
+  J.x0 = x0;
+  J.scale = scale;
+  run_all(&J);
+}
+
+/* ---------------- sparsity ----------------
+ * DOLFINx's SparsityPattern of a cell integral (sorted unique block columns
+ * of every block row) unrolled to scalar AIJ as cpp/cudolfinx/la/petsc.cpp:45-65
+ * does: row bs*R+a holds bs*C+b for each block column C, b = 0..bs-1.  Each
+ * thread builds the block rows it owns from the cells touching them. */
+typedef struct {
+  plan_t* plan;
+  int t, k, bs;
+  const int32_t* dofs;
+  int64_t* blen;      /* [nblocks] block columns per block row */
+  int32_t** bcols;    /* per thread: its rows' sorted block columns, concatenated */
+  const int32_t* row_ptr;
+  int32_t* col;
+} pat_job_t;
+
+static void* pattern_job(void* arg)
+{
+  pat_job_t* J = (pat_job_t*)arg;
+  plan_t* P = J->plan;
+  const int k = J->k;
+  const int64_t lo = P->row_lo[J->t], hi = P->row_lo[J->t + 1], nr = hi - lo;
+  const int64_t* my = P->cells[J->t];
+  const int64_t nmy = P->ncells[J->t];
+  if (J->col == NULL) {
+    /* couplings per owned row, then the sorted unique block columns */
+    int64_t* start = (int64_t*)calloc((size_t)nr + 1, sizeof(int64_t));
+    for (int64_t q = 0; q < nmy; ++q)
+      for (int i = 0; i < k; ++i) {
+        int64_t R = J->dofs[my[q] * k + i];
+        if (R >= lo && R < hi) start[R - lo + 1] += k;
+      }
+    for (int64_t r = 0; r < nr; ++r) start[r + 1] += start[r];
+    int32_t* buf = (int32_t*)malloc(sizeof(int32_t) * (size_t)(start[nr] ? start[nr] : 1));
+    int64_t* fill = (int64_t*)malloc(sizeof(int64_t) * (size_t)(nr ? nr : 1));
+    for (int64_t r = 0; r < nr; ++r) fill[r] = start[r];
+    for (int64_t q = 0; q < nmy; ++q) {
+      const int32_t* cd = J->dofs + my[q] * k;
+      for (int i = 0; i < k; ++i) {
+        int64_t R = cd[i];
+        if (R < lo || R >= hi) continue;
+        for (int j = 0; j < k; ++j) buf[fill[R - lo]++] = cd[j];
+      }
+    }
+    /* in place: sort each row's list (insertion sort, rows are short), drop repeats */
+    int64_t out = 0;
+    for (int64_t r = 0; r < nr; ++r) {
+      int32_t* a = buf + start[r];
+      int64_t n = start[r + 1] - start[r];
+      for (int64_t i = 1; i < n; ++i) {
+        int32_t v = a[i];
+        int64_t j = i - 1;
+        while (j >= 0 && a[j] > v) {
+          a[j + 1] = a[j];
+          --j;
+        }
+        a[j + 1] = v;
+      }
+      int64_t m = 0;
+      for (int64_t i = 0; i < n; ++i)
+        if (m == 0 || buf[out + m - 1] != a[i]) {
+          buf[out + m] = a[i];
+          ++m;
+        }
+      J->blen[lo + r] = m;
+      out += m;
+    }
+    J->bcols[J->t] = buf;
+    free(fill);
+    free(start);
+  } else {
+    const int bs = J->bs;
+    const int32_t* bc = J->bcols[J->t];
+    for (int64_t R = lo; R < hi; ++R) {
+      const int64_t m = J->blen[R];
+      for (int a = 0; a < bs; ++a) {
+        int32_t* dst = J->col + J->row_ptr[R * bs + a];
+        for (int64_t u = 0; u < m; ++u)
+          for (int b = 0; b < bs; ++b) dst[u * bs + b] = bc[u] * bs + b;
+      }
+      bc += m;
+    }
+  }
+  return NULL;
+}
+
+static void run_pattern(pat_job_t* proto)
+{
+  int T = proto->plan->nthreads;
+  pthread_t* th = (pthread_t*)malloc(sizeof(pthread_t) * T);
+  pat_job_t* jobs = (pat_job_t*)malloc(sizeof(pat_job_t) * T);
+  for (int t = 0; t < T; ++t) {
+    jobs[t] = *proto;
+    jobs[t].t = t;
+    pthread_create(&th[t], NULL, pattern_job, &jobs[t]);
+  }
+  for (int t = 0; t < T; ++t) pthread_join(th[t], NULL);
+  free(jobs);
+  free(th);
+}
+
+/* Returns nnz and malloc'd row_ptr [nblocks*bs+1] / col [nnz] (release with
+ * cfem_free), or -1 if nnz does not fit int32 indices. */
+int64_t cfem_pattern_build(void* plan, const int32_t* dofs, int k, int bs, int64_t nblocks, int32_t** row_ptr,
+                           int32_t** col)
+{
+  plan_t* P = (plan_t*)plan;
+  pat_job_t J;
+  memset(&J, 0, sizeof(J));
+  J.plan = P;
+  J.k = k;
+  J.bs = bs;
+  J.dofs = dofs;
+  J.blen = (int64_t*)calloc((size_t)(nblocks ? nblocks : 1), sizeof(int64_t));
+  J.bcols = (int32_t**)calloc(P->nthreads, sizeof(int32_t*));
+  run_pattern(&J);
+  const int64_t nrows = nblocks * bs;
+  int32_t* rp = (int32_t*)malloc(sizeof(int32_t) * (size_t)(nrows + 1));
+  int64_t acc = 0;
+  rp[0] = 0;
+  for (int64_t R = 0; R < nblocks; ++R)
+    for (int a = 0; a < bs; ++a) {
+      acc += J.blen[R] * bs;
+      if (acc > 2147483647) {
+        for (int t = 0; t < P->nthreads; ++t) free(J.bcols[t]);
+        free(J.bcols);
+        free(J.blen);
+        free(rp);
+        return -1;
+      }
+      rp[R * bs + a + 1] = (int32_t)acc;
+    }
+  int32_t* cl = (int32_t*)malloc(sizeof(int32_t) * (size_t)(acc ? acc : 1));
+  J.row_ptr = rp;
+  J.col = cl;
+  run_pattern(&J);
+  for (int t = 0; t < P->nthreads; ++t) free(J.bcols[t]);
+  free(J.bcols);
+  free(J.blen);
+  *row_ptr = rp;
+  *col = cl;
+  return acc;
+}
+
+void cfem_free(void* p) { free(p); }
 
 void cfem_set_bc(double* b, const int32_t* bc_dofs, int64_t n_bc, const double* g,
                  const double* x0, double scale)

@@ -68,6 +68,11 @@ def lib():
         L.cfem_assemble_vector.argtypes = [vp, i32, vp, vp, vp, i32, vp, vp]
         L.cfem_apply_lifting.argtypes = [vp, i32, vp, vp, vp, i32, vp, vp, vp, vp, vp, dbl, vp]
         L.cfem_set_bc.argtypes = [vp, vp, i64, vp, vp, dbl]
+        L.cfem_matrix_bound.argtypes = [vp, i32, vp, vp, vp, i32, vp, vp, vp, vp, vp, vp, dbl, dbl]
+        L.cfem_rhs_bound.argtypes = [vp, i32, vp, vp, vp, i32, vp, vp, vp, vp, vp, vp, dbl, vp, dbl, dbl]
+        L.cfem_pattern_build.restype = i64
+        L.cfem_pattern_build.argtypes = [vp, vp, i32, i32, i64, ctypes.POINTER(vp), ctypes.POINTER(vp)]
+        L.cfem_free.argtypes = [vp]
         r2w = np.ascontiguousarray(fo.ref_grad_tensor(2, True))
         r2 = np.ascontiguousarray(fo.ref_grad_tensor(2, False))
         w2 = np.ascontiguousarray(fo.ref_basis_integrals(2))
@@ -82,6 +87,31 @@ def lib():
 
 def _p(a):
     return None if a is None else a.ctypes.data
+
+
+def pattern(dofs, num_blocks, bs=1, nthreads=None):
+    """CSR pattern (row_ptr, col) of a cell integral on one dofmap, built by
+    row-owning threads: DOLFINx's sorted unique block columns per block row,
+    unrolled to scalar rows as cpp/cudolfinx/la/petsc.cpp:45-65 does (the same
+    arrays as fem_oracle.sparsity)."""
+    L = lib()
+    d = np.ascontiguousarray(dofs, dtype=np.int32)
+    nthreads = nthreads or os.cpu_count() or 1
+    plan = L.cfem_plan_create(nthreads, d.ctypes.data, d.shape[0], d.shape[1], num_blocks)
+    try:
+        rp, cl = ctypes.c_void_p(), ctypes.c_void_p()
+        nnz = L.cfem_pattern_build(plan, d.ctypes.data, d.shape[1], bs, num_blocks, ctypes.byref(rp),
+                                   ctypes.byref(cl))
+        if nnz < 0:
+            raise ValueError("pattern has more than 2^31-1 entries")
+        nrows = num_blocks * bs
+        row_ptr = np.ctypeslib.as_array((ctypes.c_int32 * (nrows + 1)).from_address(rp.value)).copy()
+        col = np.ctypeslib.as_array((ctypes.c_int32 * max(nnz, 1)).from_address(cl.value))[:nnz].copy()
+        L.cfem_free(rp)
+        L.cfem_free(cl)
+    finally:
+        L.cfem_plan_destroy(plan)
+    return row_ptr, col
 
 
 class CpuAssembler:
@@ -129,6 +159,24 @@ class CpuAssembler:
                                     _p(self.markers), _p(self.values), diagonal, _p(self.bc_dofs),
                                     len(self.bc_dofs))
         return self.values
+
+    def matrix_bound(self, rtol=fo.PARITY_RTOL, frel=fo.PARITY_FREL):
+        """Per-slot parity bound of assemble_matrix (fem_oracle.matrix_bound)."""
+        out = np.empty(len(self.col))
+        self.L.cfem_matrix_bound(self.plan, self.kind, _p(self.coords), _p(self.cells), _p(self.dofs), self.bs,
+                                 _p(self.c0), _p(self.c1), _p(self.row_ptr), _p(self.col), _p(self.markers),
+                                 _p(out), rtol, frel)
+        return out
+
+    def rhs_bound(self, scale=1.0, rtol=fo.PARITY_RTOL, frel=fo.PARITY_FREL):
+        """Per-entry parity bound of assemble_rhs (vector_bound + lifting_bound,
+        0 on the set_bc rows)."""
+        out = np.empty(len(self.b))
+        self.L.cfem_rhs_bound(self.plan, self.kind, _p(self.coords), _p(self.cells), _p(self.dofs), self.bs,
+                              _p(self.f), _p(self.c0), _p(self.c1), _p(self.markers), _p(self.g), None, scale,
+                              _p(out), rtol, frel)
+        out[self.bc_dofs] = 0.0
+        return out
 
     def assemble_rhs(self, scale=1.0):
         self.L.cfem_assemble_vector(self.plan, self.kind, _p(self.coords), _p(self.cells), _p(self.dofs),

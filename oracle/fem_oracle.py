@@ -677,6 +677,92 @@ def set_bc(b, bc_dofs, g, x0=None, scale=1.0):
 
 
 # ---------------------------------------------------------------------------
+# Parity bounds: how far an assembled entry may lie from the oracle's
+# ---------------------------------------------------------------------------
+#
+# An assembled entry is a sum of element contributions added in an order the
+# reference leaves open (FP64 atomics, CUDAFormIntegral.cpp:1154-1224).  Its
+# bound is per entry: PARITY_RTOL times the sum of the |contributions| (the
+# reordering error of a sum is at most (m-1) u sum|c_i|, u = 2^-53, far below
+# 1e-12 for the m <= 100 contributions of these meshes), plus PARITY_FREL
+# times the largest |entry| of each contributing element (the element
+# tensor's own rounding: an entry that is zero or cancels inside one element
+# is computed to a few ulps of that element's scale, which depends on the
+# element's coefficient and size, never on the rest of the matrix).  Entries
+# nothing contributes to, and the values written by set_diagonal / set_bc,
+# have bound 0: they must match exactly.
+
+PARITY_RTOL = 1e-12
+PARITY_FREL = 1e-14
+
+
+def _element_floor(T):
+    """Largest |entry| of each element tensor T [C, ...]."""
+    T = np.abs(np.asarray(T))
+    return T.reshape(len(T), -1).max(axis=1) if len(T) else np.zeros(0)
+
+
+def matrix_bound(Ae, dofs0, dofs1, row_ptr, col, bs0=1, bs1=1, bc0_markers=None, bc1_markers=None,
+                 rtol=PARITY_RTOL, frel=PARITY_FREL):
+    """Per-slot parity bound of assemble_matrix(Ae, ...): the same scatter of
+    rtol*|Ae| + frel*max|Ae_cell| (BC rows / columns skipped, so BC rows --
+    whose diagonal set_diagonal writes -- have bound 0)."""
+    Ae = np.asarray(Ae)
+    contrib = rtol * np.abs(Ae) + frel * _element_floor(Ae).reshape((-1,) + (1,) * (Ae.ndim - 1))
+    return assemble_matrix(contrib, dofs0, dofs1, row_ptr, col, bs0, bs1, bc0_markers, bc1_markers)
+
+
+def vector_bound(be, dofs, num_values, bs=1, rtol=PARITY_RTOL, frel=PARITY_FREL):
+    """Per-entry parity bound of assemble_vector(be, ...)."""
+    be = np.asarray(be)
+    contrib = rtol * np.abs(be) + frel * _element_floor(be).reshape((-1,) + (1,) * (be.ndim - 1))
+    return assemble_vector(contrib, dofs, num_values, bs)
+
+
+def lifting_bound(num_values, Ae, dofs0, dofs1, bc1_markers, g, x0=None, scale=1.0, bs0=1, bs1=1,
+                  rtol=PARITY_RTOL, frel=PARITY_FREL):
+    """Per-entry parity bound of apply_lifting: for row i of a cell with BC
+    columns, rtol*|scale|*sum_j |Ae_ij d_j| + frel*|scale|*max|Ae_cell|*sum_j |d_j|
+    (d = g - x0 on the cell's BC columns)."""
+    u0 = scalar_cell_dofs(dofs0, bs0)  # -1 outside a restriction
+    u1 = scalar_cell_dofs(dofs1, bs1)
+    out = np.zeros(num_values)
+    m = (u1 >= 0) & (np.asarray(bc1_markers)[np.maximum(u1, 0)] != 0)
+    has = np.nonzero(m.any(axis=1))[0]
+    if len(has) == 0:
+        return out
+    u0h, u1h, mh = u0[has], np.maximum(u1[has], 0), m[has]
+    d = np.abs(np.where(mh, g[u1h] - (x0[u1h] if x0 is not None else 0.0), 0.0))
+    A = np.abs(np.asarray(Ae)[has])
+    per_row = rtol * np.einsum("cij,cj->ci", A, d) + (frel * _element_floor(A) * d.sum(axis=1))[:, None]
+    keep = u0h >= 0
+    np.add.at(out, u0h[keep], abs(scale) * per_row[keep])
+    return out
+
+
+def diagonal_bound(Ae, dofs, num_values, bs=1, rtol=PARITY_RTOL, frel=PARITY_FREL):
+    """Per-entry parity bound of assemble_diagonal: rtol*|Ae_ii| + frel*max|Ae_cell|."""
+    Ae = np.asarray(Ae)
+    contrib = rtol * np.abs(np.diagonal(Ae, axis1=1, axis2=2)) + frel * _element_floor(Ae)[:, None]
+    return assemble_vector(contrib, dofs, num_values, bs)
+
+
+def within_bound(gpu, ref, bound):
+    """(all |gpu - ref| <= bound, worst |gpu - ref| / bound); a nonzero
+    difference where the bound is 0 counts as infinitely far."""
+    gpu = np.asarray(gpu, dtype=np.float64)
+    ref = np.asarray(ref, dtype=np.float64)
+    bound = np.broadcast_to(np.asarray(bound, dtype=np.float64), ref.shape)
+    err = np.abs(gpu - ref)
+    ok = bool(np.all(err <= bound))
+    if not err.size:
+        return ok, 0.0
+    with np.errstate(divide="ignore", invalid="ignore"):
+        ratio = np.where(err == 0.0, 0.0, err / bound)
+    return ok, float(np.max(ratio))
+
+
+# ---------------------------------------------------------------------------
 # Block / restricted systems (python/cudolfinx/form.py:107-225,
 # assemble.py:112-202, cpp/cudolfinx/fem/petsc.h:39-107, fem/utils.h:14-98)
 # ---------------------------------------------------------------------------
@@ -748,6 +834,28 @@ def assemble_block_matrix(blocks, row_ptr, col, diagonal=1.0):
             d = dpos[B["row_offset"] + np.asarray(B["bc_rows"], dtype=np.int64)]
             values[d[d >= 0]] = diagonal
     return values
+
+
+def block_matrix_bound(blocks, row_ptr, col, rtol=PARITY_RTOL, frel=PARITY_FREL):
+    """Per-slot parity bound of assemble_block_matrix (the bound of
+    matrix_bound for every block at its offsets; 0 on the BC diagonals)."""
+    bb = []
+    for B in blocks:
+        Ae = np.asarray(B["Ae"])
+        c = dict(B)
+        c["Ae"] = rtol * np.abs(Ae) + frel * _element_floor(Ae).reshape((-1,) + (1,) * (Ae.ndim - 1))
+        bb.append(c)
+    return assemble_block_matrix(bb, row_ptr, col, diagonal=0.0)
+
+
+def block_vector_bound(parts, size, rtol=PARITY_RTOL, frel=PARITY_FREL):
+    """Per-entry parity bound of assemble_block_vector."""
+    out = []
+    for be, dofs, bs, off in parts:
+        be = np.asarray(be)
+        out.append((rtol * np.abs(be) + frel * _element_floor(be).reshape((-1,) + (1,) * (be.ndim - 1)), dofs,
+                    bs, off))
+    return assemble_block_vector(out, size)
 
 
 def assemble_block_vector(parts, size):
@@ -1020,7 +1128,9 @@ def element_vectors(P):
 
 def solve_system(P):
     """Full oracle pipeline: A with BCs, b = assemble + lifting + set_bc.
-    Returns dict(row_ptr, col, A, b)."""
+    Returns dict(row_ptr, col, A, b, markers, A_bound, b_bound), the last two
+    the per-entry parity bounds (matrix_bound, vector_bound + lifting_bound,
+    0 on the set_bc rows)."""
     bs = P["bs"]
     dofs = P["dofs"]
     nscal = P["ndof"] * bs
@@ -1033,7 +1143,12 @@ def solve_system(P):
     b = assemble_vector(be, dofs, nscal, bs)
     b = apply_lifting(b, Ae, dofs, dofs, markers, P["g"], None, 1.0, bs, bs)
     b = set_bc(b, P["bc_dofs"], P["g"])
-    return {"row_ptr": row_ptr, "col": col, "A": A, "b": b, "markers": markers}
+    A_bound = matrix_bound(Ae, dofs, dofs, row_ptr, col, bs, bs, markers, markers)
+    b_bound = vector_bound(be, dofs, nscal, bs) + lifting_bound(nscal, Ae, dofs, dofs, markers, P["g"], None,
+                                                                1.0, bs, bs)
+    b_bound[np.asarray(P["bc_dofs"])] = 0.0
+    return {"row_ptr": row_ptr, "col": col, "A": A, "b": b, "markers": markers, "A_bound": A_bound,
+            "b_bound": b_bound}
 
 
 def nnz_formula(kind: str, n: int) -> int:

@@ -6,7 +6,9 @@ The reference ships no golden vectors (its tests compare against DOLFINx at
 run time, python/test/test_cuda_assembly.py:93-209) and DOLFINx cannot run in
 this environment, so these fixtures freeze the oracle's output on small
 meshes: mesh, dofmap, BC dofs, coefficients, CSR pattern, assembled matrix
-(BCs applied, unit diagonal) and right-hand side (vector + lifting + set_bc).
+(BCs applied, unit diagonal) and right-hand side (vector + lifting + set_bc),
+and each entry's parity bound (A_bound, b_bound: fem_oracle.matrix_bound,
+vector_bound + lifting_bound, 0 where set_diagonal / set_bc write).
 They pin the oracle against regressions and give the GPU tests inputs that do
 not depend on the generators.
 """
@@ -28,6 +30,7 @@ def make(kind, n):
     S = fo.solve_system(P)
     out = dict(coords=P["coords"], cells=P["cells"], dofs=P["dofs"], bc_dofs=P["bc_dofs"],
                row_ptr=S["row_ptr"], col=S["col"], A=S["A"], b=S["b"], g=P["g"],
+               A_bound=S["A_bound"], b_bound=S["b_bound"],
                ndof=np.array(P["ndof"]), bs=np.array(P["bs"]), n=np.array(n))
     for key in ("k", "f", "lam", "mu"):
         if P.get(key) is not None:

@@ -5,19 +5,15 @@ import numpy as np
 from conftest import ensure_library
 
 
-def tolerance_check(gpu, ref, rtol=1e-12, floor=1e-13):
-    """Entrywise |gpu - ref| <= rtol*|ref| + floor*max|ref|.
+def tolerance_check(gpu, ref, bound):
+    """Entrywise |gpu - ref| <= bound, the oracle's per-entry parity bound
+    (fem_oracle.matrix_bound / vector_bound / lifting_bound: 1e-12 times the
+    sum of the entry's |contributions| plus 1e-14 times each contributing
+    element's largest |entry|; 0 where the value is written, not summed).
+    Returns (ok, worst |gpu - ref| / bound)."""
+    from oracle import fem_oracle as fo
 
-    FP64 atomics add contributions in a different order than the oracle; an
-    entry whose contributions cancel ends at rounding level, so a floor
-    relative to the largest entry is part of the bound."""
-    gpu = np.asarray(gpu)
-    ref = np.asarray(ref)
-    scale = max(np.abs(ref).max() if ref.size else 0.0, 1e-300)
-    err = np.abs(gpu - ref)
-    bound = rtol * np.abs(ref) + floor * scale
-    worst = np.max(err / np.maximum(np.abs(ref), floor * scale / rtol)) if ref.size else 0.0
-    return bool(np.all(err <= bound)), float(worst)
+    return fo.within_bound(gpu, ref, bound)
 
 
 def mirror_problem(P, precision="fp64"):

@@ -1,6 +1,6 @@
 """Interior-facet (dS) integrals of discontinuous spaces on the GPU against
-the oracle: jump penalty on DG0 / DG1 (pattern bit-exact, values within 1e-12
-relative entrywise with a 1e-13*max|A| floor), average loads with lifting and
+the oracle: jump penalty on DG0 / DG1 (pattern bit-exact, values within the
+oracle's per-entry bound, fem_oracle.matrix_bound), average loads with lifting and
 set_bc, the jump-norm functional (1e-12 relative), and a DG cell term plus
 its jump term summed into one matrix on the union pattern.
 
@@ -48,10 +48,11 @@ def test_jump_penalty_matches_oracle(degree, alpha_kind):
     d = fo.dg_dofmap(C, degree)
     m = fo.macro_dofmap(d, q)
     rp_o, col_o = fo.sparsity(m, m, V.num_dofs)
-    v_o = fo.assemble_matrix(fo.interior_jump_tensors(coords, cells, q, degree, af), m, m, rp_o, col_o)
+    Ae = fo.interior_jump_tensors(coords, cells, q, degree, af)
+    v_o = fo.assemble_matrix(Ae, m, m, rp_o, col_o)
     rp, col = A.sparsity.to_host()
     assert np.array_equal(rp, rp_o) and np.array_equal(col, col_o)
-    ok, worst = tolerance_check(A.values.cpu().numpy(), v_o)
+    ok, worst = tolerance_check(A.values.cpu().numpy(), v_o, fo.matrix_bound(Ae, m, m, rp_o, col_o))
     assert ok, worst
 
 
@@ -74,13 +75,16 @@ def test_average_load_lifting_and_set_bc(degree):
     asm.set_bc(b, [bc], V)
     d = fo.dg_dofmap(C, degree)
     m = fo.macro_dofmap(d, q)
-    b_o = fo.assemble_vector(fo.interior_avg_load(coords, cells, q, degree, fo.facet_average(gv, q)), m, N)
+    be = fo.interior_avg_load(coords, cells, q, degree, fo.facet_average(gv, q))
+    b_o = fo.assemble_vector(be, m, N)
     mk = np.zeros(N, dtype=np.uint8)
     mk[bc_dofs] = 1
     Ae = fo.interior_jump_tensors(coords, cells, q, degree, np.full(len(q), 1.5))
     b_o = fo.apply_lifting(b_o, Ae, m, m, mk, gbc)
     b_o = fo.set_bc(b_o, bc_dofs, gbc)
-    ok, worst = tolerance_check(b.to_host(), b_o)
+    bound = fo.vector_bound(be, m, N) + fo.lifting_bound(N, Ae, m, m, mk, gbc)
+    bound[bc_dofs] = 0.0
+    ok, worst = tolerance_check(b.to_host(), b_o, bound)
     assert ok, worst
 
 
@@ -119,13 +123,13 @@ def test_cell_and_jump_terms_in_one_matrix():
     m = fo.macro_dofmap(d, q)
     N = V.num_dofs
     rp_o, col_o = fo.block_pattern([(d, d, 1, 1, 0, 0), (m, m, 1, 1, 0, 0)], N, N)
-    v_o = fo.assemble_block_matrix([
-        dict(Ae=fo.p1_stiffness(coords, cells), dofs0=d, dofs1=d, bs0=1, bs1=1, row_offset=0, col_offset=0),
-        dict(Ae=fo.interior_jump_tensors(coords, cells, q, 1, np.full(len(q), 4.0)), dofs0=m, dofs1=m, bs0=1,
-             bs1=1, row_offset=0, col_offset=0)], rp_o, col_o)
+    blk = [dict(Ae=fo.p1_stiffness(coords, cells), dofs0=d, dofs1=d, bs0=1, bs1=1, row_offset=0, col_offset=0),
+           dict(Ae=fo.interior_jump_tensors(coords, cells, q, 1, np.full(len(q), 4.0)), dofs0=m, dofs1=m, bs0=1,
+                bs1=1, row_offset=0, col_offset=0)]
+    v_o = fo.assemble_block_matrix(blk, rp_o, col_o)
     rp, col = A.sparsity.to_host()
     assert np.array_equal(rp, rp_o) and np.array_equal(col, col_o)
-    ok, worst = tolerance_check(A.values.cpu().numpy(), v_o)
+    ok, worst = tolerance_check(A.values.cpu().numpy(), v_o, fo.block_matrix_bound(blk, rp_o, col_o))
     assert ok, worst
 
 

@@ -33,7 +33,7 @@ def _items():
 def _check(mat, ref, prec):
     got = mat.values.cpu().numpy()
     if prec == "fp64":
-        ok, worst = tolerance_check(got, ref["A"])
+        ok, worst = tolerance_check(got, ref["A"], ref["A_bound"])
         assert ok, worst
     else:
         frob = np.linalg.norm(got - ref["A"]) / np.linalg.norm(ref["A"])

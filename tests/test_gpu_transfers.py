@@ -3,7 +3,8 @@ the last kernels that read the same buffer, read-backs on the download stream
 before the next write into the vector.  Assembling several steps in a row
 with coefficients that change every step, reading each right-hand side back
 asynchronously, must give the same results as running every step to
-completion before the next (1e-12 relative: FP64 atomics sum in any order).
+completion before the next: both within the oracle's per-entry bound of the
+oracle's system for that step's coefficients (FP64 atomics sum in any order).
 """
 import numpy as np
 import pytest
@@ -52,9 +53,14 @@ def test_overlapped_transfers_match_synchronous_steps(kind, n):
     b_ovl, A_ovl = _steps(P, True)
     b_syn, A_syn = _steps(P, False)
     for s in range(len(b_syn)):
-        ok, worst = tolerance_check(b_ovl[s], b_syn[s])
-        assert ok, (s, worst)
-        ok, worst = tolerance_check(A_ovl[s], A_syn[s])
-        assert ok, (s, worst)
+        Ps = dict(P)
+        Ps["k"] = P["k"] * (1.0 + 0.5 * s)
+        Ps["f"] = P["f"] * (1.0 - 0.25 * s)
+        S = fo.solve_system(Ps)
+        for b, A in ((b_ovl[s], A_ovl[s]), (b_syn[s], A_syn[s])):
+            ok, worst = tolerance_check(b, S["b"], S["b_bound"])
+            assert ok, (s, worst)
+            ok, worst = tolerance_check(A, S["A"], S["A_bound"])
+            assert ok, (s, worst)
     # the steps differ (the coefficients changed), so a stale upload would show
     assert np.abs(b_syn[0] - b_syn[1]).max() > 0

@@ -156,11 +156,27 @@ def test_c_port_matches_numpy_oracle(kind, n):
     P = fo.build_problem(kind, n)
     S = fo.solve_system(P)
     C = cfem.CpuAssembler(P, S["row_ptr"], S["col"], nthreads=3)
-    v = C.assemble_matrix()
-    b = C.assemble_rhs()
+    v = C.assemble_matrix().copy()
+    b = C.assemble_rhs().copy()
+    vb = C.matrix_bound()
+    bb = C.rhs_bound()
     C.close()
-    assert np.abs(v - S["A"]).max() <= 1e-13 * np.abs(S["A"]).max()
-    assert np.abs(b - S["b"]).max() <= 1e-13 * max(1.0, np.abs(S["b"]).max())
+    ok, worst = fo.within_bound(v, S["A"], S["A_bound"])
+    assert ok, worst
+    ok, worst = fo.within_bound(b, S["b"], S["b_bound"])
+    assert ok, worst
+    # the C port's bounds are the numpy oracle's (summed in another order)
+    assert np.allclose(vb, S["A_bound"], rtol=1e-12, atol=0)
+    assert np.allclose(bb, S["b_bound"], rtol=1e-12, atol=0)
+
+
+@pytest.mark.parametrize("kind,n", [("p1", 4), ("p2", 3), ("vp2", 2), ("p3", 2)])
+def test_c_pattern_matches_numpy_oracle(kind, n):
+    P = fo.build_problem(kind, n)
+    rp, col = fo.sparsity(P["dofs"], P["dofs"], P["ndof"], P["bs"], P["bs"])
+    for threads in (1, 3):
+        rp_c, col_c = cfem.pattern(P["dofs"], P["ndof"], P["bs"], nthreads=threads)
+        assert np.array_equal(rp_c, rp) and np.array_equal(col_c, col)
 
 
 def test_exterior_facets_and_facet_tensors():
