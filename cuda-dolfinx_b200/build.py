@@ -70,7 +70,8 @@ def build(force=False, verbose_ptxas=False, quiet=True):
             print(log)
     if _newer(LIB, objs):
         tmp = LIB + f".tmp{os.getpid()}"
-        cmd = [NVCC, *ARCH, "-shared", "-o", tmp, *objs, "-lpthread"]
+        # NVRTC compiles forms given as FFCx tabulate_tensor bodies at run time
+        cmd = [NVCC, *ARCH, "-shared", "-o", tmp, *objs, "-lpthread", "-lnvrtc"]
         subprocess.check_call(cmd)
         os.replace(tmp, LIB)
     return LIB

@@ -562,6 +562,7 @@ int fe_form_set_coefficient(fe_form f, int index, int coeff_kind, fe_dofmap cmap
                             int values_on_device, void* stream) {
   return guard([&] {
     FE_REQUIRE(f, "null form");
+    FE_REQUIRE(!f->ffcx, "FFCx forms take their coefficients through fe_form_set_coefficient_field");
     DeviceScope d(f->ctx);
     const int ncoef =
         (f->kind == FE_FORM_VP2_ELASTICITY || f->kind == FE_FORM_P1_ENERGY || f->kind == FE_FORM_P2_ENERGY) ? 2 : 1;
@@ -634,6 +635,7 @@ int fe_form_set_facets(fe_form f, const int32_t* pairs, int64_t num_facets) {
         FE_FAIL(FE_ERR_ARG, "facet " + std::to_string(q) + " is not a (cell, local facet 0..3) pair of the mesh");
     upload(f->facets, pairs, (size_t)(2 * num_facets));
     f->num_facets = num_facets;
+    f->facets_set = true;
   });
 }
 
@@ -681,6 +683,7 @@ int fe_form_set_interior_facets(fe_form f, const int32_t* quads, int64_t num_fac
         }
       upload(dst, m.data(), m.size());
     }
+    if (f->ffcx) ffcx_set_interior_permutations(*f);
     f->sp = nullptr;  // the byte map depends on the facets: bind again
     f->view.reset();
   });
@@ -765,6 +768,48 @@ int fe_form_destroy(fe_form f) {
   return guard([&] { delete f; });
 }
 
+int fe_form_create_ffcx(fe_context ctx, fe_mesh mesh, fe_dofmap test, fe_dofmap trial, int integral_type,
+                        const char* tabulate_name, const char* tabulate_body, int num_coefficients,
+                        const int* coefficient_sizes, int num_constants, const char* cachedir, fe_form* out) {
+  return guard([&] {
+    DeviceScope d(ctx);
+    FE_REQUIRE(out && mesh, "null argument");
+    FE_REQUIRE(test || !trial, "a trial dofmap needs a test dofmap");
+    for (fe_dofmap V : {test, trial}) {
+      if (!V) continue;
+      FE_REQUIRE(V->ctx == ctx && V->num_cells == mesh->num_cells, "dofmap and mesh cell counts differ");
+      FE_REQUIRE(!V->excluded || integral_type == FE_INTEGRAL_CELL,
+                 "facet integrals take unrestricted dofmaps");
+    }
+    auto f = std::make_unique<fe_form_s>();
+    f->ctx = ctx;
+    f->rank = (test ? 1 : 0) + (trial ? 1 : 0);
+    f->mesh = mesh;
+    f->V0 = test;
+    f->V1 = trial;
+    ffcx_create(*f, integral_type, tabulate_name, tabulate_body, num_coefficients, coefficient_sizes, num_constants,
+                cachedir);
+    *out = f.release();
+  });
+}
+
+int fe_form_set_coefficient_field(fe_form f, int index, fe_dofmap cmap, const double* values, int64_t n,
+                                  int values_on_device, void* stream) {
+  return guard([&] {
+    FE_REQUIRE(f && f->ffcx, "not a form built from an FFCx body");
+    DeviceScope d(f->ctx);
+    ffcx_set_coefficient(*f, index, cmap, values, n, values_on_device != 0, as_stream(stream));
+  });
+}
+
+int fe_form_set_constants(fe_form f, const double* values, int n, void* stream) {
+  return guard([&] {
+    FE_REQUIRE(f && f->ffcx, "not a form built from an FFCx body");
+    DeviceScope d(f->ctx);
+    ffcx_set_constants(*f, values, n, as_stream(stream));
+  });
+}
+
 int fe_bc_create(fe_context ctx, int64_t num_dofs, const uint8_t* markers, const int32_t* dofs, int64_t n_bc,
                  int64_t n_owned, const double* g, fe_bc* out) {
   return guard([&] {
@@ -830,6 +875,15 @@ int fe_assemble_matrix(fe_form a, double* values, fe_bc bc0, fe_bc bc1, double d
       FE_REQUIRE(!(flags & (FE_ASM_DETERMINISTIC | FE_ASM_SORTED_SLOT | FE_ASM_TILE | FE_ASM_ROW_GATHER |
                             FE_ASM_BLOCK)),
                  "a form bound to a block pattern assembles with the atomic scatter only");
+    if (a->ffcx) {
+      FE_REQUIRE(!(flags & (FE_ASM_DETERMINISTIC | FE_ASM_SORTED_SLOT | FE_ASM_TILE | FE_ASM_ROW_GATHER |
+                            FE_ASM_BLOCK)),
+                 "forms built from FFCx bodies assemble with the atomic scatter only");
+      if (zero) launch_zero(values, a->sp->nnz, st);
+      ffcx_assemble_matrix(*a, values, bc0, bc1, st);
+      if (bc0) launch_set_diagonal(*a->sp, *bc0, diagonal, values, st);
+      return;
+    }
     if (is_ifacet_kind(a->kind)) {
       FE_REQUIRE(!(flags & (FE_ASM_DETERMINISTIC | FE_ASM_SORTED_SLOT | FE_ASM_TILE | FE_ASM_ROW_GATHER |
                             FE_ASM_BLOCK)),
@@ -943,6 +997,12 @@ int fe_assemble_matrix_batch(fe_form a, int num_instances, const double* const* 
 int fe_assemble_scalar(fe_form M, double* result, void* stream) {
   return guard([&] {
     FE_REQUIRE(M && result, "null argument");
+    if (M->ffcx) {
+      FE_REQUIRE(M->rank == 0, "assemble_scalar needs a functional");
+      DeviceScope d(M->ctx);
+      *result = ffcx_assemble_scalar(*M, as_stream(stream));
+      return;
+    }
     FE_REQUIRE(M->rank == 0 && is_scalar_kind(M->kind), "assemble_scalar needs a functional");
     if (M->kind == FE_FORM_INTEGRAL || M->kind == FE_FORM_FACET_INTEGRAL || M->kind == FE_FORM_JUMP_NORM)
       FE_REQUIRE(M->coeff[0].kind >= 0, "coefficient 0 is not set");
@@ -967,6 +1027,13 @@ int fe_assemble_vector(fe_form Lf, double* b, unsigned flags, void* stream) {
     FE_REQUIRE(Lf, "null form");
     FE_REQUIRE(Lf->rank == 1, "assemble_vector needs a linear form");
     FE_REQUIRE(b || scalar_size(Lf->V0) == 0, "null vector");
+    if (Lf->ffcx) {
+      DeviceScope d(Lf->ctx);
+      cudaStream_t st = as_stream(stream);
+      if (flags & FE_ASM_ZERO) launch_zero(b, scalar_size(Lf->V0), st);
+      ffcx_assemble_vector(*Lf, b, st);
+      return;
+    }
     FE_REQUIRE(Lf->coeff[0].kind >= 0, "coefficient 0 (f) is not set");
     DeviceScope d(Lf->ctx);
     cudaStream_t st = as_stream(stream);
@@ -1000,6 +1067,7 @@ int fe_assemble_diagonal(fe_form a, double* b, unsigned flags, void* stream) {
   return guard([&] {
     FE_REQUIRE(a, "null form");
     FE_REQUIRE(a->rank == 2, "the diagonal is taken of a bilinear form");
+    FE_REQUIRE(!a->ffcx, "the diagonal of an FFCx form is a linear form of its own (FFCx's \"part\": \"diagonal\")");
     FE_REQUIRE(a->V0 && a->V1 && a->V0->num_blocks == a->V1->num_blocks && a->V0->bs == a->V1->bs &&
                    a->V0->k == a->V1->k,
                "the diagonal needs the same test and trial space");
@@ -1041,6 +1109,10 @@ int fe_apply_lifting(double* b, int num_forms, const fe_form* a, const fe_bc* bc
       if (!bc) continue;
       DeviceScope d(f->ctx);
       FE_REQUIRE(bc->num_dofs == scalar_size(f->V1), "bc size differs from the trial space size");
+      if (f->ffcx) {
+        ffcx_lifting(*f, *bc, x0 ? x0[i] : nullptr, scale, b, st);
+        continue;
+      }
       if (is_facet_kind(f->kind)) {
         lifting_facets(*f, *bc, x0 ? x0[i] : nullptr, scale, b, scalar_size(f->V0), st);
         continue;

@@ -224,7 +224,7 @@ FacetArgs base_args(const fe_form_s& f) {
 }  // namespace
 
 bool is_facet_kind(int kind) {
-  return kind == FE_FORM_P1_FACET_MASS || kind == FE_FORM_P2_FACET_MASS || kind == FE_FORM_P1_FACET_LOAD ||
+  return kind == FE_FORM_FFCX_EXTERIOR || kind == FE_FORM_P1_FACET_MASS || kind == FE_FORM_P2_FACET_MASS || kind == FE_FORM_P1_FACET_LOAD ||
          kind == FE_FORM_P2_FACET_LOAD || kind == FE_FORM_VP2_FACET_LOAD;
 }
 

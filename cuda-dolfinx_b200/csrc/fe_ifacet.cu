@@ -251,7 +251,7 @@ bool dg1(int kind) { return kind == FE_FORM_DG1_JUMP || kind == FE_FORM_DG1_AVG_
 }  // namespace
 
 bool is_ifacet_kind(int kind) {
-  return kind == FE_FORM_DG0_JUMP || kind == FE_FORM_DG1_JUMP || kind == FE_FORM_DG0_AVG_LOAD ||
+  return kind == FE_FORM_FFCX_INTERIOR || kind == FE_FORM_DG0_JUMP || kind == FE_FORM_DG1_JUMP || kind == FE_FORM_DG0_AVG_LOAD ||
          kind == FE_FORM_DG1_AVG_LOAD;
 }
 

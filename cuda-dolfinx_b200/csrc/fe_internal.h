@@ -192,8 +192,41 @@ struct fe_form_s {
   // batched-instance plan (fe_batch.cu); built on first use
   struct BatchPlan;
   std::unique_ptr<BatchPlan> batch;
+  // form integral given as an FFCx tabulate_tensor body (fe_ffcx.cu)
+  struct Ffcx;
+  std::unique_ptr<Ffcx> ffcx;
   fe_form_s();
   ~fe_form_s();
+};
+
+namespace fe {
+struct FfcxLibrary;
+// internal kinds of forms built from FFCx tabulate_tensor bodies (fe_ffcx.cu)
+constexpr int FE_FORM_FFCX_CELL = 41;
+constexpr int FE_FORM_FFCX_EXTERIOR = 42;
+constexpr int FE_FORM_FFCX_INTERIOR = 43;
+inline bool is_ffcx_kind(int kind) { return kind >= FE_FORM_FFCX_CELL && kind <= FE_FORM_FFCX_INTERIOR; }
+}  // namespace fe
+
+struct fe_form_s::Ffcx {
+  int integral_type = FE_INTEGRAL_CELL;
+  std::string name;                    // the tabulate_tensor function name
+  std::string body;                    // its body, as FFCx generated it
+  std::vector<int> offsets;            // coefficient q: values [offsets[q], offsets[q+1]) of a cell
+  int W = 0;                           // coefficient values per cell
+  int num_constants = 0;
+  std::vector<double> host_consts;
+  fe::DevBuf<double> consts;
+  struct Field {
+    fe_dofmap map = nullptr;           // the coefficient's space
+    const double* values = nullptr;    // device values (own or the caller's)
+    fe::DevBuf<double> own;
+  };
+  std::vector<std::unique_ptr<Field>> fields;
+  fe::DevBuf<double> packed;           // [cells][W], packed on every assembly call
+  fe::DevBuf<uint8_t> perms;           // interior facets: [facets][2] quadrature permutations
+  fe::DevBuf<double> partial;          // functionals: block partial sums + the result
+  std::shared_ptr<fe::FfcxLibrary> lib;
 };
 
 // Plans owned by a form (defined here so every translation unit can destroy them)
@@ -391,6 +424,19 @@ void assemble_matrix_facets(const fe_form_s& f, double* values, const fe_bc_s* b
 void assemble_vector_facets(const fe_form_s& f, double* b, int64_t num_values, cudaStream_t s);
 void lifting_facets(const fe_form_s& f, const fe_bc_s& bc, const double* x0, double scale, double* b,
                     int64_t num_values, cudaStream_t s);
+
+// forms from FFCx tabulate_tensor bodies (fe_ffcx.cu): NVRTC compilation of the
+// body inside the engine's skeletons, packed coefficients, constants
+void ffcx_create(fe_form_s& f, int integral_type, const char* name, const char* body, int num_coefficients,
+                 const int* coefficient_sizes, int num_constants, const char* cachedir);
+void ffcx_set_coefficient(fe_form_s& f, int index, fe_dofmap map, const double* values, int64_t n,
+                          bool on_device, cudaStream_t s);
+void ffcx_set_constants(fe_form_s& f, const double* values, int n, cudaStream_t s);
+void ffcx_set_interior_permutations(fe_form_s& f);
+void ffcx_assemble_matrix(fe_form_s& f, double* values, const fe_bc_s* bc0, const fe_bc_s* bc1, cudaStream_t s);
+void ffcx_assemble_vector(fe_form_s& f, double* b, cudaStream_t s);
+void ffcx_lifting(fe_form_s& f, const fe_bc_s& bc, const double* x0, double scale, double* b, cudaStream_t s);
+double ffcx_assemble_scalar(fe_form_s& f, cudaStream_t s);
 
 // functionals (fe_scalar.cu)
 bool is_scalar_kind(int kind);

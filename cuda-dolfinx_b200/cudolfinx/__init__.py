@@ -11,7 +11,7 @@ from .batch import AssemblyGraph, VariantTuner
 from .bcs import CUDADirichletBC
 from .coefficient import Coefficient
 from .context import get_cuda_context
-from .form import BlockCUDAForm, CUDAForm, form
+from .form import BlockCUDAForm, CUDAForm, FFCxCUDAForm, form
 from .la import CUDAMatrix, CUDAVector, Sparsity
 
 
@@ -26,5 +26,5 @@ def release_caches(mesh=None):
     release_device_caches(mesh)
 
 
-__all__ = ["AssemblyGraph", "BlockCUDAForm", "CUDAAssembler", "CUDADirichletBC", "Coefficient", "CUDAForm", "CUDAMatrix", "CUDAVector", "Sparsity", "fem", "form",
+__all__ = ["AssemblyGraph", "BlockCUDAForm", "FFCxCUDAForm", "CUDAAssembler", "CUDADirichletBC", "Coefficient", "CUDAForm", "CUDAMatrix", "CUDAVector", "Sparsity", "fem", "form",
            "get_cuda_context", "release_caches", "VariantTuner"]

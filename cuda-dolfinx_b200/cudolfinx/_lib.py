@@ -39,6 +39,7 @@ FORM = {"P1_STIFFNESS": 1, "P2_STIFFNESS": 2, "VP2_ELASTICITY": 3, "P1_MASS": 9,
         "JUMP_NORM": 35}
 INTERIOR_FACET_KINDS = ("DG0_JUMP", "DG1_JUMP", "DG0_AVG_LOAD", "DG1_AVG_LOAD", "JUMP_NORM")
 COEFF_CONSTANT, COEFF_DG0, COEFF_P1, COEFF_P2 = 0, 1, 2, 3
+INTEGRAL = {"cell": 0, "exterior_facet": 1, "interior_facet": 2}
 PREC_FP64, PREC_FP32 = 0, 1
 ASM_ZERO, ASM_DETERMINISTIC, ASM_ATOMIC, ASM_SORTED_SLOT, ASM_TILE, ASM_ROW_GATHER, ASM_BLOCK = 1, 2, 4, 8, 16, 32, 64
 ASM_FULL_SCATTER = 128
@@ -76,6 +77,12 @@ _SIGS = {
     "fe_form_bind_sparsity": (i32, [vp, vp, vp]),
     "fe_form_bind_sparsity_block": (i32, [vp, vp, i64, i64, vp]),
     "fe_form_destroy": (i32, [vp]),
+    "fe_form_create_ffcx": (i32, [vp, vp, vp, vp, i32, ctypes.c_char_p, ctypes.c_char_p, i32, vp, i32,
+                                  ctypes.c_char_p, PP]),
+    "fe_form_set_coefficient_field": (i32, [vp, i32, vp, vp, i64, i32, vp]),
+    "fe_form_set_constants": (i32, [vp, vp, i32, vp]),
+    "fe_ffcx_source": (i32, [i32, i32, i32, i32, i32, i32, i32, vp, ctypes.c_char_p, ctypes.c_char_p, vp, i64,
+                             ctypes.POINTER(i64)]),
     "fe_bc_create": (i32, [vp, i64, vp, vp, i64, i64, vp, PP]),
     "fe_bc_update": (i32, [vp, vp, vp]),
     "fe_bc_destroy": (i32, [vp]),

@@ -67,7 +67,7 @@ class CUDAAssembler:
             raise TypeError(f"Expected CUDAForm, got type '{type(a)}'.")
         if a.rank != 2:
             raise ValueError("create_matrix needs a bilinear form")
-        if a.dolfinx_form.kind in _lib.INTERIOR_FACET_KINDS:
+        if a._needs_union_pattern():
             # interior-facet couplings join the two cells of every facet
             sp = Sparsity.build_forms(self._ctx, [a])
             mat = CUDAMatrix(self._ctx, sp)
@@ -166,11 +166,13 @@ class CUDAAssembler:
         # as the reference (assemble.py:100-103): always copy host coefficients to the device
         a.to_device()
         self.pack_coefficients(a, coeffs)
-        flags = ((_lib.ASM_ZERO if zero else 0) | (_lib.ASM_DETERMINISTIC if deterministic else 0)
-                 | _lib.VARIANT_FLAGS[variant])
-        _lib.check(_lib.lib.fe_assemble_matrix(a._handle, mat.values.data_ptr(), bc0.handle if bc0 else None,
-                                               bc1.handle if bc1 else None, float(diagonal), flags,
-                                               self._ctx.stream()), "fe_assemble_matrix")
+        flags = (_lib.ASM_DETERMINISTIC if deterministic else 0) | _lib.VARIANT_FLAGS[variant]
+        # a form with several integrals: the first zeroes, the others add
+        for q, h in enumerate(a._integral_handles()):
+            _lib.check(_lib.lib.fe_assemble_matrix(h, mat.values.data_ptr(), bc0.handle if bc0 else None,
+                                                   bc1.handle if bc1 else None, float(diagonal),
+                                                   flags | (_lib.ASM_ZERO if (zero and q == 0) else 0),
+                                                   self._ctx.stream()), "fe_assemble_matrix")
         a._mark_used()
         mat._bcs = col  # keep device BC data alive while the work is queued
         return mat
@@ -272,8 +274,9 @@ class CUDAAssembler:
         for f, off, c in zip(b.forms, b.offsets, _coeffs):
             f.to_device()
             self.pack_coefficients(f, c)
-            _lib.check(_lib.lib.fe_assemble_vector(f._handle, base + 8 * off, 0, self._ctx.stream()),
-                       "fe_assemble_vector")
+            for h in f._integral_handles():
+                _lib.check(_lib.lib.fe_assemble_vector(h, base + 8 * off, 0, self._ctx.stream()),
+                           "fe_assemble_vector")
             f._mark_used()
         return vec
 
@@ -287,11 +290,13 @@ class CUDAAssembler:
         import ctypes
         b.to_device()  # assemble.py:220-222
         self.pack_coefficients(b, coeffs)
-        out = ctypes.c_double(0.0)
-        _lib.check(_lib.lib.fe_assemble_scalar(b._handle, ctypes.byref(out), self._ctx.stream()),
-                   "fe_assemble_scalar")
+        total = 0.0
+        for h in b._integral_handles():
+            out = ctypes.c_double(0.0)
+            _lib.check(_lib.lib.fe_assemble_scalar(h, ctypes.byref(out), self._ctx.stream()), "fe_assemble_scalar")
+            total += out.value
         b._mark_used()
-        return out.value
+        return total
 
     def assemble_vector(self, b: CUDAForm, vec: typing.Optional[CUDAVector] = None, constants=None, coeffs=None,
                         zero: bool = True) -> CUDAVector:
@@ -307,8 +312,10 @@ class CUDAAssembler:
             _lib.check(_lib.lib.fe_assemble_diagonal(b._handle, vec.vector.data_ptr(), _lib.ASM_ZERO if zero else 0,
                                                      self._ctx.stream()), "fe_assemble_diagonal")
         else:
-            _lib.check(_lib.lib.fe_assemble_vector(b._handle, vec.vector.data_ptr(), _lib.ASM_ZERO if zero else 0,
-                                                   self._ctx.stream()), "fe_assemble_vector")
+            for q, h in enumerate(b._integral_handles()):
+                _lib.check(_lib.lib.fe_assemble_vector(h, vec.vector.data_ptr(),
+                                                       _lib.ASM_ZERO if (zero and q == 0) else 0,
+                                                       self._ctx.stream()), "fe_assemble_vector")
         b._mark_used()
         return vec
 
@@ -324,19 +331,20 @@ class CUDAAssembler:
         elif not len(coeffs):
             coeffs = [[] for _ in a]
         import ctypes
-        n = len(a)
-        forms = (ctypes.c_void_p * max(1, n))()
-        hbcs = (ctypes.c_void_p * max(1, n))()
-        hx0 = (ctypes.c_void_p * max(1, n))()
-        keep = []
+        keep, hf, hb, hx = [], [], [], []
         for i, (f, bc, c) in enumerate(zip(a, bcs, coeffs)):
             self.pack_coefficients(f, c)
             col = self._bc_collection(bc)
             keep.append(col)
             d = col._get_cpp_bcs(f.function_spaces[1], f.restriction(1))
-            forms[i] = f._handle
-            hbcs[i] = d.handle if d else None
-            hx0[i] = x0[i].vector.data_ptr() if (x0 is not None and x0[i] is not None) else None
+            for h in f._integral_handles():  # every integral of the form lifts
+                hf.append(h)
+                hb.append(d.handle if d else None)
+                hx.append(x0[i].vector.data_ptr() if (x0 is not None and x0[i] is not None) else None)
+        n = len(hf)
+        forms = (ctypes.c_void_p * max(1, n))(*hf)
+        hbcs = (ctypes.c_void_p * max(1, n))(*hb)
+        hx0 = (ctypes.c_void_p * max(1, n))(*hx)
         b._before_write()
         _lib.check(_lib.lib.fe_apply_lifting(b.vector.data_ptr(), n, forms, hbcs, hx0 if x0 is not None else None,
                                              float(scale), self._ctx.stream()), "fe_apply_lifting")

@@ -330,6 +330,58 @@ class FormSpec:
         return self.domain if self.domain is not None else self.V.mesh
 
 
+@dataclass
+class FFCxIntegral:
+    """One integral of a form compiled by FFCx: the name and the body (the
+    statements between the outer braces) of its tabulate_tensor_integral_*
+    function, as python/cudolfinx/jit.py:15-59 extracts them from the
+    generated C file, its integral type ("cell", "exterior_facet",
+    "interior_facet") and, for facet integrals, the integration entities:
+    [F, 2] (cell, local facet) or [F, 4] (cell0, facet0, cell1, facet1).
+    Facet integrals without entities run over all exterior / interior facets
+    of the mesh."""
+    integral_type: str
+    name: str
+    body: str
+    entities: Optional[np.ndarray] = None
+
+
+@dataclass
+class FFCxForm:
+    """A variational form as FFCx compiles it (stands where a UFL form given to
+    cudolfinx.form stands in the reference): its integrals, the argument
+    spaces ([] functional, [V] linear, [V, U] bilinear: test, trial), the
+    coefficients in FFCx's order (Functions; coefficient q has
+    dofs_per_cell * bs values per cell) and the constants in the form's order
+    (each a number or array, packed flat as DOLFINx pack_constants does)."""
+    integrals: list
+    spaces: list
+    coefficients: list = field(default_factory=list)
+    constants: list = field(default_factory=list)
+    domain: Optional["Mesh"] = None
+
+    @property
+    def rank(self) -> int:
+        return len(self.spaces)
+
+    @property
+    def function_spaces(self):
+        return list(self.spaces)
+
+    @property
+    def mesh(self):
+        if self.domain is not None:
+            return self.domain
+        if self.spaces:
+            return self.spaces[0].mesh
+        return self.coefficients[0].function_space.mesh
+
+    def packed_constants(self) -> np.ndarray:
+        if not self.constants:
+            return np.zeros(0)
+        return np.concatenate([np.atleast_1d(np.asarray(c, dtype=np.float64)).ravel() for c in self.constants])
+
+
 def _trial(V: FunctionSpace, trial: Optional[FunctionSpace]) -> Optional[FunctionSpace]:
     if trial is None or trial is V:
         return None

@@ -17,7 +17,7 @@ import torch
 
 from . import _lib
 from .context import get_cuda_context
-from .fem import FormSpec, Function, FunctionSpace
+from .fem import FFCxForm, FormSpec, Function, FunctionSpace
 
 DEFAULT_CUDA_JIT_ARGS = {"max_threads_per_block": 1024, "min_blocks_per_multiprocessor": 1}
 # transfers of at least this size run on the context's side streams (below it
@@ -307,6 +307,14 @@ class CUDAForm:
             self._bound_sparsity = sparsity
             self._block_offsets = key
 
+    def _integral_handles(self) -> list:
+        """Engine forms whose sum is this form (one per integral)."""
+        return [self._handle]
+
+    def _needs_union_pattern(self) -> bool:
+        """Whether the matrix pattern must join the two cells of interior facets."""
+        return self._spec.kind in _lib.INTERIOR_FACET_KINDS
+
     # -- properties mirroring the reference --------------------------------
     @property
     def cuda_form(self):
@@ -344,6 +352,150 @@ class CUDAForm:
             release = getattr(_lib, "release", None)  # None during interpreter teardown
             if release is not None:
                 release("fe_form_destroy", h)
+
+
+class FFCxCUDAForm(CUDAForm):
+    """CUDA wrapper of a form given as FFCx tabulate_tensor bodies, the
+    reference's general path (python/cudolfinx/form.py:26-105: the form's
+    integrals wrapped by jit.py and compiled with NVRTC).  One engine form per
+    integral (fe_form_create_ffcx), all on the same spaces, coefficients and
+    constants; assembling the form sums its integrals.  ``cachedir`` keeps the
+    compiled kernels on disk (the reference's cudolfinx cache directory)."""
+
+    def __init__(self, form: FFCxForm, jit_args: typing.Optional[dict] = None, cachedir: typing.Optional[str] = None):
+        if not isinstance(form, FFCxForm):
+            raise TypeError(f"Expected a cudolfinx.fem.FFCxForm, got '{type(form)}'")
+        if not form.integrals:
+            raise ValueError("a form needs at least one integral")
+        if form.rank > 2:
+            raise ValueError("forms of rank above 2 are not supported")
+        self._ctx = get_cuda_context()
+        self._spec = form
+        self._part = "full"
+        self._cachedir = cachedir
+        self._cuda_mesh = _create_mesh_on_device(self._ctx, form.mesh)
+        self._dofmaps = [device_dofmap(self._ctx, V) for V in form.function_spaces]
+        self._coef_maps = [device_dofmap(self._ctx, c.function_space) for c in form.coefficients]
+        self._jit_args = dict(DEFAULT_CUDA_JIT_ARGS, **(jit_args or {}))
+        self._handles = []
+        self._handle = None
+        self._create_handle()
+
+    def _create_handle(self):
+        from . import fem as _fem
+
+        self._destroy_handles()
+        form = self._spec
+        sizes = (ctypes.c_int * max(1, len(form.coefficients)))(
+            *[c.function_space.dofs_per_cell * c.function_space.bs for c in form.coefficients])
+        test = self._dofmaps[0].handle if form.rank >= 1 else None
+        trial = self._dofmaps[1].handle if form.rank == 2 else None
+        consts = form.packed_constants()
+        self._entities = []
+        for itg in form.integrals:
+            if itg.integral_type not in _lib.INTEGRAL:
+                raise ValueError(f"unknown integral type {itg.integral_type!r}")
+            h = _lib.out_handle()
+            _lib.check(_lib.lib.fe_form_create_ffcx(
+                self._ctx.handle, self._cuda_mesh.handle, test, trial, _lib.INTEGRAL[itg.integral_type],
+                itg.name.encode(), itg.body.encode(), len(form.coefficients), sizes, len(consts),
+                self._cachedir.encode() if self._cachedir else None, h), "fe_form_create_ffcx")
+            self._handles.append(h.value)
+            if itg.integral_type == "exterior_facet":
+                ent = itg.entities if itg.entities is not None else _fem.exterior_facets(form.mesh)
+                ent = np.ascontiguousarray(ent, dtype=np.int32)
+                _lib.check(_lib.lib.fe_form_set_facets(h.value, ent.ctypes.data, len(ent)), "fe_form_set_facets")
+                self._entities.append(ent)
+            elif itg.integral_type == "interior_facet":
+                ent = itg.entities if itg.entities is not None else _fem.interior_facets(form.mesh)
+                ent = np.ascontiguousarray(ent, dtype=np.int32)
+                _lib.check(_lib.lib.fe_form_set_interior_facets(h.value, ent.ctypes.data, len(ent)),
+                           "fe_form_set_interior_facets")
+                self._entities.append(ent)
+        self._handle = self._handles[0]
+        self._bound_sparsity = None
+        self._external = getattr(self, "_external", False)
+        self._coef_dev = [None] * len(form.coefficients)
+        self.to_device()
+
+    def _destroy_handles(self):
+        for h in getattr(self, "_handles", []):
+            _lib.lib.fe_form_destroy(h)
+        self._handles = []
+        self._handle = None
+
+    def set_restriction(self, restrictions):
+        if len(restrictions) != self.rank:
+            raise ValueError("Number of restrictions must equal arity of form (1 for vector, 2 for matrix)!")
+        new = [None if r is None else np.ascontiguousarray(r, dtype=np.int32) for r in restrictions]
+        old = [dm.restriction for dm in self._dofmaps]
+        if all((o is None and n is None) or (o is not None and n is not None and np.array_equal(o, n))
+               for o, n in zip(old, new)):
+            return
+        self._dofmaps = [device_dofmap(self._ctx, V) if r is None else DeviceDofMap(self._ctx, V, r)
+                         for V, r in zip(self._spec.function_spaces, new)]
+        self._create_handle()
+
+    def to_device(self, coefficients: typing.Optional[list] = None):
+        """Copy the coefficients' host values and the constants to the device
+        (the reference re-uploads them on every assembly call,
+        assemble.py:100-103); every integral reads the same device arrays."""
+        ctx = self._ctx
+        for q, c in enumerate(self._spec.coefficients):
+            if coefficients is not None and not any(c is x for x in coefficients):
+                continue
+            V = c.function_space
+            vals = c.x.array
+            if hasattr(vals, "data_ptr"):  # a device tensor: read in place
+                dev = vals
+            else:
+                host = torch.from_numpy(np.ascontiguousarray(vals, dtype=np.float64))
+                dev = self._coef_dev[q]
+                if dev is None or dev.numel() != host.numel():
+                    dev = torch.empty(host.numel(), dtype=torch.float64, device=ctx.torch_device)
+                dev.copy_(host)
+            self._coef_dev[q] = dev
+            for h in self._handles:
+                _lib.check(_lib.lib.fe_form_set_coefficient_field(h, q, self._coef_maps[q].handle, dev.data_ptr(),
+                                                                  V.num_nodes * V.bs, 1, ctx.stream()),
+                           "fe_form_set_coefficient_field")
+        consts = np.ascontiguousarray(self._spec.packed_constants())
+        self._consts = consts
+        for h in self._handles:
+            _lib.check(_lib.lib.fe_form_set_constants(h, consts.ctypes.data if consts.size else None, consts.size,
+                                                      ctx.stream()), "fe_form_set_constants")
+
+    def _bind(self, sparsity):
+        if self._bound_sparsity is not sparsity:
+            for h in self._handles:
+                _lib.check(_lib.lib.fe_form_bind_sparsity(h, sparsity.handle, self._ctx.stream()),
+                           "fe_form_bind_sparsity")
+            self._bound_sparsity = sparsity
+
+    def _bind_block(self, sparsity, row_offset: int, col_offset: int):
+        key = (row_offset, col_offset)
+        if self._bound_sparsity is not sparsity or getattr(self, "_block_offsets", None) != key:
+            for h in self._handles:
+                _lib.check(_lib.lib.fe_form_bind_sparsity_block(h, sparsity.handle, int(row_offset), int(col_offset),
+                                                                self._ctx.stream()), "fe_form_bind_sparsity_block")
+            self._bound_sparsity = sparsity
+            self._block_offsets = key
+
+    def _integral_handles(self) -> list:
+        return list(self._handles)
+
+    def _needs_union_pattern(self) -> bool:
+        return any(i.integral_type == "interior_facet" for i in self._spec.integrals)
+
+    def __del__(self):
+        hs = getattr(self, "_handles", None)
+        if hs:
+            self._handles = []
+            self._handle = None
+            release = getattr(_lib, "release", None)  # None during interpreter teardown
+            if release is not None:
+                for h in hs:
+                    release("fe_form_destroy", h)
 
 
 class BlockCUDAForm:
@@ -453,6 +605,14 @@ def form(form: typing.Union[FormSpec, typing.Iterable], restriction=None,
     is honoured: the bilinear form's diagonal becomes a linear form."""
     fco = kwargs.get("form_compiler_options") or {}
     part = fco.get("part")
+    cachedir = kwargs.get("cachedir")
+    if isinstance(form, FFCxForm):
+        if part not in (None, "full"):
+            raise ValueError("the diagonal of a form given as FFCx bodies is compiled by FFCx as a linear form")
+        f = FFCxCUDAForm(form, cuda_jit_args, cachedir)
+        if restriction is not None:
+            f.set_restriction(restriction)
+        return f
     if isinstance(form, FormSpec):
         f = CUDAForm(form, cuda_jit_args, part)
         if restriction is not None:
@@ -462,6 +622,8 @@ def form(form: typing.Union[FormSpec, typing.Iterable], restriction=None,
     def _create(x):
         if x is None:
             return None
+        if isinstance(x, FFCxForm):
+            return FFCxCUDAForm(x, cuda_jit_args, cachedir)
         if isinstance(x, FormSpec):
             return CUDAForm(x, cuda_jit_args, part)
         return [_create(y) for y in x]

@@ -63,8 +63,9 @@ class Sparsity:
         """Pattern of a sum of bilinear forms on the same spaces: the union of
         their cell / interior-facet couplings (create_sparsity_pattern of a
         form with several integrals)."""
-        n = len(forms)
-        tab = (ctypes.c_void_p * n)(*[f._handle for f in forms])
+        hs = [h for f in forms for h in f._integral_handles()]
+        n = len(hs)
+        tab = (ctypes.c_void_p * n)(*hs)
         h = _lib.out_handle()
         _lib.check(_lib.lib.fe_sparsity_build_forms(n, tab, h), "fe_sparsity_build_forms")
         return cls(ctx, h.value)

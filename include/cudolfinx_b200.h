@@ -247,6 +247,58 @@ int fe_form_bind_sparsity_block(fe_form f, fe_sparsity s, int64_t row_offset, in
                                 void* stream);
 int fe_form_destroy(fe_form f);
 
+/* ---- forms from FFCx tabulate_tensor bodies ------------------------------ */
+/* Integral types (ufcx / DOLFINx IntegralType). */
+enum fe_integral_type {
+  FE_INTEGRAL_CELL = 0,
+  FE_INTEGRAL_EXTERIOR_FACET = 1,
+  FE_INTEGRAL_INTERIOR_FACET = 2
+};
+/* Replaces CUDAForm_float64 + CUDAForm::compile for one integral of a form
+ * (python/cudolfinx/form.py:26-71, jit.py:15-114; kernel source
+ * cpp/cudolfinx/fem/CUDAFormIntegral.cpp:2366-2469, NVRTC compile and cache
+ * :2472-2558).  `tabulate_body` is the body (between the outer braces) of an
+ * FFCx tabulate_tensor_integral_* function -- what jit.py extracts from the
+ * generated C file -- and `tabulate_name` its name (a C identifier).  The body
+ * reads A, w, c, coordinate_dofs, entity_local_index and quadrature_permutation
+ * with FFCx's meaning and adds into A.  The rank is 2 with a trial dofmap, 1
+ * with a test dofmap only, 0 with neither (a functional).  Coefficient q of
+ * the form has coefficient_sizes[q] values per cell (its element's dofs times
+ * block size); the form has num_constants constant values.  The body is
+ * compiled here, for the device's architecture, inside the engine's assembly
+ * skeletons; the compiled code is cached per process and, when `cachedir` is
+ * not NULL, in that directory (keyed on a hash of the whole generated source).
+ * A body NVRTC rejects gives FE_ERR_ARG with the compiler log.  Facet integrals
+ * take their facets from fe_form_set_facets / fe_form_set_interior_facets;
+ * matrices bind a pattern with fe_form_bind_sparsity (cell and exterior-facet
+ * integrals: also fe_form_bind_sparsity_block) and assemble with the atomic
+ * scatter through fe_assemble_matrix, fe_assemble_vector, fe_apply_lifting and
+ * fe_assemble_scalar. */
+int fe_form_create_ffcx(fe_context ctx, fe_mesh mesh, fe_dofmap test, fe_dofmap trial, int integral_type,
+                        const char* tabulate_name, const char* tabulate_body, int num_coefficients,
+                        const int* coefficient_sizes, int num_constants, const char* cachedir,
+                        fe_form* out);
+/* Coefficient `index` of an FFCx form: a function on the space of dofmap
+ * `cmap` (k*bs values per cell, which must equal the coefficient's size),
+ * `values` its num_blocks*bs dof values (host, copied on `stream`, or device
+ * memory read in place when values_on_device != 0).  The values are packed
+ * per cell before every assembly call, as pack_coefficients does
+ * (cpp/cudolfinx/fem/CUDAAssembler.cpp:59-96). */
+int fe_form_set_coefficient_field(fe_form f, int index, fe_dofmap cmap, const double* values, int64_t n,
+                                  int values_on_device, void* stream);
+/* The CUDA C++ translation unit fe_form_create_ffcx compiles for an integral
+ * with these sizes (test / trial dofs per cell k0 / k1 and block sizes; unused
+ * for lower ranks), without compiling it and without a GPU: for inspecting the
+ * generated kernels (the reference keeps its generated sources in its cache
+ * directory).  Writes at most capacity-1 characters and a terminating NUL to
+ * `out` (may be NULL) and the full length to *length. */
+int fe_ffcx_source(int integral_type, int rank, int k0, int bs0, int k1, int bs1, int num_coefficients,
+                   const int* coefficient_sizes, const char* tabulate_name, const char* tabulate_body, char* out,
+                   int64_t capacity, int64_t* length);
+/* The constant values of an FFCx form (host; replaces CUDAFormConstants,
+ * cpp/cudolfinx/fem/CUDAFormConstants.h:36-70, 123-145). */
+int fe_form_set_constants(fe_form f, const double* values, int n, void* stream);
+
 /* ---- Dirichlet BCs ------------------------------------------------------- */
 /* Replaces CUDADirichletBC (cpp/cudolfinx/fem/CUDADirichletBC.h:56-194):
  * markers u8[num_dofs] (scalar dofs), dof list int32[n_bc] with the n_owned

@@ -1163,3 +1163,245 @@ def nnz_formula(kind: str, n: int) -> int:
         return 1311 * n ** 3 + 459 * n ** 2 + 45 * n + 1
     p2 = 230 * n ** 3 + 138 * n ** 2 + 24 * n + 1
     return p2 if kind == "p2" else 9 * p2
+
+
+# ---------------------------------------------------------------------------
+# Quadrature-evaluated forms: the oracle of forms given as FFCx
+# tabulate_tensor bodies (python/cudolfinx/jit.py:15-114 feeds the reference
+# such bodies; FFCx integrates with a basix quadrature rule).  Everything here
+# is evaluated per cell in physical coordinates with numpy, independently of
+# any generated code: the rule and the points are the only shared input.
+# ---------------------------------------------------------------------------
+REF_TET = np.array([[0.0, 0.0, 0.0], [1.0, 0.0, 0.0], [0.0, 1.0, 0.0], [0.0, 0.0, 1.0]])
+
+
+def _gauss01(n):
+    t, w = np.polynomial.legendre.leggauss(n)
+    return 0.5 * (t + 1.0), 0.5 * w
+
+
+@lru_cache(maxsize=None)
+def tet_rule(n: int):
+    """Collapsed Gauss-Legendre rule on the reference tetrahedron: n^3 points,
+    x = a(1-b)(1-c), y = b(1-c), z = c; exact for total degree <= 2n - 3."""
+    t, w = _gauss01(n)
+    a, b, c = np.meshgrid(t, t, t, indexing="ij")
+    wa, wb, wc = np.meshgrid(w, w, w, indexing="ij")
+    X = np.stack([a * (1 - b) * (1 - c), b * (1 - c), c], axis=-1).reshape(-1, 3)
+    W = (wa * wb * wc * (1 - b) * (1 - c) ** 2).ravel()
+    return X, W
+
+
+@lru_cache(maxsize=None)
+def tri_rule(n: int):
+    """Collapsed Gauss-Legendre rule on the reference triangle: n^2 points,
+    x = a(1-b), y = b; exact for total degree <= 2n - 2."""
+    t, w = _gauss01(n)
+    a, b = np.meshgrid(t, t, indexing="ij")
+    wa, wb = np.meshgrid(w, w, indexing="ij")
+    return np.stack([a * (1 - b), b], axis=-1).reshape(-1, 2), (wa * wb * (1 - b)).ravel()
+
+
+def lagrange_tables(degree: int, X):
+    """Values [N, k] and reference gradients [N, k, 3] of the Lagrange basis
+    (degree 0: the constant; 1, 2, 3: the basix-ordered bases above) at the
+    reference points X [N, 3]."""
+    X = np.asarray(X, dtype=float)
+    if degree == 0:
+        return np.ones((len(X), 1)), np.zeros((len(X), 1, 3))
+    phi = _basis(degree)
+    xs, ys, zs = X[:, 0], X[:, 1], X[:, 2]
+
+    def ev(p):
+        out = np.zeros(len(X))
+        for (a, b, c), v in p.items():
+            out += float(v) * xs ** a * ys ** b * zs ** c
+        return out
+
+    V = np.stack([ev(p) for p in phi], axis=1)
+    D = np.stack([np.stack([ev(_pdiff(p, ax)) for ax in range(3)], axis=-1) for p in phi], axis=1)
+    return V, D
+
+
+def facet_points(f: int, P2):
+    """Reference-tetrahedron points of the reference-triangle points P2 [N, 2]
+    on local facet f: v0 + x (v1 - v0) + y (v2 - v0), (v0, v1, v2) the facet's
+    vertices in TET_FACETS order."""
+    v = REF_TET[list(TET_FACETS[f])]
+    P2 = np.asarray(P2, dtype=float)
+    return v[0] + P2[:, :1] * (v[1] - v[0]) + P2[:, 1:2] * (v[2] - v[0])
+
+
+def facet_permutation(global_vertices) -> int:
+    """Quadrature permutation code of a triangle facet: 2*rot + ref, rot the
+    position (in the cell's local facet order) of its lowest-numbered global
+    vertex, ref = 1 when the vertex after it (cyclically) is numbered above
+    the vertex before it."""
+    gv = list(global_vertices)
+    rot = 0
+    for t in (1, 2):
+        if gv[t] < gv[rot]:
+            rot = t
+    pre, post = gv[(rot + 2) % 3], gv[(rot + 1) % 3]
+    return 2 * rot + (1 if post > pre else 0)
+
+
+def permute_facet_points(P2, code: int):
+    """Points of the rule for facet permutation `code`: reflected (x, y) -> (y, x)
+    when ref, then rotated rot times by (x, y) -> (1 - x - y, x).  With the
+    codes of facet_permutation the two cells of an interior facet then see
+    the same physical points (checked in tests/test_oracle.py)."""
+    P = np.asarray(P2, dtype=float).copy()
+    rot, ref = code // 2, code % 2
+    if ref:
+        P = P[:, ::-1].copy()
+    for _ in range(rot):
+        P = np.stack([1.0 - P[:, 0] - P[:, 1], P[:, 0]], axis=1)
+    return P
+
+
+def _jacobians(coords, cells):
+    x = coords[cells]  # [C, 4, 3]
+    J = np.transpose(x[:, 1:] - x[:, :1], (0, 2, 1))  # J[c, r, k] = x_{k+1, r} - x_{0, r}
+    return x, J, np.linalg.det(J), np.linalg.inv(J)
+
+
+def _phys_grad(K, D):
+    """grad_x phi = K^T grad_X phi: K [C, 3, 3], D [..., k, 3] -> [C, ..., k, 3]."""
+    return np.einsum("cba,...ib->c...ia", K, D)
+
+
+def quad_cell_forms(coords, cells, u, kappa, n=4):
+    """The nonlinear P1 test forms, with u and kappa P1 fields given per cell
+    [C, 4] (vertex values), integrated by tet_rule(n):
+      residual  R_i  = int exp(u) kappa phi_i + grad u . grad phi_i,
+      jacobian  J_ij = int exp(u) kappa phi_j phi_i + grad phi_j . grad phi_i,
+      functional     = int exp(u) kappa.
+    Returns (R [C, 4], J [C, 4, 4], M [C])."""
+    X, w = tet_rule(n)
+    V, D = lagrange_tables(1, X)
+    _, _, det, K = _jacobians(coords, cells)
+    G = _phys_grad(K, D[0])  # P1 gradients are constant: [C, 4, 3]
+    uq = u @ V.T  # [C, N]
+    kq = kappa @ V.T
+    gu = np.einsum("ci,cia->ca", u, G)
+    dx = np.abs(det)[:, None] * w[None, :]  # [C, N]
+    e = np.exp(uq) * kq * dx
+    R = e @ V + (dx.sum(axis=1) * np.einsum("ca,cia->ci", gu, G).T).T
+    Jm = np.einsum("cq,qi,qj->cij", e, V, V) + dx.sum(axis=1)[:, None, None] * np.einsum("cia,cja->cij", G, G)
+    return R, Jm, e.sum(axis=1)
+
+
+def quad_cell_matrix(coords, cells, test_degree, trial_degree, integrand, n=4):
+    """[C, k0, k1] of int integrand(V0, G0, V1, G1) dx by tet_rule(n), with
+    V [N, k] values and G [C, N, k, 3] physical gradients of the test / trial
+    bases; integrand returns [C, N, k0, k1]."""
+    X, w = tet_rule(n)
+    V0, D0 = lagrange_tables(test_degree, X)
+    V1, D1 = lagrange_tables(trial_degree, X)
+    _, _, det, K = _jacobians(coords, cells)
+    G0, G1 = _phys_grad(K, D0), _phys_grad(K, D1)
+    f = integrand(V0, G0, V1, G1)
+    return np.einsum("cqij,cq->cij", f, np.abs(det)[:, None] * w[None, :])
+
+
+def exterior_facet_forms(coords, cells, facets, u, kappa, n=3):
+    """The reference's exterior-facet test forms on P1 (u, kappa P1 given per
+    cell [C, 4]) over facets [F, 2] (cell, local facet), tri_rule(n):
+      residual R_i  = int_F u kappa phi_i (grad u . n) ds,
+      jacobian J_ij = int_F (phi_j kappa phi_i (grad u . n) + u kappa phi_i (grad phi_j . n)) ds,
+    n the outward unit normal.  Returns (R [F, 4], J [F, 4, 4])."""
+    P2, w = tri_rule(n)
+    c, lf = facets[:, 0], facets[:, 1]
+    x, _, _, K = _jacobians(coords, cells)
+    R = np.zeros((len(facets), 4))
+    Jm = np.zeros((len(facets), 4, 4))
+    D = lagrange_tables(1, REF_TET[:1])[1][0]  # [4, 3]
+    for f in range(4):
+        sel = np.nonzero(lf == f)[0]
+        if not len(sel):
+            continue
+        V = lagrange_tables(1, facet_points(f, P2))[0]  # [N, 4]
+        xc = x[c[sel]]
+        fv = xc[:, list(TET_FACETS[f])]  # [S, 3, 3]
+        cr = np.cross(fv[:, 1] - fv[:, 0], fv[:, 2] - fv[:, 0])
+        area2 = np.linalg.norm(cr, axis=1)
+        nrm = cr / area2[:, None]
+        opp = xc[:, f]  # the vertex off the facet: the normal points away from it
+        sgn = np.sign(np.einsum("sa,sa->s", nrm, fv[:, 0] - opp))
+        nrm = nrm * sgn[:, None]
+        G = _phys_grad(K[c[sel]], D)  # [S, 4, 3]
+        us, ks = u[c[sel]], kappa[c[sel]]
+        uq, kq = us @ V.T, ks @ V.T  # [S, N]
+        gun = np.einsum("si,sia,sa->s", us, G, nrm)  # grad u . n, constant on P1
+        gpn = np.einsum("sja,sa->sj", G, nrm)
+        ds = area2[:, None] * w[None, :]
+        R[sel] = np.einsum("sq,qi->si", uq * kq * gun[:, None] * ds, V)
+        Jm[sel] = (np.einsum("sq,qi,qj->sij", kq * gun[:, None] * ds, V, V)
+                   + np.einsum("sq,qi,sj->sij", uq * kq * ds, V, gpn))
+    return R, Jm
+
+
+def interior_facet_points(coords, cells, quads, n=3):
+    """Physical points [F, N, 3] and measures w*|J_F| [F, N] of tri_rule(n)
+    on every interior facet, placed as cell 0 sees them (its facet
+    permutation applied), plus the reference points of cell 0 [F, N, 3]."""
+    P2, w = tri_rule(n)
+    quads = np.asarray(quads)
+    c0, f0 = quads[:, 0], quads[:, 1]
+    x = coords[cells[c0]]
+    Xref = np.zeros((len(quads), len(w), 3))
+    for e in range(len(quads)):
+        gv = cells[c0[e]][list(TET_FACETS[f0[e]])]
+        Xref[e] = facet_points(f0[e], permute_facet_points(P2, facet_permutation(gv)))
+    J = np.transpose(x[:, 1:] - x[:, :1], (0, 2, 1))
+    Xphys = x[:, :1] + np.einsum("frk,fqk->fqr", J, Xref)
+    fv = x[np.arange(len(quads))[:, None], np.array(TET_FACETS)[f0]]
+    area2 = np.linalg.norm(np.cross(fv[:, 1] - fv[:, 0], fv[:, 2] - fv[:, 0]), axis=1)
+    return Xphys, area2[:, None] * w[None, :], Xref
+
+
+def interior_facet_forms(coords, cells, quads, u_dg1, kappa_p1, p1_cells, alpha, n=3):
+    """Interior-facet test forms of DG1 (u, the test and trial spaces) with a P1
+    kappa, by tri_rule(n) at points located on each side independently
+    (barycentric coordinates of the physical points):
+      residual   R  [F, 8] = int avg(v) avg(kappa) avg(u^2) dS,
+      jacobian   Jm [F, 8, 8] = int avg(v) avg(kappa) avg(2 u du) dS,
+      functional M  [F]    = int avg(u^2) avg(kappa) dS,
+      SIPG       S  [F, 8, 8] = int (-avg(grad du . n) jump(v) - jump(du) avg(grad v . n)
+                                     + alpha jump(du) jump(v)) dS,
+    macro dofs cell 0's then cell 1's, jump(w) = w(cell 0) - w(cell 1), n the
+    unit normal pointing out of cell 0; u_dg1 [C, 4] per cell, kappa_p1
+    vertex values through p1_cells."""
+    quads = np.asarray(quads)
+    Xp, dS, _ = interior_facet_points(coords, cells, quads, n)
+    c0, f0, c1 = quads[:, 0], quads[:, 1], quads[:, 2]
+    L0 = _barycentric(coords, cells, c0, Xp)  # [F, N, 4]: the P1 / DG1 basis values
+    L1 = _barycentric(coords, cells, c1, Xp)
+    _, _, _, K = _jacobians(coords, cells)
+    D = lagrange_tables(1, REF_TET[:1])[1][0]
+    G0, G1 = _phys_grad(K[c0], D), _phys_grad(K[c1], D)  # [F, 4, 3]
+    x0 = coords[cells[c0]]
+    fv = x0[np.arange(len(quads))[:, None], np.array(TET_FACETS)[f0]]
+    cr = np.cross(fv[:, 1] - fv[:, 0], fv[:, 2] - fv[:, 0])
+    nrm = cr / np.linalg.norm(cr, axis=1)[:, None]
+    opp = x0[np.arange(len(quads)), f0]
+    nrm = nrm * np.sign(np.einsum("fa,fa->f", nrm, fv[:, 0] - opp))[:, None]
+    kv = np.asarray(kappa_p1)
+    k0 = np.einsum("fqi,fi->fq", L0, kv[p1_cells[c0]])
+    k1 = np.einsum("fqi,fi->fq", L1, kv[p1_cells[c1]])
+    u0 = np.einsum("fqi,fi->fq", L0, u_dg1[c0])
+    u1 = np.einsum("fqi,fi->fq", L1, u_dg1[c1])
+    kav = 0.5 * (k0 + k1)
+    u2av = 0.5 * (u0 ** 2 + u1 ** 2)
+    Vm = np.concatenate([0.5 * L0, 0.5 * L1], axis=2)  # avg(v) of the macro basis
+    R = np.einsum("fq,fqi->fi", dS * kav * u2av, Vm)
+    dU = np.concatenate([0.5 * 2 * u0[:, :, None] * L0, 0.5 * 2 * u1[:, :, None] * L1], axis=2)  # avg(2 u du)
+    Jm = np.einsum("fq,fqi,fqj->fij", dS * kav, Vm, dU)
+    M = np.einsum("fq->f", dS * u2av * kav)
+    jump = np.concatenate([L0, -L1], axis=2)  # [F, N, 8]
+    gn = np.concatenate([np.einsum("fia,fa->fi", G0, nrm), np.einsum("fia,fa->fi", G1, nrm)], axis=1)  # [F, 8]
+    avg_gn = 0.5 * gn  # avg(grad w . n) of each macro basis function (constant per facet on P1)
+    S = (-np.einsum("fq,fj,fqi->fij", dS, avg_gn, jump) - np.einsum("fq,fqj,fi->fij", dS, jump, avg_gn)
+         + alpha * np.einsum("fq,fqi,fqj->fij", dS, jump, jump))
+    return R, Jm, M, S
