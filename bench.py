@@ -1839,8 +1839,7 @@ def main():
     ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batch", "multimesh", "serve", "blocksys", "interp", "dg"],
                     default="p2")
     ap.add_argument("--variant", choices=["auto", "tile", "atomic", "atomic-full", "sorted-slot", "deterministic",
-                                          "row-gather",
-                                          "block"], default="auto")
+                                          "row-gather", "block", "grouped"], default="auto")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--serve-requests", type=int, default=0, help="serve workload: requests per rate")
     ap.add_argument("--serve-rates", default="", help="serve workload: comma-separated arrival rates (req/s)")

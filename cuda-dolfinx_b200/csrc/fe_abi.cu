@@ -907,6 +907,14 @@ int fe_assemble_matrix(fe_form a, double* values, fe_bc bc0, fe_bc bc1, double d
       assemble_matrix_gather(*a, values, bc0, bc1, diagonal, zero, st);
       return;
     }
+    if (flags & FE_ASM_GROUPED) {
+      FE_REQUIRE(grouped_supported(*a), "the grouped variant supports P2 stiffness on an unrestricted pattern");
+      if (assemble_matrix_grouped(*a, values, bc0, bc1, zero, st)) {
+        if (bc0) launch_set_diagonal(*a->sp, *bc0, diagonal, values, st);
+        return;
+      }
+      // no repeated group structure in this mesh: the atomic scatter below
+    }
     if (flags & FE_ASM_DETERMINISTIC) {
       if (tile_supported(*a)) {
         assemble_matrix_tiled(*a, values, bc0, bc1, zero, true, st);

@@ -195,6 +195,10 @@ struct fe_form_s {
   // form integral given as an FFCx tabulate_tensor body (fe_ffcx.cu)
   struct Ffcx;
   std::unique_ptr<Ffcx> ffcx;
+  // grouped-summation plan (fe_group.cu); built on first use
+  struct GroupPlan;
+  std::unique_ptr<GroupPlan> groups;
+  bool group_plan_failed = false;  // the mesh has no repeated group structure
   fe_form_s();
   ~fe_form_s();
 };
@@ -280,6 +284,17 @@ struct fe_form_s::BlockPlan {
   fe::DevBuf<uint16_t> glocal;        // [cells][4] block-local geometry node of each cell vertex
   fe::DevBuf<int32_t> rec_ptr;        // P1: [nblocks+1] per-cell records of each block, padded to
                                       // whole warps and stored in the kernel's lane order
+};
+
+struct fe_form_s::GroupPlan {
+  int64_t ngroups = 0, ntemplates = 0;
+  fe::DevBuf<int32_t> tmpl_of;        // [groups] template of each group
+  fe::DevBuf<int4> tmeta;             // per template: entry offset, entry count, contribution offset,
+                                      // first-dof offset
+  fe::DevBuf<int32_t> tnd;            // per template: group-local dofs
+  fe::DevBuf<uint2> ent;              // distinct (row, column) entries of all templates
+  fe::DevBuf<uint16_t> contrib;       // their (cell, upper entry) contributions
+  fe::DevBuf<uint16_t> first;         // group-local dof -> (cell, local dof) of its first appearance
 };
 
 struct fe_form_s::BatchPlan {
@@ -403,6 +418,13 @@ void reset_tile_plan(fe_form_s& f);
 bool tile_supported(const fe_form_s& f);
 void assemble_matrix_tiled(fe_form_s& f, double* values, const fe_bc_s* bc0, const fe_bc_s* bc1, bool zero,
                            bool deterministic, cudaStream_t s);
+
+// grouped assembly (fe_group.cu) for P2 stiffness: false when the form or its
+// mesh does not take it (the caller falls back to the atomic scatter)
+bool grouped_supported(const fe_form_s& f);
+void reset_group_plan(fe_form_s& f);
+bool assemble_matrix_grouped(fe_form_s& f, double* values, const fe_bc_s* bc0, const fe_bc_s* bc1, bool zero,
+                             cudaStream_t s);
 
 // cell-block assembly (fe_block.cu) for P1/P2 stiffness
 bool block_supported(const fe_form_s& f);

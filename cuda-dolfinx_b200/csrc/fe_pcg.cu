@@ -14,6 +14,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <type_traits>
 #include <mutex>
 #include <vector>
 
@@ -420,6 +421,294 @@ extern "C" int fe_pcg_solve_noalloc(fe_sparsity s, const double* values, const d
   if (!(res <= rtol)) {
     fe::set_last_error("PCG stopped after " + std::to_string(it) + " iterations at relative residual " +
                        std::to_string(res));
+    return FE_ERR_NOT_CONVERGED;
+  }
+  return FE_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Mixed-precision solve (served requests): inner Jacobi-PCG iterations read an
+// FP32 copy of the matrix values -- for block-size-3 patterns (vector P2) in a
+// 3x3 block-column layout, one column index per block, about 4.4 bytes per
+// nonzero instead of the 12 of FP64 CSR -- and an FP64 refinement loop
+// recomputes r = b - A x with the FP64 values until |r| <= rtol |b|.  The
+// inner solves start from d = 0 and stop at inner_rtol relative to their
+// right-hand side; x += d after each.
+// ---------------------------------------------------------------------------
+namespace fe {
+namespace {
+
+template <int SUB>
+__global__ void __launch_bounds__(kThreads) k_spmv32(int64_t n, const int32_t* __restrict__ rp,
+                                                     const int32_t* __restrict__ col, const float* __restrict__ val,
+                                                     const double* __restrict__ p, double* __restrict__ Ap,
+                                                     double* __restrict__ part, const Scalars* sc) {
+  __shared__ double sh[32];
+  if (sc->done) return;
+  const int lane = threadIdx.x % SUB;
+  double pap = 0.0;
+  for_rows<SUB>(n, [&](int64_t row, bool active) {
+    double acc = 0.0;
+    const int32_t lo = active ? __ldg(rp + row) : 0, hi = active ? __ldg(rp + row + 1) : 0;
+    for (int32_t s = lo + lane; s < hi; s += SUB) acc += (double)__ldg(val + s) * __ldg(p + __ldg(col + s));
+#pragma unroll
+    for (int o = SUB / 2; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o, SUB);
+    if (active && lane == 0) {
+      Ap[row] = acc;
+      pap += p[row] * acc;
+    }
+  });
+  pap = block_sum(pap, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = pap;
+}
+
+// block rows of a block-size-3 pattern: block k of block row R covers rows
+// 3R..3R+2 and columns 3C..3C+2 (C = bcol[k]), its 9 values row-major
+template <int SUB>
+__global__ void __launch_bounds__(kThreads) k_spmv_b3(int64_t nb, const int32_t* __restrict__ brp,
+                                                      const int32_t* __restrict__ bcol, const float* __restrict__ bval,
+                                                      const double* __restrict__ p, double* __restrict__ Ap,
+                                                      double* __restrict__ part, const Scalars* sc) {
+  __shared__ double sh[32];
+  if (sc->done) return;
+  const int lane = threadIdx.x % SUB;
+  double pap = 0.0;
+  for_rows<SUB>(nb, [&](int64_t R, bool active) {
+    double y0 = 0.0, y1 = 0.0, y2 = 0.0;
+    const int32_t lo = active ? __ldg(brp + R) : 0, hi = active ? __ldg(brp + R + 1) : 0;
+    for (int32_t k = lo + lane; k < hi; k += SUB) {
+      const int64_t c3 = 3 * (int64_t)__ldg(bcol + k);
+      const double x0 = __ldg(p + c3), x1 = __ldg(p + c3 + 1), x2 = __ldg(p + c3 + 2);
+      const float* v = bval + 9 * (int64_t)k;
+      y0 += (double)__ldg(v + 0) * x0 + (double)__ldg(v + 1) * x1 + (double)__ldg(v + 2) * x2;
+      y1 += (double)__ldg(v + 3) * x0 + (double)__ldg(v + 4) * x1 + (double)__ldg(v + 5) * x2;
+      y2 += (double)__ldg(v + 6) * x0 + (double)__ldg(v + 7) * x1 + (double)__ldg(v + 8) * x2;
+    }
+#pragma unroll
+    for (int o = SUB / 2; o > 0; o >>= 1) {
+      y0 += __shfl_down_sync(0xffffffffu, y0, o, SUB);
+      y1 += __shfl_down_sync(0xffffffffu, y1, o, SUB);
+      y2 += __shfl_down_sync(0xffffffffu, y2, o, SUB);
+    }
+    if (active && lane == 0) {
+      Ap[3 * R] = y0;
+      Ap[3 * R + 1] = y1;
+      Ap[3 * R + 2] = y2;
+      pap += p[3 * R] * y0 + p[3 * R + 1] * y1 + p[3 * R + 2] * y2;
+    }
+  });
+  pap = block_sum(pap, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = pap;
+}
+
+// block layout of a block-size-3 pattern (checked: the three rows of a block
+// row list the same columns, in triples 3C, 3C+1, 3C+2)
+__global__ void k_b3_layout(int64_t nb, const int32_t* __restrict__ rp, const int32_t* __restrict__ col,
+                            int32_t* __restrict__ brp, int32_t* __restrict__ bcol, unsigned* err) {
+  const int64_t R = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (R >= nb) return;
+  const int32_t s0 = rp[3 * R], len = rp[3 * R + 1] - s0;
+  brp[R] = s0 / 9;
+  if (R == nb - 1) brp[nb] = rp[3 * nb] / 9;
+  if (len % 3 || rp[3 * R + 2] - rp[3 * R + 1] != len || rp[3 * R + 3] - rp[3 * R + 2] != len || s0 % 9) {
+    atomicOr(err, DEV_ERR_BLOCK);
+    return;
+  }
+  for (int32_t k = 0; k < len / 3; ++k) {
+    const int32_t c = col[s0 + 3 * k];
+    bool ok = c % 3 == 0;
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b) ok &= col[s0 + a * len + 3 * k + b] == c + b;
+    if (!ok) atomicOr(err, DEV_ERR_BLOCK);
+    bcol[s0 / 9 + k] = c / 3;
+  }
+}
+
+__global__ void k_to_b3(int64_t nb, const int32_t* __restrict__ rp, const int32_t* __restrict__ brp,
+                        const double* __restrict__ val, float* __restrict__ bval) {
+  const int64_t R = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (R >= nb) return;
+  const int32_t b0 = brp[R], m = brp[R + 1] - b0;
+  for (int a = 0; a < 3; ++a) {
+    const double* src = val + rp[3 * R + a];
+    for (int32_t k = 0; k < m; ++k)
+      for (int b = 0; b < 3; ++b) bval[9 * (int64_t)(b0 + k) + 3 * a + b] = (float)src[3 * k + b];
+  }
+}
+
+__global__ void k_to_f32(int64_t n, const double* __restrict__ v, float* __restrict__ w) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    w[i] = (float)v[i];
+}
+
+// inner start: r is the right-hand side, d = 0, z = p = dinv r; partial r.z, r.r, r.r
+__global__ void __launch_bounds__(kThreads) k_init_zero(int64_t n, const double* __restrict__ r,
+                                                        const double* __restrict__ dinv, double* __restrict__ z,
+                                                        double* __restrict__ p, double* __restrict__ d,
+                                                        double* __restrict__ part) {
+  __shared__ double sh[32];
+  double rz = 0.0, rr = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)kThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kThreads) {
+    const double rv = r[i], zv = dinv[i] * rv;
+    z[i] = zv;
+    p[i] = zv;
+    d[i] = 0.0;
+    rz += rv * zv;
+    rr += rv * rv;
+  }
+  rz = block_sum(rz, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = rz;
+  rr = block_sum(rr, sh);
+  if (threadIdx.x == 0) part[gridDim.x + blockIdx.x] = rr;
+  if (threadIdx.x == 0) part[2 * gridDim.x + blockIdx.x] = rr;  // the "b.b" of the inner system
+}
+
+__global__ void k_axpy(int64_t n, const double* __restrict__ d, double* __restrict__ x) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    x[i] += d[i];
+}
+
+int sub_for(double mean) { return mean <= 6 ? 4 : (mean <= 14 ? 8 : (mean <= 40 ? 16 : 32)); }
+
+template <typename F>
+void launch_sub(int sub, F&& f) {
+  switch (sub) {
+    case 4: f(std::integral_constant<int, 4>{}); break;
+    case 8: f(std::integral_constant<int, 8>{}); break;
+    case 16: f(std::integral_constant<int, 16>{}); break;
+    default: f(std::integral_constant<int, 32>{}); break;
+  }
+}
+
+}  // namespace
+
+int pcg_solve_mixed(const fe_sparsity_s& A, const double* val, const double* b, double* x, double rtol,
+                    double inner_rtol, int max_iter, int block_size, int* iterations, int* refinements,
+                    double* rel_res, cudaStream_t s) {
+  FE_REQUIRE(A.num_rows == A.num_cols, "PCG needs a square matrix");
+  FE_REQUIRE(block_size == 1 || block_size == 3, "block size must be 1 or 3");
+  FE_REQUIRE(block_size == 1 || A.num_rows % 3 == 0, "the pattern does not have block size 3");
+  FE_REQUIRE(inner_rtol > 0.0 && inner_rtol < 1.0, "inner_rtol must lie in (0, 1)");
+  const int64_t n = A.num_rows, nnz = A.nnz, nb = n / 3;
+  const unsigned grid = (unsigned)(A.ctx->num_sms * 4);
+  const unsigned grid_rows = (unsigned)(A.ctx->num_sms * 8);
+  StreamScratch buf(s);
+  double* r = buf.get<double>(n);
+  double* z = buf.get<double>(n);
+  double* p = buf.get<double>(n);
+  double* Ap = buf.get<double>(n);
+  double* dinv = buf.get<double>(n);
+  double* d = buf.get<double>(n);
+  double* part = buf.get<double>(3 * (int64_t)grid_rows);
+  Scalars* sco = buf.get<Scalars>(1);
+  Scalars* sci = buf.get<Scalars>(1);
+  float* v32 = buf.get<float>(nnz);
+  int32_t* brp = nullptr;
+  int32_t* bcol = nullptr;
+  if (block_size == 3) {
+    brp = buf.get<int32_t>(nb + 1);
+    bcol = buf.get<int32_t>(std::max<int64_t>(1, nnz / 9));
+    if (nb) {
+      // the layout is checked before anything reads it
+      k_b3_layout<<<(unsigned)((nb + 255) / 256), 256, 0, s>>>(nb, A.row_ptr.p, A.col.p, brp, bcol, A.ctx->err.p);
+      FE_CUDA(cudaGetLastError());
+      unsigned w = 0;
+      FE_CUDA(cudaMemcpyAsync(&w, A.ctx->err.p, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+      FE_CUDA(cudaStreamSynchronize(s));
+      if (w & DEV_ERR_BLOCK) {
+        FE_CUDA(cudaMemsetAsync(A.ctx->err.p, 0, sizeof(unsigned), s));
+        FE_CUDA(cudaStreamSynchronize(s));
+        FE_FAIL(FE_ERR_ARG, "the pattern is not block-structured with block size 3");
+      }
+      k_to_b3<<<(unsigned)((nb + 255) / 256), 256, 0, s>>>(nb, A.row_ptr.p, brp, val, v32);
+    }
+  } else if (nnz) {
+    k_to_f32<<<grid, kThreads, 0, s>>>(nnz, val, v32);
+  }
+  FE_CUDA(cudaGetLastError());
+  const int sub64 = sub_for(n ? (double)nnz / (double)n : 0.0);
+  const int sub32 = block_size == 3 ? sub_for(nb ? (double)nnz / 9.0 / (double)nb : 0.0) : sub64;
+  int inner_total = 0, outer = 0;
+  Scalars ho{}, hi{};
+  for (;; ++outer) {
+    // r = b - A x in FP64 (also dinv from the FP64 diagonal); stop at rtol
+    Scalars h0{};
+    h0.tol2 = rtol * rtol;
+    h0.max_iter = 1;
+    FE_CUDA(cudaMemcpyAsync(sco, &h0, sizeof(h0), cudaMemcpyHostToDevice, s));
+    launch_sub(sub64, [&](auto S) {
+      k_init<decltype(S)::value><<<grid_rows, kThreads, 0, s>>>(n, A.row_ptr.p, A.col.p, val, A.diag.p, b, x, r, z,
+                                                                p, dinv, part);
+    });
+    k_reduce<<<1, 1024, 0, s>>>(part, grid_rows, 0, sco);
+    FE_CUDA(cudaGetLastError());
+    FE_CUDA(cudaMemcpyAsync(&ho, sco, sizeof(ho), cudaMemcpyDeviceToHost, s));
+    FE_CUDA(cudaStreamSynchronize(s));
+    if (ho.rr <= rtol * rtol * ho.bb || ho.bb == 0.0 || inner_total >= max_iter) break;
+    // inner FP32 solve of A d = r from d = 0
+    Scalars h1{};
+    h1.tol2 = inner_rtol * inner_rtol;
+    h1.max_iter = max_iter - inner_total;
+    FE_CUDA(cudaMemcpyAsync(sci, &h1, sizeof(h1), cudaMemcpyHostToDevice, s));
+    k_init_zero<<<grid, kThreads, 0, s>>>(n, r, dinv, z, p, d, part);
+    k_reduce<<<1, 1024, 0, s>>>(part, grid, 0, sci);
+    FE_CUDA(cudaGetLastError());
+    const unsigned gsp = grid_rows;
+    for (int it = 0;; it += 16) {
+      for (int q = 0; q < 16; ++q) {
+        if (block_size == 3) {
+          launch_sub(sub32, [&](auto S) {
+            k_spmv_b3<decltype(S)::value><<<gsp, kThreads, 0, s>>>(nb, brp, bcol, v32, p, Ap, part, sci);
+          });
+        } else {
+          launch_sub(sub32, [&](auto S) {
+            k_spmv32<decltype(S)::value><<<gsp, kThreads, 0, s>>>(n, A.row_ptr.p, A.col.p, v32, p, Ap, part, sci);
+          });
+        }
+        k_reduce<<<1, 1024, 0, s>>>(part, gsp, 1, sci);
+        k_update<<<grid, kThreads, 0, s>>>(n, d, r, z, p, Ap, dinv, part, sci);
+        k_reduce<<<1, 1024, 0, s>>>(part, grid, 2, sci);
+        k_update_p<<<grid, kThreads, 0, s>>>(n, z, p, sci);
+      }
+      FE_CUDA(cudaGetLastError());
+      FE_CUDA(cudaMemcpyAsync(&hi, sci, sizeof(hi), cudaMemcpyDeviceToHost, s));
+      FE_CUDA(cudaStreamSynchronize(s));
+      if (hi.done) break;
+    }
+    inner_total += hi.iter;
+    k_axpy<<<grid, kThreads, 0, s>>>(n, d, x);
+    FE_CUDA(cudaGetLastError());
+    if (hi.iter == 0) break;  // no progress possible
+  }
+  buf.release();
+  if (iterations) *iterations = inner_total;
+  if (refinements) *refinements = outer;
+  if (rel_res) *rel_res = ho.bb > 0 ? sqrt(ho.rr / ho.bb) : 0.0;
+  return inner_total;
+}
+
+}  // namespace fe
+
+extern "C" int fe_pcg_solve_mixed(fe_sparsity s, const double* values, const double* b, double* x, double rtol,
+                                  double inner_rtol, int max_iter, int block_size, int* iterations,
+                                  int* refinements, double* rel_residual, void* stream) {
+  int it = 0, ref = 0;
+  double res = 0.0;
+  try {
+    if (!s || !values || !b || !x) FE_FAIL(FE_ERR_ARG, "null argument");
+    FE_CUDA(cudaSetDevice(s->ctx->device));
+    const cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    fe::pcg_solve_mixed(*s, values, b, x, rtol, inner_rtol, max_iter, block_size, &it, &ref, &res, st);
+    if (iterations) *iterations = it;
+    if (refinements) *refinements = ref;
+    if (rel_residual) *rel_residual = res;
+  } catch (const fe::Error& e) {
+    fe::set_last_error(e.what());
+    return e.code;
+  }
+  if (!(res <= rtol)) {
+    fe::set_last_error("mixed-precision PCG stopped after " + std::to_string(it) + " inner iterations and " +
+                       std::to_string(ref) + " refinements at relative residual " + std::to_string(res));
     return FE_ERR_NOT_CONVERGED;
   }
   return FE_OK;

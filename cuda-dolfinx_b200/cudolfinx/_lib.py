@@ -43,8 +43,9 @@ INTEGRAL = {"cell": 0, "exterior_facet": 1, "interior_facet": 2}
 PREC_FP64, PREC_FP32 = 0, 1
 ASM_ZERO, ASM_DETERMINISTIC, ASM_ATOMIC, ASM_SORTED_SLOT, ASM_TILE, ASM_ROW_GATHER, ASM_BLOCK = 1, 2, 4, 8, 16, 32, 64
 ASM_FULL_SCATTER = 128
+ASM_GROUPED = 256
 VARIANT_FLAGS = {"auto": 0, "deterministic": ASM_DETERMINISTIC, "atomic": ASM_ATOMIC, "sorted-slot": ASM_SORTED_SLOT,
-                 "tile": ASM_TILE, "row-gather": ASM_ROW_GATHER, "block": ASM_BLOCK, "atomic-full": ASM_ATOMIC | ASM_FULL_SCATTER}
+                 "tile": ASM_TILE, "row-gather": ASM_ROW_GATHER, "block": ASM_BLOCK, "atomic-full": ASM_ATOMIC | ASM_FULL_SCATTER, "grouped": ASM_GROUPED}
 
 _SIGS = {
     "fe_last_error": (ctypes.c_char_p, []),
@@ -96,6 +97,8 @@ _SIGS = {
     "fe_set_bc": (i32, [vp, i64, vp, vp, dbl, vp]),
     "fe_pcg_solve": (i32, [vp, vp, vp, vp, dbl, i32, ctypes.POINTER(i32), ctypes.POINTER(dbl), vp]),
     "fe_pcg_solve_noalloc": (i32, [vp, vp, vp, vp, dbl, i32, ctypes.POINTER(i32), ctypes.POINTER(dbl), vp]),
+    "fe_pcg_solve_mixed": (i32, [vp, vp, vp, vp, dbl, dbl, i32, i32, ctypes.POINTER(i32), ctypes.POINTER(i32),
+                                 ctypes.POINTER(dbl), vp]),
 }
 
 for _name, (_res, _args) in _SIGS.items():

@@ -368,16 +368,33 @@ class CUDAAssembler:
 
     # -- solve ---------------------------------------------------------------
     def solve(self, A: CUDAMatrix, b: CUDAVector, x: typing.Optional[CUDAVector] = None, rtol: float = 1e-8,
-              max_iter: int = 20000, raise_on_failure: bool = True):
-        """Jacobi-preconditioned CG on the device; returns (x, iterations, relative residual)."""
+              max_iter: int = 20000, raise_on_failure: bool = True, precision: str = "fp64", block_size: int = 1,
+              inner_rtol: float = 1e-4):
+        """Jacobi-preconditioned CG on the device; returns (x, iterations,
+        relative residual).  ``precision="mixed"``: inner iterations on an FP32
+        copy of the values (``block_size=3``: in a 3x3 block-column layout, for
+        vector-valued spaces), refined in FP64 to ``rtol``; iterations counts
+        the inner ones."""
         import ctypes
+        if precision not in ("fp64", "mixed"):
+            raise ValueError("precision must be 'fp64' or 'mixed'")
         if x is None:
             x = CUDAVector(self._ctx, b.size)
         x._before_write()
         it, res = ctypes.c_int(0), ctypes.c_double(0.0)
-        st = _lib.lib.fe_pcg_solve(A.sparsity.handle, A.values.data_ptr(), b.vector.data_ptr(), x.vector.data_ptr(),
-                                   float(rtol), int(max_iter), ctypes.byref(it), ctypes.byref(res), self._ctx.stream())
+        if precision == "mixed":
+            ref = ctypes.c_int(0)
+            st = _lib.lib.fe_pcg_solve_mixed(A.sparsity.handle, A.values.data_ptr(), b.vector.data_ptr(),
+                                             x.vector.data_ptr(), float(rtol), float(inner_rtol), int(max_iter),
+                                             int(block_size), ctypes.byref(it), ctypes.byref(ref), ctypes.byref(res),
+                                             self._ctx.stream())
+            what = "fe_pcg_solve_mixed"
+        else:
+            st = _lib.lib.fe_pcg_solve(A.sparsity.handle, A.values.data_ptr(), b.vector.data_ptr(),
+                                       x.vector.data_ptr(), float(rtol), int(max_iter), ctypes.byref(it),
+                                       ctypes.byref(res), self._ctx.stream())
+            what = "fe_pcg_solve"
         if st == _lib.FE_ERR_NOT_CONVERGED and not raise_on_failure:
             return x, it.value, res.value
-        _lib.check(st, "fe_pcg_solve")
+        _lib.check(st, what)
         return x, it.value, res.value

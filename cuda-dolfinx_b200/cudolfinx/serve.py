@@ -17,11 +17,14 @@ requests as they arrive and keeps several of them on the device at once:
   least-recently-used first); requests wait in arrival order otherwise, and a
   request larger than the whole budget is answered with an error;
 * every worker drives its own CUDA stream, so the assemblies and solves of
-  concurrent requests overlap on the device.
+  concurrent requests overlap on the device;
+* solves run in mixed precision: inner Jacobi-PCG iterations on an FP32 copy
+  of the matrix values (vector P2 in 3x3 blocks: 4.4 instead of 12 bytes per
+  nonzero), refined against the FP64 residual to the request's rtol.
 
 ``plain`` mode is the one-at-a-time FP64 path the server is compared with:
 one worker, no caches (each request builds its mesh, pattern and forms),
-FP64 element tensors.
+FP64 element tensors, the FP64 solver.
 """
 from __future__ import annotations
 
@@ -87,10 +90,12 @@ def problem_sizes(kind: str, n: int) -> dict:
 
 def slot_bytes(kind: str, n: int) -> int:
     """Device bytes of one slot: CSR values, cell-to-slot map, b, x, BC data,
-    PCG scratch (5 vectors + its element of the pattern share), coefficients."""
+    solver scratch (6 vectors, an FP32 copy of the values and, for vector P2,
+    its block-column index), coefficients."""
     s = problem_sizes(kind, n)
     ncoef = 2 if kind == "vp2" else 1
-    return (8 * s["nnz"] + s["cells"] * s["k"] * s["k"] + 8 * 2 * s["rows"] + 9 * s["rows"] + 8 * 5 * s["rows"]
+    return (8 * s["nnz"] + s["cells"] * s["k"] * s["k"] + 8 * 2 * s["rows"] + 9 * s["rows"] + 8 * 6 * s["rows"]
+            + 4 * s["nnz"] + (s["nnz"] // 9 * 4 + s["rows"] // 3 * 4 if kind == "vp2" else 0)
             + 8 * ncoef * s["cells"])
 
 
@@ -270,7 +275,7 @@ class _Slot:
         self.V = sh.V
 
 
-def _execute(asm, slot: _Slot, req: Request, variant: str = "auto"):
+def _execute(asm, slot: _Slot, req: Request, variant: str = "auto", solver: str = "fp64"):
     import torch
     for dev, host in zip(slot.coef, req.coef):
         dev.copy_(torch.from_numpy(np.ascontiguousarray(host, dtype=np.float64)), non_blocking=True)
@@ -279,7 +284,8 @@ def _execute(asm, slot: _Slot, req: Request, variant: str = "auto"):
     asm.apply_lifting(slot.b, [slot.a], [slot.bcs])
     asm.set_bc(slot.b, slot.bcs, slot.V)
     slot.x.vector.zero_()
-    x, its, res = asm.solve(slot.A, slot.b, slot.x, rtol=req.rtol, raise_on_failure=False)
+    x, its, res = asm.solve(slot.A, slot.b, slot.x, rtol=req.rtol, raise_on_failure=False, precision=solver,
+                            block_size=slot.V.bs)
     xh = x.vector.to("cpu")  # waits for this stream only
     return xh.numpy(), its, res
 
@@ -292,11 +298,13 @@ class Server:
     ``precision``: element tensors of the P2 and vector-P2 forms ("fp32" or
     "fp64"; P1 is always FP64).  ``variant``: matrix assembly variant
     ("deterministic" makes every result bitwise independent of what else
-    runs).  ``plain=True``: the one-at-a-time FP64 path (one worker, nothing
-    cached)."""
+    runs).  ``solver``: "mixed" (FP32 values in the inner PCG iterations, in
+    3x3 blocks for vector P2, refined in FP64 to the request's rtol) or "fp64".
+    ``plain=True``: the one-at-a-time FP64 path (one worker, nothing cached,
+    FP64 solver)."""
 
     def __init__(self, workers: int = 4, hbm_budget: int = 40 << 30, precision: str = "fp32", plain: bool = False,
-                 variant: str = "auto"):
+                 variant: str = "auto", solver: str = "mixed"):
         import torch
 
         from .assemble import CUDAAssembler
@@ -304,6 +312,7 @@ class Server:
         self.variant = variant
         self.workers = 1 if plain else int(workers)
         self.precision = "fp64" if plain else precision
+        self.solver = "fp64" if plain else solver
         self.ledger = SlotLedger(hbm_budget)
         self._shared: dict = {}
         self._shared_lock = threading.Lock()
@@ -403,7 +412,7 @@ class Server:
                                 raise
                             with cond:
                                 self.ledger.register(key, slot, nb)
-                        x, its, res = _execute(self._asm, slot, req, self.variant)
+                        x, its, res = _execute(self._asm, slot, req, self.variant, self.solver)
                 except Exception as e:  # the request fails, the server goes on
                     x, its, res, err = None, 0, float("nan"), f"{type(e).__name__}: {e}"
                 done = time.perf_counter() - t0

@@ -121,6 +121,10 @@ enum fe_precision {
 #define FE_ASM_BLOCK 64u          /* Morton cell blocks combined in shared memory, then coalesced
                                      reductions (P1/P2)                                              */
 #define FE_ASM_FULL_SCATTER 128u  /* atomic scatter into both triangles, as the reference does      */
+#define FE_ASM_GROUPED 256u       /* P2 stiffness: consecutive cells in groups of 48, each group's element
+                                     entries summed per distinct CSR slot in shared memory, then one
+                                     reduction per slot (falls back to the atomic scatter when the
+                                     mesh's groups share no structure)                                */
 
 /* ---- errors / context --------------------------------------------------- */
 const char* fe_last_error(void);
@@ -380,6 +384,21 @@ int fe_interpolate(fe_dofmap target, double* u1, fe_dofmap source, const double*
  * the stream.  Returns FE_ERR_NOT_CONVERGED if max_iter was reached. */
 int fe_pcg_solve(fe_sparsity s, const double* values, const double* b, double* x, double rtol,
                  int max_iter, int* iterations, double* rel_residual, void* stream);
+
+/* Mixed-precision Jacobi-PCG (no counterpart in the reference; the served
+ * requests of cudolfinx.serve use it).  Inner PCG iterations read an FP32 copy
+ * of the values -- with block_size 3 (vector P2 patterns) in a 3x3
+ * block-column layout, one column index per block -- and stop at inner_rtol
+ * relative to their right-hand side; an FP64 refinement loop recomputes
+ * r = b - A x from the FP64 values and adds the inner solutions until
+ * |r| <= rtol |b|, so the result meets rtol in FP64.  max_iter bounds the
+ * inner iterations in total; *iterations receives them, *refinements the
+ * outer steps.  Allocates its scratch with cudaMallocAsync on `stream` and
+ * synchronises it.  Returns FE_ERR_NOT_CONVERGED when max_iter is reached and
+ * FE_ERR_ARG when block_size is 3 and the pattern is not block-structured. */
+int fe_pcg_solve_mixed(fe_sparsity s, const double* values, const double* b, double* x, double rtol,
+                       double inner_rtol, int max_iter, int block_size, int* iterations, int* refinements,
+                       double* rel_residual, void* stream);
 
 /* Allocation-free variant of fe_pcg_solve (no counterpart in the reference).
  * For callers that cannot allocate device memory while they solve: an

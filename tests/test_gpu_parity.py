@@ -35,12 +35,14 @@ def _problem_from_golden(path):
     return P, G
 
 
-VARIANTS = ["auto", "atomic", "atomic-full", "tile", "deterministic", "sorted-slot", "row-gather", "block"]
+VARIANTS = ["auto", "atomic", "atomic-full", "tile", "deterministic", "sorted-slot", "row-gather", "block", "grouped"]
 
 
 def _supported(kind, variant):
     if variant == "row-gather":
         return kind in ("p1", "p1k")
+    if variant == "grouped":
+        return kind == "p2"
     if variant in ("tile", "block"):
         return kind in ("p1", "p1k", "p2")
     return True
@@ -199,6 +201,30 @@ def test_pcg_solution_matches_direct_solve():
         assert np.linalg.norm(xh - x_ref) <= 1e-7 * np.linalg.norm(x_ref)
 
 
+def test_mixed_precision_pcg_meets_rtol_in_fp64():
+    # inner iterations on FP32 values (block size 3: 3x3 block columns),
+    # refined in FP64: the FP64 residual meets rtol and x matches a direct solve
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spla
+
+    for kind, n, bs in (("p2", 5, 1), ("vp2", 3, 3), ("p1", 8, 1)):
+        P = fo.build_problem(kind, n, seed=9)
+        R = run_system(P)
+        N = len(R["row_ptr"]) - 1
+        A = sp.csr_matrix((R["A"], R["col"], R["row_ptr"]), shape=(N, N))
+        x_ref = spla.spsolve(A.tocsc(), R["b"])
+        x, it, res = R["asm"].solve(R["Aobj"], R["bobj"], rtol=1e-10, precision="mixed", block_size=bs)
+        xh = x.to_host()
+        assert res <= 1e-10 and it > 0
+        assert np.linalg.norm(A @ xh - R["b"]) <= 1.5e-10 * np.linalg.norm(R["b"])
+        assert np.linalg.norm(xh - x_ref) <= 1e-7 * np.linalg.norm(x_ref)
+    # a scalar pattern is not block-structured
+    P = fo.build_problem("p2", 3, seed=9)
+    R = run_system(P)
+    with pytest.raises(RuntimeError, match="block size 3"):
+        R["asm"].solve(R["Aobj"], R["bobj"], precision="mixed", block_size=3)
+
+
 def test_pcg_reports_non_convergence():
     P = fo.build_problem("p2", 5, seed=8)
     R = run_system(P)
@@ -238,3 +264,47 @@ def test_empty_bc_and_empty_mesh():
     A = asm.assemble_matrix(a, bcs=[])
     A.assemble()
     assert A.sparsity.nnz == 0
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_grouped_variant_on_permuted_cells_and_renumbered_dofs(precision):
+    # the grouped plan comes from the dofmap and the cell centroids only: a
+    # random cell order and a random dof numbering give the same matrix
+    from conftest import ensure_library
+    ensure_library()
+    import cudolfinx as cx
+    from cudolfinx import fem
+
+    n = 7
+    P = fo.build_problem("p2", n, seed=21)
+    rng = np.random.default_rng(5)
+    cp = rng.permutation(len(P["cells"]))
+    cells = P["cells"][cp]
+    mesh = fem.Mesh(P["coords"], cells, grid_n=n)
+    V = fem.functionspace(mesh, ("P", 2))
+    dp = rng.permutation(V.num_nodes).astype(np.int32)  # new number of each dof
+    V.dofs = np.ascontiguousarray(dp[V.dofs])
+    V1 = fem.functionspace(mesh, ("P", 1))
+    k = fem.Function(V1, P["k"])
+    bdofs = np.sort(dp[P["bc_dofs"]]).astype(np.int32)
+    g = np.zeros(V.num_dofs)
+    g[dp] = P["g"]
+    bc = fem.dirichletbc(fem.Function(V, g), bdofs)
+    asm = cx.CUDAAssembler()
+    a = cx.form(fem.stiffness(V, k, precision=precision))
+    A = asm.assemble_matrix(a, bcs=[bc], variant="grouped")
+    A.assemble()
+    rp, col = A.sparsity.to_host()
+    rp_o, col_o = fo.sparsity(V.dofs, V.dofs, V.num_nodes)
+    assert np.array_equal(rp, rp_o) and np.array_equal(col, col_o)
+    Ae = fo.p2_stiffness(P["coords"], cells, P["k"][cells])
+    mk = np.zeros(V.num_dofs, dtype=np.uint8)
+    mk[bdofs] = 1
+    ref = fo.assemble_matrix(Ae, V.dofs, V.dofs, rp_o, col_o, 1, 1, mk, mk, 1.0, bdofs)
+    if precision == "fp64":
+        ok, worst = tolerance_check(A.values.cpu().numpy(), ref,
+                                    fo.matrix_bound(Ae, V.dofs, V.dofs, rp_o, col_o, 1, 1, mk, mk))
+        assert ok, worst
+    else:
+        rel = np.linalg.norm(A.values.cpu().numpy() - ref) / np.linalg.norm(ref)
+        assert 0.0 < rel < 2e-6, rel
