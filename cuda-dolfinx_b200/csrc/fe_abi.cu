@@ -50,6 +50,7 @@ std::string decode_device_error(unsigned w) {
   if (w & DEV_ERR_BLOCK) s += " [CSR rows of a block row are not block-structured]";
   if (w & DEV_ERR_INDEX) s += " [index out of range]";
   if (w & DEV_ERR_FACET) s += " [the two sides of an interior facet are different triangles]";
+  if (w & DEV_ERR_BARRIER) s += " [a grid barrier timed out]";
   return s;
 }
 

@@ -13,12 +13,14 @@
 // of its row's FP32 off-diagonal entries, so element rows sum to zero as the
 // exact ones do), and then forms every instance's values with FP64
 // accumulation in one persistent launch:
-//   k_batch_pack    k_s(c) (FP64, one array per instance) -> kp[c][s] (FP32),
-//                   a tiled transpose (the batch's pack_coefficients)
-//   k_batch_elem_*  unit-coefficient element tensors E[c][i*K+j]
-//   k_batch_fill    rec[r] = {E of record r, cell of record r}, records in
-//                   slot order (the sorted-slot plan of fe_gather.cu)
-//   k_batch_gather  persistent; one warp per (8 slots x 32*IPL instances):
+//   k_batch_elem_*  unit-coefficient element tensors E[c][i*K+j]     } once per
+//   k_batch_fill    rec[r] = {E of record r, cell of record r}, records } mesh and
+//                   in slot order (the sorted-slot plan of fe_gather.cu)  } pattern
+//   k_batch_fused   one persistent cooperative launch per call: k_s(c)
+//                   (FP64, one array per instance) -> kp[c][s] (FP32), a
+//                   tiled transpose (the batch's pack_coefficients); a grid
+//                   barrier; then the gather, one warp per (8 slots x 32*IPL
+//                   instances):
 //                   lane = instance while summing a slot's records (the
 //                   coefficient row kp[c][..] is one coalesced load), lane =
 //                   slot while storing (a staging tile in shared memory turns
@@ -68,38 +70,6 @@ __global__ void k_plan_slot_row(const int32_t* __restrict__ row_ptr, int64_t num
   const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (r >= num_rows) return;
   for (int32_t s = row_ptr[r]; s < row_ptr[r + 1]; ++s) slot_row[s] = (int32_t)r;
-}
-
-// ---- pack ----------------------------------------------------------------
-struct PackArgs {
-  int64_t num_cells;
-  int num_inst;       // instances in this launch
-  int64_t ld;         // row stride of kp (floats)
-  int col0;           // first kp column of this launch
-  float* kp;
-  const double* coef[kMaxBatchLaunch];
-};
-
-// 32 cells x 32 instances per block: coalesced reads along cells, coalesced
-// writes along instances; columns past num_inst are written as zero.
-__global__ void __launch_bounds__(256) k_batch_pack(const __grid_constant__ PackArgs a) {
-  __shared__ float t[32][33];
-  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-  const int64_t c0 = blockIdx.x * 32ll;
-  const int s0 = blockIdx.y * 32;
-#pragma unroll
-  for (int j = 0; j < 4; ++j) {
-    const int sl = ty + 8 * j, s = s0 + sl;
-    const int64_t c = c0 + tx;
-    t[sl][tx] = (s < a.num_inst && c < a.num_cells) ? (float)__ldg(a.coef[s] + c) : 0.0f;
-  }
-  __syncthreads();
-#pragma unroll
-  for (int j = 0; j < 4; ++j) {
-    const int cl = ty + 8 * j;
-    const int64_t c = c0 + cl;
-    if (c < a.num_cells && a.col0 + s0 + tx < a.ld) a.kp[c * a.ld + a.col0 + s0 + tx] = t[tx][cl];
-  }
 }
 
 // ---- unit-coefficient element tensors (FP32 out, FP64 geometry) ----------
@@ -263,12 +233,18 @@ struct KVec<4> {
 // load and kLoadBatch of them are in flight.  Staged results use column
 // (i % IPL) * 32 + i / IPL for instance i, so the per-lane writes are
 // conflict-free.
-template <int IPL>
-__global__ void __launch_bounds__(32 * GatherCfg<IPL>::WARPS, GatherCfg<IPL>::MIN_BLOCKS)
-    k_batch_gather(const __grid_constant__ GatherArgs a) {
+// kp loads: through the read-only path when kp was written by an earlier
+// launch, at L2 (ld.global.cg) when this launch wrote it before a grid barrier
+template <bool L2ONLY, typename KV>
+__device__ __forceinline__ KV load_kp(const KV* p) {
+  if constexpr (L2ONLY) return __ldcg(p);
+  else return __ldg(p);
+}
+
+template <int IPL, bool L2ONLY>
+__device__ __forceinline__ void gather_items(const GatherArgs& a, unsigned char* smem_raw) {
   using Cfg = GatherCfg<IPL>;
   using KV = typename KVec<IPL>::T;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   unsigned char* wbase = smem_raw + wid * Cfg::WARP_SMEM;
   BatchRec* __restrict__ R = reinterpret_cast<BatchRec*>(wbase);
@@ -316,7 +292,7 @@ __global__ void __launch_bounds__(32 * GatherCfg<IPL>::WARPS, GatherCfg<IPL>::MI
       for (; q0 + kLoadBatch <= cnt; q0 += kLoadBatch) {
         KV kv[kLoadBatch];
 #pragma unroll
-        for (int u = 0; u < kLoadBatch; ++u) kv[u] = __ldg(kb + (int64_t)R[q0 + u].cell * ldv);
+        for (int u = 0; u < kLoadBatch; ++u) kv[u] = load_kp<L2ONLY>(kb + (int64_t)R[q0 + u].cell * ldv);
 #pragma unroll
         for (int u = 0; u < kLoadBatch; ++u) consume(base + q0 + u, R[q0 + u].ae, kv[u]);
       }
@@ -324,7 +300,7 @@ __global__ void __launch_bounds__(32 * GatherCfg<IPL>::WARPS, GatherCfg<IPL>::MI
         KV kv[kLoadBatch];
 #pragma unroll
         for (int u = 0; u < kLoadBatch; ++u)
-          if (q0 + u < cnt) kv[u] = __ldg(kb + (int64_t)R[q0 + u].cell * ldv);
+          if (q0 + u < cnt) kv[u] = load_kp<L2ONLY>(kb + (int64_t)R[q0 + u].cell * ldv);
 #pragma unroll
         for (int u = 0; u < kLoadBatch; ++u)
           if (q0 + u < cnt) consume(base + q0 + u, R[q0 + u].ae, kv[u]);
@@ -376,17 +352,83 @@ __global__ void __launch_bounds__(32 * GatherCfg<IPL>::WARPS, GatherCfg<IPL>::MI
   }
 }
 
+// One persistent launch per batch of instances: phase 1 packs the instances'
+// coefficients into kp (32 cells x 32 instances per tile, the transpose of
+// a plain pack kernel), a grid barrier, phase 2 gathers (gather_items).  Launched
+// cooperatively, so every block is resident and the barrier completes; its
+// wait is still bounded: a block that waits too long sets DEV_ERR_BARRIER in
+// the error word and returns.
+struct FusedArgs {
+  int64_t num_cells;
+  int64_t pack_cols;    // kp columns this launch writes (its instances + trailing zero padding)
+  const double* coef[kMaxBatchLaunch];
+  float* kp;            // the packed coefficients the gather reads (g.kp)
+  unsigned* barrier;    // zeroed before the launch
+  unsigned* err;
+  GatherArgs g;
+};
+
+constexpr long long kBarrierSpins = 1ll << 26;  // x ~100 ns: a few seconds
+
 template <int IPL>
-void launch_gather(const GatherArgs& ga, int num_sms, cudaStream_t s) {
+__global__ void __launch_bounds__(32 * GatherCfg<IPL>::WARPS, GatherCfg<IPL>::MIN_BLOCKS)
+    k_batch_fused(const __grid_constant__ FusedArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float(*t)[33] = reinterpret_cast<float(*)[33]>(smem_raw);  // 32 x 33 floats of the gather buffers
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  const int64_t tiles_c = (a.num_cells + 31) / 32, tiles_s = (a.pack_cols + 31) / 32;
+  for (int64_t tile = blockIdx.x; tile < tiles_c * tiles_s; tile += gridDim.x) {
+    const int64_t c0 = (tile % tiles_c) * 32;
+    const int s0 = (int)(tile / tiles_c) * 32;
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int sl = ty + 8 * j, si = s0 + sl;
+      const int64_t c = c0 + tx;
+      t[sl][tx] = (si < a.g.num_inst && c < a.num_cells) ? (float)__ldg(a.coef[si] + c) : 0.0f;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int cl = ty + 8 * j;
+      const int64_t c = c0 + cl;
+      if (c < a.num_cells && s0 + tx < a.pack_cols) a.kp[c * a.g.ld + a.g.col0 + s0 + tx] = t[tx][cl];
+    }
+  }
+  // grid barrier
+  __shared__ int abort_flag;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    atomicAdd(a.barrier, 1u);
+    long long spins = 0;
+    while (*(volatile unsigned*)a.barrier < gridDim.x && spins < kBarrierSpins) {
+      __nanosleep(100);
+      ++spins;
+    }
+    abort_flag = spins >= kBarrierSpins;
+    if (abort_flag) atomicOr(a.err, DEV_ERR_BARRIER);
+    __threadfence();
+  }
+  __syncthreads();
+  if (abort_flag) return;
+  gather_items<IPL, true>(a.g, smem_raw);
+}
+
+template <int IPL>
+void launch_fused(FusedArgs& fa, int num_sms, cudaStream_t s) {
   using Cfg = GatherCfg<IPL>;
   // per device and cheap: set on every launch rather than cached
-  FE_CUDA(cudaFuncSetAttribute(k_batch_gather<IPL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM));
+  FE_CUDA(cudaFuncSetAttribute(k_batch_fused<IPL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM));
   int per_sm = 0;
-  FE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_gather<IPL>, 32 * Cfg::WARPS, Cfg::SMEM));
-  const int64_t want = (ga.num_items + Cfg::WARPS - 1) / Cfg::WARPS;
+  FE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_fused<IPL>, 32 * Cfg::WARPS, Cfg::SMEM));
+  const int64_t want = std::max<int64_t>((fa.g.num_items + Cfg::WARPS - 1) / Cfg::WARPS,
+                                         ((fa.num_cells + 31) / 32) * ((fa.pack_cols + 31) / 32));
   const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)num_sms * std::max(1, per_sm)));
-  k_batch_gather<IPL><<<(unsigned)grid, 32 * Cfg::WARPS, Cfg::SMEM, s>>>(ga);
-  FE_CUDA(cudaGetLastError());
+  FE_CUDA(cudaMemsetAsync(fa.barrier, 0, sizeof(unsigned), s));
+  void* args[] = {&fa};
+  FE_CUDA(cudaLaunchCooperativeKernel((const void*)k_batch_fused<IPL>, dim3((unsigned)grid), dim3(32 * Cfg::WARPS),
+                                      args, Cfg::SMEM, s));
 }
 
 }  // namespace
@@ -443,21 +485,10 @@ void assemble_matrix_batch(fe_form_s& f, int num_instances, const double* const*
     B.kp.alloc(std::max<int64_t>(1, C * ld));
     B.kp_ld = ld;
   }
-  if (C) {
-    for (int i0 = 0; i0 < num_instances; i0 += kMaxBatchLaunch) {
-      PackArgs pa{};
-      pa.num_cells = C;
-      pa.num_inst = std::min(kMaxBatchLaunch, num_instances - i0);
-      pa.ld = ld;
-      pa.col0 = i0;
-      pa.kp = B.kp.p;
-      for (int i = 0; i < pa.num_inst; ++i) pa.coef[i] = coefficients[i0 + i];
-      // the last launch also zeroes the padding columns up to ld
-      const int64_t cols = (i0 + kMaxBatchLaunch >= num_instances) ? ld - i0 : pa.num_inst;
-      dim3 grid(nblocks(C, 32), nblocks(cols, 32));
-      k_batch_pack<<<grid, 256, 0, s>>>(pa);
-      FE_CUDA(cudaGetLastError());
-    }
+  // the unit-coefficient element tensors and the slot-sorted records depend
+  // only on the mesh (immutable once created) and the plan: built on the
+  // first call
+  if (C && !B.rec_valid) {
     ElemArgs ea{C, f.mesh->x.p, f.mesh->geom.p, B.E.p};
     if (f.kind == FE_FORM_P1_STIFFNESS) k_batch_elem_p1<<<nblocks(C, 128), 128, 0, s>>>(ea);
     else k_batch_elem_p2<<<nblocks(C, 128), 128, 0, s>>>(ea);
@@ -465,16 +496,25 @@ void assemble_matrix_batch(fe_form_s& f, int num_instances, const double* const*
     k_batch_fill<<<nblocks(B.num_records, 256), 256, 0, s>>>(B.rec_cell.p, B.rec_entry.p, B.num_records, KK, B.E.p,
                                                              reinterpret_cast<BatchRec*>(B.rec.p));
     FE_CUDA(cudaGetLastError());
+    B.rec_valid = true;
   }
-  if (!nnz) return;
+  if (!B.barrier.p) B.barrier.alloc(1);
   for (int i0 = 0; i0 < num_instances; i0 += kMaxBatchLaunch) {
-    GatherArgs ga{};
+    FusedArgs fa{};
+    fa.num_cells = C;
+    fa.kp = B.kp.p;
+    fa.barrier = B.barrier.p;
+    fa.err = device_error_word(f.ctx);
+    GatherArgs& ga = fa.g;
     ga.nnz = nnz;
     ga.num_inst = std::min(kMaxBatchLaunch, num_instances - i0);
+    // the last launch also zeroes the padding columns up to ld
+    fa.pack_cols = (i0 + kMaxBatchLaunch >= num_instances) ? ld - i0 : ga.num_inst;
+    for (int i = 0; i < ga.num_inst; ++i) fa.coef[i] = coefficients[i0 + i];
     ga.col0 = i0;
     ga.ld = ld;
     ga.num_chunks = (ga.num_inst + chunk - 1) / chunk;
-    ga.num_items = ((nnz + kSlotsPerItem - 1) / kSlotsPerItem) * ga.num_chunks;
+    ga.num_items = nnz ? ((nnz + kSlotsPerItem - 1) / kSlotsPerItem) * ga.num_chunks : 0;
     FE_REQUIRE(ga.num_items < INT32_MAX, "batch too large for one gather launch");
     ga.seg = f.gather->seg.p;
     ga.rec = reinterpret_cast<const BatchRec*>(B.rec.p);
@@ -486,9 +526,10 @@ void assemble_matrix_batch(fe_form_s& f, int num_instances, const double* const*
     ga.diagonal = diagonal;
     ga.zero = zero ? 1 : 0;
     for (int i = 0; i < ga.num_inst; ++i) ga.values[i] = values[i0 + i];
-    if (ipl == 4) launch_gather<4>(ga, f.ctx->num_sms, s);
-    else if (ipl == 2) launch_gather<2>(ga, f.ctx->num_sms, s);
-    else launch_gather<1>(ga, f.ctx->num_sms, s);
+    if (!C && !nnz) continue;
+    if (ipl == 4) launch_fused<4>(fa, f.ctx->num_sms, s);
+    else if (ipl == 2) launch_fused<2>(fa, f.ctx->num_sms, s);
+    else launch_fused<1>(fa, f.ctx->num_sms, s);
   }
 }
 

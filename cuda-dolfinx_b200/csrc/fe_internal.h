@@ -39,7 +39,8 @@ enum DeviceError : unsigned {
   DEV_ERR_ROW_WIDE = 2u,   // a block row has more than 255 block columns
   DEV_ERR_BLOCK = 4u,      // the CSR rows of one block row differ
   DEV_ERR_INDEX = 8u,      // an index outside its array
-  DEV_ERR_FACET = 16u      // the two local facets of an interior facet are not the same triangle
+  DEV_ERR_FACET = 16u,     // the two local facets of an interior facet are not the same triangle
+  DEV_ERR_BARRIER = 32u    // a grid barrier was not reached by every block in time
 };
 
 // RAII device buffer.
@@ -304,7 +305,9 @@ struct fe_form_s::BatchPlan {
   fe::DevBuf<uint8_t> rec_entry;      // [records] local entry i*K+j of each record
   fe::DevBuf<int32_t> slot_row;       // [nnz] CSR row of each slot
   fe::DevBuf<double> E;               // [cells][KK] unit-coefficient element tensors (FP32 values)
-  fe::DevBuf<double2> rec;            // [records] {entry value, cell}, refreshed per call (16 B each)
+  fe::DevBuf<double2> rec;            // [records] {entry value, cell} (16 B each)
+  bool rec_valid = false;             // E and rec built (they depend on the mesh and the plan only)
+  fe::DevBuf<unsigned> barrier;       // grid-barrier counter of the fused launch
   fe::DevBuf<float> kp;               // [cells][ld] packed instance coefficients (FP32)
   int64_t kp_ld = 0;
 };
