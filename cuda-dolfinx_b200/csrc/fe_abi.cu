@@ -690,6 +690,17 @@ int fe_form_set_interior_facets(fe_form f, const int32_t* quads, int64_t num_fac
   });
 }
 
+int fe_form_set_launch(fe_form f, int cells_per_cta, int stage) {
+  return guard([&] {
+    FE_REQUIRE(f, "null form");
+    FE_REQUIRE(cells_per_cta == 0 || cells_per_cta == 32 || cells_per_cta == 64 || cells_per_cta == 128,
+               "cells per CTA must be 0 (default), 32, 64 or 128");
+    FE_REQUIRE(stage == 0 || stage == 1, "stage must be 0 or 1");
+    f->launch_cells = cells_per_cta;
+    f->launch_stage = stage;
+  });
+}
+
 int fe_form_set_precision(fe_form f, int precision) {
   return guard([&] {
     FE_REQUIRE(f, "null form");
@@ -981,6 +992,8 @@ int fe_assemble_matrix(fe_form a, double* values, fe_bc bc0, fe_bc bc1, double d
     L.c1 = &a->coeff[1];
     L.values = values;
     L.upper = upper ? 1 : 0;
+    L.cta_cells = a->launch_cells;
+    L.stage = a->launch_stage;
     launch_matrix_atomic(L, st);
     if (upper) launch_mirror_lower(*a->sp, values, st);
     if (bc0) launch_set_diagonal(*a->sp, *bc0, diagonal, values, st);

@@ -164,6 +164,8 @@ struct fe_form_s {
   fe_context ctx = nullptr;
   int kind = 0, rank = 0;
   int precision = FE_PREC_FP64;
+  int launch_cells = 0;  // atomic scatter launch shape (fe_form_set_launch)
+  int launch_stage = 1;
   fe_mesh mesh = nullptr;
   fe_dofmap V0 = nullptr, V1 = nullptr;
   fe::Coefficient coeff[2];
@@ -350,6 +352,8 @@ struct MatLaunch {
   const Coefficient* c1;
   double* values;
   int upper = 0;  // reduce only into the upper triangle and the diagonal
+  int cta_cells = 0;  // cells per CTA of the P1 / P2 atomic kernels (0: 128)
+  int stage = 1;      // P2 atomic kernel: stage the byte maps in shared memory
 };
 void launch_zero(double* v, int64_t n, cudaStream_t s);
 // symmetric-pattern transpose map (built once per pattern); false if the

@@ -15,6 +15,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <type_traits>
 
 #include "fe_element_code.cuh"
 #include "fe_internal.h"
@@ -149,8 +150,9 @@ struct MatArgs {
 // ---------------------------------------------------------------------------
 // P1 stiffness, one thread per cell, FP64 atomics
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kBlock) k_mat_p1_atomic(const MatArgs a) {
-  const int64_t c = blockIdx.x * (int64_t)kBlock + threadIdx.x;
+template <int NT>
+__global__ void __launch_bounds__(NT) k_mat_p1_atomic(const MatArgs a) {
+  const int64_t c = blockIdx.x * (int64_t)NT + threadIdx.x;
   if (c >= a.num_cells) return;
   CellGeo g;
   cell_geometry(a.x, load_geom(a.geom, c), g);
@@ -196,17 +198,21 @@ __global__ void __launch_bounds__(kBlock) k_mat_p1_atomic(const MatArgs a) {
 // ---------------------------------------------------------------------------
 // P2 stiffness, one thread per cell, FP64 atomics
 // ---------------------------------------------------------------------------
-template <int COEF, typename T>
-__global__ void __launch_bounds__(kBlock) k_mat_p2_atomic(const MatArgs a) {
-  __shared__ __align__(16) uint8_t spos[kBlock * 100];
-  const int64_t c0 = blockIdx.x * (int64_t)kBlock;
+// NT cells per CTA; STAGE: the CTA's byte maps staged in shared memory with
+// 16-byte loads, else each thread reads its cell's bytes from global memory
+template <int COEF, typename T, int NT = kBlock, bool STAGE = true>
+__global__ void __launch_bounds__(NT) k_mat_p2_atomic(const MatArgs a) {
+  __shared__ __align__(16) uint8_t spos[STAGE ? NT * 100 : 16];
+  const int64_t c0 = blockIdx.x * (int64_t)NT;
   const int64_t left = a.num_cells - c0;
-  const int ncell = left < kBlock ? (int)left : kBlock;
-  stage_pos<100>(spos, a.pos, c0, ncell);
-  __syncthreads();
+  const int ncell = left < NT ? (int)left : NT;
+  if constexpr (STAGE) {
+    stage_pos<100>(spos, a.pos, c0, ncell);
+    __syncthreads();
+  }
   if ((int)threadIdx.x >= ncell) return;
   const int64_t c = c0 + threadIdx.x;
-  const uint8_t* p = spos + threadIdx.x * 100;
+  const uint8_t* p = STAGE ? spos + threadIdx.x * 100 : a.pos + c * 100;
 
   const int4 gv = load_geom(a.geom, c);
   CellGeo g;
@@ -1349,19 +1355,41 @@ void launch_matrix_atomic(const MatLaunch& L, cudaStream_t s) {
   a.upper = L.upper;
   const unsigned grid = grid_for(L.num_cells, kBlock);
   const bool f32 = L.precision == FE_PREC_FP32;
+  // tuned launch shape (fe_form_set_launch): cells per CTA and byte-map staging
+  const int nt = L.cta_cells ? L.cta_cells : kBlock;
+  const bool stage = L.stage != 0;
   switch (L.kind) {
     case FE_FORM_P1_STIFFNESS:
-      k_mat_p1_atomic<<<grid, kBlock, 0, s>>>(a);
+      if (nt == 32) k_mat_p1_atomic<32><<<grid_for(L.num_cells, 32), 32, 0, s>>>(a);
+      else if (nt == 64) k_mat_p1_atomic<64><<<grid_for(L.num_cells, 64), 64, 0, s>>>(a);
+      else k_mat_p1_atomic<kBlock><<<grid, kBlock, 0, s>>>(a);
       break;
-    case FE_FORM_P2_STIFFNESS:
+    case FE_FORM_P2_STIFFNESS: {
+      auto go = [&](auto coef, auto tv) {
+        constexpr int C = decltype(coef)::value;
+        using T = typename decltype(tv)::type;
+        if (nt == 32) {
+          if (stage) k_mat_p2_atomic<C, T, 32, true><<<grid_for(L.num_cells, 32), 32, 0, s>>>(a);
+          else k_mat_p2_atomic<C, T, 32, false><<<grid_for(L.num_cells, 32), 32, 0, s>>>(a);
+        } else if (nt == 64) {
+          if (stage) k_mat_p2_atomic<C, T, 64, true><<<grid_for(L.num_cells, 64), 64, 0, s>>>(a);
+          else k_mat_p2_atomic<C, T, 64, false><<<grid_for(L.num_cells, 64), 64, 0, s>>>(a);
+        } else {
+          if (stage) k_mat_p2_atomic<C, T, kBlock, true><<<grid, kBlock, 0, s>>>(a);
+          else k_mat_p2_atomic<C, T, kBlock, false><<<grid, kBlock, 0, s>>>(a);
+        }
+      };
+      using P1c = std::integral_constant<int, FE_COEFF_P1>;
+      using DGc = std::integral_constant<int, FE_COEFF_DG0>;
       if (a.c0.kind == FE_COEFF_P1) {
-        if (f32) k_mat_p2_atomic<FE_COEFF_P1, float><<<grid, kBlock, 0, s>>>(a);
-        else k_mat_p2_atomic<FE_COEFF_P1, double><<<grid, kBlock, 0, s>>>(a);
+        if (f32) go(P1c{}, std::common_type<float>{});
+        else go(P1c{}, std::common_type<double>{});
       } else {
-        if (f32) k_mat_p2_atomic<FE_COEFF_DG0, float><<<grid, kBlock, 0, s>>>(a);
-        else k_mat_p2_atomic<FE_COEFF_DG0, double><<<grid, kBlock, 0, s>>>(a);
+        if (f32) go(DGc{}, std::common_type<float>{});
+        else go(DGc{}, std::common_type<double>{});
       }
       break;
+    }
     case FE_FORM_VP2_ELASTICITY:
       if (f32) k_mat_vp2_atomic<float><<<grid, kBlock, 0, s>>>(a);
       else k_mat_vp2_atomic<double><<<grid, kBlock, 0, s>>>(a);

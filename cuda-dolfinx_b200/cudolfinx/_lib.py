@@ -72,6 +72,7 @@ _SIGS = {
     "fe_form_create": (i32, [vp, i32, vp, vp, vp, PP]),
     "fe_form_set_coefficient": (i32, [vp, i32, i32, vp, vp, i64, i32, vp]),
     "fe_form_set_precision": (i32, [vp, i32]),
+    "fe_form_set_launch": (i32, [vp, i32, i32]),
     "fe_form_set_facets": (i32, [vp, vp, i64]),
     "fe_form_set_interior_facets": (i32, [vp, vp, i64]),
     "fe_assemble_scalar": (i32, [vp, ctypes.POINTER(dbl), vp]),

@@ -25,14 +25,23 @@ from .la import CUDAMatrix
 # matrix variants worth timing per form kind (all parity-tested)
 CANDIDATES = {
     "P1_STIFFNESS": ("atomic", "block", "tile"),
-    "P2_STIFFNESS": ("atomic", "block"),
+    "P2_STIFFNESS": ("atomic", "block", "grouped"),
     "VP2_ELASTICITY": ("atomic", "atomic-full"),
+}
+# launch shapes of the atomic scatter timed per form kind: (cells per CTA,
+# byte maps staged in shared memory)
+LAUNCHES = {
+    "P1_STIFFNESS": ((128, 1), (64, 1), (32, 1)),
+    "P2_STIFFNESS": ((128, 1), (64, 1), (32, 1), (128, 0), (64, 0)),
 }
 
 
 class VariantTuner:
     """Chooses the fastest matrix variant per (form kind, precision, size
-    class); size classes are powers of two of the cell count."""
+    class) and, for the atomic scatter, its launch shape (cells per CTA and
+    shared-memory staging of the byte maps); size classes are powers of two of
+    the cell count.  ``choose`` returns the variant name and leaves the
+    chosen launch shape set on the form."""
 
     def __init__(self, reps: int = 3):
         self.reps = reps
@@ -49,12 +58,19 @@ class VariantTuner:
     def choose(self, a: CUDAForm, mat: CUDAMatrix, bc0, bc1) -> str:
         k = self.key(a)
         if k in self.cache:
-            return self.cache[k]
+            v, shape = self.cache[k]
+            _lib.check(_lib.lib.fe_form_set_launch(a.cuda_form, *shape), "fe_form_set_launch")
+            return v
         stream = torch.cuda.current_stream()
         sp = stream.cuda_stream
         best, best_ms, times = None, float("inf"), {}
+        trials = []
         for v in CANDIDATES.get(a._spec.kind, ("atomic",)):
+            shapes = LAUNCHES.get(a._spec.kind, ((0, 1),)) if v in ("atomic", "atomic-full") else ((0, 1),)
+            trials += [(v, shape) for shape in shapes]
+        for v, shape in trials:
             flags = _lib.ASM_ZERO | _lib.VARIANT_FLAGS[v]
+            _lib.check(_lib.lib.fe_form_set_launch(a.cuda_form, *shape), "fe_form_set_launch")
 
             def call():
                 _lib.check(_lib.lib.fe_assemble_matrix(a.cuda_form, mat.values.data_ptr(), bc0, bc1, 1.0, flags, sp),
@@ -73,12 +89,15 @@ class VariantTuner:
             e1.record(stream)
             e1.synchronize()
             ms = e0.elapsed_time(e1) / self.reps
-            times[v] = ms
+            times[(v,) + tuple(shape)] = ms
             if ms < best_ms:
-                best, best_ms = v, ms
+                best, best_ms = (v, tuple(shape)), ms
+        if best is None:
+            best = ("atomic", (0, 1))
+        _lib.check(_lib.lib.fe_form_set_launch(a.cuda_form, *best[1]), "fe_form_set_launch")
         self.cache[k] = best
         self.timings[k] = times
-        return best
+        return best[0]
 
 
 class AssemblyGraph:

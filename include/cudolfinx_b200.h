@@ -221,6 +221,14 @@ int fe_form_set_coefficient(fe_form f, int index, int coeff_kind, fe_dofmap cmap
                             const double* values, int64_t n, int values_on_device,
                             void* stream);
 int fe_form_set_precision(fe_form f, int precision);
+/* Launch shape of the atomic scatter for P1 / P2 stiffness (no counterpart in
+ * the reference, which takes max_threads_per_block / min_blocks_per_multiprocessor
+ * in CUDAForm::compile, python/cudolfinx/form.py:66-71): cells per CTA (32, 64
+ * or 128; 0 = the default 128) and, for P2, whether the CTA stages its cells'
+ * byte maps in shared memory (1, the default) or each thread reads its own (0).
+ * Small meshes fill more SMs with smaller CTAs; cudolfinx.VariantTuner picks
+ * the pair per size class. */
+int fe_form_set_launch(fe_form f, int cells_per_cta, int stage);
 /* Integration domain of an exterior-facet form (facet kinds and
  * FE_FORM_FACET_INTEGRAL): num_facets (cell, local
  * facet) pairs, int32[2*num_facets] host array; local facet f is the facet

@@ -308,3 +308,26 @@ def test_grouped_variant_on_permuted_cells_and_renumbered_dofs(precision):
     else:
         rel = np.linalg.norm(A.values.cpu().numpy() - ref) / np.linalg.norm(ref)
         assert 0.0 < rel < 2e-6, rel
+
+
+@pytest.mark.parametrize("kind", ["p1", "p2"])
+@pytest.mark.parametrize("shape", [(32, 1), (64, 1), (128, 1), (64, 0), (128, 0)])
+def test_atomic_launch_shapes(kind, shape):
+    # the tuner's launch shapes of the atomic scatter (cells per CTA, byte-map staging)
+    from cudolfinx import _lib
+
+    if kind == "p1" and shape[1] == 0:
+        pytest.skip("the P1 kernel reads its byte map directly in every shape")
+    P = fo.build_problem(kind, 5, seed=17)
+    S = fo.solve_system(P)
+    M = mirror_problem(P)
+    cx = M["cx"]
+    asm = cx.CUDAAssembler()
+    a = cx.form(M["a"])
+    _lib.check(_lib.lib.fe_form_set_launch(a.cuda_form, *shape), "fe_form_set_launch")
+    A = asm.assemble_matrix(a, bcs=asm.pack_bcs([M["bc"]]), variant="atomic-full")
+    A.assemble()
+    ok, worst = tolerance_check(A.values.cpu().numpy(), S["A"], S["A_bound"])
+    assert ok, worst
+    with pytest.raises(RuntimeError, match="cells per CTA"):
+        _lib.check(_lib.lib.fe_form_set_launch(a.cuda_form, 48, 1), "fe_form_set_launch")
