@@ -81,8 +81,9 @@ SERVE = dict(requests=120, rates=(50.0, 200.0, 1000.0), nmin=8, nmax=48, workers
                   "(k DG0 lognormal, f=1, g=x+y+z), 30% vector-P2 elasticity (lam, mu DG0 lognormal, body force "
                   "(0,0,-1), u=0); unit-cube meshes n^3 x 6 tets, n log-uniform")
 L2_BYTES = 126 * 1024 * 1024
-# kernels of one step besides the matrix call: zero b, vector, lifting, set_bc
-VECTOR_KERNELS = 4
+# kernels of one step besides the matrix call: zero b, then vector + lifting +
+# set_bc in one kernel (fe_assemble_rhs)
+VECTOR_KERNELS = 2
 
 
 def matrix_kernels(kind: str, variant: str, big: bool = False) -> int:
@@ -437,8 +438,6 @@ def run_gpu(args, rank, world, local_rank):
     stream = torch.cuda.current_stream()
     sp = stream.cuda_stream
     flags = _lib.ASM_ZERO | _lib.VARIANT_FLAGS[args.variant]
-    forms = (ctypes.c_void_p * 1)(a.cuda_form)
-    bcs1 = (ctypes.c_void_p * 1)(hbc)
     Lib = _lib.lib
     Ap, bp = A.values.data_ptr(), b.vector.data_ptr()
 
@@ -454,9 +453,8 @@ def run_gpu(args, rank, world, local_rank):
         _lib.check(Lib.fe_assemble_matrix(a.cuda_form, Ap, hbc, hbc, 1.0, flags, h), "matrix")
         if ev1 is not None:
             ev1.record(stream)
-        _lib.check(Lib.fe_assemble_vector(L.cuda_form, bp, _lib.ASM_ZERO, hv), "vector")
-        _lib.check(Lib.fe_apply_lifting(bp, 1, forms, bcs1, None, 1.0, hv), "lifting")
-        _lib.check(Lib.fe_set_bc(bp, nrows, hbc, None, 1.0, hv), "set_bc")
+        # b = L - A g on the BC columns, then g on the BC rows: one kernel
+        _lib.check(Lib.fe_assemble_rhs(L.cuda_form, a.cuda_form, hbc, bp, None, 1.0, _lib.ASM_ZERO, hv), "rhs")
 
     step()  # plan build (deterministic), lift-cell list
     torch.cuda.synchronize()
@@ -528,9 +526,7 @@ def run_gpu(args, rank, world, local_rank):
 
         def e2e_step():
             asm.assemble_matrix(a2, A2, bcs=dbc2)
-            asm.assemble_vector(L2, b2)
-            asm.apply_lifting(b2, [a2], [dbc2])
-            asm.set_bc(b2, dbc2, I2["V"])
+            asm.assemble_rhs(L2, a2, dbc2, vec=b2)
             b2.copy_to_host(bhost)
 
         for _ in range(max(1, args.warmup)):
@@ -1592,8 +1588,9 @@ def serve_request_bytes(kind, n, iterations):
 
 
 def serve_launches(iterations):
-    # matrix (zero, kernel, diagonal) + vector (zero, kernel, lifting, set_bc) + PCG (2 + 80 per 16 iterations)
-    return 3 + 4 + 2 + 80 * ((iterations + 16) // 16)
+    # matrix (zero, kernel, diagonal) + right-hand side (zero, fused vector/lifting/set_bc) + PCG (2 + 80 per 16
+    # iterations)
+    return 3 + 2 + 2 + 80 * ((iterations + 16) // 16)
 
 
 def run_gpu_serve(args, rank, world, local_rank):

@@ -43,6 +43,12 @@ struct DeviceScope {
 
 cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
+// Re-raise the status of a nested C-ABI call inside a guard (its message is
+// already the thread's last error).
+void rethrow_status(int status) {
+  if (status != FE_OK) throw Error(status, g_last_error);
+}
+
 std::string decode_device_error(unsigned w) {
   std::string s;
   if (w & DEV_ERR_PATTERN) s += " [cell coupling missing from the CSR pattern]";
@@ -828,11 +834,17 @@ int fe_bc_create(fe_context ctx, int64_t num_dofs, const uint8_t* markers, const
     DeviceScope d(ctx);
     FE_REQUIRE(out && num_dofs >= 0 && n_bc >= 0 && n_owned >= 0 && n_owned <= n_bc, "invalid argument");
     FE_REQUIRE(markers && g && (dofs || !n_bc), "null input array");
+    std::vector<uint8_t> listed((size_t)num_dofs, 0);
+    int64_t distinct = 0, marked = 0;
     for (int64_t q = 0; q < n_bc; ++q) {
       FE_REQUIRE(dofs[q] >= 0 && dofs[q] < num_dofs, "BC dof out of range at " + std::to_string(q));
       FE_REQUIRE(markers[dofs[q]], "BC dof " + std::to_string(dofs[q]) + " is not marked");
+      distinct += !listed[dofs[q]];
+      listed[dofs[q]] = 1;
     }
+    for (int64_t d = 0; d < num_dofs; ++d) marked += markers[d] != 0;
     auto bc = std::make_unique<fe_bc_s>();
+    bc->markers_are_dofs = distinct == n_bc && marked == n_bc;
     bc->ctx = ctx;
     bc->num_dofs = num_dofs;
     bc->n_bc = n_bc;
@@ -1183,6 +1195,71 @@ int fe_interpolate(fe_dofmap target, double* u1, fe_dofmap source, const double*
     FE_REQUIRE((u1 || !target->num_blocks) && (u0 || !source->num_blocks), "null coefficient array");
     DeviceScope d(target->ctx);
     interpolate(*target, u1, *source, u0, matrix, as_stream(stream));
+  });
+}
+
+int fe_assemble_rhs(fe_form Lf, fe_form a, fe_bc bc, double* b, const double* x0, double scale, unsigned flags,
+                    void* stream) {
+  return guard([&] {
+    FE_REQUIRE(Lf && a, "null form");
+    FE_REQUIRE(Lf->rank == 1 && a->rank == 2, "assemble_rhs takes a linear and a bilinear form");
+    FE_REQUIRE(Lf->ctx == a->ctx && (!bc || bc->ctx == a->ctx), "the forms and the BC belong to different contexts");
+    FE_REQUIRE(scalar_size(Lf->V0) == scalar_size(a->V0) && scalar_size(a->V0) == scalar_size(a->V1),
+               "assemble_rhs needs one space for the vector, the test and the trial space");
+    FE_REQUIRE(!bc || bc->num_dofs == scalar_size(a->V1), "bc size differs from the trial space size");
+    const int64_t n = scalar_size(Lf->V0);
+    FE_REQUIRE(b || n == 0, "null vector");
+    const bool fused = bc && bc->markers_are_dofs && !Lf->ffcx && !a->ffcx && Lf->mesh == a->mesh &&
+                       Lf->V0->dofs.p == a->V0->dofs.p && a->V0->dofs.p == a->V1->dofs.p &&
+                       rhs_fused_supported(Lf->kind, a->kind) && Lf->coeff[0].kind >= 0;
+    if (!fused) {
+      // the same result through the three calls
+      rethrow_status(fe_assemble_vector(Lf, b, flags & FE_ASM_ZERO, stream));
+      if (bc) {
+        const double* xs[1] = {x0};
+        rethrow_status(fe_apply_lifting(b, 1, &a, &bc, x0 ? xs : nullptr, scale, stream));
+        rethrow_status(fe_set_bc(b, n, bc, x0, scale, stream));
+      }
+      return;
+    }
+    const int need = (a->kind == FE_FORM_VP2_ELASTICITY) ? 2 : (a->kind == FE_FORM_P2_STIFFNESS ? 1 : 0);
+    for (int q = 0; q < need; ++q) FE_REQUIRE(a->coeff[q].kind >= 0, "coefficient not set");
+    DeviceScope d(a->ctx);
+    cudaStream_t st = as_stream(stream);
+    if (flags & FE_ASM_ZERO) launch_zero(b, n, st);
+    auto& cells = lift_cells(*bc, *a->V1, st);
+    VecLaunch V{};
+    V.kind = Lf->kind;
+    V.num_cells = Lf->mesh->num_cells;
+    V.x = Lf->mesh->x.p;
+    V.geom = Lf->mesh->geom.p;
+    V.dofs = Lf->V0->dofs.p;
+    V.k = Lf->V0->k;
+    V.bs = Lf->V0->bs;
+    V.f = &Lf->coeff[0];
+    V.b = b;
+    V.num_values = n;
+    LiftLaunch L{};
+    L.kind = a->kind;
+    L.precision = a->precision;
+    L.cells = cells.cells.p;
+    L.num_list = cells.count;
+    L.x = a->mesh->x.p;
+    L.geom = a->mesh->geom.p;
+    L.dofs0 = a->V0->dofs.p;
+    L.dofs1 = a->V1->dofs.p;
+    L.k0 = a->V0->k;
+    L.k1 = a->V1->k;
+    L.bs = a->V0->bs;
+    L.c0 = &a->coeff[0];
+    L.c1 = &a->coeff[1];
+    L.bc1 = bc->markers.p;
+    L.g = bc->g.p;
+    L.x0 = x0;
+    L.scale = scale;
+    L.b = b;
+    L.num_values = n;
+    launch_rhs_fused(V, L, bc->dofs.p, bc->n_bc, st);
   });
 }
 

@@ -138,6 +138,7 @@ struct fe_sparsity_s {
 struct fe_bc_s {
   fe_context ctx = nullptr;
   int64_t num_dofs = 0, n_bc = 0, n_owned = 0;
+  bool markers_are_dofs = false;  // the marked dofs are exactly the listed ones, each listed once
   fe::DevBuf<uint8_t> markers;   // [num_dofs]
   fe::DevBuf<int32_t> dofs;      // [n_bc], owned first
   fe::DevBuf<double> g;          // [num_dofs]
@@ -408,6 +409,13 @@ void launch_mark_cells(const int32_t* dofs, int64_t num_cells, int k, int bs, co
                        int32_t* out_cells, unsigned long long* out_count, cudaStream_t s);
 void launch_set_bc(double* b, int64_t num_values, const int32_t* dofs, int64_t n_bc, const double* g,
                    const double* x0, double scale, cudaStream_t s);
+// assemble_vector + apply_lifting + set_bc in one kernel for the pairs
+// (P1 load, P1 stiffness), (P2 load, P2 stiffness), (P3 load, P3 stiffness),
+// (vector-P2 load, elasticity); the lifting launch's bc1 markers are the rows
+// the scatters skip and bc_dofs the rows the kernel stores.
+bool rhs_fused_supported(int vec_kind, int mat_kind);
+void launch_rhs_fused(const VecLaunch& v, const LiftLaunch& l, const int32_t* bc_dofs, int64_t n_bc,
+                      cudaStream_t s);
 
 // same-map interpolation u1 = I u0 (fe_interp.cu); im is the host
 // [target.k][source.k] matrix; one owner cell per target dof

@@ -15,6 +15,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <type_traits>
 
 #include "fe_element_code.cuh"
@@ -851,15 +852,20 @@ struct VecArgs {
   CoefDev f;
   double* __restrict__ b;
   int64_t num_values;
+  const uint8_t* __restrict__ skip;  // rows set_bc overwrites in the same launch (fused RHS), else null
 };
 
 __device__ __forceinline__ void add_guarded(double* b, int64_t row, int64_t n, double v) {
   if (row >= 0 && row < n) atomicAdd(b + row, v);
 }
 
-__global__ void __launch_bounds__(kBlock) k_vec_p1(const VecArgs a) {
-  const int64_t c = blockIdx.x * (int64_t)kBlock + threadIdx.x;
-  if (c >= a.num_cells) return;
+// The vector and lifting scatters: rows marked in `skip` are left to the
+// set_bc part of the fused right-hand-side kernel, which stores them.
+__device__ __forceinline__ void add_guarded(double* b, int64_t row, int64_t n, const uint8_t* skip, double v) {
+  if (row >= 0 && row < n && !(skip && __ldg(skip + row))) atomicAdd(b + row, v);
+}
+
+__device__ __forceinline__ void vec_p1(const VecArgs& a, const int64_t c) {
   CellGeo g;
   cell_geometry(a.x, load_geom(a.geom, c), g);
   const int4 d = __ldg(reinterpret_cast<const int4*>(a.dofs) + c);
@@ -878,38 +884,47 @@ __global__ void __launch_bounds__(kBlock) k_vec_p1(const VecArgs a) {
   const double s = f[0] + f[1] + f[2] + f[3];
   const double w = g.adet * (1.0 / 120.0);
 #pragma unroll
-  for (int i = 0; i < 4; ++i) add_guarded(a.b, r[i], a.num_values, w * (f[i] + s));
+  for (int i = 0; i < 4; ++i) add_guarded(a.b, r[i], a.num_values, a.skip, w * (f[i] + s));
 }
 
-__global__ void __launch_bounds__(kBlock) k_vec_p2(const VecArgs a) {
+__global__ void __launch_bounds__(kBlock) k_vec_p1(const VecArgs a) {
   const int64_t c = blockIdx.x * (int64_t)kBlock + threadIdx.x;
-  if (c >= a.num_cells) return;
+  if (c < a.num_cells) vec_p1(a, c);
+}
+
+__device__ __forceinline__ void vec_p2(const VecArgs& a, const int64_t c) {
   CellGeo g;
   cell_geometry(a.x, load_geom(a.geom, c), g);
   const double s = coef_cell(a.f, c) * g.adet;
   const int32_t* d = a.dofs + c * 10;
 #pragma unroll
-  for (int i = 0; i < 10; ++i) add_guarded(a.b, __ldg(d + i), a.num_values, s * p2_basis_integral(i));
+  for (int i = 0; i < 10; ++i) add_guarded(a.b, __ldg(d + i), a.num_values, a.skip, s * p2_basis_integral(i));
+}
+
+__global__ void __launch_bounds__(kBlock) k_vec_p2(const VecArgs a) {
+  const int64_t c = blockIdx.x * (int64_t)kBlock + threadIdx.x;
+  if (c < a.num_cells) vec_p2(a, c);
 }
 
 // P3 load with a DG0 / constant f: |det J| f int_ref phi_i.  The edge basis
 // functions of the equispaced cubic element integrate to exactly zero, so only
 // the vertex and face rows receive a contribution.
-__global__ void __launch_bounds__(kBlock) k_vec_p3(const VecArgs a) {
-  const int64_t c = blockIdx.x * (int64_t)kBlock + threadIdx.x;
-  if (c >= a.num_cells) return;
+__device__ __forceinline__ void vec_p3(const VecArgs& a, const int64_t c) {
   CellGeo g;
   cell_geometry(a.x, load_geom(a.geom, c), g);
   const double s = coef_cell(a.f, c) * g.adet;
   const int32_t* d = a.dofs + c * 20;
 #pragma unroll
   for (int i = 0; i < 20; ++i)
-    if (i < 4 || i >= 16) add_guarded(a.b, __ldg(d + i), a.num_values, s * p3_basis_integral(i));
+    if (i < 4 || i >= 16) add_guarded(a.b, __ldg(d + i), a.num_values, a.skip, s * p3_basis_integral(i));
 }
 
-__global__ void __launch_bounds__(kBlock) k_vec_vp2(const VecArgs a) {
+__global__ void __launch_bounds__(kBlock) k_vec_p3(const VecArgs a) {
   const int64_t c = blockIdx.x * (int64_t)kBlock + threadIdx.x;
-  if (c >= a.num_cells) return;
+  if (c < a.num_cells) vec_p3(a, c);
+}
+
+__device__ __forceinline__ void vec_vp2(const VecArgs& a, const int64_t c) {
   CellGeo g;
   cell_geometry(a.x, load_geom(a.geom, c), g);
   double f[3];
@@ -921,8 +936,13 @@ __global__ void __launch_bounds__(kBlock) k_vec_vp2(const VecArgs a) {
     const int64_t R = __ldg(d + i);
     const double w = p2_basis_integral(i);
 #pragma unroll
-    for (int q = 0; q < 3; ++q) add_guarded(a.b, 3 * R + q, a.num_values, f[q] * w);
+    for (int q = 0; q < 3; ++q) add_guarded(a.b, 3 * R + q, a.num_values, a.skip, f[q] * w);
   }
+}
+
+__global__ void __launch_bounds__(kBlock) k_vec_vp2(const VecArgs a) {
+  const int64_t c = blockIdx.x * (int64_t)kBlock + threadIdx.x;
+  if (c < a.num_cells) vec_vp2(a, c);
 }
 
 // ---------------------------------------------------------------------------
@@ -943,11 +963,10 @@ struct LiftArgs {
   double scale;
   double* __restrict__ b;
   int64_t num_values;
+  const uint8_t* __restrict__ skip;  // as VecArgs::skip
 };
 
-__global__ void __launch_bounds__(kBlock) k_lift_p1(const LiftArgs a) {
-  const int64_t t = blockIdx.x * (int64_t)kBlock + threadIdx.x;
-  if (t >= a.num_list) return;
+__device__ __forceinline__ void lift_p1(const LiftArgs& a, const int64_t t) {
   const int64_t c = a.cells[t];
   CellGeo g;
   cell_geometry(a.x, load_geom(a.geom, c), g);
@@ -967,14 +986,17 @@ __global__ void __launch_bounds__(kBlock) k_lift_p1(const LiftArgs a) {
     double acc = 0.0;
 #pragma unroll
     for (int j = 0; j < 4; ++j) acc += s * (G[i][0] * G[j][0] + G[i][1] * G[j][1] + G[i][2] * G[j][2]) * dv[j];
-    add_guarded(a.b, r[i], a.num_values, -a.scale * acc);
+    add_guarded(a.b, r[i], a.num_values, a.skip, -a.scale * acc);
   }
 }
 
-template <int COEF, typename T>
-__global__ void __launch_bounds__(kBlock) k_lift_p2(const LiftArgs a) {
+__global__ void __launch_bounds__(kBlock) k_lift_p1(const LiftArgs a) {
   const int64_t t = blockIdx.x * (int64_t)kBlock + threadIdx.x;
-  if (t >= a.num_list) return;
+  if (t < a.num_list) lift_p1(a, t);
+}
+
+template <int COEF, typename T>
+__device__ __forceinline__ void lift_p2(const LiftArgs& a, const int64_t t) {
   const int64_t c = a.cells[t];
   CellGeo g;
   cell_geometry(a.x, load_geom(a.geom, c), g);
@@ -1011,13 +1033,17 @@ __global__ void __launch_bounds__(kBlock) k_lift_p2(const LiftArgs a) {
     p2_stiffness_const<T>(gq, emit);
   }
 #pragma unroll
-  for (int i = 0; i < 10; ++i) add_guarded(a.b, __ldg(d0 + i), a.num_values, -a.scale * be[i]);
+  for (int i = 0; i < 10; ++i) add_guarded(a.b, __ldg(d0 + i), a.num_values, a.skip, -a.scale * be[i]);
+}
+
+template <int COEF, typename T>
+__global__ void __launch_bounds__(kBlock) k_lift_p2(const LiftArgs a) {
+  const int64_t t = blockIdx.x * (int64_t)kBlock + threadIdx.x;
+  if (t < a.num_list) lift_p2<COEF, T>(a, t);
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kBlockP3) k_lift_p3(const LiftArgs a) {
-  const int64_t t = blockIdx.x * (int64_t)kBlockP3 + threadIdx.x;
-  if (t >= a.num_list) return;
+__device__ __forceinline__ void lift_p3(const LiftArgs& a, const int64_t t) {
   const int64_t c = a.cells[t];
   CellGeo g;
   cell_geometry(a.x, load_geom(a.geom, c), g);
@@ -1041,13 +1067,17 @@ __global__ void __launch_bounds__(kBlockP3) k_lift_p3(const LiftArgs a) {
     if (i != j) be[j] += v * dv[i];
   });
 #pragma unroll
-  for (int i = 0; i < 20; ++i) add_guarded(a.b, __ldg(d0 + i), a.num_values, -a.scale * be[i]);
+  for (int i = 0; i < 20; ++i) add_guarded(a.b, __ldg(d0 + i), a.num_values, a.skip, -a.scale * be[i]);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kBlockP3) k_lift_p3(const LiftArgs a) {
+  const int64_t t = blockIdx.x * (int64_t)kBlockP3 + threadIdx.x;
+  if (t < a.num_list) lift_p3<T>(a, t);
 }
 
 template <int K, int COEF>
-__global__ void __launch_bounds__(kBlock) k_lift_mass(const LiftArgs a) {
-  const int64_t t = blockIdx.x * (int64_t)kBlock + threadIdx.x;
-  if (t >= a.num_list) return;
+__device__ __forceinline__ void lift_mass(const LiftArgs& a, const int64_t t) {
   const int64_t c = a.cells[t];
   const double adet = cell_adet(a.x, load_geom(a.geom, c));
   double dv[K], be[K];
@@ -1064,13 +1094,17 @@ __global__ void __launch_bounds__(kBlock) k_lift_mass(const LiftArgs a) {
     if (i != j) be[j] += v * dv[i];
   });
 #pragma unroll
-  for (int i = 0; i < K; ++i) add_guarded(a.b, __ldg(d0 + i), a.num_values, -a.scale * be[i]);
+  for (int i = 0; i < K; ++i) add_guarded(a.b, __ldg(d0 + i), a.num_values, a.skip, -a.scale * be[i]);
+}
+
+template <int K, int COEF>
+__global__ void __launch_bounds__(kBlock) k_lift_mass(const LiftArgs a) {
+  const int64_t t = blockIdx.x * (int64_t)kBlock + threadIdx.x;
+  if (t < a.num_list) lift_mass<K, COEF>(a, t);
 }
 
 template <int COEF>
-__global__ void __launch_bounds__(kBlock) k_lift_vmass(const LiftArgs a) {
-  const int64_t t = blockIdx.x * (int64_t)kBlock + threadIdx.x;
-  if (t >= a.num_list) return;
+__device__ __forceinline__ void lift_vmass(const LiftArgs& a, const int64_t t) {
   const int64_t c = a.cells[t];
   const double adet = cell_adet(a.x, load_geom(a.geom, c));
   double dv[30], be[30];
@@ -1097,14 +1131,18 @@ __global__ void __launch_bounds__(kBlock) k_lift_vmass(const LiftArgs a) {
   for (int i = 0; i < 10; ++i) {
     const int64_t R = __ldg(d0 + i);
 #pragma unroll
-    for (int q = 0; q < 3; ++q) add_guarded(a.b, 3 * R + q, a.num_values, -a.scale * be[3 * i + q]);
+    for (int q = 0; q < 3; ++q) add_guarded(a.b, 3 * R + q, a.num_values, a.skip, -a.scale * be[3 * i + q]);
   }
 }
 
-template <typename T>
-__global__ void __launch_bounds__(kBlock) k_lift_vp2(const LiftArgs a) {
+template <int COEF>
+__global__ void __launch_bounds__(kBlock) k_lift_vmass(const LiftArgs a) {
   const int64_t t = blockIdx.x * (int64_t)kBlock + threadIdx.x;
-  if (t >= a.num_list) return;
+  if (t < a.num_list) lift_vmass<COEF>(a, t);
+}
+
+template <typename T>
+__device__ __forceinline__ void lift_vp2(const LiftArgs& a, const int64_t t) {
   const int64_t c = a.cells[t];
   CellGeo g;
   cell_geometry(a.x, load_geom(a.geom, c), g);
@@ -1130,8 +1168,14 @@ __global__ void __launch_bounds__(kBlock) k_lift_vp2(const LiftArgs a) {
   for (int i = 0; i < 10; ++i) {
     const int64_t R = __ldg(d0 + i);
 #pragma unroll
-    for (int q = 0; q < 3; ++q) add_guarded(a.b, 3 * R + q, a.num_values, -a.scale * be[3 * i + q]);
+    for (int q = 0; q < 3; ++q) add_guarded(a.b, 3 * R + q, a.num_values, a.skip, -a.scale * be[3 * i + q]);
   }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kBlock) k_lift_vp2(const LiftArgs a) {
+  const int64_t t = blockIdx.x * (int64_t)kBlock + threadIdx.x;
+  if (t < a.num_list) lift_vp2<T>(a, t);
 }
 
 // ---------------------------------------------------------------------------
@@ -1277,6 +1321,57 @@ __global__ void k_set_bc(double* __restrict__ b, int64_t num_values, const int32
 }
 
 unsigned grid_for(int64_t n, int block) { return (unsigned)((n + block - 1) / block); }
+
+// ---------------------------------------------------------------------------
+// Right-hand side in one launch: assemble_vector(L) + apply_lifting([a], [bc])
+// + set_bc(bc) (assemble.py:136-166, 287-339, 341-380, which the reference runs
+// as three kernels with a context synchronise after each).  The CTAs are split
+// in three ranges: lifting over the cells with a marked trial dof (the longest
+// threads, first), the element vectors of all cells, and the BC dofs.  The two
+// scatters skip the marked rows, and the third range stores
+// b[d] = scale (g[d] - x0[d]) there, so no row is both accumulated and stored
+// in the launch; the result equals the three calls in sequence (up to the
+// order of the FP64 additions into unmarked rows).
+// ---------------------------------------------------------------------------
+enum RhsPair { RHS_P1 = 1, RHS_P2 = 2, RHS_P3 = 3, RHS_VP2 = 4 };
+
+struct RhsArgs {
+  VecArgs v;
+  LiftArgs l;
+  const int32_t* __restrict__ bc_dofs;
+  int64_t n_bc;
+  int64_t lift_ctas, vec_ctas;
+};
+
+template <int PAIR, int COEF, typename T, int NT>
+__global__ void __launch_bounds__(NT) k_rhs_fused(const RhsArgs a) {
+  int64_t blk = blockIdx.x;
+  if (blk < a.lift_ctas) {
+    const int64_t t = blk * NT + threadIdx.x;
+    if (t >= a.l.num_list) return;
+    if constexpr (PAIR == RHS_P1) lift_p1(a.l, t);
+    else if constexpr (PAIR == RHS_P2) lift_p2<COEF, T>(a.l, t);
+    else if constexpr (PAIR == RHS_P3) lift_p3<T>(a.l, t);
+    else lift_vp2<T>(a.l, t);
+    return;
+  }
+  blk -= a.lift_ctas;
+  if (blk < a.vec_ctas) {
+    const int64_t c = blk * NT + threadIdx.x;
+    if (c >= a.v.num_cells) return;
+    if constexpr (PAIR == RHS_P1) vec_p1(a.v, c);
+    else if constexpr (PAIR == RHS_P2) vec_p2(a.v, c);
+    else if constexpr (PAIR == RHS_P3) vec_p3(a.v, c);
+    else vec_vp2(a.v, c);
+    return;
+  }
+  blk -= a.vec_ctas;
+  const int64_t q = blk * NT + threadIdx.x;
+  if (q >= a.n_bc) return;
+  const int32_t d = __ldg(a.bc_dofs + q);
+  if (d < 0 || d >= a.v.num_values) return;
+  a.v.b[d] = a.l.scale * (__ldg(a.l.g + d) - (a.l.x0 ? __ldg(a.l.x0 + d) : 0.0));
+}
 
 
 }  // namespace
@@ -1533,8 +1628,8 @@ void launch_set_diagonal(const fe_sparsity_s& sp, const fe_bc_s& bc, double diag
   FE_CUDA(cudaGetLastError());
 }
 
-void launch_vector(const VecLaunch& L, cudaStream_t s) {
-  if (L.num_cells == 0) return;
+namespace {
+VecArgs vec_args(const VecLaunch& L) {
   VecArgs a{};
   a.num_cells = L.num_cells;
   a.x = L.x;
@@ -1543,6 +1638,32 @@ void launch_vector(const VecLaunch& L, cudaStream_t s) {
   a.f = to_dev(L.f);
   a.b = L.b;
   a.num_values = L.num_values;
+  return a;
+}
+
+LiftArgs lift_args(const LiftLaunch& L) {
+  LiftArgs a{};
+  a.cells = L.cells;
+  a.num_list = L.num_list;
+  a.x = L.x;
+  a.geom = L.geom;
+  a.dofs0 = L.dofs0;
+  a.dofs1 = L.dofs1;
+  a.c0 = to_dev(L.c0);
+  a.c1 = to_dev(L.c1);
+  a.bc1 = L.bc1;
+  a.g = L.g;
+  a.x0 = L.x0;
+  a.scale = L.scale;
+  a.b = L.b;
+  a.num_values = L.num_values;
+  return a;
+}
+}  // namespace
+
+void launch_vector(const VecLaunch& L, cudaStream_t s) {
+  if (L.num_cells == 0) return;
+  const VecArgs a = vec_args(L);
   const unsigned grid = grid_for(L.num_cells, kBlock);
   switch (L.kind) {
     case FE_FORM_P1_LOAD:
@@ -1565,21 +1686,7 @@ void launch_vector(const VecLaunch& L, cudaStream_t s) {
 
 void launch_lifting(const LiftLaunch& L, cudaStream_t s) {
   if (L.num_list == 0) return;
-  LiftArgs a{};
-  a.cells = L.cells;
-  a.num_list = L.num_list;
-  a.x = L.x;
-  a.geom = L.geom;
-  a.dofs0 = L.dofs0;
-  a.dofs1 = L.dofs1;
-  a.c0 = to_dev(L.c0);
-  a.c1 = to_dev(L.c1);
-  a.bc1 = L.bc1;
-  a.g = L.g;
-  a.x0 = L.x0;
-  a.scale = L.scale;
-  a.b = L.b;
-  a.num_values = L.num_values;
+  const LiftArgs a = lift_args(L);
   const unsigned grid = grid_for(L.num_list, kBlock);
   const bool f32 = L.precision == FE_PREC_FP32;
   switch (L.kind) {
@@ -1619,6 +1726,58 @@ void launch_lifting(const LiftLaunch& L, cudaStream_t s) {
     }
     default:
       FE_FAIL(FE_ERR_ARG, "lifting needs a bilinear form, got kind " + std::to_string(L.kind));
+  }
+  FE_CUDA(cudaGetLastError());
+}
+
+bool rhs_fused_supported(int vec_kind, int mat_kind) {
+  return (vec_kind == FE_FORM_P1_LOAD && mat_kind == FE_FORM_P1_STIFFNESS) ||
+         (vec_kind == FE_FORM_P2_LOAD && mat_kind == FE_FORM_P2_STIFFNESS) ||
+         (vec_kind == FE_FORM_P3_LOAD && mat_kind == FE_FORM_P3_STIFFNESS) ||
+         (vec_kind == FE_FORM_VP2_LOAD && mat_kind == FE_FORM_VP2_ELASTICITY);
+}
+
+void launch_rhs_fused(const VecLaunch& V, const LiftLaunch& Lf, const int32_t* bc_dofs, int64_t n_bc,
+                      cudaStream_t s) {
+  FE_REQUIRE(rhs_fused_supported(V.kind, Lf.kind), "no fused right-hand side for this pair of form kinds");
+  RhsArgs a{};
+  a.v = vec_args(V);
+  a.l = lift_args(Lf);
+  a.v.skip = a.l.skip = Lf.bc1;  // the BC's markers: exactly its dofs (checked when the BC is created)
+  a.bc_dofs = bc_dofs;
+  a.n_bc = n_bc;
+  const int pair = V.kind == FE_FORM_P1_LOAD ? RHS_P1
+                   : V.kind == FE_FORM_P2_LOAD ? RHS_P2
+                   : V.kind == FE_FORM_P3_LOAD ? RHS_P3
+                                               : RHS_VP2;
+  const int nt = pair == RHS_P3 ? kBlockP3 : kBlock;
+  a.lift_ctas = (Lf.num_list + nt - 1) / nt;
+  a.vec_ctas = (V.num_cells + nt - 1) / nt;
+  const int64_t total = a.lift_ctas + a.vec_ctas + (n_bc + nt - 1) / nt;
+  if (total == 0) return;
+  FE_REQUIRE(total < (int64_t)INT_MAX, "right-hand side too large for one launch");
+  const unsigned grid = (unsigned)total;
+  const bool f32 = Lf.precision == FE_PREC_FP32;
+  switch (pair) {
+    case RHS_P1:
+      k_rhs_fused<RHS_P1, 0, double, kBlock><<<grid, kBlock, 0, s>>>(a);
+      break;
+    case RHS_P2:
+      if (a.l.c0.kind == FE_COEFF_P1) {
+        if (f32) k_rhs_fused<RHS_P2, FE_COEFF_P1, float, kBlock><<<grid, kBlock, 0, s>>>(a);
+        else k_rhs_fused<RHS_P2, FE_COEFF_P1, double, kBlock><<<grid, kBlock, 0, s>>>(a);
+      } else {
+        if (f32) k_rhs_fused<RHS_P2, FE_COEFF_DG0, float, kBlock><<<grid, kBlock, 0, s>>>(a);
+        else k_rhs_fused<RHS_P2, FE_COEFF_DG0, double, kBlock><<<grid, kBlock, 0, s>>>(a);
+      }
+      break;
+    case RHS_P3:
+      if (f32) k_rhs_fused<RHS_P3, 0, float, kBlockP3><<<grid, kBlockP3, 0, s>>>(a);
+      else k_rhs_fused<RHS_P3, 0, double, kBlockP3><<<grid, kBlockP3, 0, s>>>(a);
+      break;
+    default:
+      if (f32) k_rhs_fused<RHS_VP2, 0, float, kBlock><<<grid, kBlock, 0, s>>>(a);
+      else k_rhs_fused<RHS_VP2, 0, double, kBlock><<<grid, kBlock, 0, s>>>(a);
   }
   FE_CUDA(cudaGetLastError());
 }

@@ -96,6 +96,7 @@ _SIGS = {
     "fe_assemble_vector": (i32, [vp, vp, u32, vp]),
     "fe_apply_lifting": (i32, [vp, i32, vp, vp, vp, dbl, vp]),
     "fe_set_bc": (i32, [vp, i64, vp, vp, dbl, vp]),
+    "fe_assemble_rhs": (i32, [vp, vp, vp, vp, vp, dbl, u32, vp]),
     "fe_pcg_solve": (i32, [vp, vp, vp, vp, dbl, i32, ctypes.POINTER(i32), ctypes.POINTER(dbl), vp]),
     "fe_pcg_solve_noalloc": (i32, [vp, vp, vp, vp, dbl, i32, ctypes.POINTER(i32), ctypes.POINTER(dbl), vp]),
     "fe_pcg_solve_mixed": (i32, [vp, vp, vp, vp, dbl, dbl, i32, i32, ctypes.POINTER(i32), ctypes.POINTER(i32),

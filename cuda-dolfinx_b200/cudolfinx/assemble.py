@@ -352,6 +352,38 @@ class CUDAAssembler:
             f._mark_used()
         b._keep = keep
 
+    def assemble_rhs(self, L: CUDAForm, a: CUDAForm, bcs, vec: typing.Optional[CUDAVector] = None,
+                     x0: typing.Optional[CUDAVector] = None, scale: float = 1.0, zero: bool = True) -> CUDAVector:
+        """The right-hand side of A x = b in one call: ``assemble_vector(L)``,
+        ``apply_lifting(b, [a], [bcs], [x0], scale)`` and ``set_bc(b, bcs, V,
+        x0, scale)`` with V the trial space of `a`.  One kernel for the
+        built-in cell forms on one space (fe_assemble_rhs), the three calls
+        otherwise; the result is the same."""
+        if not isinstance(L, CUDAForm) or not isinstance(a, CUDAForm):
+            raise TypeError("Expected CUDAForm arguments")
+        hl, ha = L._integral_handles(), a._integral_handles()
+        if len(hl) != 1 or len(ha) != 1 or L.part == "diagonal":
+            vec = self.assemble_vector(L, vec, zero=zero)
+            self.apply_lifting(vec, [a], [bcs], None if x0 is None else [x0], scale)
+            self.set_bc(vec, bcs, a.function_spaces[1], x0, scale, restriction=a.restriction(1))
+            return vec
+        if vec is None:
+            vec = self.create_vector(L)
+        L.to_device()
+        a.to_device()
+        self.pack_coefficients(L, None)
+        self.pack_coefficients(a, None)
+        col = self._bc_collection(bcs)
+        d = col._get_cpp_bcs(a.function_spaces[1], a.restriction(1))
+        vec._before_write()
+        _lib.check(_lib.lib.fe_assemble_rhs(hl[0], ha[0], d.handle if d else None, vec.vector.data_ptr(),
+                                            x0.vector.data_ptr() if x0 is not None else None, float(scale),
+                                            _lib.ASM_ZERO if zero else 0, self._ctx.stream()), "fe_assemble_rhs")
+        L._mark_used()
+        a._mark_used()
+        vec._keep_bc = col
+        return vec
+
     def set_bc(self, b: CUDAVector, bcs, V: FunctionSpace, x0: typing.Optional[CUDAVector] = None,
                scale: float = 1.0, restriction: typing.Optional[np.ndarray] = None):
         """b[bc dofs] = scale * (g - x0) on the BCs of V (in the numbering of

@@ -280,9 +280,7 @@ def _execute(asm, slot: _Slot, req: Request, variant: str = "auto", solver: str 
     for dev, host in zip(slot.coef, req.coef):
         dev.copy_(torch.from_numpy(np.ascontiguousarray(host, dtype=np.float64)), non_blocking=True)
     asm.assemble_matrix(slot.a, slot.A, bcs=slot.bcs, variant=variant)
-    asm.assemble_vector(slot.L, slot.b)
-    asm.apply_lifting(slot.b, [slot.a], [slot.bcs])
-    asm.set_bc(slot.b, slot.bcs, slot.V)
+    asm.assemble_rhs(slot.L, slot.a, slot.bcs, vec=slot.b)
     slot.x.vector.zero_()
     x, its, res = asm.solve(slot.A, slot.b, slot.x, rtol=req.rtol, raise_on_failure=False, precision=solver,
                             block_size=slot.V.bs)

@@ -159,6 +159,62 @@ def test_lifting_with_x0_and_scale():
     assert ok, worst
 
 
+@pytest.mark.parametrize("kind,n", [("p1", 6), ("p1k", 5), ("p2", 4), ("vp2", 3), ("p3", 3)])
+def test_fused_rhs_matches_the_three_calls(kind, n):
+    # fe_assemble_rhs (vector + lifting + set_bc in one kernel) against the
+    # oracle under its bound, and against the three calls: BC rows equal
+    import torch
+
+    P = fo.build_problem(kind, n, seed=11)
+    M = mirror_problem(P)
+    cx = M["cx"]
+    asm = cx.CUDAAssembler()
+    a, L = cx.form(M["a"]), cx.form(M["L"])
+    bcs = asm.pack_bcs([M["bc"]])
+    bs = P["bs"]
+    nscal = P["ndof"] * bs
+    x0h = np.random.default_rng(1).standard_normal(nscal)
+    x0 = asm.create_vector(L)
+    x0.vector.copy_(torch.from_numpy(x0h))
+    fused = asm.assemble_rhs(L, a, bcs, x0=x0, scale=-0.7)
+    b3 = asm.assemble_vector(L)
+    asm.apply_lifting(b3, [a], [bcs], x0=[x0], scale=-0.7)
+    asm.set_bc(b3, bcs, M["V"], x0=x0, scale=-0.7)
+    markers = np.zeros(nscal, np.uint8)
+    markers[P["bc_dofs"]] = 1
+    be, Ae = fo.element_vectors(P), fo.element_matrices(P)
+    dofs = P["dofs"]
+    ref = fo.assemble_vector(be, dofs, nscal, bs)
+    ref = fo.apply_lifting(ref, Ae, dofs, dofs, markers, P["g"], x0h, -0.7, bs, bs)
+    ref = fo.set_bc(ref, P["bc_dofs"], P["g"], x0h, -0.7)
+    bound = fo.vector_bound(be, dofs, nscal, bs) + fo.lifting_bound(nscal, Ae, dofs, dofs, markers, P["g"], x0h,
+                                                                    -0.7, bs, bs)
+    bound[P["bc_dofs"]] = 0.0
+    out, out3 = fused.to_host(), b3.to_host()
+    ok, worst = tolerance_check(out, ref, bound)
+    assert ok, worst
+    assert np.array_equal(out[P["bc_dofs"]], out3[P["bc_dofs"]])
+    ok, worst = tolerance_check(out, out3, 2 * bound)
+    assert ok, worst
+    # re-assembly into the same vector (zero=True) gives the same values again
+    asm.assemble_rhs(L, a, bcs, vec=fused, x0=x0, scale=-0.7)
+    ok, worst = tolerance_check(fused.to_host(), ref, bound)
+    assert ok, worst
+
+
+def test_fused_rhs_without_bcs_is_the_vector():
+    P = fo.build_problem("p2", 3, seed=12)
+    M = mirror_problem(P)
+    cx = M["cx"]
+    asm = cx.CUDAAssembler()
+    a, L = cx.form(M["a"]), cx.form(M["L"])
+    out = asm.assemble_rhs(L, a, []).to_host()
+    be = fo.element_vectors(P)
+    ref = fo.assemble_vector(be, P["dofs"], P["ndof"])
+    ok, worst = tolerance_check(out, ref, fo.vector_bound(be, P["dofs"], P["ndof"]))
+    assert ok, worst
+
+
 def test_bc_update_changes_values_not_pattern():
     P = fo.build_problem("p2", 3, seed=5)
     M = mirror_problem(P)

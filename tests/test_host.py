@@ -256,3 +256,11 @@ def test_boundary_dofs_bcs_and_elasticity_specs_without_gpu():
     assert fem.elasticity(Vv, 1.0, 2.0).kind == "VP2_ELASTICITY"
     with pytest.raises(ValueError):
         fem.elasticity(V, 1.0, 2.0)
+
+
+def test_fused_rhs_validates_its_arguments_on_the_host():
+    ensure_library()
+    from cudolfinx import _lib
+
+    st = _lib.lib.fe_assemble_rhs(None, None, None, None, None, 1.0, 0, None)
+    assert st != 0 and "null form" in _lib.last_error()
