@@ -353,12 +353,17 @@ class FFCxForm:
     spaces ([] functional, [V] linear, [V, U] bilinear: test, trial), the
     coefficients in FFCx's order (Functions; coefficient q has
     dofs_per_cell * bs values per cell) and the constants in the form's order
-    (each a number or array, packed flat as DOLFINx pack_constants does)."""
+    (each a number or array, packed flat as DOLFINx pack_constants does).
+    ``coefficient_sizes``, when given, are the values per cell the compiled
+    form expects of each coefficient (the dimensions of the coefficient
+    elements FFCx compiled it for); a coefficient whose space gives another
+    number is rejected when the CUDA form is created."""
     integrals: list
     spaces: list
     coefficients: list = field(default_factory=list)
     constants: list = field(default_factory=list)
     domain: Optional["Mesh"] = None
+    coefficient_sizes: Optional[list] = None
 
     @property
     def rank(self) -> int:

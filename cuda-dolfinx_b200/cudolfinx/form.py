@@ -386,8 +386,16 @@ class FFCxCUDAForm(CUDAForm):
 
         self._destroy_handles()
         form = self._spec
-        sizes = (ctypes.c_int * max(1, len(form.coefficients)))(
-            *[c.function_space.dofs_per_cell * c.function_space.bs for c in form.coefficients])
+        given = [c.function_space.dofs_per_cell * c.function_space.bs for c in form.coefficients]
+        if form.coefficient_sizes is not None:
+            if len(form.coefficient_sizes) != len(given):
+                raise RuntimeError(f"the form has {len(form.coefficient_sizes)} coefficient(s), "
+                                   f"{len(given)} given")
+            for q, (want, got) in enumerate(zip(form.coefficient_sizes, given)):
+                if int(want) != got:
+                    raise RuntimeError(f"coefficient {q} has {int(want)} values per cell in the compiled form; "
+                                       f"its function space gives {got}")
+        sizes = (ctypes.c_int * max(1, len(given)))(*given)
         test = self._dofmaps[0].handle if form.rank >= 1 else None
         trial = self._dofmaps[1].handle if form.rank == 2 else None
         consts = form.packed_constants()

@@ -312,7 +312,8 @@ def test_compile_errors_cache_and_argument_checks(tmp_path):
     k = fem.Function(W, np.ones(mesh.num_cells))
     # the coefficient's element must have the declared number of values per cell
     with pytest.raises(RuntimeError, match="values per cell"):
-        cx.form(fem.FFCxForm([_integral(B)], [V, V], [fem.Function(V, np.ones(V.num_dofs))]))
+        cx.form(fem.FFCxForm([_integral(B)], [V, V], [fem.Function(V, np.ones(V.num_dofs))],
+                             coefficient_sizes=B["coefficient_sizes"]))
     # on-disk cache: the second form loads the cubin written by the first
     a1 = cx.form(fem.FFCxForm([_integral(B)], [V, V], [k]), cachedir=str(tmp_path))
     files = sorted(p.name for p in tmp_path.iterdir())
