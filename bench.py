@@ -68,8 +68,9 @@ BATCH = dict(n=48, instances=256, cpu_sample=4,
              desc="256 instances of P1 Poisson on one 48^3 x 6 = 663,552-tet mesh, DG0 k log-uniform "
                   "[1e-2,1e2] per cell and instance, one shared pattern, homogeneous Dirichlet; FP32 element "
                   "tensors, FP64 accumulation")
-# kernels of one batched call with <= 448 instances: pack, element tensors, record fill, gather
-BATCH_KERNELS = 4
+# kernels of one batched call with <= 384 instances: one cooperative persistent kernel (coefficient
+# pack, grid barrier, gather); the unit element tensors and slot records are built once per mesh
+BATCH_KERNELS = 1
 # many independent meshes in one captured graph
 MULTI = dict(count=64, nmin=8, nmax=64, cpu_every=8,
              desc="64 unit-cube tet meshes, n^3 x 6 cells with n ~ U{8..64} (seeded), P1 (k=1) and P2 (k P1 "
@@ -81,9 +82,10 @@ SERVE = dict(requests=120, rates=(50.0, 200.0, 1000.0), nmin=8, nmax=48, workers
                   "(k DG0 lognormal, f=1, g=x+y+z), 30% vector-P2 elasticity (lam, mu DG0 lognormal, body force "
                   "(0,0,-1), u=0); unit-cube meshes n^3 x 6 tets, n log-uniform")
 L2_BYTES = 126 * 1024 * 1024
-# kernels of one step besides the matrix call: zero b, then vector + lifting +
-# set_bc in one kernel (fe_assemble_rhs)
-VECTOR_KERNELS = 2
+# kernels of one step besides the matrix call: zero b, the lifting, then the
+# element vectors + set_bc in one kernel (fe_assemble_rhs); 4 with the three
+# separate calls (--rhs calls)
+VECTOR_KERNELS = 3
 
 
 def matrix_kernels(kind: str, variant: str, big: bool = False) -> int:
@@ -441,7 +443,10 @@ def run_gpu(args, rank, world, local_rank):
     Lib = _lib.lib
     Ap, bp = A.values.data_ptr(), b.vector.data_ptr()
 
-    def step(ev0=None, ev1=None, st=None, st_vec=None):
+    lift_forms = (ctypes.c_void_p * 1)(a.cuda_form)
+    lift_bcs = (ctypes.c_void_p * 1)(hbc)
+
+    def step(ev0=None, ev1=None, st=None, st_vec=None, ev2=None):
         # the matrix call owns its zeroing: a zero pass before the atomic
         # scatter, none for the gather variants (they write every value once);
         # b does not depend on A, so a captured step runs the vector calls on a
@@ -453,8 +458,15 @@ def run_gpu(args, rank, world, local_rank):
         _lib.check(Lib.fe_assemble_matrix(a.cuda_form, Ap, hbc, hbc, 1.0, flags, h), "matrix")
         if ev1 is not None:
             ev1.record(stream)
-        # b = L - A g on the BC columns, then g on the BC rows: one kernel
-        _lib.check(Lib.fe_assemble_rhs(L.cuda_form, a.cuda_form, hbc, bp, None, 1.0, _lib.ASM_ZERO, hv), "rhs")
+        # b = L - A g on the BC columns, then g on the BC rows
+        if args.rhs == "calls":
+            _lib.check(Lib.fe_assemble_vector(L.cuda_form, bp, _lib.ASM_ZERO, hv), "vector")
+            _lib.check(Lib.fe_apply_lifting(bp, 1, lift_forms, lift_bcs, None, 1.0, hv), "lifting")
+            _lib.check(Lib.fe_set_bc(bp, A.sparsity.num_rows, hbc, None, 1.0, hv), "set_bc")
+        else:
+            _lib.check(Lib.fe_assemble_rhs(L.cuda_form, a.cuda_form, hbc, bp, None, 1.0, _lib.ASM_ZERO, hv), "rhs")
+        if ev2 is not None:
+            ev2.record(stream)
 
     step()  # plan build (deterministic), lift-cell list
     torch.cuda.synchronize()
@@ -470,12 +482,14 @@ def run_gpu(args, rank, world, local_rank):
     time.sleep(0.3)
     e_start = torch.cuda.Event(enable_timing=True)
     e_end = torch.cuda.Event(enable_timing=True)
-    mats = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    # matrix-call time (roofline basis): eager steps with events around the call
+    mats = [tuple(torch.cuda.Event(enable_timing=True) for _ in range(3)) for _ in range(args.steps)]
+    # matrix-call time (roofline basis): eager steps with events around the
+    # call; the right-hand side follows it on the same stream
     for k in range(args.steps):
-        step(*mats[k])
+        step(mats[k][0], mats[k][1], ev2=mats[k][2])
     torch.cuda.synchronize()
-    mat_ms = statistics.mean(m0.elapsed_time(m1) for m0, m1 in mats)
+    mat_ms = statistics.mean(m0.elapsed_time(m1) for m0, m1, _ in mats)
+    rhs_ms = statistics.mean(m1.elapsed_time(m2) for _, m1, m2 in mats)
     # whole steps: the step's engine calls captured once in a CUDA graph and
     # replayed (every plan and cache exists after the warm-up, so the calls
     # are pure kernel launches); eager steps if the capture is refused
@@ -507,7 +521,7 @@ def run_gpu(args, rank, world, local_rank):
     torch.cuda.synchronize()
     total_ms = e_start.elapsed_time(e_end)
     clk = clocks.stop()
-    total_ms, mat_ms = reduce_over_ranks([total_ms, mat_ms])
+    total_ms, mat_ms, rhs_ms = reduce_over_ranks([total_ms, mat_ms, rhs_ms])
     ms_per_step = total_ms / args.steps
     cx.get_cuda_context().synchronize()
 
@@ -590,7 +604,9 @@ def run_gpu(args, rank, world, local_rank):
                      "kernel_ms": mat_ms, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"
                      if "hbm_gbs" in peaks else "fallback 6650 GB/s"},
         "matrix_nnz_per_s": nnz / (mat_ms / 1e3),
-        "gpu_launches": (matrix_kernels(W["kind"], args.variant, len(I["cells"]) >= (1 << 20)) + VECTOR_KERNELS)
+        "rhs_ms": rhs_ms,
+        "gpu_launches": (matrix_kernels(W["kind"], args.variant, len(I["cells"]) >= (1 << 20))
+                         + VECTOR_KERNELS + (args.rhs == "calls"))
         * args.steps,
         "clocks": clk,
         "setup_s": setup_s,
@@ -794,11 +810,12 @@ def run_gpu_batch(args, rank, world, local_rank):
         "data": "synthetic (seeded mesh; coefficients from a seeded device generator)",
         "config": {"workload": BATCH["desc"] if S == BATCH["instances"] else
                    BATCH["desc"].replace("256 instances", f"{S} instances"), "instances": S, "cells": C, "dofs": nrows, "nnz": nnz,
-                   "step": "fe_assemble_matrix_batch: pack coefficients + unit element tensors + record fill + "
-                           "persistent gather into %d CSR value arrays" % S,
+                   "step": "fe_assemble_matrix_batch: one persistent launch (pack coefficients, grid barrier, "
+                           "gather) into %d CSR value arrays; unit element tensors and slot records built once "
+                           "per mesh, before the timed steps" % S,
                    "l2": "inputs larger than L2 (values %.2f GB per step)" % (8 * S * nnz / 1e9),
                    "parallelism": f"replicas x{world}"},
-        "roofline": {"bound": "hbm", "kernel": "batched assembly call (4 launches)", "achieved": achieved,
+        "roofline": {"bound": "hbm", "kernel": "batched assembly call (one persistent launch)", "achieved": achieved,
                      "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": load_traffic("batch"),
                      "algorithmic_bytes": alg, "kernel_ms": call_ms,
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if "hbm_gbs" in peaks
@@ -1606,9 +1623,9 @@ def serve_working_set(kind, n, solver="fp64"):
 
 
 def serve_launches(iterations):
-    # matrix (zero, kernel, diagonal) + right-hand side (zero, fused vector/lifting/set_bc) + PCG (2 + 80 per 16
+    # matrix (zero, kernel, diagonal) + right-hand side (zero, lifting, vector with set_bc) + PCG (2 + 80 per 16
     # iterations)
-    return 3 + 2 + 2 + 80 * ((iterations + 16) // 16)
+    return 3 + 3 + 2 + 80 * ((iterations + 16) // 16)
 
 
 def run_gpu_serve(args, rank, world, local_rank):
@@ -1866,7 +1883,7 @@ def main():
     ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batch", "multimesh", "serve", "blocksys", "interp", "dg"],
                     default="p2")
     ap.add_argument("--variant", choices=["auto", "tile", "atomic", "atomic-full", "sorted-slot", "deterministic",
-                                          "row-gather", "block", "grouped"], default="auto")
+                                          "row-gather", "block", "grouped", "coalesced"], default="auto")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--serve-requests", type=int, default=0, help="serve workload: requests per rate")
     ap.add_argument("--serve-rates", default="", help="serve workload: comma-separated arrival rates (req/s)")
@@ -1876,6 +1893,9 @@ def main():
                     help="batch workload: number of instances (default 256; smaller for profiling)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-graph", action="store_true", help="time eager steps instead of replaying a CUDA graph")
+    ap.add_argument("--rhs", choices=["fused", "calls"], default="fused",
+                    help="right-hand side of the step: fe_assemble_rhs (default) or the three calls "
+                         "(assemble_vector, apply_lifting, set_bc)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-parity", action="store_true", help="skip the full-size parity check against the oracle")
     ap.add_argument("--no-precision", action="store_true", help="skip the FP32-vs-FP64 precision report")

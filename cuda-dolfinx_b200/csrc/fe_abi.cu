@@ -931,6 +931,8 @@ int fe_assemble_matrix(fe_form a, double* values, fe_bc bc0, fe_bc bc1, double d
       assemble_matrix_gather(*a, values, bc0, bc1, diagonal, zero, st);
       return;
     }
+    if (flags & FE_ASM_COALESCED)
+      FE_REQUIRE(a->kind == FE_FORM_P2_STIFFNESS, "the coalesced variant supports P2 stiffness only");
     if (flags & FE_ASM_GROUPED) {
       FE_REQUIRE(grouped_supported(*a), "the grouped variant supports P2 stiffness on an unrestricted pattern");
       if (assemble_matrix_grouped(*a, values, bc0, bc1, zero, st)) {
@@ -1006,6 +1008,7 @@ int fe_assemble_matrix(fe_form a, double* values, fe_bc bc0, fe_bc bc1, double d
     L.upper = upper ? 1 : 0;
     L.cta_cells = a->launch_cells;
     L.stage = a->launch_stage;
+    L.coalesced = (flags & FE_ASM_COALESCED) ? 1 : 0;
     launch_matrix_atomic(L, st);
     if (upper) launch_mirror_lower(*a->sp, values, st);
     if (bc0) launch_set_diagonal(*a->sp, *bc0, diagonal, values, st);

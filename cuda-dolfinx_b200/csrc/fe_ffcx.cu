@@ -60,6 +60,7 @@ struct FfcxLibrary {
   int device = 0;
   cudaLibrary_t lib = nullptr;
   cudaKernel_t mat = nullptr, vec = nullptr, lift = nullptr, scalar = nullptr, scalar_sum = nullptr;
+  std::vector<char> cubin;  // kept to fill other cache directories
   ~FfcxLibrary() {
     if (lib) (void)cudaLibraryUnload(lib);
   }
@@ -437,10 +438,19 @@ std::shared_ptr<FfcxLibrary> load_library(int device, int rank, const std::strin
   const std::string hash = hex64(fnv1a(key_src));
   const std::string key = std::to_string(device) + "/" + hash;
   std::lock_guard<std::mutex> lock(g_lib_mutex);
-  auto it = g_libs.find(key);
-  if (it != g_libs.end()) return it->second;
-  std::vector<char> cubin;
   const std::string stem = cachedir.empty() ? std::string() : cachedir + "/" + name + "_" + hash;
+  auto write_cache = [&](const std::vector<char>& bin) {
+    if (stem.empty()) return;
+    std::ofstream(stem + ".cu", std::ios::binary) << key_src;
+    std::ofstream(stem + ".cubin", std::ios::binary).write(bin.data(), (std::streamsize)bin.size());
+  };
+  auto it = g_libs.find(key);
+  if (it != g_libs.end()) {
+    // loaded already in this process: still fill a cache directory that lacks it
+    if (!stem.empty() && !std::ifstream(stem + ".cubin", std::ios::binary)) write_cache(it->second->cubin);
+    return it->second;
+  }
+  std::vector<char> cubin;
   if (!stem.empty()) {
     // a cached cubin is used only if its recorded source is this source
     std::ifstream fs(stem + ".cu", std::ios::binary), fb(stem + ".cubin", std::ios::binary);
@@ -451,14 +461,12 @@ std::shared_ptr<FfcxLibrary> load_library(int device, int rank, const std::strin
   }
   if (cubin.empty()) {
     cubin = nvrtc_compile(src, name, arch);
-    if (!stem.empty()) {
-      std::ofstream(stem + ".cu", std::ios::binary) << key_src;
-      std::ofstream(stem + ".cubin", std::ios::binary).write(cubin.data(), (std::streamsize)cubin.size());
-    }
+    write_cache(cubin);
   }
   auto L = std::make_shared<FfcxLibrary>();
   L->device = device;
-  FE_CUDA(cudaLibraryLoadData(&L->lib, cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0));
+  L->cubin = cubin;
+  FE_CUDA(cudaLibraryLoadData(&L->lib, L->cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0));
   if (rank == 2) {
     FE_CUDA(cudaLibraryGetKernel(&L->mat, L->lib, "fe_ffcx_mat"));
     FE_CUDA(cudaLibraryGetKernel(&L->lift, L->lib, "fe_ffcx_lift"));

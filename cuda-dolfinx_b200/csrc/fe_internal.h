@@ -355,6 +355,7 @@ struct MatLaunch {
   int upper = 0;  // reduce only into the upper triangle and the diagonal
   int cta_cells = 0;  // cells per CTA of the P1 / P2 atomic kernels (0: 128)
   int stage = 1;      // P2 atomic kernel: stage the byte maps in shared memory
+  int coalesced = 0;  // P2: reductions issued per warp, row by row (k_mat_p2_coal)
 };
 void launch_zero(double* v, int64_t n, cudaStream_t s);
 // symmetric-pattern transpose map (built once per pattern); false if the
@@ -403,13 +404,15 @@ struct LiftLaunch {
   double scale;
   double* b;
   int64_t num_values;
+  const uint8_t* skip = nullptr;  // rows left out of the scatter (stored by set_bc in the same pass)
 };
 void launch_lifting(const LiftLaunch& a, cudaStream_t s);
 void launch_mark_cells(const int32_t* dofs, int64_t num_cells, int k, int bs, const uint8_t* markers,
                        int32_t* out_cells, unsigned long long* out_count, cudaStream_t s);
 void launch_set_bc(double* b, int64_t num_values, const int32_t* dofs, int64_t n_bc, const double* g,
                    const double* x0, double scale, cudaStream_t s);
-// assemble_vector + apply_lifting + set_bc in one kernel for the pairs
+// assemble_vector + apply_lifting + set_bc in two launches (lifting; vector
+// and set_bc) for the pairs
 // (P1 load, P1 stiffness), (P2 load, P2 stiffness), (P3 load, P3 stiffness),
 // (vector-P2 load, elasticity); the lifting launch's bc1 markers are the rows
 // the scatters skip and bc_dofs the rows the kernel stores.

@@ -268,6 +268,86 @@ __global__ void __launch_bounds__(NT) k_mat_p2_atomic(const MatArgs a) {
 }
 
 // ---------------------------------------------------------------------------
+// P2 stiffness with the reductions coalesced per warp ("coalesced" variant).
+// The L2 applies FP64 reductions per 32-byte sector: on B200 one warp
+// instruction whose 32 reductions land in 32 sectors runs at ~210 G/s, with
+// 2 per sector at ~400 G/s, with 4 at ~500 G/s.  In the thread-per-cell
+// scatter each lane reduces into its own cell's rows, so an instruction
+// touches ~30 sectors.  Here each thread still computes one cell's element
+// tensor, but writes its 55 unique entries to shared memory; the warp then
+// issues its 32 cells' 3200 reductions cell by cell, row by row, consecutive
+// lanes on consecutive columns of a row: the 10 entries of a cell's row lie
+// in one CSR row, ~1.8 per sector.
+// ---------------------------------------------------------------------------
+constexpr int kCoalThreads = 64;
+
+template <int COEF, typename T>
+__global__ void __launch_bounds__(kCoalThreads) k_mat_p2_coal(const MatArgs a) {
+  constexpr int NT = kCoalThreads;
+  __shared__ __align__(16) uint8_t spos[NT * 100];
+  __shared__ double sE[NT * 55];
+  __shared__ int32_t srp[NT * 10];  // row start of each local row, -1 for a masked row
+  __shared__ uint16_t smc[NT];      // masked columns of each cell
+  const int64_t c0 = blockIdx.x * (int64_t)NT;
+  const int64_t left = a.num_cells - c0;
+  const int ncell = left < NT ? (int)left : NT;
+  stage_pos<100>(spos, a.pos, c0, ncell);
+  const int tid = threadIdx.x;
+  if (tid < ncell) {
+    const int64_t c = c0 + tid;
+    CellGeo g;
+    cell_geometry(a.x, load_geom(a.geom, c), g);
+    double Gh[6];
+    ghat(g, Gh);
+    const int32_t* d0 = a.dofs0 + c * 10;
+    const int32_t* d1 = a.dofs1 + c * 10;
+    unsigned mc = 0;
+#pragma unroll
+    for (int i = 0; i < 10; ++i) {
+      // masked rows / columns: BC dofs and dofs outside a restriction (-1)
+      const int r = __ldg(d0 + i), cc = __ldg(d1 + i);
+      const bool mrow = r < 0 || (a.bc0 && __ldg(a.bc0 + r));
+      srp[tid * 10 + i] = mrow ? -1 : __ldg(a.row_ptr + r);
+      mc |= (cc < 0 || (a.bc1 && __ldg(a.bc1 + cc)) ? 1u : 0u) << i;
+    }
+    smc[tid] = (uint16_t)mc;
+    double* E = sE + tid * 55;
+    auto emit = [&](int i, int j, double v) { E[i * (21 - i) / 2 + (j - i)] = v; };
+    if constexpr (COEF == FE_COEFF_P1) {
+      const int4 km = __ldg(reinterpret_cast<const int4*>(a.c0.map) + c);
+      const double k[4] = {__ldg(a.c0.v + km.x), __ldg(a.c0.v + km.y), __ldg(a.c0.v + km.z),
+                           __ldg(a.c0.v + km.w)};
+      T q[24];
+#pragma unroll
+      for (int m = 0; m < 4; ++m)
+#pragma unroll
+        for (int s2 = 0; s2 < 6; ++s2) q[m * 6 + s2] = (T)(k[m] * Gh[s2]);
+      p2_stiffness_p1coef<T>(q, emit);
+    } else {
+      const double k = coef_cell(a.c0, c);
+      T gq[6];
+#pragma unroll
+      for (int s2 = 0; s2 < 6; ++s2) gq[s2] = (T)(k * Gh[s2]);
+      p2_stiffness_const<T>(gq, emit);
+    }
+  }
+  __syncthreads();  // the staged byte maps and every cell's entries
+  // the warp's cells, flattened (cell, row, column): consecutive lanes take
+  // consecutive columns of one cell's row
+  const int lane = tid & 31, w0 = tid & ~31;
+  const int wcells = ncell - w0 < 32 ? ncell - w0 : 32;
+  double* __restrict__ vals = a.values;
+  for (int t = lane; t < wcells * 100; t += 32) {
+    const int q = w0 + t / 100, e = t % 100;
+    const int i = e / 10, j = e - 10 * (e / 10);
+    const int rs = srp[q * 10 + i];
+    if (rs < 0 || ((smc[q] >> j) & 1u)) continue;
+    const int lo = i < j ? i : j, hi = i < j ? j : i;
+    atomicAdd(vals + rs + spos[q * 100 + e], sE[q * 55 + lo * (21 - lo) / 2 + (hi - lo)]);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Mass matrices c*u*v*dx (P1: K = 4, P2: K = 10), one thread per cell, FP64
 // atomics.  Only |det J| and the coefficient enter the element tensor.
 // ---------------------------------------------------------------------------
@@ -1323,41 +1403,36 @@ __global__ void k_set_bc(double* __restrict__ b, int64_t num_values, const int32
 unsigned grid_for(int64_t n, int block) { return (unsigned)((n + block - 1) / block); }
 
 // ---------------------------------------------------------------------------
-// Right-hand side in one launch: assemble_vector(L) + apply_lifting([a], [bc])
-// + set_bc(bc) (assemble.py:136-166, 287-339, 341-380, which the reference runs
-// as three kernels with a context synchronise after each).  The CTAs are split
-// in three ranges: lifting over the cells with a marked trial dof (the longest
-// threads, first), the element vectors of all cells, and the BC dofs.  The two
-// scatters skip the marked rows, and the third range stores
+// Right-hand side: assemble_vector(L) + apply_lifting([a], [bc]) + set_bc(bc)
+// (assemble.py:136-166, 287-339, 341-380, three kernels with a context
+// synchronise after each in the reference) in two launches without a
+// synchronise: the lifting over the cells with a marked trial dof, and one
+// kernel whose CTAs take the element vectors of all cells, then the BC dofs.
+// Both scatters skip the marked rows and the BC range stores
 // b[d] = scale (g[d] - x0[d]) there, so no row is both accumulated and stored
-// in the launch; the result equals the three calls in sequence (up to the
-// order of the FP64 additions into unmarked rows).
+// and the launches need no order; the result equals the three calls (up to
+// the order of the FP64 additions into unmarked rows).  The lifting keeps a
+// launch of its own: its element tensor needs 70-164 registers per thread,
+// which in one kernel would hold the light vector threads (32 registers) to
+// its occupancy.
 // ---------------------------------------------------------------------------
 enum RhsPair { RHS_P1 = 1, RHS_P2 = 2, RHS_P3 = 3, RHS_VP2 = 4 };
 
 struct RhsArgs {
   VecArgs v;
-  LiftArgs l;
   const int32_t* __restrict__ bc_dofs;
   int64_t n_bc;
-  int64_t lift_ctas, vec_ctas;
+  const double* __restrict__ g;
+  const double* __restrict__ x0;
+  double scale;
+  int64_t vec_ctas;
 };
 
-template <int PAIR, int COEF, typename T, int NT>
-__global__ void __launch_bounds__(NT) k_rhs_fused(const RhsArgs a) {
-  int64_t blk = blockIdx.x;
-  if (blk < a.lift_ctas) {
-    const int64_t t = blk * NT + threadIdx.x;
-    if (t >= a.l.num_list) return;
-    if constexpr (PAIR == RHS_P1) lift_p1(a.l, t);
-    else if constexpr (PAIR == RHS_P2) lift_p2<COEF, T>(a.l, t);
-    else if constexpr (PAIR == RHS_P3) lift_p3<T>(a.l, t);
-    else lift_vp2<T>(a.l, t);
-    return;
-  }
-  blk -= a.lift_ctas;
+template <int PAIR>
+__global__ void __launch_bounds__(kBlock) k_rhs_vec_bc(const RhsArgs a) {
+  const int64_t blk = blockIdx.x;
   if (blk < a.vec_ctas) {
-    const int64_t c = blk * NT + threadIdx.x;
+    const int64_t c = blk * kBlock + threadIdx.x;
     if (c >= a.v.num_cells) return;
     if constexpr (PAIR == RHS_P1) vec_p1(a.v, c);
     else if constexpr (PAIR == RHS_P2) vec_p2(a.v, c);
@@ -1365,14 +1440,12 @@ __global__ void __launch_bounds__(NT) k_rhs_fused(const RhsArgs a) {
     else vec_vp2(a.v, c);
     return;
   }
-  blk -= a.vec_ctas;
-  const int64_t q = blk * NT + threadIdx.x;
+  const int64_t q = (blk - a.vec_ctas) * kBlock + threadIdx.x;
   if (q >= a.n_bc) return;
   const int32_t d = __ldg(a.bc_dofs + q);
   if (d < 0 || d >= a.v.num_values) return;
-  a.v.b[d] = a.l.scale * (__ldg(a.l.g + d) - (a.l.x0 ? __ldg(a.l.x0 + d) : 0.0));
+  a.v.b[d] = a.scale * (__ldg(a.g + d) - (a.x0 ? __ldg(a.x0 + d) : 0.0));
 }
-
 
 }  // namespace
 
@@ -1463,7 +1536,9 @@ void launch_matrix_atomic(const MatLaunch& L, cudaStream_t s) {
       auto go = [&](auto coef, auto tv) {
         constexpr int C = decltype(coef)::value;
         using T = typename decltype(tv)::type;
-        if (nt == 32) {
+        if (L.coalesced && !a.upper) {
+          k_mat_p2_coal<C, T><<<grid_for(L.num_cells, kCoalThreads), kCoalThreads, 0, s>>>(a);
+        } else if (nt == 32) {
           if (stage) k_mat_p2_atomic<C, T, 32, true><<<grid_for(L.num_cells, 32), 32, 0, s>>>(a);
           else k_mat_p2_atomic<C, T, 32, false><<<grid_for(L.num_cells, 32), 32, 0, s>>>(a);
         } else if (nt == 64) {
@@ -1657,6 +1732,7 @@ LiftArgs lift_args(const LiftLaunch& L) {
   a.scale = L.scale;
   a.b = L.b;
   a.num_values = L.num_values;
+  a.skip = L.skip;
   return a;
 }
 }  // namespace
@@ -1740,44 +1816,35 @@ bool rhs_fused_supported(int vec_kind, int mat_kind) {
 void launch_rhs_fused(const VecLaunch& V, const LiftLaunch& Lf, const int32_t* bc_dofs, int64_t n_bc,
                       cudaStream_t s) {
   FE_REQUIRE(rhs_fused_supported(V.kind, Lf.kind), "no fused right-hand side for this pair of form kinds");
+  // the BC's markers: exactly its dofs (checked when the BC is created)
+  LiftLaunch L = Lf;
+  L.skip = Lf.bc1;
+  launch_lifting(L, s);
   RhsArgs a{};
   a.v = vec_args(V);
-  a.l = lift_args(Lf);
-  a.v.skip = a.l.skip = Lf.bc1;  // the BC's markers: exactly its dofs (checked when the BC is created)
+  a.v.skip = Lf.bc1;
   a.bc_dofs = bc_dofs;
   a.n_bc = n_bc;
-  const int pair = V.kind == FE_FORM_P1_LOAD ? RHS_P1
-                   : V.kind == FE_FORM_P2_LOAD ? RHS_P2
-                   : V.kind == FE_FORM_P3_LOAD ? RHS_P3
-                                               : RHS_VP2;
-  const int nt = pair == RHS_P3 ? kBlockP3 : kBlock;
-  a.lift_ctas = (Lf.num_list + nt - 1) / nt;
-  a.vec_ctas = (V.num_cells + nt - 1) / nt;
-  const int64_t total = a.lift_ctas + a.vec_ctas + (n_bc + nt - 1) / nt;
+  a.g = Lf.g;
+  a.x0 = Lf.x0;
+  a.scale = Lf.scale;
+  a.vec_ctas = (V.num_cells + kBlock - 1) / kBlock;
+  const int64_t total = a.vec_ctas + (n_bc + kBlock - 1) / kBlock;
   if (total == 0) return;
   FE_REQUIRE(total < (int64_t)INT_MAX, "right-hand side too large for one launch");
   const unsigned grid = (unsigned)total;
-  const bool f32 = Lf.precision == FE_PREC_FP32;
-  switch (pair) {
-    case RHS_P1:
-      k_rhs_fused<RHS_P1, 0, double, kBlock><<<grid, kBlock, 0, s>>>(a);
+  switch (V.kind) {
+    case FE_FORM_P1_LOAD:
+      k_rhs_vec_bc<RHS_P1><<<grid, kBlock, 0, s>>>(a);
       break;
-    case RHS_P2:
-      if (a.l.c0.kind == FE_COEFF_P1) {
-        if (f32) k_rhs_fused<RHS_P2, FE_COEFF_P1, float, kBlock><<<grid, kBlock, 0, s>>>(a);
-        else k_rhs_fused<RHS_P2, FE_COEFF_P1, double, kBlock><<<grid, kBlock, 0, s>>>(a);
-      } else {
-        if (f32) k_rhs_fused<RHS_P2, FE_COEFF_DG0, float, kBlock><<<grid, kBlock, 0, s>>>(a);
-        else k_rhs_fused<RHS_P2, FE_COEFF_DG0, double, kBlock><<<grid, kBlock, 0, s>>>(a);
-      }
+    case FE_FORM_P2_LOAD:
+      k_rhs_vec_bc<RHS_P2><<<grid, kBlock, 0, s>>>(a);
       break;
-    case RHS_P3:
-      if (f32) k_rhs_fused<RHS_P3, 0, float, kBlockP3><<<grid, kBlockP3, 0, s>>>(a);
-      else k_rhs_fused<RHS_P3, 0, double, kBlockP3><<<grid, kBlockP3, 0, s>>>(a);
+    case FE_FORM_P3_LOAD:
+      k_rhs_vec_bc<RHS_P3><<<grid, kBlock, 0, s>>>(a);
       break;
     default:
-      if (f32) k_rhs_fused<RHS_VP2, 0, float, kBlock><<<grid, kBlock, 0, s>>>(a);
-      else k_rhs_fused<RHS_VP2, 0, double, kBlock><<<grid, kBlock, 0, s>>>(a);
+      k_rhs_vec_bc<RHS_VP2><<<grid, kBlock, 0, s>>>(a);
   }
   FE_CUDA(cudaGetLastError());
 }

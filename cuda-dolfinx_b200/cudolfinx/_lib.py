@@ -44,8 +44,10 @@ PREC_FP64, PREC_FP32 = 0, 1
 ASM_ZERO, ASM_DETERMINISTIC, ASM_ATOMIC, ASM_SORTED_SLOT, ASM_TILE, ASM_ROW_GATHER, ASM_BLOCK = 1, 2, 4, 8, 16, 32, 64
 ASM_FULL_SCATTER = 128
 ASM_GROUPED = 256
+ASM_COALESCED = 512
 VARIANT_FLAGS = {"auto": 0, "deterministic": ASM_DETERMINISTIC, "atomic": ASM_ATOMIC, "sorted-slot": ASM_SORTED_SLOT,
-                 "tile": ASM_TILE, "row-gather": ASM_ROW_GATHER, "block": ASM_BLOCK, "atomic-full": ASM_ATOMIC | ASM_FULL_SCATTER, "grouped": ASM_GROUPED}
+                 "tile": ASM_TILE, "row-gather": ASM_ROW_GATHER, "block": ASM_BLOCK, "atomic-full": ASM_ATOMIC | ASM_FULL_SCATTER, "grouped": ASM_GROUPED,
+                 "coalesced": ASM_COALESCED}
 
 _SIGS = {
     "fe_last_error": (ctypes.c_char_p, []),

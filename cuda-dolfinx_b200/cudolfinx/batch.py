@@ -25,7 +25,7 @@ from .la import CUDAMatrix
 # matrix variants worth timing per form kind (all parity-tested)
 CANDIDATES = {
     "P1_STIFFNESS": ("atomic", "block", "tile"),
-    "P2_STIFFNESS": ("atomic", "block", "grouped"),
+    "P2_STIFFNESS": ("atomic", "block", "grouped", "coalesced"),
     "VP2_ELASTICITY": ("atomic", "atomic-full"),
 }
 # launch shapes of the atomic scatter timed per form kind: (cells per CTA,

@@ -125,6 +125,9 @@ enum fe_precision {
                                      entries summed per distinct CSR slot in shared memory, then one
                                      reduction per slot (falls back to the atomic scatter when the
                                      mesh's groups share no structure)                                */
+#define FE_ASM_COALESCED 512u     /* P2 stiffness: element tensors staged per warp in shared memory,
+                                     the warp's reductions issued row by row (consecutive lanes on one
+                                     cell's CSR row, so an instruction's reductions share L2 sectors) */
 
 /* ---- errors / context --------------------------------------------------- */
 const char* fe_last_error(void);
@@ -366,16 +369,18 @@ int fe_apply_lifting(double* b, int num_forms, const fe_form* a, const fe_bc* bc
  * "part": "diagonal" (python/test/test_cuda_assembly.py:199-208), e.g. for a
  * Jacobi preconditioner.  FE_ASM_ZERO zeroes b first. */
 int fe_assemble_diagonal(fe_form a, double* b, unsigned flags, void* stream);
-/* The right-hand side of a linear system in one kernel: b = [0 with
+/* The right-hand side of a linear system in one call: b = [0 with
  * FE_ASM_ZERO] + L - scale * A (g - x0) on the BC columns, then
  * b[d] = scale * (g[d] - x0[d]) on the BC dofs.  Replaces the sequence
  * assemble_vector_on_device + apply_lifting_on_device([a], [bc]) +
  * set_bc_on_device (wrappers/fem.cpp:291-309, 327-383; assemble.py:136-166, 287-339,
- * 341-380), which the reference runs as three kernels.  One launch when L and
- * a are a (P1 load, P1 stiffness), (P2 load, P2 stiffness), (P3 load, P3
- * stiffness) or (vector-P2 load, elasticity) pair on one space and the BC's
- * markers are its dof list; other forms (FFCx, facet, restricted) take the
- * three calls, with the same result.  bc may be NULL (b = L).  x0 may be
+ * 341-380), which the reference runs as three kernels with a synchronise
+ * after each.  Two launches with no order between them (the lifting; the
+ * element vectors with set_bc) when L and a are a (P1 load, P1 stiffness),
+ * (P2 load, P2 stiffness), (P3 load, P3 stiffness) or (vector-P2 load,
+ * elasticity) pair on one space and the BC's markers are its dof list: the
+ * scatters skip the BC rows that set_bc stores.  Other forms (FFCx, facet,
+ * restricted) take the three calls, with the same result.  bc may be NULL (b = L).  x0 may be
  * NULL.  Entries outside the BC rows equal the three calls' up to the order of
  * FP64 additions; the BC rows are equal. */
 int fe_assemble_rhs(fe_form L, fe_form a, fe_bc bc, double* b, const double* x0, double scale,

@@ -35,13 +35,14 @@ def _problem_from_golden(path):
     return P, G
 
 
-VARIANTS = ["auto", "atomic", "atomic-full", "tile", "deterministic", "sorted-slot", "row-gather", "block", "grouped"]
+VARIANTS = ["auto", "atomic", "atomic-full", "tile", "deterministic", "sorted-slot", "row-gather", "block", "grouped",
+            "coalesced"]
 
 
 def _supported(kind, variant):
     if variant == "row-gather":
         return kind in ("p1", "p1k")
-    if variant == "grouped":
+    if variant in ("grouped", "coalesced"):
         return kind == "p2"
     if variant in ("tile", "block"):
         return kind in ("p1", "p1k", "p2")
@@ -322,8 +323,9 @@ def test_empty_bc_and_empty_mesh():
     assert A.sparsity.nnz == 0
 
 
+@pytest.mark.parametrize("variant", ["grouped", "coalesced"])
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
-def test_grouped_variant_on_permuted_cells_and_renumbered_dofs(precision):
+def test_grouped_variant_on_permuted_cells_and_renumbered_dofs(precision, variant):
     # the grouped plan comes from the dofmap and the cell centroids only: a
     # random cell order and a random dof numbering give the same matrix
     from conftest import ensure_library
@@ -348,7 +350,7 @@ def test_grouped_variant_on_permuted_cells_and_renumbered_dofs(precision):
     bc = fem.dirichletbc(fem.Function(V, g), bdofs)
     asm = cx.CUDAAssembler()
     a = cx.form(fem.stiffness(V, k, precision=precision))
-    A = asm.assemble_matrix(a, bcs=[bc], variant="grouped")
+    A = asm.assemble_matrix(a, bcs=[bc], variant=variant)
     A.assemble()
     rp, col = A.sparsity.to_host()
     rp_o, col_o = fo.sparsity(V.dofs, V.dofs, V.num_nodes)
