@@ -389,3 +389,39 @@ def test_atomic_launch_shapes(kind, shape):
     assert ok, worst
     with pytest.raises(RuntimeError, match="cells per CTA"):
         _lib.check(_lib.lib.fe_form_set_launch(a.cuda_form, 48, 1), "fe_form_set_launch")
+
+
+@pytest.mark.parametrize("kind,n", [("p1", 7), ("p1k", 8)])
+@pytest.mark.parametrize("bcs", ["same", "rows-only", "none"])
+def test_block_variant_bc_paths(kind, n, bcs):
+    # the P1 block kernel has two paths: with the same BCs on rows and
+    # columns (or none) each cell adds its off-diagonal pairs once and the
+    # flush writes every row's diagonal as minus its off-diagonal sum; with
+    # row BCs only, every entry goes to its own slot.  Both against the oracle.
+    import torch
+
+    from cudolfinx import _lib
+
+    P = fo.build_problem(kind, n, seed=21)
+    M = mirror_problem(P)
+    cx = M["cx"]
+    asm = cx.CUDAAssembler()
+    a = cx.form(M["a"])
+    A = asm.create_matrix(a)
+    hbc = asm.pack_bcs([M["bc"]])._get_cpp_bcs(M["V"]).handle
+    b0, b1 = {"same": (hbc, hbc), "rows-only": (hbc, None), "none": (None, None)}[bcs]
+    flags = _lib.ASM_ZERO | _lib.VARIANT_FLAGS["block"]
+    _lib.check(_lib.lib.fe_assemble_matrix(a.cuda_form, A.values.data_ptr(), b0, b1, 1.0, flags,
+                                           torch.cuda.current_stream().cuda_stream), "block")
+    torch.cuda.synchronize()
+    rp, col = A.sparsity.to_host()
+    mk = np.zeros(P["ndof"], np.uint8)
+    mk[P["bc_dofs"]] = 1
+    m0 = mk if b0 is not None else None
+    m1 = mk if b1 is not None else None
+    Ae = fo.element_matrices(P)
+    ref = fo.assemble_matrix(Ae, P["dofs"], P["dofs"], rp, col, 1, 1, m0, m1, 1.0,
+                             P["bc_dofs"] if b0 is not None else None)
+    bound = fo.matrix_bound(Ae, P["dofs"], P["dofs"], rp, col, 1, 1, m0, m1)
+    ok, worst = tolerance_check(A.values.cpu().numpy(), ref, bound)
+    assert ok, worst
