@@ -281,17 +281,20 @@ __global__ void __launch_bounds__(NT) k_mat_p2_atomic(const MatArgs a) {
 // ---------------------------------------------------------------------------
 constexpr int kCoalThreads = 64;
 
-template <int COEF, typename T>
-__global__ void __launch_bounds__(kCoalThreads) k_mat_p2_coal(const MatArgs a) {
+// STAGE: the CTA's byte maps copied to shared memory first (6.4 KB), else
+// read from global memory (L1) in the reduction loop, which leaves room for a
+// seventh CTA per SM
+template <int COEF, typename T, bool STAGE>
+__global__ void __launch_bounds__(kCoalThreads, 7) k_mat_p2_coal(const MatArgs a) {
   constexpr int NT = kCoalThreads;
-  __shared__ __align__(16) uint8_t spos[NT * 100];
+  __shared__ __align__(16) uint8_t spos[STAGE ? NT * 100 : 16];
   __shared__ double sE[NT * 55];
   __shared__ int32_t srp[NT * 10];  // row start of each local row, -1 for a masked row
   __shared__ uint16_t smc[NT];      // masked columns of each cell
   const int64_t c0 = blockIdx.x * (int64_t)NT;
   const int64_t left = a.num_cells - c0;
   const int ncell = left < NT ? (int)left : NT;
-  stage_pos<100>(spos, a.pos, c0, ncell);
+  if constexpr (STAGE) stage_pos<100>(spos, a.pos, c0, ncell);
   const int tid = threadIdx.x;
   if (tid < ncell) {
     const int64_t c = c0 + tid;
@@ -332,18 +335,34 @@ __global__ void __launch_bounds__(kCoalThreads) k_mat_p2_coal(const MatArgs a) {
     }
   }
   __syncthreads();  // the staged byte maps and every cell's entries
-  // the warp's cells, flattened (cell, row, column): consecutive lanes take
-  // consecutive columns of one cell's row
+  // lanes 10*h + j (h = 0..2, j = 0..9) take column j of row 3*r + h of one
+  // cell, for r = 0..3: four instructions per cell, each on three rows; the
+  // entry indices of a lane are the same for every cell
   const int lane = tid & 31, w0 = tid & ~31;
   const int wcells = ncell - w0 < 32 ? ncell - w0 : 32;
-  double* __restrict__ vals = a.values;
-  for (int t = lane; t < wcells * 100; t += 32) {
-    const int q = w0 + t / 100, e = t % 100;
-    const int i = e / 10, j = e - 10 * (e / 10);
-    const int rs = srp[q * 10 + i];
-    if (rs < 0 || ((smc[q] >> j) & 1u)) continue;
+  const int h = lane / 10, j = lane - 10 * h;
+  int ei[4], eu[4];
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    const int i = 3 * r + h;
     const int lo = i < j ? i : j, hi = i < j ? j : i;
-    atomicAdd(vals + rs + spos[q * 100 + e], sE[q * 55 + lo * (21 - lo) / 2 + (hi - lo)]);
+    const bool ok = lane < 30 && i < 10;
+    ei[r] = ok ? i : -1;
+    eu[r] = lo * (21 - lo) / 2 + (hi - lo);
+  }
+  double* __restrict__ vals = a.values;
+  for (int q = w0; q < w0 + wcells; ++q) {
+    const bool cmask = (smc[q] >> j) & 1u;
+    const int32_t* rq = srp + q * 10;
+    const uint8_t* pq = STAGE ? spos + q * 100 : a.pos + (c0 + q) * 100;
+    const double* Eq = sE + q * 55;
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      if (ei[r] < 0 || cmask) continue;
+      const int rs = rq[ei[r]];
+      if (rs < 0) continue;
+      atomicAdd(vals + rs + pq[ei[r] * 10 + j], Eq[eu[r]]);
+    }
   }
 }
 
@@ -1537,7 +1556,11 @@ void launch_matrix_atomic(const MatLaunch& L, cudaStream_t s) {
         constexpr int C = decltype(coef)::value;
         using T = typename decltype(tv)::type;
         if (L.coalesced && !a.upper) {
-          k_mat_p2_coal<C, T><<<grid_for(L.num_cells, kCoalThreads), kCoalThreads, 0, s>>>(a);
+          // shared memory before L1: the staged element tensors set the CTAs per SM
+          auto k = stage ? k_mat_p2_coal<C, T, true> : k_mat_p2_coal<C, T, false>;
+          FE_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                       cudaSharedmemCarveoutMaxShared));
+          k<<<grid_for(L.num_cells, kCoalThreads), kCoalThreads, 0, s>>>(a);
         } else if (nt == 32) {
           if (stage) k_mat_p2_atomic<C, T, 32, true><<<grid_for(L.num_cells, 32), 32, 0, s>>>(a);
           else k_mat_p2_atomic<C, T, 32, false><<<grid_for(L.num_cells, 32), 32, 0, s>>>(a);
