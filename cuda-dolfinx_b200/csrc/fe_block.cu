@@ -81,9 +81,6 @@ struct BlockArgs {
   const uint16_t* __restrict__ glocal;     // P1: [records][4] block-local node of each vertex
   const int32_t* __restrict__ rec_ptr;     // P1: [nblocks+1] record offsets (lrow, pos, glocal,
                                            // cell_id and dofs1 are indexed by record)
-  const uint16_t* __restrict__ mirror;     // P1 symmetric path: per window slot, the window slot of its
-                                           // transpose (0xFFFF: the transposed row is not in the window)
-  const int32_t* __restrict__ wmir_ptr;    // [nblocks+1] start of each block's mirror entries
 };
 
 __device__ __forceinline__ void block_geom(const double* __restrict__ x, int4 v, double K[3][3], double& adet) {
@@ -146,9 +143,6 @@ __device__ __forceinline__ long long to_fixed(double v, const FixedScale& f) { r
 // cells whose entry bound lies below 2^(ex - kDirect*) take the FP64 path:
 // the P1 bound is the cell's largest entry itself, the P2 one an upper bound
 constexpr int kDirectP1 = 8;
-// symmetric P1 path: a diagonal entry is the sum of 3 rounded off-diagonal
-// contributions per cell, so cells route to FP64 two binary orders earlier
-constexpr int kDirectP1Sym = 6;
 constexpr int kDirectP2 = 6;
 
 // element tensor of block-ordered cell cb, entries (i, j, value) for i <= j
@@ -350,15 +344,6 @@ struct P1Smem {
   static constexpr size_t SMEM = OFF_RINFO + sizeof(uint32_t) * Tr::RCAP;
 };
 
-// SYM (square form, the same BCs on rows and columns; P1 element rows sum to
-// zero for any cellwise coefficient): each cell adds only its 6 off-diagonal
-// pairs, once, into the window slot of the pair's upper-triangle entry (12
-// shared atomics instead of 32; no BC masking at this stage).  The flush
-// reads an entry below the diagonal from its transpose's slot (the plan's
-// mirror table), applies the BC masks, and writes each row's diagonal as
-// minus the sum of the row's off-diagonal fixed-point values, BC columns
-// included: per element, A_ii = -sum_{j != i} A_ij.
-template <bool SYM>
 __global__ void __launch_bounds__(BlockTraits<FE_FORM_P1_STIFFNESS>::NT, 4) k_block_p1(const BlockArgs a,
                                                                                     int square) {
   using Tr = BlockTraits<FE_FORM_P1_STIFFNESS>;
@@ -416,7 +401,7 @@ __global__ void __launch_bounds__(BlockTraits<FE_FORM_P1_STIFFNESS>::NT, 4) k_bl
   __syncthreads();
   const double kfac = a.coef_kind != FE_COEFF_CONSTANT ? (double)__uint_as_float(s_bmax) : fabs(a.coef_const);
   const double bmax = 1.25 * a.gbound[b] * kfac;
-  const FixedScale fs = fixed_scale(bmax, a.fx_bits, SYM ? kDirectP1Sym : kDirectP1);
+  const FixedScale fs = fixed_scale(bmax, a.fx_bits, kDirectP1);
 
   // lane l of warp w takes cells l*span + w, l*span + w + NW, ...: the 32
   // cells of one warp instruction lie span cells apart along the curve, and
@@ -446,15 +431,6 @@ __global__ void __launch_bounds__(BlockTraits<FE_FORM_P1_STIFFNESS>::NT, 4) k_bl
       atomicAdd(w1 + idx, hi + ((old + lo < old) ? 1u : 0u));
     };
     auto emit = [&](int i, int j, double v) {
-      if constexpr (SYM) {
-        // the pair once, into its upper-triangle slot (window rows ascend with
-        // the global rows); the diagonal comes from the row sums
-        if (i == j) return;
-        const int slot = lr[i] < lr[j] ? wbase[i] + (int)((pw[i] >> (8 * j)) & 0xffu)
-                                       : wbase[j] + (int)((pw[j] >> (8 * i)) & 0xffu);
-        add(slot, to_fixed(v, fs));
-        return;
-      }
       const long long w = to_fixed(v, fs);
       const bool ok_ij = ((own >> i) & 1u) && !((cmask >> j) & 1u);
       add(ok_ij ? wbase[i] + (int)((pw[i] >> (8 * j)) & 0xffu) : kP1Wcap, w);
@@ -519,47 +495,14 @@ __global__ void __launch_bounds__(BlockTraits<FE_FORM_P1_STIFFNESS>::NT, 4) k_bl
   }
   __syncthreads();
   const double inv = 1.0 / fs.scale;  // exact: a power of two
-  if constexpr (SYM) {
-    // half-warp per window row: lanes over the row's slots; the two rows of
-    // a warp run the same number of rounds so the shuffles see all lanes
-    const uint16_t* __restrict__ mir = a.mirror + a.wmir_ptr[b];
-    const int half = lane >> 4, hl = lane & 15;
-    for (int r0 = 2 * warp; r0 < nrows; r0 += 2 * NW) {
-      const int r = r0 + half;
-      const bool active = r < nrows;
-      const int so = active ? s_soff[r] : 0, len = active ? s_soff[r + 1] - so : 0;
-      const bool rbc = active && ((s_rinfo[r] >> 30) & 1u);
-      const int32_t gb = active ? s_gbase[r] : 0;
-      long long sum = 0;
-      int dslot = -1;
-      for (int e = hl; e < len; e += 16) {
-        const int w = so + e;
-        const int m = __ldg(mir + w);
-        if (m == 0xFFFF) continue;  // no cell of the block couples the two rows
-        if (m == w) {
-          dslot = e;
-          continue;
-        }
-        const int src = m >= so + len ? w : m;  // upper: own slot; lower: the transpose's
-        const long long v = (long long)(((unsigned long long)w1[src] << 32) | w0[src]);
-        sum += v;
-        const bool cbc = (s_rinfo[s_wrow[m]] >> 30) & 1u;
-        if (v != 0 && !rbc && !cbc) atomicAdd(a.values + gb + e, __ll2double_rn(v) * inv);
-      }
-#pragma unroll
-      for (int o = 8; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o, 16);
-      if (dslot >= 0 && !rbc && sum != 0) atomicAdd(a.values + gb + dslot, -__ll2double_rn(sum) * inv);
-    }
-  } else {
-    // flat flush: consecutive lanes take consecutive window slots
-    for (int w = tid; w < wtot; w += NT) {
-      const uint32_t lo = w0[w], hi = w1[w];
-      if (lo | hi) {
-        const int r = s_wrow[w];
-        // hi * 2^32 + lo, rounded once to double (both halves convert exactly)
-        const double v = fma((double)(int32_t)hi, 4294967296.0, (double)lo);
-        atomicAdd(a.values + s_gbase[r] + (w - s_soff[r]), v * inv);
-      }
+  // flat flush: consecutive lanes take consecutive window slots
+  for (int w = tid; w < wtot; w += NT) {
+    const uint32_t lo = w0[w], hi = w1[w];
+    if (lo | hi) {
+      const int r = s_wrow[w];
+      // hi * 2^32 + lo, rounded once to double (both halves convert exactly)
+      const double v = fma((double)(int32_t)hi, 4294967296.0, (double)lo);
+      atomicAdd(a.values + s_gbase[r] + (w - s_soff[r]), v * inv);
     }
   }
 }
@@ -805,64 +748,6 @@ std::unique_ptr<fe_form_s::BlockPlan> build_block_plan(const fe_form_s& f) {
     cell_id.swap(cell_r);
   }
 
-  // P1 on one dofmap: the mirror table of the symmetric path.  For window
-  // slot (R, C) of a block, the window slot of (C, R) when row C is a window
-  // row of the block, else 0xFFFF (then no cell of the block couples R and
-  // C, and the slot stays zero).
-  std::vector<uint16_t> mirror;
-  std::vector<int32_t> wmir_ptr;
-  int fx_bits_sym = fx_bits;
-  if (KIND == FE_FORM_P1_STIFFNESS && f.V0 == f.V1 && !V0.excluded) {
-    {
-      // a row's diagonal sums K-1 off-diagonal contributions per cell
-      std::vector<int32_t> cnt(V0.num_blocks, 0);
-      int32_t maxcnt = 0;
-      for (int64_t q = 0; q < C * K; ++q) maxcnt = std::max(maxcnt, ++cnt[V0.host[q]]);
-      int bits = 0;
-      while ((int64_t(1) << bits) < (int64_t)(K - 1) * maxcnt + 1) ++bits;
-      fx_bits_sym = std::min(57, 62 - bits);
-    }
-    const int64_t nb = (int64_t)block_ptr.size() - 1;
-    std::vector<int32_t> hcol(f.sp->nnz);
-    if (f.sp->nnz)
-      FE_CUDA(cudaMemcpy(hcol.data(), f.sp->col.p, (size_t)f.sp->nnz * sizeof(int32_t), cudaMemcpyDeviceToHost));
-    wmir_ptr.assign(nb + 1, 0);
-    for (int64_t b = 0; b < nb; ++b) {
-      const int32_t r0 = brow_ptr[b], r1 = brow_ptr[b + 1];
-      const int32_t last = r1 - 1;
-      const int32_t wt = r1 > r0 ? soff[last] + (rp[rows[last] + 1] - rp[rows[last]]) : 0;
-      wmir_ptr[b + 1] = wmir_ptr[b] + wt;
-    }
-    mirror.assign((size_t)wmir_ptr[nb], 0xFFFF);
-    const int nthreads = (int)std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
-    auto work = [&](int tid) {
-      std::vector<int32_t> stamp(V0.num_blocks, -1), loc(V0.num_blocks, 0);
-      for (int64_t b = tid; b < nb; b += nthreads) {
-        const int32_t r0 = brow_ptr[b], r1 = brow_ptr[b + 1];
-        for (int32_t u = r0; u < r1; ++u) {
-          stamp[rows[u]] = (int32_t)b;
-          loc[rows[u]] = u;
-        }
-        uint16_t* mb = mirror.data() + wmir_ptr[b];
-        for (int32_t u = r0; u < r1; ++u) {
-          const int32_t R = rows[u];
-          for (int32_t e = rp[R]; e < rp[R + 1]; ++e) {
-            const int32_t Cc = hcol[e];
-            if (stamp[Cc] != (int32_t)b) continue;
-            const int32_t* lo = hcol.data() + rp[Cc];
-            const int32_t* hi = hcol.data() + rp[Cc + 1];
-            const int32_t* it = std::lower_bound(lo, hi, R);
-            if (it == hi || *it != R) continue;  // an unsymmetric pattern: no transpose
-            mb[soff[u] + (e - rp[R])] = (uint16_t)(soff[loc[Cc]] + (it - lo));
-          }
-        }
-      }
-    };
-    std::vector<std::thread> pool;
-    for (int t = 0; t < nthreads; ++t) pool.emplace_back(work, t);
-    for (auto& t : pool) t.join();
-  }
-
   auto P = std::make_unique<fe_form_s::BlockPlan>();
   P->nblocks = (int64_t)block_ptr.size() - 1;
   P->fx_bits = fx_bits;
@@ -892,12 +777,6 @@ std::unique_ptr<fe_form_s::BlockPlan> build_block_plan(const fe_form_s& f) {
     up(P->gx, gx);
     up(P->glocal, glocal);
     up(P->rec_ptr, rec_ptr);
-    if (!wmir_ptr.empty()) {
-      up(P->mirror, mirror);
-      up(P->wmir_ptr, wmir_ptr);
-      P->fx_bits_sym = fx_bits_sym;
-      P->has_mirror = true;
-    }
   }
   return P;
 }
@@ -934,22 +813,11 @@ void launch_block(const fe_form_s& f, const fe_form_s::BlockPlan& P, double* val
   a.gx = P.gx.p;
   a.glocal = P.glocal.p;
   a.rec_ptr = P.rec_ptr.p;
-  a.mirror = P.mirror.p;
-  a.wmir_ptr = P.wmir_ptr.p;
   if (P.nblocks == 0) return;
   if constexpr (KIND == FE_FORM_P1_STIFFNESS) {
     constexpr size_t smem = P1Smem::SMEM;
-    // the symmetric path needs the same BCs on rows and columns (the diagonal
-    // is summed over every column, the BC ones included)
-    const bool sym = P.has_mirror && f.V0 == f.V1 && bc0 == bc1;
-    if (sym) {
-      a.fx_bits = P.fx_bits_sym;
-      FE_CUDA(cudaFuncSetAttribute(k_block_p1<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      k_block_p1<true><<<(unsigned)P.nblocks, BlockTraits<KIND>::NT, smem, s>>>(a, 1);
-    } else {
-      FE_CUDA(cudaFuncSetAttribute(k_block_p1<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      k_block_p1<false><<<(unsigned)P.nblocks, BlockTraits<KIND>::NT, smem, s>>>(a, f.V0 == f.V1 ? 1 : 0);
-    }
+    FE_CUDA(cudaFuncSetAttribute(k_block_p1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_block_p1<<<(unsigned)P.nblocks, BlockTraits<KIND>::NT, smem, s>>>(a, f.V0 == f.V1 ? 1 : 0);
     FE_CUDA(cudaGetLastError());
     return;
   }

@@ -288,12 +288,6 @@ struct fe_form_s::BlockPlan {
   fe::DevBuf<uint16_t> glocal;        // [cells][4] block-local geometry node of each cell vertex
   fe::DevBuf<int32_t> rec_ptr;        // P1: [nblocks+1] per-cell records of each block, padded to
                                       // whole warps and stored in the kernel's lane order
-  // P1 on one dofmap (symmetric path): per window slot the window slot of its
-  // transpose, 0xFFFF if absent; blocks start at wmir_ptr
-  bool has_mirror = false;
-  fe::DevBuf<uint16_t> mirror;
-  fe::DevBuf<int32_t> wmir_ptr;
-  int fx_bits_sym = 50;               // fixed-point bits when a row's diagonal sums its off-diagonals
 };
 
 struct fe_form_s::GroupPlan {

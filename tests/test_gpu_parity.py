@@ -394,10 +394,8 @@ def test_atomic_launch_shapes(kind, shape):
 @pytest.mark.parametrize("kind,n", [("p1", 7), ("p1k", 8)])
 @pytest.mark.parametrize("bcs", ["same", "rows-only", "none"])
 def test_block_variant_bc_paths(kind, n, bcs):
-    # the P1 block kernel has two paths: with the same BCs on rows and
-    # columns (or none) each cell adds its off-diagonal pairs once and the
-    # flush writes every row's diagonal as minus its off-diagonal sum; with
-    # row BCs only, every entry goes to its own slot.  Both against the oracle.
+    # the P1 block kernel with the same BCs on rows and columns, with row BCs
+    # only, and with none, against the oracle
     import torch
 
     from cudolfinx import _lib
@@ -408,7 +406,8 @@ def test_block_variant_bc_paths(kind, n, bcs):
     asm = cx.CUDAAssembler()
     a = cx.form(M["a"])
     A = asm.create_matrix(a)
-    hbc = asm.pack_bcs([M["bc"]])._get_cpp_bcs(M["V"]).handle
+    dbc = asm.pack_bcs([M["bc"]])  # keeps the BC object (and its handle) alive
+    hbc = dbc._get_cpp_bcs(M["V"]).handle
     b0, b1 = {"same": (hbc, hbc), "rows-only": (hbc, None), "none": (None, None)}[bcs]
     flags = _lib.ASM_ZERO | _lib.VARIANT_FLAGS["block"]
     _lib.check(_lib.lib.fe_assemble_matrix(a.cuda_form, A.values.data_ptr(), b0, b1, 1.0, flags,
