@@ -294,8 +294,16 @@ __global__ void __launch_bounds__(kCoalThreads, 7) k_mat_p2_coal(const MatArgs a
   const int64_t c0 = blockIdx.x * (int64_t)NT;
   const int64_t left = a.num_cells - c0;
   const int ncell = left < NT ? (int)left : NT;
-  if constexpr (STAGE) stage_pos<100>(spos, a.pos, c0, ncell);
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31, w0 = tid & ~31;
+  const int wcells = ncell - w0 < 0 ? 0 : (ncell - w0 < 32 ? ncell - w0 : 32);
+  if constexpr (STAGE) {
+    // each warp stages its own cells' byte maps (from a 16-byte boundary:
+    // (c0 + w0) * 100 is a multiple of 3200; the map buffer is padded to 16)
+    const uint4* src = reinterpret_cast<const uint4*>(a.pos + (c0 + w0) * 100);
+    uint4* dst = reinterpret_cast<uint4*>(spos + w0 * 100);
+    const int nvec = (wcells * 100 + 15) / 16;
+    for (int t = lane; t < nvec; t += 32) dst[t] = __ldg(src + t);
+  }
   if (tid < ncell) {
     const int64_t c = c0 + tid;
     CellGeo g;
@@ -334,12 +342,10 @@ __global__ void __launch_bounds__(kCoalThreads, 7) k_mat_p2_coal(const MatArgs a
       p2_stiffness_const<T>(gq, emit);
     }
   }
-  __syncthreads();  // the staged byte maps and every cell's entries
+  __syncwarp();  // the warp's staged byte maps and its cells' entries
   // lanes 10*h + j (h = 0..2, j = 0..9) take column j of row 3*r + h of one
   // cell, for r = 0..3: four instructions per cell, each on three rows; the
   // entry indices of a lane are the same for every cell
-  const int lane = tid & 31, w0 = tid & ~31;
-  const int wcells = ncell - w0 < 32 ? ncell - w0 : 32;
   const int h = lane / 10, j = lane - 10 * h;
   int ei[4], eu[4];
 #pragma unroll
@@ -351,6 +357,7 @@ __global__ void __launch_bounds__(kCoalThreads, 7) k_mat_p2_coal(const MatArgs a
     eu[r] = lo * (21 - lo) / 2 + (hi - lo);
   }
   double* __restrict__ vals = a.values;
+#pragma unroll 2
   for (int q = w0; q < w0 + wcells; ++q) {
     const bool cmask = (smc[q] >> j) & 1u;
     const int32_t* rq = srp + q * 10;
