@@ -578,10 +578,12 @@ def run_gpu(args, rank, world, local_rank):
     peak = peaks.get("hbm_gbs", 6650.0)
     achieved = alg / (mat_ms / 1e3) / 1e9
     # the variant "auto" resolves to (fe_assemble_matrix's default): the block
-    # kernel for P1 meshes of >= 2^20 cells, the atomic scatter otherwise
+    # kernel for P1 meshes of >= 2^20 cells, the coalesced scatter for P2
+    # stiffness, the atomic scatter otherwise
     resolved = args.variant
     if resolved == "auto":
-        resolved = "block" if (W["kind"] == "p1" and len(I["cells"]) >= (1 << 20)) else "atomic"
+        resolved = ("block" if (W["kind"] == "p1" and len(I["cells"]) >= (1 << 20))
+                    else "coalesced" if W["kind"] == "p2" else "atomic")
     kernel_key = f"{args.workload}:{resolved}"
     traffic = load_traffic(kernel_key)
     out = {

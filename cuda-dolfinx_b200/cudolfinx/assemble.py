@@ -145,12 +145,16 @@ class CUDAAssembler:
         """Assemble a bilinear form into a device CSR matrix (not finalised).
 
         ``variant``: "auto" (block variant for P1 on meshes of >= 2^20 cells,
-        atomic scatter otherwise), "deterministic" (bitwise reproducible:
-        ordered tile gather for P1/P2, sorted-slot otherwise), "atomic"
-        (FP64-atomic scatter), "sorted-slot" (global sorted-slot reduction),
-        "block" (Morton cell blocks combined in shared memory, P1/P2), "tile"
-        (owner-computes row tiles, P1/P2), "row-gather" (P1), "atomic-full"
-        (atomic scatter into both triangles, the reference's scheme).
+        coalesced scatter for P2 stiffness, atomic scatter otherwise),
+        "deterministic" (bitwise reproducible: ordered tile gather for P1/P2,
+        sorted-slot otherwise), "atomic" (FP64-atomic scatter, one thread's
+        reductions per cell), "coalesced" (P2: a warp's reductions issued row
+        by row from shared memory), "grouped" (P2: one reduction per distinct
+        slot of 48-cell groups), "sorted-slot" (global sorted-slot
+        reduction), "block" (Morton cell blocks combined in shared memory,
+        P1/P2), "tile" (owner-computes row tiles, P1/P2), "row-gather" (P1),
+        "atomic-full" (atomic scatter into both triangles, the reference's
+        scheme).
         ``deterministic=True`` is the same as variant="deterministic"."""
         if variant not in _lib.VARIANT_FLAGS:
             raise ValueError(f"unknown variant {variant!r}; expected one of {sorted(_lib.VARIANT_FLAGS)}")
