@@ -932,7 +932,8 @@ int fe_assemble_matrix(fe_form a, double* values, fe_bc bc0, fe_bc bc1, double d
       return;
     }
     if (flags & FE_ASM_COALESCED)
-      FE_REQUIRE(a->kind == FE_FORM_P2_STIFFNESS, "the coalesced variant supports P2 stiffness only");
+      FE_REQUIRE(a->kind == FE_FORM_P2_STIFFNESS || a->kind == FE_FORM_VP2_ELASTICITY,
+                 "the coalesced variant supports P2 stiffness and vector-P2 elasticity");
     if (flags & FE_ASM_GROUPED) {
       FE_REQUIRE(grouped_supported(*a), "the grouped variant supports P2 stiffness on an unrestricted pattern");
       if (assemble_matrix_grouped(*a, values, bc0, bc1, zero, st)) {
@@ -982,7 +983,13 @@ int fe_assemble_matrix(fe_form a, double* values, fe_bc bc0, fe_bc bc1, double d
     // the atomic path: 0.73 instead of 0.85 ms; P1 n=32: equal).  For P2 the
     // pass costs what the halved reductions save (n=96: 2.80 ms either way),
     // so it keeps both reductions, as does FE_ASM_FULL_SCATTER for every form.
-    const bool upper = zero && !view && !(flags & FE_ASM_FULL_SCATTER) &&
+    // P2 stiffness and vector-P2 elasticity by default with warp-coalesced
+    // reductions (measured on B200 at P2 n=96: 2.44 ms per matrix call against
+    // 2.81 ms for the thread-per-cell reductions, which FE_ASM_ATOMIC keeps)
+    const bool coalesced = (flags & FE_ASM_COALESCED) ||
+                           (!(flags & FE_ASM_ATOMIC) && !view &&
+                            (a->kind == FE_FORM_P2_STIFFNESS || a->kind == FE_FORM_VP2_ELASTICITY));
+    const bool upper = !coalesced && zero && !view && !(flags & FE_ASM_FULL_SCATTER) &&
                        (a->kind == FE_FORM_VP2_ELASTICITY || a->kind == FE_FORM_P3_STIFFNESS ||
                         a->kind == FE_FORM_P1_STIFFNESS || a->kind == FE_FORM_P1_MASS ||
                         a->kind == FE_FORM_VP2_MASS) && a->V0 == a->V1 &&
@@ -1009,13 +1016,7 @@ int fe_assemble_matrix(fe_form a, double* values, fe_bc bc0, fe_bc bc1, double d
     L.upper = upper ? 1 : 0;
     L.cta_cells = a->launch_cells;
     L.stage = a->launch_stage;
-    // P2 stiffness by default with the warp-coalesced reductions (measured on
-    // B200 at P2 n=96: 2.44 ms per matrix call against 2.81 ms for the
-    // thread-per-cell reductions, which FE_ASM_ATOMIC keeps)
-    L.coalesced = ((flags & FE_ASM_COALESCED) ||
-                   (!(flags & FE_ASM_ATOMIC) && !view && a->kind == FE_FORM_P2_STIFFNESS))
-                      ? 1
-                      : 0;
+    L.coalesced = coalesced ? 1 : 0;
     launch_matrix_atomic(L, st);
     if (upper) launch_mirror_lower(*a->sp, values, st);
     if (bc0) launch_set_diagonal(*a->sp, *bc0, diagonal, values, st);

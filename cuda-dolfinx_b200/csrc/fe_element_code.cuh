@@ -1019,6 +1019,160 @@ __device__ __forceinline__ void p2_block_upper(const T* W, Emit&& emit) {
   }
 }
 
+// int_ref d_p phi_i d_q phi_j of the P2 basis, index (i*10 + j)*9 + p*3 + q.
+__device__ const double kP2GradGrad[900] = {
+    0x1.999999999999ap-4, 0x1.999999999999ap-4, 0x1.999999999999ap-4, 0x1.999999999999ap-4, 0x1.999999999999ap-4, 0x1.999999999999ap-4,
+    0x1.999999999999ap-4, 0x1.999999999999ap-4, 0x1.999999999999ap-4, 0x1.1111111111111p-5, 0x0.0p+0, 0x0.0p+0,
+    0x1.1111111111111p-5, 0x0.0p+0, 0x0.0p+0, 0x1.1111111111111p-5, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x1.1111111111111p-5, 0x0.0p+0, 0x0.0p+0, 0x1.1111111111111p-5, 0x0.0p+0,
+    0x0.0p+0, 0x1.1111111111111p-5, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.1111111111111p-5,
+    0x0.0p+0, 0x0.0p+0, 0x1.1111111111111p-5, 0x0.0p+0, 0x0.0p+0, 0x1.1111111111111p-5,
+    0x0.0p+0, 0x1.1111111111111p-5, 0x1.1111111111111p-5, 0x0.0p+0, 0x1.1111111111111p-5, 0x1.1111111111111p-5,
+    0x0.0p+0, 0x1.1111111111111p-5, 0x1.1111111111111p-5, 0x1.1111111111111p-5, 0x0.0p+0, 0x1.1111111111111p-5,
+    0x1.1111111111111p-5, 0x0.0p+0, 0x1.1111111111111p-5, 0x1.1111111111111p-5, 0x0.0p+0, 0x1.1111111111111p-5,
+    0x1.1111111111111p-5, 0x1.1111111111111p-5, 0x0.0p+0, 0x1.1111111111111p-5, 0x1.1111111111111p-5, 0x0.0p+0,
+    0x1.1111111111111p-5, 0x1.1111111111111p-5, 0x0.0p+0, -0x1.1111111111111p-5, -0x1.1111111111111p-5, -0x1.1111111111111p-3,
+    -0x1.1111111111111p-5, -0x1.1111111111111p-5, -0x1.1111111111111p-3, -0x1.1111111111111p-5, -0x1.1111111111111p-5, -0x1.1111111111111p-3,
+    -0x1.1111111111111p-5, -0x1.1111111111111p-3, -0x1.1111111111111p-5, -0x1.1111111111111p-5, -0x1.1111111111111p-3, -0x1.1111111111111p-5,
+    -0x1.1111111111111p-5, -0x1.1111111111111p-3, -0x1.1111111111111p-5, -0x1.1111111111111p-3, -0x1.1111111111111p-5, -0x1.1111111111111p-5,
+    -0x1.1111111111111p-3, -0x1.1111111111111p-5, -0x1.1111111111111p-5, -0x1.1111111111111p-3, -0x1.1111111111111p-5, -0x1.1111111111111p-5,
+    0x1.1111111111111p-5, 0x1.1111111111111p-5, 0x1.1111111111111p-5, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.999999999999ap-4, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, -0x1.1111111111111p-5, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, -0x1.1111111111111p-5,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, -0x1.1111111111111p-5, -0x1.1111111111111p-5, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, -0x1.1111111111111p-5, 0x0.0p+0, 0x1.999999999999ap-4,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    -0x1.1111111111111p-5, 0x1.999999999999ap-4, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.1111111111111p-5, 0x1.1111111111111p-5, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x1.1111111111111p-5, 0x0.0p+0, 0x1.1111111111111p-5, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, -0x1.1111111111111p-3, -0x1.999999999999ap-4, -0x1.999999999999ap-4,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.1111111111111p-5, 0x1.1111111111111p-5, 0x1.1111111111111p-5,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    -0x1.1111111111111p-5, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.999999999999ap-4, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, -0x1.1111111111111p-5, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, -0x1.1111111111111p-5, 0x1.999999999999ap-4,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    -0x1.1111111111111p-5, 0x0.0p+0, -0x1.1111111111111p-5, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.999999999999ap-4, -0x1.1111111111111p-5, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x1.1111111111111p-5, 0x1.1111111111111p-5, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, -0x1.999999999999ap-4, -0x1.1111111111111p-3, -0x1.999999999999ap-4,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x1.1111111111111p-5, 0x1.1111111111111p-5, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x1.1111111111111p-5, 0x1.1111111111111p-5, 0x1.1111111111111p-5, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, -0x1.1111111111111p-5, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, -0x1.1111111111111p-5, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.999999999999ap-4,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x1.999999999999ap-4, -0x1.1111111111111p-5, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.999999999999ap-4, 0x0.0p+0, -0x1.1111111111111p-5,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    -0x1.1111111111111p-5, -0x1.1111111111111p-5, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, -0x1.999999999999ap-4, -0x1.999999999999ap-4, -0x1.1111111111111p-3,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x1.1111111111111p-5, 0x0.0p+0, 0x1.1111111111111p-5, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.1111111111111p-5, 0x1.1111111111111p-5,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.1111111111111p-5, 0x1.1111111111111p-5, 0x1.1111111111111p-5,
+    0x1.1111111111111p-5, 0x1.1111111111111p-5, 0x1.1111111111111p-5, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    -0x1.1111111111111p-5, 0x0.0p+0, 0x0.0p+0, -0x1.1111111111111p-5, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, -0x1.1111111111111p-5, 0x0.0p+0,
+    0x0.0p+0, 0x1.999999999999ap-4, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x1.999999999999ap-4, 0x0.0p+0, 0x0.0p+0, -0x1.1111111111111p-5,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.1111111111111p-2, 0x1.1111111111111p-3,
+    0x0.0p+0, 0x1.1111111111111p-3, 0x1.1111111111111p-2, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x1.1111111111111p-2, 0x0.0p+0, 0x1.1111111111111p-3, 0x1.1111111111111p-3, 0x0.0p+0, 0x1.1111111111111p-3,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.1111111111111p-3, 0x1.1111111111111p-3, 0x0.0p+0,
+    0x1.1111111111111p-2, 0x1.1111111111111p-3, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    -0x1.1111111111111p-2, -0x1.1111111111111p-2, -0x1.1111111111111p-3, -0x1.1111111111111p-3, -0x1.1111111111111p-3, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, -0x1.1111111111111p-3, 0x0.0p+0, -0x1.1111111111111p-3,
+    -0x1.1111111111111p-2, -0x1.1111111111111p-3, -0x1.1111111111111p-2, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, -0x1.1111111111111p-3, -0x1.1111111111111p-3, 0x0.0p+0, -0x1.1111111111111p-3, -0x1.1111111111111p-3,
+    0x1.1111111111111p-5, 0x1.1111111111111p-5, 0x1.1111111111111p-5, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x1.1111111111111p-5, 0x1.1111111111111p-5, 0x1.1111111111111p-5, -0x1.1111111111111p-5, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.999999999999ap-4, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, -0x1.1111111111111p-5, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, -0x1.1111111111111p-5, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.999999999999ap-4,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, -0x1.1111111111111p-5,
+    0x0.0p+0, 0x1.1111111111111p-2, 0x1.1111111111111p-3, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x1.1111111111111p-3, 0x1.1111111111111p-3, 0x1.1111111111111p-2, 0x0.0p+0, 0x1.1111111111111p-3,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.1111111111111p-3, 0x0.0p+0, 0x1.1111111111111p-2,
+    0x1.1111111111111p-3, 0x1.1111111111111p-3, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x1.1111111111111p-3, 0x1.1111111111111p-2, 0x0.0p+0, -0x1.1111111111111p-2, -0x1.1111111111111p-2, -0x1.1111111111111p-3,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, -0x1.1111111111111p-3, -0x1.1111111111111p-3, 0x0.0p+0,
+    -0x1.1111111111111p-3, 0x0.0p+0, -0x1.1111111111111p-3, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    -0x1.1111111111111p-3, 0x0.0p+0, -0x1.1111111111111p-3, 0x0.0p+0, -0x1.1111111111111p-3, -0x1.1111111111111p-3,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, -0x1.1111111111111p-3, -0x1.1111111111111p-2, -0x1.1111111111111p-2,
+    0x1.1111111111111p-5, 0x1.1111111111111p-5, 0x1.1111111111111p-5, 0x1.1111111111111p-5, 0x1.1111111111111p-5, 0x1.1111111111111p-5,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, -0x1.1111111111111p-5, 0x0.0p+0, 0x0.0p+0,
+    0x1.999999999999ap-4, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x1.999999999999ap-4, 0x0.0p+0, 0x0.0p+0, -0x1.1111111111111p-5, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, -0x1.1111111111111p-5,
+    0x0.0p+0, 0x0.0p+0, -0x1.1111111111111p-5, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x1.1111111111111p-3, 0x1.1111111111111p-2, 0x0.0p+0, 0x1.1111111111111p-3, 0x1.1111111111111p-3,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.1111111111111p-3, 0x0.0p+0, 0x1.1111111111111p-3,
+    0x1.1111111111111p-3, 0x0.0p+0, 0x1.1111111111111p-2, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x1.1111111111111p-2, 0x1.1111111111111p-3, 0x0.0p+0, 0x1.1111111111111p-3, 0x1.1111111111111p-2, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, -0x1.1111111111111p-3, -0x1.1111111111111p-3, 0x0.0p+0,
+    -0x1.1111111111111p-3, -0x1.1111111111111p-3, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    -0x1.1111111111111p-2, -0x1.1111111111111p-3, -0x1.1111111111111p-2, -0x1.1111111111111p-3, 0x0.0p+0, -0x1.1111111111111p-3,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, -0x1.1111111111111p-3, -0x1.1111111111111p-3,
+    -0x1.1111111111111p-3, -0x1.1111111111111p-2, -0x1.1111111111111p-2, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    -0x1.1111111111111p-5, -0x1.1111111111111p-5, -0x1.1111111111111p-5, -0x1.1111111111111p-5, -0x1.1111111111111p-5, -0x1.1111111111111p-5,
+    -0x1.1111111111111p-3, -0x1.1111111111111p-3, -0x1.1111111111111p-3, 0x1.1111111111111p-5, 0x0.0p+0, 0x0.0p+0,
+    0x1.1111111111111p-5, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x1.1111111111111p-5, 0x0.0p+0, 0x0.0p+0, 0x1.1111111111111p-5, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, -0x1.999999999999ap-4,
+    0x0.0p+0, 0x0.0p+0, -0x1.999999999999ap-4, 0x0.0p+0, 0x0.0p+0, -0x1.1111111111111p-3,
+    0x0.0p+0, -0x1.1111111111111p-2, -0x1.1111111111111p-3, 0x0.0p+0, -0x1.1111111111111p-2, -0x1.1111111111111p-3,
+    0x0.0p+0, -0x1.1111111111111p-3, 0x0.0p+0, -0x1.1111111111111p-2, 0x0.0p+0, -0x1.1111111111111p-3,
+    -0x1.1111111111111p-2, 0x0.0p+0, -0x1.1111111111111p-3, -0x1.1111111111111p-3, 0x0.0p+0, 0x0.0p+0,
+    -0x1.1111111111111p-3, -0x1.1111111111111p-3, 0x0.0p+0, -0x1.1111111111111p-3, -0x1.1111111111111p-3, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.1111111111111p-2, 0x1.1111111111111p-2, 0x1.1111111111111p-3,
+    0x1.1111111111111p-2, 0x1.1111111111111p-2, 0x1.1111111111111p-3, 0x1.1111111111111p-3, 0x1.1111111111111p-3, 0x1.1111111111111p-2,
+    0x1.1111111111111p-3, 0x0.0p+0, 0x1.1111111111111p-3, 0x1.1111111111111p-3, 0x0.0p+0, 0x1.1111111111111p-3,
+    0x0.0p+0, 0x1.1111111111111p-3, 0x0.0p+0, 0x0.0p+0, 0x1.1111111111111p-3, 0x1.1111111111111p-3,
+    0x0.0p+0, 0x1.1111111111111p-3, 0x1.1111111111111p-3, 0x1.1111111111111p-3, 0x0.0p+0, 0x0.0p+0,
+    -0x1.1111111111111p-5, -0x1.1111111111111p-5, -0x1.1111111111111p-5, -0x1.1111111111111p-3, -0x1.1111111111111p-3, -0x1.1111111111111p-3,
+    -0x1.1111111111111p-5, -0x1.1111111111111p-5, -0x1.1111111111111p-5, 0x1.1111111111111p-5, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.1111111111111p-5, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, -0x1.999999999999ap-4, 0x0.0p+0, 0x0.0p+0, -0x1.1111111111111p-3, 0x0.0p+0,
+    0x0.0p+0, -0x1.999999999999ap-4, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.1111111111111p-5,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.1111111111111p-5,
+    0x0.0p+0, -0x1.1111111111111p-3, -0x1.1111111111111p-2, 0x0.0p+0, 0x0.0p+0, -0x1.1111111111111p-3,
+    0x0.0p+0, -0x1.1111111111111p-3, -0x1.1111111111111p-2, -0x1.1111111111111p-3, 0x0.0p+0, -0x1.1111111111111p-3,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, -0x1.1111111111111p-3, 0x0.0p+0, -0x1.1111111111111p-3,
+    -0x1.1111111111111p-2, -0x1.1111111111111p-3, 0x0.0p+0, -0x1.1111111111111p-3, 0x0.0p+0, 0x0.0p+0,
+    -0x1.1111111111111p-2, -0x1.1111111111111p-3, 0x0.0p+0, 0x1.1111111111111p-3, 0x1.1111111111111p-3, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x1.1111111111111p-3, 0x1.1111111111111p-3, 0x1.1111111111111p-3, 0x0.0p+0,
+    0x1.1111111111111p-2, 0x1.1111111111111p-3, 0x1.1111111111111p-2, 0x1.1111111111111p-3, 0x1.1111111111111p-2, 0x1.1111111111111p-3,
+    0x1.1111111111111p-2, 0x1.1111111111111p-3, 0x1.1111111111111p-2, 0x0.0p+0, 0x1.1111111111111p-3, 0x1.1111111111111p-3,
+    0x1.1111111111111p-3, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.1111111111111p-3, 0x1.1111111111111p-3,
+    -0x1.1111111111111p-3, -0x1.1111111111111p-3, -0x1.1111111111111p-3, -0x1.1111111111111p-5, -0x1.1111111111111p-5, -0x1.1111111111111p-5,
+    -0x1.1111111111111p-5, -0x1.1111111111111p-5, -0x1.1111111111111p-5, -0x1.1111111111111p-3, 0x0.0p+0, 0x0.0p+0,
+    -0x1.999999999999ap-4, 0x0.0p+0, 0x0.0p+0, -0x1.999999999999ap-4, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.1111111111111p-5, 0x0.0p+0,
+    0x0.0p+0, 0x1.1111111111111p-5, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x1.1111111111111p-5, 0x0.0p+0, 0x0.0p+0, 0x1.1111111111111p-5,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, -0x1.1111111111111p-3, -0x1.1111111111111p-3,
+    0x0.0p+0, -0x1.1111111111111p-3, -0x1.1111111111111p-3, 0x0.0p+0, 0x0.0p+0, -0x1.1111111111111p-3,
+    -0x1.1111111111111p-3, 0x0.0p+0, -0x1.1111111111111p-2, -0x1.1111111111111p-3, 0x0.0p+0, -0x1.1111111111111p-2,
+    0x0.0p+0, -0x1.1111111111111p-3, 0x0.0p+0, -0x1.1111111111111p-3, -0x1.1111111111111p-2, 0x0.0p+0,
+    -0x1.1111111111111p-3, -0x1.1111111111111p-2, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.1111111111111p-3,
+    0x1.1111111111111p-3, 0x1.1111111111111p-3, 0x0.0p+0, 0x1.1111111111111p-3, 0x1.1111111111111p-3, 0x0.0p+0,
+    0x0.0p+0, 0x1.1111111111111p-3, 0x0.0p+0, 0x1.1111111111111p-3, 0x0.0p+0, 0x1.1111111111111p-3,
+    0x1.1111111111111p-3, 0x0.0p+0, 0x1.1111111111111p-3, 0x1.1111111111111p-2, 0x1.1111111111111p-3, 0x1.1111111111111p-3,
+    0x1.1111111111111p-3, 0x1.1111111111111p-2, 0x1.1111111111111p-2, 0x1.1111111111111p-3, 0x1.1111111111111p-2, 0x1.1111111111111p-2,
+};
+
 // P1 mass, cellwise-constant coefficient: s = c * |det J|; emit(i, j, value), i <= j.
 template <typename T, typename Emit>
 __device__ __forceinline__ void p1_mass_const(T s, Emit&& emit) {

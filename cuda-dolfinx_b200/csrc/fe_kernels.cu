@@ -648,6 +648,146 @@ __global__ void __launch_bounds__(kBlock) k_mat_vp2_atomic(const MatArgs a) {
 }
 
 // ---------------------------------------------------------------------------
+// Vector-P2 elasticity with the reductions coalesced per warp (the vector-P2
+// default).  Entry (row (i,a), column (j,b)) of the 30x30 element matrix is
+// sum_pq C_ij^pq W^ab_pq with C_ij^pq = int_ref d_p phi_i d_q phi_j (the
+// table kP2GradGrad) and W^ab the 9 geometric weights of component block
+// (a, b) (elasticity_weights).  One thread per cell computes the 6 weight
+// blocks a <= b into shared memory; the warp then walks its 32 cells: one
+// instruction per element row (i, a), lane 3j + b on column (j, b), so the
+// 30 reductions land on the 10 consecutive slot triples of one CSR row
+// (~2 per 32-byte sector, against 1 for the thread-per-cell scatter) and no
+// transpose pass is needed.  Every entry is evaluated from its
+// upper-triangle form (the pair's smaller (node, component) as the row), in
+// one term order, so the element matrix is exactly symmetric.  With FP32
+// weights the diagonal entries of each 3x3 node block are, as in the
+// thread-per-cell kernel, minus the FP64 sum of the block row's FP32
+// off-diagonal entries (exact row sums: rigid translations stay in the null
+// space); by symmetry each lane accumulates that sum as its column sum.
+// ---------------------------------------------------------------------------
+constexpr int kVCoalThreads = 64;
+
+template <typename T>
+__global__ void __launch_bounds__(kVCoalThreads) k_mat_vp2_coal(const MatArgs a) {
+  constexpr int NT = kVCoalThreads;
+  constexpr bool kRowSums = sizeof(T) == 4;
+  __shared__ T sC[900];
+  __shared__ T sW[NT * 54];                         // per cell: blocks (00,11,22,01,02,12) x 9
+  __shared__ __align__(16) uint8_t spos[NT * 100];
+  __shared__ int32_t srp[NT * 10];                  // scalar row 3R of local node i (component 0)
+  __shared__ int32_t sL[NT * 10];                   // its length (the rows 3R+1, 3R+2 follow)
+  __shared__ uint32_t smr[NT], smc[NT];             // masked rows / columns, bit 3i + component
+  const int tid = threadIdx.x, lane = tid & 31, w0 = tid & ~31;
+  for (int t = tid; t < 900; t += NT) sC[t] = (T)kP2GradGrad[t];
+  const int64_t c0 = blockIdx.x * (int64_t)NT;
+  const int64_t left = a.num_cells - c0;
+  const int ncell = left < NT ? (int)left : NT;
+  const int wcells = ncell - w0 < 0 ? 0 : (ncell - w0 < 32 ? ncell - w0 : 32);
+  {
+    // each warp stages its own cells' byte maps ((c0 + w0) * 100 is a multiple of 16)
+    const uint4* src = reinterpret_cast<const uint4*>(a.pos + (c0 + w0) * 100);
+    uint4* dst = reinterpret_cast<uint4*>(spos + w0 * 100);
+    const int nvec = (wcells * 100 + 15) / 16;
+    for (int t = lane; t < nvec; t += 32) dst[t] = __ldg(src + t);
+  }
+  if (tid < ncell) {
+    const int64_t c = c0 + tid;
+    CellGeo g;
+    cell_geometry(a.x, load_geom(a.geom, c), g);
+    const double lam = coef_cell(a.c0, c), mu = coef_cell(a.c1, c);
+#pragma unroll 1
+    for (int blk = 0; blk < 6; ++blk) {
+      const int ca = blk < 3 ? blk : (blk == 5 ? 1 : 0);
+      const int cb = blk < 3 ? blk : (blk == 3 ? 1 : 2);
+      elasticity_weights<T>(g, lam, mu, ca, cb, sW + tid * 54 + blk * 9);
+    }
+    const int32_t* d0 = a.dofs0 + c * 10;
+    const int32_t* d1 = a.dofs1 + c * 10;
+    uint32_t mr = 0, mc = 0;
+#pragma unroll
+    for (int i = 0; i < 10; ++i) {
+      // masked rows / columns: BC dofs and nodes outside a restriction (-1)
+      const int R = __ldg(d0 + i), C = __ldg(d1 + i);
+      const int32_t r0 = R < 0 ? 0 : __ldg(a.row_ptr + 3 * R);
+      srp[tid * 10 + i] = r0;
+      sL[tid * 10 + i] = R < 0 ? 0 : __ldg(a.row_ptr + 3 * R + 1) - r0;
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        mr |= (R < 0 || (a.bc0 && __ldg(a.bc0 + 3 * R + q)) ? 1u : 0u) << (3 * i + q);
+        mc |= (C < 0 || (a.bc1 && __ldg(a.bc1 + 3 * C + q)) ? 1u : 0u) << (3 * i + q);
+      }
+    }
+    smr[tid] = mr;
+    smc[tid] = mc;
+  }
+  __syncthreads();  // the C table; the warp's own cells need only their warp
+  // lanes 30 and 31 run along (the shuffles below take the whole warp) on
+  // column (0, 0) without reducing
+  const bool lane_on = lane < 30;
+  const int j = lane_on ? lane / 3 : 0, b = lane_on ? lane - 3 * (lane / 3) : 0;
+  // stored block of components (u, v), u <= v
+  auto blk_of = [](int u, int v) { return u == v ? u : (u + v == 1 ? 3 : (u + v == 2 ? 4 : 5)); };
+  double* __restrict__ vals = a.values;
+  for (int q = w0; q < w0 + wcells; ++q) {
+    // W^{ab} and W^{ba} of this lane's column component b, for a = 0..2
+    const T* Wc = sW + q * 54;
+    T Wab[3][9], Wba[3][9];
+#pragma unroll
+    for (int ca = 0; ca < 3; ++ca) {
+      const int lo = ca < b ? ca : b, hi = ca < b ? b : ca;
+      const T* Wb = Wc + 9 * blk_of(lo, hi);
+#pragma unroll
+      for (int pq = 0; pq < 9; ++pq) {
+        const int tq = (pq % 3) * 3 + pq / 3;  // transposed index
+        Wab[ca][pq] = ca <= b ? Wb[pq] : Wb[tq];
+        Wba[ca][pq] = b <= ca ? Wb[pq] : Wb[tq];
+      }
+    }
+    const uint32_t mr = smr[q], mc = smc[q];
+    const bool cmask = !lane_on || ((mc >> (3 * j + b)) & 1u);
+    const int32_t* rq = srp + q * 10;
+    const int32_t* lq = sL + q * 10;
+    const uint8_t* pq8 = spos + q * 100;
+    double cs[3] = {0.0, 0.0, 0.0};
+#pragma unroll 1
+    for (int i = 0; i < 10; ++i) {
+      const int rs = rq[i], len = lq[i];
+      const int slot0 = rs + 3 * pq8[i * 10 + j] + b;
+#pragma unroll
+      for (int ca = 0; ca < 3; ++ca) {
+        // the pair's upper form: row (i, ca) when (i, ca) <= (j, b), else row (j, b)
+        const bool up = i < j || (i == j && ca <= b);
+        const T* Cp = sC + (up ? i * 10 + j : j * 10 + i) * 9;
+        T v = T(0);
+#pragma unroll
+        for (int pq = 0; pq < 9; ++pq) v = fma(Cp[pq], up ? Wab[ca][pq] : Wba[ca][pq], v);
+        if (kRowSums && i == j) continue;  // node-block diagonals come from the row sums
+        if (kRowSums) cs[ca] += (double)v;
+        if (!cmask && !((mr >> (3 * i + ca)) & 1u)) atomicAdd(vals + slot0 + ca * len, (double)v);
+      }
+    }
+    if constexpr (kRowSums) {
+      // cs[ca] = column sum of block (ca, b) at column j = row sum of block
+      // (b, ca) at row j (the element is exactly symmetric).  Entry (row
+      // (j, b), column (j, ca)) = -1/2 (row sum + column sum of block (b, ca)),
+      // the column sum being lane (j, ca)'s cs[b]: the node block stays
+      // symmetric and its rows sum to zero up to the FP32 rounding of one term
+      const int rs = rq[j], len = lq[j];
+      const int slot = rs + b * len + 3 * pq8[j * 10 + j];
+#pragma unroll
+      for (int ca = 0; ca < 3; ++ca) {
+        const int src = 3 * j + ca;
+        const double o0 = __shfl_sync(0xffffffffu, cs[0], src), o1 = __shfl_sync(0xffffffffu, cs[1], src),
+                     o2 = __shfl_sync(0xffffffffu, cs[2], src);
+        const double other = b == 0 ? o0 : (b == 1 ? o1 : o2);
+        if (lane_on && !((mr >> (3 * j + b)) & 1u) && !((mc >> (3 * j + ca)) & 1u))
+          atomicAdd(vals + slot + ca, -0.5 * (cs[ca] + other));
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Utilities
 // ---------------------------------------------------------------------------
 __global__ void k_zero(double* __restrict__ v, int64_t n) {
@@ -1591,8 +1731,16 @@ void launch_matrix_atomic(const MatLaunch& L, cudaStream_t s) {
       break;
     }
     case FE_FORM_VP2_ELASTICITY:
-      if (f32) k_mat_vp2_atomic<float><<<grid, kBlock, 0, s>>>(a);
-      else k_mat_vp2_atomic<double><<<grid, kBlock, 0, s>>>(a);
+      if (L.coalesced && !a.upper) {
+        auto k = f32 ? k_mat_vp2_coal<float> : k_mat_vp2_coal<double>;
+        FE_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                     cudaSharedmemCarveoutMaxShared));
+        k<<<grid_for(L.num_cells, kVCoalThreads), kVCoalThreads, 0, s>>>(a);
+      } else if (f32) {
+        k_mat_vp2_atomic<float><<<grid, kBlock, 0, s>>>(a);
+      } else {
+        k_mat_vp2_atomic<double><<<grid, kBlock, 0, s>>>(a);
+      }
       break;
     case FE_FORM_P1_MASS:
       if (a.c0.kind == FE_COEFF_P1) k_mat_mass<4, FE_COEFF_P1><<<grid, kBlock, 0, s>>>(a);

@@ -360,6 +360,14 @@ def gen() -> str:
                 exprs[(i, j)] = sum_expr('W', terms, 2)
         w(full_body(exprs, 10) if full else symmetric_body(exprs, 10))
         w("}\n\n")
+    # the same reference integrals as a table, for kernels that evaluate block
+    # entries lane by lane: kP2GradGrad[(i*10 + j)*9 + p*3 + q] = int_ref d_p phi_i d_q phi_j
+    w("// int_ref d_p phi_i d_q phi_j of the P2 basis, index (i*10 + j)*9 + p*3 + q.\n")
+    w("__device__ const double kP2GradGrad[900] = {\n")
+    vals = [lit(r_plain(p_, q_, i, j)) for i in range(10) for j in range(10) for p_ in range(3) for q_ in range(3)]
+    for k in range(0, 900, 6):
+        w("    " + ", ".join(vals[k:k + 6]) + ",\n")
+    w("};\n\n")
     w(mass_tables())
     w(facet_tables())
     w("}  // namespace fe\n")

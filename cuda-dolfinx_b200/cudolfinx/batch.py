@@ -26,7 +26,7 @@ from .la import CUDAMatrix
 CANDIDATES = {
     "P1_STIFFNESS": ("atomic", "block", "tile"),
     "P2_STIFFNESS": ("atomic", "block", "grouped", "coalesced"),
-    "VP2_ELASTICITY": ("atomic", "atomic-full"),
+    "VP2_ELASTICITY": ("coalesced", "atomic", "atomic-full"),
 }
 # launch shapes of the atomic scatter timed per form kind: (cells per CTA,
 # byte maps staged in shared memory)

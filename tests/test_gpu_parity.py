@@ -42,8 +42,10 @@ VARIANTS = ["auto", "atomic", "atomic-full", "tile", "deterministic", "sorted-sl
 def _supported(kind, variant):
     if variant == "row-gather":
         return kind in ("p1", "p1k")
-    if variant in ("grouped", "coalesced"):
+    if variant == "grouped":
         return kind == "p2"
+    if variant == "coalesced":
+        return kind in ("p2", "vp2")
     if variant in ("tile", "block"):
         return kind in ("p1", "p1k", "p2")
     return True
@@ -424,3 +426,23 @@ def test_block_variant_bc_paths(kind, n, bcs):
     bound = fo.matrix_bound(Ae, P["dofs"], P["dofs"], rp, col, 1, 1, m0, m1)
     ok, worst = tolerance_check(A.values.cpu().numpy(), ref, bound)
     assert ok, worst
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_vp2_coalesced_matches_atomic_and_is_symmetric(precision):
+    # the warp-coalesced vector-P2 kernel (default) against the thread-per-cell
+    # upper-triangle scatter: same values up to the summation order (FP64) or
+    # the FP32 rounding of the element entries; symmetric to rounding level
+    import scipy.sparse as sp
+    from scipy.sparse.linalg import norm as spnorm
+
+    P = fo.build_problem("vp2", 4, seed=13)
+    Rc = run_system(P, precision=precision, variant="coalesced")
+    Ra = run_system(P, precision=precision, variant="atomic")
+    assert np.array_equal(Rc["row_ptr"], Ra["row_ptr"]) and np.array_equal(Rc["col"], Ra["col"])
+    rel = np.linalg.norm(Rc["A"] - Ra["A"]) / np.linalg.norm(Ra["A"])
+    assert rel < (1e-14 if precision == "fp64" else 1e-6), rel
+    N = len(Rc["row_ptr"]) - 1
+    A = sp.csr_matrix((Rc["A"], Rc["col"], Rc["row_ptr"]), shape=(N, N))
+    asym = spnorm(A - A.T) / spnorm(A)
+    assert asym < 1e-14, asym
