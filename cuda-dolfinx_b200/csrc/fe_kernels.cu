@@ -696,7 +696,7 @@ __global__ void __launch_bounds__(kVCoalThreads) k_mat_vp2_coal(const MatArgs a)
     cell_geometry(a.x, load_geom(a.geom, c), g);
     const double lam = coef_cell(a.c0, c), mu = coef_cell(a.c1, c);
 #pragma unroll 1
-    for (int blk = 0; blk < 6; ++blk) {
+    for (int blk = 0; blk < 6; ++blk) {  // rolled: unrolled it takes 144 registers (FP32) instead of 108
       const int ca = blk < 3 ? blk : (blk == 5 ? 1 : 0);
       const int cb = blk < 3 ? blk : (blk == 3 ? 1 : 2);
       elasticity_weights<T>(g, lam, mu, ca, cb, sW + tid * 54 + blk * 9);
@@ -753,14 +753,24 @@ __global__ void __launch_bounds__(kVCoalThreads) k_mat_vp2_coal(const MatArgs a)
     for (int i = 0; i < 10; ++i) {
       const int rs = rq[i], len = lq[i];
       const int slot0 = rs + 3 * pq8[i * 10 + j] + b;
+      // the pair's upper form takes row (i, ca) when (i, ca) <= (j, b), else
+      // row (j, b): its C row is C_ij for i < j and C_ji for i > j (the same
+      // row for i == j), whatever the components
+      const T* Cp = sC + (i <= j ? i * 10 + j : j * 10 + i) * 9;
+      T cr[9];
+#pragma unroll
+      for (int pq = 0; pq < 9; ++pq) cr[pq] = Cp[pq];
 #pragma unroll
       for (int ca = 0; ca < 3; ++ca) {
-        // the pair's upper form: row (i, ca) when (i, ca) <= (j, b), else row (j, b)
         const bool up = i < j || (i == j && ca <= b);
-        const T* Cp = sC + (up ? i * 10 + j : j * 10 + i) * 9;
-        T v = T(0);
+        // two partial sums (a fixed order, so both lanes of a symmetric pair
+        // compute the same value)
+        T v0 = T(0), v1 = T(0);
 #pragma unroll
-        for (int pq = 0; pq < 9; ++pq) v = fma(Cp[pq], up ? Wab[ca][pq] : Wba[ca][pq], v);
+        for (int pq = 0; pq < 9; pq += 2) v0 = fma(cr[pq], up ? Wab[ca][pq] : Wba[ca][pq], v0);
+#pragma unroll
+        for (int pq = 1; pq < 9; pq += 2) v1 = fma(cr[pq], up ? Wab[ca][pq] : Wba[ca][pq], v1);
+        const T v = v0 + v1;
         if (kRowSums && i == j) continue;  // node-block diagonals come from the row sums
         if (kRowSums) cs[ca] += (double)v;
         if (!cmask && !((mr >> (3 * i + ca)) & 1u)) atomicAdd(vals + slot0 + ca * len, (double)v);
