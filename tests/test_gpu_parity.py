@@ -446,3 +446,47 @@ def test_vp2_coalesced_matches_atomic_and_is_symmetric(precision):
     A = sp.csr_matrix((Rc["A"], Rc["col"], Rc["row_ptr"]), shape=(N, N))
     asym = spnorm(A - A.T) / spnorm(A)
     assert asym < 1e-14, asym
+
+
+@pytest.mark.parametrize("renumber", [False, True])
+def test_p2_scatter_with_folded_zero_pass_over_several_chunks(renumber):
+    # P2 n=24 (82,944 cells: two 65,536-cell chunks of the coalesced scatter
+    # with the zero pass folded in).  With a random cell order and dof
+    # numbering every chunk's first-touched rows come as many short slot
+    # ranges.  Assembled twice into the same values, so the second call must
+    # zero what the first wrote.
+    from conftest import ensure_library
+    ensure_library()
+    import cudolfinx as cx
+    from cudolfinx import fem
+
+    n = 24
+    P = fo.build_problem("p2", n, seed=17)
+    rng = np.random.default_rng(5)
+    cells = P["cells"][rng.permutation(len(P["cells"]))] if renumber else P["cells"]
+    mesh = fem.Mesh(P["coords"], cells, grid_n=n)
+    V = fem.functionspace(mesh, ("P", 2))
+    dp = rng.permutation(V.num_nodes).astype(np.int32) if renumber else np.arange(V.num_nodes, dtype=np.int32)
+    if renumber:
+        V.dofs = np.ascontiguousarray(dp[V.dofs])
+    V1 = fem.functionspace(mesh, ("P", 1))
+    k = fem.Function(V1, P["k"])
+    bdofs = np.sort(dp[P["bc_dofs"]]).astype(np.int32)
+    g = np.zeros(V.num_dofs)
+    g[dp] = P["g"]
+    bc = fem.dirichletbc(fem.Function(V, g), bdofs)
+    asm = cx.CUDAAssembler()
+    a = cx.form(fem.stiffness(V, k))
+    A = asm.assemble_matrix(a, bcs=[bc])
+    asm.assemble_matrix(a, A, bcs=[bc])
+    A.assemble()
+    rp, col = A.sparsity.to_host()
+    rp_o, col_o = fo.sparsity(V.dofs, V.dofs, V.num_nodes)
+    assert np.array_equal(rp, rp_o) and np.array_equal(col, col_o)
+    Ae = fo.p2_stiffness(P["coords"], cells, P["k"][cells])
+    mk = np.zeros(V.num_dofs, dtype=np.uint8)
+    mk[bdofs] = 1
+    ref = fo.assemble_matrix(Ae, V.dofs, V.dofs, rp_o, col_o, 1, 1, mk, mk, 1.0, bdofs)
+    ok, worst = tolerance_check(A.values.cpu().numpy(), ref,
+                                fo.matrix_bound(Ae, V.dofs, V.dofs, rp_o, col_o, 1, 1, mk, mk))
+    assert ok, worst
