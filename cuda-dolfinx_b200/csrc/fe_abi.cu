@@ -994,11 +994,7 @@ int fe_assemble_matrix(fe_form a, double* values, fe_bc bc0, fe_bc bc1, double d
                         a->kind == FE_FORM_P1_STIFFNESS || a->kind == FE_FORM_P1_MASS ||
                         a->kind == FE_FORM_VP2_MASS) && a->V0 == a->V1 &&
                        bc0 == bc1 && ensure_mirror(*a->sp, st, a->V0->bs);
-    // P2 stiffness (staged, coalesced): the zero pass runs inside the scatter,
-    // each chunk's first-touched rows zeroed one chunk ahead of its cells
-    const bool zero_fused = coalesced && zero && !view && a->kind == FE_FORM_P2_STIFFNESS &&
-                            a->launch_stage != 0 && a->V0->bs == 1;
-    if (zero && !zero_fused) launch_zero(values, a->sp->nnz, st);
+    if (zero) launch_zero(values, a->sp->nnz, st);
     MatLaunch L{};
     L.kind = a->kind;
     L.precision = a->precision;
@@ -1021,8 +1017,7 @@ int fe_assemble_matrix(fe_form a, double* values, fe_bc bc0, fe_bc bc1, double d
     L.cta_cells = a->launch_cells;
     L.stage = a->launch_stage;
     L.coalesced = coalesced ? 1 : 0;
-    if (zero_fused) launch_p2_coal_zero_fused(*a, L, st);
-    else launch_matrix_atomic(L, st);
+    launch_matrix_atomic(L, st);
     if (upper) launch_mirror_lower(*a->sp, values, st);
     if (bc0) launch_set_diagonal(*a->sp, *bc0, diagonal, values, st);
   });

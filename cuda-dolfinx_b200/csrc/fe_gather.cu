@@ -29,7 +29,6 @@ void fe::reset_gather_plan(fe_form_s& f) {
   reset_row_plan(f);
   reset_block_plan(f);
   reset_batch_plan(f);
-  f.zplan.reset();  // slot ranges of the old pattern
 }
 
 namespace fe {

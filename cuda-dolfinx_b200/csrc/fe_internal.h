@@ -202,10 +202,7 @@ struct fe_form_s {
   // grouped-summation plan (fe_group.cu); built on first use
   struct GroupPlan;
   std::unique_ptr<GroupPlan> groups;
-  // zero items of the coalesced P2 scatter with the zero pass folded in
-  // (fe_kernels.cu); built on first use
-  struct ZeroPlan;
-  std::unique_ptr<ZeroPlan> zplan;
+
   bool group_plan_failed = false;  // the mesh has no repeated group structure
   fe_form_s();
   ~fe_form_s();
@@ -294,15 +291,6 @@ struct fe_form_s::BlockPlan {
                                       // whole warps and stored in the kernel's lane order
 };
 
-struct fe_form_s::ZeroPlan {
-  int32_t nitems = 0, nchunks = 0, tiles_per_chunk = 0;
-  fe::DevBuf<int2> zr;          // zero items: [begin, end) slot ranges
-  fe::DevBuf<int32_t> zchunk;   // chunk of each zero item
-  fe::DevBuf<int32_t> sched;    // work order: >= 0 cell tile, < 0 zero item -1 - z
-  fe::DevBuf<uint32_t> zneed;   // [nchunks] zero items of each chunk
-  fe::DevBuf<uint32_t> counter; // [1 + nchunks]: next item, zero items done per chunk
-};
-
 struct fe_form_s::GroupPlan {
   int64_t ngroups = 0, ntemplates = 0;
   fe::DevBuf<int32_t> tmpl_of;        // [groups] template of each group
@@ -382,9 +370,6 @@ void launch_build_slotmap(const fe_form_s& f, cudaStream_t s);
 void launch_build_view(const fe_form_s& f, const fe_sparsity_s& mono, int64_t row_offset, int64_t col_offset,
                        fe_sparsity_s& view, cudaStream_t s);
 void launch_matrix_atomic(const MatLaunch& a, cudaStream_t s);
-// P2 stiffness, coalesced reductions with the zero pass folded in (zero=true,
-// plain pattern); builds f.zplan on first use
-void launch_p2_coal_zero_fused(fe_form_s& f, const MatLaunch& a, cudaStream_t s);
 // diagonal of a cell bilinear form into b (no BCs)
 void launch_diagonal(const MatLaunch& a, double* b, int64_t num_values, cudaStream_t s);
 void launch_set_diagonal(const fe_sparsity_s& sp, const fe_bc_s& bc, double diagonal, double* values,

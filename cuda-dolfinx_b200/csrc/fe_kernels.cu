@@ -389,73 +389,6 @@ __global__ void __launch_bounds__(kCoalThreads, 7) k_mat_p2_coal(const MatArgs a
   p2_coal_tile<COEF, T, STAGE>(a, blockIdx.x * (int64_t)kCoalThreads, S);
 }
 
-// The coalesced scatter with the zero pass folded in (zero=true, plain
-// patterns).  The cells are cut in chunks of consecutive 64-cell tiles; the
-// plan lists, per chunk, the CSR slot ranges of the rows that chunk touches
-// first (in cell order).  CTAs take work items in a fixed order from a
-// counter -- zero(0), zero(1), tiles(0), zero(2), tiles(1), ... -- so each
-// chunk's rows are zeroed one chunk ahead of the cells that first reduce
-// into them, while the lines are still in L2 (the reductions hit instead of
-// reading the zeroed lines back from DRAM), and no separate pass writes the
-// whole value array.  A tile of chunk k waits (bounded) until every zero item
-// of chunks <= k is done; all of those were handed out before it to CTAs that
-// run them without waiting, so the waits end.
-struct ZeroArgs {
-  const int2* __restrict__ zr;       // zero items: [begin, end) slot ranges
-  const int32_t* __restrict__ zchunk;
-  const int32_t* __restrict__ sched; // >= 0: cell tile; < 0: zero item -1 - z
-  const uint32_t* __restrict__ zneed;
-  uint32_t* counter;                 // [0]: next item; [1 + k]: zero items of chunk k done
-  unsigned* err;
-  int32_t nitems, tiles_per_chunk;
-};
-
-constexpr long long kZeroWaitSpins = 1ll << 24;
-
-template <int COEF, typename T>
-__global__ void __launch_bounds__(kCoalThreads, 7) k_mat_p2_coal_zf(const MatArgs a, const ZeroArgs z) {
-  __shared__ P2CoalSmem<true> S;
-  __shared__ int32_t s_item;
-  __shared__ int32_t s_ready;  // chunks <= s_ready are zeroed (thread 0's view)
-  const int tid = threadIdx.x;
-  if (tid == 0) s_ready = -1;
-  for (;;) {
-    if (tid == 0) {
-      const uint32_t g = atomicAdd(z.counter, 1u);
-      s_item = g < (uint32_t)z.nitems ? __ldg(z.sched + g) : INT_MIN;
-    }
-    __syncthreads();
-    const int32_t item = s_item;
-    if (item == INT_MIN) break;
-    if (item < 0) {
-      const int zi = -1 - item;
-      const int2 r = __ldg(z.zr + zi);
-      for (int64_t q = r.x + tid; q < r.y; q += kCoalThreads) a.values[q] = 0.0;
-      __threadfence();  // each thread's zeros before the count
-      __syncthreads();
-      if (tid == 0) atomicAdd(z.counter + 1 + __ldg(z.zchunk + zi), 1u);
-    } else {
-      const int chunk = item / z.tiles_per_chunk;
-      if (tid == 0) {
-        for (int k = s_ready + 1; k <= chunk; ++k) {
-          const uint32_t need = __ldg(z.zneed + k);
-          long long spins = 0;
-          while (*(volatile uint32_t*)(z.counter + 1 + k) < need && spins < kZeroWaitSpins) {
-            __nanosleep(64);
-            ++spins;
-          }
-          if (spins >= kZeroWaitSpins) atomicOr(z.err, DEV_ERR_BARRIER);
-        }
-        if (chunk > s_ready) s_ready = chunk;
-        __threadfence();
-      }
-      __syncthreads();
-      p2_coal_tile<COEF, T, true>(a, (int64_t)item * kCoalThreads, S);
-    }
-    __syncthreads();  // shared memory and s_item are reused by the next item
-  }
-}
-
 // ---------------------------------------------------------------------------
 // Mass matrices c*u*v*dx (P1: K = 4, P2: K = 10), one thread per cell, FP64
 // atomics.  Only |det J| and the coefficient enter the element tensor.
@@ -1944,140 +1877,6 @@ bool ensure_mirror(fe_sparsity_s& sp, cudaStream_t s, int bs) {
   if (!ok) M->pairs.release();
   sp.mirror = std::move(M);
   return ok;
-}
-
-namespace {
-constexpr int32_t kZeroTilesPerChunk = 1024;  // 65,536 cells: its first-touched rows stay in L2
-constexpr int64_t kZeroItemSlots = 8192;      // doubles zeroed by one work item
-
-std::unique_ptr<fe_form_s::ZeroPlan> build_zero_plan(const fe_form_s& f) {
-  const int64_t C = f.mesh->num_cells;
-  const int K = f.V0->k;
-  const std::vector<int32_t>& D = f.V0->host;
-  const std::vector<int32_t>& rp = f.sp->host_row_ptr;
-  const int64_t nrows = f.sp->num_rows;
-  FE_REQUIRE((int64_t)rp.size() == nrows + 1 && f.V0->bs == 1 && (int64_t)D.size() == C * K,
-             "zero plan: unexpected pattern or dofmap");
-  const int64_t tiles = (C + kCoalThreads - 1) / kCoalThreads;
-  FE_REQUIRE(tiles < INT32_MAX, "zero plan: too many cells");
-  const int32_t nchunks = (int32_t)std::max<int64_t>(1, (tiles + kZeroTilesPerChunk - 1) / kZeroTilesPerChunk);
-  // first chunk (in cell order) that touches each row; untouched rows go to chunk 0
-  std::vector<int32_t> first(nrows, -1);
-  for (int64_t c = 0; c < C; ++c) {
-    const int32_t k = (int32_t)((c / kCoalThreads) / kZeroTilesPerChunk);
-    for (int i = 0; i < K; ++i) {
-      const int32_t r = D[c * K + i];
-      if (r >= 0 && r < nrows && first[r] < 0) first[r] = k;
-    }
-  }
-  // rows of each chunk, ascending (counting sort), merged into slot ranges
-  std::vector<int64_t> cnt(nchunks + 1, 0);
-  for (int64_t r = 0; r < nrows; ++r) ++cnt[1 + std::max(0, first[r])];
-  for (int32_t k = 0; k < nchunks; ++k) cnt[k + 1] += cnt[k];
-  std::vector<int32_t> rows(nrows);
-  {
-    std::vector<int64_t> at(cnt.begin(), cnt.end() - 1);
-    for (int64_t r = 0; r < nrows; ++r) rows[at[std::max(0, first[r])]++] = (int32_t)r;
-  }
-  std::vector<std::vector<int32_t>> zitems(nchunks);  // per chunk: indices into zr
-  std::vector<int2> zr;
-  std::vector<int32_t> zchunk;
-  for (int32_t k = 0; k < nchunks; ++k) {
-    int64_t u = cnt[k];
-    while (u < cnt[k + 1]) {
-      int64_t v = u + 1;
-      while (v < cnt[k + 1] && rows[v] == rows[v - 1] + 1) ++v;
-      for (int64_t b = rp[rows[u]], e = rp[rows[v - 1] + 1]; b < e; b += kZeroItemSlots) {
-        zitems[k].push_back((int32_t)zr.size());
-        zr.push_back(make_int2((int)b, (int)std::min<int64_t>(e, b + kZeroItemSlots)));
-        zchunk.push_back(k);
-      }
-      u = v;
-    }
-  }
-  // order: zero(0), zero(1), tiles(0), zero(2), tiles(1), zero(3), ...
-  std::vector<int32_t> sched;
-  auto zero_of = [&](int32_t k) {
-    if (k < nchunks)
-      for (int32_t z : zitems[k]) sched.push_back(-1 - z);
-  };
-  zero_of(0);
-  zero_of(1);
-  for (int32_t k = 0; k < nchunks; ++k) {
-    const int64_t t1 = std::min<int64_t>(tiles, (int64_t)(k + 1) * kZeroTilesPerChunk);
-    for (int64_t t = (int64_t)k * kZeroTilesPerChunk; t < t1; ++t) sched.push_back((int32_t)t);
-    zero_of(k + 2);
-  }
-  FE_REQUIRE(sched.size() < (size_t)INT32_MAX, "zero plan: too many work items");
-  std::vector<uint32_t> zneed(nchunks);
-  for (int32_t k = 0; k < nchunks; ++k) zneed[k] = (uint32_t)zitems[k].size();
-  auto P = std::make_unique<fe_form_s::ZeroPlan>();
-  P->nitems = (int32_t)sched.size();
-  P->nchunks = nchunks;
-  P->tiles_per_chunk = kZeroTilesPerChunk;
-  auto up = [](auto& d, const auto& h) {
-    using E = typename std::decay_t<decltype(h)>::value_type;
-    d.alloc(std::max<size_t>(1, h.size()));
-    if (!h.empty()) FE_CUDA(cudaMemcpy(d.p, h.data(), h.size() * sizeof(E), cudaMemcpyHostToDevice));
-  };
-  up(P->zr, zr);
-  up(P->zchunk, zchunk);
-  up(P->sched, sched);
-  up(P->zneed, zneed);
-  P->counter.alloc(1 + (size_t)nchunks);
-  return P;
-}
-}  // namespace
-
-void launch_p2_coal_zero_fused(fe_form_s& f, const MatLaunch& L, cudaStream_t s) {
-  FE_REQUIRE(L.kind == FE_FORM_P2_STIFFNESS, "zero-fused scatter: P2 stiffness only");
-  if (L.num_cells == 0) {
-    launch_zero(L.values, f.sp->nnz, s);
-    return;
-  }
-  if (!f.zplan) f.zplan = build_zero_plan(f);
-  const fe_form_s::ZeroPlan& P = *f.zplan;
-  MatArgs a{};
-  a.num_cells = L.num_cells;
-  a.x = L.x;
-  a.geom = L.geom;
-  a.dofs0 = L.dofs0;
-  a.dofs1 = L.dofs1;
-  a.pos = L.pos;
-  a.row_ptr = L.row_ptr;
-  a.bc0 = L.bc0;
-  a.bc1 = L.bc1;
-  a.c0 = to_dev(L.c0);
-  a.c1 = to_dev(L.c1);
-  a.values = L.values;
-  a.upper = 0;
-  ZeroArgs z{};
-  z.zr = P.zr.p;
-  z.zchunk = P.zchunk.p;
-  z.sched = P.sched.p;
-  z.zneed = P.zneed.p;
-  z.counter = P.counter.p;
-  z.err = device_error_word(f.ctx);
-  z.nitems = P.nitems;
-  z.tiles_per_chunk = P.tiles_per_chunk;
-  FE_CUDA(cudaMemsetAsync(P.counter.p, 0, sizeof(uint32_t) * (1 + (size_t)P.nchunks), s));
-  auto go = [&](auto kern) {
-    FE_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                 cudaSharedmemCarveoutMaxShared));
-    int per_sm = 0;
-    FE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kCoalThreads, 0));
-    const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(P.nitems, (int64_t)f.ctx->num_sms * std::max(1, per_sm)));
-    kern<<<(unsigned)grid, kCoalThreads, 0, s>>>(a, z);
-    FE_CUDA(cudaGetLastError());
-  };
-  const bool f32 = L.precision == FE_PREC_FP32;
-  if (a.c0.kind == FE_COEFF_P1) {
-    if (f32) go(k_mat_p2_coal_zf<FE_COEFF_P1, float>);
-    else go(k_mat_p2_coal_zf<FE_COEFF_P1, double>);
-  } else {
-    if (f32) go(k_mat_p2_coal_zf<FE_COEFF_DG0, float>);
-    else go(k_mat_p2_coal_zf<FE_COEFF_DG0, double>);
-  }
 }
 
 void launch_mirror_lower(const fe_sparsity_s& sp, double* values, cudaStream_t s) {

@@ -449,12 +449,11 @@ def test_vp2_coalesced_matches_atomic_and_is_symmetric(precision):
 
 
 @pytest.mark.parametrize("renumber", [False, True])
-def test_p2_scatter_with_folded_zero_pass_over_several_chunks(renumber):
-    # P2 n=24 (82,944 cells: two 65,536-cell chunks of the coalesced scatter
-    # with the zero pass folded in).  With a random cell order and dof
-    # numbering every chunk's first-touched rows come as many short slot
-    # ranges.  Assembled twice into the same values, so the second call must
-    # zero what the first wrote.
+def test_p2_default_scatter_on_a_larger_mesh(renumber):
+    # the default P2 scatter (warp-coalesced) on P2 n=24 (82,944 cells,
+    # 1,296 CTAs), in the mesh's order and with a random cell order and dof
+    # numbering; assembled twice into the same values (the second call's zero
+    # pass must clear the first's)
     from conftest import ensure_library
     ensure_library()
     import cudolfinx as cx
