@@ -34,7 +34,7 @@ def _grad2(x, y, z):
 
 
 @pytest.mark.parametrize("n,jitter,variant", [(6, 0.2, "atomic"), (20, 0.15, "atomic"),
-                                              (6, 0.2, "deterministic")])
+                                              (6, 0.2, "deterministic"), (20, 0.15, "auto")])
 def test_p3_cubic_energy_and_load_identities(n, jitter, variant):
     ensure_library()
     import cudolfinx as cx
