@@ -96,7 +96,7 @@ def matrix_kernels(kind: str, variant: str, big: bool = False) -> int:
     if variant in ("tile", "row-gather") or (variant == "deterministic" and kind in ("p1", "p2")):
         return 2
     atomic = variant == "atomic" or (variant == "auto" and not (kind == "p1" and big)
-                                     and kind not in ("p2", "vp2", "p3"))
+                                     and kind not in ("p2", "vp2"))
     if kind in ("p1", "vp2", "p3") and atomic:
         return 4  # zero + upper-triangle scatter + lower-triangle mirror + set_diagonal
     return 3  # coalesced, atomic-full, block (zero + kernel + set_diagonal), sorted-slot
@@ -584,7 +584,7 @@ def run_gpu(args, rank, world, local_rank):
     resolved = args.variant
     if resolved == "auto":
         resolved = ("block" if (W["kind"] == "p1" and len(I["cells"]) >= (1 << 20))
-                    else "coalesced" if W["kind"] in ("p2", "vp2", "p3") else "atomic")
+                    else "coalesced" if W["kind"] in ("p2", "vp2") else "atomic")
     kernel_key = f"{args.workload}:{resolved}"
     traffic = load_traffic(kernel_key)
     out = {

@@ -1019,814 +1019,6 @@ __device__ __forceinline__ void p2_block_upper(const T* W, Emit&& emit) {
   }
 }
 
-// P3 stiffness reference tensor per geometry pair s (as p3_stiffness_const sums
-// them): kP3Stiff[(i*20 + j)*6 + s], symmetric in i and j.
-__device__ const double kP3Stiff[2400] = {
-    0x1.e79e79e79e79ep-5, 0x1.e79e79e79e79ep-5, 0x1.e79e79e79e79ep-5, 0x1.e79e79e79e79ep-4, 0x1.e79e79e79e79ep-4, 0x1.e79e79e79e79ep-4,
-    -0x1.7297297297297p-7, 0x0.0p+0, 0x0.0p+0, -0x1.7297297297297p-7, -0x1.7297297297297p-7, 0x0.0p+0,
-    0x0.0p+0, -0x1.7297297297297p-7, 0x0.0p+0, -0x1.7297297297297p-7, 0x0.0p+0, -0x1.7297297297297p-7,
-    0x0.0p+0, 0x0.0p+0, -0x1.7297297297297p-7, 0x0.0p+0, -0x1.7297297297297p-7, -0x1.7297297297297p-7,
-    0x0.0p+0, -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-6,
-    0x0.0p+0, -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-6,
-    -0x1.b6db6db6db6dbp-7, 0x0.0p+0, -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-6, -0x1.b6db6db6db6dbp-7,
-    -0x1.b6db6db6db6dbp-7, 0x0.0p+0, -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-6, -0x1.b6db6db6db6dbp-7,
-    -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7, 0x0.0p+0, -0x1.b6db6db6db6dbp-6, -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7,
-    -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7, 0x0.0p+0, -0x1.b6db6db6db6dbp-6, -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7,
-    -0x1.1d41d41d41d42p-5, -0x1.1d41d41d41d42p-5, -0x1.8af8af8af8af9p-4, -0x1.1d41d41d41d42p-4, -0x1.0cccccccccccdp-3, -0x1.0cccccccccccdp-3,
-    0x1.b6db6db6db6dbp-7, 0x1.b6db6db6db6dbp-7, 0x1.8af8af8af8af9p-5, 0x1.b6db6db6db6dbp-6, 0x1.f8af8af8af8b0p-5, 0x1.f8af8af8af8b0p-5,
-    -0x1.1d41d41d41d42p-5, -0x1.8af8af8af8af9p-4, -0x1.1d41d41d41d42p-5, -0x1.0cccccccccccdp-3, -0x1.1d41d41d41d42p-4, -0x1.0cccccccccccdp-3,
-    0x1.b6db6db6db6dbp-7, 0x1.8af8af8af8af9p-5, 0x1.b6db6db6db6dbp-7, 0x1.f8af8af8af8b0p-5, 0x1.b6db6db6db6dbp-6, 0x1.f8af8af8af8b0p-5,
-    -0x1.8af8af8af8af9p-4, -0x1.1d41d41d41d42p-5, -0x1.1d41d41d41d42p-5, -0x1.0cccccccccccdp-3, -0x1.0cccccccccccdp-3, -0x1.1d41d41d41d42p-4,
-    0x1.8af8af8af8af9p-5, 0x1.b6db6db6db6dbp-7, 0x1.b6db6db6db6dbp-7, 0x1.f8af8af8af8b0p-5, 0x1.f8af8af8af8b0p-5, 0x1.b6db6db6db6dbp-6,
-    -0x1.0750750750750p-5, -0x1.0750750750750p-5, -0x1.0750750750750p-5, -0x1.0750750750750p-4, -0x1.0750750750750p-4, -0x1.0750750750750p-4,
-    0x1.0750750750750p-5, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5, 0x1.4924924924925p-4, 0x1.4924924924925p-4, 0x1.8af8af8af8af9p-4,
-    0x1.8af8af8af8af9p-5, 0x1.0750750750750p-5, 0x1.8af8af8af8af9p-5, 0x1.4924924924925p-4, 0x1.8af8af8af8af9p-4, 0x1.4924924924925p-4,
-    0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5, 0x1.0750750750750p-5, 0x1.8af8af8af8af9p-4, 0x1.4924924924925p-4, 0x1.4924924924925p-4,
-    -0x1.7297297297297p-7, 0x0.0p+0, 0x0.0p+0, -0x1.7297297297297p-7, -0x1.7297297297297p-7, 0x0.0p+0,
-    0x1.e79e79e79e79ep-5, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
-    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.7297297297297p-7, 0x0.0p+0, 0x0.0p+0,
-    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.7297297297297p-7, 0x0.0p+0,
-    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.b6db6db6db6dbp-7, 0x1.b6db6db6db6dbp-7, 0x0.0p+0,
-    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.b6db6db6db6dbp-7, 0x1.b6db6db6db6dbp-7, 0x0.0p+0,
-    -0x1.1d41d41d41d42p-5, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.f8af8af8af8b0p-5, 0x0.0p+0,
-    0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, -0x1.1d41d41d41d42p-5, 0x0.0p+0,
-    -0x1.1d41d41d41d42p-5, 0x0.0p+0, 0x0.0p+0, 0x1.f8af8af8af8b0p-5, 0x0.0p+0, 0x0.0p+0,
-    0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x0.0p+0, -0x1.1d41d41d41d42p-5, 0x0.0p+0, 0x0.0p+0,
-    -0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x0.0p+0, -0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x0.0p+0,
-    -0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x0.0p+0, -0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x0.0p+0,
-    -0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, -0x1.b6db6db6db6dbp-7, 0x0.0p+0,
-    -0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, -0x1.b6db6db6db6dbp-7, 0x0.0p+0,
-    0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x0.0p+0, 0x1.1d41d41d41d42p-5, 0x1.1d41d41d41d42p-5, 0x0.0p+0,
-    -0x1.8af8af8af8af9p-4, 0x0.0p+0, 0x0.0p+0, -0x1.f8af8af8af8b0p-5, -0x1.f8af8af8af8b0p-5, 0x0.0p+0,
-    0x1.0750750750750p-5, 0x0.0p+0, 0x0.0p+0, -0x1.0750750750750p-6, -0x1.0750750750750p-6, 0x0.0p+0,
-    -0x1.0750750750750p-5, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
-    0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x0.0p+0, 0x1.0750750750750p-6, 0x0.0p+0, 0x0.0p+0,
-    0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.0750750750750p-6, 0x0.0p+0,
-    0x0.0p+0, -0x1.7297297297297p-7, 0x0.0p+0, -0x1.7297297297297p-7, 0x0.0p+0, -0x1.7297297297297p-7,
-    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.7297297297297p-7, 0x0.0p+0, 0x0.0p+0,
-    0x0.0p+0, 0x1.e79e79e79e79ep-5, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
-    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.7297297297297p-7,
-    0x0.0p+0, -0x1.1d41d41d41d42p-5, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.f8af8af8af8b0p-5,
-    0x0.0p+0, 0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, -0x1.1d41d41d41d42p-5,
-    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x1.b6db6db6db6dbp-7,
-    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x1.b6db6db6db6dbp-7,
-    0x0.0p+0, 0x1.b6db6db6db6dbp-7, 0x0.0p+0, -0x1.1d41d41d41d42p-5, 0x0.0p+0, 0x0.0p+0,
-    0x0.0p+0, -0x1.1d41d41d41d42p-5, 0x0.0p+0, 0x1.f8af8af8af8b0p-5, 0x0.0p+0, 0x0.0p+0,
-    0x0.0p+0, -0x1.b6db6db6db6dbp-7, 0x0.0p+0, -0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x0.0p+0,
-    0x0.0p+0, -0x1.b6db6db6db6dbp-7, 0x0.0p+0, -0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x0.0p+0,
-    0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x1.1d41d41d41d42p-5, 0x0.0p+0, 0x1.1d41d41d41d42p-5,
-    0x0.0p+0, -0x1.8af8af8af8af9p-4, 0x0.0p+0, -0x1.f8af8af8af8b0p-5, 0x0.0p+0, -0x1.f8af8af8af8b0p-5,
-    0x0.0p+0, -0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, -0x1.b6db6db6db6dbp-7,
-    0x0.0p+0, -0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, -0x1.b6db6db6db6dbp-7,
-    0x0.0p+0, 0x1.0750750750750p-5, 0x0.0p+0, -0x1.0750750750750p-6, 0x0.0p+0, -0x1.0750750750750p-6,
-    0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x1.0750750750750p-6, 0x0.0p+0, 0x0.0p+0,
-    0x0.0p+0, -0x1.0750750750750p-5, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
-    0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.0750750750750p-6,
-    0x0.0p+0, 0x0.0p+0, -0x1.7297297297297p-7, 0x0.0p+0, -0x1.7297297297297p-7, -0x1.7297297297297p-7,
-    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.7297297297297p-7, 0x0.0p+0,
-    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.7297297297297p-7,
-    0x0.0p+0, 0x0.0p+0, 0x1.e79e79e79e79ep-5, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
-    0x0.0p+0, 0x0.0p+0, 0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x0.0p+0, -0x1.1d41d41d41d42p-5,
-    0x0.0p+0, 0x0.0p+0, -0x1.1d41d41d41d42p-5, 0x0.0p+0, 0x0.0p+0, 0x1.f8af8af8af8b0p-5,
-    0x0.0p+0, 0x0.0p+0, 0x1.b6db6db6db6dbp-7, 0x0.0p+0, -0x1.1d41d41d41d42p-5, 0x0.0p+0,
-    0x0.0p+0, 0x0.0p+0, -0x1.1d41d41d41d42p-5, 0x0.0p+0, 0x1.f8af8af8af8b0p-5, 0x0.0p+0,
-    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.b6db6db6db6dbp-7, 0x1.b6db6db6db6dbp-7,
-    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.b6db6db6db6dbp-7, 0x1.b6db6db6db6dbp-7,
-    0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x1.1d41d41d41d42p-5, 0x1.1d41d41d41d42p-5,
-    0x0.0p+0, 0x0.0p+0, -0x1.8af8af8af8af9p-4, 0x0.0p+0, -0x1.f8af8af8af8b0p-5, -0x1.f8af8af8af8b0p-5,
-    0x0.0p+0, 0x0.0p+0, -0x1.b6db6db6db6dbp-7, 0x0.0p+0, -0x1.b6db6db6db6dbp-7, 0x0.0p+0,
-    0x0.0p+0, 0x0.0p+0, -0x1.b6db6db6db6dbp-7, 0x0.0p+0, -0x1.b6db6db6db6dbp-7, 0x0.0p+0,
-    0x0.0p+0, 0x0.0p+0, -0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x0.0p+0, -0x1.b6db6db6db6dbp-7,
-    0x0.0p+0, 0x0.0p+0, -0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x0.0p+0, -0x1.b6db6db6db6dbp-7,
-    0x0.0p+0, 0x0.0p+0, 0x1.0750750750750p-5, 0x0.0p+0, -0x1.0750750750750p-6, -0x1.0750750750750p-6,
-    0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x1.0750750750750p-6, 0x0.0p+0,
-    0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x0.0p+0, 0x1.0750750750750p-6,
-    0x0.0p+0, 0x0.0p+0, -0x1.0750750750750p-5, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
-    0x0.0p+0, -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-6,
-    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.b6db6db6db6dbp-7, 0x1.b6db6db6db6dbp-7, 0x0.0p+0,
-    0x0.0p+0, -0x1.1d41d41d41d42p-5, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.f8af8af8af8b0p-5,
-    0x0.0p+0, 0x0.0p+0, 0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x0.0p+0, -0x1.1d41d41d41d42p-5,
-    0x0.0p+0, 0x1.edb6db6db6db7p-3, 0x1.8af8af8af8af9p-3, 0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-3,
-    0x0.0p+0, -0x1.283a83a83a83bp-4, -0x1.283a83a83a83bp-4, 0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-5,
-    0x0.0p+0, 0x0.0p+0, -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-6,
-    0x0.0p+0, 0x0.0p+0, -0x1.8af8af8af8af9p-6, -0x1.283a83a83a83bp-4, -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-5,
-    0x0.0p+0, -0x1.8af8af8af8af9p-6, 0x0.0p+0, -0x1.8af8af8af8af9p-5, -0x1.283a83a83a83bp-4, -0x1.8af8af8af8af9p-6,
-    0x0.0p+0, 0x1.edb6db6db6db7p-4, 0x0.0p+0, 0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-3, 0x1.8af8af8af8af9p-4,
-    0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-5,
-    0x0.0p+0, 0x1.283a83a83a83bp-4, 0x0.0p+0, 0x1.283a83a83a83bp-4, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-5,
-    0x0.0p+0, 0x1.8af8af8af8af9p-6, 0x1.283a83a83a83bp-4, 0x1.8af8af8af8af9p-5, 0x1.283a83a83a83bp-4, 0x1.8af8af8af8af9p-4,
-    0x0.0p+0, 0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-3, -0x1.8af8af8af8af9p-4, -0x1.8af8af8af8af9p-3, -0x1.8af8af8af8af9p-3,
-    0x0.0p+0, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-5,
-    0x0.0p+0, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-5,
-    0x0.0p+0, -0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-4, 0x1.edb6db6db6db7p-3, 0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-4,
-    0x0.0p+0, -0x1.283a83a83a83bp-2, 0x0.0p+0, -0x1.edb6db6db6db7p-3, -0x1.8af8af8af8af9p-4, -0x1.edb6db6db6db7p-3,
-    0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-5,
-    0x0.0p+0, -0x1.283a83a83a83bp-3, -0x1.8af8af8af8af9p-4, 0x0.0p+0, 0x0.0p+0, -0x1.edb6db6db6db7p-3,
-    0x0.0p+0, -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-6,
-    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.b6db6db6db6dbp-7, 0x1.b6db6db6db6dbp-7, 0x0.0p+0,
-    0x0.0p+0, 0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, -0x1.1d41d41d41d42p-5,
-    0x0.0p+0, 0x0.0p+0, -0x1.1d41d41d41d42p-5, 0x0.0p+0, 0x0.0p+0, 0x1.f8af8af8af8b0p-5,
-    0x0.0p+0, -0x1.283a83a83a83bp-4, -0x1.283a83a83a83bp-4, 0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-5,
-    0x0.0p+0, 0x1.8af8af8af8af9p-3, 0x1.edb6db6db6db7p-3, 0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-3,
-    0x0.0p+0, 0x0.0p+0, -0x1.8af8af8af8af9p-6, -0x1.283a83a83a83bp-4, -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-6,
-    0x0.0p+0, 0x0.0p+0, 0x1.edb6db6db6db7p-4, 0x1.8af8af8af8af9p-3, 0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-4,
-    0x0.0p+0, -0x1.8af8af8af8af9p-6, 0x0.0p+0, -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-6,
-    0x0.0p+0, -0x1.8af8af8af8af9p-6, 0x0.0p+0, -0x1.8af8af8af8af9p-6, -0x1.283a83a83a83bp-4, -0x1.8af8af8af8af9p-5,
-    0x0.0p+0, 0x1.283a83a83a83bp-4, 0x1.8af8af8af8af9p-6, 0x1.283a83a83a83bp-4, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-4,
-    0x0.0p+0, -0x1.8af8af8af8af9p-3, 0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-3, -0x1.8af8af8af8af9p-4, -0x1.8af8af8af8af9p-3,
-    0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5,
-    0x0.0p+0, 0x0.0p+0, 0x1.283a83a83a83bp-4, 0x1.8af8af8af8af9p-6, 0x1.283a83a83a83bp-4, 0x1.8af8af8af8af9p-5,
-    0x0.0p+0, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-5,
-    0x0.0p+0, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-5,
-    0x0.0p+0, 0x1.8af8af8af8af9p-4, -0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-4, 0x1.edb6db6db6db7p-3, 0x1.8af8af8af8af9p-4,
-    0x0.0p+0, 0x0.0p+0, -0x1.283a83a83a83bp-2, -0x1.8af8af8af8af9p-4, -0x1.edb6db6db6db7p-3, -0x1.edb6db6db6db7p-3,
-    0x0.0p+0, -0x1.8af8af8af8af9p-4, -0x1.283a83a83a83bp-3, 0x0.0p+0, 0x0.0p+0, -0x1.edb6db6db6db7p-3,
-    0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-5,
-    -0x1.b6db6db6db6dbp-7, 0x0.0p+0, -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-6, -0x1.b6db6db6db6dbp-7,
-    -0x1.1d41d41d41d42p-5, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.f8af8af8af8b0p-5, 0x0.0p+0,
-    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x1.b6db6db6db6dbp-7,
-    0x0.0p+0, 0x0.0p+0, 0x1.b6db6db6db6dbp-7, 0x0.0p+0, -0x1.1d41d41d41d42p-5, 0x0.0p+0,
-    0x0.0p+0, 0x0.0p+0, -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-6,
-    0x0.0p+0, 0x0.0p+0, -0x1.8af8af8af8af9p-6, -0x1.283a83a83a83bp-4, -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-6,
-    0x1.edb6db6db6db7p-3, 0x0.0p+0, 0x1.8af8af8af8af9p-3, 0x0.0p+0, 0x1.8af8af8af8af9p-3, 0x0.0p+0,
-    -0x1.283a83a83a83bp-4, 0x0.0p+0, -0x1.283a83a83a83bp-4, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0,
-    0x1.edb6db6db6db7p-4, 0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-3,
-    -0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x0.0p+0, -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-6, -0x1.283a83a83a83bp-4,
-    0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-6,
-    0x1.283a83a83a83bp-4, 0x0.0p+0, 0x0.0p+0, 0x1.283a83a83a83bp-4, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-6,
-    0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0,
-    0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0,
-    0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x1.283a83a83a83bp-4, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-4, 0x1.283a83a83a83bp-4,
-    0x1.8af8af8af8af9p-6, 0x0.0p+0, -0x1.8af8af8af8af9p-3, -0x1.8af8af8af8af9p-4, -0x1.8af8af8af8af9p-3, -0x1.8af8af8af8af9p-3,
-    -0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x1.8af8af8af8af9p-4, 0x1.edb6db6db6db7p-3, 0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-4,
-    0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0,
-    -0x1.283a83a83a83bp-2, 0x0.0p+0, 0x0.0p+0, -0x1.edb6db6db6db7p-3, -0x1.edb6db6db6db7p-3, -0x1.8af8af8af8af9p-4,
-    -0x1.283a83a83a83bp-3, 0x0.0p+0, -0x1.8af8af8af8af9p-4, 0x0.0p+0, -0x1.edb6db6db6db7p-3, 0x0.0p+0,
-    -0x1.b6db6db6db6dbp-7, 0x0.0p+0, -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-6, -0x1.b6db6db6db6dbp-7,
-    0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, -0x1.1d41d41d41d42p-5, 0x0.0p+0,
-    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x1.b6db6db6db6dbp-7,
-    0x0.0p+0, 0x0.0p+0, -0x1.1d41d41d41d42p-5, 0x0.0p+0, 0x1.f8af8af8af8b0p-5, 0x0.0p+0,
-    0x0.0p+0, 0x0.0p+0, -0x1.8af8af8af8af9p-6, -0x1.283a83a83a83bp-4, -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-5,
-    0x0.0p+0, 0x0.0p+0, 0x1.edb6db6db6db7p-4, 0x1.8af8af8af8af9p-3, 0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-4,
-    -0x1.283a83a83a83bp-4, 0x0.0p+0, -0x1.283a83a83a83bp-4, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0,
-    0x1.8af8af8af8af9p-3, 0x0.0p+0, 0x1.edb6db6db6db7p-3, 0x0.0p+0, 0x1.8af8af8af8af9p-3, 0x0.0p+0,
-    -0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x0.0p+0, -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-5, -0x1.283a83a83a83bp-4,
-    -0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x0.0p+0, -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-5,
-    0x1.283a83a83a83bp-4, 0x0.0p+0, 0x1.8af8af8af8af9p-6, 0x1.283a83a83a83bp-4, 0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-5,
-    -0x1.8af8af8af8af9p-3, 0x0.0p+0, 0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-3, -0x1.8af8af8af8af9p-3, -0x1.8af8af8af8af9p-4,
-    0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0,
-    0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0,
-    0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5,
-    0x0.0p+0, 0x0.0p+0, 0x1.283a83a83a83bp-4, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-5, 0x1.283a83a83a83bp-4,
-    0x1.8af8af8af8af9p-4, 0x0.0p+0, -0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-4, 0x1.edb6db6db6db7p-3,
-    -0x1.8af8af8af8af9p-4, 0x0.0p+0, -0x1.283a83a83a83bp-3, 0x0.0p+0, -0x1.edb6db6db6db7p-3, 0x0.0p+0,
-    0x0.0p+0, 0x0.0p+0, -0x1.283a83a83a83bp-2, -0x1.8af8af8af8af9p-4, -0x1.edb6db6db6db7p-3, -0x1.edb6db6db6db7p-3,
-    0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0,
-    -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7, 0x0.0p+0, -0x1.b6db6db6db6dbp-6, -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7,
-    -0x1.1d41d41d41d42p-5, 0x0.0p+0, 0x0.0p+0, 0x1.f8af8af8af8b0p-5, 0x0.0p+0, 0x0.0p+0,
-    0x0.0p+0, 0x1.b6db6db6db6dbp-7, 0x0.0p+0, -0x1.1d41d41d41d42p-5, 0x0.0p+0, 0x0.0p+0,
-    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.b6db6db6db6dbp-7, 0x1.b6db6db6db6dbp-7,
-    0x0.0p+0, -0x1.8af8af8af8af9p-6, 0x0.0p+0, -0x1.8af8af8af8af9p-5, -0x1.283a83a83a83bp-4, -0x1.8af8af8af8af9p-6,
-    0x0.0p+0, -0x1.8af8af8af8af9p-6, 0x0.0p+0, -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-6,
-    0x1.edb6db6db6db7p-4, 0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-3,
-    -0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x0.0p+0, -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-5, -0x1.283a83a83a83bp-4,
-    0x1.edb6db6db6db7p-3, 0x1.8af8af8af8af9p-3, 0x0.0p+0, 0x1.8af8af8af8af9p-3, 0x0.0p+0, 0x0.0p+0,
-    -0x1.283a83a83a83bp-4, -0x1.283a83a83a83bp-4, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x0.0p+0,
-    0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x0.0p+0,
-    0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x0.0p+0,
-    0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-6,
-    0x1.283a83a83a83bp-4, 0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x1.283a83a83a83bp-4, 0x1.8af8af8af8af9p-6,
-    0x1.8af8af8af8af9p-6, 0x1.283a83a83a83bp-4, 0x0.0p+0, 0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-5, 0x1.283a83a83a83bp-4,
-    0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-3, 0x0.0p+0, -0x1.8af8af8af8af9p-3, -0x1.8af8af8af8af9p-4, -0x1.8af8af8af8af9p-3,
-    -0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-4, 0x0.0p+0, 0x1.8af8af8af8af9p-4, 0x1.edb6db6db6db7p-3, 0x1.8af8af8af8af9p-4,
-    0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x0.0p+0,
-    -0x1.283a83a83a83bp-3, -0x1.8af8af8af8af9p-4, 0x0.0p+0, -0x1.edb6db6db6db7p-3, 0x0.0p+0, 0x0.0p+0,
-    -0x1.283a83a83a83bp-2, 0x0.0p+0, 0x0.0p+0, -0x1.edb6db6db6db7p-3, -0x1.edb6db6db6db7p-3, -0x1.8af8af8af8af9p-4,
-    -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7, 0x0.0p+0, -0x1.b6db6db6db6dbp-6, -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7,
-    0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x0.0p+0, -0x1.1d41d41d41d42p-5, 0x0.0p+0, 0x0.0p+0,
-    0x0.0p+0, -0x1.1d41d41d41d42p-5, 0x0.0p+0, 0x1.f8af8af8af8b0p-5, 0x0.0p+0, 0x0.0p+0,
-    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.b6db6db6db6dbp-7, 0x1.b6db6db6db6dbp-7,
-    0x0.0p+0, 0x1.edb6db6db6db7p-4, 0x0.0p+0, 0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-3, 0x1.8af8af8af8af9p-4,
-    0x0.0p+0, -0x1.8af8af8af8af9p-6, 0x0.0p+0, -0x1.8af8af8af8af9p-6, -0x1.283a83a83a83bp-4, -0x1.8af8af8af8af9p-5,
-    -0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x0.0p+0, -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-6, -0x1.283a83a83a83bp-4,
-    -0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x0.0p+0, -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-5,
-    -0x1.283a83a83a83bp-4, -0x1.283a83a83a83bp-4, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x0.0p+0,
-    0x1.8af8af8af8af9p-3, 0x1.edb6db6db6db7p-3, 0x0.0p+0, 0x1.8af8af8af8af9p-3, 0x0.0p+0, 0x0.0p+0,
-    0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x0.0p+0,
-    0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x0.0p+0,
-    0x1.283a83a83a83bp-4, 0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x1.8af8af8af8af9p-4, 0x1.283a83a83a83bp-4, 0x1.8af8af8af8af9p-5,
-    -0x1.8af8af8af8af9p-3, 0x1.8af8af8af8af9p-6, 0x0.0p+0, -0x1.8af8af8af8af9p-3, -0x1.8af8af8af8af9p-3, -0x1.8af8af8af8af9p-4,
-    0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-5,
-    0x0.0p+0, 0x1.283a83a83a83bp-4, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-6, 0x1.283a83a83a83bp-4,
-    0x1.8af8af8af8af9p-4, -0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-4, 0x1.edb6db6db6db7p-3,
-    -0x1.8af8af8af8af9p-4, -0x1.283a83a83a83bp-3, 0x0.0p+0, -0x1.edb6db6db6db7p-3, 0x0.0p+0, 0x0.0p+0,
-    0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x0.0p+0,
-    0x0.0p+0, -0x1.283a83a83a83bp-2, 0x0.0p+0, -0x1.edb6db6db6db7p-3, -0x1.8af8af8af8af9p-4, -0x1.edb6db6db6db7p-3,
-    -0x1.1d41d41d41d42p-5, -0x1.1d41d41d41d42p-5, -0x1.8af8af8af8af9p-4, -0x1.1d41d41d41d42p-4, -0x1.0cccccccccccdp-3, -0x1.0cccccccccccdp-3,
-    -0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x0.0p+0, -0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x0.0p+0,
-    0x0.0p+0, -0x1.b6db6db6db6dbp-7, 0x0.0p+0, -0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x0.0p+0,
-    0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x1.1d41d41d41d42p-5, 0x1.1d41d41d41d42p-5,
-    0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-5,
-    0x0.0p+0, 0x1.283a83a83a83bp-4, 0x1.8af8af8af8af9p-6, 0x1.283a83a83a83bp-4, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-4,
-    0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-6,
-    0x1.283a83a83a83bp-4, 0x0.0p+0, 0x1.8af8af8af8af9p-6, 0x1.283a83a83a83bp-4, 0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-5,
-    0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x0.0p+0,
-    0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x0.0p+0,
-    0x1.edb6db6db6db7p-3, 0x1.edb6db6db6db7p-3, 0x1.edb6db6db6db7p-3, 0x1.edb6db6db6db7p-2, 0x1.283a83a83a83bp-2, 0x1.283a83a83a83bp-2,
-    -0x1.283a83a83a83bp-4, -0x1.283a83a83a83bp-4, -0x1.8af8af8af8af9p-3, -0x1.283a83a83a83bp-3, -0x1.8af8af8af8af9p-3, -0x1.8af8af8af8af9p-3,
-    0x1.edb6db6db6db7p-4, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, 0x1.283a83a83a83bp-3, 0x1.283a83a83a83bp-3, 0x1.edb6db6db6db7p-3,
-    -0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x0.0p+0, -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-5,
-    0x1.8af8af8af8af9p-6, 0x1.edb6db6db6db7p-4, 0x1.8af8af8af8af9p-6, 0x1.283a83a83a83bp-3, 0x1.edb6db6db6db7p-3, 0x1.283a83a83a83bp-3,
-    0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x0.0p+0, -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-6,
-    0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5,
-    -0x1.8af8af8af8af9p-5, -0x1.283a83a83a83bp-2, -0x1.8af8af8af8af9p-5, -0x1.599999999999ap-2, -0x1.8af8af8af8af9p-3, -0x1.599999999999ap-2,
-    -0x1.283a83a83a83bp-2, -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-5, -0x1.599999999999ap-2, -0x1.599999999999ap-2, -0x1.8af8af8af8af9p-3,
-    -0x1.283a83a83a83bp-3, -0x1.283a83a83a83bp-3, 0x0.0p+0, -0x1.283a83a83a83bp-2, -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-5,
-    0x1.b6db6db6db6dbp-7, 0x1.b6db6db6db6dbp-7, 0x1.8af8af8af8af9p-5, 0x1.b6db6db6db6dbp-6, 0x1.f8af8af8af8b0p-5, 0x1.f8af8af8af8b0p-5,
-    -0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x0.0p+0, -0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x0.0p+0,
-    0x0.0p+0, -0x1.b6db6db6db6dbp-7, 0x0.0p+0, -0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x0.0p+0,
-    0x0.0p+0, 0x0.0p+0, -0x1.8af8af8af8af9p-4, 0x0.0p+0, -0x1.f8af8af8af8b0p-5, -0x1.f8af8af8af8b0p-5,
-    0x0.0p+0, 0x1.283a83a83a83bp-4, 0x0.0p+0, 0x1.283a83a83a83bp-4, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-5,
-    0x0.0p+0, -0x1.8af8af8af8af9p-3, 0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-3, -0x1.8af8af8af8af9p-4, -0x1.8af8af8af8af9p-3,
-    0x1.283a83a83a83bp-4, 0x0.0p+0, 0x0.0p+0, 0x1.283a83a83a83bp-4, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-6,
-    -0x1.8af8af8af8af9p-3, 0x0.0p+0, 0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-3, -0x1.8af8af8af8af9p-3, -0x1.8af8af8af8af9p-4,
-    0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x0.0p+0,
-    0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x0.0p+0,
-    -0x1.283a83a83a83bp-4, -0x1.283a83a83a83bp-4, -0x1.8af8af8af8af9p-3, -0x1.283a83a83a83bp-3, -0x1.8af8af8af8af9p-3, -0x1.8af8af8af8af9p-3,
-    0x1.8af8af8af8af9p-3, 0x1.8af8af8af8af9p-3, 0x1.edb6db6db6db7p-3, 0x1.8af8af8af8af9p-2, 0x1.8af8af8af8af9p-3, 0x1.8af8af8af8af9p-3,
-    -0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-6, 0x0.0p+0, -0x1.8af8af8af8af9p-5,
-    -0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x0.0p+0, -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-5,
-    0x0.0p+0, -0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-5, 0x0.0p+0,
-    0x0.0p+0, -0x1.8af8af8af8af9p-6, 0x0.0p+0, -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-6,
-    -0x1.8af8af8af8af9p-4, -0x1.8af8af8af8af9p-4, 0x0.0p+0, -0x1.8af8af8af8af9p-3, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5,
-    0x1.8af8af8af8af9p-4, 0x0.0p+0, -0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-4, 0x1.edb6db6db6db7p-3,
-    0x0.0p+0, 0x1.8af8af8af8af9p-4, -0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-4, 0x1.edb6db6db6db7p-3, 0x1.8af8af8af8af9p-4,
-    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-5,
-    -0x1.1d41d41d41d42p-5, -0x1.8af8af8af8af9p-4, -0x1.1d41d41d41d42p-5, -0x1.0cccccccccccdp-3, -0x1.1d41d41d41d42p-4, -0x1.0cccccccccccdp-3,
-    -0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, -0x1.b6db6db6db6dbp-7, 0x0.0p+0,
-    0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x1.1d41d41d41d42p-5, 0x0.0p+0, 0x1.1d41d41d41d42p-5,
-    0x0.0p+0, 0x0.0p+0, -0x1.b6db6db6db6dbp-7, 0x0.0p+0, -0x1.b6db6db6db6dbp-7, 0x0.0p+0,
-    0x0.0p+0, 0x1.8af8af8af8af9p-6, 0x1.283a83a83a83bp-4, 0x1.8af8af8af8af9p-5, 0x1.283a83a83a83bp-4, 0x1.8af8af8af8af9p-4,
-    0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5,
-    0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0,
-    0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0,
-    0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-6,
-    0x1.283a83a83a83bp-4, 0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x1.8af8af8af8af9p-4, 0x1.283a83a83a83bp-4, 0x1.8af8af8af8af9p-5,
-    0x1.edb6db6db6db7p-4, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, 0x1.283a83a83a83bp-3, 0x1.283a83a83a83bp-3, 0x1.edb6db6db6db7p-3,
-    -0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-6, 0x0.0p+0, -0x1.8af8af8af8af9p-5,
-    0x1.edb6db6db6db7p-3, 0x1.edb6db6db6db7p-3, 0x1.edb6db6db6db7p-3, 0x1.283a83a83a83bp-2, 0x1.edb6db6db6db7p-2, 0x1.283a83a83a83bp-2,
-    -0x1.283a83a83a83bp-4, -0x1.8af8af8af8af9p-3, -0x1.283a83a83a83bp-4, -0x1.8af8af8af8af9p-3, -0x1.283a83a83a83bp-3, -0x1.8af8af8af8af9p-3,
-    0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, 0x1.edb6db6db6db7p-4, 0x1.edb6db6db6db7p-3, 0x1.283a83a83a83bp-3, 0x1.283a83a83a83bp-3,
-    0x1.8af8af8af8af9p-6, 0x0.0p+0, -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-5, 0x0.0p+0, -0x1.8af8af8af8af9p-6,
-    0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-5,
-    -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-5, -0x1.283a83a83a83bp-2, -0x1.8af8af8af8af9p-3, -0x1.599999999999ap-2, -0x1.599999999999ap-2,
-    -0x1.283a83a83a83bp-3, 0x0.0p+0, -0x1.283a83a83a83bp-3, -0x1.8af8af8af8af9p-5, -0x1.283a83a83a83bp-2, -0x1.8af8af8af8af9p-5,
-    -0x1.283a83a83a83bp-2, -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-5, -0x1.599999999999ap-2, -0x1.599999999999ap-2, -0x1.8af8af8af8af9p-3,
-    0x1.b6db6db6db6dbp-7, 0x1.8af8af8af8af9p-5, 0x1.b6db6db6db6dbp-7, 0x1.f8af8af8af8b0p-5, 0x1.b6db6db6db6dbp-6, 0x1.f8af8af8af8b0p-5,
-    -0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, -0x1.b6db6db6db6dbp-7, 0x0.0p+0,
-    0x0.0p+0, -0x1.8af8af8af8af9p-4, 0x0.0p+0, -0x1.f8af8af8af8b0p-5, 0x0.0p+0, -0x1.f8af8af8af8b0p-5,
-    0x0.0p+0, 0x0.0p+0, -0x1.b6db6db6db6dbp-7, 0x0.0p+0, -0x1.b6db6db6db6dbp-7, 0x0.0p+0,
-    0x0.0p+0, 0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-3, -0x1.8af8af8af8af9p-4, -0x1.8af8af8af8af9p-3, -0x1.8af8af8af8af9p-3,
-    0x0.0p+0, 0x0.0p+0, 0x1.283a83a83a83bp-4, 0x1.8af8af8af8af9p-6, 0x1.283a83a83a83bp-4, 0x1.8af8af8af8af9p-5,
-    0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0,
-    0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0,
-    0x1.283a83a83a83bp-4, 0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x1.283a83a83a83bp-4, 0x1.8af8af8af8af9p-6,
-    -0x1.8af8af8af8af9p-3, 0x1.8af8af8af8af9p-6, 0x0.0p+0, -0x1.8af8af8af8af9p-3, -0x1.8af8af8af8af9p-3, -0x1.8af8af8af8af9p-4,
-    -0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x0.0p+0, -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-5,
-    -0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x0.0p+0, -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-5,
-    -0x1.283a83a83a83bp-4, -0x1.8af8af8af8af9p-3, -0x1.283a83a83a83bp-4, -0x1.8af8af8af8af9p-3, -0x1.283a83a83a83bp-3, -0x1.8af8af8af8af9p-3,
-    0x1.8af8af8af8af9p-3, 0x1.edb6db6db6db7p-3, 0x1.8af8af8af8af9p-3, 0x1.8af8af8af8af9p-3, 0x1.8af8af8af8af9p-2, 0x1.8af8af8af8af9p-3,
-    0x0.0p+0, 0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-6, 0x0.0p+0,
-    0x0.0p+0, 0x0.0p+0, -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-6,
-    -0x1.8af8af8af8af9p-4, 0x0.0p+0, -0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-3, 0x1.8af8af8af8af9p-5,
-    0x1.8af8af8af8af9p-4, -0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-4, 0x1.edb6db6db6db7p-3,
-    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, -0x1.8af8af8af8af9p-5, 0x0.0p+0, -0x1.8af8af8af8af9p-5,
-    0x0.0p+0, -0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-4, 0x1.edb6db6db6db7p-3, 0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-4,
-    -0x1.8af8af8af8af9p-4, -0x1.1d41d41d41d42p-5, -0x1.1d41d41d41d42p-5, -0x1.0cccccccccccdp-3, -0x1.0cccccccccccdp-3, -0x1.1d41d41d41d42p-4,
-    0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x0.0p+0, 0x1.1d41d41d41d42p-5, 0x1.1d41d41d41d42p-5, 0x0.0p+0,
-    0x0.0p+0, -0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, -0x1.b6db6db6db6dbp-7,
-    0x0.0p+0, 0x0.0p+0, -0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x0.0p+0, -0x1.b6db6db6db6dbp-7,
-    0x0.0p+0, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-5,
-    0x0.0p+0, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-5,
-    0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x1.283a83a83a83bp-4, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-4, 0x1.283a83a83a83bp-4,
-    0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5,
-    0x1.8af8af8af8af9p-6, 0x1.283a83a83a83bp-4, 0x0.0p+0, 0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-5, 0x1.283a83a83a83bp-4,
-    0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-5,
-    0x1.8af8af8af8af9p-6, 0x1.edb6db6db6db7p-4, 0x1.8af8af8af8af9p-6, 0x1.283a83a83a83bp-3, 0x1.edb6db6db6db7p-3, 0x1.283a83a83a83bp-3,
-    0x0.0p+0, -0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-5, 0x0.0p+0,
-    0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, 0x1.edb6db6db6db7p-4, 0x1.edb6db6db6db7p-3, 0x1.283a83a83a83bp-3, 0x1.283a83a83a83bp-3,
-    0x0.0p+0, 0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-6, 0x0.0p+0,
-    0x1.edb6db6db6db7p-3, 0x1.edb6db6db6db7p-3, 0x1.edb6db6db6db7p-3, 0x1.283a83a83a83bp-2, 0x1.283a83a83a83bp-2, 0x1.edb6db6db6db7p-2,
-    -0x1.8af8af8af8af9p-3, -0x1.283a83a83a83bp-4, -0x1.283a83a83a83bp-4, -0x1.8af8af8af8af9p-3, -0x1.8af8af8af8af9p-3, -0x1.283a83a83a83bp-3,
-    0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-4,
-    0x0.0p+0, -0x1.283a83a83a83bp-3, -0x1.283a83a83a83bp-3, -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-5, -0x1.283a83a83a83bp-2,
-    -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-5, -0x1.283a83a83a83bp-2, -0x1.8af8af8af8af9p-3, -0x1.599999999999ap-2, -0x1.599999999999ap-2,
-    -0x1.8af8af8af8af9p-5, -0x1.283a83a83a83bp-2, -0x1.8af8af8af8af9p-5, -0x1.599999999999ap-2, -0x1.8af8af8af8af9p-3, -0x1.599999999999ap-2,
-    0x1.8af8af8af8af9p-5, 0x1.b6db6db6db6dbp-7, 0x1.b6db6db6db6dbp-7, 0x1.f8af8af8af8b0p-5, 0x1.f8af8af8af8b0p-5, 0x1.b6db6db6db6dbp-6,
-    -0x1.8af8af8af8af9p-4, 0x0.0p+0, 0x0.0p+0, -0x1.f8af8af8af8b0p-5, -0x1.f8af8af8af8b0p-5, 0x0.0p+0,
-    0x0.0p+0, -0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, -0x1.b6db6db6db6dbp-7,
-    0x0.0p+0, 0x0.0p+0, -0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x0.0p+0, -0x1.b6db6db6db6dbp-7,
-    0x0.0p+0, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-5,
-    0x0.0p+0, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-5,
-    0x1.8af8af8af8af9p-6, 0x0.0p+0, -0x1.8af8af8af8af9p-3, -0x1.8af8af8af8af9p-4, -0x1.8af8af8af8af9p-3, -0x1.8af8af8af8af9p-3,
-    0x0.0p+0, 0x0.0p+0, 0x1.283a83a83a83bp-4, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-5, 0x1.283a83a83a83bp-4,
-    0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-3, 0x0.0p+0, -0x1.8af8af8af8af9p-3, -0x1.8af8af8af8af9p-4, -0x1.8af8af8af8af9p-3,
-    0x0.0p+0, 0x1.283a83a83a83bp-4, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-6, 0x1.283a83a83a83bp-4,
-    0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x0.0p+0, -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-6,
-    0x0.0p+0, -0x1.8af8af8af8af9p-6, 0x0.0p+0, -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-6,
-    0x1.8af8af8af8af9p-6, 0x0.0p+0, -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-5, 0x0.0p+0, -0x1.8af8af8af8af9p-6,
-    0x0.0p+0, 0x0.0p+0, -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-6,
-    -0x1.8af8af8af8af9p-3, -0x1.283a83a83a83bp-4, -0x1.283a83a83a83bp-4, -0x1.8af8af8af8af9p-3, -0x1.8af8af8af8af9p-3, -0x1.283a83a83a83bp-3,
-    0x1.edb6db6db6db7p-3, 0x1.8af8af8af8af9p-3, 0x1.8af8af8af8af9p-3, 0x1.8af8af8af8af9p-3, 0x1.8af8af8af8af9p-3, 0x1.8af8af8af8af9p-2,
-    0x0.0p+0, -0x1.8af8af8af8af9p-4, -0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-3,
-    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-5, 0x0.0p+0,
-    -0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-4, 0x0.0p+0, 0x1.8af8af8af8af9p-4, 0x1.edb6db6db6db7p-3, 0x1.8af8af8af8af9p-4,
-    -0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x1.8af8af8af8af9p-4, 0x1.edb6db6db6db7p-3, 0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-4,
-    -0x1.0750750750750p-5, -0x1.0750750750750p-5, -0x1.0750750750750p-5, -0x1.0750750750750p-4, -0x1.0750750750750p-4, -0x1.0750750750750p-4,
-    0x1.0750750750750p-5, 0x0.0p+0, 0x0.0p+0, -0x1.0750750750750p-6, -0x1.0750750750750p-6, 0x0.0p+0,
-    0x0.0p+0, 0x1.0750750750750p-5, 0x0.0p+0, -0x1.0750750750750p-6, 0x0.0p+0, -0x1.0750750750750p-6,
-    0x0.0p+0, 0x0.0p+0, 0x1.0750750750750p-5, 0x0.0p+0, -0x1.0750750750750p-6, -0x1.0750750750750p-6,
-    0x0.0p+0, -0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-4, 0x1.edb6db6db6db7p-3, 0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-4,
-    0x0.0p+0, 0x1.8af8af8af8af9p-4, -0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-4, 0x1.edb6db6db6db7p-3, 0x1.8af8af8af8af9p-4,
-    -0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x1.8af8af8af8af9p-4, 0x1.edb6db6db6db7p-3, 0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-4,
-    0x1.8af8af8af8af9p-4, 0x0.0p+0, -0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-4, 0x1.edb6db6db6db7p-3,
-    -0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-4, 0x0.0p+0, 0x1.8af8af8af8af9p-4, 0x1.edb6db6db6db7p-3, 0x1.8af8af8af8af9p-4,
-    0x1.8af8af8af8af9p-4, -0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-4, 0x1.edb6db6db6db7p-3,
-    0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5,
-    -0x1.8af8af8af8af9p-4, -0x1.8af8af8af8af9p-4, 0x0.0p+0, -0x1.8af8af8af8af9p-3, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5,
-    0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-5,
-    -0x1.8af8af8af8af9p-4, 0x0.0p+0, -0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-3, 0x1.8af8af8af8af9p-5,
-    0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-4,
-    0x0.0p+0, -0x1.8af8af8af8af9p-4, -0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-3,
-    0x1.283a83a83a83bp-1, 0x1.283a83a83a83bp-1, 0x1.283a83a83a83bp-1, 0x1.283a83a83a83bp-1, 0x1.283a83a83a83bp-1, 0x1.283a83a83a83bp-1,
-    -0x1.283a83a83a83bp-1, 0x0.0p+0, 0x0.0p+0, -0x1.283a83a83a83bp-1, -0x1.283a83a83a83bp-1, -0x1.283a83a83a83bp-2,
-    0x0.0p+0, -0x1.283a83a83a83bp-1, 0x0.0p+0, -0x1.283a83a83a83bp-1, -0x1.283a83a83a83bp-2, -0x1.283a83a83a83bp-1,
-    0x0.0p+0, 0x0.0p+0, -0x1.283a83a83a83bp-1, -0x1.283a83a83a83bp-2, -0x1.283a83a83a83bp-1, -0x1.283a83a83a83bp-1,
-    0x1.0750750750750p-5, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5, 0x1.4924924924925p-4, 0x1.4924924924925p-4, 0x1.8af8af8af8af9p-4,
-    -0x1.0750750750750p-5, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
-    0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x1.0750750750750p-6, 0x0.0p+0, 0x0.0p+0,
-    0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x1.0750750750750p-6, 0x0.0p+0,
-    0x0.0p+0, -0x1.283a83a83a83bp-2, 0x0.0p+0, -0x1.edb6db6db6db7p-3, -0x1.8af8af8af8af9p-4, -0x1.edb6db6db6db7p-3,
-    0x0.0p+0, 0x0.0p+0, -0x1.283a83a83a83bp-2, -0x1.8af8af8af8af9p-4, -0x1.edb6db6db6db7p-3, -0x1.edb6db6db6db7p-3,
-    0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0,
-    -0x1.8af8af8af8af9p-4, 0x0.0p+0, -0x1.283a83a83a83bp-3, 0x0.0p+0, -0x1.edb6db6db6db7p-3, 0x0.0p+0,
-    0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x0.0p+0,
-    -0x1.8af8af8af8af9p-4, -0x1.283a83a83a83bp-3, 0x0.0p+0, -0x1.edb6db6db6db7p-3, 0x0.0p+0, 0x0.0p+0,
-    -0x1.8af8af8af8af9p-5, -0x1.283a83a83a83bp-2, -0x1.8af8af8af8af9p-5, -0x1.599999999999ap-2, -0x1.8af8af8af8af9p-3, -0x1.599999999999ap-2,
-    0x1.8af8af8af8af9p-4, 0x0.0p+0, -0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-4, 0x1.edb6db6db6db7p-3,
-    -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-5, -0x1.283a83a83a83bp-2, -0x1.8af8af8af8af9p-3, -0x1.599999999999ap-2, -0x1.599999999999ap-2,
-    0x1.8af8af8af8af9p-4, -0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-4, 0x1.edb6db6db6db7p-3,
-    0x0.0p+0, -0x1.283a83a83a83bp-3, -0x1.283a83a83a83bp-3, -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-5, -0x1.283a83a83a83bp-2,
-    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-5, 0x0.0p+0,
-    -0x1.283a83a83a83bp-1, 0x0.0p+0, 0x0.0p+0, -0x1.283a83a83a83bp-1, -0x1.283a83a83a83bp-1, -0x1.283a83a83a83bp-2,
-    0x1.283a83a83a83bp-1, 0x1.283a83a83a83bp-1, 0x1.283a83a83a83bp-1, 0x1.283a83a83a83bp-1, 0x1.283a83a83a83bp-1, 0x1.283a83a83a83bp-1,
-    0x0.0p+0, 0x0.0p+0, 0x1.283a83a83a83bp-2, 0x1.283a83a83a83bp-1, 0x1.283a83a83a83bp-2, 0x1.283a83a83a83bp-2,
-    0x0.0p+0, 0x1.283a83a83a83bp-2, 0x0.0p+0, 0x1.283a83a83a83bp-2, 0x1.283a83a83a83bp-1, 0x1.283a83a83a83bp-2,
-    0x1.8af8af8af8af9p-5, 0x1.0750750750750p-5, 0x1.8af8af8af8af9p-5, 0x1.4924924924925p-4, 0x1.8af8af8af8af9p-4, 0x1.4924924924925p-4,
-    0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x0.0p+0, 0x1.0750750750750p-6, 0x0.0p+0, 0x0.0p+0,
-    0x0.0p+0, -0x1.0750750750750p-5, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
-    0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x0.0p+0, 0x1.0750750750750p-6,
-    0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-5,
-    0x0.0p+0, -0x1.8af8af8af8af9p-4, -0x1.283a83a83a83bp-3, 0x0.0p+0, 0x0.0p+0, -0x1.edb6db6db6db7p-3,
-    -0x1.283a83a83a83bp-2, 0x0.0p+0, 0x0.0p+0, -0x1.edb6db6db6db7p-3, -0x1.edb6db6db6db7p-3, -0x1.8af8af8af8af9p-4,
-    0x0.0p+0, 0x0.0p+0, -0x1.283a83a83a83bp-2, -0x1.8af8af8af8af9p-4, -0x1.edb6db6db6db7p-3, -0x1.edb6db6db6db7p-3,
-    -0x1.283a83a83a83bp-3, -0x1.8af8af8af8af9p-4, 0x0.0p+0, -0x1.edb6db6db6db7p-3, 0x0.0p+0, 0x0.0p+0,
-    0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x0.0p+0,
-    -0x1.283a83a83a83bp-2, -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-5, -0x1.599999999999ap-2, -0x1.599999999999ap-2, -0x1.8af8af8af8af9p-3,
-    0x0.0p+0, 0x1.8af8af8af8af9p-4, -0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-4, 0x1.edb6db6db6db7p-3, 0x1.8af8af8af8af9p-4,
-    -0x1.283a83a83a83bp-3, 0x0.0p+0, -0x1.283a83a83a83bp-3, -0x1.8af8af8af8af9p-5, -0x1.283a83a83a83bp-2, -0x1.8af8af8af8af9p-5,
-    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, -0x1.8af8af8af8af9p-5, 0x0.0p+0, -0x1.8af8af8af8af9p-5,
-    -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-5, -0x1.283a83a83a83bp-2, -0x1.8af8af8af8af9p-3, -0x1.599999999999ap-2, -0x1.599999999999ap-2,
-    -0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-4, 0x0.0p+0, 0x1.8af8af8af8af9p-4, 0x1.edb6db6db6db7p-3, 0x1.8af8af8af8af9p-4,
-    0x0.0p+0, -0x1.283a83a83a83bp-1, 0x0.0p+0, -0x1.283a83a83a83bp-1, -0x1.283a83a83a83bp-2, -0x1.283a83a83a83bp-1,
-    0x0.0p+0, 0x0.0p+0, 0x1.283a83a83a83bp-2, 0x1.283a83a83a83bp-1, 0x1.283a83a83a83bp-2, 0x1.283a83a83a83bp-2,
-    0x1.283a83a83a83bp-1, 0x1.283a83a83a83bp-1, 0x1.283a83a83a83bp-1, 0x1.283a83a83a83bp-1, 0x1.283a83a83a83bp-1, 0x1.283a83a83a83bp-1,
-    0x1.283a83a83a83bp-2, 0x0.0p+0, 0x0.0p+0, 0x1.283a83a83a83bp-2, 0x1.283a83a83a83bp-2, 0x1.283a83a83a83bp-1,
-    0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5, 0x1.0750750750750p-5, 0x1.8af8af8af8af9p-4, 0x1.4924924924925p-4, 0x1.4924924924925p-4,
-    0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.0750750750750p-6, 0x0.0p+0,
-    0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.0750750750750p-6,
-    0x0.0p+0, 0x0.0p+0, -0x1.0750750750750p-5, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
-    0x0.0p+0, -0x1.283a83a83a83bp-3, -0x1.8af8af8af8af9p-4, 0x0.0p+0, 0x0.0p+0, -0x1.edb6db6db6db7p-3,
-    0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-5,
-    -0x1.283a83a83a83bp-3, 0x0.0p+0, -0x1.8af8af8af8af9p-4, 0x0.0p+0, -0x1.edb6db6db6db7p-3, 0x0.0p+0,
-    0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0,
-    -0x1.283a83a83a83bp-2, 0x0.0p+0, 0x0.0p+0, -0x1.edb6db6db6db7p-3, -0x1.edb6db6db6db7p-3, -0x1.8af8af8af8af9p-4,
-    0x0.0p+0, -0x1.283a83a83a83bp-2, 0x0.0p+0, -0x1.edb6db6db6db7p-3, -0x1.8af8af8af8af9p-4, -0x1.edb6db6db6db7p-3,
-    -0x1.283a83a83a83bp-3, -0x1.283a83a83a83bp-3, 0x0.0p+0, -0x1.283a83a83a83bp-2, -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-5,
-    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-5,
-    -0x1.283a83a83a83bp-2, -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-5, -0x1.599999999999ap-2, -0x1.599999999999ap-2, -0x1.8af8af8af8af9p-3,
-    0x0.0p+0, -0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-4, 0x1.edb6db6db6db7p-3, 0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-4,
-    -0x1.8af8af8af8af9p-5, -0x1.283a83a83a83bp-2, -0x1.8af8af8af8af9p-5, -0x1.599999999999ap-2, -0x1.8af8af8af8af9p-3, -0x1.599999999999ap-2,
-    -0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x1.8af8af8af8af9p-4, 0x1.edb6db6db6db7p-3, 0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-4,
-    0x0.0p+0, 0x0.0p+0, -0x1.283a83a83a83bp-1, -0x1.283a83a83a83bp-2, -0x1.283a83a83a83bp-1, -0x1.283a83a83a83bp-1,
-    0x0.0p+0, 0x1.283a83a83a83bp-2, 0x0.0p+0, 0x1.283a83a83a83bp-2, 0x1.283a83a83a83bp-1, 0x1.283a83a83a83bp-2,
-    0x1.283a83a83a83bp-2, 0x0.0p+0, 0x0.0p+0, 0x1.283a83a83a83bp-2, 0x1.283a83a83a83bp-2, 0x1.283a83a83a83bp-1,
-    0x1.283a83a83a83bp-1, 0x1.283a83a83a83bp-1, 0x1.283a83a83a83bp-1, 0x1.283a83a83a83bp-1, 0x1.283a83a83a83bp-1, 0x1.283a83a83a83bp-1,
-};
-
-__device__ const float kP3StiffF[2400] = {
-    0.05952380952380952f, 0.05952380952380952f, 0.05952380952380952f, 0.11904761904761904f, 0.11904761904761904f, 0.11904761904761904f,
-    -0.01130952380952381f, 0.0f, 0.0f, -0.01130952380952381f, -0.01130952380952381f, 0.0f,
-    0.0f, -0.01130952380952381f, 0.0f, -0.01130952380952381f, 0.0f, -0.01130952380952381f,
-    0.0f, 0.0f, -0.01130952380952381f, 0.0f, -0.01130952380952381f, -0.01130952380952381f,
-    0.0f, -0.013392857142857142f, -0.013392857142857142f, -0.013392857142857142f, -0.013392857142857142f, -0.026785714285714284f,
-    0.0f, -0.013392857142857142f, -0.013392857142857142f, -0.013392857142857142f, -0.013392857142857142f, -0.026785714285714284f,
-    -0.013392857142857142f, 0.0f, -0.013392857142857142f, -0.013392857142857142f, -0.026785714285714284f, -0.013392857142857142f,
-    -0.013392857142857142f, 0.0f, -0.013392857142857142f, -0.013392857142857142f, -0.026785714285714284f, -0.013392857142857142f,
-    -0.013392857142857142f, -0.013392857142857142f, 0.0f, -0.026785714285714284f, -0.013392857142857142f, -0.013392857142857142f,
-    -0.013392857142857142f, -0.013392857142857142f, 0.0f, -0.026785714285714284f, -0.013392857142857142f, -0.013392857142857142f,
-    -0.03482142857142857f, -0.03482142857142857f, -0.09642857142857143f, -0.06964285714285715f, -0.13125f, -0.13125f,
-    0.013392857142857142f, 0.013392857142857142f, 0.048214285714285716f, 0.026785714285714284f, 0.06160714285714286f, 0.06160714285714286f,
-    -0.03482142857142857f, -0.09642857142857143f, -0.03482142857142857f, -0.13125f, -0.06964285714285715f, -0.13125f,
-    0.013392857142857142f, 0.048214285714285716f, 0.013392857142857142f, 0.06160714285714286f, 0.026785714285714284f, 0.06160714285714286f,
-    -0.09642857142857143f, -0.03482142857142857f, -0.03482142857142857f, -0.13125f, -0.13125f, -0.06964285714285715f,
-    0.048214285714285716f, 0.013392857142857142f, 0.013392857142857142f, 0.06160714285714286f, 0.06160714285714286f, 0.026785714285714284f,
-    -0.03214285714285714f, -0.03214285714285714f, -0.03214285714285714f, -0.06428571428571428f, -0.06428571428571428f, -0.06428571428571428f,
-    0.03214285714285714f, 0.048214285714285716f, 0.048214285714285716f, 0.08035714285714286f, 0.08035714285714286f, 0.09642857142857143f,
-    0.048214285714285716f, 0.03214285714285714f, 0.048214285714285716f, 0.08035714285714286f, 0.09642857142857143f, 0.08035714285714286f,
-    0.048214285714285716f, 0.048214285714285716f, 0.03214285714285714f, 0.09642857142857143f, 0.08035714285714286f, 0.08035714285714286f,
-    -0.01130952380952381f, 0.0f, 0.0f, -0.01130952380952381f, -0.01130952380952381f, 0.0f,
-    0.05952380952380952f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f,
-    0.0f, 0.0f, 0.0f, 0.01130952380952381f, 0.0f, 0.0f,
-    0.0f, 0.0f, 0.0f, 0.0f, 0.01130952380952381f, 0.0f,
-    0.0f, 0.0f, 0.0f, 0.013392857142857142f, 0.013392857142857142f, 0.0f,
-    0.0f, 0.0f, 0.0f, 0.013392857142857142f, 0.013392857142857142f, 0.0f,
-    -0.03482142857142857f, 0.0f, 0.0f, 0.0f, 0.06160714285714286f, 0.0f,
-    0.013392857142857142f, 0.0f, 0.0f, 0.0f, -0.03482142857142857f, 0.0f,
-    -0.03482142857142857f, 0.0f, 0.0f, 0.06160714285714286f, 0.0f, 0.0f,
-    0.013392857142857142f, 0.0f, 0.0f, -0.03482142857142857f, 0.0f, 0.0f,
-    -0.013392857142857142f, 0.0f, 0.0f, -0.013392857142857142f, 0.0f, 0.0f,
-    -0.013392857142857142f, 0.0f, 0.0f, -0.013392857142857142f, 0.0f, 0.0f,
-    -0.013392857142857142f, 0.0f, 0.0f, 0.0f, -0.013392857142857142f, 0.0f,
-    -0.013392857142857142f, 0.0f, 0.0f, 0.0f, -0.013392857142857142f, 0.0f,
-    0.048214285714285716f, 0.0f, 0.0f, 0.03482142857142857f, 0.03482142857142857f, 0.0f,
-    -0.09642857142857143f, 0.0f, 0.0f, -0.06160714285714286f, -0.06160714285714286f, 0.0f,
-    0.03214285714285714f, 0.0f, 0.0f, -0.01607142857142857f, -0.01607142857142857f, 0.0f,
-    -0.03214285714285714f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f,
-    0.048214285714285716f, 0.0f, 0.0f, 0.01607142857142857f, 0.0f, 0.0f,
-    0.048214285714285716f, 0.0f, 0.0f, 0.0f, 0.01607142857142857f, 0.0f,
-    0.0f, -0.01130952380952381f, 0.0f, -0.01130952380952381f, 0.0f, -0.01130952380952381f,
-    0.0f, 0.0f, 0.0f, 0.01130952380952381f, 0.0f, 0.0f,
-    0.0f, 0.05952380952380952f, 0.0f, 0.0f, 0.0f, 0.0f,
-    0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.01130952380952381f,
-    0.0f, -0.03482142857142857f, 0.0f, 0.0f, 0.0f, 0.06160714285714286f,
-    0.0f, 0.013392857142857142f, 0.0f, 0.0f, 0.0f, -0.03482142857142857f,
-    0.0f, 0.0f, 0.0f, 0.013392857142857142f, 0.0f, 0.013392857142857142f,
-    0.0f, 0.0f, 0.0f, 0.013392857142857142f, 0.0f, 0.013392857142857142f,
-    0.0f, 0.013392857142857142f, 0.0f, -0.03482142857142857f, 0.0f, 0.0f,
-    0.0f, -0.03482142857142857f, 0.0f, 0.06160714285714286f, 0.0f, 0.0f,
-    0.0f, -0.013392857142857142f, 0.0f, -0.013392857142857142f, 0.0f, 0.0f,
-    0.0f, -0.013392857142857142f, 0.0f, -0.013392857142857142f, 0.0f, 0.0f,
-    0.0f, 0.048214285714285716f, 0.0f, 0.03482142857142857f, 0.0f, 0.03482142857142857f,
-    0.0f, -0.09642857142857143f, 0.0f, -0.06160714285714286f, 0.0f, -0.06160714285714286f,
-    0.0f, -0.013392857142857142f, 0.0f, 0.0f, 0.0f, -0.013392857142857142f,
-    0.0f, -0.013392857142857142f, 0.0f, 0.0f, 0.0f, -0.013392857142857142f,
-    0.0f, 0.03214285714285714f, 0.0f, -0.01607142857142857f, 0.0f, -0.01607142857142857f,
-    0.0f, 0.048214285714285716f, 0.0f, 0.01607142857142857f, 0.0f, 0.0f,
-    0.0f, -0.03214285714285714f, 0.0f, 0.0f, 0.0f, 0.0f,
-    0.0f, 0.048214285714285716f, 0.0f, 0.0f, 0.0f, 0.01607142857142857f,
-    0.0f, 0.0f, -0.01130952380952381f, 0.0f, -0.01130952380952381f, -0.01130952380952381f,
-    0.0f, 0.0f, 0.0f, 0.0f, 0.01130952380952381f, 0.0f,
-    0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.01130952380952381f,
-    0.0f, 0.0f, 0.05952380952380952f, 0.0f, 0.0f, 0.0f,
-    0.0f, 0.0f, 0.013392857142857142f, 0.0f, 0.0f, -0.03482142857142857f,
-    0.0f, 0.0f, -0.03482142857142857f, 0.0f, 0.0f, 0.06160714285714286f,
-    0.0f, 0.0f, 0.013392857142857142f, 0.0f, -0.03482142857142857f, 0.0f,
-    0.0f, 0.0f, -0.03482142857142857f, 0.0f, 0.06160714285714286f, 0.0f,
-    0.0f, 0.0f, 0.0f, 0.0f, 0.013392857142857142f, 0.013392857142857142f,
-    0.0f, 0.0f, 0.0f, 0.0f, 0.013392857142857142f, 0.013392857142857142f,
-    0.0f, 0.0f, 0.048214285714285716f, 0.0f, 0.03482142857142857f, 0.03482142857142857f,
-    0.0f, 0.0f, -0.09642857142857143f, 0.0f, -0.06160714285714286f, -0.06160714285714286f,
-    0.0f, 0.0f, -0.013392857142857142f, 0.0f, -0.013392857142857142f, 0.0f,
-    0.0f, 0.0f, -0.013392857142857142f, 0.0f, -0.013392857142857142f, 0.0f,
-    0.0f, 0.0f, -0.013392857142857142f, 0.0f, 0.0f, -0.013392857142857142f,
-    0.0f, 0.0f, -0.013392857142857142f, 0.0f, 0.0f, -0.013392857142857142f,
-    0.0f, 0.0f, 0.03214285714285714f, 0.0f, -0.01607142857142857f, -0.01607142857142857f,
-    0.0f, 0.0f, 0.048214285714285716f, 0.0f, 0.01607142857142857f, 0.0f,
-    0.0f, 0.0f, 0.048214285714285716f, 0.0f, 0.0f, 0.01607142857142857f,
-    0.0f, 0.0f, -0.03214285714285714f, 0.0f, 0.0f, 0.0f,
-    0.0f, -0.013392857142857142f, -0.013392857142857142f, -0.013392857142857142f, -0.013392857142857142f, -0.026785714285714284f,
-    0.0f, 0.0f, 0.0f, 0.013392857142857142f, 0.013392857142857142f, 0.0f,
-    0.0f, -0.03482142857142857f, 0.0f, 0.0f, 0.0f, 0.06160714285714286f,
-    0.0f, 0.0f, 0.013392857142857142f, 0.0f, 0.0f, -0.03482142857142857f,
-    0.0f, 0.24107142857142858f, 0.19285714285714287f, 0.0f, 0.0f, 0.19285714285714287f,
-    0.0f, -0.07232142857142858f, -0.07232142857142858f, 0.0f, 0.0f, 0.048214285714285716f,
-    0.0f, 0.0f, -0.024107142857142858f, -0.048214285714285716f, -0.024107142857142858f, -0.024107142857142858f,
-    0.0f, 0.0f, -0.024107142857142858f, -0.07232142857142858f, -0.024107142857142858f, -0.048214285714285716f,
-    0.0f, -0.024107142857142858f, 0.0f, -0.048214285714285716f, -0.07232142857142858f, -0.024107142857142858f,
-    0.0f, 0.12053571428571429f, 0.0f, 0.09642857142857143f, 0.19285714285714287f, 0.09642857142857143f,
-    0.0f, 0.048214285714285716f, 0.0f, 0.048214285714285716f, 0.024107142857142858f, 0.048214285714285716f,
-    0.0f, 0.07232142857142858f, 0.0f, 0.07232142857142858f, 0.024107142857142858f, 0.048214285714285716f,
-    0.0f, 0.024107142857142858f, 0.07232142857142858f, 0.048214285714285716f, 0.07232142857142858f, 0.09642857142857143f,
-    0.0f, 0.024107142857142858f, -0.19285714285714287f, -0.09642857142857143f, -0.19285714285714287f, -0.19285714285714287f,
-    0.0f, 0.024107142857142858f, 0.024107142857142858f, 0.0f, 0.0f, 0.048214285714285716f,
-    0.0f, 0.024107142857142858f, 0.024107142857142858f, 0.0f, 0.0f, 0.048214285714285716f,
-    0.0f, -0.048214285714285716f, 0.09642857142857143f, 0.24107142857142858f, 0.09642857142857143f, 0.09642857142857143f,
-    0.0f, -0.2892857142857143f, 0.0f, -0.24107142857142858f, -0.09642857142857143f, -0.24107142857142858f,
-    0.0f, 0.048214285714285716f, 0.0f, 0.0f, 0.0f, 0.048214285714285716f,
-    0.0f, -0.14464285714285716f, -0.09642857142857143f, 0.0f, 0.0f, -0.24107142857142858f,
-    0.0f, -0.013392857142857142f, -0.013392857142857142f, -0.013392857142857142f, -0.013392857142857142f, -0.026785714285714284f,
-    0.0f, 0.0f, 0.0f, 0.013392857142857142f, 0.013392857142857142f, 0.0f,
-    0.0f, 0.013392857142857142f, 0.0f, 0.0f, 0.0f, -0.03482142857142857f,
-    0.0f, 0.0f, -0.03482142857142857f, 0.0f, 0.0f, 0.06160714285714286f,
-    0.0f, -0.07232142857142858f, -0.07232142857142858f, 0.0f, 0.0f, 0.048214285714285716f,
-    0.0f, 0.19285714285714287f, 0.24107142857142858f, 0.0f, 0.0f, 0.19285714285714287f,
-    0.0f, 0.0f, -0.024107142857142858f, -0.07232142857142858f, -0.048214285714285716f, -0.024107142857142858f,
-    0.0f, 0.0f, 0.12053571428571429f, 0.19285714285714287f, 0.09642857142857143f, 0.09642857142857143f,
-    0.0f, -0.024107142857142858f, 0.0f, -0.024107142857142858f, -0.048214285714285716f, -0.024107142857142858f,
-    0.0f, -0.024107142857142858f, 0.0f, -0.024107142857142858f, -0.07232142857142858f, -0.048214285714285716f,
-    0.0f, 0.07232142857142858f, 0.024107142857142858f, 0.07232142857142858f, 0.048214285714285716f, 0.09642857142857143f,
-    0.0f, -0.19285714285714287f, 0.024107142857142858f, -0.19285714285714287f, -0.09642857142857143f, -0.19285714285714287f,
-    0.0f, 0.0f, 0.048214285714285716f, 0.024107142857142858f, 0.048214285714285716f, 0.048214285714285716f,
-    0.0f, 0.0f, 0.07232142857142858f, 0.024107142857142858f, 0.07232142857142858f, 0.048214285714285716f,
-    0.0f, 0.024107142857142858f, 0.024107142857142858f, 0.0f, 0.0f, 0.048214285714285716f,
-    0.0f, 0.024107142857142858f, 0.024107142857142858f, 0.0f, 0.0f, 0.048214285714285716f,
-    0.0f, 0.09642857142857143f, -0.048214285714285716f, 0.09642857142857143f, 0.24107142857142858f, 0.09642857142857143f,
-    0.0f, 0.0f, -0.2892857142857143f, -0.09642857142857143f, -0.24107142857142858f, -0.24107142857142858f,
-    0.0f, -0.09642857142857143f, -0.14464285714285716f, 0.0f, 0.0f, -0.24107142857142858f,
-    0.0f, 0.0f, 0.048214285714285716f, 0.0f, 0.0f, 0.048214285714285716f,
-    -0.013392857142857142f, 0.0f, -0.013392857142857142f, -0.013392857142857142f, -0.026785714285714284f, -0.013392857142857142f,
-    -0.03482142857142857f, 0.0f, 0.0f, 0.0f, 0.06160714285714286f, 0.0f,
-    0.0f, 0.0f, 0.0f, 0.013392857142857142f, 0.0f, 0.013392857142857142f,
-    0.0f, 0.0f, 0.013392857142857142f, 0.0f, -0.03482142857142857f, 0.0f,
-    0.0f, 0.0f, -0.024107142857142858f, -0.048214285714285716f, -0.024107142857142858f, -0.024107142857142858f,
-    0.0f, 0.0f, -0.024107142857142858f, -0.07232142857142858f, -0.048214285714285716f, -0.024107142857142858f,
-    0.24107142857142858f, 0.0f, 0.19285714285714287f, 0.0f, 0.19285714285714287f, 0.0f,
-    -0.07232142857142858f, 0.0f, -0.07232142857142858f, 0.0f, 0.048214285714285716f, 0.0f,
-    0.12053571428571429f, 0.0f, 0.0f, 0.09642857142857143f, 0.09642857142857143f, 0.19285714285714287f,
-    -0.024107142857142858f, 0.0f, 0.0f, -0.048214285714285716f, -0.024107142857142858f, -0.07232142857142858f,
-    0.048214285714285716f, 0.0f, 0.0f, 0.048214285714285716f, 0.048214285714285716f, 0.024107142857142858f,
-    0.07232142857142858f, 0.0f, 0.0f, 0.07232142857142858f, 0.048214285714285716f, 0.024107142857142858f,
-    0.024107142857142858f, 0.0f, 0.024107142857142858f, 0.0f, 0.048214285714285716f, 0.0f,
-    0.024107142857142858f, 0.0f, 0.024107142857142858f, 0.0f, 0.048214285714285716f, 0.0f,
-    0.024107142857142858f, 0.0f, 0.07232142857142858f, 0.048214285714285716f, 0.09642857142857143f, 0.07232142857142858f,
-    0.024107142857142858f, 0.0f, -0.19285714285714287f, -0.09642857142857143f, -0.19285714285714287f, -0.19285714285714287f,
-    -0.048214285714285716f, 0.0f, 0.09642857142857143f, 0.24107142857142858f, 0.09642857142857143f, 0.09642857142857143f,
-    0.048214285714285716f, 0.0f, 0.0f, 0.0f, 0.048214285714285716f, 0.0f,
-    -0.2892857142857143f, 0.0f, 0.0f, -0.24107142857142858f, -0.24107142857142858f, -0.09642857142857143f,
-    -0.14464285714285716f, 0.0f, -0.09642857142857143f, 0.0f, -0.24107142857142858f, 0.0f,
-    -0.013392857142857142f, 0.0f, -0.013392857142857142f, -0.013392857142857142f, -0.026785714285714284f, -0.013392857142857142f,
-    0.013392857142857142f, 0.0f, 0.0f, 0.0f, -0.03482142857142857f, 0.0f,
-    0.0f, 0.0f, 0.0f, 0.013392857142857142f, 0.0f, 0.013392857142857142f,
-    0.0f, 0.0f, -0.03482142857142857f, 0.0f, 0.06160714285714286f, 0.0f,
-    0.0f, 0.0f, -0.024107142857142858f, -0.07232142857142858f, -0.024107142857142858f, -0.048214285714285716f,
-    0.0f, 0.0f, 0.12053571428571429f, 0.19285714285714287f, 0.09642857142857143f, 0.09642857142857143f,
-    -0.07232142857142858f, 0.0f, -0.07232142857142858f, 0.0f, 0.048214285714285716f, 0.0f,
-    0.19285714285714287f, 0.0f, 0.24107142857142858f, 0.0f, 0.19285714285714287f, 0.0f,
-    -0.024107142857142858f, 0.0f, 0.0f, -0.024107142857142858f, -0.048214285714285716f, -0.07232142857142858f,
-    -0.024107142857142858f, 0.0f, 0.0f, -0.024107142857142858f, -0.024107142857142858f, -0.048214285714285716f,
-    0.07232142857142858f, 0.0f, 0.024107142857142858f, 0.07232142857142858f, 0.09642857142857143f, 0.048214285714285716f,
-    -0.19285714285714287f, 0.0f, 0.024107142857142858f, -0.19285714285714287f, -0.19285714285714287f, -0.09642857142857143f,
-    0.024107142857142858f, 0.0f, 0.024107142857142858f, 0.0f, 0.048214285714285716f, 0.0f,
-    0.024107142857142858f, 0.0f, 0.024107142857142858f, 0.0f, 0.048214285714285716f, 0.0f,
-    0.0f, 0.0f, 0.048214285714285716f, 0.024107142857142858f, 0.048214285714285716f, 0.048214285714285716f,
-    0.0f, 0.0f, 0.07232142857142858f, 0.024107142857142858f, 0.048214285714285716f, 0.07232142857142858f,
-    0.09642857142857143f, 0.0f, -0.048214285714285716f, 0.09642857142857143f, 0.09642857142857143f, 0.24107142857142858f,
-    -0.09642857142857143f, 0.0f, -0.14464285714285716f, 0.0f, -0.24107142857142858f, 0.0f,
-    0.0f, 0.0f, -0.2892857142857143f, -0.09642857142857143f, -0.24107142857142858f, -0.24107142857142858f,
-    0.0f, 0.0f, 0.048214285714285716f, 0.0f, 0.048214285714285716f, 0.0f,
-    -0.013392857142857142f, -0.013392857142857142f, 0.0f, -0.026785714285714284f, -0.013392857142857142f, -0.013392857142857142f,
-    -0.03482142857142857f, 0.0f, 0.0f, 0.06160714285714286f, 0.0f, 0.0f,
-    0.0f, 0.013392857142857142f, 0.0f, -0.03482142857142857f, 0.0f, 0.0f,
-    0.0f, 0.0f, 0.0f, 0.0f, 0.013392857142857142f, 0.013392857142857142f,
-    0.0f, -0.024107142857142858f, 0.0f, -0.048214285714285716f, -0.07232142857142858f, -0.024107142857142858f,
-    0.0f, -0.024107142857142858f, 0.0f, -0.024107142857142858f, -0.048214285714285716f, -0.024107142857142858f,
-    0.12053571428571429f, 0.0f, 0.0f, 0.09642857142857143f, 0.09642857142857143f, 0.19285714285714287f,
-    -0.024107142857142858f, 0.0f, 0.0f, -0.024107142857142858f, -0.048214285714285716f, -0.07232142857142858f,
-    0.24107142857142858f, 0.19285714285714287f, 0.0f, 0.19285714285714287f, 0.0f, 0.0f,
-    -0.07232142857142858f, -0.07232142857142858f, 0.0f, 0.048214285714285716f, 0.0f, 0.0f,
-    0.024107142857142858f, 0.024107142857142858f, 0.0f, 0.048214285714285716f, 0.0f, 0.0f,
-    0.024107142857142858f, 0.024107142857142858f, 0.0f, 0.048214285714285716f, 0.0f, 0.0f,
-    0.048214285714285716f, 0.0f, 0.0f, 0.048214285714285716f, 0.048214285714285716f, 0.024107142857142858f,
-    0.07232142857142858f, 0.0f, 0.0f, 0.048214285714285716f, 0.07232142857142858f, 0.024107142857142858f,
-    0.024107142857142858f, 0.07232142857142858f, 0.0f, 0.09642857142857143f, 0.048214285714285716f, 0.07232142857142858f,
-    0.024107142857142858f, -0.19285714285714287f, 0.0f, -0.19285714285714287f, -0.09642857142857143f, -0.19285714285714287f,
-    -0.048214285714285716f, 0.09642857142857143f, 0.0f, 0.09642857142857143f, 0.24107142857142858f, 0.09642857142857143f,
-    0.048214285714285716f, 0.0f, 0.0f, 0.048214285714285716f, 0.0f, 0.0f,
-    -0.14464285714285716f, -0.09642857142857143f, 0.0f, -0.24107142857142858f, 0.0f, 0.0f,
-    -0.2892857142857143f, 0.0f, 0.0f, -0.24107142857142858f, -0.24107142857142858f, -0.09642857142857143f,
-    -0.013392857142857142f, -0.013392857142857142f, 0.0f, -0.026785714285714284f, -0.013392857142857142f, -0.013392857142857142f,
-    0.013392857142857142f, 0.0f, 0.0f, -0.03482142857142857f, 0.0f, 0.0f,
-    0.0f, -0.03482142857142857f, 0.0f, 0.06160714285714286f, 0.0f, 0.0f,
-    0.0f, 0.0f, 0.0f, 0.0f, 0.013392857142857142f, 0.013392857142857142f,
-    0.0f, 0.12053571428571429f, 0.0f, 0.09642857142857143f, 0.19285714285714287f, 0.09642857142857143f,
-    0.0f, -0.024107142857142858f, 0.0f, -0.024107142857142858f, -0.07232142857142858f, -0.048214285714285716f,
-    -0.024107142857142858f, 0.0f, 0.0f, -0.048214285714285716f, -0.024107142857142858f, -0.07232142857142858f,
-    -0.024107142857142858f, 0.0f, 0.0f, -0.024107142857142858f, -0.024107142857142858f, -0.048214285714285716f,
-    -0.07232142857142858f, -0.07232142857142858f, 0.0f, 0.048214285714285716f, 0.0f, 0.0f,
-    0.19285714285714287f, 0.24107142857142858f, 0.0f, 0.19285714285714287f, 0.0f, 0.0f,
-    0.024107142857142858f, 0.024107142857142858f, 0.0f, 0.048214285714285716f, 0.0f, 0.0f,
-    0.024107142857142858f, 0.024107142857142858f, 0.0f, 0.048214285714285716f, 0.0f, 0.0f,
-    0.07232142857142858f, 0.024107142857142858f, 0.0f, 0.09642857142857143f, 0.07232142857142858f, 0.048214285714285716f,
-    -0.19285714285714287f, 0.024107142857142858f, 0.0f, -0.19285714285714287f, -0.19285714285714287f, -0.09642857142857143f,
-    0.0f, 0.048214285714285716f, 0.0f, 0.048214285714285716f, 0.024107142857142858f, 0.048214285714285716f,
-    0.0f, 0.07232142857142858f, 0.0f, 0.048214285714285716f, 0.024107142857142858f, 0.07232142857142858f,
-    0.09642857142857143f, -0.048214285714285716f, 0.0f, 0.09642857142857143f, 0.09642857142857143f, 0.24107142857142858f,
-    -0.09642857142857143f, -0.14464285714285716f, 0.0f, -0.24107142857142858f, 0.0f, 0.0f,
-    0.0f, 0.048214285714285716f, 0.0f, 0.048214285714285716f, 0.0f, 0.0f,
-    0.0f, -0.2892857142857143f, 0.0f, -0.24107142857142858f, -0.09642857142857143f, -0.24107142857142858f,
-    -0.03482142857142857f, -0.03482142857142857f, -0.09642857142857143f, -0.06964285714285715f, -0.13125f, -0.13125f,
-    -0.013392857142857142f, 0.0f, 0.0f, -0.013392857142857142f, 0.0f, 0.0f,
-    0.0f, -0.013392857142857142f, 0.0f, -0.013392857142857142f, 0.0f, 0.0f,
-    0.0f, 0.0f, 0.048214285714285716f, 0.0f, 0.03482142857142857f, 0.03482142857142857f,
-    0.0f, 0.048214285714285716f, 0.0f, 0.048214285714285716f, 0.024107142857142858f, 0.048214285714285716f,
-    0.0f, 0.07232142857142858f, 0.024107142857142858f, 0.07232142857142858f, 0.048214285714285716f, 0.09642857142857143f,
-    0.048214285714285716f, 0.0f, 0.0f, 0.048214285714285716f, 0.048214285714285716f, 0.024107142857142858f,
-    0.07232142857142858f, 0.0f, 0.024107142857142858f, 0.07232142857142858f, 0.09642857142857143f, 0.048214285714285716f,
-    0.024107142857142858f, 0.024107142857142858f, 0.0f, 0.048214285714285716f, 0.0f, 0.0f,
-    0.024107142857142858f, 0.024107142857142858f, 0.0f, 0.048214285714285716f, 0.0f, 0.0f,
-    0.24107142857142858f, 0.24107142857142858f, 0.24107142857142858f, 0.48214285714285715f, 0.2892857142857143f, 0.2892857142857143f,
-    -0.07232142857142858f, -0.07232142857142858f, -0.19285714285714287f, -0.14464285714285716f, -0.19285714285714287f, -0.19285714285714287f,
-    0.12053571428571429f, 0.024107142857142858f, 0.024107142857142858f, 0.14464285714285716f, 0.14464285714285716f, 0.24107142857142858f,
-    -0.024107142857142858f, 0.024107142857142858f, 0.0f, 0.0f, -0.024107142857142858f, -0.048214285714285716f,
-    0.024107142857142858f, 0.12053571428571429f, 0.024107142857142858f, 0.14464285714285716f, 0.24107142857142858f, 0.14464285714285716f,
-    0.024107142857142858f, -0.024107142857142858f, 0.0f, 0.0f, -0.048214285714285716f, -0.024107142857142858f,
-    0.048214285714285716f, 0.048214285714285716f, 0.0f, 0.09642857142857143f, 0.048214285714285716f, 0.048214285714285716f,
-    -0.048214285714285716f, -0.2892857142857143f, -0.048214285714285716f, -0.3375f, -0.19285714285714287f, -0.3375f,
-    -0.2892857142857143f, -0.048214285714285716f, -0.048214285714285716f, -0.3375f, -0.3375f, -0.19285714285714287f,
-    -0.14464285714285716f, -0.14464285714285716f, 0.0f, -0.2892857142857143f, -0.048214285714285716f, -0.048214285714285716f,
-    0.013392857142857142f, 0.013392857142857142f, 0.048214285714285716f, 0.026785714285714284f, 0.06160714285714286f, 0.06160714285714286f,
-    -0.013392857142857142f, 0.0f, 0.0f, -0.013392857142857142f, 0.0f, 0.0f,
-    0.0f, -0.013392857142857142f, 0.0f, -0.013392857142857142f, 0.0f, 0.0f,
-    0.0f, 0.0f, -0.09642857142857143f, 0.0f, -0.06160714285714286f, -0.06160714285714286f,
-    0.0f, 0.07232142857142858f, 0.0f, 0.07232142857142858f, 0.024107142857142858f, 0.048214285714285716f,
-    0.0f, -0.19285714285714287f, 0.024107142857142858f, -0.19285714285714287f, -0.09642857142857143f, -0.19285714285714287f,
-    0.07232142857142858f, 0.0f, 0.0f, 0.07232142857142858f, 0.048214285714285716f, 0.024107142857142858f,
-    -0.19285714285714287f, 0.0f, 0.024107142857142858f, -0.19285714285714287f, -0.19285714285714287f, -0.09642857142857143f,
-    0.024107142857142858f, 0.024107142857142858f, 0.0f, 0.048214285714285716f, 0.0f, 0.0f,
-    0.024107142857142858f, 0.024107142857142858f, 0.0f, 0.048214285714285716f, 0.0f, 0.0f,
-    -0.07232142857142858f, -0.07232142857142858f, -0.19285714285714287f, -0.14464285714285716f, -0.19285714285714287f, -0.19285714285714287f,
-    0.19285714285714287f, 0.19285714285714287f, 0.24107142857142858f, 0.38571428571428573f, 0.19285714285714287f, 0.19285714285714287f,
-    -0.024107142857142858f, 0.0f, 0.024107142857142858f, -0.024107142857142858f, 0.0f, -0.048214285714285716f,
-    -0.024107142857142858f, 0.0f, 0.0f, -0.024107142857142858f, -0.024107142857142858f, -0.048214285714285716f,
-    0.0f, -0.024107142857142858f, 0.024107142857142858f, -0.024107142857142858f, -0.048214285714285716f, 0.0f,
-    0.0f, -0.024107142857142858f, 0.0f, -0.024107142857142858f, -0.048214285714285716f, -0.024107142857142858f,
-    -0.09642857142857143f, -0.09642857142857143f, 0.0f, -0.19285714285714287f, 0.048214285714285716f, 0.048214285714285716f,
-    0.09642857142857143f, 0.0f, -0.048214285714285716f, 0.09642857142857143f, 0.09642857142857143f, 0.24107142857142858f,
-    0.0f, 0.09642857142857143f, -0.048214285714285716f, 0.09642857142857143f, 0.24107142857142858f, 0.09642857142857143f,
-    0.0f, 0.0f, 0.0f, 0.0f, -0.048214285714285716f, -0.048214285714285716f,
-    -0.03482142857142857f, -0.09642857142857143f, -0.03482142857142857f, -0.13125f, -0.06964285714285715f, -0.13125f,
-    -0.013392857142857142f, 0.0f, 0.0f, 0.0f, -0.013392857142857142f, 0.0f,
-    0.0f, 0.048214285714285716f, 0.0f, 0.03482142857142857f, 0.0f, 0.03482142857142857f,
-    0.0f, 0.0f, -0.013392857142857142f, 0.0f, -0.013392857142857142f, 0.0f,
-    0.0f, 0.024107142857142858f, 0.07232142857142858f, 0.048214285714285716f, 0.07232142857142858f, 0.09642857142857143f,
-    0.0f, 0.0f, 0.048214285714285716f, 0.024107142857142858f, 0.048214285714285716f, 0.048214285714285716f,
-    0.024107142857142858f, 0.0f, 0.024107142857142858f, 0.0f, 0.048214285714285716f, 0.0f,
-    0.024107142857142858f, 0.0f, 0.024107142857142858f, 0.0f, 0.048214285714285716f, 0.0f,
-    0.048214285714285716f, 0.0f, 0.0f, 0.048214285714285716f, 0.048214285714285716f, 0.024107142857142858f,
-    0.07232142857142858f, 0.024107142857142858f, 0.0f, 0.09642857142857143f, 0.07232142857142858f, 0.048214285714285716f,
-    0.12053571428571429f, 0.024107142857142858f, 0.024107142857142858f, 0.14464285714285716f, 0.14464285714285716f, 0.24107142857142858f,
-    -0.024107142857142858f, 0.0f, 0.024107142857142858f, -0.024107142857142858f, 0.0f, -0.048214285714285716f,
-    0.24107142857142858f, 0.24107142857142858f, 0.24107142857142858f, 0.2892857142857143f, 0.48214285714285715f, 0.2892857142857143f,
-    -0.07232142857142858f, -0.19285714285714287f, -0.07232142857142858f, -0.19285714285714287f, -0.14464285714285716f, -0.19285714285714287f,
-    0.024107142857142858f, 0.024107142857142858f, 0.12053571428571429f, 0.24107142857142858f, 0.14464285714285716f, 0.14464285714285716f,
-    0.024107142857142858f, 0.0f, -0.024107142857142858f, -0.048214285714285716f, 0.0f, -0.024107142857142858f,
-    0.048214285714285716f, 0.0f, 0.048214285714285716f, 0.048214285714285716f, 0.09642857142857143f, 0.048214285714285716f,
-    -0.048214285714285716f, -0.048214285714285716f, -0.2892857142857143f, -0.19285714285714287f, -0.3375f, -0.3375f,
-    -0.14464285714285716f, 0.0f, -0.14464285714285716f, -0.048214285714285716f, -0.2892857142857143f, -0.048214285714285716f,
-    -0.2892857142857143f, -0.048214285714285716f, -0.048214285714285716f, -0.3375f, -0.3375f, -0.19285714285714287f,
-    0.013392857142857142f, 0.048214285714285716f, 0.013392857142857142f, 0.06160714285714286f, 0.026785714285714284f, 0.06160714285714286f,
-    -0.013392857142857142f, 0.0f, 0.0f, 0.0f, -0.013392857142857142f, 0.0f,
-    0.0f, -0.09642857142857143f, 0.0f, -0.06160714285714286f, 0.0f, -0.06160714285714286f,
-    0.0f, 0.0f, -0.013392857142857142f, 0.0f, -0.013392857142857142f, 0.0f,
-    0.0f, 0.024107142857142858f, -0.19285714285714287f, -0.09642857142857143f, -0.19285714285714287f, -0.19285714285714287f,
-    0.0f, 0.0f, 0.07232142857142858f, 0.024107142857142858f, 0.07232142857142858f, 0.048214285714285716f,
-    0.024107142857142858f, 0.0f, 0.024107142857142858f, 0.0f, 0.048214285714285716f, 0.0f,
-    0.024107142857142858f, 0.0f, 0.024107142857142858f, 0.0f, 0.048214285714285716f, 0.0f,
-    0.07232142857142858f, 0.0f, 0.0f, 0.048214285714285716f, 0.07232142857142858f, 0.024107142857142858f,
-    -0.19285714285714287f, 0.024107142857142858f, 0.0f, -0.19285714285714287f, -0.19285714285714287f, -0.09642857142857143f,
-    -0.024107142857142858f, 0.024107142857142858f, 0.0f, 0.0f, -0.024107142857142858f, -0.048214285714285716f,
-    -0.024107142857142858f, 0.0f, 0.0f, -0.024107142857142858f, -0.024107142857142858f, -0.048214285714285716f,
-    -0.07232142857142858f, -0.19285714285714287f, -0.07232142857142858f, -0.19285714285714287f, -0.14464285714285716f, -0.19285714285714287f,
-    0.19285714285714287f, 0.24107142857142858f, 0.19285714285714287f, 0.19285714285714287f, 0.38571428571428573f, 0.19285714285714287f,
-    0.0f, 0.024107142857142858f, -0.024107142857142858f, -0.048214285714285716f, -0.024107142857142858f, 0.0f,
-    0.0f, 0.0f, -0.024107142857142858f, -0.048214285714285716f, -0.024107142857142858f, -0.024107142857142858f,
-    -0.09642857142857143f, 0.0f, -0.09642857142857143f, 0.048214285714285716f, -0.19285714285714287f, 0.048214285714285716f,
-    0.09642857142857143f, -0.048214285714285716f, 0.0f, 0.09642857142857143f, 0.09642857142857143f, 0.24107142857142858f,
-    0.0f, 0.0f, 0.0f, -0.048214285714285716f, 0.0f, -0.048214285714285716f,
-    0.0f, -0.048214285714285716f, 0.09642857142857143f, 0.24107142857142858f, 0.09642857142857143f, 0.09642857142857143f,
-    -0.09642857142857143f, -0.03482142857142857f, -0.03482142857142857f, -0.13125f, -0.13125f, -0.06964285714285715f,
-    0.048214285714285716f, 0.0f, 0.0f, 0.03482142857142857f, 0.03482142857142857f, 0.0f,
-    0.0f, -0.013392857142857142f, 0.0f, 0.0f, 0.0f, -0.013392857142857142f,
-    0.0f, 0.0f, -0.013392857142857142f, 0.0f, 0.0f, -0.013392857142857142f,
-    0.0f, 0.024107142857142858f, 0.024107142857142858f, 0.0f, 0.0f, 0.048214285714285716f,
-    0.0f, 0.024107142857142858f, 0.024107142857142858f, 0.0f, 0.0f, 0.048214285714285716f,
-    0.024107142857142858f, 0.0f, 0.07232142857142858f, 0.048214285714285716f, 0.09642857142857143f, 0.07232142857142858f,
-    0.0f, 0.0f, 0.048214285714285716f, 0.024107142857142858f, 0.048214285714285716f, 0.048214285714285716f,
-    0.024107142857142858f, 0.07232142857142858f, 0.0f, 0.09642857142857143f, 0.048214285714285716f, 0.07232142857142858f,
-    0.0f, 0.048214285714285716f, 0.0f, 0.048214285714285716f, 0.024107142857142858f, 0.048214285714285716f,
-    0.024107142857142858f, 0.12053571428571429f, 0.024107142857142858f, 0.14464285714285716f, 0.24107142857142858f, 0.14464285714285716f,
-    0.0f, -0.024107142857142858f, 0.024107142857142858f, -0.024107142857142858f, -0.048214285714285716f, 0.0f,
-    0.024107142857142858f, 0.024107142857142858f, 0.12053571428571429f, 0.24107142857142858f, 0.14464285714285716f, 0.14464285714285716f,
-    0.0f, 0.024107142857142858f, -0.024107142857142858f, -0.048214285714285716f, -0.024107142857142858f, 0.0f,
-    0.24107142857142858f, 0.24107142857142858f, 0.24107142857142858f, 0.2892857142857143f, 0.2892857142857143f, 0.48214285714285715f,
-    -0.19285714285714287f, -0.07232142857142858f, -0.07232142857142858f, -0.19285714285714287f, -0.19285714285714287f, -0.14464285714285716f,
-    0.0f, 0.048214285714285716f, 0.048214285714285716f, 0.048214285714285716f, 0.048214285714285716f, 0.09642857142857143f,
-    0.0f, -0.14464285714285716f, -0.14464285714285716f, -0.048214285714285716f, -0.048214285714285716f, -0.2892857142857143f,
-    -0.048214285714285716f, -0.048214285714285716f, -0.2892857142857143f, -0.19285714285714287f, -0.3375f, -0.3375f,
-    -0.048214285714285716f, -0.2892857142857143f, -0.048214285714285716f, -0.3375f, -0.19285714285714287f, -0.3375f,
-    0.048214285714285716f, 0.013392857142857142f, 0.013392857142857142f, 0.06160714285714286f, 0.06160714285714286f, 0.026785714285714284f,
-    -0.09642857142857143f, 0.0f, 0.0f, -0.06160714285714286f, -0.06160714285714286f, 0.0f,
-    0.0f, -0.013392857142857142f, 0.0f, 0.0f, 0.0f, -0.013392857142857142f,
-    0.0f, 0.0f, -0.013392857142857142f, 0.0f, 0.0f, -0.013392857142857142f,
-    0.0f, 0.024107142857142858f, 0.024107142857142858f, 0.0f, 0.0f, 0.048214285714285716f,
-    0.0f, 0.024107142857142858f, 0.024107142857142858f, 0.0f, 0.0f, 0.048214285714285716f,
-    0.024107142857142858f, 0.0f, -0.19285714285714287f, -0.09642857142857143f, -0.19285714285714287f, -0.19285714285714287f,
-    0.0f, 0.0f, 0.07232142857142858f, 0.024107142857142858f, 0.048214285714285716f, 0.07232142857142858f,
-    0.024107142857142858f, -0.19285714285714287f, 0.0f, -0.19285714285714287f, -0.09642857142857143f, -0.19285714285714287f,
-    0.0f, 0.07232142857142858f, 0.0f, 0.048214285714285716f, 0.024107142857142858f, 0.07232142857142858f,
-    0.024107142857142858f, -0.024107142857142858f, 0.0f, 0.0f, -0.048214285714285716f, -0.024107142857142858f,
-    0.0f, -0.024107142857142858f, 0.0f, -0.024107142857142858f, -0.048214285714285716f, -0.024107142857142858f,
-    0.024107142857142858f, 0.0f, -0.024107142857142858f, -0.048214285714285716f, 0.0f, -0.024107142857142858f,
-    0.0f, 0.0f, -0.024107142857142858f, -0.048214285714285716f, -0.024107142857142858f, -0.024107142857142858f,
-    -0.19285714285714287f, -0.07232142857142858f, -0.07232142857142858f, -0.19285714285714287f, -0.19285714285714287f, -0.14464285714285716f,
-    0.24107142857142858f, 0.19285714285714287f, 0.19285714285714287f, 0.19285714285714287f, 0.19285714285714287f, 0.38571428571428573f,
-    0.0f, -0.09642857142857143f, -0.09642857142857143f, 0.048214285714285716f, 0.048214285714285716f, -0.19285714285714287f,
-    0.0f, 0.0f, 0.0f, -0.048214285714285716f, -0.048214285714285716f, 0.0f,
-    -0.048214285714285716f, 0.09642857142857143f, 0.0f, 0.09642857142857143f, 0.24107142857142858f, 0.09642857142857143f,
-    -0.048214285714285716f, 0.0f, 0.09642857142857143f, 0.24107142857142858f, 0.09642857142857143f, 0.09642857142857143f,
-    -0.03214285714285714f, -0.03214285714285714f, -0.03214285714285714f, -0.06428571428571428f, -0.06428571428571428f, -0.06428571428571428f,
-    0.03214285714285714f, 0.0f, 0.0f, -0.01607142857142857f, -0.01607142857142857f, 0.0f,
-    0.0f, 0.03214285714285714f, 0.0f, -0.01607142857142857f, 0.0f, -0.01607142857142857f,
-    0.0f, 0.0f, 0.03214285714285714f, 0.0f, -0.01607142857142857f, -0.01607142857142857f,
-    0.0f, -0.048214285714285716f, 0.09642857142857143f, 0.24107142857142858f, 0.09642857142857143f, 0.09642857142857143f,
-    0.0f, 0.09642857142857143f, -0.048214285714285716f, 0.09642857142857143f, 0.24107142857142858f, 0.09642857142857143f,
-    -0.048214285714285716f, 0.0f, 0.09642857142857143f, 0.24107142857142858f, 0.09642857142857143f, 0.09642857142857143f,
-    0.09642857142857143f, 0.0f, -0.048214285714285716f, 0.09642857142857143f, 0.09642857142857143f, 0.24107142857142858f,
-    -0.048214285714285716f, 0.09642857142857143f, 0.0f, 0.09642857142857143f, 0.24107142857142858f, 0.09642857142857143f,
-    0.09642857142857143f, -0.048214285714285716f, 0.0f, 0.09642857142857143f, 0.09642857142857143f, 0.24107142857142858f,
-    0.048214285714285716f, 0.048214285714285716f, 0.0f, 0.09642857142857143f, 0.048214285714285716f, 0.048214285714285716f,
-    -0.09642857142857143f, -0.09642857142857143f, 0.0f, -0.19285714285714287f, 0.048214285714285716f, 0.048214285714285716f,
-    0.048214285714285716f, 0.0f, 0.048214285714285716f, 0.048214285714285716f, 0.09642857142857143f, 0.048214285714285716f,
-    -0.09642857142857143f, 0.0f, -0.09642857142857143f, 0.048214285714285716f, -0.19285714285714287f, 0.048214285714285716f,
-    0.0f, 0.048214285714285716f, 0.048214285714285716f, 0.048214285714285716f, 0.048214285714285716f, 0.09642857142857143f,
-    0.0f, -0.09642857142857143f, -0.09642857142857143f, 0.048214285714285716f, 0.048214285714285716f, -0.19285714285714287f,
-    0.5785714285714286f, 0.5785714285714286f, 0.5785714285714286f, 0.5785714285714286f, 0.5785714285714286f, 0.5785714285714286f,
-    -0.5785714285714286f, 0.0f, 0.0f, -0.5785714285714286f, -0.5785714285714286f, -0.2892857142857143f,
-    0.0f, -0.5785714285714286f, 0.0f, -0.5785714285714286f, -0.2892857142857143f, -0.5785714285714286f,
-    0.0f, 0.0f, -0.5785714285714286f, -0.2892857142857143f, -0.5785714285714286f, -0.5785714285714286f,
-    0.03214285714285714f, 0.048214285714285716f, 0.048214285714285716f, 0.08035714285714286f, 0.08035714285714286f, 0.09642857142857143f,
-    -0.03214285714285714f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f,
-    0.0f, 0.048214285714285716f, 0.0f, 0.01607142857142857f, 0.0f, 0.0f,
-    0.0f, 0.0f, 0.048214285714285716f, 0.0f, 0.01607142857142857f, 0.0f,
-    0.0f, -0.2892857142857143f, 0.0f, -0.24107142857142858f, -0.09642857142857143f, -0.24107142857142858f,
-    0.0f, 0.0f, -0.2892857142857143f, -0.09642857142857143f, -0.24107142857142858f, -0.24107142857142858f,
-    0.048214285714285716f, 0.0f, 0.0f, 0.0f, 0.048214285714285716f, 0.0f,
-    -0.09642857142857143f, 0.0f, -0.14464285714285716f, 0.0f, -0.24107142857142858f, 0.0f,
-    0.048214285714285716f, 0.0f, 0.0f, 0.048214285714285716f, 0.0f, 0.0f,
-    -0.09642857142857143f, -0.14464285714285716f, 0.0f, -0.24107142857142858f, 0.0f, 0.0f,
-    -0.048214285714285716f, -0.2892857142857143f, -0.048214285714285716f, -0.3375f, -0.19285714285714287f, -0.3375f,
-    0.09642857142857143f, 0.0f, -0.048214285714285716f, 0.09642857142857143f, 0.09642857142857143f, 0.24107142857142858f,
-    -0.048214285714285716f, -0.048214285714285716f, -0.2892857142857143f, -0.19285714285714287f, -0.3375f, -0.3375f,
-    0.09642857142857143f, -0.048214285714285716f, 0.0f, 0.09642857142857143f, 0.09642857142857143f, 0.24107142857142858f,
-    0.0f, -0.14464285714285716f, -0.14464285714285716f, -0.048214285714285716f, -0.048214285714285716f, -0.2892857142857143f,
-    0.0f, 0.0f, 0.0f, -0.048214285714285716f, -0.048214285714285716f, 0.0f,
-    -0.5785714285714286f, 0.0f, 0.0f, -0.5785714285714286f, -0.5785714285714286f, -0.2892857142857143f,
-    0.5785714285714286f, 0.5785714285714286f, 0.5785714285714286f, 0.5785714285714286f, 0.5785714285714286f, 0.5785714285714286f,
-    0.0f, 0.0f, 0.2892857142857143f, 0.5785714285714286f, 0.2892857142857143f, 0.2892857142857143f,
-    0.0f, 0.2892857142857143f, 0.0f, 0.2892857142857143f, 0.5785714285714286f, 0.2892857142857143f,
-    0.048214285714285716f, 0.03214285714285714f, 0.048214285714285716f, 0.08035714285714286f, 0.09642857142857143f, 0.08035714285714286f,
-    0.048214285714285716f, 0.0f, 0.0f, 0.01607142857142857f, 0.0f, 0.0f,
-    0.0f, -0.03214285714285714f, 0.0f, 0.0f, 0.0f, 0.0f,
-    0.0f, 0.0f, 0.048214285714285716f, 0.0f, 0.0f, 0.01607142857142857f,
-    0.0f, 0.048214285714285716f, 0.0f, 0.0f, 0.0f, 0.048214285714285716f,
-    0.0f, -0.09642857142857143f, -0.14464285714285716f, 0.0f, 0.0f, -0.24107142857142858f,
-    -0.2892857142857143f, 0.0f, 0.0f, -0.24107142857142858f, -0.24107142857142858f, -0.09642857142857143f,
-    0.0f, 0.0f, -0.2892857142857143f, -0.09642857142857143f, -0.24107142857142858f, -0.24107142857142858f,
-    -0.14464285714285716f, -0.09642857142857143f, 0.0f, -0.24107142857142858f, 0.0f, 0.0f,
-    0.0f, 0.048214285714285716f, 0.0f, 0.048214285714285716f, 0.0f, 0.0f,
-    -0.2892857142857143f, -0.048214285714285716f, -0.048214285714285716f, -0.3375f, -0.3375f, -0.19285714285714287f,
-    0.0f, 0.09642857142857143f, -0.048214285714285716f, 0.09642857142857143f, 0.24107142857142858f, 0.09642857142857143f,
-    -0.14464285714285716f, 0.0f, -0.14464285714285716f, -0.048214285714285716f, -0.2892857142857143f, -0.048214285714285716f,
-    0.0f, 0.0f, 0.0f, -0.048214285714285716f, 0.0f, -0.048214285714285716f,
-    -0.048214285714285716f, -0.048214285714285716f, -0.2892857142857143f, -0.19285714285714287f, -0.3375f, -0.3375f,
-    -0.048214285714285716f, 0.09642857142857143f, 0.0f, 0.09642857142857143f, 0.24107142857142858f, 0.09642857142857143f,
-    0.0f, -0.5785714285714286f, 0.0f, -0.5785714285714286f, -0.2892857142857143f, -0.5785714285714286f,
-    0.0f, 0.0f, 0.2892857142857143f, 0.5785714285714286f, 0.2892857142857143f, 0.2892857142857143f,
-    0.5785714285714286f, 0.5785714285714286f, 0.5785714285714286f, 0.5785714285714286f, 0.5785714285714286f, 0.5785714285714286f,
-    0.2892857142857143f, 0.0f, 0.0f, 0.2892857142857143f, 0.2892857142857143f, 0.5785714285714286f,
-    0.048214285714285716f, 0.048214285714285716f, 0.03214285714285714f, 0.09642857142857143f, 0.08035714285714286f, 0.08035714285714286f,
-    0.048214285714285716f, 0.0f, 0.0f, 0.0f, 0.01607142857142857f, 0.0f,
-    0.0f, 0.048214285714285716f, 0.0f, 0.0f, 0.0f, 0.01607142857142857f,
-    0.0f, 0.0f, -0.03214285714285714f, 0.0f, 0.0f, 0.0f,
-    0.0f, -0.14464285714285716f, -0.09642857142857143f, 0.0f, 0.0f, -0.24107142857142858f,
-    0.0f, 0.0f, 0.048214285714285716f, 0.0f, 0.0f, 0.048214285714285716f,
-    -0.14464285714285716f, 0.0f, -0.09642857142857143f, 0.0f, -0.24107142857142858f, 0.0f,
-    0.0f, 0.0f, 0.048214285714285716f, 0.0f, 0.048214285714285716f, 0.0f,
-    -0.2892857142857143f, 0.0f, 0.0f, -0.24107142857142858f, -0.24107142857142858f, -0.09642857142857143f,
-    0.0f, -0.2892857142857143f, 0.0f, -0.24107142857142858f, -0.09642857142857143f, -0.24107142857142858f,
-    -0.14464285714285716f, -0.14464285714285716f, 0.0f, -0.2892857142857143f, -0.048214285714285716f, -0.048214285714285716f,
-    0.0f, 0.0f, 0.0f, 0.0f, -0.048214285714285716f, -0.048214285714285716f,
-    -0.2892857142857143f, -0.048214285714285716f, -0.048214285714285716f, -0.3375f, -0.3375f, -0.19285714285714287f,
-    0.0f, -0.048214285714285716f, 0.09642857142857143f, 0.24107142857142858f, 0.09642857142857143f, 0.09642857142857143f,
-    -0.048214285714285716f, -0.2892857142857143f, -0.048214285714285716f, -0.3375f, -0.19285714285714287f, -0.3375f,
-    -0.048214285714285716f, 0.0f, 0.09642857142857143f, 0.24107142857142858f, 0.09642857142857143f, 0.09642857142857143f,
-    0.0f, 0.0f, -0.5785714285714286f, -0.2892857142857143f, -0.5785714285714286f, -0.5785714285714286f,
-    0.0f, 0.2892857142857143f, 0.0f, 0.2892857142857143f, 0.5785714285714286f, 0.2892857142857143f,
-    0.2892857142857143f, 0.0f, 0.0f, 0.2892857142857143f, 0.2892857142857143f, 0.5785714285714286f,
-    0.5785714285714286f, 0.5785714285714286f, 0.5785714285714286f, 0.5785714285714286f, 0.5785714285714286f, 0.5785714285714286f,
-};
-
 // int_ref d_p phi_i d_q phi_j of the P2 basis, index (i*10 + j)*9 + p*3 + q.
 __device__ const double kP2GradGrad[900] = {
     0x1.999999999999ap-4, 0x1.999999999999ap-4, 0x1.999999999999ap-4, 0x1.999999999999ap-4, 0x1.999999999999ap-4, 0x1.999999999999ap-4,

@@ -576,96 +576,6 @@ __global__ void __launch_bounds__(kBlockP3) k_mat_p3_atomic(const MatArgs a) {
 }
 
 // ---------------------------------------------------------------------------
-// P3 stiffness with the reductions coalesced per warp (the P3 default).
-// Entry (i, j) = sum_s g_s S_ij^s, g_s = k Ghat_s, S the 20x20x6 reference
-// table (kP3Stiff, symmetric in i and j, read through L1).  One thread per
-// cell computes g into shared memory; the warp then walks its 32 cells with
-// one instruction per element row i, lane j on column j: the 20 reductions
-// of an instruction fall in one CSR row, both triangles, no transpose pass.
-// S_ij = S_ji with one term order, so the element matrix is exactly
-// symmetric; with FP32 element entries each diagonal entry is minus the FP64
-// sum of its row's FP32 off-diagonal entries (a lane's column sum), as in
-// the thread-per-cell kernel.
-// ---------------------------------------------------------------------------
-constexpr int kP3CoalThreads = 64;
-
-template <typename T>
-__global__ void __launch_bounds__(kP3CoalThreads) k_mat_p3_coal(const MatArgs a) {
-  constexpr int NT = kP3CoalThreads;
-  constexpr bool kRowSums = sizeof(T) == 4;
-  const T* __restrict__ S3 = kRowSums ? reinterpret_cast<const T*>(kP3StiffF) : reinterpret_cast<const T*>(kP3Stiff);
-  __shared__ __align__(16) uint8_t spos[NT * 400];
-  __shared__ T sg[NT * 6];
-  __shared__ int32_t srp[NT * 20];  // row start of local row i, -1 for a masked row
-  __shared__ uint32_t smc[NT];      // masked columns
-  const int tid = threadIdx.x, lane = tid & 31, w0 = tid & ~31;
-  const int64_t c0 = blockIdx.x * (int64_t)NT;
-  const int64_t left = a.num_cells - c0;
-  const int ncell = left < NT ? (int)left : NT;
-  const int wcells = ncell - w0 < 0 ? 0 : (ncell - w0 < 32 ? ncell - w0 : 32);
-  {
-    // each warp stages its own cells' byte maps ((c0 + w0) * 400 is a multiple of 16)
-    const uint4* src = reinterpret_cast<const uint4*>(a.pos + (c0 + w0) * 400);
-    uint4* dst = reinterpret_cast<uint4*>(spos + w0 * 400);
-    const int nvec = wcells * 25;
-    for (int t = lane; t < nvec; t += 32) dst[t] = __ldg(src + t);
-  }
-  if (tid < ncell) {
-    const int64_t c = c0 + tid;
-    CellGeo g;
-    cell_geometry(a.x, load_geom(a.geom, c), g);
-    double Gh[6];
-    ghat(g, Gh);
-    const double k = coef_cell(a.c0, c);
-#pragma unroll
-    for (int s2 = 0; s2 < 6; ++s2) sg[tid * 6 + s2] = (T)(k * Gh[s2]);
-    const int32_t* d0 = a.dofs0 + c * 20;
-    const int32_t* d1 = a.dofs1 + c * 20;
-    uint32_t mc = 0;
-#pragma unroll
-    for (int i = 0; i < 20; ++i) {
-      // masked rows / columns: BC dofs and dofs outside a restriction (-1)
-      const int r = __ldg(d0 + i), cc = __ldg(d1 + i);
-      const bool mrow = r < 0 || (a.bc0 && __ldg(a.bc0 + r));
-      srp[tid * 20 + i] = mrow ? -1 : __ldg(a.row_ptr + r);
-      mc |= (cc < 0 || (a.bc1 && __ldg(a.bc1 + cc)) ? 1u : 0u) << i;
-    }
-    smc[tid] = mc;
-  }
-  __syncwarp();  // the warp's staged maps and its cells' g, row starts, masks
-  const bool lane_on = lane < 20;
-  const int j = lane_on ? lane : 0;
-  double* __restrict__ vals = a.values;
-  for (int q = w0; q < w0 + wcells; ++q) {
-    T gq[6];
-#pragma unroll
-    for (int s2 = 0; s2 < 6; ++s2) gq[s2] = sg[q * 6 + s2];
-    const bool cmask = !lane_on || ((smc[q] >> j) & 1u);
-    const int32_t* rq = srp + q * 20;
-    const uint8_t* pq8 = spos + q * 400;
-    double cs = 0.0;
-#pragma unroll 2
-    for (int i = 0; i < 20; ++i) {
-      const T* Sp = S3 + (i * 20 + j) * 6;
-      T v0 = __ldg(Sp) * gq[0], v1 = __ldg(Sp + 1) * gq[1];
-      v0 = fma(__ldg(Sp + 2), gq[2], v0);
-      v1 = fma(__ldg(Sp + 3), gq[3], v1);
-      v0 = fma(__ldg(Sp + 4), gq[4], v0);
-      v1 = fma(__ldg(Sp + 5), gq[5], v1);
-      const T v = v0 + v1;
-      if (kRowSums && i == j) continue;  // the diagonal comes from the column sum
-      if (kRowSums) cs += (double)v;
-      const int rs = rq[i];
-      if (rs >= 0 && !cmask) atomicAdd(vals + rs + pq8[i * 20 + j], (double)v);
-    }
-    if constexpr (kRowSums) {
-      const int rs = rq[j];
-      if (lane_on && rs >= 0 && !cmask) atomicAdd(vals + rs + pq8[j * 20 + j], -cs);
-    }
-  }
-}
-
-// ---------------------------------------------------------------------------
 // Vector-P2 elasticity (bs = 3), one thread per cell, FP64 atomics
 // A[(i,a),(j,b)] = sum_pq W_ab[p][q] R0[p][q][i][j],
 // W_ab[p][q] = |det| (mu (delta_ab (KK^T)_pq + K_pb K_qa) + lam K_pa K_qb)
@@ -1871,12 +1781,6 @@ void launch_matrix_atomic(const MatLaunch& L, cudaStream_t s) {
       else k_mat_vmass<FE_COEFF_DG0><<<grid, kBlock, 0, s>>>(a);
       break;
     case FE_FORM_P3_STIFFNESS: {
-      if (L.coalesced && !a.upper) {
-        auto k = f32 ? k_mat_p3_coal<float> : k_mat_p3_coal<double>;
-        FE_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 80));
-        k<<<grid_for(L.num_cells, kP3CoalThreads), kP3CoalThreads, 0, s>>>(a);
-        break;
-      }
       // one thread per cell: splitting a cell's 210 entries over 2, 4 or 8
       // warps measured the same or slower on B200 (P3 n=48: 1.75-2.12 ms vs
       // 1.79 ms), the reductions themselves bound the kernel

@@ -362,17 +362,6 @@ def gen() -> str:
         w("}\n\n")
     # the same reference integrals as a table, for kernels that evaluate block
     # entries lane by lane: kP2GradGrad[(i*10 + j)*9 + p*3 + q] = int_ref d_p phi_i d_q phi_j
-    w("// P3 stiffness reference tensor per geometry pair s (as p3_stiffness_const sums\n")
-    w("// them): kP3Stiff[(i*20 + j)*6 + s], symmetric in i and j.\n")
-    vals3 = [lit(sym_pair(r3_plain, s_, i, j)) for i in range(20) for j in range(20) for s_ in range(6)]
-    for ty, nm in (("double", "kP3Stiff"), ("float", "kP3StiffF")):
-        w(f"__device__ const {ty} {nm}[2400] = {{\n")
-        for k in range(0, 2400, 6):
-            row = vals3[k:k + 6]
-            if ty == "float":
-                row = [repr(float.fromhex(v)) + "f" for v in row]
-            w("    " + ", ".join(row) + ",\n")
-        w("};\n\n")
     w("// int_ref d_p phi_i d_q phi_j of the P2 basis, index (i*10 + j)*9 + p*3 + q.\n")
     w("__device__ const double kP2GradGrad[900] = {\n")
     vals = [lit(r_plain(p_, q_, i, j)) for i in range(10) for j in range(10) for p_ in range(3) for q_ in range(3)]

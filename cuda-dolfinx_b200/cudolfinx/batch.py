@@ -27,7 +27,6 @@ CANDIDATES = {
     "P1_STIFFNESS": ("atomic", "block", "tile"),
     "P2_STIFFNESS": ("atomic", "block", "grouped", "coalesced"),
     "VP2_ELASTICITY": ("coalesced", "atomic", "atomic-full"),
-    "P3_STIFFNESS": ("coalesced", "atomic"),
 }
 # launch shapes of the atomic scatter timed per form kind: (cells per CTA,
 # byte maps staged in shared memory)

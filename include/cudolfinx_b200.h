@@ -125,7 +125,7 @@ enum fe_precision {
                                      entries summed per distinct CSR slot in shared memory, then one
                                      reduction per slot (falls back to the atomic scatter when the
                                      mesh's groups share no structure)                                */
-#define FE_ASM_COALESCED 512u     /* P2 / P3 stiffness, vector-P2 elasticity (the default): the
+#define FE_ASM_COALESCED 512u     /* P2 stiffness, vector-P2 elasticity (the default for both): the
                                      warp's reductions issued row by row from shared memory
                                      (consecutive lanes on one cell's CSR row, so an instruction's
                                      reductions share L2 sectors); FE_ASM_ATOMIC keeps one thread's
