@@ -88,18 +88,24 @@ L2_BYTES = 126 * 1024 * 1024
 VECTOR_KERNELS = 3
 
 
-def matrix_kernels(kind: str, variant: str, big: bool = False) -> int:
+def matrix_kernels(kind: str, variant: str, big: bool = False, nnz: int = 1 << 30) -> int:
     """Kernel launches of one fe_assemble_matrix call (with BCs): 2 for the
-    single-pass variants (row gather, tile, ordered tile; + set_diagonal), 3
-    for the atomic scatter (zero + scatter + set_diagonal) and the sorted-slot
-    reduction (element tensors + gather + set_diagonal)."""
+    single-pass variants (row gather, tile, ordered tile: kernel +
+    set_diagonal) and for the scatters after the zero pass that also writes
+    the BC diagonal (coalesced, block, atomic with both reductions: zero +
+    kernel), 3 with the upper-triangle scatter (zero + scatter + transpose
+    pass) and for the sorted-slot reduction (element tensors + gather +
+    set_diagonal)."""
     if variant in ("tile", "row-gather") or (variant == "deterministic" and kind in ("p1", "p2")):
         return 2
+    if variant in ("sorted-slot", "deterministic"):
+        return 3
     atomic = variant == "atomic" or (variant == "auto" and not (kind == "p1" and big)
                                      and kind not in ("p2", "vp2"))
-    if kind in ("p1", "vp2", "p3") and atomic:
-        return 4  # zero + upper-triangle scatter + lower-triangle mirror + set_diagonal
-    return 3  # coalesced, atomic-full, block (zero + kernel + set_diagonal), sorted-slot
+    small_p1 = kind in ("p1", "p1k") and nnz < (1 << 22)
+    if kind in ("p1", "vp2", "p3") and atomic and not small_p1:
+        return 3  # zero + upper-triangle scatter + lower-triangle transpose
+    return 2  # zero (with the BC diagonal) + kernel
 
 
 _PINNED: list = []
@@ -611,7 +617,7 @@ def run_gpu(args, rank, world, local_rank):
                      if "hbm_gbs" in peaks else "fallback 6650 GB/s"},
         "matrix_nnz_per_s": nnz / (mat_ms / 1e3),
         "rhs_ms": rhs_ms,
-        "gpu_launches": (matrix_kernels(W["kind"], args.variant, len(I["cells"]) >= (1 << 20))
+        "gpu_launches": (matrix_kernels(W["kind"], args.variant, len(I["cells"]) >= (1 << 20), nnz)
                          + VECTOR_KERNELS + (args.rhs == "calls"))
         * args.steps,
         "clocks": clk,
@@ -1515,7 +1521,8 @@ def run_gpu_multimesh(args, rank, world, local_rank):
         pass
     peak = peaks.get("hbm_gbs", 6650.0)
     achieved = alg / (ms / 1e3) / 1e9
-    launches = sum(matrix_kernels(I["kind"], it["variant"], len(I["cells"]) >= (1 << 20)) for I, it in zip(Is, G.items))
+    launches = sum(matrix_kernels(I["kind"], it["variant"], len(I["cells"]) >= (1 << 20), item[1].sparsity.nnz)
+                   for I, item, it in zip(Is, items, G.items))
     chosen = {}
     for it in G.items:
         chosen[it["variant"]] = chosen.get(it["variant"], 0) + 1

@@ -8,6 +8,7 @@
 //  * coefficients are uploaded once and gathered inside the element kernels
 //    (no pack_coefficients pass, no re-upload on every assemble call);
 //  * the CSR column search is done once per (form, pattern) into a byte map.
+#include <algorithm>
 #include <atomic>
 #include <cstring>
 #include <string>
@@ -845,6 +846,11 @@ int fe_bc_create(fe_context ctx, int64_t num_dofs, const uint8_t* markers, const
     for (int64_t d = 0; d < num_dofs; ++d) marked += markers[d] != 0;
     auto bc = std::make_unique<fe_bc_s>();
     bc->markers_are_dofs = distinct == n_bc && marked == n_bc;
+    {
+      std::vector<int32_t> owned(dofs, dofs + n_owned);
+      std::sort(owned.begin(), owned.end());
+      upload(bc->rows_sorted, owned.data(), owned.size());
+    }
     bc->ctx = ctx;
     bc->num_dofs = num_dofs;
     bc->n_bc = n_bc;
@@ -971,8 +977,7 @@ int fe_assemble_matrix(fe_form a, double* values, fe_bc bc0, fe_bc bc1, double d
     const bool want_block = (flags & FE_ASM_BLOCK) || auto_block;
     if (flags & FE_ASM_BLOCK) FE_REQUIRE(block_supported(*a), "the block variant supports P1/P2 stiffness only");
     if (want_block && block_supported(*a)) {
-      assemble_matrix_block(*a, values, bc0, bc1, zero, st);
-      if (bc0) launch_set_diagonal(*a->sp, *bc0, diagonal, values, st);
+      assemble_matrix_block(*a, values, bc0, bc1, zero, diagonal, st);
       return;
     }
     // every built-in bilinear form is symmetric: on a symmetric pattern with
@@ -989,12 +994,20 @@ int fe_assemble_matrix(fe_form a, double* values, fe_bc bc0, fe_bc bc1, double d
     const bool coalesced = (flags & FE_ASM_COALESCED) ||
                            (!(flags & FE_ASM_ATOMIC) && !view &&
                             (a->kind == FE_FORM_P2_STIFFNESS || a->kind == FE_FORM_VP2_ELASTICITY));
-    const bool upper = !coalesced && zero && !view && !(flags & FE_ASM_FULL_SCATTER) &&
+    // A pattern whose values fit in L2 many times over (P1 below 2^22 nonzeros,
+    // 32 MB) keeps both reductions: there the call is launch-bound and the
+    // transpose pass would be one more launch on its path.
+    const bool small = a->kind == FE_FORM_P1_STIFFNESS && a->sp->nnz < (int64_t(1) << 22);
+    const bool upper = !coalesced && !small && zero && !view && !(flags & FE_ASM_FULL_SCATTER) &&
                        (a->kind == FE_FORM_VP2_ELASTICITY || a->kind == FE_FORM_P3_STIFFNESS ||
                         a->kind == FE_FORM_P1_STIFFNESS || a->kind == FE_FORM_P1_MASS ||
                         a->kind == FE_FORM_VP2_MASS) && a->V0 == a->V1 &&
                        bc0 == bc1 && ensure_mirror(*a->sp, st, a->V0->bs);
-    if (zero) launch_zero(values, a->sp->nnz, st);
+    // the element scatters skip BC rows: their diagonal is written with the
+    // zero pass (plain patterns; a block view's row table is not the values')
+    const bool zero_diag = zero && !view;
+    if (zero_diag) launch_zero_diagonal(*a->sp, bc0, diagonal, values, st);
+    else if (zero) launch_zero(values, a->sp->nnz, st);
     MatLaunch L{};
     L.kind = a->kind;
     L.precision = a->precision;
@@ -1019,7 +1032,7 @@ int fe_assemble_matrix(fe_form a, double* values, fe_bc bc0, fe_bc bc1, double d
     L.coalesced = coalesced ? 1 : 0;
     launch_matrix_atomic(L, st);
     if (upper) launch_mirror_lower(*a->sp, values, st);
-    if (bc0) launch_set_diagonal(*a->sp, *bc0, diagonal, values, st);
+    if (bc0 && !zero_diag) launch_set_diagonal(*a->sp, *bc0, diagonal, values, st);
   });
 }
 

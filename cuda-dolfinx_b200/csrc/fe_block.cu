@@ -835,20 +835,23 @@ void reset_block_plan(fe_form_s& f) { f.blocks.reset(); }
 bool block_supported(const fe_form_s& f) { return tile_supported(f); }
 
 void assemble_matrix_block(fe_form_s& f, double* values, const fe_bc_s* bc0, const fe_bc_s* bc1, bool zero,
-                           cudaStream_t s) {
+                           double diagonal, cudaStream_t s) {
   const Coefficient& kc = f.coeff[0];
   const fe_dofmap_s* want_map = (kc.kind == FE_COEFF_P1) ? kc.map : nullptr;
   if (f.blocks && f.blocks->coef_map_owner != want_map) f.blocks.reset();  // coefficient space changed
   if (!f.blocks)
     f.blocks = (f.kind == FE_FORM_P1_STIFFNESS) ? build_block_plan<FE_FORM_P1_STIFFNESS>(f)
                                                 : build_block_plan<FE_FORM_P2_STIFFNESS>(f);
-  if (zero) launch_zero(values, f.sp->nnz, s);
+  // BC rows take no window flush and no direct reduction: their diagonal is
+  // written with the zero pass
+  if (zero) launch_zero_diagonal(*f.sp, bc0, diagonal, values, s);
   if (f.kind == FE_FORM_P1_STIFFNESS)
     launch_block<FE_FORM_P1_STIFFNESS, double>(f, *f.blocks, values, bc0, bc1, s);
   else if (f.precision == FE_PREC_FP32)
     launch_block<FE_FORM_P2_STIFFNESS, float>(f, *f.blocks, values, bc0, bc1, s);
   else
     launch_block<FE_FORM_P2_STIFFNESS, double>(f, *f.blocks, values, bc0, bc1, s);
+  if (!zero && bc0) launch_set_diagonal(*f.sp, *bc0, diagonal, values, s);
 }
 
 }  // namespace fe

@@ -139,6 +139,7 @@ struct fe_bc_s {
   fe_context ctx = nullptr;
   int64_t num_dofs = 0, n_bc = 0, n_owned = 0;
   bool markers_are_dofs = false;  // the marked dofs are exactly the listed ones, each listed once
+  fe::DevBuf<int32_t> rows_sorted;  // the n_owned owned dofs in ascending order (k_zero_diag)
   fe::DevBuf<uint8_t> markers;   // [num_dofs]
   fe::DevBuf<int32_t> dofs;      // [n_bc], owned first
   fe::DevBuf<double> g;          // [num_dofs]
@@ -359,6 +360,10 @@ struct MatLaunch {
   int coalesced = 0;  // P2: reductions issued per warp, row by row (k_mat_p2_coal)
 };
 void launch_zero(double* v, int64_t n, cudaStream_t s);
+// values = 0, then values[diag slot of each owned bc row] = diagonal, in one
+// launch (for scatters that skip BC rows); bc may be null (zero only)
+void launch_zero_diagonal(const fe_sparsity_s& sp, const fe_bc_s* bc, double diagonal, double* values,
+                          cudaStream_t s);
 // symmetric-pattern transpose map (built once per pattern); false if the
 // pattern is not symmetric or lacks a diagonal entry
 bool ensure_mirror(fe_sparsity_s& sp, cudaStream_t s, int bs = 1);
@@ -449,7 +454,7 @@ bool assemble_matrix_grouped(fe_form_s& f, double* values, const fe_bc_s* bc0, c
 bool block_supported(const fe_form_s& f);
 void reset_block_plan(fe_form_s& f);
 void assemble_matrix_block(fe_form_s& f, double* values, const fe_bc_s* bc0, const fe_bc_s* bc1, bool zero,
-                           cudaStream_t s);
+                           double diagonal, cudaStream_t s);
 
 // exterior-facet forms (fe_facet.cu)
 bool is_facet_kind(int kind);

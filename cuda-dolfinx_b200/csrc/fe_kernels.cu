@@ -829,6 +829,44 @@ __global__ void k_zero(double* __restrict__ v, int64_t n) {
   }
 }
 
+// The zero pass and set_diagonal in one launch, for kernels that never
+// reduce into a BC row (the element scatters skip them): block b owns the
+// slots [b*chunk, (b+1)*chunk), zeroes them, then stores `value` on the
+// diagonal slots of the owned BC rows that fall in its range (rows sorted
+// ascending, so a binary search on row_ptr finds the first candidate); the
+// same block writes both, so no ordering across blocks is needed.
+__global__ void __launch_bounds__(256) k_zero_diag(double* __restrict__ v, int64_t n, int64_t chunk,
+                                                   const int32_t* __restrict__ row_ptr,
+                                                   const int32_t* __restrict__ diag,
+                                                   const int32_t* __restrict__ rows, int64_t nrows_bc,
+                                                   int64_t num_rows, double value) {
+  const int64_t lo = blockIdx.x * chunk;
+  const int64_t hi = lo + chunk < n ? lo + chunk : n;
+  if (lo >= hi) return;
+  // chunk is even and v is 16-byte aligned: double2 stores over [lo, hi)
+  double2* v2 = reinterpret_cast<double2*>(v + lo);
+  const int64_t n2 = (hi - lo) / 2;
+  for (int64_t t = threadIdx.x; t < n2; t += blockDim.x) v2[t] = make_double2(0.0, 0.0);
+  if (threadIdx.x == 0 && ((hi - lo) & 1)) v[hi - 1] = 0.0;
+  __syncthreads();
+  if (nrows_bc == 0) return;
+  // first BC row whose slots end after lo
+  int64_t a = 0, b = nrows_bc;
+  while (a < b) {
+    const int64_t m = (a + b) / 2;
+    const int32_t r = __ldg(rows + m);
+    if (r < 0 || r >= num_rows || __ldg(row_ptr + r + 1) <= lo) a = m + 1;
+    else b = m;
+  }
+  for (int64_t k = a + threadIdx.x; k < nrows_bc; k += blockDim.x) {
+    const int32_t r = __ldg(rows + k);
+    if (r < 0 || r >= num_rows) continue;
+    if (__ldg(row_ptr + r) >= hi) break;  // rows ascend: the later ones start later
+    const int32_t d = __ldg(diag + r);
+    if (d >= lo && d < hi) v[d] = value;
+  }
+}
+
 // set_diagonal (CUDAAssembler.cpp:131-164) with the diagonal slot precomputed
 __global__ void k_set_diagonal(const int32_t* __restrict__ dofs, int64_t n_owned,
                                const int32_t* __restrict__ diag, int64_t num_rows, double value,
@@ -1652,6 +1690,27 @@ void launch_zero(double* v, int64_t n, cudaStream_t s) {
   const int64_t want = (n / 2 + 255) / 256;
   const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)sms * 8));
   k_zero<<<grid, 256, 0, s>>>(v, n);
+  FE_CUDA(cudaGetLastError());
+}
+
+void launch_zero_diagonal(const fe_sparsity_s& sp, const fe_bc_s* bc, double diagonal, double* values,
+                          cudaStream_t s) {
+  const int64_t n = sp.nnz;
+  if (n <= 0) return;
+  if ((reinterpret_cast<uintptr_t>(values) & 15) != 0 || (bc && !bc->rows_sorted.p && bc->n_owned)) {
+    launch_zero(values, n, s);
+    if (bc) launch_set_diagonal(sp, *bc, diagonal, values, s);
+    return;
+  }
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int64_t blocks = std::max<int64_t>(1, std::min<int64_t>((n / 2 + 255) / 256, (int64_t)sms * 8));
+  int64_t chunk = (n + blocks - 1) / blocks;
+  chunk += chunk & 1;  // even, so every block's range starts on 16 bytes
+  const unsigned grid = (unsigned)((n + chunk - 1) / chunk);
+  k_zero_diag<<<grid, 256, 0, s>>>(values, n, chunk, sp.row_ptr.p, sp.diag.p, bc ? bc->rows_sorted.p : nullptr,
+                                   bc ? bc->n_owned : 0, sp.num_rows, diagonal);
   FE_CUDA(cudaGetLastError());
 }
 
