@@ -102,8 +102,7 @@ def matrix_kernels(kind: str, variant: str, big: bool = False, nnz: int = 1 << 3
         return 3
     atomic = variant == "atomic" or (variant == "auto" and not (kind == "p1" and big)
                                      and kind not in ("p2", "vp2"))
-    small_p1 = kind in ("p1", "p1k") and nnz < (1 << 22)
-    if kind in ("p1", "vp2", "p3") and atomic and not small_p1:
+    if kind in ("p1", "vp2", "p3") and atomic:
         return 3  # zero + upper-triangle scatter + lower-triangle transpose
     return 2  # zero (with the BC diagonal) + kernel
 

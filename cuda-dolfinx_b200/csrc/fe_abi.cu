@@ -994,11 +994,7 @@ int fe_assemble_matrix(fe_form a, double* values, fe_bc bc0, fe_bc bc1, double d
     const bool coalesced = (flags & FE_ASM_COALESCED) ||
                            (!(flags & FE_ASM_ATOMIC) && !view &&
                             (a->kind == FE_FORM_P2_STIFFNESS || a->kind == FE_FORM_VP2_ELASTICITY));
-    // A pattern whose values fit in L2 many times over (P1 below 2^22 nonzeros,
-    // 32 MB) keeps both reductions: there the call is launch-bound and the
-    // transpose pass would be one more launch on its path.
-    const bool small = a->kind == FE_FORM_P1_STIFFNESS && a->sp->nnz < (int64_t(1) << 22);
-    const bool upper = !coalesced && !small && zero && !view && !(flags & FE_ASM_FULL_SCATTER) &&
+    const bool upper = !coalesced && zero && !view && !(flags & FE_ASM_FULL_SCATTER) &&
                        (a->kind == FE_FORM_VP2_ELASTICITY || a->kind == FE_FORM_P3_STIFFNESS ||
                         a->kind == FE_FORM_P1_STIFFNESS || a->kind == FE_FORM_P1_MASS ||
                         a->kind == FE_FORM_VP2_MASS) && a->V0 == a->V1 &&

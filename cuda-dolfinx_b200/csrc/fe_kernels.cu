@@ -848,16 +848,19 @@ __global__ void __launch_bounds__(256) k_zero_diag(double* __restrict__ v, int64
   const int64_t n2 = (hi - lo) / 2;
   for (int64_t t = threadIdx.x; t < n2; t += blockDim.x) v2[t] = make_double2(0.0, 0.0);
   if (threadIdx.x == 0 && ((hi - lo) & 1)) v[hi - 1] = 0.0;
-  __syncthreads();
   if (nrows_bc == 0) return;
-  // first BC row whose slots end after lo
-  int64_t a = 0, b = nrows_bc;
-  while (a < b) {
-    const int64_t m = (a + b) / 2;
-    const int32_t r = __ldg(rows + m);
-    if (r < 0 || r >= num_rows || __ldg(row_ptr + r + 1) <= lo) a = m + 1;
-    else b = m;
-  }
+  // first BC row whose slots end after lo, in two rounds of a 256-way search
+  // (the rows ascend, so "ends at or before lo" holds for a prefix)
+  auto before = [&](int64_t k) {
+    if (k >= nrows_bc) return false;
+    const int32_t r = __ldg(rows + k);
+    return r < 0 || r >= num_rows || __ldg(row_ptr + r + 1) <= lo;
+  };
+  const int64_t step = (nrows_bc + blockDim.x - 1) / blockDim.x;
+  const int c1 = __syncthreads_count(before((int64_t)threadIdx.x * step));  // also orders the zeros
+  const int64_t base = c1 == 0 ? 0 : (int64_t)(c1 - 1) * step + 1;
+  const int c2 = __syncthreads_count(threadIdx.x < step - 1 && c1 > 0 && before(base + threadIdx.x));
+  const int64_t a = c1 == 0 ? 0 : base + c2;
   for (int64_t k = a + threadIdx.x; k < nrows_bc; k += blockDim.x) {
     const int32_t r = __ldg(rows + k);
     if (r < 0 || r >= num_rows) continue;
