@@ -139,7 +139,14 @@ struct fe_bc_s {
   fe_context ctx = nullptr;
   int64_t num_dofs = 0, n_bc = 0, n_owned = 0;
   bool markers_are_dofs = false;  // the marked dofs are exactly the listed ones, each listed once
-  fe::DevBuf<int32_t> rows_sorted;  // the n_owned owned dofs in ascending order (k_zero_diag)
+  fe::DevBuf<int32_t> rows_sorted;  // the n_owned owned dofs in ascending order
+  // per pattern id: the owned rows' diagonal slots (ascending) and, per block
+  // of the zero-with-diagonal pass, its first slot index; built on first use
+  struct DiagSlots {
+    fe::DevBuf<int32_t> slots, starts;
+    int64_t chunk = 0, grid = 0;
+  };
+  std::map<uint64_t, std::unique_ptr<DiagSlots>> diag_slots;
   fe::DevBuf<uint8_t> markers;   // [num_dofs]
   fe::DevBuf<int32_t> dofs;      // [n_bc], owned first
   fe::DevBuf<double> g;          // [num_dofs]

@@ -832,14 +832,12 @@ __global__ void k_zero(double* __restrict__ v, int64_t n) {
 // The zero pass and set_diagonal in one launch, for kernels that never
 // reduce into a BC row (the element scatters skip them): block b owns the
 // slots [b*chunk, (b+1)*chunk), zeroes them, then stores `value` on the
-// diagonal slots of the owned BC rows that fall in its range (rows sorted
-// ascending, so a binary search on row_ptr finds the first candidate); the
-// same block writes both, so no ordering across blocks is needed.
+// diagonal slots of the owned BC rows that fall in its range -- dslot (sorted
+// ascending) from bstart[b] to bstart[b+1], both precomputed per pattern and
+// BC -- so the same block writes both and no ordering across blocks is needed.
 __global__ void __launch_bounds__(256) k_zero_diag(double* __restrict__ v, int64_t n, int64_t chunk,
-                                                   const int32_t* __restrict__ row_ptr,
-                                                   const int32_t* __restrict__ diag,
-                                                   const int32_t* __restrict__ rows, int64_t nrows_bc,
-                                                   int64_t num_rows, double value) {
+                                                   const int32_t* __restrict__ dslot,
+                                                   const int32_t* __restrict__ bstart, double value) {
   const int64_t lo = blockIdx.x * chunk;
   const int64_t hi = lo + chunk < n ? lo + chunk : n;
   if (lo >= hi) return;
@@ -848,26 +846,11 @@ __global__ void __launch_bounds__(256) k_zero_diag(double* __restrict__ v, int64
   const int64_t n2 = (hi - lo) / 2;
   for (int64_t t = threadIdx.x; t < n2; t += blockDim.x) v2[t] = make_double2(0.0, 0.0);
   if (threadIdx.x == 0 && ((hi - lo) & 1)) v[hi - 1] = 0.0;
-  if (nrows_bc == 0) return;
-  // first BC row whose slots end after lo, in two rounds of a 256-way search
-  // (the rows ascend, so "ends at or before lo" holds for a prefix)
-  auto before = [&](int64_t k) {
-    if (k >= nrows_bc) return false;
-    const int32_t r = __ldg(rows + k);
-    return r < 0 || r >= num_rows || __ldg(row_ptr + r + 1) <= lo;
-  };
-  const int64_t step = (nrows_bc + blockDim.x - 1) / blockDim.x;
-  const int c1 = __syncthreads_count(before((int64_t)threadIdx.x * step));  // also orders the zeros
-  const int64_t base = c1 == 0 ? 0 : (int64_t)(c1 - 1) * step + 1;
-  const int c2 = __syncthreads_count(threadIdx.x < step - 1 && c1 > 0 && before(base + threadIdx.x));
-  const int64_t a = c1 == 0 ? 0 : base + c2;
-  for (int64_t k = a + threadIdx.x; k < nrows_bc; k += blockDim.x) {
-    const int32_t r = __ldg(rows + k);
-    if (r < 0 || r >= num_rows) continue;
-    if (__ldg(row_ptr + r) >= hi) break;  // rows ascend: the later ones start later
-    const int32_t d = __ldg(diag + r);
-    if (d >= lo && d < hi) v[d] = value;
-  }
+  if (!dslot) return;
+  const int32_t k0 = __ldg(bstart + blockIdx.x), k1 = __ldg(bstart + blockIdx.x + 1);
+  if (k0 == k1) return;
+  __syncthreads();  // the zeros of this range before its diagonal values
+  for (int32_t k = k0 + threadIdx.x; k < k1; k += blockDim.x) v[__ldg(dslot + k)] = value;
 }
 
 // set_diagonal (CUDAAssembler.cpp:131-164) with the diagonal slot precomputed
@@ -1696,11 +1679,21 @@ void launch_zero(double* v, int64_t n, cudaStream_t s) {
   FE_CUDA(cudaGetLastError());
 }
 
+namespace {
+__global__ void k_gather_diag(const int32_t* __restrict__ rows, int64_t n, const int32_t* __restrict__ diag,
+                              int64_t num_rows, int32_t* __restrict__ out) {
+  const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const int32_t r = rows[k];
+  out[k] = (r >= 0 && r < num_rows) ? diag[r] : -1;
+}
+}  // namespace
+
 void launch_zero_diagonal(const fe_sparsity_s& sp, const fe_bc_s* bc, double diagonal, double* values,
                           cudaStream_t s) {
   const int64_t n = sp.nnz;
   if (n <= 0) return;
-  if ((reinterpret_cast<uintptr_t>(values) & 15) != 0 || (bc && !bc->rows_sorted.p && bc->n_owned)) {
+  if ((reinterpret_cast<uintptr_t>(values) & 15) != 0) {
     launch_zero(values, n, s);
     if (bc) launch_set_diagonal(sp, *bc, diagonal, values, s);
     return;
@@ -1711,9 +1704,43 @@ void launch_zero_diagonal(const fe_sparsity_s& sp, const fe_bc_s* bc, double dia
   const int64_t blocks = std::max<int64_t>(1, std::min<int64_t>((n / 2 + 255) / 256, (int64_t)sms * 8));
   int64_t chunk = (n + blocks - 1) / blocks;
   chunk += chunk & 1;  // even, so every block's range starts on 16 bytes
-  const unsigned grid = (unsigned)((n + chunk - 1) / chunk);
-  k_zero_diag<<<grid, 256, 0, s>>>(values, n, chunk, sp.row_ptr.p, sp.diag.p, bc ? bc->rows_sorted.p : nullptr,
-                                   bc ? bc->n_owned : 0, sp.num_rows, diagonal);
+  const int64_t grid = (n + chunk - 1) / chunk;
+  const int32_t* dslot = nullptr;
+  const int32_t* bstart = nullptr;
+  if (bc && bc->n_owned) {
+    // the BC rows' diagonal slots (ascending: rows ascend) and each block's
+    // first one, once per (pattern, launch shape)
+    auto& D = bc->diag_slots[sp.id];
+    if (!D || D->chunk != chunk || D->grid != grid) {
+      D = std::make_unique<fe_bc_s::DiagSlots>();
+      DevBuf<int32_t> tmp((size_t)bc->n_owned);
+      k_gather_diag<<<(unsigned)((bc->n_owned + 255) / 256), 256, 0, s>>>(bc->rows_sorted.p, bc->n_owned,
+                                                                           sp.diag.p, sp.num_rows, tmp.p);
+      FE_CUDA(cudaGetLastError());
+      std::vector<int32_t> h((size_t)bc->n_owned);
+      FE_CUDA(cudaMemcpyAsync(h.data(), tmp.p, h.size() * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+      FE_CUDA(cudaStreamSynchronize(s));
+      std::vector<int32_t> slots;
+      slots.reserve(h.size());
+      for (int32_t d : h)
+        if (d >= 0) slots.push_back(d);
+      std::sort(slots.begin(), slots.end());
+      std::vector<int32_t> starts((size_t)grid + 1);
+      for (int64_t b = 0; b <= grid; ++b)
+        starts[b] = (int32_t)(std::lower_bound(slots.begin(), slots.end(), (int64_t)std::min(b * chunk, n)) -
+                              slots.begin());
+      D->slots.alloc(std::max<size_t>(1, slots.size()));
+      if (!slots.empty())
+        FE_CUDA(cudaMemcpy(D->slots.p, slots.data(), slots.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+      D->starts.alloc(starts.size());
+      FE_CUDA(cudaMemcpy(D->starts.p, starts.data(), starts.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+      D->chunk = chunk;
+      D->grid = grid;
+    }
+    dslot = D->slots.p;
+    bstart = D->starts.p;
+  }
+  k_zero_diag<<<(unsigned)grid, 256, 0, s>>>(values, n, chunk, dslot, bstart, diagonal);
   FE_CUDA(cudaGetLastError());
 }
 
