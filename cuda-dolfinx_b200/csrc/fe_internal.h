@@ -146,7 +146,7 @@ struct fe_bc_s {
     fe::DevBuf<int32_t> slots, starts;
     int64_t chunk = 0, grid = 0;
   };
-  std::map<uint64_t, std::unique_ptr<DiagSlots>> diag_slots;
+  mutable std::map<uint64_t, std::unique_ptr<DiagSlots>> diag_slots;  // a cache: filled on const use
   fe::DevBuf<uint8_t> markers;   // [num_dofs]
   fe::DevBuf<int32_t> dofs;      // [n_bc], owned first
   fe::DevBuf<double> g;          // [num_dofs]
