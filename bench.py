@@ -494,9 +494,11 @@ def run_gpu(args, rank, world, local_rank):
     mats = [tuple(torch.cuda.Event(enable_timing=True) for _ in range(3)) for _ in range(args.steps)]
     # matrix-call time (roofline basis): eager steps with events around the
     # call; the right-hand side follows it on the same stream
+    torch.cuda.nvtx.range_push("timed")  # lets a profiler select these launches (--nvtx-include timed/)
     for k in range(args.steps):
         step(mats[k][0], mats[k][1], ev2=mats[k][2])
     torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
     mat_ms = statistics.mean(m0.elapsed_time(m1) for m0, m1, _ in mats)
     rhs_ms = statistics.mean(m1.elapsed_time(m2) for _, m1, m2 in mats)
     # whole steps: the step's engine calls captured once in a CUDA graph and
