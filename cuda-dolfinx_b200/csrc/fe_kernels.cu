@@ -1818,10 +1818,7 @@ void launch_matrix_atomic(const MatLaunch& L, cudaStream_t s) {
         constexpr int C = decltype(coef)::value;
         using T = typename decltype(tv)::type;
         if (L.coalesced && !a.upper) {
-          // shared memory before L1: the staged element tensors set the CTAs per SM
           auto k = stage ? k_mat_p2_coal<C, T, true> : k_mat_p2_coal<C, T, false>;
-          FE_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                       cudaSharedmemCarveoutMaxShared));
           k<<<grid_for(L.num_cells, kCoalThreads), kCoalThreads, 0, s>>>(a);
         } else if (nt == 32) {
           if (stage) k_mat_p2_atomic<C, T, 32, true><<<grid_for(L.num_cells, 32), 32, 0, s>>>(a);
@@ -1848,8 +1845,6 @@ void launch_matrix_atomic(const MatLaunch& L, cudaStream_t s) {
     case FE_FORM_VP2_ELASTICITY:
       if (L.coalesced && !a.upper) {
         auto k = f32 ? k_mat_vp2_coal<float> : k_mat_vp2_coal<double>;
-        FE_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                     cudaSharedmemCarveoutMaxShared));
         k<<<grid_for(L.num_cells, kVCoalThreads), kVCoalThreads, 0, s>>>(a);
       } else if (f32) {
         k_mat_vp2_atomic<float><<<grid, kBlock, 0, s>>>(a);
