@@ -234,14 +234,19 @@ struct KVec<4> {
 // (i % IPL) * 32 + i / IPL for instance i, so the per-lane writes are
 // conflict-free.
 // kp loads: through the read-only path when kp was written by an earlier
-// launch, at L2 (ld.global.cg) when this launch wrote it before a grid barrier
-template <bool L2ONLY, typename KV>
+// launch; when this launch wrote it before its grid barrier, through L1 with
+// ld.global.ca.  That is coherent here: L1 holds nothing of kp when the
+// launch starts, and every 128-byte line of kp is written whole by one
+// transpose tile (32 floats from a column that is a multiple of 32, rows of
+// ld floats with ld a multiple of 32), so a line an SM's L1 holds after the
+// barrier is one its own CTAs wrote in full, or one read after the barrier.
+template <bool WRITTEN_HERE, typename KV>
 __device__ __forceinline__ KV load_kp(const KV* p) {
-  if constexpr (L2ONLY) return __ldcg(p);
+  if constexpr (WRITTEN_HERE) return __ldca(p);
   else return __ldg(p);
 }
 
-template <int IPL, bool L2ONLY>
+template <int IPL, bool WRITTEN_HERE>
 __device__ __forceinline__ void gather_items(const GatherArgs& a, unsigned char* smem_raw) {
   using Cfg = GatherCfg<IPL>;
   using KV = typename KVec<IPL>::T;
@@ -292,7 +297,7 @@ __device__ __forceinline__ void gather_items(const GatherArgs& a, unsigned char*
       for (; q0 + kLoadBatch <= cnt; q0 += kLoadBatch) {
         KV kv[kLoadBatch];
 #pragma unroll
-        for (int u = 0; u < kLoadBatch; ++u) kv[u] = load_kp<L2ONLY>(kb + (int64_t)R[q0 + u].cell * ldv);
+        for (int u = 0; u < kLoadBatch; ++u) kv[u] = load_kp<WRITTEN_HERE>(kb + (int64_t)R[q0 + u].cell * ldv);
 #pragma unroll
         for (int u = 0; u < kLoadBatch; ++u) consume(base + q0 + u, R[q0 + u].ae, kv[u]);
       }
@@ -300,7 +305,7 @@ __device__ __forceinline__ void gather_items(const GatherArgs& a, unsigned char*
         KV kv[kLoadBatch];
 #pragma unroll
         for (int u = 0; u < kLoadBatch; ++u)
-          if (q0 + u < cnt) kv[u] = load_kp<L2ONLY>(kb + (int64_t)R[q0 + u].cell * ldv);
+          if (q0 + u < cnt) kv[u] = load_kp<WRITTEN_HERE>(kb + (int64_t)R[q0 + u].cell * ldv);
 #pragma unroll
         for (int u = 0; u < kLoadBatch; ++u)
           if (q0 + u < cnt) consume(base + q0 + u, R[q0 + u].ae, kv[u]);

@@ -137,3 +137,18 @@ def test_batch_empty_and_unsupported():
     kd = [torch.ones(len(Pv["cells"]), dtype=torch.float64, device="cuda")]
     with pytest.raises(RuntimeError, match="P1/P2 stiffness"):
         asm.assemble_matrix_batch(av, kd)
+
+
+def test_batch_second_call_with_new_coefficients():
+    # two calls into the same matrices with different coefficients: the
+    # second must see only its own packed coefficients (nothing of the first
+    # call's packed copy may be read back through a cache)
+    P, M, a, asm, bcs, torch = _setup("p1", 5)
+    k1 = _instances(P, 40, seed=21)
+    k2 = _instances(P, 40, seed=22)
+    mats = asm.assemble_matrix_batch(a, torch.tensor(np.stack(k1), device="cuda"), bcs=bcs)
+    mats = asm.assemble_matrix_batch(a, torch.tensor(np.stack(k2), device="cuda"), mats=mats, bcs=bcs)
+    torch.cuda.synchronize()
+    for i in (0, 17, 39):
+        rp, col, ref = _oracle_matrix(P, k2[i])
+        _check(mats[i].values.cpu().numpy(), ref)
