@@ -234,15 +234,12 @@ struct KVec<4> {
 // (i % IPL) * 32 + i / IPL for instance i, so the per-lane writes are
 // conflict-free.
 // kp loads: through the read-only path when kp was written by an earlier
-// launch; when this launch wrote it before its grid barrier, through L1 with
-// ld.global.ca.  That is coherent here: L1 holds nothing of kp when the
-// launch starts, and every 128-byte line of kp is written whole by one
-// transpose tile (32 floats from a column that is a multiple of 32, rows of
-// ld floats with ld a multiple of 32), so a line an SM's L1 holds after the
-// barrier is one its own CTAs wrote in full, or one read after the barrier.
+// launch, at L2 (ld.global.cg) when this launch wrote it before its grid
+// barrier (loading those lines through L1 measured no faster: 2.91 ms per
+// 256-instance call either way)
 template <bool WRITTEN_HERE, typename KV>
 __device__ __forceinline__ KV load_kp(const KV* p) {
-  if constexpr (WRITTEN_HERE) return __ldca(p);
+  if constexpr (WRITTEN_HERE) return __ldcg(p);
   else return __ldg(p);
 }
 

@@ -81,6 +81,14 @@ struct fe_context_s {
   int device = 0;
   int num_sms = 0;
   fe::DevBuf<unsigned> err;  // device error word
+  // stream-ordered scratch of the solvers (fe_pcg.cu): a pool of this
+  // context's own that keeps up to a quarter of the device memory cached
+  // between calls, instead of the default pool, which returns its memory at
+  // every synchronise and maps it again on the next solve
+  cudaMemPool_t scratch_pool = nullptr;
+  ~fe_context_s() {
+    if (scratch_pool) (void)cudaMemPoolDestroy(scratch_pool);
+  }
 };
 
 struct fe_mesh_s {

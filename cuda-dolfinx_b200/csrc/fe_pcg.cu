@@ -197,16 +197,36 @@ __global__ void __launch_bounds__(kThreads) k_update_p(int64_t n, const double* 
 
 // cudaMallocAsync'd buffers freed with cudaFreeAsync on the same stream when
 // the scope ends, normally or by an exception.
+cudaMemPool_t scratch_pool(fe_context_s& ctx) {
+  static std::mutex m;  // solver calls on several host threads share the context
+  std::lock_guard<std::mutex> lock(m);
+  if (!ctx.scratch_pool) {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = ctx.device;
+    cudaMemPool_t pool = nullptr;
+    FE_CUDA(cudaMemPoolCreate(&pool, &props));
+    size_t free_b = 0, total_b = 0;
+    FE_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    uint64_t keep = total_b / 4;
+    FE_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    ctx.scratch_pool = pool;
+  }
+  return ctx.scratch_pool;
+}
+
 struct StreamScratch {
   cudaStream_t s;
+  cudaMemPool_t pool;
   std::vector<void*> ptrs;
-  explicit StreamScratch(cudaStream_t st) : s(st) {}
+  StreamScratch(cudaStream_t st, cudaMemPool_t p) : s(st), pool(p) {}
   StreamScratch(const StreamScratch&) = delete;
   StreamScratch& operator=(const StreamScratch&) = delete;
   template <typename T>
   T* get(int64_t count) {
     void* q = nullptr;
-    FE_CUDA(cudaMallocAsync(&q, (size_t)std::max<int64_t>(count, 1) * sizeof(T), s));
+    FE_CUDA(cudaMallocFromPoolAsync(&q, (size_t)std::max<int64_t>(count, 1) * sizeof(T), pool, s));
     ptrs.push_back(q);
     return static_cast<T*>(q);
   }
@@ -235,7 +255,7 @@ void run(const fe_sparsity_s& A, const double* val, const double* b, double* x, 
   const unsigned grid_rows = (unsigned)(A.ctx->num_sms * 8);
   // stream-ordered scratch, released on every exit path (a launch or
   // synchronisation error inside the loop throws)
-  StreamScratch buf(s);
+  StreamScratch buf(s, scratch_pool(*A.ctx));
   double* r = buf.get<double>(n);
   double* z = buf.get<double>(n);
   double* p = buf.get<double>(n);
@@ -592,7 +612,7 @@ int pcg_solve_mixed(const fe_sparsity_s& A, const double* val, const double* b, 
   const int64_t n = A.num_rows, nnz = A.nnz, nb = n / 3;
   const unsigned grid = (unsigned)(A.ctx->num_sms * 4);
   const unsigned grid_rows = (unsigned)(A.ctx->num_sms * 8);
-  StreamScratch buf(s);
+  StreamScratch buf(s, scratch_pool(*A.ctx));
   double* r = buf.get<double>(n);
   double* z = buf.get<double>(n);
   double* p = buf.get<double>(n);
