@@ -1610,21 +1610,20 @@ def run_reference_multimesh(args):
 def serve_request_bytes(kind, n, iterations, solver="fp64"):
     """Bytes one request must move: its matrix assembly (values written,
     slot map, dofmap, geometry, coordinates, coefficients), b, and per PCG
-    iteration one SpMV (values and columns: 12 B per entry in FP64; 8 B with
-    FP32 values; 4 + 4/9 B in the 3x3 block-column layout of vector-P2; row
-    pointers, p, Ap) plus the vector updates (x, r, z, p, Ap, dinv).  With
-    solver="mixed" the iterations are the FP32 inner ones; the FP64
-    refinement passes (a few per request) are not counted."""
+    iteration one SpMV (values and columns: 12 B per entry in FP64; 4 + 4/9 B
+    in the FP32 3x3 block-column layout the server's mixed solver uses for
+    vector P2; row pointers, p, Ap) plus the vector updates (x, r, z, p, Ap,
+    dinv).  For vector P2 with solver="mixed" the iterations are the FP32
+    inner ones; the FP64 refinement passes (a few per request) are not
+    counted."""
     from cudolfinx import serve
 
     sz = serve.problem_sizes(kind, n)
     C, N, nnz, k = sz["cells"], sz["rows"], sz["nnz"], sz["k"]
     asm = 8 * nnz + k * k * C + 4 * k * C + 16 * C + 24 * sz["vertices"] + 8 * C * (2 if kind == "vp2" else 1)
     vec = 8 * N + 4 * k * C + 16 * C
-    if solver == "mixed":
-        per_nnz = 4 + 4 / 9 if kind == "vp2" else 8
-    else:
-        per_nnz = 12
+    # the server's mixed solver runs FP32 inner iterations for vector P2 only
+    per_nnz = 4 + 4 / 9 if (solver == "mixed" and kind == "vp2") else 12
     per_it = per_nnz * nnz + 4 * N + 16 * N + 8 * 10 * N
     return asm + vec + iterations * per_it
 
@@ -1636,7 +1635,7 @@ def serve_working_set(kind, n, solver="fp64"):
     from cudolfinx import serve
 
     sz = serve.problem_sizes(kind, n)
-    per_nnz = (4 + 4 / 9 if kind == "vp2" else 8) if solver == "mixed" else 12
+    per_nnz = 4 + 4 / 9 if (solver == "mixed" and kind == "vp2") else 12
     return per_nnz * sz["nnz"] + (4 + 6 * 8) * sz["rows"]
 
 
@@ -1727,7 +1726,7 @@ def run_gpu_serve(args, rank, world, local_rank):
         "value": value, "unit": "req/s", "n_gpus": world, "steps": count, "warmup": 4,
         "ms_per_step": 1e3 / top["throughput_rps"] if top["throughput_rps"] else None,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32-element(P2, vP2)/f64-accumulate, f32-inner/f64-refined PCG",
+        "dtype": "f32-element(P2, vP2)/f64-accumulate; PCG f32-inner/f64-refined (vP2), f64 (P1, P2)",
         "data": "synthetic (seeded request stream)",
         "config": {"workload": SERVE["desc"] + f" in [{SERVE['nmin']}, {nmax}] (bounded sample of the "
                    f"10,000-request stream: {count} requests per rate)", "requests": count, "rates_rps": rates,

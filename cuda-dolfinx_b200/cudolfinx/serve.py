@@ -18,9 +18,11 @@ requests as they arrive and keeps several of them on the device at once:
   request larger than the whole budget is answered with an error;
 * every worker drives its own CUDA stream, so the assemblies and solves of
   concurrent requests overlap on the device;
-* solves run in mixed precision: inner Jacobi-PCG iterations on an FP32 copy
-  of the matrix values (vector P2 in 3x3 blocks: 4.4 instead of 12 bytes per
-  nonzero), refined against the FP64 residual to the request's rtol.
+* vector-P2 solves run in mixed precision: inner Jacobi-PCG iterations on an
+  FP32 copy of the matrix values in 3x3 blocks (4.4 instead of 12 bytes per
+  nonzero), refined against the FP64 residual to the request's rtol; scalar
+  P1 / P2 solves stay FP64 (their refinement restarts cost more iterations
+  than the FP32 values save: P2 n=48 70.5 against 63.9 ms on B200).
 
 ``plain`` mode is the one-at-a-time FP64 path the server is compared with:
 one worker, no caches (each request builds its mesh, pattern and forms),
@@ -282,6 +284,8 @@ def _execute(asm, slot: _Slot, req: Request, variant: str = "auto", solver: str 
     asm.assemble_matrix(slot.a, slot.A, bcs=slot.bcs, variant=variant)
     asm.assemble_rhs(slot.L, slot.a, slot.bcs, vec=slot.b)
     slot.x.vector.zero_()
+    if solver == "mixed" and slot.V.bs != 3:
+        solver = "fp64"  # scalar systems: the FP64 solve is the faster one
     x, its, res = asm.solve(slot.A, slot.b, slot.x, rtol=req.rtol, raise_on_failure=False, precision=solver,
                             block_size=slot.V.bs)
     xh = x.vector.to("cpu")  # waits for this stream only
@@ -296,8 +300,9 @@ class Server:
     ``precision``: element tensors of the P2 and vector-P2 forms ("fp32" or
     "fp64"; P1 is always FP64).  ``variant``: matrix assembly variant
     ("deterministic" makes every result bitwise independent of what else
-    runs).  ``solver``: "mixed" (FP32 values in the inner PCG iterations, in
-    3x3 blocks for vector P2, refined in FP64 to the request's rtol) or "fp64".
+    runs).  ``solver``: "mixed" (vector P2: FP32 values in 3x3 blocks in the
+    inner PCG iterations, refined in FP64 to the request's rtol; P1 / P2:
+    FP64) or "fp64".
     ``plain=True``: the one-at-a-time FP64 path (one worker, nothing cached,
     FP64 solver)."""
 
