@@ -106,8 +106,9 @@ enum fe_precision {
 };
 
 /* Flags of fe_assemble_matrix.  Without a variant flag the default runs: the
- * block variant for P1 stiffness on meshes of >= 2^20 cells, the FP64-atomic
- * scatter otherwise (the fastest measured on B200 for each case). */
+ * block variant for P1 stiffness on meshes of >= 2^20 cells, the coalesced
+ * variant for P2 stiffness and vector-P2 elasticity, the FP64-atomic scatter
+ * otherwise (the fastest measured on B200 for each case). */
 #define FE_ASM_ZERO 1u            /* overwrite instead of accumulating (assemble.py:52 zero=True)   */
 #define FE_ASM_DETERMINISTIC 2u   /* bitwise reproducible: ordered tile gather (P1/P2), else sorted-slot */
 #define FE_ASM_ATOMIC 4u          /* FP64-atomic scatter through the slot map (zero pass first); for

@@ -452,8 +452,8 @@ def test_vp2_coalesced_matches_atomic_and_is_symmetric(precision):
 def test_p2_default_scatter_on_a_larger_mesh(renumber):
     # the default P2 scatter (warp-coalesced) on P2 n=24 (82,944 cells,
     # 1,296 CTAs), in the mesh's order and with a random cell order and dof
-    # numbering; assembled twice into the same values (the second call's zero
-    # pass must clear the first's)
+    # numbering; assembled twice into the same values, the second time over
+    # NaN (the zero pass must reach every slot)
     from conftest import ensure_library
     ensure_library()
     import cudolfinx as cx
@@ -477,8 +477,10 @@ def test_p2_default_scatter_on_a_larger_mesh(renumber):
     asm = cx.CUDAAssembler()
     a = cx.form(fem.stiffness(V, k))
     A = asm.assemble_matrix(a, bcs=[bc])
+    A.values.fill_(float("nan"))
     asm.assemble_matrix(a, A, bcs=[bc])
     A.assemble()
+    assert np.isfinite(A.values.cpu().numpy()).all()
     rp, col = A.sparsity.to_host()
     rp_o, col_o = fo.sparsity(V.dofs, V.dofs, V.num_nodes)
     assert np.array_equal(rp, rp_o) and np.array_equal(col, col_o)
