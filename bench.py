@@ -62,6 +62,8 @@ WORKLOADS = {
     "p3": dict(kind="p3", n=48, precision="fp64",
                desc="equispaced P3 Poisson n=48: 663,552 tets, 3,048,625 dofs, k DG0 lognormal, f DG0 U[-1,1], "
                     "g=x+y+z"),
+    "p3mid": dict(kind="p3", n=32, precision="fp64",
+                  desc="equispaced P3 Poisson n=32 (profiling size): 196,608 tets, k DG0 lognormal, f DG0, g=x+y+z"),
 }
 # batched workload: many DG0-coefficient instances on one mesh and pattern
 BATCH = dict(n=48, instances=256, cpu_sample=4,
@@ -101,7 +103,7 @@ def matrix_kernels(kind: str, variant: str, big: bool = False, nnz: int = 1 << 3
     if variant in ("sorted-slot", "deterministic"):
         return 3
     atomic = variant == "atomic" or (variant == "auto" and not (kind == "p1" and big)
-                                     and kind not in ("p2", "vp2"))
+                                     and kind not in ("p2", "vp2", "p3"))
     if kind in ("p1", "vp2", "p3") and atomic:
         return 3  # zero + upper-triangle scatter + lower-triangle transpose
     return 2  # zero (with the BC diagonal) + kernel
@@ -587,11 +589,13 @@ def run_gpu(args, rank, world, local_rank):
     achieved = alg / (mat_ms / 1e3) / 1e9
     # the variant "auto" resolves to (fe_assemble_matrix's default): the block
     # kernel for P1 meshes of >= 2^20 cells, the coalesced scatter for P2
-    # stiffness, the atomic scatter otherwise
+    # stiffness, vector-P2 elasticity and FP64 P3 stiffness, the atomic
+    # scatter otherwise
     resolved = args.variant
     if resolved == "auto":
         resolved = ("block" if (W["kind"] == "p1" and len(I["cells"]) >= (1 << 20))
-                    else "coalesced" if W["kind"] in ("p2", "vp2") else "atomic")
+                    else "coalesced" if (W["kind"] in ("p2", "vp2") or (W["kind"] == "p3" and W["precision"] == "fp64"))
+                    else "atomic")
     kernel_key = f"{args.workload}:{resolved}"
     traffic = load_traffic(kernel_key)
     out = {

@@ -938,8 +938,9 @@ int fe_assemble_matrix(fe_form a, double* values, fe_bc bc0, fe_bc bc1, double d
       return;
     }
     if (flags & FE_ASM_COALESCED)
-      FE_REQUIRE(a->kind == FE_FORM_P2_STIFFNESS || a->kind == FE_FORM_VP2_ELASTICITY,
-                 "the coalesced variant supports P2 stiffness and vector-P2 elasticity");
+      FE_REQUIRE(a->kind == FE_FORM_P2_STIFFNESS || a->kind == FE_FORM_VP2_ELASTICITY ||
+                     (a->kind == FE_FORM_P3_STIFFNESS && a->precision == FE_PREC_FP64),
+                 "the coalesced variant supports P2 stiffness, vector-P2 elasticity and FP64 P3 stiffness");
     if (flags & FE_ASM_GROUPED) {
       FE_REQUIRE(grouped_supported(*a), "the grouped variant supports P2 stiffness on an unrestricted pattern");
       if (assemble_matrix_grouped(*a, values, bc0, bc1, zero, st)) {
@@ -993,7 +994,8 @@ int fe_assemble_matrix(fe_form a, double* values, fe_bc bc0, fe_bc bc1, double d
     // 2.81 ms for the thread-per-cell reductions, which FE_ASM_ATOMIC keeps)
     const bool coalesced = (flags & FE_ASM_COALESCED) ||
                            (!(flags & FE_ASM_ATOMIC) && !view &&
-                            (a->kind == FE_FORM_P2_STIFFNESS || a->kind == FE_FORM_VP2_ELASTICITY));
+                            (a->kind == FE_FORM_P2_STIFFNESS || a->kind == FE_FORM_VP2_ELASTICITY ||
+                             (a->kind == FE_FORM_P3_STIFFNESS && a->precision == FE_PREC_FP64)));
     const bool upper = !coalesced && zero && !view && !(flags & FE_ASM_FULL_SCATTER) &&
                        (a->kind == FE_FORM_VP2_ELASTICITY || a->kind == FE_FORM_P3_STIFFNESS ||
                         a->kind == FE_FORM_P1_STIFFNESS || a->kind == FE_FORM_P1_MASS ||

@@ -579,6 +579,100 @@ __global__ void __launch_bounds__(kBlockP3) k_mat_p3_atomic(const MatArgs a) {
 }
 
 // ---------------------------------------------------------------------------
+// P3 stiffness (cellwise-constant coefficient, FP64) with the reductions
+// coalesced per warp ("coalesced" variant, the FP64 P3 default).  The
+// 210-entry element tensor is too large to stage per cell, so each thread
+// computes only its cell's geometry, g[s] = k * Ghat_s (6 doubles), row
+// starts and column masks; the warp then walks its 32 cells and evaluates
+// the 400 entries of each in 13 rounds, lane l of round r on entry
+// e = 32r + l = 20i + j: value = sum_s g[s] * kP3GradGradSym[s*400 + e] (the
+// terms of p3_stiffness_const; one term order for (i, j) and (j, i), so the
+// element matrix is exactly symmetric).  Consecutive lanes take consecutive
+// columns of one or two element rows, so an instruction's reductions fall in
+// two CSR rows and share L2 sectors, and no transpose pass is needed.
+// ---------------------------------------------------------------------------
+constexpr int kP3CoalThreads = 128;
+
+__global__ void __launch_bounds__(kP3CoalThreads) k_mat_p3_coal(const MatArgs a) {
+  constexpr int NT = kP3CoalThreads;
+  __shared__ double stab[2400];        // s-major: conflict-free for consecutive entries
+  __shared__ double sg[NT * 6];
+  __shared__ int32_t srp[NT * 20];     // row start of each local row, -1 for a masked row
+  __shared__ uint32_t smc[NT];         // masked columns of each cell
+  const int tid = threadIdx.x, lane = tid & 31, w0 = tid & ~31;
+  for (int t = tid; t < 2400; t += NT) stab[t] = kP3GradGradSym[t];
+  const int64_t c0 = blockIdx.x * (int64_t)NT;
+  const int64_t left = a.num_cells - c0;
+  const int ncell = left < NT ? (int)left : NT;
+  const int wcells = ncell - w0 < 0 ? 0 : (ncell - w0 < 32 ? ncell - w0 : 32);
+  if (tid < ncell) {
+    const int64_t c = c0 + tid;
+    CellGeo g;
+    cell_geometry(a.x, load_geom(a.geom, c), g);
+    double Gh[6];
+    ghat(g, Gh);
+    const double k = coef_cell(a.c0, c);
+#pragma unroll
+    for (int q = 0; q < 6; ++q) sg[tid * 6 + q] = k * Gh[q];
+    const int32_t* d0 = a.dofs0 + c * 20;
+    const int32_t* d1 = a.dofs1 + c * 20;
+    uint32_t mc = 0;
+#pragma unroll
+    for (int i = 0; i < 20; ++i) {
+      // masked rows / columns: BC dofs and dofs outside a restriction (-1)
+      const int r = __ldg(d0 + i), cc = __ldg(d1 + i);
+      const bool mrow = r < 0 || (a.bc0 && __ldg(a.bc0 + r));
+      srp[tid * 20 + i] = mrow ? -1 : __ldg(a.row_ptr + r);
+      mc |= (cc < 0 || (a.bc1 && __ldg(a.bc1 + cc)) ? 1u : 0u) << i;
+    }
+    smc[tid] = mc;
+  }
+  __syncthreads();  // the table; each warp's cells need only their warp
+  // a cell's 400 slot bytes as 100 words, word w = lane + 32k in register k
+  // of the lane (coalesced 128-byte loads), fetched one cell ahead; entry e
+  // of round r is byte e % 4 of word e / 4 = 8r + lane / 4, held by lane
+  // 8 (r % 4) + lane / 4 in register r / 4
+  auto load_words = [&](int64_t c, uint32_t w[4]) {
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(a.pos + c * 400);  // 400 c is a multiple of 16
+#pragma unroll
+    for (int k = 0; k < 4; ++k) w[k] = (lane + 32 * k < 100) ? __ldg(src + lane + 32 * k) : 0u;
+  };
+  double* __restrict__ vals = a.values;
+  // the 400 entries of the warp's local cell q from the words w
+  auto cell_rounds = [&](int q, const uint32_t w[4]) {
+    const double* gq = sg + q * 6;
+    const double g0 = gq[0], g1 = gq[1], g2 = gq[2], g3 = gq[3], g4 = gq[4], g5 = gq[5];
+    const uint32_t mc = smc[q];
+    const int32_t* rq = srp + q * 20;
+#pragma unroll
+    for (int r = 0; r < 13; ++r) {
+      const uint32_t word = __shfl_sync(0xffffffffu, w[r / 4], 8 * (r % 4) + lane / 4);
+      const int e = 32 * r + lane;
+      if (e >= 400) continue;
+      const int i = e / 20, j = e - 20 * (e / 20);
+      const int rs = rq[i];
+      if (rs < 0 || ((mc >> j) & 1u)) continue;
+      const double* tp = stab + e;
+      const double v = fma(g2, tp[800], fma(g1, tp[400], g0 * tp[0])) +
+                       fma(g5, tp[2000], fma(g4, tp[1600], g3 * tp[1200]));
+      atomicAdd(vals + rs + ((word >> (8 * (lane & 3))) & 0xffu), v);
+    }
+  };
+  // two word buffers in turn, each filled one cell ahead of its use (no
+  // register copy that would wait for the load)
+  uint32_t wa[4] = {0u, 0u, 0u, 0u}, wb[4] = {0u, 0u, 0u, 0u};
+  const int qend = w0 + wcells;
+  if (wcells > 0) load_words(c0 + w0, wa);
+  for (int q = w0; q < qend; q += 2) {
+    if (q + 1 < qend) load_words(c0 + q + 1, wb);
+    cell_rounds(q, wa);
+    if (q + 1 >= qend) break;
+    if (q + 2 < qend) load_words(c0 + q + 2, wa);
+    cell_rounds(q + 1, wb);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Vector-P2 elasticity (bs = 3), one thread per cell, FP64 atomics
 // A[(i,a),(j,b)] = sum_pq W_ab[p][q] R0[p][q][i][j],
 // W_ab[p][q] = |det| (mu (delta_ab (KK^T)_pq + K_pb K_qa) + lam K_pa K_qb)
@@ -1872,6 +1966,11 @@ void launch_matrix_atomic(const MatLaunch& L, cudaStream_t s) {
       else k_mat_vmass<FE_COEFF_DG0><<<grid, kBlock, 0, s>>>(a);
       break;
     case FE_FORM_P3_STIFFNESS: {
+      if (L.coalesced && !a.upper) {
+        FE_REQUIRE(!f32, "the coalesced P3 kernel evaluates FP64 element tensors");
+        k_mat_p3_coal<<<grid_for(L.num_cells, kP3CoalThreads), kP3CoalThreads, 0, s>>>(a);
+        break;
+      }
       // one thread per cell: splitting a cell's 210 entries over 2, 4 or 8
       // warps measured the same or slower on B200 (P3 n=48: 1.75-2.12 ms vs
       // 1.79 ms), the reductions themselves bound the kernel

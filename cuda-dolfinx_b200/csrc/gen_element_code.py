@@ -296,6 +296,16 @@ def gen() -> str:
     w(symmetric_body(exprs3, 20))
     w("}\n")
     w(f"constexpr double kP3ConstTermMax = {lit(maxabs3)};\n\n")
+    # the same coefficients as a table for kernels that evaluate entries lane
+    # by lane: kP3GradGradSym[s*400 + i*20 + j] (every (i, j), so the table
+    # is symmetric in i, j entry for entry)
+    w("// P3 stiffness coefficients by geometry pair s: entry (i, j) = sum_s g[s] *\n")
+    w("// kP3GradGradSym[s*400 + i*20 + j] (the terms of p3_stiffness_const).\n")
+    w("__device__ const double kP3GradGradSym[2400] = {\n")
+    vals3 = [lit(sym_pair(r3_plain, s_, i, j)) for s_ in range(6) for i in range(20) for j in range(20)]
+    for k in range(0, 2400, 6):
+        w("    " + ", ".join(vals3[k:k + 6]) + ",\n")
+    w("};\n\n")
 
     # P2 stiffness, P1 coefficient: q[m*6+s] = k_m * Ghat_s
     w("// P2 stiffness with a P1 coefficient: q[m*6+s] = k_m * Ghat_s,\n")

@@ -145,12 +145,13 @@ class CUDAAssembler:
         """Assemble a bilinear form into a device CSR matrix (not finalised).
 
         ``variant``: "auto" (block variant for P1 on meshes of >= 2^20 cells,
-        coalesced scatter for P2 stiffness and vector-P2 elasticity, atomic
-        scatter otherwise),
+        coalesced scatter for P2 stiffness, vector-P2 elasticity and FP64 P3
+        stiffness, atomic scatter otherwise),
         "deterministic" (bitwise reproducible: ordered tile gather for P1/P2,
         sorted-slot otherwise), "atomic" (FP64-atomic scatter, one thread's
-        reductions per cell), "coalesced" (P2, vector P2: a warp's reductions
-        issued row by row from shared memory), "grouped" (P2: one reduction per distinct
+        reductions per cell), "coalesced" (P2, vector P2, FP64 P3: a warp's
+        reductions issued row by row, consecutive lanes on consecutive columns),
+        "grouped" (P2: one reduction per distinct
         slot of 48-cell groups), "sorted-slot" (global sorted-slot
         reduction), "block" (Morton cell blocks combined in shared memory,
         P1/P2), "tile" (owner-computes row tiles, P1/P2), "row-gather" (P1),

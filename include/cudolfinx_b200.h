@@ -107,8 +107,8 @@ enum fe_precision {
 
 /* Flags of fe_assemble_matrix.  Without a variant flag the default runs: the
  * block variant for P1 stiffness on meshes of >= 2^20 cells, the coalesced
- * variant for P2 stiffness and vector-P2 elasticity, the FP64-atomic scatter
- * otherwise (the fastest measured on B200 for each case). */
+ * variant for P2 stiffness, vector-P2 elasticity and FP64 P3 stiffness, the
+ * FP64-atomic scatter otherwise (the fastest measured on B200 for each case). */
 #define FE_ASM_ZERO 1u            /* overwrite instead of accumulating (assemble.py:52 zero=True)   */
 #define FE_ASM_DETERMINISTIC 2u   /* bitwise reproducible: ordered tile gather (P1/P2), else sorted-slot */
 #define FE_ASM_ATOMIC 4u          /* FP64-atomic scatter through the slot map (zero pass first); for
@@ -126,11 +126,11 @@ enum fe_precision {
                                      entries summed per distinct CSR slot in shared memory, then one
                                      reduction per slot (falls back to the atomic scatter when the
                                      mesh's groups share no structure)                                */
-#define FE_ASM_COALESCED 512u     /* P2 stiffness, vector-P2 elasticity (the default for both): the
-                                     warp's reductions issued row by row from shared memory
-                                     (consecutive lanes on one cell's CSR row, so an instruction's
-                                     reductions share L2 sectors); FE_ASM_ATOMIC keeps one thread's
-                                     reductions per cell                                            */
+#define FE_ASM_COALESCED 512u     /* P2 stiffness, vector-P2 elasticity, FP64 P3 stiffness (the default
+                                     for each): the warp's reductions issued row by row (consecutive
+                                     lanes on one cell's CSR row, so an instruction's reductions
+                                     share L2 sectors); FE_ASM_ATOMIC keeps one thread's reductions
+                                     per cell                                                       */
 
 /* ---- errors / context --------------------------------------------------- */
 const char* fe_last_error(void);

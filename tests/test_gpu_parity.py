@@ -45,7 +45,7 @@ def _supported(kind, variant):
     if variant == "grouped":
         return kind == "p2"
     if variant == "coalesced":
-        return kind in ("p2", "vp2")
+        return kind in ("p2", "vp2", "p3")
     if variant in ("tile", "block"):
         return kind in ("p1", "p1k", "p2")
     return True
