@@ -444,6 +444,411 @@ __device__ __forceinline__ void p3_stiffness_const(const T* g, Emit&& emit) {
 }
 constexpr double kP3ConstTermMax = 0x1.283a83a83a83bp-1;
 
+// P3 stiffness coefficients by geometry pair s: entry (i, j) = sum_s g[s] *
+// kP3GradGradSym[s*400 + i*20 + j] (the terms of p3_stiffness_const).
+__device__ const double kP3GradGradSym[2400] = {
+    0x1.e79e79e79e79ep-5, -0x1.7297297297297p-7, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7, -0x1.1d41d41d41d42p-5, 0x1.b6db6db6db6dbp-7,
+    -0x1.1d41d41d41d42p-5, 0x1.b6db6db6db6dbp-7, -0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-5, -0x1.0750750750750p-5, 0x1.0750750750750p-5,
+    0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5, -0x1.7297297297297p-7, 0x1.e79e79e79e79ep-5, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, -0x1.1d41d41d41d42p-5, 0x1.b6db6db6db6dbp-7, -0x1.1d41d41d41d42p-5, 0x1.b6db6db6db6dbp-7,
+    -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7, 0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-4,
+    0x1.0750750750750p-5, -0x1.0750750750750p-5, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    -0x1.b6db6db6db6dbp-7, -0x1.1d41d41d41d42p-5, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x1.edb6db6db6db7p-3, -0x1.283a83a83a83bp-4, 0x1.edb6db6db6db7p-4, -0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-5, 0x1.283a83a83a83bp-4,
+    0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5,
+    -0x1.283a83a83a83bp-2, -0x1.283a83a83a83bp-3, -0x1.b6db6db6db6dbp-7, 0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, -0x1.283a83a83a83bp-4, 0x1.8af8af8af8af9p-3, -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-6,
+    0x1.283a83a83a83bp-4, -0x1.8af8af8af8af9p-3, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x0.0p+0,
+    0x1.8af8af8af8af9p-4, -0x1.8af8af8af8af9p-4, 0x0.0p+0, 0x0.0p+0, -0x1.b6db6db6db6dbp-7, -0x1.1d41d41d41d42p-5,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.edb6db6db6db7p-4, -0x1.8af8af8af8af9p-6,
+    0x1.edb6db6db6db7p-3, -0x1.283a83a83a83bp-4, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-5, 0x1.283a83a83a83bp-4,
+    0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5, -0x1.283a83a83a83bp-3, -0x1.283a83a83a83bp-2,
+    -0x1.b6db6db6db6dbp-7, 0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-6, -0x1.283a83a83a83bp-4, 0x1.8af8af8af8af9p-3, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6,
+    0x1.283a83a83a83bp-4, -0x1.8af8af8af8af9p-3, 0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-4, -0x1.8af8af8af8af9p-4,
+    0x0.0p+0, 0x0.0p+0, -0x1.1d41d41d41d42p-5, -0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x1.283a83a83a83bp-4, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6,
+    0x1.edb6db6db6db7p-3, -0x1.283a83a83a83bp-4, 0x1.edb6db6db6db7p-4, -0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6,
+    0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-5, -0x1.283a83a83a83bp-2, -0x1.283a83a83a83bp-3, 0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.283a83a83a83bp-4, -0x1.8af8af8af8af9p-3,
+    0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, -0x1.283a83a83a83bp-4, 0x1.8af8af8af8af9p-3, -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-6,
+    0x0.0p+0, 0x0.0p+0, -0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-4, 0x0.0p+0, 0x0.0p+0,
+    -0x1.1d41d41d41d42p-5, -0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-5, 0x1.283a83a83a83bp-4, 0x1.edb6db6db6db7p-4, -0x1.8af8af8af8af9p-6,
+    0x1.edb6db6db6db7p-3, -0x1.283a83a83a83bp-4, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-5,
+    -0x1.283a83a83a83bp-3, -0x1.283a83a83a83bp-2, 0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, 0x1.283a83a83a83bp-4, -0x1.8af8af8af8af9p-3,
+    -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-6, -0x1.283a83a83a83bp-4, 0x1.8af8af8af8af9p-3, 0x0.0p+0, 0x0.0p+0,
+    -0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-4, 0x0.0p+0, 0x0.0p+0, -0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-5,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-6, 0x0.0p+0,
+    0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x1.8af8af8af8af9p-6, 0x0.0p+0,
+    0x1.edb6db6db6db7p-3, -0x1.8af8af8af8af9p-3, 0x0.0p+0, 0x0.0p+0, -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-5,
+    0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-4, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x1.8af8af8af8af9p-6, 0x0.0p+0,
+    0x1.8af8af8af8af9p-6, 0x0.0p+0, -0x1.8af8af8af8af9p-3, 0x1.edb6db6db6db7p-3, 0x0.0p+0, 0x0.0p+0,
+    -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-5, -0x1.0750750750750p-5, 0x1.0750750750750p-5, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, -0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-4, -0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-4,
+    0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-4, 0x0.0p+0, 0x0.0p+0,
+    0x1.283a83a83a83bp-1, -0x1.283a83a83a83bp-1, 0x0.0p+0, 0x0.0p+0, 0x1.0750750750750p-5, -0x1.0750750750750p-5,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-4,
+    0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-4, -0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-4, -0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-4,
+    0x0.0p+0, 0x0.0p+0, -0x1.283a83a83a83bp-1, 0x1.283a83a83a83bp-1, 0x0.0p+0, 0x0.0p+0,
+    0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    -0x1.283a83a83a83bp-2, 0x0.0p+0, -0x1.283a83a83a83bp-3, 0x0.0p+0, -0x1.283a83a83a83bp-2, 0x0.0p+0,
+    -0x1.283a83a83a83bp-3, 0x0.0p+0, -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x0.0p+0,
+    0x1.283a83a83a83bp-1, 0x1.283a83a83a83bp-2, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, -0x1.283a83a83a83bp-3, 0x0.0p+0, -0x1.283a83a83a83bp-2, 0x0.0p+0,
+    -0x1.283a83a83a83bp-3, 0x0.0p+0, -0x1.283a83a83a83bp-2, 0x0.0p+0, -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-5,
+    0x0.0p+0, 0x0.0p+0, 0x1.283a83a83a83bp-2, 0x1.283a83a83a83bp-1, 0x1.e79e79e79e79ep-5, 0x0.0p+0,
+    -0x1.7297297297297p-7, 0x0.0p+0, -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x0.0p+0,
+    -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7, -0x1.1d41d41d41d42p-5, 0x1.b6db6db6db6dbp-7, -0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-5,
+    -0x1.1d41d41d41d42p-5, 0x1.b6db6db6db6dbp-7, -0x1.0750750750750p-5, 0x1.8af8af8af8af9p-5, 0x1.0750750750750p-5, 0x1.8af8af8af8af9p-5,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, -0x1.7297297297297p-7, 0x0.0p+0, 0x1.e79e79e79e79ep-5, 0x0.0p+0,
+    -0x1.1d41d41d41d42p-5, 0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x0.0p+0, 0x1.b6db6db6db6dbp-7, -0x1.1d41d41d41d42p-5,
+    -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7, 0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-4, -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7,
+    0x1.0750750750750p-5, 0x1.8af8af8af8af9p-5, -0x1.0750750750750p-5, 0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    -0x1.b6db6db6db6dbp-7, 0x0.0p+0, -0x1.1d41d41d41d42p-5, 0x0.0p+0, 0x1.edb6db6db6db7p-3, -0x1.283a83a83a83bp-4,
+    0x0.0p+0, 0x0.0p+0, -0x1.8af8af8af8af9p-6, 0x1.edb6db6db6db7p-4, 0x1.8af8af8af8af9p-5, 0x1.283a83a83a83bp-4,
+    0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-5, -0x1.283a83a83a83bp-2,
+    0x1.8af8af8af8af9p-5, -0x1.283a83a83a83bp-3, -0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x1.b6db6db6db6dbp-7, 0x0.0p+0,
+    -0x1.283a83a83a83bp-4, 0x1.8af8af8af8af9p-3, 0x0.0p+0, 0x0.0p+0, -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-6,
+    0x1.283a83a83a83bp-4, -0x1.8af8af8af8af9p-3, 0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6,
+    0x1.8af8af8af8af9p-4, 0x0.0p+0, -0x1.8af8af8af8af9p-4, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, -0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x1.b6db6db6db6dbp-7, 0x0.0p+0,
+    -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-3, -0x1.283a83a83a83bp-4,
+    0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x0.0p+0, 0x1.283a83a83a83bp-4, -0x1.8af8af8af8af9p-3,
+    0x1.8af8af8af8af9p-4, 0x0.0p+0, -0x1.8af8af8af8af9p-4, 0x0.0p+0, -0x1.b6db6db6db6dbp-7, 0x0.0p+0,
+    -0x1.1d41d41d41d42p-5, 0x0.0p+0, 0x1.edb6db6db6db7p-4, -0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x0.0p+0,
+    -0x1.283a83a83a83bp-4, 0x1.edb6db6db6db7p-3, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6,
+    0x1.8af8af8af8af9p-5, 0x1.283a83a83a83bp-4, -0x1.8af8af8af8af9p-5, -0x1.283a83a83a83bp-3, 0x1.8af8af8af8af9p-5, -0x1.283a83a83a83bp-2,
+    -0x1.1d41d41d41d42p-5, 0x0.0p+0, -0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x1.283a83a83a83bp-4,
+    0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, 0x1.edb6db6db6db7p-3, -0x1.283a83a83a83bp-4,
+    0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, 0x1.edb6db6db6db7p-4, -0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-5, -0x1.283a83a83a83bp-2,
+    -0x1.8af8af8af8af9p-5, -0x1.283a83a83a83bp-3, 0x1.b6db6db6db6dbp-7, 0x0.0p+0, -0x1.b6db6db6db6dbp-7, 0x0.0p+0,
+    0x1.283a83a83a83bp-4, -0x1.8af8af8af8af9p-3, 0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6,
+    -0x1.283a83a83a83bp-4, 0x1.8af8af8af8af9p-3, 0x0.0p+0, 0x0.0p+0, -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-6,
+    -0x1.8af8af8af8af9p-4, 0x0.0p+0, 0x1.8af8af8af8af9p-4, 0x0.0p+0, -0x1.8af8af8af8af9p-4, 0x0.0p+0,
+    0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x1.edb6db6db6db7p-3, -0x1.8af8af8af8af9p-3,
+    0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x0.0p+0, -0x1.8af8af8af8af9p-5, 0x0.0p+0, -0x1.8af8af8af8af9p-5,
+    0x1.8af8af8af8af9p-5, 0x0.0p+0, -0x1.8af8af8af8af9p-4, 0x0.0p+0, 0x1.8af8af8af8af9p-6, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, 0x0.0p+0,
+    -0x1.8af8af8af8af9p-3, 0x1.edb6db6db6db7p-3, 0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x0.0p+0, -0x1.8af8af8af8af9p-5,
+    0x0.0p+0, -0x1.8af8af8af8af9p-5, -0x1.1d41d41d41d42p-5, 0x0.0p+0, -0x1.b6db6db6db6dbp-7, 0x0.0p+0,
+    0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x0.0p+0, 0x1.283a83a83a83bp-4, 0x1.8af8af8af8af9p-5,
+    0x1.edb6db6db6db7p-4, -0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, 0x1.edb6db6db6db7p-3, -0x1.283a83a83a83bp-4,
+    0x1.8af8af8af8af9p-5, -0x1.283a83a83a83bp-3, -0x1.8af8af8af8af9p-5, -0x1.283a83a83a83bp-2, 0x1.b6db6db6db6dbp-7, 0x0.0p+0,
+    -0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x0.0p+0,
+    -0x1.8af8af8af8af9p-3, 0x1.283a83a83a83bp-4, -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x0.0p+0,
+    -0x1.283a83a83a83bp-4, 0x1.8af8af8af8af9p-3, -0x1.8af8af8af8af9p-4, 0x0.0p+0, 0x1.8af8af8af8af9p-4, 0x0.0p+0,
+    -0x1.0750750750750p-5, 0x0.0p+0, 0x1.0750750750750p-5, 0x0.0p+0, -0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-4,
+    0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-4, -0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-4,
+    0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-4, 0x1.283a83a83a83bp-1, 0x0.0p+0,
+    -0x1.283a83a83a83bp-1, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0,
+    -0x1.283a83a83a83bp-2, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, -0x1.283a83a83a83bp-3,
+    -0x1.283a83a83a83bp-2, 0x0.0p+0, -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-5, -0x1.283a83a83a83bp-3, 0x0.0p+0,
+    0x0.0p+0, 0x1.283a83a83a83bp-1, 0x0.0p+0, 0x1.283a83a83a83bp-2, 0x1.0750750750750p-5, 0x0.0p+0,
+    -0x1.0750750750750p-5, 0x0.0p+0, 0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-4, 0x0.0p+0, 0x0.0p+0,
+    -0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-4, 0x0.0p+0, 0x0.0p+0,
+    -0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-4, -0x1.283a83a83a83bp-1, 0x0.0p+0, 0x1.283a83a83a83bp-1, 0x0.0p+0,
+    0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0, -0x1.283a83a83a83bp-3, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, -0x1.283a83a83a83bp-2, -0x1.283a83a83a83bp-3, 0x0.0p+0,
+    -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-5, -0x1.283a83a83a83bp-2, 0x0.0p+0, 0x0.0p+0, 0x1.283a83a83a83bp-2,
+    0x0.0p+0, 0x1.283a83a83a83bp-1, 0x1.e79e79e79e79ep-5, 0x0.0p+0, 0x0.0p+0, -0x1.7297297297297p-7,
+    -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x0.0p+0,
+    -0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-5, -0x1.1d41d41d41d42p-5, 0x1.b6db6db6db6dbp-7, -0x1.1d41d41d41d42p-5, 0x1.b6db6db6db6dbp-7,
+    -0x1.0750750750750p-5, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5, 0x1.0750750750750p-5, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, -0x1.7297297297297p-7, 0x0.0p+0, 0x0.0p+0, 0x1.e79e79e79e79ep-5,
+    0x1.b6db6db6db6dbp-7, -0x1.1d41d41d41d42p-5, 0x1.b6db6db6db6dbp-7, -0x1.1d41d41d41d42p-5, 0x0.0p+0, 0x0.0p+0,
+    0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-4, -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7,
+    0x1.0750750750750p-5, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5, -0x1.0750750750750p-5, -0x1.b6db6db6db6dbp-7, 0x0.0p+0,
+    0x0.0p+0, 0x1.b6db6db6db6dbp-7, 0x1.8af8af8af8af9p-3, -0x1.283a83a83a83bp-4, -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-6,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.283a83a83a83bp-4, -0x1.8af8af8af8af9p-3,
+    0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-4, 0x0.0p+0, 0x0.0p+0, -0x1.8af8af8af8af9p-4,
+    -0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x0.0p+0, -0x1.1d41d41d41d42p-5, -0x1.283a83a83a83bp-4, 0x1.edb6db6db6db7p-3,
+    -0x1.8af8af8af8af9p-6, 0x1.edb6db6db6db7p-4, 0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6,
+    0x1.8af8af8af8af9p-5, 0x1.283a83a83a83bp-4, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-5, -0x1.283a83a83a83bp-2,
+    -0x1.283a83a83a83bp-3, 0x1.8af8af8af8af9p-5, -0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x0.0p+0, 0x1.b6db6db6db6dbp-7,
+    -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-3, -0x1.283a83a83a83bp-4, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, 0x1.283a83a83a83bp-4, -0x1.8af8af8af8af9p-3,
+    0x1.8af8af8af8af9p-4, 0x0.0p+0, 0x0.0p+0, -0x1.8af8af8af8af9p-4, -0x1.b6db6db6db6dbp-7, 0x0.0p+0,
+    0x0.0p+0, -0x1.1d41d41d41d42p-5, -0x1.8af8af8af8af9p-6, 0x1.edb6db6db6db7p-4, -0x1.283a83a83a83bp-4, 0x1.edb6db6db6db7p-3,
+    0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6,
+    0x1.8af8af8af8af9p-5, 0x1.283a83a83a83bp-4, -0x1.8af8af8af8af9p-5, -0x1.283a83a83a83bp-3, -0x1.283a83a83a83bp-2, 0x1.8af8af8af8af9p-5,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, -0x1.8af8af8af8af9p-4, 0x0.0p+0,
+    0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x1.8af8af8af8af9p-6,
+    0x0.0p+0, 0x0.0p+0, 0x1.edb6db6db6db7p-3, -0x1.8af8af8af8af9p-3, 0x1.8af8af8af8af9p-6, 0x0.0p+0,
+    0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x0.0p+0, -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-5, 0x0.0p+0,
+    0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x0.0p+0, -0x1.8af8af8af8af9p-4, 0x0.0p+0, 0x1.8af8af8af8af9p-6,
+    0x0.0p+0, 0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x0.0p+0, -0x1.8af8af8af8af9p-3, 0x1.edb6db6db6db7p-3,
+    0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x0.0p+0, -0x1.8af8af8af8af9p-5,
+    -0x1.8af8af8af8af9p-5, 0x0.0p+0, -0x1.1d41d41d41d42p-5, 0x0.0p+0, 0x0.0p+0, -0x1.b6db6db6db6dbp-7,
+    0x1.283a83a83a83bp-4, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x0.0p+0,
+    0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, 0x1.edb6db6db6db7p-3, -0x1.283a83a83a83bp-4, 0x1.edb6db6db6db7p-4, -0x1.8af8af8af8af9p-6,
+    0x1.8af8af8af8af9p-5, -0x1.283a83a83a83bp-2, -0x1.283a83a83a83bp-3, -0x1.8af8af8af8af9p-5, 0x1.b6db6db6db6dbp-7, 0x0.0p+0,
+    0x0.0p+0, -0x1.b6db6db6db6dbp-7, -0x1.8af8af8af8af9p-3, 0x1.283a83a83a83bp-4, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, -0x1.283a83a83a83bp-4, 0x1.8af8af8af8af9p-3,
+    -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-4, 0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-4,
+    -0x1.1d41d41d41d42p-5, 0x0.0p+0, 0x0.0p+0, -0x1.b6db6db6db6dbp-7, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6,
+    0x1.283a83a83a83bp-4, 0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6,
+    0x1.edb6db6db6db7p-4, -0x1.8af8af8af8af9p-6, 0x1.edb6db6db6db7p-3, -0x1.283a83a83a83bp-4, 0x1.8af8af8af8af9p-5, -0x1.283a83a83a83bp-3,
+    -0x1.283a83a83a83bp-2, -0x1.8af8af8af8af9p-5, 0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x0.0p+0, -0x1.b6db6db6db6dbp-7,
+    0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-3, 0x1.283a83a83a83bp-4, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-6, -0x1.283a83a83a83bp-4, 0x1.8af8af8af8af9p-3,
+    -0x1.8af8af8af8af9p-4, 0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-4, -0x1.0750750750750p-5, 0x0.0p+0,
+    0x0.0p+0, 0x1.0750750750750p-5, 0x1.8af8af8af8af9p-4, -0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-4, -0x1.8af8af8af8af9p-5,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-4,
+    0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-4, 0x1.283a83a83a83bp-1, 0x0.0p+0, 0x0.0p+0, -0x1.283a83a83a83bp-1,
+    0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0, -0x1.283a83a83a83bp-2,
+    0x0.0p+0, -0x1.283a83a83a83bp-3, 0x0.0p+0, 0x0.0p+0, -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-5,
+    -0x1.283a83a83a83bp-2, 0x0.0p+0, -0x1.283a83a83a83bp-3, 0x0.0p+0, 0x0.0p+0, 0x1.283a83a83a83bp-1,
+    0x1.283a83a83a83bp-2, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-5,
+    0x0.0p+0, -0x1.283a83a83a83bp-3, 0x0.0p+0, -0x1.283a83a83a83bp-2, 0x0.0p+0, 0x0.0p+0,
+    -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-5, -0x1.283a83a83a83bp-3, 0x0.0p+0, -0x1.283a83a83a83bp-2, 0x0.0p+0,
+    0x0.0p+0, 0x1.283a83a83a83bp-2, 0x1.283a83a83a83bp-1, 0x0.0p+0, 0x1.0750750750750p-5, 0x0.0p+0,
+    0x0.0p+0, -0x1.0750750750750p-5, -0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-5,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, -0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-4,
+    -0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-4, -0x1.283a83a83a83bp-1, 0x0.0p+0, 0x0.0p+0, 0x1.283a83a83a83bp-1,
+    0x1.e79e79e79e79ep-4, -0x1.7297297297297p-7, -0x1.7297297297297p-7, 0x0.0p+0, -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7,
+    -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-6, -0x1.b6db6db6db6dbp-6, -0x1.1d41d41d41d42p-4, 0x1.b6db6db6db6dbp-6,
+    -0x1.0cccccccccccdp-3, 0x1.f8af8af8af8b0p-5, -0x1.0cccccccccccdp-3, 0x1.f8af8af8af8b0p-5, -0x1.0750750750750p-4, 0x1.4924924924925p-4,
+    0x1.4924924924925p-4, 0x1.8af8af8af8af9p-4, -0x1.7297297297297p-7, 0x0.0p+0, 0x1.7297297297297p-7, 0x0.0p+0,
+    0x1.b6db6db6db6dbp-7, 0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x0.0p+0, 0x1.f8af8af8af8b0p-5, -0x1.1d41d41d41d42p-5,
+    -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x0.0p+0, 0x1.1d41d41d41d42p-5, -0x1.f8af8af8af8b0p-5,
+    -0x1.0750750750750p-6, 0x0.0p+0, 0x1.0750750750750p-6, 0x0.0p+0, -0x1.7297297297297p-7, 0x1.7297297297297p-7,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.b6db6db6db6dbp-7, 0x1.b6db6db6db6dbp-7,
+    -0x1.1d41d41d41d42p-5, 0x1.f8af8af8af8b0p-5, -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7, 0x1.1d41d41d41d42p-5, -0x1.f8af8af8af8b0p-5,
+    0x0.0p+0, 0x0.0p+0, -0x1.0750750750750p-6, 0x1.0750750750750p-6, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, -0x1.b6db6db6db6dbp-7, 0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, -0x1.8af8af8af8af9p-5, -0x1.283a83a83a83bp-4, -0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-4,
+    0x1.8af8af8af8af9p-5, 0x1.283a83a83a83bp-4, 0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-4, 0x0.0p+0, 0x0.0p+0,
+    0x1.edb6db6db6db7p-3, -0x1.edb6db6db6db7p-3, 0x0.0p+0, 0x0.0p+0, -0x1.b6db6db6db6dbp-7, 0x1.b6db6db6db6dbp-7,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, -0x1.283a83a83a83bp-4, 0x1.8af8af8af8af9p-3,
+    -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-6, 0x1.283a83a83a83bp-4, -0x1.8af8af8af8af9p-3, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6,
+    0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-4, -0x1.8af8af8af8af9p-4, 0x0.0p+0, 0x0.0p+0,
+    -0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x1.b6db6db6db6dbp-7, 0x0.0p+0, -0x1.8af8af8af8af9p-5, -0x1.283a83a83a83bp-4,
+    0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-4, -0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5, 0x1.283a83a83a83bp-4,
+    0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-4, 0x1.edb6db6db6db7p-3, 0x0.0p+0,
+    -0x1.edb6db6db6db7p-3, 0x0.0p+0, -0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x1.b6db6db6db6dbp-7, 0x0.0p+0,
+    -0x1.283a83a83a83bp-4, 0x1.8af8af8af8af9p-3, 0x0.0p+0, 0x0.0p+0, -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-6,
+    0x1.283a83a83a83bp-4, -0x1.8af8af8af8af9p-3, 0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6,
+    0x1.8af8af8af8af9p-4, 0x0.0p+0, -0x1.8af8af8af8af9p-4, 0x0.0p+0, -0x1.b6db6db6db6dbp-6, 0x1.f8af8af8af8b0p-5,
+    -0x1.1d41d41d41d42p-5, 0x0.0p+0, -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-4, -0x1.8af8af8af8af9p-6,
+    0x1.8af8af8af8af9p-3, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5,
+    0x1.8af8af8af8af9p-4, -0x1.8af8af8af8af9p-3, 0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-5, -0x1.edb6db6db6db7p-3, -0x1.edb6db6db6db7p-3,
+    -0x1.b6db6db6db6dbp-6, -0x1.1d41d41d41d42p-5, 0x1.f8af8af8af8b0p-5, 0x0.0p+0, 0x1.8af8af8af8af9p-4, -0x1.8af8af8af8af9p-6,
+    -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-3, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5,
+    0x1.8af8af8af8af9p-4, -0x1.8af8af8af8af9p-3, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-4, -0x1.edb6db6db6db7p-3,
+    0x1.8af8af8af8af9p-5, -0x1.edb6db6db6db7p-3, -0x1.1d41d41d41d42p-4, -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7, 0x0.0p+0,
+    0x1.8af8af8af8af9p-5, 0x1.283a83a83a83bp-4, 0x1.8af8af8af8af9p-5, 0x1.283a83a83a83bp-4, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5,
+    0x1.edb6db6db6db7p-2, -0x1.283a83a83a83bp-3, 0x1.283a83a83a83bp-3, 0x0.0p+0, 0x1.283a83a83a83bp-3, 0x0.0p+0,
+    0x1.8af8af8af8af9p-4, -0x1.599999999999ap-2, -0x1.599999999999ap-2, -0x1.283a83a83a83bp-2, 0x1.b6db6db6db6dbp-6, -0x1.b6db6db6db6dbp-7,
+    -0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x1.283a83a83a83bp-4, -0x1.8af8af8af8af9p-3, 0x1.283a83a83a83bp-4, -0x1.8af8af8af8af9p-3,
+    0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5, -0x1.283a83a83a83bp-3, 0x1.8af8af8af8af9p-2, -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-6,
+    -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-3, 0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-4, 0x0.0p+0,
+    -0x1.0cccccccccccdp-3, 0x0.0p+0, 0x1.1d41d41d41d42p-5, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-6,
+    0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-4, 0x1.283a83a83a83bp-3, -0x1.8af8af8af8af9p-6,
+    0x1.283a83a83a83bp-2, -0x1.8af8af8af8af9p-3, 0x1.edb6db6db6db7p-3, -0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-3,
+    -0x1.8af8af8af8af9p-5, -0x1.599999999999ap-2, 0x1.f8af8af8af8b0p-5, 0x0.0p+0, -0x1.f8af8af8af8b0p-5, 0x0.0p+0,
+    -0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-3,
+    0x0.0p+0, -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-3, 0x1.8af8af8af8af9p-3, -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-5,
+    0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-4, -0x1.8af8af8af8af9p-5, 0x1.edb6db6db6db7p-3, -0x1.0cccccccccccdp-3, 0x1.1d41d41d41d42p-5,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-6,
+    0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-5, 0x1.283a83a83a83bp-3, -0x1.8af8af8af8af9p-6, 0x1.edb6db6db6db7p-3, -0x1.8af8af8af8af9p-5,
+    0x1.283a83a83a83bp-2, -0x1.8af8af8af8af9p-3, 0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-3, -0x1.599999999999ap-2,
+    0x1.f8af8af8af8b0p-5, -0x1.f8af8af8af8b0p-5, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    -0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-3, 0x1.8af8af8af8af9p-5, 0x0.0p+0, -0x1.8af8af8af8af9p-6,
+    -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-3, 0x1.8af8af8af8af9p-3, 0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-5,
+    0x1.8af8af8af8af9p-4, 0x1.edb6db6db6db7p-3, -0x1.0750750750750p-4, -0x1.0750750750750p-6, -0x1.0750750750750p-6, 0x0.0p+0,
+    0x1.edb6db6db6db7p-3, 0x1.8af8af8af8af9p-4, 0x1.edb6db6db6db7p-3, 0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-4,
+    0x1.8af8af8af8af9p-4, -0x1.8af8af8af8af9p-3, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5,
+    0x1.283a83a83a83bp-1, -0x1.283a83a83a83bp-1, -0x1.283a83a83a83bp-1, -0x1.283a83a83a83bp-2, 0x1.4924924924925p-4, 0x0.0p+0,
+    0x1.0750750750750p-6, 0x0.0p+0, -0x1.edb6db6db6db7p-3, -0x1.8af8af8af8af9p-4, 0x0.0p+0, 0x0.0p+0,
+    0x1.8af8af8af8af9p-5, -0x1.edb6db6db6db7p-3, -0x1.599999999999ap-2, 0x1.8af8af8af8af9p-4, -0x1.8af8af8af8af9p-3, 0x1.8af8af8af8af9p-4,
+    -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-5, -0x1.283a83a83a83bp-1, 0x1.283a83a83a83bp-1, 0x1.283a83a83a83bp-1, 0x1.283a83a83a83bp-2,
+    0x1.4924924924925p-4, 0x1.0750750750750p-6, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    -0x1.edb6db6db6db7p-3, -0x1.8af8af8af8af9p-4, -0x1.edb6db6db6db7p-3, 0x1.8af8af8af8af9p-5, -0x1.599999999999ap-2, 0x1.8af8af8af8af9p-4,
+    -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-3, 0x1.8af8af8af8af9p-4, -0x1.283a83a83a83bp-1, 0x1.283a83a83a83bp-1,
+    0x1.283a83a83a83bp-1, 0x1.283a83a83a83bp-2, 0x1.8af8af8af8af9p-4, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, -0x1.edb6db6db6db7p-3, -0x1.edb6db6db6db7p-3,
+    -0x1.283a83a83a83bp-2, 0x0.0p+0, -0x1.599999999999ap-2, 0x1.edb6db6db6db7p-3, -0x1.599999999999ap-2, 0x1.edb6db6db6db7p-3,
+    -0x1.283a83a83a83bp-2, 0x1.283a83a83a83bp-2, 0x1.283a83a83a83bp-2, 0x1.283a83a83a83bp-1, 0x1.e79e79e79e79ep-4, -0x1.7297297297297p-7,
+    0x0.0p+0, -0x1.7297297297297p-7, -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-6, -0x1.b6db6db6db6dbp-6,
+    -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7, -0x1.0cccccccccccdp-3, 0x1.f8af8af8af8b0p-5, -0x1.1d41d41d41d42p-4, 0x1.b6db6db6db6dbp-6,
+    -0x1.0cccccccccccdp-3, 0x1.f8af8af8af8b0p-5, -0x1.0750750750750p-4, 0x1.4924924924925p-4, 0x1.8af8af8af8af9p-4, 0x1.4924924924925p-4,
+    -0x1.7297297297297p-7, 0x0.0p+0, 0x0.0p+0, 0x1.7297297297297p-7, 0x1.b6db6db6db6dbp-7, 0x1.b6db6db6db6dbp-7,
+    0x1.f8af8af8af8b0p-5, -0x1.1d41d41d41d42p-5, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7, 0x1.1d41d41d41d42p-5, -0x1.f8af8af8af8b0p-5, -0x1.0750750750750p-6, 0x0.0p+0,
+    0x0.0p+0, 0x1.0750750750750p-6, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, -0x1.7297297297297p-7, 0x1.7297297297297p-7,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, -0x1.1d41d41d41d42p-5, 0x1.f8af8af8af8b0p-5,
+    0x1.b6db6db6db6dbp-7, 0x1.b6db6db6db6dbp-7, 0x1.1d41d41d41d42p-5, -0x1.f8af8af8af8b0p-5, -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7,
+    0x0.0p+0, 0x0.0p+0, -0x1.0750750750750p-6, 0x1.0750750750750p-6, 0x0.0p+0, 0x0.0p+0,
+    -0x1.b6db6db6db6dbp-7, 0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-6, -0x1.283a83a83a83bp-4, 0x1.8af8af8af8af9p-3, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6,
+    0x1.283a83a83a83bp-4, -0x1.8af8af8af8af9p-3, 0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-4, -0x1.8af8af8af8af9p-4,
+    0x0.0p+0, 0x0.0p+0, -0x1.b6db6db6db6dbp-7, 0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, -0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-4, -0x1.8af8af8af8af9p-5, -0x1.283a83a83a83bp-4,
+    0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-5, 0x1.283a83a83a83bp-4, 0x0.0p+0, 0x0.0p+0,
+    0x1.edb6db6db6db7p-3, -0x1.edb6db6db6db7p-3, 0x0.0p+0, 0x0.0p+0, -0x1.b6db6db6db6dbp-6, 0x1.f8af8af8af8b0p-5,
+    0x0.0p+0, -0x1.1d41d41d41d42p-5, -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-3, 0x1.8af8af8af8af9p-5,
+    0x1.8af8af8af8af9p-4, -0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5,
+    0x1.8af8af8af8af9p-4, -0x1.8af8af8af8af9p-3, 0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-5, -0x1.edb6db6db6db7p-3, -0x1.edb6db6db6db7p-3,
+    -0x1.b6db6db6db6dbp-6, -0x1.1d41d41d41d42p-5, 0x0.0p+0, 0x1.f8af8af8af8b0p-5, -0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-4,
+    0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-3, -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-4, -0x1.8af8af8af8af9p-3,
+    0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-4, -0x1.edb6db6db6db7p-3,
+    -0x1.edb6db6db6db7p-3, 0x1.8af8af8af8af9p-5, -0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x0.0p+0, 0x1.b6db6db6db6dbp-7,
+    -0x1.283a83a83a83bp-4, -0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-4, -0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-5, 0x1.283a83a83a83bp-4, 0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-4,
+    0x1.edb6db6db6db7p-3, 0x0.0p+0, 0x0.0p+0, -0x1.edb6db6db6db7p-3, -0x1.b6db6db6db6dbp-7, 0x0.0p+0,
+    0x0.0p+0, 0x1.b6db6db6db6dbp-7, 0x1.8af8af8af8af9p-3, -0x1.283a83a83a83bp-4, -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-6,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x1.283a83a83a83bp-4, -0x1.8af8af8af8af9p-3,
+    0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-4, 0x0.0p+0, 0x0.0p+0, -0x1.8af8af8af8af9p-4,
+    -0x1.0cccccccccccdp-3, 0x0.0p+0, 0x0.0p+0, 0x1.1d41d41d41d42p-5, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-5,
+    0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-4, 0x0.0p+0, 0x0.0p+0, 0x1.283a83a83a83bp-2, -0x1.8af8af8af8af9p-3,
+    0x1.283a83a83a83bp-3, -0x1.8af8af8af8af9p-6, 0x1.edb6db6db6db7p-3, -0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-3,
+    -0x1.599999999999ap-2, -0x1.8af8af8af8af9p-5, 0x1.f8af8af8af8b0p-5, 0x0.0p+0, 0x0.0p+0, -0x1.f8af8af8af8b0p-5,
+    0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-3, 0x0.0p+0, 0x0.0p+0,
+    -0x1.8af8af8af8af9p-3, 0x1.8af8af8af8af9p-3, 0x0.0p+0, -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-5,
+    0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-4, 0x1.edb6db6db6db7p-3, -0x1.8af8af8af8af9p-5, -0x1.1d41d41d41d42p-4, -0x1.b6db6db6db6dbp-7,
+    0x0.0p+0, -0x1.b6db6db6db6dbp-7, 0x1.283a83a83a83bp-4, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5,
+    0x1.8af8af8af8af9p-5, 0x1.283a83a83a83bp-4, 0x1.283a83a83a83bp-3, 0x0.0p+0, 0x1.edb6db6db6db7p-2, -0x1.283a83a83a83bp-3,
+    0x1.283a83a83a83bp-3, 0x0.0p+0, 0x1.8af8af8af8af9p-4, -0x1.599999999999ap-2, -0x1.283a83a83a83bp-2, -0x1.599999999999ap-2,
+    0x1.b6db6db6db6dbp-6, -0x1.b6db6db6db6dbp-7, 0x0.0p+0, -0x1.b6db6db6db6dbp-7, -0x1.8af8af8af8af9p-3, 0x1.283a83a83a83bp-4,
+    0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5, 0x1.283a83a83a83bp-4, -0x1.8af8af8af8af9p-3, -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-6,
+    -0x1.283a83a83a83bp-3, 0x1.8af8af8af8af9p-2, -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-3, 0x1.8af8af8af8af9p-4,
+    0x0.0p+0, 0x1.8af8af8af8af9p-4, -0x1.0cccccccccccdp-3, 0x1.1d41d41d41d42p-5, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-6,
+    0x1.edb6db6db6db7p-3, -0x1.8af8af8af8af9p-5, 0x1.283a83a83a83bp-3, -0x1.8af8af8af8af9p-6, 0x1.283a83a83a83bp-2, -0x1.8af8af8af8af9p-3,
+    0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-5, -0x1.599999999999ap-2, -0x1.8af8af8af8af9p-3, 0x1.f8af8af8af8b0p-5, -0x1.f8af8af8af8b0p-5,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, -0x1.8af8af8af8af9p-3, 0x1.8af8af8af8af9p-5,
+    -0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-5, 0x0.0p+0, -0x1.8af8af8af8af9p-6,
+    -0x1.8af8af8af8af9p-3, 0x1.8af8af8af8af9p-3, 0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-5, 0x1.edb6db6db6db7p-3, 0x1.8af8af8af8af9p-4,
+    -0x1.0750750750750p-4, -0x1.0750750750750p-6, 0x0.0p+0, -0x1.0750750750750p-6, 0x1.8af8af8af8af9p-4, 0x1.edb6db6db6db7p-3,
+    0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-4, 0x1.edb6db6db6db7p-3, 0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5,
+    0x1.8af8af8af8af9p-4, -0x1.8af8af8af8af9p-3, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5, 0x1.283a83a83a83bp-1, -0x1.283a83a83a83bp-1,
+    -0x1.283a83a83a83bp-2, -0x1.283a83a83a83bp-1, 0x1.4924924924925p-4, 0x0.0p+0, 0x0.0p+0, 0x1.0750750750750p-6,
+    -0x1.8af8af8af8af9p-4, -0x1.edb6db6db6db7p-3, 0x1.8af8af8af8af9p-5, -0x1.edb6db6db6db7p-3, 0x0.0p+0, 0x0.0p+0,
+    -0x1.8af8af8af8af9p-3, 0x1.8af8af8af8af9p-4, -0x1.599999999999ap-2, 0x1.8af8af8af8af9p-4, -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-5,
+    -0x1.283a83a83a83bp-1, 0x1.283a83a83a83bp-1, 0x1.283a83a83a83bp-2, 0x1.283a83a83a83bp-1, 0x1.8af8af8af8af9p-4, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, -0x1.edb6db6db6db7p-3, -0x1.edb6db6db6db7p-3,
+    0x0.0p+0, 0x0.0p+0, -0x1.599999999999ap-2, 0x1.edb6db6db6db7p-3, -0x1.283a83a83a83bp-2, 0x0.0p+0,
+    -0x1.599999999999ap-2, 0x1.edb6db6db6db7p-3, -0x1.283a83a83a83bp-2, 0x1.283a83a83a83bp-2, 0x1.283a83a83a83bp-1, 0x1.283a83a83a83bp-2,
+    0x1.4924924924925p-4, 0x1.0750750750750p-6, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    -0x1.edb6db6db6db7p-3, 0x1.8af8af8af8af9p-5, -0x1.edb6db6db6db7p-3, -0x1.8af8af8af8af9p-4, -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-5,
+    -0x1.599999999999ap-2, 0x1.8af8af8af8af9p-4, -0x1.8af8af8af8af9p-3, 0x1.8af8af8af8af9p-4, -0x1.283a83a83a83bp-1, 0x1.283a83a83a83bp-1,
+    0x1.283a83a83a83bp-2, 0x1.283a83a83a83bp-1, 0x1.e79e79e79e79ep-4, 0x0.0p+0, -0x1.7297297297297p-7, -0x1.7297297297297p-7,
+    -0x1.b6db6db6db6dbp-6, -0x1.b6db6db6db6dbp-6, -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7,
+    -0x1.0cccccccccccdp-3, 0x1.f8af8af8af8b0p-5, -0x1.0cccccccccccdp-3, 0x1.f8af8af8af8b0p-5, -0x1.1d41d41d41d42p-4, 0x1.b6db6db6db6dbp-6,
+    -0x1.0750750750750p-4, 0x1.8af8af8af8af9p-4, 0x1.4924924924925p-4, 0x1.4924924924925p-4, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    -0x1.7297297297297p-7, 0x0.0p+0, 0x0.0p+0, 0x1.7297297297297p-7, 0x1.f8af8af8af8b0p-5, -0x1.1d41d41d41d42p-5,
+    0x1.b6db6db6db6dbp-7, 0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x1.1d41d41d41d42p-5, -0x1.f8af8af8af8b0p-5, -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7, -0x1.0750750750750p-6, 0x0.0p+0,
+    0x0.0p+0, 0x1.0750750750750p-6, -0x1.7297297297297p-7, 0x0.0p+0, 0x1.7297297297297p-7, 0x0.0p+0,
+    -0x1.1d41d41d41d42p-5, 0x1.f8af8af8af8b0p-5, 0x0.0p+0, 0x0.0p+0, 0x1.b6db6db6db6dbp-7, 0x1.b6db6db6db6dbp-7,
+    0x1.1d41d41d41d42p-5, -0x1.f8af8af8af8b0p-5, 0x0.0p+0, 0x0.0p+0, -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7,
+    -0x1.0750750750750p-6, 0x0.0p+0, 0x1.0750750750750p-6, 0x0.0p+0, -0x1.b6db6db6db6dbp-6, 0x0.0p+0,
+    0x1.f8af8af8af8b0p-5, -0x1.1d41d41d41d42p-5, 0x1.8af8af8af8af9p-3, 0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-5,
+    -0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-4, -0x1.8af8af8af8af9p-3,
+    0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-4, -0x1.edb6db6db6db7p-3, 0x1.8af8af8af8af9p-5, -0x1.edb6db6db6db7p-3,
+    -0x1.b6db6db6db6dbp-6, 0x0.0p+0, -0x1.1d41d41d41d42p-5, 0x1.f8af8af8af8b0p-5, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-3,
+    -0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-4, -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-4, -0x1.8af8af8af8af9p-3,
+    0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-4, -0x1.edb6db6db6db7p-3,
+    -0x1.edb6db6db6db7p-3, 0x1.8af8af8af8af9p-5, -0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x1.b6db6db6db6dbp-7, 0x0.0p+0,
+    -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-3, -0x1.283a83a83a83bp-4,
+    0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, 0x0.0p+0, 0x0.0p+0, 0x1.283a83a83a83bp-4, -0x1.8af8af8af8af9p-3,
+    0x1.8af8af8af8af9p-4, 0x0.0p+0, -0x1.8af8af8af8af9p-4, 0x0.0p+0, -0x1.b6db6db6db6dbp-7, 0x0.0p+0,
+    0x1.b6db6db6db6dbp-7, 0x0.0p+0, -0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-4, 0x0.0p+0, 0x0.0p+0,
+    -0x1.283a83a83a83bp-4, -0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-4, 0x0.0p+0, 0x0.0p+0,
+    0x1.8af8af8af8af9p-5, 0x1.283a83a83a83bp-4, 0x1.edb6db6db6db7p-3, 0x0.0p+0, -0x1.edb6db6db6db7p-3, 0x0.0p+0,
+    -0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x0.0p+0, 0x1.b6db6db6db6dbp-7, -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-6,
+    0x1.8af8af8af8af9p-3, -0x1.283a83a83a83bp-4, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0,
+    0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-6, 0x1.283a83a83a83bp-4, -0x1.8af8af8af8af9p-3, 0x1.8af8af8af8af9p-4, 0x0.0p+0,
+    0x0.0p+0, -0x1.8af8af8af8af9p-4, -0x1.b6db6db6db6dbp-7, 0x0.0p+0, 0x0.0p+0, 0x1.b6db6db6db6dbp-7,
+    0x1.8af8af8af8af9p-4, -0x1.8af8af8af8af9p-5, -0x1.283a83a83a83bp-4, -0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x0.0p+0,
+    0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-5, 0x1.283a83a83a83bp-4,
+    0x1.edb6db6db6db7p-3, 0x0.0p+0, 0x0.0p+0, -0x1.edb6db6db6db7p-3, -0x1.0cccccccccccdp-3, 0x0.0p+0,
+    0x0.0p+0, 0x1.1d41d41d41d42p-5, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-5,
+    0x0.0p+0, 0x0.0p+0, 0x1.283a83a83a83bp-2, -0x1.8af8af8af8af9p-3, 0x1.edb6db6db6db7p-3, -0x1.8af8af8af8af9p-5,
+    0x1.283a83a83a83bp-3, -0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-5, -0x1.599999999999ap-2, -0x1.8af8af8af8af9p-3, -0x1.8af8af8af8af9p-5,
+    0x1.f8af8af8af8b0p-5, 0x0.0p+0, 0x0.0p+0, -0x1.f8af8af8af8b0p-5, 0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-3,
+    0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-4, 0x0.0p+0, 0x0.0p+0, -0x1.8af8af8af8af9p-3, 0x1.8af8af8af8af9p-3,
+    -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-5, 0x0.0p+0, -0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-5, 0x1.edb6db6db6db7p-3,
+    0x1.8af8af8af8af9p-4, -0x1.8af8af8af8af9p-5, -0x1.0cccccccccccdp-3, 0x0.0p+0, 0x1.1d41d41d41d42p-5, 0x0.0p+0,
+    0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x0.0p+0, 0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-5,
+    0x1.edb6db6db6db7p-3, -0x1.8af8af8af8af9p-5, 0x1.283a83a83a83bp-2, -0x1.8af8af8af8af9p-3, 0x1.283a83a83a83bp-3, -0x1.8af8af8af8af9p-6,
+    0x1.8af8af8af8af9p-5, -0x1.599999999999ap-2, -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-3, 0x1.f8af8af8af8b0p-5, 0x0.0p+0,
+    -0x1.f8af8af8af8b0p-5, 0x0.0p+0, -0x1.8af8af8af8af9p-3, 0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x0.0p+0,
+    0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-4, -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-3, 0x1.8af8af8af8af9p-3,
+    0x0.0p+0, -0x1.8af8af8af8af9p-6, 0x1.8af8af8af8af9p-5, 0x1.edb6db6db6db7p-3, -0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-4,
+    -0x1.1d41d41d41d42p-4, 0x0.0p+0, -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5,
+    0x1.283a83a83a83bp-4, 0x1.8af8af8af8af9p-5, 0x1.283a83a83a83bp-4, 0x1.8af8af8af8af9p-5, 0x1.283a83a83a83bp-3, 0x0.0p+0,
+    0x1.283a83a83a83bp-3, 0x0.0p+0, 0x1.edb6db6db6db7p-2, -0x1.283a83a83a83bp-3, 0x1.8af8af8af8af9p-4, -0x1.283a83a83a83bp-2,
+    -0x1.599999999999ap-2, -0x1.599999999999ap-2, 0x1.b6db6db6db6dbp-6, 0x0.0p+0, -0x1.b6db6db6db6dbp-7, -0x1.b6db6db6db6dbp-7,
+    0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-3, 0x1.283a83a83a83bp-4, -0x1.8af8af8af8af9p-3, 0x1.283a83a83a83bp-4,
+    -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-6, -0x1.8af8af8af8af9p-6, -0x1.283a83a83a83bp-3, 0x1.8af8af8af8af9p-2,
+    -0x1.8af8af8af8af9p-3, 0x0.0p+0, 0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-4, -0x1.0750750750750p-4, 0x0.0p+0,
+    -0x1.0750750750750p-6, -0x1.0750750750750p-6, 0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-4, 0x1.8af8af8af8af9p-4, 0x1.edb6db6db6db7p-3,
+    0x1.8af8af8af8af9p-4, 0x1.edb6db6db6db7p-3, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5, 0x1.8af8af8af8af9p-5,
+    0x1.8af8af8af8af9p-4, -0x1.8af8af8af8af9p-3, 0x1.283a83a83a83bp-1, -0x1.283a83a83a83bp-2, -0x1.283a83a83a83bp-1, -0x1.283a83a83a83bp-1,
+    0x1.8af8af8af8af9p-4, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, -0x1.edb6db6db6db7p-3, -0x1.edb6db6db6db7p-3,
+    0x0.0p+0, 0x0.0p+0, 0x0.0p+0, 0x0.0p+0, -0x1.599999999999ap-2, 0x1.edb6db6db6db7p-3,
+    -0x1.599999999999ap-2, 0x1.edb6db6db6db7p-3, -0x1.283a83a83a83bp-2, 0x0.0p+0, -0x1.283a83a83a83bp-2, 0x1.283a83a83a83bp-1,
+    0x1.283a83a83a83bp-2, 0x1.283a83a83a83bp-2, 0x1.4924924924925p-4, 0x0.0p+0, 0x0.0p+0, 0x1.0750750750750p-6,
+    0x1.8af8af8af8af9p-5, -0x1.edb6db6db6db7p-3, -0x1.8af8af8af8af9p-4, -0x1.edb6db6db6db7p-3, 0x0.0p+0, 0x0.0p+0,
+    -0x1.8af8af8af8af9p-3, 0x1.8af8af8af8af9p-4, -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-5, -0x1.599999999999ap-2, 0x1.8af8af8af8af9p-4,
+    -0x1.283a83a83a83bp-1, 0x1.283a83a83a83bp-2, 0x1.283a83a83a83bp-1, 0x1.283a83a83a83bp-1, 0x1.4924924924925p-4, 0x0.0p+0,
+    0x1.0750750750750p-6, 0x0.0p+0, -0x1.edb6db6db6db7p-3, 0x1.8af8af8af8af9p-5, 0x0.0p+0, 0x0.0p+0,
+    -0x1.8af8af8af8af9p-4, -0x1.edb6db6db6db7p-3, -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-5, -0x1.8af8af8af8af9p-3, 0x1.8af8af8af8af9p-4,
+    -0x1.599999999999ap-2, 0x1.8af8af8af8af9p-4, -0x1.283a83a83a83bp-1, 0x1.283a83a83a83bp-2, 0x1.283a83a83a83bp-1, 0x1.283a83a83a83bp-1,
+};
+
 // P2 stiffness with a P1 coefficient: q[m*6+s] = k_m * Ghat_s,
 // Ghat = |detJ| K K^T (s over (00,11,22,01,02,12)).  Calls emit(i, j, value)
 // for the 55 unique entries i <= j (FP32: off-diagonal entries first, then
