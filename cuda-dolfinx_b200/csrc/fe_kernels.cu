@@ -284,8 +284,9 @@ __global__ void __launch_bounds__(NT) k_mat_p2_atomic(const MatArgs a) {
 constexpr int kCoalThreads = 64;
 
 // STAGE: the CTA's byte maps copied to shared memory first (6.4 KB), else
-// read from global memory (L1) in the reduction loop, which leaves room for a
-// seventh CTA per SM
+// fetched as words and handed out by shuffles in the reduction loop, which
+// leaves room for a seventh CTA per SM (measured slower on B200: P2 n=96
+// 2.66 against 2.46 ms)
 template <bool STAGE>
 struct P2CoalSmem {
   __align__(16) uint8_t spos[STAGE ? kCoalThreads * 100 : 16];
@@ -367,18 +368,54 @@ __device__ __forceinline__ void p2_coal_tile(const MatArgs& a, const int64_t c0,
     eu[r] = lo * (21 - lo) / 2 + (hi - lo);
   }
   double* __restrict__ vals = a.values;
+  if constexpr (STAGE) {
 #pragma unroll 2
-  for (int q = w0; q < w0 + wcells; ++q) {
-    const bool cmask = (smc[q] >> j) & 1u;
-    const int32_t* rq = srp + q * 10;
-    const uint8_t* pq = STAGE ? spos + q * 100 : a.pos + (c0 + q) * 100;
-    const double* Eq = sE + q * 55;
+    for (int q = w0; q < w0 + wcells; ++q) {
+      const bool cmask = (smc[q] >> j) & 1u;
+      const int32_t* rq = srp + q * 10;
+      const uint8_t* pq = spos + q * 100;
+      const double* Eq = sE + q * 55;
 #pragma unroll
-    for (int r = 0; r < 4; ++r) {
-      if (ei[r] < 0 || cmask) continue;
-      const int rs = rq[ei[r]];
-      if (rs < 0) continue;
-      atomicAdd(vals + rs + pq[ei[r] * 10 + j], Eq[eu[r]]);
+      for (int r = 0; r < 4; ++r) {
+        if (ei[r] < 0 || cmask) continue;
+        const int rs = rq[ei[r]];
+        if (rs < 0) continue;
+        atomicAdd(vals + rs + pq[ei[r] * 10 + j], Eq[eu[r]]);
+      }
+    }
+  } else {
+    // the slot bytes unstaged: lane w < 25 loads word w of a cell's 25 (one
+    // coalesced 100-byte load per cell, one cell ahead, into alternating
+    // registers), and byte b = 10 ei + j comes from lane b / 4 by a shuffle
+    auto word_of = [&](int q) -> uint32_t {
+      const uint32_t* src = reinterpret_cast<const uint32_t*>(a.pos + (c0 + q) * 100);  // 100 c: 4-byte aligned
+      return lane < 25 ? __ldg(src + lane) : 0u;
+    };
+    int bi[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) bi[r] = ei[r] < 0 ? 0 : ei[r] * 10 + j;
+    auto cell = [&](int q, uint32_t w) {
+      const bool cmask = (smc[q] >> j) & 1u;
+      const int32_t* rq = srp + q * 10;
+      const double* Eq = sE + q * 55;
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const uint32_t word = __shfl_sync(0xffffffffu, w, bi[r] >> 2);
+        if (ei[r] < 0 || cmask) continue;
+        const int rs = rq[ei[r]];
+        if (rs < 0) continue;
+        atomicAdd(vals + rs + ((word >> (8 * (bi[r] & 3))) & 0xffu), Eq[eu[r]]);
+      }
+    };
+    const int qend = w0 + wcells;
+    uint32_t wa = 0u, wb = 0u;
+    if (wcells > 0) wa = word_of(w0);
+    for (int q = w0; q < qend; q += 2) {
+      if (q + 1 < qend) wb = word_of(q + 1);
+      cell(q, wa);
+      if (q + 1 >= qend) break;
+      if (q + 2 < qend) wa = word_of(q + 2);
+      cell(q + 1, wb);
     }
   }
 }
@@ -387,7 +424,7 @@ __device__ __forceinline__ void p2_coal_tile(const MatArgs& a, const int64_t c0,
 // is then 168 (the P1-coefficient kernel takes 168 instead of 128; measured
 // 1 % faster at P2 n=96 than with the cap of 7 CTAs)
 template <int COEF, typename T, bool STAGE>
-__global__ void __launch_bounds__(kCoalThreads, 6) k_mat_p2_coal(const MatArgs a) {
+__global__ void __launch_bounds__(kCoalThreads, STAGE ? 6 : 7) k_mat_p2_coal(const MatArgs a) {
   __shared__ P2CoalSmem<STAGE> S;
   p2_coal_tile<COEF, T, STAGE>(a, blockIdx.x * (int64_t)kCoalThreads, S);
 }

@@ -393,6 +393,26 @@ def test_atomic_launch_shapes(kind, shape):
         _lib.check(_lib.lib.fe_form_set_launch(a.cuda_form, 48, 1), "fe_form_set_launch")
 
 
+@pytest.mark.parametrize("stage", [1, 0])
+def test_coalesced_p2_slot_byte_fetch(stage):
+    # the coalesced P2 kernel with its slot bytes staged in shared memory (1)
+    # or fetched as words and handed out by shuffles (0), on P2 n=9 (4,374
+    # cells: a partial last CTA)
+    from cudolfinx import _lib
+
+    P = fo.build_problem("p2", 9, seed=23)
+    S = fo.solve_system(P)
+    M = mirror_problem(P)
+    cx = M["cx"]
+    asm = cx.CUDAAssembler()
+    a = cx.form(M["a"])
+    _lib.check(_lib.lib.fe_form_set_launch(a.cuda_form, 64, stage), "fe_form_set_launch")
+    A = asm.assemble_matrix(a, bcs=asm.pack_bcs([M["bc"]]), variant="coalesced")
+    A.assemble()
+    ok, worst = tolerance_check(A.values.cpu().numpy(), S["A"], S["A_bound"])
+    assert ok, worst
+
+
 @pytest.mark.parametrize("kind,n", [("p1", 7), ("p1k", 8)])
 @pytest.mark.parametrize("bcs", ["same", "rows-only", "none"])
 def test_block_variant_bc_paths(kind, n, bcs):
