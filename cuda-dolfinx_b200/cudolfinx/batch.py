@@ -27,6 +27,7 @@ CANDIDATES = {
     "P1_STIFFNESS": ("atomic", "block", "tile"),
     "P2_STIFFNESS": ("atomic", "block", "grouped", "coalesced"),
     "VP2_ELASTICITY": ("coalesced", "atomic", "atomic-full"),
+    "P3_STIFFNESS": ("coalesced", "atomic"),  # coalesced: FP64 element tensors only (skipped for FP32)
 }
 # launch shapes of the atomic scatter timed per form kind: (cells per CTA,
 # byte maps staged in shared memory)
