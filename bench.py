@@ -551,10 +551,18 @@ def run_gpu(args, rank, world, local_rank):
         coef_bytes = sum(np.asarray(c.x.array).nbytes for c in I2["a"].coefficients + I2["L"].coefficients
                          if hasattr(c, "x"))
 
+        vs2 = torch.cuda.Stream()
+
         def e2e_step():
+            # as in the device leg, the right-hand side (independent of A) on
+            # a second stream, concurrent with the matrix; each call uploads
+            # its form's host coefficients, b is read back after the RHS
+            vs2.wait_stream(stream)
             asm.assemble_matrix(a2, A2, bcs=dbc2)
-            asm.assemble_rhs(L2, a2, dbc2, vec=b2)
-            b2.copy_to_host(bhost)
+            with torch.cuda.stream(vs2):
+                asm.assemble_rhs(L2, a2, dbc2, vec=b2)
+                b2.copy_to_host(bhost)
+            stream.wait_stream(vs2)
 
         for _ in range(max(1, args.warmup)):
             e2e_step()

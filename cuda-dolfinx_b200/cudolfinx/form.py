@@ -24,6 +24,11 @@ DEFAULT_CUDA_JIT_ARGS = {"max_threads_per_block": 1024, "min_blocks_per_multipro
 # on the current stream: for a few hundred kB the extra event round trip costs
 # more than the overlap gains)
 OVERLAP_MIN_BYTES = 1 << 20
+# device copies per uploaded coefficient: an upload fills the copy whose last
+# tracked readers are the oldest, so re-uploading a coefficient (every
+# assembly call uploads its host values, as the reference does) waits for
+# kernels of the calls before the last two, not for the one still running
+COEF_RING = 3
 
 _mesh_cache: dict[int, "DeviceMesh"] = {}
 _dofmap_cache: dict[int, "DeviceDofMap"] = {}
@@ -164,7 +169,10 @@ class CUDAForm:
             _lib.check(_lib.lib.fe_form_set_precision(self._handle, _lib.PREC_FP32), "fe_form_set_precision")
         self._bound_sparsity = None
         self._coef_refs: list = [None] * len(form.coefficients)
-        self._coef_free: list = [None] * len(form.coefficients)  # event after the last tracked read
+        nc = len(form.coefficients)
+        self._coef_ring: list = [None] * nc   # per coefficient: COEF_RING device copies (large uploads)
+        self._coef_slot: list = [0] * nc      # the copy the engine reads now
+        self._coef_free: list = [[None] * COEF_RING for _ in range(nc)]  # per copy: event after its last tracked read
         self._external = getattr(self, "_external", False)
         self._aux_dofmaps: dict = {}
         self.to_device()
@@ -244,10 +252,12 @@ class CUDAForm:
         return self._upload(i, kind, None, arr)
 
     def _upload(self, i: int, kind: int, cmap, arr: np.ndarray):
-        """Host -> device copy of coefficient i on the context's upload stream.
-        It waits only for the last tracked kernel that read the same device
-        buffer (so it overlaps other work still running on the compute stream),
-        or for all work queued on the current stream when that is unknown."""
+        """Host -> device copy of coefficient i on the context's upload stream,
+        into the next of the coefficient's COEF_RING device copies, which the
+        engine then reads in place.  The copy waits only for the last tracked
+        kernels that read that device copy (so it overlaps the kernels still
+        reading the newer copies, on any stream), or for all work queued on
+        the current stream when that is unknown."""
         ctx = self._ctx
         if arr.nbytes < OVERLAP_MIN_BYTES:
             # small copies: the event round trip would cost more than the overlap
@@ -256,13 +266,25 @@ class CUDAForm:
             return None
         self._overlapped = True
         up = ctx.upload_stream()
-        free = self._coef_free[i]
+        ring = self._coef_ring[i]
+        if ring is None or ring[0].numel() != arr.size:
+            # (the old copies carry record_stream marks of their uploads and
+            # readers: the allocator reuses them only after those finish)
+            ring = [torch.empty(arr.size, dtype=torch.float64, device=ctx.torch_device) for _ in range(COEF_RING)]
+            self._coef_ring[i] = ring
+            self._coef_free[i] = [None] * COEF_RING
+        slot = (self._coef_slot[i] + 1) % COEF_RING
+        free = self._coef_free[i][slot]
         if self._external or free is None:
             up.wait_stream(ctx.torch_stream())
         else:
             up.wait_event(free)
-        _lib.check(_lib.lib.fe_form_set_coefficient(self._handle, i, kind, cmap, arr.ctypes.data, arr.size, 0,
+        with torch.cuda.stream(up):
+            ring[slot].copy_(torch.from_numpy(arr), non_blocking=True)
+        ring[slot].record_stream(up)
+        _lib.check(_lib.lib.fe_form_set_coefficient(self._handle, i, kind, cmap, ring[slot].data_ptr(), arr.size, 1,
                                                     up.cuda_stream), "fe_form_set_coefficient")
+        self._coef_slot[i] = slot
         ev = torch.cuda.Event()
         ev.record(up)
         return ev
@@ -285,10 +307,13 @@ class CUDAForm:
         Only forms with side-stream uploads need it."""
         if not getattr(self, "_overlapped", False):
             return
+        cur = self._ctx.torch_stream()
         ev = torch.cuda.Event()
-        ev.record(self._ctx.torch_stream())
+        ev.record(cur)
         for i in range(len(self._coef_free)):
-            self._coef_free[i] = ev
+            self._coef_free[i][self._coef_slot[i]] = ev
+            if self._coef_ring[i] is not None:
+                self._coef_ring[i][self._coef_slot[i]].record_stream(cur)
 
     # -- pattern binding ----------------------------------------------------
     def _bind(self, sparsity):
