@@ -16,7 +16,7 @@ from oracle import fem_oracle as fo
 pytestmark = pytest.mark.gpu
 
 
-def _steps(P, overlapped, nsteps=4):
+def _steps(P, overlapped, nsteps=4, rhs_stream=False):
     M = mirror_problem(P)
     cx = M["cx"]
     asm = cx.CUDAAssembler()
@@ -28,15 +28,22 @@ def _steps(P, overlapped, nsteps=4):
     b = asm.create_vector(L)
     bcs = asm.pack_bcs([M["bc"]])
     outs, mats = [], []
+    side = torch.cuda.Stream() if rhs_stream else None
     for s in range(nsteps):
         k.x.array = k0 * (1.0 + 0.5 * s)
         f.x.array = f0 * (1.0 - 0.25 * s)
+        if side is not None:
+            side.wait_stream(torch.cuda.current_stream())
         asm.assemble_matrix(a, A, bcs=bcs)
-        asm.assemble_vector(L, b)
-        asm.apply_lifting(b, [a], [bcs])
-        asm.set_bc(b, bcs, M["V"])
+        with torch.cuda.stream(side if side is not None else torch.cuda.current_stream()):
+            asm.assemble_vector(L, b)
+            asm.apply_lifting(b, [a], [bcs])
+            asm.set_bc(b, bcs, M["V"])
+            if overlapped:
+                outs.append(b.copy_to_host())
+        if side is not None:
+            torch.cuda.current_stream().wait_stream(side)
         if overlapped:
-            outs.append(b.copy_to_host())
             mats.append(A.values.clone())
         else:
             torch.cuda.synchronize()
@@ -47,11 +54,15 @@ def _steps(P, overlapped, nsteps=4):
     return [o.numpy() if hasattr(o, "numpy") else o for o in outs], [m.cpu().numpy() for m in mats]
 
 
-@pytest.mark.parametrize("kind,n", [("p2", 5), ("p1k", 10)])
-def test_overlapped_transfers_match_synchronous_steps(kind, n):
+# p1k n=28: a DG0 k of 131,712 values (1.05 MB), large enough for the upload
+# stream and the device copies that uploads rotate through; more steps than
+# copies, with the right-hand side on a second stream as well
+@pytest.mark.parametrize("kind,n,rhs_stream", [("p2", 5, False), ("p1k", 10, False), ("p1k", 28, False),
+                                               ("p1k", 28, True)])
+def test_overlapped_transfers_match_synchronous_steps(kind, n, rhs_stream):
     P = fo.build_problem(kind, n, seed=12)
-    b_ovl, A_ovl = _steps(P, True)
-    b_syn, A_syn = _steps(P, False)
+    b_ovl, A_ovl = _steps(P, True, nsteps=5 if n >= 28 else 4, rhs_stream=rhs_stream)
+    b_syn, A_syn = _steps(P, False, nsteps=len(b_ovl))
     for s in range(len(b_syn)):
         Ps = dict(P)
         Ps["k"] = P["k"] * (1.0 + 0.5 * s)
