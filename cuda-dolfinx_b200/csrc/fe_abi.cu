@@ -989,9 +989,10 @@ int fe_assemble_matrix(fe_form a, double* values, fe_bc bc0, fe_bc bc1, double d
     // the atomic path: 0.73 instead of 0.85 ms; P1 n=32: equal).  For P2 the
     // pass costs what the halved reductions save (n=96: 2.80 ms either way),
     // so it keeps both reductions, as does FE_ASM_FULL_SCATTER for every form.
-    // P2 stiffness and vector-P2 elasticity by default with warp-coalesced
-    // reductions (measured on B200 at P2 n=96: 2.44 ms per matrix call against
-    // 2.81 ms for the thread-per-cell reductions, which FE_ASM_ATOMIC keeps)
+    // P2 stiffness, vector-P2 elasticity and FP64 P3 stiffness by default
+    // with warp-coalesced reductions (measured on B200 at P2 n=96: 2.44 ms per
+    // matrix call against 2.81 ms for the thread-per-cell reductions, which
+    // FE_ASM_ATOMIC keeps; P3 n=48: 1.30 against 1.78 ms for the upper mode)
     const bool coalesced = (flags & FE_ASM_COALESCED) ||
                            (!(flags & FE_ASM_ATOMIC) && !view &&
                             (a->kind == FE_FORM_P2_STIFFNESS || a->kind == FE_FORM_VP2_ELASTICITY ||
