@@ -552,11 +552,19 @@ def run_gpu(args, rank, world, local_rank):
                          if hasattr(c, "x"))
 
         vs2 = torch.cuda.Stream()
+        # the fork and join cost more than they overlap on launch-bound sizes
+        # (P1 n=32: 4.9e9 against 6.4-7.0e9 nnz/s in sequence)
+        fork = nnz >= (1 << 22)
 
         def e2e_step():
             # as in the device leg, the right-hand side (independent of A) on
             # a second stream, concurrent with the matrix; each call uploads
             # its form's host coefficients, b is read back after the RHS
+            if not fork:
+                asm.assemble_matrix(a2, A2, bcs=dbc2)
+                asm.assemble_rhs(L2, a2, dbc2, vec=b2)
+                b2.copy_to_host(bhost)
+                return
             vs2.wait_stream(stream)
             asm.assemble_matrix(a2, A2, bcs=dbc2)
             with torch.cuda.stream(vs2):

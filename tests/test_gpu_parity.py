@@ -393,6 +393,47 @@ def test_atomic_launch_shapes(kind, shape):
         _lib.check(_lib.lib.fe_form_set_launch(a.cuda_form, 48, 1), "fe_form_set_launch")
 
 
+def test_coalesced_p3_on_permuted_cells_and_renumbered_dofs():
+    # the coalesced P3 kernel (FP64 default) reads each cell's slot bytes as
+    # words from the byte map: a random cell order and dof numbering give the
+    # oracle's matrix for that numbering
+    from conftest import ensure_library
+    ensure_library()
+    import cudolfinx as cx
+    from cudolfinx import fem
+
+    n = 5
+    P = fo.build_problem("p3", n, seed=29)
+    rng = np.random.default_rng(7)
+    cp = rng.permutation(len(P["cells"]))
+    cells = P["cells"][cp]
+    mesh = fem.Mesh(P["coords"], cells, grid_n=n)
+    V = fem.functionspace(mesh, ("P", 3))
+    dp = rng.permutation(V.num_nodes).astype(np.int32)
+    V.dofs = np.ascontiguousarray(dp[V.dofs])
+    W = fem.functionspace(mesh, ("DG", 0))
+    kc = P["k"][cp]
+    k = fem.Function(W, kc)
+    bdofs = np.sort(dp[P["bc_dofs"]]).astype(np.int32)
+    g = np.zeros(V.num_dofs)
+    g[dp] = P["g"]
+    bc = fem.dirichletbc(fem.Function(V, g), bdofs)
+    asm = cx.CUDAAssembler()
+    a = cx.form(fem.stiffness(V, k))
+    A = asm.assemble_matrix(a, bcs=[bc], variant="coalesced")
+    A.assemble()
+    rp, col = A.sparsity.to_host()
+    rp_o, col_o = fo.sparsity(V.dofs, V.dofs, V.num_nodes)
+    assert np.array_equal(rp, rp_o) and np.array_equal(col, col_o)
+    Ae = fo.p3_stiffness(P["coords"], cells, kc)
+    mk = np.zeros(V.num_dofs, dtype=np.uint8)
+    mk[bdofs] = 1
+    ref = fo.assemble_matrix(Ae, V.dofs, V.dofs, rp_o, col_o, 1, 1, mk, mk, 1.0, bdofs)
+    ok, worst = tolerance_check(A.values.cpu().numpy(), ref,
+                                fo.matrix_bound(Ae, V.dofs, V.dofs, rp_o, col_o, 1, 1, mk, mk))
+    assert ok, worst
+
+
 @pytest.mark.parametrize("stage", [1, 0])
 def test_coalesced_p2_slot_byte_fetch(stage):
     # the coalesced P2 kernel with its slot bytes staged in shared memory (1)
