@@ -1,4 +1,4 @@
-"""Many meshes of different sizes, P1 and P2 mixed, assembled by one CUDA
+"""Many meshes of different sizes, P1, P2 and P3 mixed, assembled by one CUDA
 graph replay (cudolfinx.AssemblyGraph) against the oracle; the variant
 autotuner's choice per item is one of the parity-tested variants."""
 import numpy as np
@@ -11,7 +11,7 @@ from oracle import fem_oracle as fo
 pytestmark = pytest.mark.gpu
 
 CASES = [("p1", 3, "fp64"), ("p2", 2, "fp32"), ("p1", 5, "fp64"), ("p2", 3, "fp64"), ("p1k", 4, "fp64"),
-         ("p2", 4, "fp32")]
+         ("p2", 4, "fp32"), ("p3", 2, "fp64"), ("p3", 3, "fp32")]
 
 
 def _items():
