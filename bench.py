@@ -1479,7 +1479,7 @@ def run_gpu_multimesh(args, rank, world, local_rank):
         a = cx.form(I["a"])
         items.append((a, asm.create_matrix(a), asm.pack_bcs([I["bc"]])))
     t_tune = time.perf_counter()
-    G = cx.AssemblyGraph(items, variants="tune")
+    G = cx.AssemblyGraph(items, variants="tune", branches=args.graph_branches)
     tune_s = time.perf_counter() - t_tune
     G.capture()
     setup_s = time.perf_counter() - t_setup
@@ -1557,7 +1557,8 @@ def run_gpu_multimesh(args, rank, world, local_rank):
         "config": {"workload": MULTI["desc"], "meshes": len(Is), "cells": sum(len(I["cells"]) for I in Is),
                    "nnz": nnz, "ns": [int(I["n"]) for I in Is], "kinds": [I["kind"] for I in Is],
                    "variants_chosen": chosen, "step": "one CUDA graph replay: every mesh's matrix assembly "
-                   "(zero, assemble with BC skip, unit diagonal)", "l2": "inputs larger than L2",
+                   "(zero, assemble with BC skip, unit diagonal)", "graph_branches": args.graph_branches,
+                   "l2": "inputs larger than L2",
                    "parallelism": f"replicas x{world}"},
         "roofline": {"bound": "hbm", "kernel": "graph of matrix assemblies", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "traffic": None, "algorithmic_bytes": alg,
@@ -1922,6 +1923,8 @@ def main():
     ap.add_argument("--variant", choices=["auto", "tile", "atomic", "atomic-full", "sorted-slot", "deterministic",
                                           "row-gather", "block", "grouped", "coalesced"], default="auto")
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--graph-branches", type=int, default=8,
+                    help="multimesh: parallel branches of the captured graph (independent meshes overlap)")
     ap.add_argument("--serve-requests", type=int, default=0, help="serve workload: requests per rate")
     ap.add_argument("--serve-rates", default="", help="serve workload: comma-separated arrival rates (req/s)")
     ap.add_argument("--serve-nmax", type=int, default=0, help="serve workload: largest n (default 48)")
