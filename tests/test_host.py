@@ -264,3 +264,29 @@ def test_fused_rhs_validates_its_arguments_on_the_host():
 
     st = _lib.lib.fe_assemble_rhs(None, None, None, None, None, 1.0, 0, None)
     assert st != 0 and "null form" in _lib.last_error()
+
+
+def test_assembly_graph_branches_balance_nonzeros_and_keep_forms_together():
+    # the capture's split of the items over parallel branches: each form's
+    # items on one branch, largest forms first onto the least-loaded branch
+    from types import SimpleNamespace
+
+    ensure_library()
+    from cudolfinx.batch import AssemblyGraph
+
+    forms = [object() for _ in range(6)]
+    sizes = [900, 500, 400, 300, 200, 100]
+    g = object.__new__(AssemblyGraph)
+    g.items = [{"a": f, "mat": SimpleNamespace(sparsity=SimpleNamespace(nnz=n))} for f, n in zip(forms, sizes)]
+    g.items.append({"a": forms[0], "mat": SimpleNamespace(sparsity=SimpleNamespace(nnz=50))})  # a second item of form 0
+    groups = g._branch_items(3)
+    assert sorted(len(x) for x in groups) == [2, 2, 3]
+    flat = [it for grp in groups for it in grp]
+    assert len(flat) == len(g.items) and all(any(it is x for x in flat) for it in g.items)
+    for grp in groups:  # both items of form 0 share a branch
+        if any(it["a"] is forms[0] for it in grp):
+            assert sum(it["a"] is forms[0] for it in grp) == 2
+    loads = sorted(sum(it["mat"].sparsity.nnz for it in grp) for grp in groups)
+    assert loads == [700, 800, 950]
+    assert len(g._branch_items(1)) == 1
+    assert len(g._branch_items(16)) == 6  # no empty branches
